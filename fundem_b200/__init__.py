@@ -1,0 +1,345 @@
+"""fundem_b200 -- B200-native level-set DEM timestep.
+
+Python bindings over the C ABI of libfundem_b200.so (include/fundem_b200.h).
+The library is built in-tree (`python -m fundem_b200.build`) and loaded from
+fundem_b200/_lib/; there is no fallback: if the library or a CUDA device is
+missing, the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libfundem_b200.so")
+
+FP64, FP32_MIXED = 0, 1
+PP, PW, GX, GY, GXY = 0, 1, 2, 3, 4
+
+# every symbol declared in include/fundem_b200.h
+EXPORTS = [
+    "fundem_version", "fundem_status_string", "fundem_create", "fundem_destroy", "fundem_set_precision",
+    "fundem_set_records", "fundem_add_material", "fundem_add_geometry", "fundem_mass_properties",
+    "fundem_add_objects", "fundem_set_wall_motion", "fundem_move", "fundem_add_bonds", "fundem_set_periodic",
+    "fundem_setup", "fundem_detect", "fundem_step", "fundem_step_begin", "fundem_step_end", "fundem_sync",
+    "fundem_status_word", "fundem_num_objects", "fundem_get_objects", "fundem_set_objects",
+    "fundem_device_view_get", "fundem_num_contacts", "fundem_get_contacts", "fundem_set_contacts",
+    "fundem_num_pairs", "fundem_num_bonds", "fundem_get_bonds", "fundem_set_bond_activation",
+    "fundem_get_geometry", "fundem_get_grid", "fundem_launch_count",
+]
+
+
+class FundemError(RuntimeError):
+    pass
+
+
+class DeviceView(C.Structure):
+    _fields_ = [("pos", C.c_void_p), ("vel", C.c_void_p), ("angvel", C.c_void_p), ("force", C.c_void_p),
+                ("torque", C.c_void_p), ("quat", C.c_void_p), ("mat", C.c_void_p), ("geo", C.c_void_p),
+                ("n", C.c_int)]
+
+
+_lib = None
+
+
+def lib():
+    """Load libfundem_b200.so (raises when it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FundemError(f"{LIB_PATH} is missing: build it with `python -m fundem_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        P, I, D, LL = C.c_void_p, C.c_int, C.POINTER(C.c_double), C.c_longlong
+        IP = C.POINTER(C.c_int)
+        L.fundem_version.restype = C.c_char_p
+        L.fundem_status_string.restype = C.c_char_p
+        L.fundem_status_string.argtypes = [I]
+        L.fundem_create.argtypes = [C.POINTER(P), I, P]
+        L.fundem_destroy.argtypes = [P]
+        L.fundem_set_precision.argtypes = [P, I]
+        L.fundem_set_records.argtypes = [P, I]
+        L.fundem_add_material.argtypes = [P, I, C.c_double, C.c_double, C.c_double, C.c_double, IP]
+        L.fundem_add_geometry.argtypes = [P, I, C.c_double, D, D, C.c_double, IP, D, I, D, IP]
+        L.fundem_mass_properties.argtypes = [C.c_double, D, C.c_double, IP, D, D, D, D]
+        L.fundem_add_objects.argtypes = [P, I, I, D, D, D, D, IP, IP]
+        L.fundem_set_wall_motion.argtypes = [P, I, D, D]
+        L.fundem_move.argtypes = [P, I, I, D]
+        L.fundem_add_bonds.argtypes = [P, I, IP, IP, D, D, D, D, D, D, D, D, D]
+        L.fundem_set_periodic.argtypes = [P, I, I]
+        L.fundem_setup.argtypes = [P, D, D]
+        L.fundem_detect.argtypes = [P]
+        L.fundem_step.argtypes = [P, I, D, C.c_double]
+        L.fundem_step_begin.argtypes = [P, D, C.c_double]
+        L.fundem_step_end.argtypes = [P, D, C.c_double]
+        L.fundem_sync.argtypes = [P]
+        L.fundem_status_word.argtypes = [P, C.POINTER(C.c_uint)]
+        L.fundem_num_objects.argtypes = [P, I, IP]
+        L.fundem_get_objects.argtypes = [P, I, D, D, D, D, D, D]
+        L.fundem_set_objects.argtypes = [P, I, D, D, D, D, D, D]
+        L.fundem_device_view_get.argtypes = [P, I, C.POINTER(DeviceView)]
+        L.fundem_num_contacts.argtypes = [P, I, C.POINTER(LL)]
+        L.fundem_get_contacts.argtypes = [P, I, IP, IP, D, D, D, D, D, D]
+        L.fundem_set_contacts.argtypes = [P, I, LL, IP, IP, D]
+        L.fundem_num_pairs.argtypes = [P, I, C.POINTER(LL)]
+        L.fundem_num_bonds.argtypes = [P, IP]
+        L.fundem_get_bonds.argtypes = [P, IP, D, D]
+        L.fundem_set_bond_activation.argtypes = [P, IP]
+        L.fundem_get_geometry.argtypes = [P, I, I, D, D, D, D]
+        L.fundem_get_grid.argtypes = [P, I, D, D, D, IP]
+        L.fundem_launch_count.argtypes = [P, C.POINTER(LL)]
+        _lib = L
+    return _lib
+
+
+def _d(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _i(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+def _f64(x, n=None):
+    a = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1))
+    if n is not None:
+        assert a.size == n, (a.size, n)
+    return a
+
+
+def _i32(x):
+    return np.ascontiguousarray(np.asarray(x, dtype=np.int32).reshape(-1))
+
+
+def _check(r, what=""):
+    if r != 0:
+        msg = lib().fundem_status_string(r).decode()
+        raise FundemError(f"{what}: {msg} ({r})")
+
+
+def mass_properties(density, origin, spacing, size, sdf):
+    """Mass, centroid and inertia of a template from its SDF and a density
+    (LSSolver.h:470-586), computed by the library's host code."""
+    m, c, I = np.zeros(1), np.zeros(3), np.zeros(6)
+    _check(lib().fundem_mass_properties(float(density), _d(_f64(origin, 3)), float(spacing), _i(_i32(size)),
+                                        _d(_f64(sdf)), _d(m), _d(c), _d(I)), "mass_properties")
+    return float(m[0]), c, I
+
+
+def _rot(q, v):
+    qv = np.asarray(q[1:], float)
+    t = 2.0 * np.cross(qv, v)
+    return v + t * q[0] + np.cross(qv, t)
+
+
+class Simulation:
+    """One level-set DEM simulation on one GPU."""
+
+    def __init__(self, device=0, stream=None, precision=FP64, records=True):
+        self.L = lib()
+        h = C.c_void_p()
+        _check(self.L.fundem_create(C.byref(h), int(device), stream), "create")
+        self.h = h
+        _check(self.L.fundem_set_precision(self.h, int(precision)), "set_precision")
+        _check(self.L.fundem_set_records(self.h, int(bool(records))), "set_records")
+        self.gravity = np.array([0.0, 0.0, -9.81])
+        self.dt = 1e-6
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.fundem_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------------ build
+    @classmethod
+    def from_scenario(cls, sc, device=0, precision=FP64, records=True, setup=True):
+        """Register a Scenario exactly as the reference API receives it:
+        materials, geometries (explicit mass, or density through the
+        addParticleCluster centroid handling, LSSolver.h:125-165), particles,
+        walls, wall motion, bonds and periodicity."""
+        s = cls(device=device, precision=precision, records=records)
+        for (kn, ks, mu, e) in sc.particle_materials:
+            s.add_material(False, kn, ks, mu, e)
+        for (mu, e) in sc.wall_materials:
+            s.add_material(True, 0.0, 0.0, mu, e)
+        pos = np.array(sc.particles.pos, dtype=np.float64, copy=True)
+        for gi, g in enumerate(sc.particle_geometries):
+            if g.density is None:
+                s.add_geometry(False, g.mass, g.inertia, g.origin, g.spacing, g.size, g.sdf, g.nodes)
+            else:
+                m, c, I = mass_properties(g.density, g.origin, g.spacing, g.size, g.sdf)
+                s.add_geometry(False, m, I, np.asarray(g.origin, float) - c, g.spacing, g.size, g.sdf,
+                               np.asarray(g.nodes, float) - c)
+                for i in np.nonzero(sc.particles.geo == gi)[0]:
+                    pos[i] = pos[i] + _rot(sc.particles.quat[i], c)
+        for g in sc.wall_geometries:
+            s.add_geometry(True, 0.0, None, g.origin, g.spacing, g.size, g.sdf, g.nodes)
+        P = sc.particles
+        s.add_objects(False, pos, P.vel, P.angvel, P.quat, P.mat, P.geo)
+        W = sc.walls
+        if len(W):
+            s.add_objects(True, W.pos, W.vel, W.angvel, W.quat, W.mat, W.geo)
+        for (idx, v, w) in sc.wall_motion:
+            s.set_wall_motion(idx, v, w)
+        B = sc.bonds
+        if len(B):
+            s.add_bonds(B.master, B.slave, B.point, B.normal, B.radius, B.length, B.young, B.poisson,
+                        B.tensile, B.cohesion, B.friction)
+        s.set_periodic(sc.periodic_x, sc.periodic_y)
+        s.gravity = np.asarray(sc.gravity, float)
+        s.dt = float(sc.dt)
+        if setup:
+            s.setup(sc.domain_min, sc.domain_max)
+        return s
+
+    def add_material(self, wall, kn, ks, mu, e):
+        i = C.c_int()
+        _check(self.L.fundem_add_material(self.h, int(wall), kn, ks, mu, e, C.byref(i)), "add_material")
+        return i.value
+
+    def add_geometry(self, wall, mass, inertia, origin, spacing, size, sdf, nodes):
+        i = C.c_int()
+        nodes = _f64(nodes)
+        inertia = None if inertia is None else _f64(inertia, 6)
+        _check(self.L.fundem_add_geometry(self.h, int(wall), float(mass), _d(inertia), _d(_f64(origin, 3)),
+                                          float(spacing), _i(_i32(size)), _d(_f64(sdf)), nodes.size // 3,
+                                          _d(nodes), C.byref(i)), "add_geometry")
+        return i.value
+
+    def add_objects(self, wall, pos, vel, angvel, quat, mat, geo):
+        pos = _f64(pos)
+        n = pos.size // 3
+        _check(self.L.fundem_add_objects(self.h, int(wall), n, _d(pos), _d(_f64(vel, 3 * n)),
+                                         _d(_f64(angvel, 3 * n)), _d(_f64(quat, 4 * n)), _i(_i32(mat)),
+                                         _i(_i32(geo))), "add_objects")
+
+    def set_wall_motion(self, idx, vel, angvel):
+        _check(self.L.fundem_set_wall_motion(self.h, int(idx), _d(_f64(vel, 3)), _d(_f64(angvel, 3))),
+               "set_wall_motion")
+
+    def add_bonds(self, master, slave, point, normal, radius, length, young, poisson, tensile=None,
+                  cohesion=None, friction=None):
+        master = _i32(master)
+        n = master.size
+        z = np.zeros(n)
+        _check(self.L.fundem_add_bonds(self.h, n, _i(master), _i(_i32(slave)), _d(_f64(point, 3 * n)),
+                                       _d(_f64(normal, 3 * n)), _d(_f64(radius, n)), _d(_f64(length, n)),
+                                       _d(_f64(young, n)), _d(_f64(poisson, n)),
+                                       _d(_f64(z if tensile is None else tensile, n)),
+                                       _d(_f64(z if cohesion is None else cohesion, n)),
+                                       _d(_f64(z if friction is None else friction, n))), "add_bonds")
+
+    def set_periodic(self, x, y):
+        _check(self.L.fundem_set_periodic(self.h, int(bool(x)), int(bool(y))), "set_periodic")
+
+    def set_records(self, full):
+        _check(self.L.fundem_set_records(self.h, int(bool(full))), "set_records")
+
+    # ------------------------------------------------------------------ run
+    def setup(self, minb, maxb):
+        _check(self.L.fundem_setup(self.h, _d(_f64(minb, 3)), _d(_f64(maxb, 3))), "setup")
+
+    def detect(self):
+        _check(self.L.fundem_detect(self.h), "detect")
+
+    def step(self, n=1, dt=None, gravity=None):
+        g = _f64(self.gravity if gravity is None else gravity, 3)
+        _check(self.L.fundem_step(self.h, int(n), _d(g), float(self.dt if dt is None else dt)), "step")
+
+    def step_begin(self, dt=None, gravity=None):
+        g = _f64(self.gravity if gravity is None else gravity, 3)
+        _check(self.L.fundem_step_begin(self.h, _d(g), float(self.dt if dt is None else dt)), "step_begin")
+
+    def step_end(self, dt=None, gravity=None):
+        g = _f64(self.gravity if gravity is None else gravity, 3)
+        _check(self.L.fundem_step_end(self.h, _d(g), float(self.dt if dt is None else dt)), "step_end")
+
+    def sync(self):
+        _check(self.L.fundem_sync(self.h), "sync")
+
+    # ------------------------------------------------------------------ state
+    def num(self, wall=False):
+        n = C.c_int()
+        _check(self.L.fundem_num_objects(self.h, int(wall), C.byref(n)), "num_objects")
+        return n.value
+
+    def state(self, wall=False):
+        n = self.num(wall)
+        out = {k: np.zeros((n, 3)) for k in ("pos", "vel", "angvel", "force", "torque")}
+        out["quat"] = np.zeros((n, 4))
+        _check(self.L.fundem_get_objects(self.h, int(wall), _d(out["pos"]), _d(out["vel"]), _d(out["angvel"]),
+                                         _d(out["quat"]), _d(out["force"]), _d(out["torque"])), "get_objects")
+        return out
+
+    def set_state(self, wall=False, pos=None, vel=None, angvel=None, quat=None, force=None, torque=None):
+        n = self.num(wall)
+        f = lambda a, k: None if a is None else _f64(a, n * k)
+        _check(self.L.fundem_set_objects(self.h, int(wall), _d(f(pos, 3)), _d(f(vel, 3)), _d(f(angvel, 3)),
+                                         _d(f(quat, 4)), _d(f(force, 3)), _d(f(torque, 3))), "set_objects")
+
+    def device_view(self, wall=False):
+        v = DeviceView()
+        _check(self.L.fundem_device_view_get(self.h, int(wall), C.byref(v)), "device_view")
+        return v
+
+    def num_contacts(self, kind=PP):
+        n = C.c_longlong()
+        _check(self.L.fundem_num_contacts(self.h, int(kind), C.byref(n)), "num_contacts")
+        return n.value
+
+    def num_pairs(self, kind=PP):
+        n = C.c_longlong()
+        _check(self.L.fundem_num_pairs(self.h, int(kind), C.byref(n)), "num_pairs")
+        return n.value
+
+    def contacts(self, kind=PP):
+        n = self.num_contacts(kind)
+        c = dict(master=np.zeros(n, np.int32), slave=np.zeros(n, np.int32), point=np.zeros((n, 3)),
+                 normal=np.zeros((n, 3)), overlap=np.zeros(n), spring=np.zeros((n, 3)), en=np.zeros(n),
+                 es=np.zeros(n))
+        if n:
+            _check(self.L.fundem_get_contacts(self.h, int(kind), _i(c["master"]), _i(c["slave"]), _d(c["point"]),
+                                              _d(c["normal"]), _d(c["overlap"]), _d(c["spring"]), _d(c["en"]),
+                                              _d(c["es"])), "get_contacts")
+        return c
+
+    def set_contacts(self, kind, node, partner, spring):
+        node = _i32(node)
+        _check(self.L.fundem_set_contacts(self.h, int(kind), node.size, _i(node), _i(_i32(partner)),
+                                          _d(_f64(spring, 3 * node.size))), "set_contacts")
+
+    def bonds(self):
+        n = C.c_int()
+        _check(self.L.fundem_num_bonds(self.h, C.byref(n)), "num_bonds")
+        n = n.value
+        act, pt, en = np.zeros(n, np.int32), np.zeros((n, 3)), np.zeros((n, 6))
+        if n:
+            _check(self.L.fundem_get_bonds(self.h, _i(act), _d(pt), _d(en)), "get_bonds")
+        return dict(activated=act, point=pt, un=en[:, 0], us=en[:, 1], ub=en[:, 2], ut=en[:, 3], sn=en[:, 4],
+                    ss=en[:, 5])
+
+    def set_bond_activation(self, act):
+        _check(self.L.fundem_set_bond_activation(self.h, _i(_i32(act))), "set_bond_activation")
+
+    def geometry(self, geo, wall=False):
+        r, im, I, Ii = np.zeros(1), np.zeros(1), np.zeros(6), np.zeros(6)
+        _check(self.L.fundem_get_geometry(self.h, int(wall), int(geo), _d(r), _d(im), _d(I), _d(Ii)), "geometry")
+        return dict(radius=float(r[0]), inv_mass=float(im[0]), inertia=I, inv_inertia=Ii)
+
+    def grid(self, wall=False):
+        mn, mx, inv = np.zeros(3), np.zeros(3), np.zeros(3)
+        sz = np.zeros(3, np.int32)
+        _check(self.L.fundem_get_grid(self.h, int(wall), _d(mn), _d(mx), _d(inv), _i(sz)), "grid")
+        return dict(min=mn, max=mx, inv_cell=inv, size=sz)
+
+    def launch_count(self):
+        n = C.c_longlong()
+        _check(self.L.fundem_launch_count(self.h, C.byref(n)), "launch_count")
+        return n.value

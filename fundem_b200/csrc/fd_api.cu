@@ -1,0 +1,1455 @@
+// fd_api.cu -- host side of libfundem_b200: template preprocessing, device
+// memory, step orchestration and the C ABI declared in include/fundem_b200.h.
+#include "../../include/fundem_b200.h"
+#include "fd_kernels.cuh"
+
+#include <algorithm>
+#include <cfloat>
+#include <functional>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace {
+
+using fd::CellTableDev;
+using fd::GeoSetDev;
+using fd::ObjDev;
+using fd::PairListDev;
+
+struct CudaError : std::runtime_error {
+    explicit CudaError(const std::string& s) : std::runtime_error(s) {}
+};
+#define FD_CUDA(x)                                                                                   \
+    do {                                                                                             \
+        cudaError_t e_ = (x);                                                                        \
+        if (e_ != cudaSuccess) throw CudaError(std::string(#x) + ": " + cudaGetErrorString(e_));     \
+    } while (0)
+
+template <typename T> struct DevArray {
+    T* p = nullptr;
+    size_t n = 0;
+    DevArray() = default;
+    DevArray(const DevArray&) = delete;
+    DevArray& operator=(const DevArray&) = delete;
+    ~DevArray() { release(); }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void alloc(size_t count, bool zero = true)
+    {
+        release();
+        n = count;
+        if (count == 0) return;
+        FD_CUDA(cudaMalloc((void**)&p, sizeof(T) * count));
+        if (zero) FD_CUDA(cudaMemset(p, 0, sizeof(T) * count));
+    }
+    // grow keeping the first `keep` elements
+    void grow(size_t count, size_t keep)
+    {
+        if (count <= n) return;
+        T* q = nullptr;
+        FD_CUDA(cudaMalloc((void**)&q, sizeof(T) * count));
+        FD_CUDA(cudaMemset(q, 0, sizeof(T) * count));
+        if (p && keep) FD_CUDA(cudaMemcpy(q, p, sizeof(T) * std::min(keep, n), cudaMemcpyDeviceToDevice));
+        if (p) cudaFree(p);
+        p = q;
+        n = count;
+    }
+    void upload(const T* h, size_t count, cudaStream_t s)
+    {
+        if (count) FD_CUDA(cudaMemcpyAsync(p, h, sizeof(T) * count, cudaMemcpyHostToDevice, s));
+    }
+    void upload(const std::vector<T>& h, cudaStream_t s)
+    {
+        if (h.size() > n) alloc(h.size(), false);
+        upload(h.data(), h.size(), s);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// host-side template preprocessing
+// ---------------------------------------------------------------------------
+struct HostGeo {
+    double mass = 0.0;
+    fd_sym inertia{0, 0, 0, 0, 0, 0};
+    double3 origin{0, 0, 0};
+    double spacing = 1.0;
+    int3 size{2, 2, 2};
+    std::vector<double> sdf;
+    std::vector<double3> nodes;
+};
+
+// inverse with the |det| < 1e-30 -> zero rule of myMat.h:163-194
+fd_sym host_inverse(const fd_sym& A)
+{
+    const double det = A.xx * (A.yy * A.zz - A.yz * A.yz) + A.xy * (A.yz * A.xz - A.xy * A.zz) +
+                       A.xz * (A.xy * A.yz - A.yy * A.xz);
+    fd_sym r{0, 0, 0, 0, 0, 0};
+    if (std::fabs(det) < 1e-30) return r;
+    const double di = 1.0 / det;
+    r.xx = (A.yy * A.zz - A.yz * A.yz) * di;
+    r.yy = (A.xx * A.zz - A.xz * A.xz) * di;
+    r.zz = (A.xx * A.yy - A.xy * A.xy) * di;
+    r.xy = -(A.xy * A.zz - A.xz * A.yz) * di;
+    r.xz = (A.xy * A.yz - A.xz * A.yy) * di;
+    r.yz = -(A.xx * A.yz - A.xz * A.xy) * di;
+    return r;
+}
+
+double host_len(double3 v) { return std::sqrt(v.x * v.x + v.y * v.y + v.z * v.z); }
+
+// Split node indices into spatially coherent clusters of at most 32 nodes:
+// recursive bisection along the widest axis, left part a multiple of 32.
+void cluster_nodes(const std::vector<double3>& nodes, std::vector<int>& idx, int lo, int hi,
+                   std::vector<std::pair<int, int>>& out)
+{
+    const int n = hi - lo;
+    if (n <= 32) {
+        out.push_back({lo, n});
+        return;
+    }
+    double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, mx[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+    for (int k = lo; k < hi; ++k) {
+        const double3 p = nodes[idx[k]];
+        const double v[3] = {p.x, p.y, p.z};
+        for (int d = 0; d < 3; ++d) { mn[d] = std::min(mn[d], v[d]); mx[d] = std::max(mx[d], v[d]); }
+    }
+    int axis = 0;
+    for (int d = 1; d < 3; ++d)
+        if (mx[d] - mn[d] > mx[axis] - mn[axis]) axis = d;
+    auto key = [&](int i) { const double3 p = nodes[i]; return axis == 0 ? p.x : (axis == 1 ? p.y : p.z); };
+    std::stable_sort(idx.begin() + lo, idx.begin() + hi, [&](int a, int b) { return key(a) < key(b); });
+    int left = 32 * (int)std::lround(n / 64.0);
+    if (left <= 0) left = 32;
+    if (left >= n) left = n - n / 2;
+    cluster_nodes(nodes, idx, lo, lo + left, out);
+    cluster_nodes(nodes, idx, lo + left, hi, out);
+}
+
+// Lower bound, for every grid node, of the distance to the union of cells
+// whose corner minimum is <= 0 (the only cells where the trilinear SDF can be
+// <= 0).  Exact squared box distance by three separable min-plus passes.
+std::vector<float> distance_bound(const HostGeo& g)
+{
+    const int nx = g.size.x, ny = g.size.y, nz = g.size.z;
+    const int cx = nx - 1, cy = ny - 1, cz = nz - 1;
+    const double INF = 1e300;
+    auto S = [&](int x, int y, int z) { return g.sdf[(size_t)z * ny * nx + (size_t)y * nx + x]; };
+    std::vector<double> F((size_t)cx * cy * cz, INF);
+    for (int z = 0; z < cz; ++z)
+        for (int y = 0; y < cy; ++y)
+            for (int x = 0; x < cx; ++x) {
+                double m = S(x, y, z);
+                for (int dz = 0; dz < 2; ++dz)
+                    for (int dy = 0; dy < 2; ++dy)
+                        for (int dx = 0; dx < 2; ++dx) m = std::min(m, S(x + dx, y + dy, z + dz));
+                if (m <= 0.0) F[(size_t)z * cy * cx + (size_t)y * cx + x] = 0.0;
+            }
+    auto gap2 = [](int c, int a) {
+        const int g = std::max(0, std::max(c - a, a - c - 1));
+        return (double)g * g;
+    };
+    // pass x: cells (cz, cy, cx) -> (cz, cy, nx)
+    std::vector<double> D1((size_t)cz * cy * nx, INF);
+    for (int z = 0; z < cz; ++z)
+        for (int y = 0; y < cy; ++y)
+            for (int a = 0; a < nx; ++a) {
+                double m = INF;
+                for (int c = 0; c < cx; ++c) {
+                    const double f = F[(size_t)z * cy * cx + (size_t)y * cx + c];
+                    if (f < INF) m = std::min(m, f + gap2(c, a));
+                }
+                D1[(size_t)z * cy * nx + (size_t)y * nx + a] = m;
+            }
+    std::vector<double> D2((size_t)cz * ny * nx, INF);
+    for (int z = 0; z < cz; ++z)
+        for (int a = 0; a < ny; ++a)
+            for (int x = 0; x < nx; ++x) {
+                double m = INF;
+                for (int c = 0; c < cy; ++c) {
+                    const double f = D1[(size_t)z * cy * nx + (size_t)c * nx + x];
+                    if (f < INF) m = std::min(m, f + gap2(c, a));
+                }
+                D2[(size_t)z * ny * nx + (size_t)a * nx + x] = m;
+            }
+    std::vector<float> out((size_t)nz * ny * nx);
+    for (int a = 0; a < nz; ++a)
+        for (int y = 0; y < ny; ++y)
+            for (int x = 0; x < nx; ++x) {
+                double m = INF;
+                for (int c = 0; c < cz; ++c) {
+                    const double f = D2[(size_t)c * ny * nx + (size_t)y * nx + x];
+                    if (f < INF) m = std::min(m, f + gap2(c, a));
+                }
+                float r;
+                if (m >= INF) r = FLT_MAX;
+                else {
+                    const double d = std::sqrt(m) * g.spacing * (1.0 - 1e-12);
+                    r = (float)d;
+                    if ((double)r > d) r = std::nextafter(r, 0.0f);
+                }
+                out[(size_t)a * ny * nx + (size_t)y * nx + x] = r;
+            }
+    return out;
+}
+
+double lipschitz_bound(const HostGeo& g)
+{
+    const int nx = g.size.x, ny = g.size.y, nz = g.size.z;
+    auto S = [&](int x, int y, int z) { return g.sdf[(size_t)z * ny * nx + (size_t)y * nx + x]; };
+    double L[3] = {0, 0, 0};
+    for (int z = 0; z < nz; ++z)
+        for (int y = 0; y < ny; ++y)
+            for (int x = 0; x < nx; ++x) {
+                if (x + 1 < nx) L[0] = std::max(L[0], std::fabs(S(x + 1, y, z) - S(x, y, z)));
+                if (y + 1 < ny) L[1] = std::max(L[1], std::fabs(S(x, y + 1, z) - S(x, y, z)));
+                if (z + 1 < nz) L[2] = std::max(L[2], std::fabs(S(x, y, z + 1) - S(x, y, z)));
+            }
+    return std::sqrt(L[0] * L[0] + L[1] * L[1] + L[2] * L[2]) / g.spacing * (1.0 + 1e-9);
+}
+
+struct GeoSetHost {
+    std::vector<HostGeo> geos;
+    // device
+    DevArray<FdGeo> d_geo;
+    DevArray<double> d_sdf;
+    DevArray<float> d_sdf32;
+    DevArray<float> d_dist;
+    DevArray<double3> d_nodes;
+    DevArray<int> d_lid;
+    DevArray<FdCluster> d_clusters;
+    std::vector<FdGeo> table;
+    double rmax = 0.0, grid_rmax = 0.0;
+    bool built = false;
+
+    void build(bool wall, cudaStream_t s)
+    {
+        table.clear();
+        std::vector<double> sdf;
+        std::vector<float> sdf32, dist;
+        std::vector<double3> nodes;
+        std::vector<int> lid;
+        std::vector<FdCluster> clusters;
+        rmax = grid_rmax = 0.0;
+        for (const HostGeo& g : geos) {
+            FdGeo t{};
+            t.origin = g.origin;
+            t.spacing = g.spacing;
+            t.inv_spacing = 1.0 / g.spacing;
+            t.size = g.size;
+            t.sdf_off = (long long)sdf.size();
+            t.dist_off = (long long)dist.size();
+            sdf.insert(sdf.end(), g.sdf.begin(), g.sdf.end());
+            for (double v : g.sdf) sdf32.push_back((float)v);
+            std::vector<float> D = distance_bound(g);
+            dist.insert(dist.end(), D.begin(), D.end());
+            double r = 0.0;
+            for (const double3& p : g.nodes) r = std::max(r, host_len(p));
+            t.radius = r;
+            double gr = 0.0;
+            for (int c = 0; c < 8; ++c) {
+                const double3 corner = make_double3(g.origin.x + ((c & 1) ? (g.size.x - 1) * g.spacing : 0.0),
+                                                    g.origin.y + ((c & 2) ? (g.size.y - 1) * g.spacing : 0.0),
+                                                    g.origin.z + ((c & 4) ? (g.size.z - 1) * g.spacing : 0.0));
+                gr = std::max(gr, host_len(corner));
+            }
+            t.grid_radius = gr * (1.0 + 1e-9);
+            t.lip = lipschitz_bound(g);
+            const double mass = wall ? 0.0 : g.mass;
+            t.inv_mass = mass > 0.0 ? 1.0 / mass : 0.0;
+            t.inertia = mass > 0.0 ? g.inertia : fd_sym{0, 0, 0, 0, 0, 0};
+            t.inv_inertia = host_inverse(t.inertia);
+            // clusters
+            std::vector<int> idx(g.nodes.size());
+            std::iota(idx.begin(), idx.end(), 0);
+            std::vector<std::pair<int, int>> parts;
+            if (!idx.empty()) cluster_nodes(g.nodes, idx, 0, (int)idx.size(), parts);
+            t.node_off = (int)nodes.size();
+            t.node_count = (int)g.nodes.size();
+            t.clus_off = (int)clusters.size();
+            t.clus_count = (int)parts.size();
+            for (auto& pr : parts) {
+                FdCluster cl{};
+                double3 c = make_double3(0, 0, 0);
+                for (int k = pr.first; k < pr.first + pr.second; ++k) {
+                    const double3 p = g.nodes[idx[k]];
+                    c.x += p.x; c.y += p.y; c.z += p.z;
+                }
+                c.x /= pr.second; c.y /= pr.second; c.z /= pr.second;
+                double rr = 0.0;
+                for (int k = pr.first; k < pr.first + pr.second; ++k) {
+                    const double3 p = g.nodes[idx[k]];
+                    rr = std::max(rr, host_len(make_double3(p.x - c.x, p.y - c.y, p.z - c.z)));
+                }
+                cl.centre = c;
+                cl.radius = rr;
+                cl.start = pr.first;
+                cl.count = pr.second;
+                clusters.push_back(cl);
+            }
+            for (int k : idx) {
+                nodes.push_back(g.nodes[k]);
+                lid.push_back(k);
+            }
+            rmax = std::max(rmax, t.radius);
+            grid_rmax = std::max(grid_rmax, t.grid_radius);
+            table.push_back(t);
+        }
+        d_geo.alloc(std::max<size_t>(table.size(), 1));
+        d_geo.upload(table.data(), table.size(), s);
+        d_sdf.alloc(std::max<size_t>(sdf.size(), 1));
+        d_sdf.upload(sdf.data(), sdf.size(), s);
+        d_sdf32.alloc(std::max<size_t>(sdf32.size(), 1));
+        d_sdf32.upload(sdf32.data(), sdf32.size(), s);
+        d_dist.alloc(std::max<size_t>(dist.size(), 1));
+        d_dist.upload(dist.data(), dist.size(), s);
+        d_nodes.alloc(std::max<size_t>(nodes.size(), 1));
+        d_nodes.upload(nodes.data(), nodes.size(), s);
+        d_lid.alloc(std::max<size_t>(lid.size(), 1));
+        d_lid.upload(lid.data(), lid.size(), s);
+        d_clusters.alloc(std::max<size_t>(clusters.size(), 1));
+        d_clusters.upload(clusters.data(), clusters.size(), s);
+        FD_CUDA(cudaStreamSynchronize(s));
+        built = true;
+    }
+
+    GeoSetDev view() const
+    {
+        GeoSetDev v;
+        v.n = (int)table.size();
+        v.geo = d_geo.p;
+        v.sdf = d_sdf.p;
+        v.sdf32 = d_sdf32.p;
+        v.dist = d_dist.p;
+        v.nodes = d_nodes.p;
+        v.node_lid = d_lid.p;
+        v.clusters = d_clusters.p;
+        v.rmax = rmax;
+        v.grid_rmax = grid_rmax;
+        return v;
+    }
+};
+
+struct MatHost {
+    std::vector<double> kn, ks, mu, e;
+    DevArray<double> d_kn, d_ks, d_mu, d_e;
+    void upload(cudaStream_t s)
+    {
+        d_kn.upload(kn, s);
+        d_ks.upload(ks, s);
+        d_mu.upload(mu, s);
+        d_e.upload(e, s);
+    }
+    fd::MatDev view() const { return fd::MatDev{d_kn.p, d_ks.p, d_mu.p, d_e.p}; }
+};
+
+struct ObjHost {
+    std::vector<double3> pos, vel, angvel, force, torque;
+    std::vector<fd_quat> q;
+    std::vector<int> mat, geo;
+    DevArray<double3> d_pos, d_vel, d_angvel, d_force, d_torque;
+    DevArray<fd_quat> d_q;
+    DevArray<int> d_mat, d_geo, d_node_base;
+    DevArray<long long> d_hash;
+    int n_dev = 0;
+    bool dirty = true;
+
+    int n() const { return (int)pos.size(); }
+    void upload(const std::vector<int>& node_base, cudaStream_t s)
+    {
+        const size_t n = pos.size();
+        const size_t m = std::max<size_t>(n, 1);
+        d_pos.alloc(m); d_vel.alloc(m); d_angvel.alloc(m); d_force.alloc(m); d_torque.alloc(m);
+        d_q.alloc(m); d_mat.alloc(m); d_geo.alloc(m); d_hash.alloc(m); d_node_base.alloc(m);
+        d_pos.upload(pos.data(), n, s); d_vel.upload(vel.data(), n, s); d_angvel.upload(angvel.data(), n, s);
+        d_force.upload(force.data(), n, s); d_torque.upload(torque.data(), n, s); d_q.upload(q.data(), n, s);
+        d_mat.upload(mat.data(), n, s); d_geo.upload(geo.data(), n, s);
+        d_node_base.upload(node_base.data(), std::min(n, node_base.size()), s);
+        n_dev = (int)n;
+        dirty = false;
+    }
+    ObjDev view()
+    {
+        ObjDev v;
+        v.n = n_dev;
+        v.pos = d_pos.p; v.vel = d_vel.p; v.angvel = d_angvel.p; v.force = d_force.p; v.torque = d_torque.p;
+        v.q = d_q.p; v.mat = d_mat.p; v.geo = d_geo.p; v.hash = d_hash.p; v.node_base = d_node_base.p;
+        return v;
+    }
+};
+
+struct PairGen {
+    DevArray<int> pairA, pairB, seg_off, seg_cnt, c_off, c_cnt, c_node, c_slave, counters;
+    DevArray<double> pf, c_spring, c_point, c_normal, c_overlap, c_en, c_es;
+};
+
+struct PairList {
+    PairGen gen[2];
+    int cur = 0;
+    int cap_pairs = 0, cap_contacts = 0;
+    int n_obj = 0;
+    DevArray<int> rev_cnt, rev_off, rev_fill, rev_pair;
+    bool allocated = false;
+
+    void alloc(int nobj, int capp, int capc)
+    {
+        n_obj = nobj;
+        cap_pairs = std::max(capp, 16);
+        cap_contacts = std::max(capc, 64);
+        const size_t m = std::max(nobj, 1);
+        for (PairGen& g : gen) {
+            g.pairA.alloc(cap_pairs); g.pairB.alloc(cap_pairs); g.seg_off.alloc(m); g.seg_cnt.alloc(m);
+            g.c_off.alloc(cap_pairs); g.c_cnt.alloc(cap_pairs); g.pf.alloc((size_t)cap_pairs * 9);
+            g.c_node.alloc(cap_contacts); g.c_slave.alloc(cap_contacts); g.c_spring.alloc((size_t)cap_contacts * 3);
+            g.c_point.alloc((size_t)cap_contacts * 3); g.c_normal.alloc((size_t)cap_contacts * 3);
+            g.c_overlap.alloc(cap_contacts); g.c_en.alloc(cap_contacts); g.c_es.alloc(cap_contacts);
+            g.counters.alloc(2);
+        }
+        rev_cnt.alloc(m); rev_off.alloc(m); rev_fill.alloc(m); rev_pair.alloc(cap_pairs);
+        allocated = true;
+    }
+    void grow(int capp, int capc)
+    {
+        if (capp > cap_pairs) {
+            for (PairGen& g : gen) {
+                g.pairA.grow(capp, cap_pairs); g.pairB.grow(capp, cap_pairs); g.c_off.grow(capp, cap_pairs);
+                g.c_cnt.grow(capp, cap_pairs); g.pf.grow((size_t)capp * 9, (size_t)cap_pairs * 9);
+            }
+            rev_pair.grow(capp, 0);
+            cap_pairs = capp;
+        }
+        if (capc > cap_contacts) {
+            for (PairGen& g : gen) {
+                g.c_node.grow(capc, cap_contacts); g.c_slave.grow(capc, cap_contacts);
+                g.c_spring.grow((size_t)capc * 3, (size_t)cap_contacts * 3);
+                g.c_point.grow((size_t)capc * 3, (size_t)cap_contacts * 3);
+                g.c_normal.grow((size_t)capc * 3, (size_t)cap_contacts * 3);
+                g.c_overlap.grow(capc, cap_contacts); g.c_en.grow(capc, cap_contacts); g.c_es.grow(capc, cap_contacts);
+            }
+            cap_contacts = capc;
+        }
+    }
+    PairListDev view()
+    {
+        PairGen& c = gen[cur];
+        PairGen& o = gen[cur ^ 1];
+        PairListDev v;
+        v.pairA = c.pairA.p; v.pairB = c.pairB.p; v.seg_off = c.seg_off.p; v.seg_cnt = c.seg_cnt.p;
+        v.c_off = c.c_off.p; v.c_cnt = c.c_cnt.p; v.pf = c.pf.p; v.n_pairs = c.counters.p; v.cap_pairs = cap_pairs;
+        v.o_pairB = o.pairB.p; v.o_seg_off = o.seg_off.p; v.o_seg_cnt = o.seg_cnt.p; v.o_c_off = o.c_off.p;
+        v.o_c_cnt = o.c_cnt.p;
+        v.c_node = c.c_node.p; v.c_slave = c.c_slave.p; v.c_spring = c.c_spring.p; v.c_point = c.c_point.p;
+        v.c_normal = c.c_normal.p; v.c_overlap = c.c_overlap.p; v.c_en = c.c_en.p; v.c_es = c.c_es.p;
+        v.n_contacts = c.counters.p + 1; v.cap_contacts = cap_contacts;
+        v.o_c_node = o.c_node.p; v.o_c_spring = o.c_spring.p;
+        v.rev_cnt = rev_cnt.p; v.rev_off = rev_off.p; v.rev_fill = rev_fill.p; v.rev_pair = rev_pair.p;
+        return v;
+    }
+};
+
+struct CellTable {
+    FdGrid g{};
+    DevArray<int> count, start, fill, sorted;
+    void alloc(const FdGrid& grid, int nobj)
+    {
+        g = grid;
+        count.alloc((size_t)g.num); start.alloc((size_t)g.num); fill.alloc((size_t)g.num);
+        sorted.alloc(std::max(nobj, 1));
+    }
+    CellTableDev view() { return CellTableDev{g, count.p, start.p, fill.p, sorted.p}; }
+};
+
+struct Ghost {
+    DevArray<double3> pos;
+    DevArray<long long> hash;
+    CellTable cells;
+    bool active = false;
+    fd::GhostDev view() { return fd::GhostDev{pos.p, hash.p, cells.view()}; }
+};
+
+struct BondHost {
+    std::vector<int> master, slave, active;
+    std::vector<double3> point;
+    std::vector<double> B, radius, L0, ts, coh, mu, energy;
+    std::vector<double3> frames;
+    DevArray<int> d_master, d_slave, d_active, d_plist_off, d_plist;
+    DevArray<double3> d_point, d_frames;
+    DevArray<double> d_B, d_radius, d_L0, d_ts, d_coh, d_mu, d_energy, d_out;
+    int n_dev = 0;
+    bool dirty = false;
+};
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// the simulation object
+// ---------------------------------------------------------------------------
+struct fundem_sim {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int precision = FUNDEM_FP64;
+    int records = 1;
+    MatHost pmat, wmat;
+    GeoSetHost pgeo, wgeo;
+    ObjHost P, W;
+    BondHost bonds;
+    bool perX = false, perY = false;
+    bool geo_dirty = true;
+    bool setup_done = false;
+    bool detected = false;
+    FdGrid pgrid{}, wgrid{};
+    CellTable ptab;
+    PairList lists[FD_NKIND];
+    Ghost ghosts[3];
+    DevArray<int> scan_tmp;
+    DevArray<int> wcount;  // wall-grid histogram (walls are looped over directly)
+    DevArray<unsigned int> flags;
+    std::vector<int> node_base;
+    long long n_nodes = 0;
+    long long launches = 0;
+    std::string last_error;
+
+    void build_node_base()
+    {
+        node_base.resize(P.pos.size());
+        long long acc = 0;
+        for (size_t i = 0; i < P.pos.size(); ++i) {
+            node_base[i] = (int)acc;
+            acc += (long long)pgeo.geos[P.geo[i]].nodes.size();
+        }
+        n_nodes = acc;
+    }
+
+    static FdGrid make_grid(double3 mn, double3 mx, double cell, const FdGrid* prev)
+    {
+        // spatialGrid::set, mySpatialGrid.h:212-240
+        if (mx.x <= mn.x) mx.x = mn.x + cell;
+        if (mx.y <= mn.y) mx.y = mn.y + cell;
+        if (mx.z <= mn.z) mx.z = mn.z + cell;
+        FdGrid g{};
+        g.minb = mn;
+        g.maxb = mx;
+        g.size = prev ? prev->size : make_int3(2, 2, 2);
+        g.inv = prev ? prev->inv : make_double3(0, 0, 0);
+        if (g.size.x == 0) g.size = make_int3(2, 2, 2);
+        if (fd_is_zero(cell)) {
+            g.num = 8;
+            return g;
+        }
+        const double dx = mx.x - mn.x, dy = mx.y - mn.y, dz = mx.z - mn.z;
+        g.size.x = dx > 2. * cell ? (int)(dx / cell) : 2;
+        g.size.y = dy > 2. * cell ? (int)(dy / cell) : 2;
+        g.size.z = dz > 2. * cell ? (int)(dz / cell) : 2;
+        g.inv.x = dx > 0.0 ? (double)g.size.x / dx : 0.0;
+        g.inv.y = dy > 0.0 ? (double)g.size.y / dy : 0.0;
+        g.inv.z = dz > 0.0 ? (double)g.size.z / dz : 0.0;
+        g.num = (long long)g.size.x * g.size.y * g.size.z;
+        return g;
+    }
+
+    fd::StepArgs step_args(double dt)
+    {
+        fd::StepArgs a;
+        a.dt = dt;
+        a.gravity = make_double3(0, 0, 0);
+        a.periodic_x = perX;
+        a.periodic_y = perY;
+        a.records = records;
+        a.flags = flags.p;
+        return a;
+    }
+
+    fd::BondDev bond_view()
+    {
+        fd::BondDev b{};
+        BondHost& B = bonds;
+        b.n = B.n_dev;
+        b.master = B.d_master.p; b.slave = B.d_slave.p; b.active = B.d_active.p; b.point = B.d_point.p;
+        b.B = B.d_B.p; b.radius = B.d_radius.p; b.L0 = B.d_L0.p; b.ts = B.d_ts.p; b.coh = B.d_coh.p;
+        b.mu = B.d_mu.p; b.frames = B.d_frames.p; b.energy = B.d_energy.p; b.out = B.d_out.p;
+        b.plist_off = B.d_plist_off.p; b.plist = B.d_plist.p;
+        return b;
+    }
+
+    void upload_bonds()
+    {
+        BondHost& B = bonds;
+        const size_t n = B.master.size();
+        const size_t m = std::max<size_t>(n, 1);
+        B.d_master.alloc(m); B.d_slave.alloc(m); B.d_active.alloc(m); B.d_point.alloc(m);
+        B.d_B.alloc(4 * m); B.d_radius.alloc(m); B.d_L0.alloc(m); B.d_ts.alloc(m); B.d_coh.alloc(m);
+        B.d_mu.alloc(m); B.d_frames.alloc(8 * m); B.d_energy.alloc(6 * m); B.d_out.alloc(9 * m);
+        B.d_master.upload(B.master.data(), n, stream); B.d_slave.upload(B.slave.data(), n, stream);
+        B.d_active.upload(B.active.data(), n, stream); B.d_point.upload(B.point.data(), n, stream);
+        B.d_B.upload(B.B.data(), 4 * n, stream); B.d_radius.upload(B.radius.data(), n, stream);
+        B.d_L0.upload(B.L0.data(), n, stream); B.d_ts.upload(B.ts.data(), n, stream);
+        B.d_coh.upload(B.coh.data(), n, stream); B.d_mu.upload(B.mu.data(), n, stream);
+        B.d_frames.upload(B.frames.data(), 8 * n, stream); B.d_energy.upload(B.energy.data(), 6 * n, stream);
+        // per-particle bond lists, bond order within a particle
+        const int np = P.n();
+        std::vector<int> cnt(np + 1, 0);
+        for (size_t k = 0; k < n; ++k) { cnt[B.master[k]]++; cnt[B.slave[k]]++; }
+        std::vector<int> off(np + 1, 0);
+        for (int i = 0; i < np; ++i) off[i + 1] = off[i] + cnt[i];
+        std::vector<int> fillv(np, 0), plist(std::max(off[np], 1));
+        for (size_t k = 0; k < n; ++k) {
+            plist[off[B.master[k]] + fillv[B.master[k]]++] = (int)(2 * k);
+            plist[off[B.slave[k]] + fillv[B.slave[k]]++] = (int)(2 * k + 1);
+        }
+        B.d_plist_off.alloc(np + 1);
+        B.d_plist_off.upload(off.data(), np + 1, stream);
+        B.d_plist.alloc(plist.size());
+        B.d_plist.upload(plist.data(), plist.size(), stream);
+        B.n_dev = (int)n;
+        B.dirty = false;
+    }
+
+    void setup(double3 mn, double3 mx)
+    {
+        FD_CUDA(cudaSetDevice(device));
+        if (geo_dirty) {
+            pgeo.build(false, stream);
+            wgeo.build(true, stream);
+            pmat.upload(stream);
+            wmat.upload(stream);
+            geo_dirty = false;
+        }
+        const bool counts_changed = (P.n() != P.n_dev) || !setup_done;
+        if (P.dirty || counts_changed) {
+            build_node_base();
+            P.upload(node_base, stream);
+        }
+        if (W.dirty || W.n() != W.n_dev) {
+            std::vector<int> zeros(W.pos.size(), 0);
+            W.upload(zeros, stream);
+        }
+        if (bonds.dirty || bonds.n_dev != (int)bonds.master.size()) upload_bonds();
+        const double pcell = P.n() > 0 ? 2.0 * pgeo.rmax : 0.0;
+        const double wcell = W.n() > 0 ? 2.0 * wgeo.rmax : 0.0;
+        pgrid = make_grid(mn, mx, pcell, setup_done ? &pgrid : nullptr);
+        wgrid = make_grid(mn, mx, wcell, setup_done ? &wgrid : nullptr);
+        ptab.alloc(pgrid, P.n());
+        wcount.alloc((size_t)std::max<long long>(wgrid.num, 1));
+        const int np = P.n();
+        const int nw = W.n();
+        // capacities (grown after the first detection)
+        const int kinds_cap[FD_NKIND] = {std::max(64, 16 * np), std::max(64, np * std::min(nw, 8)),
+                                         std::max(64, 4 * np), std::max(64, 4 * np), std::max(64, 4 * np)};
+        for (int k = 0; k < FD_NKIND; ++k) {
+            if (!lists[k].allocated || counts_changed) lists[k].alloc(np, kinds_cap[k], 4 * kinds_cap[k]);
+        }
+        const bool act[3] = {perX, perY, perX && perY};
+        for (int d = 0; d < 3; ++d) {
+            ghosts[d].active = act[d];
+            if (act[d]) {
+                ghosts[d].pos.alloc(std::max(np, 1));
+                ghosts[d].hash.alloc(std::max(np, 1));
+                ghosts[d].cells.alloc(pgrid, np);
+            }
+        }
+        size_t st = std::max<size_t>(fd::scan_tmp_size(pgrid.num), fd::scan_tmp_size(np));
+        scan_tmp.alloc(st + 16);
+        if (!flags.p) flags.alloc(1);
+        FD_CUDA(cudaStreamSynchronize(stream));
+        setup_done = true;
+    }
+
+    // hash + detection (+ forces) of one step, LSSolver.h:1201-1215
+    void detect_all(bool with_force, double dt)
+    {
+        ObjDev Pv = P.view(), Wv = W.view();
+        GeoSetDev G = pgeo.view(), GW = wgeo.view();
+        fd::MatDev M = pmat.view(), MW = wmat.view();
+        fd::StepArgs a = step_args(dt);
+        CellTableDev T = ptab.view();
+        fd::launch_hash_count(Pv, T, stream);
+        fd::launch_cell_table(Pv, T, scan_tmp.p, scan_tmp.n, stream);
+        launches += 3;
+        // wall hash (visibility and cell for the node test)
+        if (W.n_dev > 0) {
+            CellTableDev wt{wgrid, wcount.p, nullptr, nullptr, nullptr};
+            fd::launch_hash_count(Wv, wt, stream);
+            launches += 1;
+        }
+        int active[FD_NKIND] = {1, 1, 0, 0, 0};
+        for (int k = 0; k < FD_NKIND; ++k) lists[k].cur ^= 1;
+        PairListDev Lpp = lists[FD_PP].view();
+        fd::launch_broad_pp(Pv, G, T, Lpp, flags.p, stream);
+        fd::launch_narrow(FD_PP, Pv, G, M, Wv, GW, MW, pgrid, wgrid, nullptr, Lpp, a, with_force, stream);
+        PairListDev Lpw = lists[FD_PW].view();
+        fd::launch_broad_pw(Pv, G, Wv, GW, wgrid, Lpw, flags.p, stream);
+        fd::launch_narrow(FD_PW, Pv, G, M, Wv, GW, MW, pgrid, wgrid, nullptr, Lpw, a, with_force, stream);
+        launches += 4;
+        PairListDev Lg[3];
+        if (perX || perY) {
+            const int kinds[3] = {FD_GX, FD_GY, FD_GXY};
+            for (int d = 0; d < 3; ++d) {
+                if (!ghosts[d].active) continue;
+                if (d == 0) { fd::launch_wrap(Pv, pgrid, 0, stream); launches++; }
+                if (d == 1) { fd::launch_wrap(Pv, pgrid, 1, stream); launches++; }
+                fd::GhostDev gh = ghosts[d].view();
+                fd::launch_ghost_build(Pv, gh, kinds[d], stream);
+                ObjDev ghostobj = Pv;
+                ghostobj.hash = ghosts[d].hash.p;
+                fd::launch_cell_table(ghostobj, gh.cells, scan_tmp.p, scan_tmp.n, stream);
+                launches += 3;
+            }
+            for (int d = 0; d < 3; ++d) {
+                if (!ghosts[d].active) continue;
+                fd::GhostDev gh = ghosts[d].view();
+                Lg[d] = lists[kinds[d]].view();
+                fd::launch_broad_ghost(Pv, G, gh, Lg[d], flags.p, stream);
+                fd::launch_narrow(kinds[d], Pv, G, M, Wv, GW, MW, pgrid, wgrid, &gh, Lg[d], a, with_force, stream);
+                active[kinds[d]] = 1;
+                launches += 2;
+            }
+        }
+        if (!with_force) return;
+        fd::launch_reverse(Pv, Lpp, scan_tmp.p, scan_tmp.n, stream);
+        launches += 4;
+        for (int d = 0; d < 3; ++d)
+            if (ghosts[d].active) {
+                PairListDev L = lists[FD_GX + d].view();
+                fd::launch_reverse(Pv, L, scan_tmp.p, scan_tmp.n, stream);
+                launches += 4;
+            }
+        fd::BondDev bd = bond_view();
+        if (bd.n > 0) { fd::launch_bonds(Pv, bd, stream); launches++; }
+        PairListDev views[FD_NKIND];
+        for (int k = 0; k < FD_NKIND; ++k) views[k] = lists[k].view();
+        fd::launch_reduce(Pv, views, active, bd, stream);
+        launches++;
+    }
+
+    // copy the device state of a set back into its host mirror
+    void pull(ObjHost& O)
+    {
+        if (!(O.n_dev == O.n() && !O.dirty && O.n() > 0)) return;
+        FD_CUDA(cudaStreamSynchronize(stream));
+        const size_t n = O.n();
+        FD_CUDA(cudaMemcpy(O.pos.data(), O.d_pos.p, sizeof(double3) * n, cudaMemcpyDeviceToHost));
+        FD_CUDA(cudaMemcpy(O.vel.data(), O.d_vel.p, sizeof(double3) * n, cudaMemcpyDeviceToHost));
+        FD_CUDA(cudaMemcpy(O.angvel.data(), O.d_angvel.p, sizeof(double3) * n, cudaMemcpyDeviceToHost));
+        FD_CUDA(cudaMemcpy(O.q.data(), O.d_q.p, sizeof(fd_quat) * n, cudaMemcpyDeviceToHost));
+        FD_CUDA(cudaMemcpy(O.force.data(), O.d_force.p, sizeof(double3) * n, cudaMemcpyDeviceToHost));
+        FD_CUDA(cudaMemcpy(O.torque.data(), O.d_torque.p, sizeof(double3) * n, cudaMemcpyDeviceToHost));
+    }
+
+    // grow list capacities to three times the last counts when they come
+    // within a factor two of the limit (synchronises the stream)
+    void ensure_capacity()
+    {
+        FD_CUDA(cudaStreamSynchronize(stream));
+        for (int k = 0; k < FD_NKIND; ++k) {
+            PairList& L = lists[k];
+            if (!L.allocated) continue;
+            int c[2] = {0, 0};
+            FD_CUDA(cudaMemcpy(c, L.gen[L.cur].counters.p, sizeof(c), cudaMemcpyDeviceToHost));
+            const int needp = 2 * c[0] > L.cap_pairs ? 3 * c[0] : 0;
+            const int needc = 2 * c[1] > L.cap_contacts ? 3 * c[1] : 0;
+            if (needp || needc) L.grow(std::max(needp, L.cap_pairs), std::max(needc, L.cap_contacts));
+        }
+    }
+
+    void front(double3 g, double dt)
+    {
+        ObjDev Pv = P.view(), Wv = W.view();
+        fd::launch_kick(Pv, pgeo.view(), g, 0.5 * dt, stream);
+        fd::launch_drift(Pv, dt, stream);
+        fd::launch_drift(Wv, dt, stream);
+        launches += 3;
+    }
+    void back(double3 g, double dt)
+    {
+        fd::launch_kick(P.view(), pgeo.view(), g, 0.5 * dt, stream);
+        launches++;
+    }
+};
+
+namespace {
+int guard(fundem_sim* s, const std::function<void()>& f)
+{
+    try {
+        f();
+        return FUNDEM_OK;
+    } catch (const CudaError& e) {
+        if (s) s->last_error = e.what();
+        return FUNDEM_ERR_CUDA;
+    } catch (const std::invalid_argument& e) {
+        if (s) s->last_error = e.what();
+        return FUNDEM_ERR_ARG;
+    } catch (const std::logic_error& e) {
+        if (s) s->last_error = e.what();
+        return FUNDEM_ERR_STATE;
+    } catch (const std::exception& e) {
+        if (s) s->last_error = e.what();
+        return FUNDEM_ERR_CUDA;
+    }
+}
+double3 d3(const double* p) { return make_double3(p[0], p[1], p[2]); }
+// host rotations used by bond creation (myQua.h:104-128, host branch)
+double3 hrot(const fd_quat& q, double3 v)
+{
+    const double3 qv = make_double3(q.q1, q.q2, q.q3);
+    const double3 t = cross3(qv, v) * 2.0;
+    return v + t * q.q0 + cross3(qv, t);
+}
+double3 hrrot(double3 v, const fd_quat& q)
+{
+    const double3 qv = make_double3(-q.q1, -q.q2, -q.q3);
+    const double3 t = cross3(qv, v) * 2.0;
+    return v + t * q.q0 + cross3(qv, t);
+}
+double3 hnormalize(double3 v)
+{
+    const double l2 = v.x * v.x + v.y * v.y + v.z * v.z;
+    if (fd_is_zero(l2)) return make_double3(0, 0, 0);
+    const double inv = 1.0 / std::sqrt(l2);
+    return make_double3(v.x * inv, v.y * inv, v.z * inv);
+}
+fd_quat hnormalize_q(fd_quat q)
+{
+    const double l2 = q.q0 * q.q0 + q.q1 * q.q1 + q.q2 * q.q2 + q.q3 * q.q3;
+    if (fd_is_zero(l2)) return q;
+    const double inv = 1.0 / std::sqrt(l2);
+    return fd_quat{q.q0 * inv, q.q1 * inv, q.q2 * inv, q.q3 * inv};
+}
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char* fundem_version(void) { return "fundem_b200 0.1 (sm_100a)"; }
+
+const char* fundem_status_string(int s)
+{
+    switch (s) {
+    case FUNDEM_OK: return "ok";
+    case FUNDEM_ERR_ARG: return "invalid argument";
+    case FUNDEM_ERR_CUDA: return "CUDA error";
+    case FUNDEM_ERR_CAPACITY: return "list capacity exceeded";
+    case FUNDEM_ERR_STATE: return "call out of order";
+    case FUNDEM_ERR_NUMERIC: return "non-finite state";
+    }
+    return "unknown status";
+}
+
+int fundem_create(fundem_sim** out, int device, void* stream)
+{
+    if (!out) return FUNDEM_ERR_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) return FUNDEM_ERR_CUDA;
+    if (cudaSetDevice(device) != cudaSuccess) return FUNDEM_ERR_CUDA;
+    fundem_sim* s = new fundem_sim();
+    s->device = device;
+    s->stream = (cudaStream_t)stream;
+    *out = s;
+    return FUNDEM_OK;
+}
+
+int fundem_destroy(fundem_sim* s)
+{
+    if (!s) return FUNDEM_ERR_ARG;
+    cudaSetDevice(s->device);
+    cudaStreamSynchronize(s->stream);
+    delete s;
+    return FUNDEM_OK;
+}
+
+int fundem_set_precision(fundem_sim* s, int mode)
+{
+    if (!s || (mode != FUNDEM_FP64 && mode != FUNDEM_FP32_MIXED)) return FUNDEM_ERR_ARG;
+    s->precision = mode;
+    return FUNDEM_OK;
+}
+
+int fundem_set_records(fundem_sim* s, int full)
+{
+    if (!s) return FUNDEM_ERR_ARG;
+    s->records = full ? 1 : 0;
+    return FUNDEM_OK;
+}
+
+int fundem_add_material(fundem_sim* s, int wall, double kn, double ks, double mu, double e, int* id_out)
+{
+    if (!s) return FUNDEM_ERR_ARG;
+    MatHost& m = wall ? s->wmat : s->pmat;
+    if (wall) { kn = 0.0; ks = 0.0; }
+    m.kn.push_back(kn > 0. ? kn : 0.0);
+    m.ks.push_back(ks > 0. ? ks : 0.0);
+    m.mu.push_back(mu > 0. ? mu : 0.0);
+    m.e.push_back((e > 0. && e < 1.0) ? e : 1.0);
+    if (id_out) *id_out = (int)m.kn.size() - 1;
+    s->geo_dirty = true;
+    return FUNDEM_OK;
+}
+
+int fundem_add_geometry(fundem_sim* s, int wall, double mass, const double inertia[6], const double origin[3],
+                        double spacing, const int size[3], const double* sdf, int n_nodes, const double* nodes,
+                        int* id_out)
+{
+    if (!s || !origin || !size || !sdf || n_nodes < 0 || (n_nodes > 0 && !nodes)) return FUNDEM_ERR_ARG;
+    if (size[0] < 2 || size[1] < 2 || size[2] < 2 || !(spacing > 0.0)) return FUNDEM_ERR_ARG;
+    HostGeo g;
+    g.mass = wall ? 0.0 : mass;
+    if (inertia && !wall) g.inertia = fd_sym{inertia[0], inertia[1], inertia[2], inertia[3], inertia[4], inertia[5]};
+    g.origin = d3(origin);
+    g.spacing = spacing;
+    g.size = make_int3(size[0], size[1], size[2]);
+    const size_t ns = (size_t)size[0] * size[1] * size[2];
+    g.sdf.assign(sdf, sdf + ns);
+    for (int k = 0; k < n_nodes; ++k) g.nodes.push_back(d3(nodes + 3 * k));
+    GeoSetHost& set = wall ? s->wgeo : s->pgeo;
+    set.geos.push_back(std::move(g));
+    if (id_out) *id_out = (int)set.geos.size() - 1;
+    s->geo_dirty = true;
+    return FUNDEM_OK;
+}
+
+int fundem_mass_properties(double density, const double origin[3], double h, const int size[3], const double* sdf,
+                           double* mass_out, double centroid[3], double inertia[6])
+{
+    if (!origin || !size || !sdf || size[0] < 2 || size[1] < 2 || size[2] < 2 || !(h > 0.0)) return FUNDEM_ERR_ARG;
+    const double PI = 3.14159265358979323846;
+    auto H = [&](double phi) {
+        const double sp = 1.5;
+        if (phi < -sp) return 1.0;
+        if (phi > sp) return 0.0;
+        const double x = -phi / sp;
+        return 0.5 * (1.0 + x + std::sin(PI * x) / PI);
+    };
+    const double mg = density * h * h * h;
+    double mass = 0.0;
+    auto idx = [&](int x, int y, int z) { return (size_t)z * size[1] * size[0] + (size_t)y * size[0] + x; };
+    for (int x = 0; x < size[0]; x++)
+        for (int y = 0; y < size[1]; y++)
+            for (int z = 0; z < size[2]; z++) mass += H(sdf[idx(x, y, z)] / h);
+    mass *= mg;
+    double3 c = make_double3(0, 0, 0);
+    fd_sym I{0, 0, 0, 0, 0, 0};
+    if (mass > 0.) {
+        for (int x = 0; x < size[0]; x++)
+            for (int y = 0; y < size[1]; y++)
+                for (int z = 0; z < size[2]; z++) {
+                    const double w = H(sdf[idx(x, y, z)] / h);
+                    c.x += w * (origin[0] + double(x) * h);
+                    c.y += w * (origin[1] + double(y) * h);
+                    c.z += w * (origin[2] + double(z) * h);
+                }
+        c = c * (mg / mass);
+        for (int x = 0; x < size[0]; x++)
+            for (int y = 0; y < size[1]; y++)
+                for (int z = 0; z < size[2]; z++) {
+                    const double w = H(sdf[idx(x, y, z)] / h);
+                    const double3 r = (d3(origin) + h * make_double3(double(x), double(y), double(z))) - c;
+                    I.xx += w * (r.y * r.y + r.z * r.z) * mg;
+                    I.yy += w * (r.x * r.x + r.z * r.z) * mg;
+                    I.zz += w * (r.y * r.y + r.x * r.x) * mg;
+                    I.xy -= w * r.x * r.y * mg;
+                    I.xz -= w * r.x * r.z * mg;
+                    I.yz -= w * r.y * r.z * mg;
+                }
+    }
+    if (mass_out) *mass_out = mass;
+    if (centroid) { centroid[0] = c.x; centroid[1] = c.y; centroid[2] = c.z; }
+    if (inertia) {
+        inertia[0] = I.xx; inertia[1] = I.yy; inertia[2] = I.zz;
+        inertia[3] = I.xy; inertia[4] = I.xz; inertia[5] = I.yz;
+    }
+    return FUNDEM_OK;
+}
+
+int fundem_add_objects(fundem_sim* s, int wall, int n, const double* pos, const double* vel, const double* angvel,
+                       const double* quat, const int* mat, const int* geo)
+{
+    if (!s || n < 0 || (n > 0 && (!pos || !quat || !mat || !geo))) return FUNDEM_ERR_ARG;
+    ObjHost& O = wall ? s->W : s->P;
+    const MatHost& M = wall ? s->wmat : s->pmat;
+    const GeoSetHost& G = wall ? s->wgeo : s->pgeo;
+    {
+        int r = guard(s, [&] { s->pull(O); });
+        if (r) return r;
+    }
+    for (int i = 0; i < n; ++i) {
+        // LSParticle::addParticle rejects unknown ids, LSParticle.h:276-286
+        if (mat[i] < 0 || mat[i] >= (int)M.kn.size()) return FUNDEM_ERR_ARG;
+        if (geo[i] < 0 || geo[i] >= (int)G.geos.size()) return FUNDEM_ERR_ARG;
+    }
+    for (int i = 0; i < n; ++i) {
+        O.pos.push_back(d3(pos + 3 * i));
+        O.vel.push_back(vel ? d3(vel + 3 * i) : make_double3(0, 0, 0));
+        O.angvel.push_back(angvel ? d3(angvel + 3 * i) : make_double3(0, 0, 0));
+        O.force.push_back(make_double3(0, 0, 0));
+        O.torque.push_back(make_double3(0, 0, 0));
+        O.q.push_back(hnormalize_q(fd_quat{quat[4 * i], quat[4 * i + 1], quat[4 * i + 2], quat[4 * i + 3]}));
+        O.mat.push_back(mat[i]);
+        O.geo.push_back(geo[i]);
+    }
+    O.dirty = true;
+    return FUNDEM_OK;
+}
+
+int fundem_set_wall_motion(fundem_sim* s, int index, const double vel[3], const double angvel[3])
+{
+    if (!s || index < 0 || index >= s->W.n()) return FUNDEM_ERR_ARG;
+    return guard(s, [&] {
+        s->pull(s->W);
+        if (vel) s->W.vel[index] = d3(vel);
+        if (angvel) s->W.angvel[index] = d3(angvel);
+        s->W.dirty = true;
+    });
+}
+
+int fundem_move(fundem_sim* s, int wall, int index, const double offset[3])
+{
+    if (!s || !offset) return FUNDEM_ERR_ARG;
+    ObjHost& O = wall ? s->W : s->P;
+    if (index < 0 || index >= O.n()) return FUNDEM_ERR_ARG;
+    return guard(s, [&] {
+        s->pull(O);
+        O.pos[index] = O.pos[index] + d3(offset);
+        O.dirty = true;
+    });
+}
+
+int fundem_add_bonds(fundem_sim* s, int n, const int* master, const int* slave, const double* point,
+                     const double* normal, const double* radius, const double* length, const double* young,
+                     const double* poisson, const double* tensile, const double* cohesion, const double* friction)
+{
+    if (!s || n < 0) return FUNDEM_ERR_ARG;
+    if (n > 0 && (!master || !slave || !point || !normal || !radius || !length || !young || !poisson))
+        return FUNDEM_ERR_ARG;
+    // bonds are built from the current host-side state (the reference reads
+    // positionHostRef/orientationHostRef, LSSolver.h:300-316)
+    {
+        int r = guard(s, [&] { s->pull(s->P); });
+        if (r) return r;
+    }
+    const double PI = 3.14159265358979323846;
+    BondHost& B = s->bonds;
+    int added = 0;
+    for (int k = 0; k < n; ++k) {
+        const int mi = master[k], sj = slave[k];
+        if (mi < 0 || sj < 0 || mi >= s->P.n() || sj >= s->P.n()) continue;  // LSSolver.h:300
+        const double3 gn = d3(normal + 3 * k);
+        const double Rb = radius[k], Lb = length[k], Eb = young[k], nu = poisson[k];
+        if (fd_is_zero(lengthSq3(gn)) || Rb <= 0. || Lb <= 0. || Eb <= 0. || nu <= -1.0 || nu >= 0.5) continue;
+        const double Gb = Eb / (2. * (1. + nu));
+        const double Ab = PI * Rb * Rb;
+        const double Ib = Ab * Rb * Rb / 4.;
+        const double Jb = 2. * Ib;
+        const double Kn = Eb * Ab / Lb, Kt = Gb * Jb / Lb, Ks = 12. * Eb * Ib / (Lb * Lb * Lb), Kb = Eb * Ib / Lb;
+        const double B1 = Kn, B2 = Lb * Lb * Ks, B4 = Kt, B3 = Kb - B2 / 4. - B4 / 2.;
+        const double3 nn = gn * (1.0 / std::sqrt(gn.x * gn.x + gn.y * gn.y + gn.z * gn.z));
+        const double3 c = d3(point + 3 * k);
+        const double3 gpi = c + (0.5 * Lb) * nn, gpj = c - (0.5 * Lb) * nn;
+        const fd_quat qi = s->P.q[mi], qj = s->P.q[sj];
+        const double3 lpi = hrrot(gpi - s->P.pos[mi], qi);
+        const double3 lpj = hrrot(gpj - s->P.pos[sj], qj);
+        const double3 n1i = -nn;
+        const double3 ref = (std::fabs(n1i.x) < 0.9) ? make_double3(1., 0., 0.) : make_double3(0., 1., 0.);
+        const double3 n2i = hnormalize(cross3(ref, n1i));
+        const double3 n3i = hnormalize(cross3(n1i, n2i));
+        const double3 n1j = -n1i, n2j = n2i, n3j = n3i;
+        B.master.push_back(mi);
+        B.slave.push_back(sj);
+        B.active.push_back(1);
+        B.point.push_back(c);
+        B.B.insert(B.B.end(), {B1, B2, B3, B4});
+        B.radius.push_back(Rb);
+        B.L0.push_back(Lb);
+        B.ts.push_back(tensile ? tensile[k] : 0.0);
+        B.coh.push_back(cohesion ? cohesion[k] : 0.0);
+        B.mu.push_back(friction ? friction[k] : 0.0);
+        B.energy.insert(B.energy.end(), {0., 0., 0., 0., 0., 0.});
+        B.frames.push_back(hnormalize(hrrot(n1i, qi)));
+        B.frames.push_back(hnormalize(hrrot(n2i, qi)));
+        B.frames.push_back(hnormalize(hrrot(n3i, qi)));
+        B.frames.push_back(lpi);
+        B.frames.push_back(hnormalize(hrrot(n1j, qj)));
+        B.frames.push_back(hnormalize(hrrot(n2j, qj)));
+        B.frames.push_back(hnormalize(hrrot(n3j, qj)));
+        B.frames.push_back(lpj);
+        ++added;
+    }
+    B.dirty = true;
+    return added == n ? FUNDEM_OK : FUNDEM_ERR_ARG;
+}
+
+int fundem_set_periodic(fundem_sim* s, int x, int y)
+{
+    if (!s) return FUNDEM_ERR_ARG;
+    s->perX = x != 0;
+    s->perY = y != 0;
+    return FUNDEM_OK;
+}
+
+int fundem_setup(fundem_sim* s, const double mn[3], const double mx[3])
+{
+    if (!s || !mn || !mx) return FUNDEM_ERR_ARG;
+    if (!(mx[0] - mn[0] > 0.0) || !(mx[1] - mn[1] > 0.0) || !(mx[2] - mn[2] > 0.0)) return FUNDEM_ERR_ARG;
+    return guard(s, [&] { s->setup(d3(mn), d3(mx)); });
+}
+
+int fundem_detect(fundem_sim* s)
+{
+    if (!s) return FUNDEM_ERR_ARG;
+    if (!s->setup_done) return FUNDEM_ERR_STATE;
+    return guard(s, [&] {
+        FD_CUDA(cudaSetDevice(s->device));
+        s->detect_all(false, 0.0);
+        s->ensure_capacity();
+        s->detected = true;
+    });
+}
+
+int fundem_step_begin(fundem_sim* s, const double g[3], double dt)
+{
+    if (!s || !g) return FUNDEM_ERR_ARG;
+    if (!s->setup_done) return FUNDEM_ERR_STATE;
+    return guard(s, [&] {
+        s->front(d3(g), dt);
+        s->detect_all(true, dt);
+    });
+}
+
+int fundem_step_end(fundem_sim* s, const double g[3], double dt)
+{
+    if (!s || !g) return FUNDEM_ERR_ARG;
+    if (!s->setup_done) return FUNDEM_ERR_STATE;
+    return guard(s, [&] { s->back(d3(g), dt); });
+}
+
+int fundem_step(fundem_sim* s, int nsteps, const double g[3], double dt)
+{
+    if (!s || !g || nsteps < 0) return FUNDEM_ERR_ARG;
+    if (!s->setup_done) return FUNDEM_ERR_STATE;
+    return guard(s, [&] {
+        FD_CUDA(cudaSetDevice(s->device));
+        for (int k = 0; k < nsteps; ++k) {
+            s->front(d3(g), dt);
+            s->detect_all(true, dt);
+            s->back(d3(g), dt);
+        }
+        FD_CUDA(cudaGetLastError());
+    });
+}
+
+int fundem_sync(fundem_sim* s)
+{
+    if (!s) return FUNDEM_ERR_ARG;
+    unsigned int f = 0;
+    int r = guard(s, [&] {
+        FD_CUDA(cudaStreamSynchronize(s->stream));
+        FD_CUDA(cudaGetLastError());
+        if (s->flags.p) FD_CUDA(cudaMemcpy(&f, s->flags.p, sizeof(unsigned int), cudaMemcpyDeviceToHost));
+    });
+    if (r) return r;
+    if (f & (FD_FLAG_PAIR_OVERFLOW | FD_FLAG_CONTACT_OVERFLOW | FD_FLAG_NEIGHBOR_OVERFLOW | FD_FLAG_CLUSTER_OVERFLOW))
+        return FUNDEM_ERR_CAPACITY;
+    if (f & FD_FLAG_NONFINITE) return FUNDEM_ERR_NUMERIC;
+    return FUNDEM_OK;
+}
+
+int fundem_status_word(fundem_sim* s, unsigned int* out)
+{
+    if (!s || !out) return FUNDEM_ERR_ARG;
+    *out = 0;
+    if (!s->flags.p) return FUNDEM_OK;
+    return guard(s, [&] {
+        FD_CUDA(cudaMemcpyAsync(out, s->flags.p, sizeof(unsigned int), cudaMemcpyDeviceToHost, s->stream));
+    });
+}
+
+int fundem_num_objects(fundem_sim* s, int wall, int* n)
+{
+    if (!s || !n) return FUNDEM_ERR_ARG;
+    *n = wall ? s->W.n() : s->P.n();
+    return FUNDEM_OK;
+}
+
+int fundem_get_objects(fundem_sim* s, int wall, double* pos, double* vel, double* angvel, double* quat, double* force,
+                       double* torque)
+{
+    if (!s) return FUNDEM_ERR_ARG;
+    ObjHost& O = wall ? s->W : s->P;
+    return guard(s, [&] {
+        const size_t n = O.n();
+        const bool dev = (O.n_dev == (int)n) && !O.dirty && n > 0;
+        auto get = [&](double* dst, const void* dsrc, const void* hsrc, size_t bytes) {
+            if (!dst || bytes == 0) return;
+            if (dev) FD_CUDA(cudaMemcpyAsync(dst, dsrc, bytes, cudaMemcpyDeviceToHost, s->stream));
+            else std::memcpy(dst, hsrc, bytes);
+        };
+        get(pos, O.d_pos.p, O.pos.data(), sizeof(double3) * n);
+        get(vel, O.d_vel.p, O.vel.data(), sizeof(double3) * n);
+        get(angvel, O.d_angvel.p, O.angvel.data(), sizeof(double3) * n);
+        get(quat, O.d_q.p, O.q.data(), sizeof(fd_quat) * n);
+        get(force, O.d_force.p, O.force.data(), sizeof(double3) * n);
+        get(torque, O.d_torque.p, O.torque.data(), sizeof(double3) * n);
+        FD_CUDA(cudaStreamSynchronize(s->stream));
+    });
+}
+
+int fundem_set_objects(fundem_sim* s, int wall, const double* pos, const double* vel, const double* angvel,
+                       const double* quat, const double* force, const double* torque)
+{
+    if (!s) return FUNDEM_ERR_ARG;
+    ObjHost& O = wall ? s->W : s->P;
+    return guard(s, [&] {
+        const size_t n = O.n();
+        const bool dev = (O.n_dev == (int)n) && !O.dirty && n > 0;
+        auto put = [&](void* ddst, void* hdst, const double* src, size_t bytes) {
+            if (!src || bytes == 0) return;
+            std::memcpy(hdst, src, bytes);
+            if (dev) FD_CUDA(cudaMemcpyAsync(ddst, src, bytes, cudaMemcpyHostToDevice, s->stream));
+        };
+        put(O.d_pos.p, O.pos.data(), pos, sizeof(double3) * n);
+        put(O.d_vel.p, O.vel.data(), vel, sizeof(double3) * n);
+        put(O.d_angvel.p, O.angvel.data(), angvel, sizeof(double3) * n);
+        put(O.d_q.p, O.q.data(), quat, sizeof(fd_quat) * n);
+        put(O.d_force.p, O.force.data(), force, sizeof(double3) * n);
+        put(O.d_torque.p, O.torque.data(), torque, sizeof(double3) * n);
+        FD_CUDA(cudaStreamSynchronize(s->stream));
+    });
+}
+
+int fundem_device_view_get(fundem_sim* s, int wall, fundem_device_view* out)
+{
+    if (!s || !out) return FUNDEM_ERR_ARG;
+    if (!s->setup_done) return FUNDEM_ERR_STATE;
+    ObjHost& O = wall ? s->W : s->P;
+    out->pos = (double*)O.d_pos.p;
+    out->vel = (double*)O.d_vel.p;
+    out->angvel = (double*)O.d_angvel.p;
+    out->force = (double*)O.d_force.p;
+    out->torque = (double*)O.d_torque.p;
+    out->quat = (double*)O.d_q.p;
+    out->mat = O.d_mat.p;
+    out->geo = O.d_geo.p;
+    out->n = O.n_dev;
+    return FUNDEM_OK;
+}
+
+int fundem_num_pairs(fundem_sim* s, int kind, long long* n)
+{
+    if (!s || !n || kind < 0 || kind >= FD_NKIND) return FUNDEM_ERR_ARG;
+    *n = 0;
+    PairList& L = s->lists[kind];
+    if (!L.allocated) return FUNDEM_OK;
+    return guard(s, [&] {
+        int c[2] = {0, 0};
+        FD_CUDA(cudaStreamSynchronize(s->stream));
+        FD_CUDA(cudaMemcpy(c, L.gen[L.cur].counters.p, sizeof(c), cudaMemcpyDeviceToHost));
+        *n = std::min(c[0], L.cap_pairs);
+    });
+}
+
+int fundem_num_contacts(fundem_sim* s, int kind, long long* n)
+{
+    if (!s || !n || kind < 0 || kind >= FD_NKIND) return FUNDEM_ERR_ARG;
+    *n = 0;
+    PairList& L = s->lists[kind];
+    if (!L.allocated) return FUNDEM_OK;
+    return guard(s, [&] {
+        int c[2] = {0, 0};
+        FD_CUDA(cudaStreamSynchronize(s->stream));
+        FD_CUDA(cudaMemcpy(c, L.gen[L.cur].counters.p, sizeof(c), cudaMemcpyDeviceToHost));
+        *n = std::min(c[1], L.cap_contacts);
+    });
+}
+
+int fundem_get_contacts(fundem_sim* s, int kind, int* node, int* partner, double* point, double* normal,
+                        double* overlap, double* spring, double* en, double* es)
+{
+    if (!s || kind < 0 || kind >= FD_NKIND) return FUNDEM_ERR_ARG;
+    PairList& L = s->lists[kind];
+    if (!L.allocated) return FUNDEM_OK;
+    return guard(s, [&] {
+        int c[2] = {0, 0};
+        FD_CUDA(cudaStreamSynchronize(s->stream));
+        PairGen& g = L.gen[L.cur];
+        FD_CUDA(cudaMemcpy(c, g.counters.p, sizeof(c), cudaMemcpyDeviceToHost));
+        const size_t n = (size_t)std::min(c[1], L.cap_contacts);
+        std::vector<int> hn(n), hs(n);
+        std::vector<double> hsp(3 * n), hpt(3 * n), hnm(3 * n), hov(n), hen(n), hes(n);
+        if (n) {
+            FD_CUDA(cudaMemcpy(hn.data(), g.c_node.p, sizeof(int) * n, cudaMemcpyDeviceToHost));
+            FD_CUDA(cudaMemcpy(hs.data(), g.c_slave.p, sizeof(int) * n, cudaMemcpyDeviceToHost));
+            FD_CUDA(cudaMemcpy(hsp.data(), g.c_spring.p, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost));
+            FD_CUDA(cudaMemcpy(hpt.data(), g.c_point.p, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost));
+            FD_CUDA(cudaMemcpy(hnm.data(), g.c_normal.p, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost));
+            FD_CUDA(cudaMemcpy(hov.data(), g.c_overlap.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
+            FD_CUDA(cudaMemcpy(hen.data(), g.c_en.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
+            FD_CUDA(cudaMemcpy(hes.data(), g.c_es.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
+        }
+        std::vector<size_t> order(n);
+        std::iota(order.begin(), order.end(), 0);
+        std::sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+            return hn[a] != hn[b] ? hn[a] < hn[b] : hs[a] < hs[b];
+        });
+        for (size_t k = 0; k < n; ++k) {
+            const size_t j = order[k];
+            if (node) node[k] = hn[j];
+            if (partner) partner[k] = hs[j];
+            for (int d = 0; d < 3; ++d) {
+                if (spring) spring[3 * k + d] = hsp[3 * j + d];
+                if (point) point[3 * k + d] = hpt[3 * j + d];
+                if (normal) normal[3 * k + d] = hnm[3 * j + d];
+            }
+            if (overlap) overlap[k] = hov[j];
+            if (en) en[k] = hen[j];
+            if (es) es[k] = hes[j];
+        }
+    });
+}
+
+int fundem_set_contacts(fundem_sim* s, int kind, long long n, const int* node, const int* partner, const double* spring)
+{
+    if (!s || kind < 0 || kind >= FD_NKIND || n < 0 || (n > 0 && (!node || !partner || !spring))) return FUNDEM_ERR_ARG;
+    if (!s->setup_done) return FUNDEM_ERR_STATE;
+    PairList& L = s->lists[kind];
+    return guard(s, [&] {
+        // group by (particle of node, partner); the list becomes the current
+        // generation so the next detection reads it as history
+        const int np = s->P.n();
+        std::vector<size_t> order((size_t)n);
+        std::iota(order.begin(), order.end(), 0);
+        auto owner = [&](int nid) {
+            return (int)(std::upper_bound(s->node_base.begin(), s->node_base.end(), nid) - s->node_base.begin()) - 1;
+        };
+        for (long long k = 0; k < n; ++k)
+            if (node[k] < 0 || node[k] >= s->n_nodes) throw std::invalid_argument("node id out of range");
+        std::sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+            const int oa = owner(node[a]), ob = owner(node[b]);
+            if (oa != ob) return oa < ob;
+            if (partner[a] != partner[b]) return partner[a] < partner[b];
+            return node[a] < node[b];
+        });
+        std::vector<int> pairA, pairB, c_off, c_cnt, seg_off(np, 0), seg_cnt(np, 0), cn, cs;
+        std::vector<double> csp;
+        for (size_t t = 0; t < order.size(); ++t) {
+            const size_t k = order[t];
+            const int A = owner(node[k]), B = partner[k];
+            if (pairA.empty() || pairA.back() != A || pairB.back() != B) {
+                if (seg_cnt[A] == 0) seg_off[A] = (int)pairA.size();
+                seg_cnt[A]++;
+                pairA.push_back(A);
+                pairB.push_back(B);
+                c_off.push_back((int)cn.size());
+                c_cnt.push_back(0);
+            }
+            c_cnt.back()++;
+            cn.push_back(node[k]);
+            cs.push_back(B);
+            csp.insert(csp.end(), {spring[3 * k], spring[3 * k + 1], spring[3 * k + 2]});
+        }
+        L.grow(std::max<int>(L.cap_pairs, (int)pairA.size() * 2), std::max<int>(L.cap_contacts, (int)cn.size() * 2));
+        PairGen& g = L.gen[L.cur];
+        g.pairA.upload(pairA.data(), pairA.size(), s->stream);
+        g.pairB.upload(pairB.data(), pairB.size(), s->stream);
+        g.seg_off.upload(seg_off.data(), np, s->stream);
+        g.seg_cnt.upload(seg_cnt.data(), np, s->stream);
+        g.c_off.upload(c_off.data(), c_off.size(), s->stream);
+        g.c_cnt.upload(c_cnt.data(), c_cnt.size(), s->stream);
+        g.c_node.upload(cn.data(), cn.size(), s->stream);
+        g.c_slave.upload(cs.data(), cs.size(), s->stream);
+        g.c_spring.upload(csp.data(), csp.size(), s->stream);
+        const int counters[2] = {(int)pairA.size(), (int)cn.size()};
+        g.counters.upload(counters, 2, s->stream);
+        FD_CUDA(cudaStreamSynchronize(s->stream));
+    });
+}
+
+int fundem_num_bonds(fundem_sim* s, int* n)
+{
+    if (!s || !n) return FUNDEM_ERR_ARG;
+    *n = (int)s->bonds.master.size();
+    return FUNDEM_OK;
+}
+
+int fundem_get_bonds(fundem_sim* s, int* activated, double* point, double* energy6)
+{
+    if (!s) return FUNDEM_ERR_ARG;
+    BondHost& B = s->bonds;
+    return guard(s, [&] {
+        const size_t n = B.master.size();
+        const bool dev = B.n_dev == (int)n && !B.dirty && n > 0;
+        FD_CUDA(cudaStreamSynchronize(s->stream));
+        if (activated) {
+            if (dev) FD_CUDA(cudaMemcpy(activated, B.d_active.p, sizeof(int) * n, cudaMemcpyDeviceToHost));
+            else std::memcpy(activated, B.active.data(), sizeof(int) * n);
+        }
+        if (point) {
+            if (dev) FD_CUDA(cudaMemcpy(point, B.d_point.p, sizeof(double3) * n, cudaMemcpyDeviceToHost));
+            else std::memcpy(point, B.point.data(), sizeof(double3) * n);
+        }
+        if (energy6) {
+            if (dev) FD_CUDA(cudaMemcpy(energy6, B.d_energy.p, sizeof(double) * 6 * n, cudaMemcpyDeviceToHost));
+            else std::memcpy(energy6, B.energy.data(), sizeof(double) * 6 * n);
+        }
+    });
+}
+
+int fundem_set_bond_activation(fundem_sim* s, const int* activated)
+{
+    if (!s || !activated) return FUNDEM_ERR_ARG;
+    BondHost& B = s->bonds;
+    return guard(s, [&] {
+        const size_t n = B.master.size();
+        std::memcpy(B.active.data(), activated, sizeof(int) * n);
+        if (B.n_dev == (int)n && !B.dirty && n > 0)
+            FD_CUDA(cudaMemcpy(B.d_active.p, activated, sizeof(int) * n, cudaMemcpyHostToDevice));
+    });
+}
+
+int fundem_get_geometry(fundem_sim* s, int wall, int geo, double* radius, double* inv_mass, double inertia[6],
+                        double inv_inertia[6])
+{
+    if (!s) return FUNDEM_ERR_ARG;
+    GeoSetHost& G = wall ? s->wgeo : s->pgeo;
+    if (geo < 0 || geo >= (int)G.geos.size()) return FUNDEM_ERR_ARG;
+    const HostGeo& g = G.geos[geo];
+    double r = 0.0;
+    for (const double3& p : g.nodes) r = std::max(r, host_len(p));
+    const double mass = wall ? 0.0 : g.mass;
+    const fd_sym I = mass > 0.0 ? g.inertia : fd_sym{0, 0, 0, 0, 0, 0};
+    const fd_sym Ii = host_inverse(I);
+    if (radius) *radius = r;
+    if (inv_mass) *inv_mass = mass > 0.0 ? 1.0 / mass : 0.0;
+    if (inertia) { inertia[0] = I.xx; inertia[1] = I.yy; inertia[2] = I.zz; inertia[3] = I.xy; inertia[4] = I.xz; inertia[5] = I.yz; }
+    if (inv_inertia) { inv_inertia[0] = Ii.xx; inv_inertia[1] = Ii.yy; inv_inertia[2] = Ii.zz; inv_inertia[3] = Ii.xy; inv_inertia[4] = Ii.xz; inv_inertia[5] = Ii.yz; }
+    return FUNDEM_OK;
+}
+
+int fundem_get_grid(fundem_sim* s, int wall, double minb[3], double maxb[3], double inv_cell[3], int size[3])
+{
+    if (!s) return FUNDEM_ERR_ARG;
+    if (!s->setup_done) return FUNDEM_ERR_STATE;
+    const FdGrid& g = wall ? s->wgrid : s->pgrid;
+    if (minb) { minb[0] = g.minb.x; minb[1] = g.minb.y; minb[2] = g.minb.z; }
+    if (maxb) { maxb[0] = g.maxb.x; maxb[1] = g.maxb.y; maxb[2] = g.maxb.z; }
+    if (inv_cell) { inv_cell[0] = g.inv.x; inv_cell[1] = g.inv.y; inv_cell[2] = g.inv.z; }
+    if (size) { size[0] = g.size.x; size[1] = g.size.y; size[2] = g.size.z; }
+    return FUNDEM_OK;
+}
+
+int fundem_launch_count(fundem_sim* s, long long* n)
+{
+    if (!s || !n) return FUNDEM_ERR_ARG;
+    *n = s->launches;
+    return FUNDEM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,1008 @@
+// fd_kernels.cu -- sm_100a kernels of the level-set DEM timestep.
+//
+// Per step (one CUDA stream, no host synchronisation):
+//   kick + drift (+ wall drift)            particleIntegrationKernel.cu:3-48
+//   hash + counting sort into a dense cell table
+//                                          mySpatialGrid.cu:4-26, buildHashStartEnd.cu:47-137
+//   broad phase: one thread per particle lists candidate partners (bounding
+//                spheres, or SDF-grid spheres for walls and ghosts), sorted
+//                by partner id, into an A-major pair list
+//   narrow phase + contact force, fused: one warp per candidate pair streams
+//                A's surface nodes cluster by cluster through B's SDF,
+//                culls whole clusters with exact-conservative bounds, applies
+//                the reference's node predicate bit for bit
+//                (LSParticleContactDetectionKernel.cu:4-607), carries the
+//                sliding spring from the previous step, evaluates the linear
+//                spring-dashpot law (contactKernel.cuh:4-77) and reduces the
+//                pair's force and torques with warp shuffles
+//   reverse index of the pair list (pairs grouped by partner)
+//   bonds (contactKernel.cu:293-371), one thread per bond
+//   per-particle reduction in a fixed order (no atomics on forces)
+#include "fd_kernels.cuh"
+
+#include <cstdio>
+
+namespace fd {
+
+namespace {
+
+constexpr int TPB = 256;
+constexpr int MAX_CAND = 64;        // candidate partners per particle and kind
+constexpr int MAX_CLUSTERS = 64;    // clusters per template (two warp-wide batches)
+constexpr int NARROW_WARPS = 8;     // warps per block in the narrow kernel
+constexpr double PI_D = 3.14159265358979323846;
+
+inline int nblocks(long long n, int tpb = TPB) { return (int)((n + tpb - 1) / tpb); }
+
+__device__ __forceinline__ void set_flag(unsigned int* flags, unsigned int f)
+{
+    if (flags) atomicOr(flags, f);
+}
+
+// ---------------------------------------------------------------------------
+// scan (exclusive, int), three-phase: tile scan, scan of tile sums, add
+// ---------------------------------------------------------------------------
+constexpr int SCAN_TPB = 512;
+constexpr int SCAN_ITEMS = 8;
+constexpr int SCAN_TILE = SCAN_TPB * SCAN_ITEMS;
+
+__device__ __forceinline__ int block_excl_scan(int v, int* total)
+{
+    __shared__ int warp_sum[SCAN_TPB / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sum[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        int s = (lane < SCAN_TPB / 32) ? warp_sum[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        if (lane < SCAN_TPB / 32) warp_sum[lane] = s;
+    }
+    __syncthreads();
+    const int before = (wid > 0) ? warp_sum[wid - 1] : 0;
+    if (total) *total = warp_sum[SCAN_TPB / 32 - 1];
+    const int r = before + x - v;
+    __syncthreads();
+    return r;
+}
+
+__global__ void k_scan_tile(const int* in, int* out, long long n, int* tile_sums)
+{
+    const long long base = (long long)blockIdx.x * SCAN_TILE + (long long)threadIdx.x * SCAN_ITEMS;
+    int v[SCAN_ITEMS];
+    int s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+        const long long i = base + k;
+        v[k] = (i < n) ? in[i] : 0;
+        s += v[k];
+    }
+    int total;
+    int run = block_excl_scan(s, &total);
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+        const long long i = base + k;
+        if (i < n) out[i] = run;
+        run += v[k];
+    }
+    if (tile_sums && threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+__global__ void k_scan_add(int* out, long long n, const int* tile_off)
+{
+    const long long i = (long long)blockIdx.x * SCAN_TILE + threadIdx.x;
+    const int add = tile_off[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+        const long long j = i + (long long)k * SCAN_TPB;
+        if (j < n && j < (long long)(blockIdx.x + 1) * SCAN_TILE) out[j] += add;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// integration, particleIntegrationKernel.cu:3-48 and myQua.h:77-93
+// ---------------------------------------------------------------------------
+__global__ void k_kick(ObjDev P, GeoSetDev G, double3 g, double h)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.n) return;
+    const int gi = P.geo[i];
+    const FdGeo& geo = G.geo[gi];
+    const double invM = geo.inv_mass;
+    if (fd_is_zero(invM)) return;
+    P.vel[i] = P.vel[i] + (P.force[i] * invM + g) * h;
+    const double3 w = P.angvel[i];
+    const fd_quat q = P.q[i];
+    const double3 Iw = fd_smv(fd_rot_tensor(q, geo.inertia), w);
+    P.angvel[i] = w + fd_smv(fd_rot_tensor(q, geo.inv_inertia), P.torque[i] - cross3(w, Iw)) * h;
+}
+
+__device__ __forceinline__ fd_quat quat_integrate(fd_quat q, double3 w, double dt)
+{
+    const double3 v = w * (0.5 * dt);
+    fd_quat d;
+    d.q0 = -q.q1 * v.x - q.q2 * v.y - q.q3 * v.z;
+    d.q1 = q.q0 * v.x + q.q3 * v.y - q.q2 * v.z;
+    d.q2 = -q.q3 * v.x + q.q0 * v.y + q.q1 * v.z;
+    d.q3 = q.q2 * v.x - q.q1 * v.y + q.q0 * v.z;
+    fd_quat s = {q.q0 + d.q0, q.q1 + d.q1, q.q2 + d.q2, q.q3 + d.q3};
+    return fd_normalize_q(s);
+}
+
+__global__ void k_drift(ObjDev O, double dt)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= O.n) return;
+    O.pos[i] = O.pos[i] + dt * O.vel[i];
+    O.q[i] = quat_integrate(O.q[i], O.angvel[i], dt);
+}
+
+// ---------------------------------------------------------------------------
+// hashing and the dense cell table (counting sort)
+// ---------------------------------------------------------------------------
+__global__ void k_hash_count(ObjDev O, FdGrid g, int* count)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= O.n) return;
+    const long long h = fd_hash(O.pos[i], g);
+    O.hash[i] = h;
+    if (h >= 0 && h < g.num) atomicAdd(&count[h], 1);
+}
+
+__global__ void k_scatter(const long long* hash, int n, long long num, const int* start, int* fill, int* sorted)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const long long h = hash[i];
+    if (h < 0 || h >= num) return;
+    const int slot = start[h] + atomicAdd(&fill[h], 1);
+    sorted[slot] = i;
+}
+
+// ---------------------------------------------------------------------------
+// periodic wrap and ghosts, mySpatialGrid.cu:28-56, 87-152, 214-240
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double3 wrap_x(double3 p, const FdGrid& g)
+{
+    const double3 off = mk3(g.maxb.x - g.minb.x, 0., 0.);
+    if (p.x < g.minb.x) p = p + off;
+    else if (p.x >= g.maxb.x) p = p - off;
+    return p;
+}
+__device__ __forceinline__ double3 wrap_y(double3 p, const FdGrid& g)
+{
+    const double3 off = mk3(0., g.maxb.y - g.minb.y, 0.);
+    if (p.y < g.minb.y) p = p + off;
+    else if (p.y >= g.maxb.y) p = p - off;
+    return p;
+}
+
+__global__ void k_wrap(ObjDev P, FdGrid g, int dim)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.n) return;
+    P.pos[i] = dim == 0 ? wrap_x(P.pos[i], g) : wrap_y(P.pos[i], g);
+}
+
+__global__ void k_ghost_build(ObjDev P, GhostDev Gh, int kind)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.n) return;
+    const FdGrid& g = Gh.cells.g;
+    const double3 p = P.pos[i];
+    const double3 ox = mk3(g.maxb.x - g.minb.x, 0., 0.), oy = mk3(0., g.maxb.y - g.minb.y, 0.);
+    const int3 c = fd_cell_of(p, g);
+    double3 r = p;
+    if (kind == FD_GX && c.x == 0) r = r + ox;
+    if (kind == FD_GY && c.y == 0) r = r + oy;
+    if (kind == FD_GXY && c.x == 0 && c.y == 0) r = r + (ox + oy);
+    Gh.pos[i] = r;
+    // calculateGhostHashKernel, including its z test against maxBound.y (:236)
+    int3 gc = fd_cell_of(r, g);
+    bool out = false;
+    if (r.x < g.minb.x) { gc.x = 0; out = true; }
+    else if (r.x >= g.maxb.x) { gc.x = g.size.x - 1; out = true; }
+    if (r.y < g.minb.y) { gc.y = 0; out = true; }
+    else if (r.y >= g.maxb.y) { gc.y = g.size.y - 1; out = true; }
+    if (r.z < g.minb.z) { gc.z = 0; out = true; }
+    else if (r.z >= g.maxb.y) { gc.z = g.size.z - 1; out = true; }
+    const long long h = out ? fd_lin3(gc.x, gc.y, gc.z, g.size) : -1;
+    Gh.hash[i] = h;
+    if (h >= 0 && h < g.num) atomicAdd(&Gh.cells.count[h], 1);
+}
+
+// ---------------------------------------------------------------------------
+// broad phase
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int cell_index_clamped(double x, double mn, double inv, int size)
+{
+    double v = (x - mn) * inv;
+    v = fmin(fmax(v, -1.0), (double)size);
+    int c = (int)v;
+    return c < 0 ? 0 : (c > size - 1 ? size - 1 : c);
+}
+
+// cells the nodes of a body of radius r centred at c can search, in grid g
+__device__ __forceinline__ void body_search_range(double3 c, double r, const FdGrid& g, int3& lo, int3& hi)
+{
+    lo.x = max(cell_index_clamped(c.x - r, g.minb.x, g.inv.x, g.size.x) - 1, 0);
+    lo.y = max(cell_index_clamped(c.y - r, g.minb.y, g.inv.y, g.size.y) - 1, 0);
+    lo.z = max(cell_index_clamped(c.z - r, g.minb.z, g.inv.z, g.size.z) - 1, 0);
+    hi.x = min(cell_index_clamped(c.x + r, g.minb.x, g.inv.x, g.size.x) + 1, g.size.x - 1);
+    hi.y = min(cell_index_clamped(c.y + r, g.minb.y, g.inv.y, g.size.y) + 1, g.size.y - 1);
+    hi.z = min(cell_index_clamped(c.z + r, g.minb.z, g.inv.z, g.size.z) + 1, g.size.z - 1);
+}
+
+__device__ __forceinline__ void decode_cell(long long h, int3 s, int3& c)
+{
+    c.x = (int)(h % s.x);
+    c.y = (int)((h / s.x) % s.y);
+    c.z = (int)(h / ((long long)s.x * s.y));
+}
+
+__device__ void emit_pairs(int A, int* buf, int cnt, int total, PairListDev& L, unsigned int* flags)
+{
+    if (total > MAX_CAND) set_flag(flags, FD_FLAG_NEIGHBOR_OVERFLOW);
+    // insertion sort by partner id: deterministic pair order
+    for (int a = 1; a < cnt; ++a) {
+        const int v = buf[a];
+        int b = a - 1;
+        while (b >= 0 && buf[b] > v) { buf[b + 1] = buf[b]; --b; }
+        buf[b + 1] = v;
+    }
+    int base = 0;
+    if (cnt > 0) base = atomicAdd(L.n_pairs, cnt);
+    if (cnt > 0 && base + cnt > L.cap_pairs) {
+        set_flag(flags, FD_FLAG_PAIR_OVERFLOW);
+        L.seg_off[A] = 0;
+        L.seg_cnt[A] = 0;
+        return;
+    }
+    L.seg_off[A] = base;
+    L.seg_cnt[A] = cnt;
+    for (int k = 0; k < cnt; ++k) {
+        L.pairA[base + k] = A;
+        L.pairB[base + k] = buf[k];
+    }
+}
+
+constexpr double BOUND_REL = 1e-9;
+
+__global__ void k_broad_pp(ObjDev P, GeoSetDev G, CellTableDev T, PairListDev L, unsigned int* flags)
+{
+    const int A = blockIdx.x * blockDim.x + threadIdx.x;
+    if (A >= P.n) return;
+    const double3 cA = P.pos[A];
+    const double rA = G.geo[P.geo[A]].radius;
+    int3 lo, hi;
+    body_search_range(cA, rA * (1.0 + BOUND_REL), T.g, lo, hi);
+    int buf[MAX_CAND];
+    int cnt = 0, total = 0;
+    for (int z = lo.z; z <= hi.z; ++z)
+        for (int y = lo.y; y <= hi.y; ++y)
+            for (int x = lo.x; x <= hi.x; ++x) {
+                const long long h = fd_lin3(x, y, z, T.g.size);
+                const int c = T.count[h];
+                if (c == 0) continue;
+                const int s = T.start[h];
+                for (int k = s; k < s + c; ++k) {
+                    const int B = T.sorted[k];
+                    if (B <= A) continue;
+                    const double3 d = cA - P.pos[B];
+                    const double rs = rA + G.geo[P.geo[B]].radius;
+                    if (lengthSq3(d) > rs * rs * (1.0 + 4.0 * BOUND_REL)) continue;
+                    if (cnt < MAX_CAND) buf[cnt++] = B;
+                    ++total;
+                }
+            }
+    emit_pairs(A, buf, cnt, total, L, flags);
+}
+
+__global__ void k_broad_pw(ObjDev P, GeoSetDev G, ObjDev W, GeoSetDev GW, FdGrid wg, PairListDev L,
+                           unsigned int* flags)
+{
+    const int A = blockIdx.x * blockDim.x + threadIdx.x;
+    if (A >= P.n) return;
+    const double3 cA = P.pos[A];
+    const double rA = G.geo[P.geo[A]].radius;
+    int3 lo, hi;
+    body_search_range(cA, rA * (1.0 + BOUND_REL), wg, lo, hi);
+    int buf[MAX_CAND];
+    int cnt = 0, total = 0;
+    for (int w = 0; w < W.n; ++w) {
+        const long long h = W.hash[w];
+        if (h < 0 || h >= wg.num) continue;
+        int3 c;
+        decode_cell(h, wg.size, c);
+        if (c.x < lo.x || c.x > hi.x || c.y < lo.y || c.y > hi.y || c.z < lo.z || c.z > hi.z) continue;
+        const double rs = rA + GW.geo[W.geo[w]].grid_radius;
+        if (lengthSq3(cA - W.pos[w]) > rs * rs * (1.0 + 4.0 * BOUND_REL)) continue;
+        if (cnt < MAX_CAND) buf[cnt++] = w;
+        ++total;
+    }
+    emit_pairs(A, buf, cnt, total, L, flags);
+}
+
+__global__ void k_broad_ghost(ObjDev P, GeoSetDev G, GhostDev Gh, PairListDev L, unsigned int* flags)
+{
+    const int A = blockIdx.x * blockDim.x + threadIdx.x;
+    if (A >= P.n) return;
+    const double3 cA = P.pos[A];
+    const double rA = G.geo[P.geo[A]].radius;
+    const CellTableDev& T = Gh.cells;
+    int3 lo, hi;
+    body_search_range(cA, rA * (1.0 + BOUND_REL), T.g, lo, hi);
+    int buf[MAX_CAND];
+    int cnt = 0, total = 0;
+    for (int z = lo.z; z <= hi.z; ++z)
+        for (int y = lo.y; y <= hi.y; ++y)
+            for (int x = lo.x; x <= hi.x; ++x) {
+                const long long h = fd_lin3(x, y, z, T.g.size);
+                const int c = T.count[h];
+                if (c == 0) continue;
+                const int s = T.start[h];
+                for (int k = s; k < s + c; ++k) {
+                    const int j = T.sorted[k];
+                    const double rs = rA + G.geo[P.geo[j]].grid_radius;
+                    if (lengthSq3(cA - Gh.pos[j]) > rs * rs * (1.0 + 4.0 * BOUND_REL)) continue;
+                    if (cnt < MAX_CAND) buf[cnt++] = j;
+                    ++total;
+                }
+            }
+    emit_pairs(A, buf, cnt, total, L, flags);
+}
+
+// ---------------------------------------------------------------------------
+// contact law, contactKernel.cuh:4-77
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double3 sliding_spring(double3 prev, double3 sv, double3 n, double3 fn, double mu,
+                                                  double k, double c, double dt)
+{
+    double3 spring = mk3(0., 0., 0.);
+    if (mu > 0. && k > 0.) {
+        double3 p1 = prev - dot3(prev, n) * n;
+        const double ap1 = length3(p1);
+        if (!fd_is_zero(ap1)) p1 = p1 * (length3(prev) / ap1);
+        spring = p1 + sv * dt;
+        double3 sf = -k * spring - c * sv;
+        const double asf = length3(sf);
+        const double afn = length3(fn);
+        if (!fd_is_zero(asf) && asf > mu * afn) {
+            sf = sf * (mu * afn / asf);
+            spring = -(sf + c * sv) * (1.0 / k);
+        }
+    }
+    return spring;
+}
+
+__device__ __forceinline__ void linear_contact(double3& F, double3& spring, double3 vc, double3 n, double delta,
+                                               double dt, double kn, double ks, double mu, double res, double m)
+{
+    if (delta > 0.) {
+        const double lr = log(res);
+        const double diss = -lr / (double)sqrtf((float)(lr * lr + PI_D * PI_D));
+        const double cn = 2. * diss * (double)sqrtf((float)(m * kn));
+        const double3 vn = dot3(vc, n) * n;
+        const double3 fn = (kn * delta) * n - cn * vn;
+        const double cs = 2. * diss * (double)sqrtf((float)(m * ks));
+        const double3 vs = vc - vn;
+        spring = sliding_spring(spring, vs, n, fn, mu, ks, cs, dt);
+        const double3 fs = -ks * spring - cs * vs;
+        F = fn + fs;
+    } else {
+        spring = mk3(0., 0., 0.);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// narrow phase + force, one warp per candidate pair
+// ---------------------------------------------------------------------------
+struct NarrowArgs {
+    ObjDev P;
+    GeoSetDev G;
+    MatDev M;
+    ObjDev W;
+    GeoSetDev GW;
+    MatDev MW;
+    FdGrid pgrid;
+    FdGrid wgrid;
+    GhostDev gh;
+    PairListDev L;
+    StepArgs a;
+    int with_force;
+};
+
+// the slave side of a pair, by kind
+template <int KIND> struct Slave;
+template <> struct Slave<FD_PP> {
+    __device__ static double3 pos(const NarrowArgs& n, int j) { return n.P.pos[j]; }
+    __device__ static fd_quat q(const NarrowArgs& n, int j) { return n.P.q[j]; }
+    __device__ static const FdGeo& geo(const NarrowArgs& n, int j) { return n.G.geo[n.P.geo[j]]; }
+    __device__ static const GeoSetDev& set(const NarrowArgs& n) { return n.G; }
+    __device__ static long long hash(const NarrowArgs& n, int j) { return n.P.hash[j]; }
+    __device__ static const FdGrid& grid(const NarrowArgs& n) { return n.pgrid; }
+    static constexpr bool radius_test = true;
+};
+template <> struct Slave<FD_PW> {
+    __device__ static double3 pos(const NarrowArgs& n, int j) { return n.W.pos[j]; }
+    __device__ static fd_quat q(const NarrowArgs& n, int j) { return n.W.q[j]; }
+    __device__ static const FdGeo& geo(const NarrowArgs& n, int j) { return n.GW.geo[n.W.geo[j]]; }
+    __device__ static const GeoSetDev& set(const NarrowArgs& n) { return n.GW; }
+    __device__ static long long hash(const NarrowArgs& n, int j) { return n.W.hash[j]; }
+    __device__ static const FdGrid& grid(const NarrowArgs& n) { return n.wgrid; }
+    static constexpr bool radius_test = false;
+};
+struct SlaveGhost {
+    __device__ static double3 pos(const NarrowArgs& n, int j) { return n.gh.pos[j]; }
+    __device__ static fd_quat q(const NarrowArgs& n, int j) { return n.P.q[j]; }
+    __device__ static const FdGeo& geo(const NarrowArgs& n, int j) { return n.G.geo[n.P.geo[j]]; }
+    __device__ static const GeoSetDev& set(const NarrowArgs& n) { return n.G; }
+    __device__ static long long hash(const NarrowArgs& n, int j) { return n.gh.hash[j]; }
+    __device__ static const FdGrid& grid(const NarrowArgs& n) { return n.pgrid; }
+    static constexpr bool radius_test = false;
+};
+template <> struct Slave<FD_GX> : SlaveGhost {};
+template <> struct Slave<FD_GY> : SlaveGhost {};
+template <> struct Slave<FD_GXY> : SlaveGhost {};
+
+// Evaluate node predicate for one node.  Returns true when overlap >= 0 and
+// fills the grid fraction and the eight corner values.
+template <int KIND>
+__device__ __forceinline__ bool node_predicate(const double3 gp, const int3 bcell, const FdGrid& sg, const double3 cB,
+                                               const fd_quat qB, const FdGeo& GB, const double* sdf, double rB2,
+                                               double& overlap, double& fx, double& fy, double& fz, double p[8])
+{
+    int3 lo, hi;
+    fd_node_range(gp, sg, lo, hi);
+    if (bcell.x < lo.x || bcell.x > hi.x || bcell.y < lo.y || bcell.y > hi.y || bcell.z < lo.z || bcell.z > hi.z)
+        return false;
+    const double3 rel = mk3(gp.x - cB.x, gp.y - cB.y, gp.z - cB.z);
+    if (Slave<KIND>::radius_test) {
+        if (xm_len2(rel) > rB2) return false;
+    }
+    const double3 lp = xm_rrot(rel, qB);
+    const double gx = (lp.x - GB.origin.x) * GB.inv_spacing;
+    const double gy = (lp.y - GB.origin.y) * GB.inv_spacing;
+    const double gz = (lp.z - GB.origin.z) * GB.inv_spacing;
+    const int i0 = (int)floor(gx), j0 = (int)floor(gy), k0 = (int)floor(gz);
+    if (i0 < 0 || j0 < 0 || k0 < 0) return false;
+    if (i0 >= GB.size.x - 1 || j0 >= GB.size.y - 1 || k0 >= GB.size.z - 1) return false;
+    fx = gx - (double)i0;
+    fy = gy - (double)j0;
+    fz = gz - (double)k0;
+    const long long sx = GB.size.x, sxy = (long long)GB.size.x * GB.size.y;
+    const double* S = sdf + GB.sdf_off + (long long)k0 * sxy + (long long)j0 * sx + i0;
+    p[0] = __ldg(S);
+    p[1] = __ldg(S + 1);
+    p[2] = __ldg(S + sx);
+    p[3] = __ldg(S + sx + 1);
+    p[4] = __ldg(S + sxy);
+    p[5] = __ldg(S + sxy + 1);
+    p[6] = __ldg(S + sxy + sx);
+    p[7] = __ldg(S + sxy + sx + 1);
+    overlap = -xm_trilinear(fx, fy, fz, p);
+    return overlap >= 0.;
+}
+
+// cluster culling: true when no node of the cluster can be a contact
+template <int KIND>
+__device__ __forceinline__ bool cluster_culled(const FdCluster& cl, const fd_quat qA, const double3 cA,
+                                               const double3 cB, const fd_quat qB, const FdGeo& GB,
+                                               const GeoSetDev& SB, double rB)
+{
+    const double3 cw = fd_rot(qA, cl.centre) + cA;
+    const double3 rel = cw - cB;
+    const double rho = cl.radius * (1.0 + 1e-7) + 1e-12 * (GB.spacing + rB);
+    if (Slave<KIND>::radius_test) {
+        const double lim = rB + rho;
+        if (lengthSq3(rel) > lim * lim) return true;
+    }
+    const double3 lp = fd_rrot(rel, qB);
+    const double3 g = mk3((lp.x - GB.origin.x) * GB.inv_spacing, (lp.y - GB.origin.y) * GB.inv_spacing,
+                          (lp.z - GB.origin.z) * GB.inv_spacing);
+    const double rg = rho * GB.inv_spacing;
+    // sphere entirely outside the grid box: every node fails the bounds test
+    if (g.x < -rg || g.y < -rg || g.z < -rg) return true;
+    if (g.x > GB.size.x - 1 + rg || g.y > GB.size.y - 1 + rg || g.z > GB.size.z - 1 + rg) return true;
+    // distance bound: D(v) is a lower bound on the distance from grid node v
+    // to any cell where the trilinear SDF can be <= 0; D is 1-Lipschitz
+    const int vx = min(max((int)rint(g.x), 0), GB.size.x - 1);
+    const int vy = min(max((int)rint(g.y), 0), GB.size.y - 1);
+    const int vz = min(max((int)rint(g.z), 0), GB.size.z - 1);
+    const double D = (double)__ldg(SB.dist + GB.dist_off + fd_lin3(vx, vy, vz, GB.size));
+    const double3 dv = mk3((g.x - vx) * GB.spacing, (g.y - vy) * GB.spacing, (g.z - vz) * GB.spacing);
+    if (D - length3(dv) > rho) return true;
+    // Lipschitz bound of the trilinear SDF around the centre
+    if (g.x >= 0. && g.y >= 0. && g.z >= 0. && g.x < GB.size.x - 1 && g.y < GB.size.y - 1 && g.z < GB.size.z - 1) {
+        const int i0 = (int)floor(g.x), j0 = (int)floor(g.y), k0 = (int)floor(g.z);
+        const long long sx = GB.size.x, sxy = (long long)GB.size.x * GB.size.y;
+        const double* S = SB.sdf + GB.sdf_off + (long long)k0 * sxy + (long long)j0 * sx + i0;
+        double p[8] = {__ldg(S), __ldg(S + 1), __ldg(S + sx), __ldg(S + sx + 1),
+                       __ldg(S + sxy), __ldg(S + sxy + 1), __ldg(S + sxy + sx), __ldg(S + sxy + sx + 1)};
+        const double phi = xm_trilinear(g.x - i0, g.y - j0, g.z - k0, p);
+        const double bound = GB.lip * rho;
+        if (phi - bound > 1e-7 * (fabs(phi) + bound) + 1e-12 * GB.spacing) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(NARROW_WARPS * 32) k_narrow(NarrowArgs n)
+{
+    __shared__ unsigned int s_mask[NARROW_WARPS][MAX_CLUSTERS];
+    __shared__ unsigned char s_cl[NARROW_WARPS][MAX_CLUSTERS];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const unsigned int lt_mask = (1u << lane) - 1u;
+    PairListDev& L = n.L;
+    const int npairs = min(*L.n_pairs, L.cap_pairs);
+    const int nwarps = gridDim.x * NARROW_WARPS;
+    const bool periodic = (KIND == FD_PP || KIND == FD_PW) && (n.a.periodic_x || n.a.periodic_y);
+    for (int p = blockIdx.x * NARROW_WARPS + wib; p < npairs; p += nwarps) {
+        const int A = L.pairA[p];
+        const int B = L.pairB[p];
+        const int gA = n.P.geo[A];
+        const FdGeo& GA = n.G.geo[gA];
+        const double3 cA = n.P.pos[A];
+        const fd_quat qA = n.P.q[A];
+        const double3 cB = Slave<KIND>::pos(n, B);
+        const fd_quat qB = Slave<KIND>::q(n, B);
+        const FdGeo& GB = Slave<KIND>::geo(n, B);
+        const GeoSetDev& SB = Slave<KIND>::set(n);
+        const FdGrid& sg = Slave<KIND>::grid(n);
+        const double rB = GB.radius;
+        const double rB2 = rB * rB;
+        int3 bcell;
+        decode_cell(Slave<KIND>::hash(n, B), sg.size, bcell);
+        const int ncl = GA.clus_count;
+        if (ncl > MAX_CLUSTERS) set_flag(n.a.flags, FD_FLAG_CLUSTER_OVERFLOW);
+        // ---- cluster culling, one cluster per lane
+        unsigned long long keep = 0ull;
+        for (int c0 = 0; c0 < min(ncl, MAX_CLUSTERS); c0 += 32) {
+            const int c = c0 + lane;
+            bool k = false;
+            if (c < ncl) {
+                const FdCluster cl = n.G.clusters[GA.clus_off + c];
+                k = !cluster_culled<KIND>(cl, qA, cA, cB, qB, GB, SB, rB);
+            }
+            keep |= ((unsigned long long)__ballot_sync(0xffffffffu, k)) << c0;
+        }
+        // ---- phase 1: exact predicate over surviving clusters
+        int nk = 0, total = 0;
+        while (keep) {
+            const int c = __ffsll((long long)keep) - 1;
+            keep &= keep - 1ull;
+            const FdCluster cl = n.G.clusters[GA.clus_off + c];
+            bool hit = false;
+            if (lane < cl.count) {
+                const double3 node = n.G.nodes[GA.node_off + cl.start + lane];
+                const double3 r = xm_rot(qA, node);
+                const double3 gp = mk3(r.x + cA.x, r.y + cA.y, r.z + cA.z);
+                double ov, fx, fy, fz, pv[8];
+                hit = node_predicate<KIND>(gp, bcell, sg, cB, qB, GB, SB.sdf, rB2, ov, fx, fy, fz, pv);
+            }
+            const unsigned int m = __ballot_sync(0xffffffffu, hit);
+            if (m) {
+                if (lane == 0) {
+                    s_cl[wib][nk] = (unsigned char)c;
+                    s_mask[wib][nk] = m;
+                }
+                ++nk;
+                total += __popc(m);
+            }
+        }
+        __syncwarp();
+        if (total == 0) {
+            if (lane < 9) L.pf[(long long)p * 9 + lane] = 0.0;
+            if (lane == 0) { L.c_off[p] = 0; L.c_cnt[p] = 0; }
+            continue;
+        }
+        int base = 0;
+        if (lane == 0) base = atomicAdd(L.n_contacts, total);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        const bool store = (base + total <= L.cap_contacts);
+        if (!store) set_flag(n.a.flags, FD_FLAG_CONTACT_OVERFLOW);
+        // ---- history: the same pair in the previous step's list
+        int oc_off = 0, oc_cnt = 0;
+        {
+            const int os = L.o_seg_off[A], on = L.o_seg_cnt[A];
+            int found = -1;
+            for (int k0 = 0; k0 < on && found < 0; k0 += 32) {
+                const int k = k0 + lane;
+                const bool eq = (k < on) && (L.o_pairB[os + k] == B);
+                const unsigned int m = __ballot_sync(0xffffffffu, eq);
+                if (m) found = os + k0 + __ffs(m) - 1;
+            }
+            if (found >= 0) { oc_off = L.o_c_off[found]; oc_cnt = L.o_c_cnt[found]; }
+        }
+        // ---- phase 2: contact geometry, history, force, records
+        double3 accF = mk3(0., 0., 0.), accTA = mk3(0., 0., 0.), accTB = mk3(0., 0., 0.);
+        // force-side state (positions after the periodic wrap, LSSolver.h:1175-1190)
+        double3 ri = cA, rj = cB;
+        if (periodic) {
+            if (n.a.periodic_x) { ri = wrap_x(ri, n.pgrid); if (KIND == FD_PP) rj = wrap_x(rj, n.pgrid); }
+            if (n.a.periodic_y) { ri = wrap_y(ri, n.pgrid); if (KIND == FD_PP) rj = wrap_y(rj, n.pgrid); }
+        }
+        const double3 vi = n.P.vel[A], wi = n.P.angvel[A];
+        const int mi = n.P.mat[A];
+        const double invMi = GA.inv_mass;
+        const double kni = n.M.kn[mi], ksi = n.M.ks[mi], mui = n.M.mu[mi], ei = n.M.e[mi];
+        double3 vj, wj;
+        double kn = 0., ks = 0., effM = 0., mu, res;
+        if (KIND == FD_PW) {
+            vj = n.W.vel[B];
+            wj = n.W.angvel[B];
+            const int mj = n.W.mat[B];
+            mu = fmin(mui, n.MW.mu[mj]);
+            res = fmin(ei, n.MW.e[mj]);
+            if (invMi > 0.) effM = 1. / invMi;
+            kn = kni;
+            ks = ksi;
+        } else {
+            vj = n.P.vel[B];
+            wj = n.P.angvel[B];
+            const double invMj = GB.inv_mass;
+            const int mj = n.P.mat[B];
+            const double knj = n.M.kn[mj], ksj = n.M.ks[mj];
+            if (kni > 0. && knj > 0.) kn = kni * knj / (kni + knj);
+            if (ksi > 0. && ksj > 0.) ks = ksi * ksj / (ksi + ksj);
+            if (invMi > 0. || invMj > 0.) effM = 1. / (invMi + invMj);
+            res = fmin(ei, n.M.e[mj]);
+            mu = fmin(mui, n.M.mu[mj]);
+        }
+        const int node_base = n.P.node_base[A];
+        int written = 0;
+        for (int t = 0; t < nk; ++t) {
+            const int c = s_cl[wib][t];
+            const unsigned int m = s_mask[wib][t];
+            if (m & (1u << lane)) {
+                const FdCluster cl = n.G.clusters[GA.clus_off + c];
+                const int pool = GA.node_off + cl.start + lane;
+                const double3 node = n.G.nodes[pool];
+                const double3 r = xm_rot(qA, node);
+                const double3 gp = mk3(r.x + cA.x, r.y + cA.y, r.z + cA.z);
+                double ov = 0., fx = 0., fy = 0., fz = 0., pv[8];
+                node_predicate<KIND>(gp, bcell, sg, cB, qB, GB, SB.sdf, rB2, ov, fx, fy, fz, pv);
+                double3 nrm = fd_gradient_q(fx, fy, fz, pv);
+                nrm = fd_rot(qB, nrm);
+                nrm = fd_normalize(nrm);
+                const double3 pt = gp + (0.5 * ov) * nrm;
+                const int nid = node_base + n.G.node_lid[pool];
+                double3 spring = mk3(0., 0., 0.);
+                for (int j = 0; j < oc_cnt; ++j) {
+                    if (L.o_c_node[oc_off + j] == nid) {
+                        const double* sp = L.o_c_spring + 3ll * (oc_off + j);
+                        spring = mk3(sp[0], sp[1], sp[2]);
+                        break;
+                    }
+                }
+                double3 F = mk3(0., 0., 0.);
+                if (n.with_force) {
+                    const double3 vc = (vi + cross3(wi, pt - ri)) - (vj + cross3(wj, pt - rj));
+                    linear_contact(F, spring, vc, nrm, ov, n.a.dt, kn, ks, mu, res, effM);
+                    accF += F;
+                    accTA += cross3(pt - ri, F);
+                    accTB += cross3(pt - rj, -F);
+                }
+                if (store) {
+                    const long long slot = base + written + __popc(m & lt_mask);
+                    L.c_node[slot] = nid;
+                    L.c_slave[slot] = B;
+                    L.c_spring[3 * slot + 0] = spring.x;
+                    L.c_spring[3 * slot + 1] = spring.y;
+                    L.c_spring[3 * slot + 2] = spring.z;
+                    if (n.a.records) {
+                        L.c_point[3 * slot + 0] = pt.x;
+                        L.c_point[3 * slot + 1] = pt.y;
+                        L.c_point[3 * slot + 2] = pt.z;
+                        L.c_normal[3 * slot + 0] = nrm.x;
+                        L.c_normal[3 * slot + 1] = nrm.y;
+                        L.c_normal[3 * slot + 2] = nrm.z;
+                        L.c_overlap[slot] = ov;
+                        L.c_en[slot] = 0.5 * ov * ov * kn;
+                        L.c_es[slot] = 0.5 * lengthSq3(spring) * ks;
+                    }
+                }
+            }
+            written += __popc(m);
+        }
+        const double red[9] = {warp_sum(accF.x), warp_sum(accF.y), warp_sum(accF.z),
+                               warp_sum(accTA.x), warp_sum(accTA.y), warp_sum(accTA.z),
+                               warp_sum(accTB.x), warp_sum(accTB.y), warp_sum(accTB.z)};
+        if (lane < 9) L.pf[(long long)p * 9 + lane] = red[lane];
+        if (lane == 0) {
+            L.c_off[p] = store ? base : 0;
+            L.c_cnt[p] = store ? total : 0;
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// reverse index: pairs grouped by partner B, sorted by A
+// ---------------------------------------------------------------------------
+__global__ void k_rev_count(PairListDev L, int n_obj)
+{
+    const int npairs = min(*L.n_pairs, L.cap_pairs);
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npairs; p += gridDim.x * blockDim.x) {
+        const int B = L.pairB[p];
+        if (B >= 0 && B < n_obj) atomicAdd(&L.rev_cnt[B], 1);
+    }
+}
+__global__ void k_rev_fill(PairListDev L, int n_obj)
+{
+    const int npairs = min(*L.n_pairs, L.cap_pairs);
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npairs; p += gridDim.x * blockDim.x) {
+        const int B = L.pairB[p];
+        if (B >= 0 && B < n_obj) {
+            const int slot = L.rev_off[B] + atomicAdd(&L.rev_fill[B], 1);
+            L.rev_pair[slot] = p;
+        }
+    }
+}
+__global__ void k_rev_sort(PairListDev L, int n_obj)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_obj) return;
+    int* seg = L.rev_pair + L.rev_off[i];
+    const int cnt = L.rev_cnt[i];
+    for (int a = 1; a < cnt; ++a) {
+        const int v = seg[a];
+        const int key = L.pairA[v];
+        int b = a - 1;
+        while (b >= 0 && L.pairA[seg[b]] > key) { seg[b + 1] = seg[b]; --b; }
+        seg[b + 1] = v;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// bonds, contactKernel.cuh:138-199 and contactKernel.cu:293-371
+// ---------------------------------------------------------------------------
+__global__ void k_bonds(ObjDev P, BondDev Bd)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= Bd.n) return;
+    double* E = Bd.energy + 6ll * k;
+    double* O = Bd.out + 9ll * k;
+    for (int t = 0; t < 9; ++t) O[t] = 0.;
+    if (Bd.active[k] == 0) {
+        for (int t = 0; t < 6; ++t) E[t] = 0.;
+        return;
+    }
+    const int i = Bd.master[k], j = Bd.slave[k];
+    const fd_quat qi = P.q[i], qj = P.q[j];
+    const double3* f = Bd.frames + 8ll * k;
+    const double3 n1i = fd_rot(qi, f[0]), n2i = fd_rot(qi, f[1]), n3i = fd_rot(qi, f[2]);
+    const double3 n1j = fd_rot(qj, f[4]), n2j = fd_rot(qj, f[5]), n3j = fd_rot(qj, f[6]);
+    const double3 ri = P.pos[i], rj = P.pos[j];
+    const double3 rbi = fd_rot(qi, f[3]) + ri;
+    const double3 rbj = fd_rot(qj, f[7]) + rj;
+    Bd.point[k] = 0.5 * (rbi + rbj);
+    double3 F = mk3(0., 0., 0.), Mij = mk3(0., 0., 0.), Mji = mk3(0., 0., 0.);
+    int act = 1;
+    const double3 rij = rbi - rbj;
+    const double D = length3(rij);
+    if (!fd_is_zero(D)) {
+        const double B1 = Bd.B[4 * k], B2 = Bd.B[4 * k + 1], B3 = Bd.B[4 * k + 2], B4 = Bd.B[4 * k + 3];
+        const double R = Bd.radius[k], D0 = Bd.L0[k];
+        const double3 nij = fd_normalize(rij);
+        const double3 e = -nij;
+        E[0] = 0.5 * B1 * (D - D0) * (D - D0);
+        E[1] = B2 * (0.5 * dot3(n1j - n1i, e) - 0.25 * dot3(n1i, n1j) + 0.75);
+        E[2] = (0.25 * B2 + B3 + 0.5 * B4) * (dot3(n1i, n1j) + 1.);
+        E[3] = -0.5 * B4 * (dot3(n1i, n1j) + dot3(n2i, n2j) + dot3(n3i, n3j) - 1);
+        const double3 dn = n1j - n1i;
+        F = B1 * (D - D0) * e + B2 / (2 * D) * (dn - dot3(dn, e) * e);
+        const double3 MTB = B3 * cross3(n1j, n1i) - 0.5 * B4 * (cross3(n2j, n2i) + cross3(n3j, n3i));
+        Mij = -0.5 * B2 * cross3(e, n1i) + MTB;
+        Mji = 0.5 * B2 * cross3(e, n1j) - MTB;
+        const double bnf = dot3(F, nij);
+        const double3 bsf = F - bnf * nij;
+        const double btt = dot3(MTB, nij);
+        const double3 bbt = MTB - btt * nij;
+        const double Ab = R * R * PI_D;
+        const double Ib = Ab * R * R / 4.;
+        const double Jb = 2 * Ib;
+        E[4] = -bnf / Ab + length3(bbt) / Ib * R;
+        E[5] = length3(bsf) / Ab + fabs(btt) / Jb * R;
+        if (Bd.ts[k] > 0. && E[4] > Bd.ts[k]) act = 0;
+        else if (Bd.coh[k] > 0. && E[5] > Bd.coh[k] - Bd.mu[k] * E[4]) act = 0;
+    }
+    Bd.active[k] = act;
+    const double3 Ti = Mij + cross3(rbi - ri, F);
+    const double3 Tj = Mji + cross3(rbj - rj, -F);
+    O[0] = F.x; O[1] = F.y; O[2] = F.z;
+    O[3] = Ti.x; O[4] = Ti.y; O[5] = Ti.z;
+    O[6] = Tj.x; O[7] = Tj.y; O[8] = Tj.z;
+}
+
+// ---------------------------------------------------------------------------
+// per-particle reduction, fixed order
+// ---------------------------------------------------------------------------
+struct ReduceArgs {
+    ObjDev P;
+    PairListDev L[FD_NKIND];
+    int active[FD_NKIND];
+    BondDev B;
+};
+
+__device__ __forceinline__ double3 ld3(const double* p) { return mk3(p[0], p[1], p[2]); }
+
+__global__ void k_reduce(ReduceArgs r)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= r.P.n) return;
+    double3 F = mk3(0., 0., 0.), T = mk3(0., 0., 0.);
+    for (int kind = 0; kind < FD_NKIND; ++kind) {
+        if (!r.active[kind]) continue;
+        const PairListDev& L = r.L[kind];
+        const int s = L.seg_off[i], c = L.seg_cnt[i];
+        for (int k = s; k < s + c; ++k) {
+            const double* pf = L.pf + 9ll * k;
+            F += ld3(pf);
+            T += ld3(pf + 3);
+        }
+        if (kind == FD_PW) continue;
+        const int rs = L.rev_off[i], rc = L.rev_cnt[i];
+        for (int e = rs; e < rs + rc; ++e) {
+            const int k = L.rev_pair[e];
+            if (kind != FD_PP && L.pairA[k] == i) continue;  // a particle against its own ghost
+            const double* pf = L.pf + 9ll * k;
+            F += -ld3(pf);
+            T += ld3(pf + 6);
+        }
+    }
+    if (r.B.n > 0) {
+        for (int e = r.B.plist_off[i]; e < r.B.plist_off[i + 1]; ++e) {
+            const int code = r.B.plist[e];
+            const int b = code >> 1, side = code & 1;
+            const double* o = r.B.out + 9ll * b;
+            if (side == 0) { F += ld3(o); T += ld3(o + 3); }
+            else { F += -ld3(o); T += ld3(o + 6); }
+        }
+    }
+    r.P.force[i] = F;
+    r.P.torque[i] = T;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+size_t scan_tmp_size(long long n)
+{
+    size_t total = 0;
+    long long m = n;
+    while (m > SCAN_TILE) {
+        m = (m + SCAN_TILE - 1) / SCAN_TILE;
+        total += (size_t)m;
+    }
+    return total + 1;
+}
+
+void scan_exclusive(const int* in, int* out, long long n, int* tmp, cudaStream_t s)
+{
+    if (n <= 0) return;
+    if (n <= SCAN_TILE) {
+        k_scan_tile<<<1, SCAN_TPB, 0, s>>>(in, out, n, nullptr);
+        return;
+    }
+    const long long tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+    int* sums = tmp;
+    k_scan_tile<<<(unsigned)tiles, SCAN_TPB, 0, s>>>(in, out, n, sums);
+    scan_exclusive(sums, sums, tiles, tmp + tiles, s);
+    k_scan_add<<<(unsigned)tiles, SCAN_TPB, 0, s>>>(out, n, sums);
+}
+
+void launch_kick(const ObjDev& P, const GeoSetDev& G, double3 gravity, double h, cudaStream_t s)
+{
+    if (P.n > 0) k_kick<<<nblocks(P.n), TPB, 0, s>>>(P, G, gravity, h);
+}
+void launch_drift(const ObjDev& O, double dt, cudaStream_t s)
+{
+    if (O.n > 0) k_drift<<<nblocks(O.n), TPB, 0, s>>>(O, dt);
+}
+void launch_hash_count(const ObjDev& O, CellTableDev& T, cudaStream_t s)
+{
+    cudaMemsetAsync(T.count, 0, sizeof(int) * T.g.num, s);
+    if (O.n > 0) k_hash_count<<<nblocks(O.n), TPB, 0, s>>>(O, T.g, T.count);
+}
+void launch_cell_table(ObjDev& O, CellTableDev& T, int* scan_tmp, size_t, cudaStream_t s)
+{
+    scan_exclusive(T.count, T.start, T.g.num, scan_tmp, s);
+    cudaMemsetAsync(T.fill, 0, sizeof(int) * T.g.num, s);
+    if (O.n > 0) k_scatter<<<nblocks(O.n), TPB, 0, s>>>(O.hash, O.n, T.g.num, T.start, T.fill, T.sorted);
+}
+void launch_wrap(ObjDev& P, const FdGrid& g, int dim, cudaStream_t s)
+{
+    if (P.n > 0) k_wrap<<<nblocks(P.n), TPB, 0, s>>>(P, g, dim);
+}
+void launch_ghost_build(const ObjDev& P, GhostDev& Gh, int kind, cudaStream_t s)
+{
+    cudaMemsetAsync(Gh.cells.count, 0, sizeof(int) * Gh.cells.g.num, s);
+    if (P.n > 0) k_ghost_build<<<nblocks(P.n), TPB, 0, s>>>(P, Gh, kind);
+}
+void launch_broad_pp(const ObjDev& P, const GeoSetDev& G, const CellTableDev& T, PairListDev& L,
+                     unsigned int* flags, cudaStream_t s)
+{
+    cudaMemsetAsync(L.n_pairs, 0, sizeof(int), s);
+    if (P.n > 0) k_broad_pp<<<nblocks(P.n), TPB, 0, s>>>(P, G, T, L, flags);
+}
+void launch_broad_pw(const ObjDev& P, const GeoSetDev& G, const ObjDev& W, const GeoSetDev& GW,
+                     const FdGrid& wg, PairListDev& L, unsigned int* flags, cudaStream_t s)
+{
+    cudaMemsetAsync(L.n_pairs, 0, sizeof(int), s);
+    if (P.n > 0) k_broad_pw<<<nblocks(P.n), TPB, 0, s>>>(P, G, W, GW, wg, L, flags);
+}
+void launch_broad_ghost(const ObjDev& P, const GeoSetDev& G, const GhostDev& Gh, PairListDev& L,
+                        unsigned int* flags, cudaStream_t s)
+{
+    cudaMemsetAsync(L.n_pairs, 0, sizeof(int), s);
+    if (P.n > 0) k_broad_ghost<<<nblocks(P.n), TPB, 0, s>>>(P, G, Gh, L, flags);
+}
+
+void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& M, const ObjDev& W,
+                   const GeoSetDev& GW, const MatDev& MW, const FdGrid& pgrid, const FdGrid& wgrid,
+                   const GhostDev* gh, PairListDev& L, const StepArgs& a, int with_force, cudaStream_t s)
+{
+    cudaMemsetAsync(L.n_contacts, 0, sizeof(int), s);
+    NarrowArgs n;
+    n.P = P; n.G = G; n.M = M; n.W = W; n.GW = GW; n.MW = MW; n.pgrid = pgrid; n.wgrid = wgrid;
+    if (gh) n.gh = *gh; else memset(&n.gh, 0, sizeof(n.gh));
+    n.L = L; n.a = a; n.with_force = with_force;
+    const long long need = ((long long)L.cap_pairs + NARROW_WARPS - 1) / NARROW_WARPS;
+    const int grid = (int)(need < 148 * 24 ? (need > 0 ? need : 1) : 148 * 24);
+    switch (kind) {
+    case FD_PP: k_narrow<FD_PP><<<grid, NARROW_WARPS * 32, 0, s>>>(n); break;
+    case FD_PW: k_narrow<FD_PW><<<grid, NARROW_WARPS * 32, 0, s>>>(n); break;
+    case FD_GX: k_narrow<FD_GX><<<grid, NARROW_WARPS * 32, 0, s>>>(n); break;
+    case FD_GY: k_narrow<FD_GY><<<grid, NARROW_WARPS * 32, 0, s>>>(n); break;
+    case FD_GXY: k_narrow<FD_GXY><<<grid, NARROW_WARPS * 32, 0, s>>>(n); break;
+    }
+}
+
+void launch_reverse(const ObjDev& P, PairListDev& L, int* scan_tmp, size_t, cudaStream_t s)
+{
+    if (P.n <= 0) return;
+    cudaMemsetAsync(L.rev_cnt, 0, sizeof(int) * P.n, s);
+    cudaMemsetAsync(L.rev_fill, 0, sizeof(int) * P.n, s);
+    const int g = 148 * 8;
+    k_rev_count<<<g, TPB, 0, s>>>(L, P.n);
+    scan_exclusive(L.rev_cnt, L.rev_off, P.n, scan_tmp, s);
+    k_rev_fill<<<g, TPB, 0, s>>>(L, P.n);
+    k_rev_sort<<<nblocks(P.n), TPB, 0, s>>>(L, P.n);
+}
+
+void launch_bonds(const ObjDev& P, BondDev& B, cudaStream_t s)
+{
+    if (B.n > 0) k_bonds<<<nblocks(B.n), TPB, 0, s>>>(P, B);
+}
+
+void launch_reduce(ObjDev& P, PairListDev* lists, const int* active, const BondDev& B, cudaStream_t s)
+{
+    if (P.n <= 0) return;
+    ReduceArgs r;
+    r.P = P;
+    for (int k = 0; k < FD_NKIND; ++k) { r.L[k] = lists[k]; r.active[k] = active[k]; }
+    r.B = B;
+    k_reduce<<<nblocks(P.n), TPB, 0, s>>>(r);
+}
+
+}  // namespace fd

@@ -1,0 +1,148 @@
+// fd_kernels.cuh -- launch interface of the timestep kernels (fd_kernels.cu).
+#pragma once
+#include "fd_internal.cuh"
+
+namespace fd {
+
+// Everything one simulation keeps on the device.  Plain pointers; ownership
+// and sizes live in the host-side Sim object (fd_api.cu).
+struct PairListDev {
+    // pairs of the current step (A-major segments, partners ascending)
+    int* pairA;
+    int* pairB;
+    int* seg_off;      // per particle A: first pair
+    int* seg_cnt;      // per particle A: number of pairs
+    int* c_off;        // per pair: first contact
+    int* c_cnt;        // per pair: number of contacts
+    double* pf;        // per pair: F (3), torque on A (3), torque on B (3)
+    int* n_pairs;      // device counter
+    int cap_pairs;
+    // previous step (history source)
+    int* o_pairB;
+    int* o_seg_off;
+    int* o_seg_cnt;
+    int* o_c_off;
+    int* o_c_cnt;
+    // contacts of the current step
+    int* c_node;
+    int* c_slave;
+    double* c_spring;  // 3 per contact
+    double* c_point;   // 3 per contact (records)
+    double* c_normal;  // 3 per contact (records)
+    double* c_overlap; // records
+    double* c_en;      // records
+    double* c_es;      // records
+    int* n_contacts;   // device counter
+    int cap_contacts;
+    // previous contacts
+    int* o_c_node;
+    double* o_c_spring;
+    // reverse index (pairs grouped by partner B)
+    int* rev_cnt;
+    int* rev_off;
+    int* rev_fill;
+    int* rev_pair;
+};
+
+struct ObjDev {
+    int n;
+    double3* pos;
+    double3* vel;
+    double3* angvel;
+    double3* force;
+    double3* torque;
+    fd_quat* q;
+    int* mat;
+    int* geo;
+    long long* hash;   // cell hash of the current step (-1 when not hashed)
+    int* node_base;    // first global boundary node of each object
+};
+
+struct GeoSetDev {
+    int n;
+    const FdGeo* geo;
+    const double* sdf;
+    const float* sdf32;
+    const float* dist;
+    const double3* nodes;     // cluster order
+    const int* node_lid;      // original local index of each node (cluster order)
+    const FdCluster* clusters;
+    double rmax;              // largest bounding radius over the set
+    double grid_rmax;         // largest grid radius over the set
+};
+
+struct MatDev {
+    const double* kn;
+    const double* ks;
+    const double* mu;
+    const double* e;
+};
+
+struct CellTableDev {
+    FdGrid g;
+    int* count;
+    int* start;
+    int* fill;
+    int* sorted;   // object index per slot
+};
+
+struct GhostDev {
+    double3* pos;
+    long long* hash;
+    CellTableDev cells;
+};
+
+struct BondDev {
+    int n;
+    const int* master;
+    const int* slave;
+    int* active;
+    double3* point;
+    const double* B;      // 4 per bond
+    const double* radius;
+    const double* L0;
+    const double* ts;
+    const double* coh;
+    const double* mu;
+    const double3* frames; // 8 per bond: mn1 mn2 mn3 mp sn1 sn2 sn3 sp
+    double* energy;        // 6 per bond: Un Us Ub Ut sn ss
+    double* out;           // 9 per bond: F, Ti, Tj
+    const int* plist_off;  // per particle (n+1): bonds touching it
+    const int* plist;      // bond id * 2 + side
+};
+
+struct StepArgs {
+    double dt;
+    double3 gravity;
+    int periodic_x, periodic_y;
+    int records;
+    unsigned int* flags;
+};
+
+// integration and hashing
+void launch_kick(const ObjDev& P, const GeoSetDev& G, double3 gravity, double h, cudaStream_t s);
+void launch_drift(const ObjDev& O, double dt, cudaStream_t s);
+void launch_hash_count(const ObjDev& O, CellTableDev& T, cudaStream_t s);
+void launch_cell_table(ObjDev& O, CellTableDev& T, int* scan_tmp, size_t scan_tmp_ints, cudaStream_t s);
+void launch_wrap(ObjDev& P, const FdGrid& g, int dim, cudaStream_t s);
+void launch_ghost_build(const ObjDev& P, GhostDev& Gh, int kind, cudaStream_t s);
+
+// pair lists
+void launch_broad_pp(const ObjDev& P, const GeoSetDev& G, const CellTableDev& T, PairListDev& L,
+                     unsigned int* flags, cudaStream_t s);
+void launch_broad_pw(const ObjDev& P, const GeoSetDev& G, const ObjDev& W, const GeoSetDev& GW,
+                     const FdGrid& wg, PairListDev& L, unsigned int* flags, cudaStream_t s);
+void launch_broad_ghost(const ObjDev& P, const GeoSetDev& G, const GhostDev& Gh, PairListDev& L,
+                        unsigned int* flags, cudaStream_t s);
+void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& M, const ObjDev& W,
+                   const GeoSetDev& GW, const MatDev& MW, const FdGrid& pgrid, const FdGrid& wgrid,
+                   const GhostDev* gh, PairListDev& L, const StepArgs& a, int with_force, cudaStream_t s);
+void launch_reverse(const ObjDev& P, PairListDev& L, int* scan_tmp, size_t scan_tmp_ints, cudaStream_t s);
+void launch_bonds(const ObjDev& P, BondDev& B, cudaStream_t s);
+void launch_reduce(ObjDev& P, PairListDev* lists, const int* active, const BondDev& B, cudaStream_t s);
+
+// exclusive scan of n ints (out may alias in); returns needed tmp ints when tmp == nullptr
+size_t scan_tmp_size(long long n);
+void scan_exclusive(const int* in, int* out, long long n, int* tmp, cudaStream_t s);
+
+}  // namespace fd

@@ -1,0 +1,145 @@
+/*
+ * fundem_b200.h -- C ABI of the B200 level-set DEM timestep (libfundem_b200.so).
+ *
+ * Plain C: opaque handle, caller-owned host arrays (or device pointers where
+ * stated), status codes, no exceptions across the boundary.  All device work
+ * is stream-ordered on the simulation's stream.  Arrays of 3-vectors are
+ * packed xyz doubles; quaternions are scalar-first (q0, q1, q2, q3).
+ *
+ * Each entry point names the reference interface it replaces (paths relative
+ * to the reference project).  The reference's own boundary is a set of
+ * extern "C" kernel launchers driven by header-only C++ classes; here the
+ * launch sequence of one step is owned by the library, and the
+ * header-compatible C++ classes (fundem_b200/kernel/*.h) sit on top of these
+ * functions.
+ */
+#ifndef FUNDEM_B200_H
+#define FUNDEM_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct fundem_sim fundem_sim;
+
+typedef enum {
+    FUNDEM_OK = 0,
+    FUNDEM_ERR_ARG = 1,       /* invalid argument (the reference prints to stderr and skips) */
+    FUNDEM_ERR_CUDA = 2,      /* a CUDA call failed */
+    FUNDEM_ERR_CAPACITY = 3,  /* a pair/contact/candidate list overflowed during a step */
+    FUNDEM_ERR_STATE = 4,     /* call out of order (e.g. step before setup) */
+    FUNDEM_ERR_NUMERIC = 5    /* non-finite particle state detected */
+} fundem_status;
+
+enum { FUNDEM_FP64 = 0, FUNDEM_FP32_MIXED = 1 };
+/* contact list kinds */
+enum { FUNDEM_PP = 0, FUNDEM_PW = 1, FUNDEM_GX = 2, FUNDEM_GY = 3, FUNDEM_GXY = 4 };
+
+const char* fundem_version(void);
+const char* fundem_status_string(int status);
+
+/* LSSolver(dir, stream, maxGPUThread, device), kernel/LSSolver.h:14-21, and
+   activateGPUDevice, LSSolver.h:601-613 (which calls exit(1) on failure;
+   this returns FUNDEM_ERR_CUDA).  stream may be NULL (the legacy stream). */
+int fundem_create(fundem_sim** out, int device, void* stream);
+int fundem_destroy(fundem_sim* sim);
+/* precision of the contact path (FUNDEM_FP64 reproduces the reference) */
+int fundem_set_precision(fundem_sim* sim, int mode);
+/* when nonzero every step writes full contact records (point, normal,
+   overlap, energies); otherwise only node, partner and sliding spring */
+int fundem_set_records(fundem_sim* sim, int full_records);
+
+/* LSSolver::addParticleMaterial / addWallMaterial, LSSolver.h:33-42, 175-183
+   (clamps of LSParticle::addMaterial, LSParticle.h:221-231) */
+int fundem_add_material(fundem_sim* sim, int wall, double kn, double ks, double mu, double e, int* id_out);
+/* LSSolver::addParticleGeometry / addWallGeometry, LSSolver.h:58-76, 196-213
+   (LSParticle::addGeometry, LSParticle.h:233-267).  sdf is x-fastest,
+   size[0]*size[1]*size[2] values; nodes are n_nodes xyz triples. */
+int fundem_add_geometry(fundem_sim* sim, int wall, double mass, const double inertia[6], const double origin[3],
+                        double spacing, const int size[3], const double* sdf, int n_nodes, const double* nodes,
+                        int* id_out);
+/* mass, centroid and inertia from a density (LSSolver.h:470-586; host) */
+int fundem_mass_properties(double density, const double origin[3], double spacing, const int size[3],
+                           const double* sdf, double* mass, double centroid[3], double inertia[6]);
+/* LSSolver::addParticle / addWall, LSSolver.h:88-104, 225-238 (host arrays) */
+int fundem_add_objects(fundem_sim* sim, int wall, int n, const double* pos, const double* vel, const double* angvel,
+                       const double* quat, const int* mat, const int* geo);
+/* setFixedVelocityToWall / setFixedAngularVelocityToWall, LSSolver.h:266-282;
+   moveLSParticle / moveWall, LSSolver.h:244-258 */
+int fundem_set_wall_motion(fundem_sim* sim, int index, const double vel[3], const double angvel[3]);
+int fundem_move(fundem_sim* sim, int wall, int index, const double offset[3]);
+/* addBondedInteraction, LSSolver.h:296-317 (VBondedInteraction::add,
+   VBondedInteraction.h:74-195); uses the current host-side state */
+int fundem_add_bonds(fundem_sim* sim, int n, const int* master, const int* slave, const double* point,
+                     const double* normal, const double* radius, const double* length, const double* young,
+                     const double* poisson, const double* tensile, const double* cohesion, const double* friction);
+/* addPeriodicBoundaryXD / YD / removePeriodicBoundary, LSSolver.h:384-414 */
+int fundem_set_periodic(fundem_sim* sim, int x, int y);
+
+/* LSSolver::upload, LSSolver.h:692-703: domain and grids, template tables,
+   device state.  May be called again (multi-phase runs): state already on
+   the device is kept, contact history is kept when the node count is
+   unchanged (SolidInteraction.h:23-49). */
+int fundem_setup(fundem_sim* sim, const double domain_min[3], const double domain_max[3]);
+/* the pre-loop detection (LSSolver.h:1093-1094 and the periodic variants) */
+int fundem_detect(fundem_sim* sim);
+/* nsteps iterations of the loop body of LSSolver::compute* (LSSolver.h:1097-1107):
+   kick, drift, detection, forces, bonds, kick.  No host synchronisation. */
+int fundem_step(fundem_sim* sim, int nsteps, const double gravity[3], double dt);
+/* one step split at the addExternalForceTorque hook (LSSolver.h:588): after
+   step_begin the force/torque arrays hold the step's contact and bond sums;
+   the caller may add to them (stream-ordered) before step_end. */
+int fundem_step_begin(fundem_sim* sim, const double gravity[3], double dt);
+int fundem_step_end(fundem_sim* sim, const double gravity[3], double dt);
+/* wait for the stream; returns the accumulated device error status */
+int fundem_sync(fundem_sim* sim);
+/* record one status word per step into a host ring without stalling */
+int fundem_status_word(fundem_sim* sim, unsigned int* flags);
+
+/* state transfer (host arrays; any pointer may be NULL) */
+int fundem_num_objects(fundem_sim* sim, int wall, int* n);
+int fundem_get_objects(fundem_sim* sim, int wall, double* pos, double* vel, double* angvel, double* quat,
+                       double* force, double* torque);
+int fundem_set_objects(fundem_sim* sim, int wall, const double* pos, const double* vel, const double* angvel,
+                       const double* quat, const double* force, const double* torque);
+/* raw device pointers of the state (LSParticle::position() ... , LSParticle.h:768-777) */
+typedef struct {
+    double* pos;
+    double* vel;
+    double* angvel;
+    double* force;
+    double* torque;
+    double* quat;
+    int* mat;
+    int* geo;
+    int n;
+} fundem_device_view;
+int fundem_device_view_get(fundem_sim* sim, int wall, fundem_device_view* out);
+
+/* contact lists in canonical (node, partner) order; records are valid only
+   for steps run with full records (the pre-loop detection always writes them) */
+int fundem_num_contacts(fundem_sim* sim, int kind, long long* n);
+int fundem_get_contacts(fundem_sim* sim, int kind, int* node, int* partner, double* point, double* normal,
+                        double* overlap, double* spring, double* en, double* es);
+/* replace the history (previous step's list) of one kind */
+int fundem_set_contacts(fundem_sim* sim, int kind, long long n, const int* node, const int* partner,
+                        const double* spring);
+/* candidate pairs of the last detection */
+int fundem_num_pairs(fundem_sim* sim, int kind, long long* n);
+
+/* bond state (VBondedInteraction getters, VBondedInteraction.h:448-494) */
+int fundem_num_bonds(fundem_sim* sim, int* n);
+int fundem_get_bonds(fundem_sim* sim, int* activated, double* point, double* energy6);
+int fundem_set_bond_activation(fundem_sim* sim, const int* activated);
+
+/* derived template data (geometryInfo, LSParticle.h:53-173) */
+int fundem_get_geometry(fundem_sim* sim, int wall, int geo, double* radius, double* inv_mass, double inertia[6],
+                        double inv_inertia[6]);
+int fundem_get_grid(fundem_sim* sim, int wall, double minb[3], double maxb[3], double inv_cell[3], int size[3]);
+/* kernel launches issued by this simulation so far */
+int fundem_launch_count(fundem_sim* sim, long long* n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
