@@ -1,0 +1,308 @@
+#!/usr/bin/env python
+"""Throughput of the level-set DEM timestep on B200: particle-steps/s.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl fundem|reference]
+
+Workload (default): the scaled, periodic, bonded column -- 262,144
+superellipsoids from 8 templates (32^3 SDFs, 642 surface nodes), periodic in
+x and y, floor wall and a top platen moving at 1 m/s, V-model bonds between
+pairs whose surface gap is below 0.05 of the mean diameter, dt = 5e-7 s,
+FP64.  A step is one pass of the whole timestep (kicks, drift, hashing,
+broad phase, narrow phase + contact law, ghosts, bonds, reduction) over the
+resident state.  Inputs are larger than L2 (state + templates + lists are
+several hundred MB), so no L2 flush is needed between steps.
+
+--impl reference times the CPU restatement of the reference algorithm (the
+reference itself has no CPU code) on a bounded sample of the same workload,
+with all host threads.
+
+Under torchrun each rank runs an independent replica (the path does not
+shard: a single simulation lives on one GPU); value = all ranks' particle
+steps / the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s"
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+# algorithmic bytes per unit (FP64): per particle-step and per node-contact-step
+BYTES_PARTICLE_STEP = 216
+BYTES_CONTACT_STEP = 64
+BYTES_BOND_STEP = 340
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm = [float(s[1]) for s in self.samples if len(s) >= 9 and s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if len(s) >= 9 and s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            if len(s) < 9:
+                continue
+            for k, nm in enumerate(names):
+                if "Active" in s[5 + k] and "Not" not in s[5 + k]:
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def peaks():
+    try:
+        with open(PEAKS) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle (a restatement of the reference algorithm) on a
+# bounded sample of the same workload, all host threads
+# ---------------------------------------------------------------------------
+def cpu_sample_scenario(n=2048):
+    from fundem_b200 import scenario as S
+    rng = np.random.default_rng(7)
+    geos = S.superellipsoid_templates(rng, 8, n=32, level=3, density=2500.0, explicit_mass=True)
+    rb = max(S.node_radius(g) for g in geos)
+    sc = S.bonded_periodic(n=n, n_templates=8, seed=7, pitch=2.0 * rb * 1.01, resolve=False, dt=5e-7)
+    return sc
+
+
+def cpu_baseline(seconds=15.0, n=2048):
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    sc = cpu_sample_scenario(n)
+    w = O.OracleWorld.from_scenario(sc)
+    w.initial_detect()
+    w.step(1)
+    steps, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        w.step(1)
+        steps += 1
+    dt = time.perf_counter() - t0
+    return {"value": n * steps / dt, "unit": METRIC, "cores": threads, "kind": "port",
+            "sample": f"{n} particles of the bonded periodic column (8 templates, 32^3 SDF, 642 nodes, "
+                      f"{len(sc.bonds)} bonds), {steps} steps in {dt:.1f} s"}
+
+
+# ---------------------------------------------------------------------------
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    res = cpu_baseline(seconds=max(5.0, 3.0 * args.steps / 10.0), n=args.cpu_sample)
+    line = {"metric": METRIC, "value": res["value"], "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": "bonded periodic column, bounded CPU sample", "sample_particles": args.cpu_sample},
+            "cpu_baseline": res,
+            "e2e": {"value": res["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_fundem(args, rank, world, dist):
+    import torch
+    import fundem_b200 as F
+    from fundem_b200 import build, workloads
+
+    build.build()
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    t_build = time.perf_counter()
+    sim, sc, info = workloads.bonded_column(n=args.n, footprint=tuple(args.footprint), seed=1 + rank, device=dev,
+                                            log=log if rank == 0 else None)
+    t_build = time.perf_counter() - t_build
+    n = info["n"]
+    g = np.asarray(sc.gravity, float)
+    dt = sc.dt
+    sim.step(args.warmup)
+    sim.sync()
+    pairs = sim.num_pairs(0)
+    contacts = sim.num_contacts(0) + sim.num_contacts(1) + sum(sim.num_contacts(k) for k in (2, 3, 4))
+    nbonds = int(sim.bonds()["activated"].sum())
+    sim.set_profiling(True)
+    sim.kernel_times()
+    sim.work_counters()
+    l0 = sim.launch_count()
+    clocks = ClockSampler(dev)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if args.profile:
+        torch.cuda.profiler.start()
+    e0.record()
+    sim.step(args.steps)
+    e1.record()
+    torch.cuda.synchronize()
+    if args.profile:
+        torch.cuda.profiler.stop()
+    sim.sync()
+    if dist:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    launches = sim.launch_count() - l0
+    kt = sim.kernel_times()
+    wc = sim.work_counters()
+    sim.set_profiling(False)
+    contacts_end = sim.num_contacts(0) + sim.num_contacts(1) + sum(sim.num_contacts(k) for k in (2, 3, 4))
+    t_max = ms
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    value = world * n * args.steps / (t_max / 1e3)
+
+    # end to end through the C ABI with host buffers: upload the state from
+    # host memory, run the steps reading back the status word every step,
+    # download the state
+    st = sim.state()
+    host = {k: np.ascontiguousarray(v) for k, v in st.items()}
+    state_bytes = sum(v.nbytes for v in host.values())
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_steps = 0 if args.no_e2e else args.steps
+    sim.set_state(**host)
+    for _ in range(e2e_steps):
+        sim.step(1)
+        sim.status_word()
+    out = sim.state()
+    sim.sync()
+    t_e2e = time.perf_counter() - t0
+    e2e_val = n * e2e_steps / t_e2e
+    if dist:
+        t = torch.tensor([t_e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_val = world * n * args.steps / float(t.item())
+
+    if rank != 0:
+        return
+    pk, pk_kind = peaks()
+    nar_ms, nar_n = kt["narrow_pp"]
+    nar_avg = nar_ms / max(nar_n, 1)
+    # algorithmic bytes of one particle-particle narrow-phase launch: every
+    # particle's state (216 B) plus every node contact's history and ids (64 B)
+    nar_bytes = BYTES_PARTICLE_STEP * n + BYTES_CONTACT_STEP * 0.5 * (contacts + contacts_end)
+    achieved = nar_bytes / (nar_avg / 1e3) / 1e9 if nar_avg > 0 else None
+    step_bytes = BYTES_PARTICLE_STEP * n + BYTES_CONTACT_STEP * 0.5 * (contacts + contacts_end) + BYTES_BOND_STEP * nbonds
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(seconds=args.cpu_seconds, n=args.cpu_sample)
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "bonded periodic column (config 1 shape)", "particles_per_gpu": n,
+                   "templates": 8, "sdf_grid": "32^3", "surface_nodes": 642, "dt": dt,
+                   "bonds": info["bonds"], "periodic": "xy", "precision": "fp64",
+                   "footprint": info["footprint"], "layers": info["layers"],
+                   "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}",
+                   "pairs": pairs, "node_contacts": contacts, "setup_s": round(t_build, 1)},
+        "e2e": {"value": e2e_val, "unit": METRIC, "h2d_bytes_per_step": state_bytes / args.steps,
+                "d2h_bytes_per_step": 4 + state_bytes / args.steps,
+                "note": "state uploaded from host arrays, status word read every step, state downloaded"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk, "unit": "GB/s",
+                     "frac": (achieved / pk) if achieved else None, "traffic": None,
+                     "kernel": "k_narrow<PP> (narrow phase + contact law)", "peak_source": pk_kind,
+                     "kernel_ms": nar_avg, "algorithmic_bytes": nar_bytes,
+                     "step_achieved_gbs": step_bytes / (t_max / args.steps / 1e3) / 1e9},
+        "kernel_ms_per_step": {k: v[0] / max(args.steps, 1) for k, v in kt.items()},
+        "narrow_work_per_step": {"pairs": wc[0] / args.steps, "clusters": wc[1] / args.steps,
+                                 "clusters_kept": wc[2] / args.steps, "node_contacts": wc[3] / args.steps},
+        "cpu_baseline": cpu,
+        "clocks": clk,
+        "gpu_launches": launches,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="fundem", choices=["fundem", "reference"])
+    ap.add_argument("--n", type=int, default=262144)
+    ap.add_argument("--footprint", type=int, nargs=2, default=[128, 128])
+    ap.add_argument("--cpu-sample", type=int, default=2048)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as D
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        D.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+        dist = D
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_fundem(args, rank, world, dist)
+    finally:
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

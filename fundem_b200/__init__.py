@@ -23,12 +23,14 @@ EXPORTS = [
     "fundem_version", "fundem_status_string", "fundem_create", "fundem_destroy", "fundem_set_precision",
     "fundem_set_records", "fundem_add_material", "fundem_add_geometry", "fundem_mass_properties",
     "fundem_add_objects", "fundem_set_wall_motion", "fundem_move", "fundem_add_bonds", "fundem_set_periodic",
-    "fundem_setup", "fundem_detect", "fundem_step", "fundem_step_begin", "fundem_step_end", "fundem_sync",
+    "fundem_setup", "fundem_detect", "fundem_detect_proximity", "fundem_step", "fundem_step_begin", "fundem_step_end", "fundem_sync",
     "fundem_status_word", "fundem_num_objects", "fundem_get_objects", "fundem_set_objects",
     "fundem_device_view_get", "fundem_num_contacts", "fundem_get_contacts", "fundem_set_contacts",
     "fundem_num_pairs", "fundem_num_bonds", "fundem_get_bonds", "fundem_set_bond_activation",
-    "fundem_get_geometry", "fundem_get_grid", "fundem_launch_count",
+    "fundem_get_geometry", "fundem_get_grid", "fundem_launch_count", "fundem_set_profiling",
+    "fundem_kernel_time", "fundem_work_counters",
 ]
+TIMERS = {"integrate": 0, "hash": 1, "broad": 2, "narrow_pp": 3, "narrow_pw": 4, "ghost": 5, "reduce": 6}
 
 
 class FundemError(RuntimeError):
@@ -70,6 +72,7 @@ def lib():
         L.fundem_set_periodic.argtypes = [P, I, I]
         L.fundem_setup.argtypes = [P, D, D]
         L.fundem_detect.argtypes = [P]
+        L.fundem_detect_proximity.argtypes = [P, C.c_double]
         L.fundem_step.argtypes = [P, I, D, C.c_double]
         L.fundem_step_begin.argtypes = [P, D, C.c_double]
         L.fundem_step_end.argtypes = [P, D, C.c_double]
@@ -89,6 +92,9 @@ def lib():
         L.fundem_get_geometry.argtypes = [P, I, I, D, D, D, D]
         L.fundem_get_grid.argtypes = [P, I, D, D, D, IP]
         L.fundem_launch_count.argtypes = [P, C.POINTER(LL)]
+        L.fundem_set_profiling.argtypes = [P, I]
+        L.fundem_kernel_time.argtypes = [P, I, C.POINTER(C.c_double), C.POINTER(LL)]
+        L.fundem_work_counters.argtypes = [P, C.POINTER(C.c_ulonglong)]
         _lib = L
     return _lib
 
@@ -249,6 +255,9 @@ class Simulation:
     def detect(self):
         _check(self.L.fundem_detect(self.h), "detect")
 
+    def detect_proximity(self, gap):
+        _check(self.L.fundem_detect_proximity(self.h, float(gap)), "detect_proximity")
+
     def step(self, n=1, dt=None, gravity=None):
         g = _f64(self.gravity if gravity is None else gravity, 3)
         _check(self.L.fundem_step(self.h, int(n), _d(g), float(self.dt if dt is None else dt)), "step")
@@ -338,6 +347,29 @@ class Simulation:
         sz = np.zeros(3, np.int32)
         _check(self.L.fundem_get_grid(self.h, int(wall), _d(mn), _d(mx), _d(inv), _i(sz)), "grid")
         return dict(min=mn, max=mx, inv_cell=inv, size=sz)
+
+    def set_profiling(self, on):
+        _check(self.L.fundem_set_profiling(self.h, int(bool(on))), "set_profiling")
+
+    def kernel_times(self):
+        """{group: (milliseconds, intervals)} since the last call."""
+        out = {}
+        for name, k in TIMERS.items():
+            ms, n = C.c_double(), C.c_longlong()
+            _check(self.L.fundem_kernel_time(self.h, k, C.byref(ms), C.byref(n)), "kernel_time")
+            out[name] = (ms.value, n.value)
+        return out
+
+    def work_counters(self):
+        """(pairs, clusters examined, clusters kept, node contacts) since the last call."""
+        a = (C.c_ulonglong * 4)()
+        _check(self.L.fundem_work_counters(self.h, a), "work_counters")
+        return tuple(int(x) for x in a)
+
+    def status_word(self):
+        w = C.c_uint()
+        _check(self.L.fundem_status_word(self.h, C.byref(w)), "status_word")
+        return w.value
 
     def launch_count(self):
         n = C.c_longlong()

@@ -20,6 +20,8 @@ SOURCES = ["fd_kernels.cu", "fd_api.cu"]
 HEADERS = ["fd_internal.cuh", "fd_kernels.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "nvcc")
+# extra compiler definitions, e.g. FUNDEM_NVCC_DEFS="-DFD_NARROW_MIN_BLOCKS=1"
+EXTRA = os.environ.get("FUNDEM_NVCC_DEFS", "").split()
 
 
 def _stale() -> bool:
@@ -38,7 +40,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     for src in SOURCES:
         obj = os.path.join(LIBDIR, src.replace(".cu", ".o"))
         cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
-               "-I", os.path.join(ROOT, "include"), "-c", os.path.join(CSRC, src), "-o", obj]
+               "-I", os.path.join(ROOT, "include"), *EXTRA, "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
             print(" ".join(cmd))

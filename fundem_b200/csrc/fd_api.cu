@@ -512,10 +512,30 @@ struct fundem_sim {
     DevArray<int> scan_tmp;
     DevArray<int> wcount;  // wall-grid histogram (walls are looped over directly)
     DevArray<unsigned int> flags;
+    DevArray<unsigned long long> stats;  // narrow-phase work counters (profiling only)
     std::vector<int> node_base;
     long long n_nodes = 0;
     long long launches = 0;
     std::string last_error;
+    // optional CUDA-event timing of kernel groups (fundem_set_profiling)
+    bool profiling = false;
+    std::vector<cudaEvent_t> tev[FUNDEM_NTIMERS][2];
+    void tbegin(int cat)
+    {
+        if (!profiling) return;
+        cudaEvent_t e;
+        FD_CUDA(cudaEventCreate(&e));
+        FD_CUDA(cudaEventRecord(e, stream));
+        tev[cat][0].push_back(e);
+    }
+    void tend(int cat)
+    {
+        if (!profiling) return;
+        cudaEvent_t e;
+        FD_CUDA(cudaEventCreate(&e));
+        FD_CUDA(cudaEventRecord(e, stream));
+        tev[cat][1].push_back(e);
+    }
 
     void build_node_base()
     {
@@ -555,15 +575,17 @@ struct fundem_sim {
         return g;
     }
 
-    fd::StepArgs step_args(double dt)
+    fd::StepArgs step_args(double dt, double probe = 0.0)
     {
         fd::StepArgs a;
         a.dt = dt;
+        a.probe = probe;
         a.gravity = make_double3(0, 0, 0);
         a.periodic_x = perX;
         a.periodic_y = perY;
         a.records = records;
         a.flags = flags.p;
+        a.stats = profiling ? stats.p : nullptr;
         return a;
     }
 
@@ -641,10 +663,10 @@ struct fundem_sim {
         const int np = P.n();
         const int nw = W.n();
         // capacities (grown after the first detection)
-        const int kinds_cap[FD_NKIND] = {std::max(64, 16 * np), std::max(64, np * std::min(nw, 8)),
-                                         std::max(64, 4 * np), std::max(64, 4 * np), std::max(64, 4 * np)};
+        const int kinds_cap[FD_NKIND] = {std::max(64, 8 * np), std::max(64, np * std::min(nw, 4)),
+                                         std::max(64, np), std::max(64, np), std::max(64, np)};
         for (int k = 0; k < FD_NKIND; ++k) {
-            if (!lists[k].allocated || counts_changed) lists[k].alloc(np, kinds_cap[k], 4 * kinds_cap[k]);
+            if (!lists[k].allocated || counts_changed) lists[k].alloc(np, kinds_cap[k], 2 * kinds_cap[k]);
         }
         const bool act[3] = {perX, perY, perX && perY};
         for (int d = 0; d < 3; ++d) {
@@ -658,18 +680,20 @@ struct fundem_sim {
         size_t st = std::max<size_t>(fd::scan_tmp_size(pgrid.num), fd::scan_tmp_size(np));
         scan_tmp.alloc(st + 16);
         if (!flags.p) flags.alloc(1);
+        if (!stats.p) stats.alloc(8);
         FD_CUDA(cudaStreamSynchronize(stream));
         setup_done = true;
     }
 
     // hash + detection (+ forces) of one step, LSSolver.h:1201-1215
-    void detect_all(bool with_force, double dt)
+    void detect_all(bool with_force, double dt, double probe = 0.0)
     {
         ObjDev Pv = P.view(), Wv = W.view();
         GeoSetDev G = pgeo.view(), GW = wgeo.view();
         fd::MatDev M = pmat.view(), MW = wmat.view();
-        fd::StepArgs a = step_args(dt);
+        fd::StepArgs a = step_args(dt, probe);
         CellTableDev T = ptab.view();
+        tbegin(FUNDEM_T_HASH);
         fd::launch_hash_count(Pv, T, stream);
         fd::launch_cell_table(Pv, T, scan_tmp.p, scan_tmp.n, stream);
         launches += 3;
@@ -679,17 +703,27 @@ struct fundem_sim {
             fd::launch_hash_count(Wv, wt, stream);
             launches += 1;
         }
+        tend(FUNDEM_T_HASH);
         int active[FD_NKIND] = {1, 1, 0, 0, 0};
         for (int k = 0; k < FD_NKIND; ++k) lists[k].cur ^= 1;
         PairListDev Lpp = lists[FD_PP].view();
-        fd::launch_broad_pp(Pv, G, T, Lpp, flags.p, stream);
+        tbegin(FUNDEM_T_BROAD);
+        fd::launch_broad_pp(Pv, G, T, Lpp, flags.p, probe, stream);
+        tend(FUNDEM_T_BROAD);
+        tbegin(FUNDEM_T_NARROW_PP);
         fd::launch_narrow(FD_PP, Pv, G, M, Wv, GW, MW, pgrid, wgrid, nullptr, Lpp, a, with_force, stream);
+        tend(FUNDEM_T_NARROW_PP);
         PairListDev Lpw = lists[FD_PW].view();
-        fd::launch_broad_pw(Pv, G, Wv, GW, wgrid, Lpw, flags.p, stream);
+        tbegin(FUNDEM_T_BROAD);
+        fd::launch_broad_pw(Pv, G, Wv, GW, wgrid, Lpw, flags.p, probe, stream);
+        tend(FUNDEM_T_BROAD);
+        tbegin(FUNDEM_T_NARROW_PW);
         fd::launch_narrow(FD_PW, Pv, G, M, Wv, GW, MW, pgrid, wgrid, nullptr, Lpw, a, with_force, stream);
+        tend(FUNDEM_T_NARROW_PW);
         launches += 4;
         PairListDev Lg[3];
         if (perX || perY) {
+            tbegin(FUNDEM_T_GHOST);
             const int kinds[3] = {FD_GX, FD_GY, FD_GXY};
             for (int d = 0; d < 3; ++d) {
                 if (!ghosts[d].active) continue;
@@ -706,13 +740,15 @@ struct fundem_sim {
                 if (!ghosts[d].active) continue;
                 fd::GhostDev gh = ghosts[d].view();
                 Lg[d] = lists[kinds[d]].view();
-                fd::launch_broad_ghost(Pv, G, gh, Lg[d], flags.p, stream);
+                fd::launch_broad_ghost(Pv, G, gh, Lg[d], flags.p, probe, stream);
                 fd::launch_narrow(kinds[d], Pv, G, M, Wv, GW, MW, pgrid, wgrid, &gh, Lg[d], a, with_force, stream);
                 active[kinds[d]] = 1;
                 launches += 2;
             }
+            tend(FUNDEM_T_GHOST);
         }
         if (!with_force) return;
+        tbegin(FUNDEM_T_REDUCE);
         fd::launch_reverse(Pv, Lpp, scan_tmp.p, scan_tmp.n, stream);
         launches += 4;
         for (int d = 0; d < 3; ++d)
@@ -727,6 +763,7 @@ struct fundem_sim {
         for (int k = 0; k < FD_NKIND; ++k) views[k] = lists[k].view();
         fd::launch_reduce(Pv, views, active, bd, stream);
         launches++;
+        tend(FUNDEM_T_REDUCE);
     }
 
     // copy the device state of a set back into its host mirror
@@ -762,14 +799,18 @@ struct fundem_sim {
     void front(double3 g, double dt)
     {
         ObjDev Pv = P.view(), Wv = W.view();
+        tbegin(FUNDEM_T_INTEGRATE);
         fd::launch_kick(Pv, pgeo.view(), g, 0.5 * dt, stream);
         fd::launch_drift(Pv, dt, stream);
         fd::launch_drift(Wv, dt, stream);
+        tend(FUNDEM_T_INTEGRATE);
         launches += 3;
     }
     void back(double3 g, double dt)
     {
+        tbegin(FUNDEM_T_INTEGRATE);
         fd::launch_kick(P.view(), pgeo.view(), g, 0.5 * dt, stream);
+        tend(FUNDEM_T_INTEGRATE);
         launches++;
     }
 };
@@ -1114,6 +1155,17 @@ int fundem_detect(fundem_sim* s)
     });
 }
 
+int fundem_detect_proximity(fundem_sim* s, double gap)
+{
+    if (!s || !(gap >= 0.0)) return FUNDEM_ERR_ARG;
+    if (!s->setup_done) return FUNDEM_ERR_STATE;
+    return guard(s, [&] {
+        FD_CUDA(cudaSetDevice(s->device));
+        s->detect_all(false, 0.0, gap);
+        s->ensure_capacity();
+    });
+}
+
 int fundem_step_begin(fundem_sim* s, const double g[3], double dt)
 {
     if (!s || !g) return FUNDEM_ERR_ARG;
@@ -1443,6 +1495,47 @@ int fundem_get_grid(fundem_sim* s, int wall, double minb[3], double maxb[3], dou
     if (inv_cell) { inv_cell[0] = g.inv.x; inv_cell[1] = g.inv.y; inv_cell[2] = g.inv.z; }
     if (size) { size[0] = g.size.x; size[1] = g.size.y; size[2] = g.size.z; }
     return FUNDEM_OK;
+}
+
+int fundem_set_profiling(fundem_sim* s, int on)
+{
+    if (!s) return FUNDEM_ERR_ARG;
+    s->profiling = on != 0;
+    return FUNDEM_OK;
+}
+
+int fundem_kernel_time(fundem_sim* s, int group, double* ms_total, long long* count)
+{
+    if (!s || group < 0 || group >= FUNDEM_NTIMERS || !ms_total || !count) return FUNDEM_ERR_ARG;
+    return guard(s, [&] {
+        FD_CUDA(cudaStreamSynchronize(s->stream));
+        auto& a = s->tev[group][0];
+        auto& b = s->tev[group][1];
+        double t = 0.0;
+        const size_t n = std::min(a.size(), b.size());
+        for (size_t k = 0; k < n; ++k) {
+            float ms = 0.f;
+            FD_CUDA(cudaEventElapsedTime(&ms, a[k], b[k]));
+            t += ms;
+        }
+        for (cudaEvent_t e : a) cudaEventDestroy(e);
+        for (cudaEvent_t e : b) cudaEventDestroy(e);
+        a.clear();
+        b.clear();
+        *ms_total = t;
+        *count = (long long)n;
+    });
+}
+
+int fundem_work_counters(fundem_sim* s, unsigned long long out[4])
+{
+    if (!s || !out) return FUNDEM_ERR_ARG;
+    if (!s->stats.p) { out[0] = out[1] = out[2] = out[3] = 0; return FUNDEM_OK; }
+    return guard(s, [&] {
+        FD_CUDA(cudaStreamSynchronize(s->stream));
+        FD_CUDA(cudaMemcpy(out, s->stats.p, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+        FD_CUDA(cudaMemset(s->stats.p, 0, 8 * sizeof(unsigned long long)));
+    });
 }
 
 int fundem_launch_count(fundem_sim* s, long long* n)

@@ -130,22 +130,29 @@ __device__ __forceinline__ double3 fd_rrot(double3 v, fd_quat q)
 // and trilinear value (LSParticleContactDetectionKernel.cuh:4-32).  The
 // pattern is the one nvcc's default contraction gives the reference build:
 // in a sum of products the leftmost product is fused first and the sum is
-// accumulated left to right.
+// accumulated left to right; differences of products are handled by xm_sub.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double xm_sub(double a, double b, double c, double d) { return __fma_rn(a, b, -(c * d)); }
-__device__ __forceinline__ double3 xm_cross(double3 a, double3 b)
+// a*b - c*d with the left (RIGHT = false) or the right product kept exact
+template <bool RIGHT> __device__ __forceinline__ double xm_sub(double a, double b, double c, double d)
 {
-    return mk3(xm_sub(a.y, b.z, a.z, b.y), xm_sub(a.z, b.x, a.x, b.z), xm_sub(a.x, b.y, a.y, b.x));
+    return RIGHT ? __fma_rn(-c, d, a * b) : __fma_rn(a, b, -(c * d));
+}
+template <bool RIGHT> __device__ __forceinline__ double3 xm_cross(double3 a, double3 b)
+{
+    return mk3(xm_sub<RIGHT>(a.y, b.z, a.z, b.y), xm_sub<RIGHT>(a.z, b.x, a.x, b.z), xm_sub<RIGHT>(a.x, b.y, a.y, b.x));
 }
 __device__ __forceinline__ double xm_len2(double3 v) { return __fma_rn(v.z, v.z, __fma_rn(v.x, v.x, v.y * v.y)); }
-__device__ __forceinline__ double3 xm_rot_qv(double q0, double3 qv, double3 v)
+template <bool RIGHT> __device__ __forceinline__ double3 xm_rot_qv(double q0, double3 qv, double3 v)
 {
-    const double3 t = xm_cross(qv, v) * 2.0;
-    const double3 c = xm_cross(qv, t);
+    const double3 t = xm_cross<RIGHT>(qv, v) * 2.0;
+    const double3 c = xm_cross<RIGHT>(qv, t);
     return mk3(__fma_rn(t.x, q0, v.x) + c.x, __fma_rn(t.y, q0, v.y) + c.y, __fma_rn(t.z, q0, v.z) + c.z);
 }
-__device__ __forceinline__ double3 xm_rot(fd_quat q, double3 v) { return xm_rot_qv(q.q0, mk3(q.q1, q.q2, q.q3), v); }
-__device__ __forceinline__ double3 xm_rrot(double3 v, fd_quat q) { return xm_rot_qv(q.q0, mk3(-q.q1, -q.q2, -q.q3), v); }
+// the reference build keeps the left product exact in the forward rotation and
+// the right one in the reverse rotation (negated quaternion components); this
+// reproduces its overlaps bit for bit
+__device__ __forceinline__ double3 xm_rot(fd_quat q, double3 v) { return xm_rot_qv<false>(q.q0, mk3(q.q1, q.q2, q.q3), v); }
+__device__ __forceinline__ double3 xm_rrot(double3 v, fd_quat q) { return xm_rot_qv<true>(q.q0, mk3(-q.q1, -q.q2, -q.q3), v); }
 __device__ __forceinline__ double xm_trilinear(double x, double y, double z, const double p[8])
 {
     const double wx0 = 1.0 - x, wx1 = x, wy0 = 1.0 - y, wy1 = y, wz0 = 1.0 - z, wz1 = z;

@@ -277,7 +277,44 @@ __device__ void emit_pairs(int A, int* buf, int cnt, int total, PairListDev& L, 
 
 constexpr double BOUND_REL = 1e-9;
 
-__global__ void k_broad_pp(ObjDev P, GeoSetDev G, CellTableDev T, PairListDev L, unsigned int* flags)
+// Body-level cull of a candidate pair: true when no surface node of a body of
+// radius rA centred at cA can reach a cell of B's SDF grid where the
+// trilinear value can be <= -probe... i.e. no contact (or proximity pair) is
+// possible.  Uses the same exact-conservative bounds as the cluster cull: the
+// grid box, the distance-to-possibly-inside-cells field (probe == 0 only) and
+// the Lipschitz bound of the trilinear SDF.
+__device__ __forceinline__ bool body_culled(const double3 cA, double rA, const double3 cB, const fd_quat qB,
+                                            const FdGeo& GB, const GeoSetDev& SB, double probe)
+{
+    const double3 lp = fd_rrot(cA - cB, qB);
+    const double3 g = mk3((lp.x - GB.origin.x) * GB.inv_spacing, (lp.y - GB.origin.y) * GB.inv_spacing,
+                          (lp.z - GB.origin.z) * GB.inv_spacing);
+    const double rho = rA * (1.0 + 1e-7) + 1e-12 * (GB.spacing + rA);
+    const double rg = rho * GB.inv_spacing;
+    if (g.x < -rg || g.y < -rg || g.z < -rg) return true;
+    if (g.x > GB.size.x - 1 + rg || g.y > GB.size.y - 1 + rg || g.z > GB.size.z - 1 + rg) return true;
+    if (probe == 0.0) {
+        const int vx = min(max((int)rint(g.x), 0), GB.size.x - 1);
+        const int vy = min(max((int)rint(g.y), 0), GB.size.y - 1);
+        const int vz = min(max((int)rint(g.z), 0), GB.size.z - 1);
+        const double D = (double)__ldg(SB.dist + GB.dist_off + fd_lin3(vx, vy, vz, GB.size));
+        const double3 dv = mk3((g.x - vx) * GB.spacing, (g.y - vy) * GB.spacing, (g.z - vz) * GB.spacing);
+        if (D - length3(dv) > rho) return true;
+    }
+    if (g.x >= 0. && g.y >= 0. && g.z >= 0. && g.x < GB.size.x - 1 && g.y < GB.size.y - 1 && g.z < GB.size.z - 1) {
+        const int i0 = (int)floor(g.x), j0 = (int)floor(g.y), k0 = (int)floor(g.z);
+        const long long sx = GB.size.x, sxy = (long long)GB.size.x * GB.size.y;
+        const double* S = SB.sdf + GB.sdf_off + (long long)k0 * sxy + (long long)j0 * sx + i0;
+        double p[8] = {__ldg(S), __ldg(S + 1), __ldg(S + sx), __ldg(S + sx + 1),
+                       __ldg(S + sxy), __ldg(S + sxy + 1), __ldg(S + sxy + sx), __ldg(S + sxy + sx + 1)};
+        const double phi = xm_trilinear(g.x - i0, g.y - j0, g.z - k0, p);
+        const double bound = GB.lip * rho;
+        if (phi - bound - probe > 1e-7 * (fabs(phi) + bound + probe) + 1e-12 * GB.spacing) return true;
+    }
+    return false;
+}
+
+__global__ void k_broad_pp(ObjDev P, GeoSetDev G, CellTableDev T, PairListDev L, unsigned int* flags, double probe)
 {
     const int A = blockIdx.x * blockDim.x + threadIdx.x;
     if (A >= P.n) return;
@@ -297,9 +334,12 @@ __global__ void k_broad_pp(ObjDev P, GeoSetDev G, CellTableDev T, PairListDev L,
                 for (int k = s; k < s + c; ++k) {
                     const int B = T.sorted[k];
                     if (B <= A) continue;
-                    const double3 d = cA - P.pos[B];
-                    const double rs = rA + G.geo[P.geo[B]].radius;
+                    const double3 cB = P.pos[B];
+                    const double3 d = cA - cB;
+                    const FdGeo& GB = G.geo[P.geo[B]];
+                    const double rs = rA + GB.radius;
                     if (lengthSq3(d) > rs * rs * (1.0 + 4.0 * BOUND_REL)) continue;
+                    if (body_culled(cA, rA, cB, P.q[B], GB, G, probe)) continue;
                     if (cnt < MAX_CAND) buf[cnt++] = B;
                     ++total;
                 }
@@ -308,7 +348,7 @@ __global__ void k_broad_pp(ObjDev P, GeoSetDev G, CellTableDev T, PairListDev L,
 }
 
 __global__ void k_broad_pw(ObjDev P, GeoSetDev G, ObjDev W, GeoSetDev GW, FdGrid wg, PairListDev L,
-                           unsigned int* flags)
+                           unsigned int* flags, double probe)
 {
     const int A = blockIdx.x * blockDim.x + threadIdx.x;
     if (A >= P.n) return;
@@ -324,15 +364,18 @@ __global__ void k_broad_pw(ObjDev P, GeoSetDev G, ObjDev W, GeoSetDev GW, FdGrid
         int3 c;
         decode_cell(h, wg.size, c);
         if (c.x < lo.x || c.x > hi.x || c.y < lo.y || c.y > hi.y || c.z < lo.z || c.z > hi.z) continue;
-        const double rs = rA + GW.geo[W.geo[w]].grid_radius;
-        if (lengthSq3(cA - W.pos[w]) > rs * rs * (1.0 + 4.0 * BOUND_REL)) continue;
+        const FdGeo& GB = GW.geo[W.geo[w]];
+        const double rs = rA + GB.grid_radius;
+        const double3 cW = W.pos[w];
+        if (lengthSq3(cA - cW) > rs * rs * (1.0 + 4.0 * BOUND_REL)) continue;
+        if (body_culled(cA, rA, cW, W.q[w], GB, GW, probe)) continue;
         if (cnt < MAX_CAND) buf[cnt++] = w;
         ++total;
     }
     emit_pairs(A, buf, cnt, total, L, flags);
 }
 
-__global__ void k_broad_ghost(ObjDev P, GeoSetDev G, GhostDev Gh, PairListDev L, unsigned int* flags)
+__global__ void k_broad_ghost(ObjDev P, GeoSetDev G, GhostDev Gh, PairListDev L, unsigned int* flags, double probe)
 {
     const int A = blockIdx.x * blockDim.x + threadIdx.x;
     if (A >= P.n) return;
@@ -352,8 +395,11 @@ __global__ void k_broad_ghost(ObjDev P, GeoSetDev G, GhostDev Gh, PairListDev L,
                 const int s = T.start[h];
                 for (int k = s; k < s + c; ++k) {
                     const int j = T.sorted[k];
-                    const double rs = rA + G.geo[P.geo[j]].grid_radius;
-                    if (lengthSq3(cA - Gh.pos[j]) > rs * rs * (1.0 + 4.0 * BOUND_REL)) continue;
+                    const FdGeo& GB = G.geo[P.geo[j]];
+                    const double rs = rA + GB.grid_radius;
+                    const double3 cj = Gh.pos[j];
+                    if (lengthSq3(cA - cj) > rs * rs * (1.0 + 4.0 * BOUND_REL)) continue;
+                    if (body_culled(cA, rA, cj, P.q[j], GB, G, probe)) continue;
                     if (cnt < MAX_CAND) buf[cnt++] = j;
                     ++total;
                 }
@@ -459,7 +505,8 @@ template <> struct Slave<FD_GXY> : SlaveGhost {};
 template <int KIND>
 __device__ __forceinline__ bool node_predicate(const double3 gp, const int3 bcell, const FdGrid& sg, const double3 cB,
                                                const fd_quat qB, const FdGeo& GB, const double* sdf, double rB2,
-                                               double& overlap, double& fx, double& fy, double& fz, double p[8])
+                                               double probe, double& overlap, double& fx, double& fy, double& fz,
+                                               double p[8])
 {
     int3 lo, hi;
     fd_node_range(gp, sg, lo, hi);
@@ -490,47 +537,96 @@ __device__ __forceinline__ bool node_predicate(const double3 gp, const int3 bcel
     p[6] = __ldg(S + sxy + sx);
     p[7] = __ldg(S + sxy + sx + 1);
     overlap = -xm_trilinear(fx, fy, fz, p);
-    return overlap >= 0.;
+    return overlap >= -probe;
 }
 
-// cluster culling: true when no node of the cluster can be a contact
-template <int KIND>
-__device__ __forceinline__ bool cluster_culled(const FdCluster& cl, const fd_quat qA, const double3 cA,
-                                               const double3 cB, const fd_quat qB, const FdGeo& GB,
-                                               const GeoSetDev& SB, double rB)
+// Per-pair rigid transform from A's body frame into B's body frame, in
+// FP32, for culling only (the exact predicate stays in FP64):
+// p_B = M p_A + t with M = R(qB)^T R(qA), t = R(qB)^T (cA - cB).
+struct CullXf {
+    float m[9];
+    float t[3];
+};
+
+__device__ __forceinline__ void quat_matrix(const fd_quat q, double R[9])
 {
-    const double3 cw = fd_rot(qA, cl.centre) + cA;
-    const double3 rel = cw - cB;
-    const double rho = cl.radius * (1.0 + 1e-7) + 1e-12 * (GB.spacing + rB);
+    const double q0 = q.q0, q1 = q.q1, q2 = q.q2, q3 = q.q3;
+    R[0] = 1.0 - 2.0 * (q2 * q2 + q3 * q3); R[1] = 2.0 * (q1 * q2 - q0 * q3); R[2] = 2.0 * (q1 * q3 + q0 * q2);
+    R[3] = 2.0 * (q1 * q2 + q0 * q3); R[4] = 1.0 - 2.0 * (q1 * q1 + q3 * q3); R[5] = 2.0 * (q2 * q3 - q0 * q1);
+    R[6] = 2.0 * (q1 * q3 - q0 * q2); R[7] = 2.0 * (q2 * q3 + q0 * q1); R[8] = 1.0 - 2.0 * (q1 * q1 + q2 * q2);
+}
+
+__device__ __forceinline__ CullXf cull_transform(const fd_quat qA, const double3 cA, const fd_quat qB, const double3 cB)
+{
+    double RA[9], RB[9];
+    quat_matrix(qA, RA);
+    quat_matrix(qB, RB);
+    CullXf x;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            x.m[3 * i + j] = (float)(RB[i] * RA[j] + RB[3 + i] * RA[3 + j] + RB[6 + i] * RA[6 + j]);
+    const double3 d = cA - cB;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) x.t[i] = (float)(RB[i] * d.x + RB[3 + i] * d.y + RB[6 + i] * d.z);
+    return x;
+}
+
+// Cluster culling: true when no node of the cluster can pass the node
+// predicate (or, with probe > 0, come within `probe` of B).  Conservative:
+// single-precision evaluation with relative margins far above its rounding
+// (about 1e-7 relative), bounds that hold in exact arithmetic:
+//   * B's bounding sphere (particle pairs: the reference's radius test),
+//   * B's SDF grid box (nodes outside it are never contacts),
+//   * D(v): lower bound on the distance from grid node v to any cell whose
+//     corner minimum is <= 0, 1-Lipschitz in the position,
+//   * the Lipschitz bound of the trilinear SDF (coarse grids such as plane
+//     walls, where it is tight).
+template <int KIND>
+__device__ __forceinline__ bool cluster_culled(const FdCluster& cl, const CullXf& x, const FdGeo& GB,
+                                               const GeoSetDev& SB, double rB, double probe)
+{
+    const float cx = (float)cl.centre.x, cy = (float)cl.centre.y, cz = (float)cl.centre.z;
+    const float px = fmaf(x.m[0], cx, fmaf(x.m[1], cy, fmaf(x.m[2], cz, x.t[0])));
+    const float py = fmaf(x.m[3], cx, fmaf(x.m[4], cy, fmaf(x.m[5], cz, x.t[1])));
+    const float pz = fmaf(x.m[6], cx, fmaf(x.m[7], cy, fmaf(x.m[8], cz, x.t[2])));
+    const float scale = (float)(rB + cl.radius + GB.spacing);
+    const float margin = 2e-5f * scale;
+    const float rho = (float)cl.radius + margin;
     if (Slave<KIND>::radius_test) {
-        const double lim = rB + rho;
-        if (lengthSq3(rel) > lim * lim) return true;
+        const float lim = (float)rB + rho;
+        if (px * px + py * py + pz * pz > lim * lim) return true;
     }
-    const double3 lp = fd_rrot(rel, qB);
-    const double3 g = mk3((lp.x - GB.origin.x) * GB.inv_spacing, (lp.y - GB.origin.y) * GB.inv_spacing,
-                          (lp.z - GB.origin.z) * GB.inv_spacing);
-    const double rg = rho * GB.inv_spacing;
-    // sphere entirely outside the grid box: every node fails the bounds test
-    if (g.x < -rg || g.y < -rg || g.z < -rg) return true;
-    if (g.x > GB.size.x - 1 + rg || g.y > GB.size.y - 1 + rg || g.z > GB.size.z - 1 + rg) return true;
-    // distance bound: D(v) is a lower bound on the distance from grid node v
-    // to any cell where the trilinear SDF can be <= 0; D is 1-Lipschitz
-    const int vx = min(max((int)rint(g.x), 0), GB.size.x - 1);
-    const int vy = min(max((int)rint(g.y), 0), GB.size.y - 1);
-    const int vz = min(max((int)rint(g.z), 0), GB.size.z - 1);
-    const double D = (double)__ldg(SB.dist + GB.dist_off + fd_lin3(vx, vy, vz, GB.size));
-    const double3 dv = mk3((g.x - vx) * GB.spacing, (g.y - vy) * GB.spacing, (g.z - vz) * GB.spacing);
-    if (D - length3(dv) > rho) return true;
-    // Lipschitz bound of the trilinear SDF around the centre
-    if (g.x >= 0. && g.y >= 0. && g.z >= 0. && g.x < GB.size.x - 1 && g.y < GB.size.y - 1 && g.z < GB.size.z - 1) {
-        const int i0 = (int)floor(g.x), j0 = (int)floor(g.y), k0 = (int)floor(g.z);
+    const float is = (float)GB.inv_spacing;
+    const float gx = (px - (float)GB.origin.x) * is, gy = (py - (float)GB.origin.y) * is,
+                gz = (pz - (float)GB.origin.z) * is;
+    const float rg = rho * is + 1e-4f;
+    if (gx < -rg || gy < -rg || gz < -rg) return true;
+    if (gx > GB.size.x - 1 + rg || gy > GB.size.y - 1 + rg || gz > GB.size.z - 1 + rg) return true;
+    if (probe == 0.0) {
+        const int vx = min(max(__float2int_rn(gx), 0), GB.size.x - 1);
+        const int vy = min(max(__float2int_rn(gy), 0), GB.size.y - 1);
+        const int vz = min(max(__float2int_rn(gz), 0), GB.size.z - 1);
+        const float D = __ldg(SB.dist + GB.dist_off + fd_lin3(vx, vy, vz, GB.size));
+        const float sp = (float)GB.spacing;
+        const float dx = (gx - vx) * sp, dy = (gy - vy) * sp, dz = (gz - vz) * sp;
+        if (D - sqrtf(dx * dx + dy * dy + dz * dz) > rho) return true;
+    }
+    // the Lipschitz bound only helps where the field is distance-like
+    if (GB.lip < 4.0 && gx >= 0.f && gy >= 0.f && gz >= 0.f && gx < GB.size.x - 1 && gy < GB.size.y - 1 &&
+        gz < GB.size.z - 1) {
+        const int i0 = (int)gx, j0 = (int)gy, k0 = (int)gz;
         const long long sx = GB.size.x, sxy = (long long)GB.size.x * GB.size.y;
-        const double* S = SB.sdf + GB.sdf_off + (long long)k0 * sxy + (long long)j0 * sx + i0;
-        double p[8] = {__ldg(S), __ldg(S + 1), __ldg(S + sx), __ldg(S + sx + 1),
-                       __ldg(S + sxy), __ldg(S + sxy + 1), __ldg(S + sxy + sx), __ldg(S + sxy + sx + 1)};
-        const double phi = xm_trilinear(g.x - i0, g.y - j0, g.z - k0, p);
-        const double bound = GB.lip * rho;
-        if (phi - bound > 1e-7 * (fabs(phi) + bound) + 1e-12 * GB.spacing) return true;
+        const float* S = SB.sdf32 + GB.sdf_off + (long long)k0 * sxy + (long long)j0 * sx + i0;
+        const float fx = gx - i0, fy = gy - j0, fz = gz - k0;
+        const float c00 = __ldg(S) * (1.f - fx) + __ldg(S + 1) * fx;
+        const float c10 = __ldg(S + sx) * (1.f - fx) + __ldg(S + sx + 1) * fx;
+        const float c01 = __ldg(S + sxy) * (1.f - fx) + __ldg(S + sxy + 1) * fx;
+        const float c11 = __ldg(S + sxy + sx) * (1.f - fx) + __ldg(S + sxy + sx + 1) * fx;
+        const float phi = (c00 * (1.f - fy) + c10 * fy) * (1.f - fz) + (c01 * (1.f - fy) + c11 * fy) * fz;
+        const float bound = (float)GB.lip * rho + (float)probe;
+        if (phi - bound > 1e-5f * (fabsf(phi) + bound + (float)GB.spacing)) return true;
     }
     return false;
 }
@@ -542,8 +638,11 @@ __device__ __forceinline__ double warp_sum(double v)
     return v;
 }
 
+#ifndef FD_NARROW_MIN_BLOCKS
+#define FD_NARROW_MIN_BLOCKS 2
+#endif
 template <int KIND>
-__global__ void __launch_bounds__(NARROW_WARPS * 32) k_narrow(NarrowArgs n)
+__global__ void __launch_bounds__(NARROW_WARPS * 32, FD_NARROW_MIN_BLOCKS) k_narrow(NarrowArgs n)
 {
     __shared__ unsigned int s_mask[NARROW_WARPS][MAX_CLUSTERS];
     __shared__ unsigned char s_cl[NARROW_WARPS][MAX_CLUSTERS];
@@ -574,14 +673,22 @@ __global__ void __launch_bounds__(NARROW_WARPS * 32) k_narrow(NarrowArgs n)
         if (ncl > MAX_CLUSTERS) set_flag(n.a.flags, FD_FLAG_CLUSTER_OVERFLOW);
         // ---- cluster culling, one cluster per lane
         unsigned long long keep = 0ull;
-        for (int c0 = 0; c0 < min(ncl, MAX_CLUSTERS); c0 += 32) {
-            const int c = c0 + lane;
-            bool k = false;
-            if (c < ncl) {
-                const FdCluster cl = n.G.clusters[GA.clus_off + c];
-                k = !cluster_culled<KIND>(cl, qA, cA, cB, qB, GB, SB, rB);
+        {
+            const CullXf xf = cull_transform(qA, cA, qB, cB);
+            for (int c0 = 0; c0 < min(ncl, MAX_CLUSTERS); c0 += 32) {
+                const int c = c0 + lane;
+                bool k = false;
+                if (c < ncl) {
+                    const FdCluster cl = n.G.clusters[GA.clus_off + c];
+                    k = !cluster_culled<KIND>(cl, xf, GB, SB, rB, n.a.probe);
+                }
+                keep |= ((unsigned long long)__ballot_sync(0xffffffffu, k)) << c0;
             }
-            keep |= ((unsigned long long)__ballot_sync(0xffffffffu, k)) << c0;
+        }
+        if (n.a.stats && lane == 0) {
+            atomicAdd(&n.a.stats[0], 1ull);
+            atomicAdd(&n.a.stats[1], (unsigned long long)min(ncl, MAX_CLUSTERS));
+            atomicAdd(&n.a.stats[2], (unsigned long long)__popcll(keep));
         }
         // ---- phase 1: exact predicate over surviving clusters
         int nk = 0, total = 0;
@@ -595,7 +702,7 @@ __global__ void __launch_bounds__(NARROW_WARPS * 32) k_narrow(NarrowArgs n)
                 const double3 r = xm_rot(qA, node);
                 const double3 gp = mk3(r.x + cA.x, r.y + cA.y, r.z + cA.z);
                 double ov, fx, fy, fz, pv[8];
-                hit = node_predicate<KIND>(gp, bcell, sg, cB, qB, GB, SB.sdf, rB2, ov, fx, fy, fz, pv);
+                hit = node_predicate<KIND>(gp, bcell, sg, cB, qB, GB, SB.sdf, rB2, n.a.probe, ov, fx, fy, fz, pv);
             }
             const unsigned int m = __ballot_sync(0xffffffffu, hit);
             if (m) {
@@ -608,6 +715,7 @@ __global__ void __launch_bounds__(NARROW_WARPS * 32) k_narrow(NarrowArgs n)
             }
         }
         __syncwarp();
+        if (n.a.stats && lane == 0) atomicAdd(&n.a.stats[3], (unsigned long long)total);
         if (total == 0) {
             if (lane < 9) L.pf[(long long)p * 9 + lane] = 0.0;
             if (lane == 0) { L.c_off[p] = 0; L.c_cnt[p] = 0; }
@@ -678,7 +786,7 @@ __global__ void __launch_bounds__(NARROW_WARPS * 32) k_narrow(NarrowArgs n)
                 const double3 r = xm_rot(qA, node);
                 const double3 gp = mk3(r.x + cA.x, r.y + cA.y, r.z + cA.z);
                 double ov = 0., fx = 0., fy = 0., fz = 0., pv[8];
-                node_predicate<KIND>(gp, bcell, sg, cB, qB, GB, SB.sdf, rB2, ov, fx, fy, fz, pv);
+                node_predicate<KIND>(gp, bcell, sg, cB, qB, GB, SB.sdf, rB2, n.a.probe, ov, fx, fy, fz, pv);
                 double3 nrm = fd_gradient_q(fx, fy, fz, pv);
                 nrm = fd_rot(qB, nrm);
                 nrm = fd_normalize(nrm);
@@ -940,22 +1048,22 @@ void launch_ghost_build(const ObjDev& P, GhostDev& Gh, int kind, cudaStream_t s)
     if (P.n > 0) k_ghost_build<<<nblocks(P.n), TPB, 0, s>>>(P, Gh, kind);
 }
 void launch_broad_pp(const ObjDev& P, const GeoSetDev& G, const CellTableDev& T, PairListDev& L,
-                     unsigned int* flags, cudaStream_t s)
+                     unsigned int* flags, double probe, cudaStream_t s)
 {
     cudaMemsetAsync(L.n_pairs, 0, sizeof(int), s);
-    if (P.n > 0) k_broad_pp<<<nblocks(P.n), TPB, 0, s>>>(P, G, T, L, flags);
+    if (P.n > 0) k_broad_pp<<<nblocks(P.n), TPB, 0, s>>>(P, G, T, L, flags, probe);
 }
 void launch_broad_pw(const ObjDev& P, const GeoSetDev& G, const ObjDev& W, const GeoSetDev& GW,
-                     const FdGrid& wg, PairListDev& L, unsigned int* flags, cudaStream_t s)
+                     const FdGrid& wg, PairListDev& L, unsigned int* flags, double probe, cudaStream_t s)
 {
     cudaMemsetAsync(L.n_pairs, 0, sizeof(int), s);
-    if (P.n > 0) k_broad_pw<<<nblocks(P.n), TPB, 0, s>>>(P, G, W, GW, wg, L, flags);
+    if (P.n > 0) k_broad_pw<<<nblocks(P.n), TPB, 0, s>>>(P, G, W, GW, wg, L, flags, probe);
 }
 void launch_broad_ghost(const ObjDev& P, const GeoSetDev& G, const GhostDev& Gh, PairListDev& L,
-                        unsigned int* flags, cudaStream_t s)
+                        unsigned int* flags, double probe, cudaStream_t s)
 {
     cudaMemsetAsync(L.n_pairs, 0, sizeof(int), s);
-    if (P.n > 0) k_broad_ghost<<<nblocks(P.n), TPB, 0, s>>>(P, G, Gh, L, flags);
+    if (P.n > 0) k_broad_ghost<<<nblocks(P.n), TPB, 0, s>>>(P, G, Gh, L, flags, probe);
 }
 
 void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& M, const ObjDev& W,

@@ -113,10 +113,12 @@ struct BondDev {
 
 struct StepArgs {
     double dt;
+    double probe;      // contact when overlap >= -probe (0 in a timestep)
     double3 gravity;
     int periodic_x, periodic_y;
     int records;
     unsigned int* flags;
+    unsigned long long* stats;  // optional: pairs, clusters, clusters kept, contacts (narrow kernels)
 };
 
 // integration and hashing
@@ -129,11 +131,11 @@ void launch_ghost_build(const ObjDev& P, GhostDev& Gh, int kind, cudaStream_t s)
 
 // pair lists
 void launch_broad_pp(const ObjDev& P, const GeoSetDev& G, const CellTableDev& T, PairListDev& L,
-                     unsigned int* flags, cudaStream_t s);
+                     unsigned int* flags, double probe, cudaStream_t s);
 void launch_broad_pw(const ObjDev& P, const GeoSetDev& G, const ObjDev& W, const GeoSetDev& GW,
-                     const FdGrid& wg, PairListDev& L, unsigned int* flags, cudaStream_t s);
+                     const FdGrid& wg, PairListDev& L, unsigned int* flags, double probe, cudaStream_t s);
 void launch_broad_ghost(const ObjDev& P, const GeoSetDev& G, const GhostDev& Gh, PairListDev& L,
-                        unsigned int* flags, cudaStream_t s);
+                        unsigned int* flags, double probe, cudaStream_t s);
 void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& M, const ObjDev& W,
                    const GeoSetDev& GW, const MatDev& MW, const FdGrid& pgrid, const FdGrid& wgrid,
                    const GhostDev* gh, PairListDev& L, const StepArgs& a, int with_force, cudaStream_t s);

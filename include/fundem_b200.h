@@ -83,6 +83,10 @@ int fundem_set_periodic(fundem_sim* sim, int x, int y);
 int fundem_setup(fundem_sim* sim, const double domain_min[3], const double domain_max[3]);
 /* the pre-loop detection (LSSolver.h:1093-1094 and the periodic variants) */
 int fundem_detect(fundem_sim* sim);
+/* detection without forces that also lists node-partner pairs separated by
+   a gap up to `gap` (overlap >= -gap); for building packings and placing
+   bonds.  No counterpart in the reference. */
+int fundem_detect_proximity(fundem_sim* sim, double gap);
 /* nsteps iterations of the loop body of LSSolver::compute* (LSSolver.h:1097-1107):
    kick, drift, detection, forces, bonds, kick.  No host synchronisation. */
 int fundem_step(fundem_sim* sim, int nsteps, const double gravity[3], double dt);
@@ -138,6 +142,18 @@ int fundem_get_geometry(fundem_sim* sim, int wall, int geo, double* radius, doub
 int fundem_get_grid(fundem_sim* sim, int wall, double minb[3], double maxb[3], double inv_cell[3], int size[3]);
 /* kernel launches issued by this simulation so far */
 int fundem_launch_count(fundem_sim* sim, long long* n);
+/* CUDA-event timing of kernel groups on the simulation's stream (off by
+   default).  fundem_kernel_time returns the summed device time and the
+   number of timed intervals since the last query, then resets. */
+enum {
+    FUNDEM_T_INTEGRATE = 0, FUNDEM_T_HASH = 1, FUNDEM_T_BROAD = 2, FUNDEM_T_NARROW_PP = 3,
+    FUNDEM_T_NARROW_PW = 4, FUNDEM_T_GHOST = 5, FUNDEM_T_REDUCE = 6, FUNDEM_NTIMERS = 7
+};
+int fundem_set_profiling(fundem_sim* sim, int on);
+int fundem_kernel_time(fundem_sim* sim, int group, double* ms_total, long long* count);
+/* narrow-phase work since the last call while profiling is on: candidate
+   pairs, node clusters examined, clusters that survived culling, node contacts */
+int fundem_work_counters(fundem_sim* sim, unsigned long long out[4]);
 
 #ifdef __cplusplus
 }

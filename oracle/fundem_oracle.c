@@ -8,9 +8,11 @@
  * Floating point: the contact-membership arithmetic (node rotation, relative
  * position, radius test, body-frame grid coordinate and trilinear value) is
  * written with explicit fma() calls in the pattern nvcc's default contraction
- * gives the reference build (left product fused first, sums accumulated left
- * to right), so that pair lists and overlaps can be compared bit for bit with
- * the reference run on a GPU.  Everything else is plain IEEE double with
+ * gives the reference build (sums of products accumulated left to right; in
+ * a difference of products the left product is fused, except in the reverse
+ * rotation, whose negated quaternion components make the right one fused),
+ * so that pair lists and overlaps compare bit for bit with the reference run
+ * on a GPU.  Everything else is plain IEEE double with
  * contraction disabled (-ffp-contract=off).  Device-only intrinsics of the
  * reference (rsqrt in normalize) are replaced by 1/sqrt, as the reference's own
  * host path does (myVec.h:128-134); this moves normals by about one ulp.
@@ -30,8 +32,16 @@ typedef struct { double q0, q1, q2, q3; } qt;
 typedef struct { double xx, yy, zz, xy, xz, yz; } sm;
 
 static int g_fma = 1;
+/* which product each contracted a*b - c*d keeps exact: bit0 forward rotation
+   t = q x v, bit1 forward q x t, bit2 reverse rotation t, bit3 reverse q x t,
+   bit4 first sum of the trilinear value; set bit = right-hand product fused.
+   12 (the reverse rotation, whose quaternion components are negated, fuses
+   the right-hand product; everything else the left) reproduces every overlap
+   of the reference build bit for bit (tests/test_oracle_cpu.py). */
+static int g_pattern = 12;
 void orc_set_fma_mode(int mode) { g_fma = mode ? 1 : 0; }
 int orc_get_fma_mode(void) { return g_fma; }
+void orc_set_fma_pattern(int p) { g_pattern = p; }
 void orc_set_threads(int n)
 {
 #ifdef _OPENMP
@@ -80,6 +90,15 @@ static inline double msub(double a, double b, double c, double d)
 {
     return g_fma ? fma(a, b, -(c * d)) : a * b - c * d;
 }
+static inline double msub_p(double a, double b, double c, double d, int right)
+{
+    if (!g_fma) return a * b - c * d;
+    return right ? fma(-c, d, a * b) : fma(a, b, -(c * d));
+}
+static inline d3 cross_p(d3 a, d3 b, int right)
+{
+    return v3(msub_p(a.y, b.z, a.z, b.y, right), msub_p(a.z, b.x, a.x, b.z, right), msub_p(a.x, b.y, a.y, b.x, right));
+}
 /* x*x + y*y + z*z contracted: fma(z, z, fma(x, x, y*y)) */
 static inline double len2_c(d3 v)
 {
@@ -98,16 +117,16 @@ static inline double ats(double v, double t, double s, double w)
 static inline d3 rotq_c(qt q, d3 v)
 {
     d3 qv = v3(q.q1, q.q2, q.q3);
-    d3 t = mul(cross_c(qv, v), 2.0);
-    d3 c = cross_c(qv, t);
+    d3 t = mul(cross_p(qv, v, g_pattern & 1), 2.0);
+    d3 c = cross_p(qv, t, (g_pattern >> 1) & 1);
     return v3(ats(v.x, t.x, q.q0, c.x), ats(v.y, t.y, q.q0, c.y), ats(v.z, t.z, q.q0, c.z));
 }
 /* reverseRotateVectorByQuaternion, myQua.h:120-128 */
 static inline d3 rrotq_c(d3 v, qt q)
 {
     d3 qv = v3(-q.q1, -q.q2, -q.q3);
-    d3 t = mul(cross_c(qv, v), 2.0);
-    d3 c = cross_c(qv, t);
+    d3 t = mul(cross_p(qv, v, (g_pattern >> 2) & 1), 2.0);
+    d3 c = cross_p(qv, t, (g_pattern >> 3) & 1);
     return v3(ats(v.x, t.x, q.q0, c.x), ats(v.y, t.y, q.q0, c.y), ats(v.z, t.z, q.q0, c.z));
 }
 /* plain versions for everything outside the membership predicate */
@@ -131,7 +150,8 @@ static inline double trilinear_c(double x, double y, double z, const double p[8]
         return p[0] * wx0 * wy0 * wz0 + p[1] * wx1 * wy0 * wz0 + p[2] * wx0 * wy1 * wz0 +
                p[3] * wx1 * wy1 * wz0 + p[4] * wx0 * wy0 * wz1 + p[5] * wx1 * wy0 * wz1 +
                p[6] * wx0 * wy1 * wz1 + p[7] * wx1 * wy1 * wz1;
-    double s = fma(p[0] * wx0 * wy0, wz0, p[1] * wx1 * wy0 * wz0);
+    double s = (g_pattern & 16) ? fma(p[1] * wx1 * wy0, wz0, p[0] * wx0 * wy0 * wz0)
+                                : fma(p[0] * wx0 * wy0, wz0, p[1] * wx1 * wy0 * wz0);
     s = fma(p[2] * wx0 * wy1, wz0, s);
     s = fma(p[3] * wx1 * wy1, wz0, s);
     s = fma(p[4] * wx0 * wy0, wz1, s);

@@ -40,6 +40,8 @@ void orc_set_threads(int n);
    arithmetic (default); 0: plain IEEE mul and add. */
 void orc_set_fma_mode(int mode);
 int orc_get_fma_mode(void);
+/* choose, per contracted difference of products, which product is fused */
+void orc_set_fma_pattern(int pattern);
 
 int orc_add_material(orc_world* w, int wall, double kn, double ks, double mu, double e);
 int orc_add_geometry(orc_world* w, int wall, double mass, const double inertia[6],

@@ -44,6 +44,7 @@ def lib():
         L.orc_destroy.argtypes = [P]
         L.orc_set_threads.argtypes = [C.c_int]
         L.orc_set_fma_mode.argtypes = [C.c_int]
+        L.orc_set_fma_pattern.argtypes = [C.c_int]
         L.orc_add_material.argtypes = [P, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double]
         L.orc_add_geometry.argtypes = [P, C.c_int, C.c_double, D, D, C.c_double, I, D, C.c_int, D]
         L.orc_mass_properties.argtypes = [C.c_double, D, C.c_double, I, D, D, D, D]
@@ -117,6 +118,10 @@ def set_threads(n):
 
 def set_fma_mode(m):
     lib().orc_set_fma_mode(int(m))
+
+
+def set_fma_pattern(p):
+    lib().orc_set_fma_pattern(int(p))
 
 
 def _rot(q, v):

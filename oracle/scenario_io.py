@@ -74,6 +74,11 @@ def write_reference_scenario(sc, path, n_steps, dump_steps=()):
         w.i32(len(g.tris))
         w.arr(g.tris, "<i4")
 
+    for gi, g in enumerate(sc.particle_geometries):
+        if g.density is not None:
+            mats = np.unique(sc.particles.mat[sc.particles.geo == gi])
+            if len(mats) > 1:
+                raise ValueError("addParticleCluster gives one material to all particles of a geometry")
     w.i32(len(sc.particle_geometries))
     for g in sc.particle_geometries:
         geo(g, True)

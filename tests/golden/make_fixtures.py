@@ -55,6 +55,9 @@ def scenario_bytes(name):
 
 
 def run(out, cases):
+    # the reference resolves relative output directories against the
+    # executable's location (LSSolver.h:638-644): pass absolute paths
+    out = os.path.abspath(out)
     os.makedirs(out, exist_ok=True)
     for name in cases:
         d = os.path.join(out, name)

@@ -56,6 +56,8 @@ def cluster(seed=3, n=48, grid_n=16, level=2):
                     particle_geometries=geos, wall_geometries=wall_geos, particles=objs, walls=walls,
                     name="cluster")
     sc.particles.mat[::3] = 1
+    # addParticleCluster takes one material for all of a geometry's particles
+    sc.particles.mat[sc.particles.geo == 3] = 0
     return sc
 
 
