@@ -260,7 +260,8 @@ def run_fundem(args, rank, world, dist):
                      "step_achieved_gbs": step_bytes / (t_max / args.steps / 1e3) / 1e9},
         "kernel_ms_per_step": {k: v[0] / max(args.steps, 1) for k, v in kt.items()},
         "narrow_work_per_step": {"pairs": wc[0] / args.steps, "clusters": wc[1] / args.steps,
-                                 "clusters_kept": wc[2] / args.steps, "node_contacts": wc[3] / args.steps},
+                                 "clusters_kept": wc[2] / args.steps, "node_contacts": wc[3] / args.steps,
+                                 "exact_node_tests": wc[4] / args.steps},
         "cpu_baseline": cpu,
         "clocks": clk,
         "gpu_launches": launches,

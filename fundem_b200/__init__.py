@@ -361,8 +361,9 @@ class Simulation:
         return out
 
     def work_counters(self):
-        """(pairs, clusters examined, clusters kept, node contacts) since the last call."""
-        a = (C.c_ulonglong * 4)()
+        """(pairs, clusters examined, clusters kept, node contacts, exact node
+        tests) since the last call."""
+        a = (C.c_ulonglong * 5)()
         _check(self.L.fundem_work_counters(self.h, a), "work_counters")
         return tuple(int(x) for x in a)
 

@@ -223,6 +223,7 @@ struct GeoSetHost {
     DevArray<double> d_sdf;
     DevArray<float> d_sdf32;
     DevArray<float> d_dist;
+    DevArray<float> d_cellmin;
     DevArray<double3> d_nodes;
     DevArray<int> d_lid;
     DevArray<FdCluster> d_clusters;
@@ -234,7 +235,7 @@ struct GeoSetHost {
     {
         table.clear();
         std::vector<double> sdf;
-        std::vector<float> sdf32, dist;
+        std::vector<float> sdf32, dist, cellmin;
         std::vector<double3> nodes;
         std::vector<int> lid;
         std::vector<FdCluster> clusters;
@@ -247,6 +248,21 @@ struct GeoSetHost {
             t.size = g.size;
             t.sdf_off = (long long)sdf.size();
             t.dist_off = (long long)dist.size();
+            t.cellmin_off = (long long)cellmin.size();
+            {
+                // per-cell minimum of the eight corner values, rounded down
+                const int nx = g.size.x, ny = g.size.y, nz = g.size.z;
+                auto S = [&](int x, int y, int z) { return g.sdf[(size_t)z * ny * nx + (size_t)y * nx + x]; };
+                for (int z = 0; z < nz - 1; ++z)
+                    for (int y = 0; y < ny - 1; ++y)
+                        for (int x = 0; x < nx - 1; ++x) {
+                            double m = S(x, y, z);
+                            for (int d = 1; d < 8; ++d) m = std::min(m, S(x + (d & 1), y + ((d >> 1) & 1), z + (d >> 2)));
+                            float f = (float)m;
+                            if ((double)f > m) f = std::nextafter(f, -FLT_MAX);
+                            cellmin.push_back(f);
+                        }
+            }
             sdf.insert(sdf.end(), g.sdf.begin(), g.sdf.end());
             for (double v : g.sdf) sdf32.push_back((float)v);
             std::vector<float> D = distance_bound(g);
@@ -311,6 +327,8 @@ struct GeoSetHost {
         d_sdf32.upload(sdf32.data(), sdf32.size(), s);
         d_dist.alloc(std::max<size_t>(dist.size(), 1));
         d_dist.upload(dist.data(), dist.size(), s);
+        d_cellmin.alloc(std::max<size_t>(cellmin.size(), 1));
+        d_cellmin.upload(cellmin.data(), cellmin.size(), s);
         d_nodes.alloc(std::max<size_t>(nodes.size(), 1));
         d_nodes.upload(nodes.data(), nodes.size(), s);
         d_lid.alloc(std::max<size_t>(lid.size(), 1));
@@ -329,6 +347,7 @@ struct GeoSetHost {
         v.sdf = d_sdf.p;
         v.sdf32 = d_sdf32.p;
         v.dist = d_dist.p;
+        v.cellmin = d_cellmin.p;
         v.nodes = d_nodes.p;
         v.node_lid = d_lid.p;
         v.clusters = d_clusters.p;
@@ -836,13 +855,7 @@ int guard(fundem_sim* s, const std::function<void()>& f)
     }
 }
 double3 d3(const double* p) { return make_double3(p[0], p[1], p[2]); }
-// host rotations used by bond creation (myQua.h:104-128, host branch)
-double3 hrot(const fd_quat& q, double3 v)
-{
-    const double3 qv = make_double3(q.q1, q.q2, q.q3);
-    const double3 t = cross3(qv, v) * 2.0;
-    return v + t * q.q0 + cross3(qv, t);
-}
+// host reverse rotation used by bond creation (myQua.h:120-128, host branch)
 double3 hrrot(double3 v, const fd_quat& q)
 {
     const double3 qv = make_double3(-q.q1, -q.q2, -q.q3);
@@ -1527,13 +1540,13 @@ int fundem_kernel_time(fundem_sim* s, int group, double* ms_total, long long* co
     });
 }
 
-int fundem_work_counters(fundem_sim* s, unsigned long long out[4])
+int fundem_work_counters(fundem_sim* s, unsigned long long out[5])
 {
     if (!s || !out) return FUNDEM_ERR_ARG;
-    if (!s->stats.p) { out[0] = out[1] = out[2] = out[3] = 0; return FUNDEM_OK; }
+    if (!s->stats.p) { for (int k = 0; k < 5; ++k) out[k] = 0; return FUNDEM_OK; }
     return guard(s, [&] {
         FD_CUDA(cudaStreamSynchronize(s->stream));
-        FD_CUDA(cudaMemcpy(out, s->stats.p, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+        FD_CUDA(cudaMemcpy(out, s->stats.p, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
         FD_CUDA(cudaMemset(s->stats.p, 0, 8 * sizeof(unsigned long long)));
     });
 }

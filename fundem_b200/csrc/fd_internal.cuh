@@ -46,6 +46,7 @@ struct FdGeo {
     int3 size;             // grid nodes per axis
     long long sdf_off;     // offset into the SDF pools
     long long dist_off;    // offset into the distance-bound pool (one float per grid node)
+    long long cellmin_off; // offset into the cell-minimum pool (one float per cell, rounded down)
     int node_off;          // first node (cluster order) in the node pools
     int node_count;
     int clus_off;          // first cluster in the cluster pool

@@ -29,6 +29,7 @@ namespace {
 constexpr int TPB = 256;
 constexpr int MAX_CAND = 64;        // candidate partners per particle and kind
 constexpr int MAX_CLUSTERS = 64;    // clusters per template (two warp-wide batches)
+constexpr int MAX_NODE_QUEUE = 32 * MAX_CLUSTERS;  // per-warp queue of nodes for the exact test
 constexpr int NARROW_WARPS = 8;     // warps per block in the narrow kernel
 constexpr double PI_D = 3.14159265358979323846;
 
@@ -631,6 +632,55 @@ __device__ __forceinline__ bool cluster_culled(const FdCluster& cl, const CullXf
     return false;
 }
 
+// Node filter: true when a node certainly fails the node predicate.  The
+// node is mapped into B's frame in single precision (position error below
+// perr); it is dropped only when
+//   * it lies farther than rB + perr from B's centre (particle pairs), or
+//   * it lies outside B's grid box by more than the error, or
+//   * (distance-like fields) the single-precision trilinear value exceeds the
+//     probe by more than the field's Lipschitz bound times the error, or
+//   * it sits inside one cell, away from the cell faces by more than the
+//     error, whose eight corner values all exceed the probe (the trilinear
+//     value is a convex combination of them).
+// Nodes that pass go to the exact double-precision predicate.
+template <int KIND>
+__device__ __forceinline__ bool node_filtered(const double3 p, const CullXf& x, const FdGeo& GB, const GeoSetDev& SB,
+                                              float rB, float perr, double probe)
+{
+    const float cx = (float)p.x, cy = (float)p.y, cz = (float)p.z;
+    const float px = fmaf(x.m[0], cx, fmaf(x.m[1], cy, fmaf(x.m[2], cz, x.t[0])));
+    const float py = fmaf(x.m[3], cx, fmaf(x.m[4], cy, fmaf(x.m[5], cz, x.t[1])));
+    const float pz = fmaf(x.m[6], cx, fmaf(x.m[7], cy, fmaf(x.m[8], cz, x.t[2])));
+    if (Slave<KIND>::radius_test) {
+        const float lim = rB + perr;
+        if (px * px + py * py + pz * pz > lim * lim) return true;
+    }
+    const float is = (float)GB.inv_spacing;
+    const float gx = (px - (float)GB.origin.x) * is, gy = (py - (float)GB.origin.y) * is,
+                gz = (pz - (float)GB.origin.z) * is;
+    const float ge = perr * is + 1e-4f;
+    const float hx = (float)(GB.size.x - 1), hy = (float)(GB.size.y - 1), hz = (float)(GB.size.z - 1);
+    if (gx < -ge || gy < -ge || gz < -ge || gx > hx + ge || gy > hy + ge || gz > hz + ge) return true;
+    if (gx < ge || gy < ge || gz < ge || gx > hx - ge || gy > hy - ge || gz > hz - ge) return false;
+    const int i0 = (int)gx, j0 = (int)gy, k0 = (int)gz;
+    const float fx = gx - i0, fy = gy - j0, fz = gz - k0;
+    if (GB.lip < 4.0) {
+        const long long sx = GB.size.x, sxy = (long long)GB.size.x * GB.size.y;
+        const float* S = SB.sdf32 + GB.sdf_off + (long long)k0 * sxy + (long long)j0 * sx + i0;
+        const float c00 = __ldg(S) * (1.f - fx) + __ldg(S + 1) * fx;
+        const float c10 = __ldg(S + sx) * (1.f - fx) + __ldg(S + sx + 1) * fx;
+        const float c01 = __ldg(S + sxy) * (1.f - fx) + __ldg(S + sxy + 1) * fx;
+        const float c11 = __ldg(S + sxy + sx) * (1.f - fx) + __ldg(S + sxy + sx + 1) * fx;
+        const float phi = (c00 * (1.f - fy) + c10 * fy) * (1.f - fz) + (c01 * (1.f - fy) + c11 * fy) * fz;
+        const float slack = (float)GB.lip * perr + 1e-5f * (fabsf(phi) + (float)GB.spacing);
+        return phi - (float)probe > slack;
+    }
+    if (fx < ge || fy < ge || fz < ge || fx > 1.f - ge || fy > 1.f - ge || fz > 1.f - ge) return false;
+    const float cm = __ldg(SB.cellmin + GB.cellmin_off +
+                           ((long long)k0 * (GB.size.y - 1) + j0) * (GB.size.x - 1) + i0);
+    return cm > (float)probe;
+}
+
 __device__ __forceinline__ double warp_sum(double v)
 {
 #pragma unroll
@@ -644,8 +694,7 @@ __device__ __forceinline__ double warp_sum(double v)
 template <int KIND>
 __global__ void __launch_bounds__(NARROW_WARPS * 32, FD_NARROW_MIN_BLOCKS) k_narrow(NarrowArgs n)
 {
-    __shared__ unsigned int s_mask[NARROW_WARPS][MAX_CLUSTERS];
-    __shared__ unsigned char s_cl[NARROW_WARPS][MAX_CLUSTERS];
+    __shared__ unsigned short s_node[NARROW_WARPS][MAX_NODE_QUEUE];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     const unsigned int lt_mask = (1u << lane) - 1u;
@@ -673,8 +722,8 @@ __global__ void __launch_bounds__(NARROW_WARPS * 32, FD_NARROW_MIN_BLOCKS) k_nar
         if (ncl > MAX_CLUSTERS) set_flag(n.a.flags, FD_FLAG_CLUSTER_OVERFLOW);
         // ---- cluster culling, one cluster per lane
         unsigned long long keep = 0ull;
+        const CullXf xf = cull_transform(qA, cA, qB, cB);
         {
-            const CullXf xf = cull_transform(qA, cA, qB, cB);
             for (int c0 = 0; c0 < min(ncl, MAX_CLUSTERS); c0 += 32) {
                 const int c = c0 + lane;
                 bool k = false;
@@ -690,31 +739,45 @@ __global__ void __launch_bounds__(NARROW_WARPS * 32, FD_NARROW_MIN_BLOCKS) k_nar
             atomicAdd(&n.a.stats[1], (unsigned long long)min(ncl, MAX_CLUSTERS));
             atomicAdd(&n.a.stats[2], (unsigned long long)__popcll(keep));
         }
-        // ---- phase 1: exact predicate over surviving clusters
-        int nk = 0, total = 0;
+        // ---- phase 1a: single-precision filter over the surviving clusters
+        // nodes; nodes that may pass the predicate are queued in cluster order
+        const float perr = 4e-6f * (float)(length3(cA - cB) + GA.radius + rB + GB.spacing);
+        int ncand = 0;
         while (keep) {
             const int c = __ffsll((long long)keep) - 1;
             keep &= keep - 1ull;
             const FdCluster cl = n.G.clusters[GA.clus_off + c];
+            const int k = cl.start + lane;
+            bool cand = false;
+            if (lane < cl.count)
+                cand = !node_filtered<KIND>(n.G.nodes[GA.node_off + k], xf, GB, SB, (float)rB, perr, n.a.probe);
+            const unsigned int m = __ballot_sync(0xffffffffu, cand);
+            if (cand) s_node[wib][ncand + __popc(m & lt_mask)] = (unsigned short)k;
+            ncand += __popc(m);
+        }
+        __syncwarp();
+        // ---- phase 1b: the exact predicate on the queued nodes; contacts are
+        // compacted in place (a slot is rewritten only after it was read)
+        int total = 0;
+        for (int b0 = 0; b0 < ncand; b0 += 32) {
+            const int idx = b0 + lane;
             bool hit = false;
-            if (lane < cl.count) {
-                const double3 node = n.G.nodes[GA.node_off + cl.start + lane];
+            int k = 0;
+            if (idx < ncand) {
+                k = s_node[wib][idx];
+                const double3 node = n.G.nodes[GA.node_off + k];
                 const double3 r = xm_rot(qA, node);
                 const double3 gp = mk3(r.x + cA.x, r.y + cA.y, r.z + cA.z);
                 double ov, fx, fy, fz, pv[8];
                 hit = node_predicate<KIND>(gp, bcell, sg, cB, qB, GB, SB.sdf, rB2, n.a.probe, ov, fx, fy, fz, pv);
             }
             const unsigned int m = __ballot_sync(0xffffffffu, hit);
-            if (m) {
-                if (lane == 0) {
-                    s_cl[wib][nk] = (unsigned char)c;
-                    s_mask[wib][nk] = m;
-                }
-                ++nk;
-                total += __popc(m);
-            }
+            __syncwarp();
+            if (hit) s_node[wib][total + __popc(m & lt_mask)] = (unsigned short)k;
+            total += __popc(m);
         }
         __syncwarp();
+        if (n.a.stats && lane == 0) atomicAdd(&n.a.stats[4], (unsigned long long)ncand);
         if (n.a.stats && lane == 0) atomicAdd(&n.a.stats[3], (unsigned long long)total);
         if (total == 0) {
             if (lane < 9) L.pf[(long long)p * 9 + lane] = 0.0;
@@ -775,13 +838,10 @@ __global__ void __launch_bounds__(NARROW_WARPS * 32, FD_NARROW_MIN_BLOCKS) k_nar
             mu = fmin(mui, n.M.mu[mj]);
         }
         const int node_base = n.P.node_base[A];
-        int written = 0;
-        for (int t = 0; t < nk; ++t) {
-            const int c = s_cl[wib][t];
-            const unsigned int m = s_mask[wib][t];
-            if (m & (1u << lane)) {
-                const FdCluster cl = n.G.clusters[GA.clus_off + c];
-                const int pool = GA.node_off + cl.start + lane;
+        for (int b0 = 0; b0 < total; b0 += 32) {
+            const int idx = b0 + lane;
+            if (idx < total) {
+                const int pool = GA.node_off + s_node[wib][idx];
                 const double3 node = n.G.nodes[pool];
                 const double3 r = xm_rot(qA, node);
                 const double3 gp = mk3(r.x + cA.x, r.y + cA.y, r.z + cA.z);
@@ -809,7 +869,7 @@ __global__ void __launch_bounds__(NARROW_WARPS * 32, FD_NARROW_MIN_BLOCKS) k_nar
                     accTB += cross3(pt - rj, -F);
                 }
                 if (store) {
-                    const long long slot = base + written + __popc(m & lt_mask);
+                    const long long slot = base + idx;
                     L.c_node[slot] = nid;
                     L.c_slave[slot] = B;
                     L.c_spring[3 * slot + 0] = spring.x;
@@ -828,7 +888,6 @@ __global__ void __launch_bounds__(NARROW_WARPS * 32, FD_NARROW_MIN_BLOCKS) k_nar
                     }
                 }
             }
-            written += __popc(m);
         }
         const double red[9] = {warp_sum(accF.x), warp_sum(accF.y), warp_sum(accF.z),
                                warp_sum(accTA.x), warp_sum(accTA.y), warp_sum(accTA.z),

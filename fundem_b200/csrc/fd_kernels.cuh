@@ -64,6 +64,7 @@ struct GeoSetDev {
     const double* sdf;
     const float* sdf32;
     const float* dist;
+    const float* cellmin;
     const double3* nodes;     // cluster order
     const int* node_lid;      // original local index of each node (cluster order)
     const FdCluster* clusters;

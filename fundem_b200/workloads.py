@@ -92,7 +92,9 @@ def bonded_column(n=262144, footprint=(128, 128), seed=1, pitch=2.42e-3, jitter=
     nz = int(np.ceil(n / (nx * ny)))
     box = np.array([nx, ny, nz]) * pitch
     pos = S.lattice_positions(rng, n, np.zeros(3), box + 1e-12, pitch, jitter)
-    pos[:, 2] += 0.5 * pitch
+    # lift the bed so no surface node starts below the floor
+    rmax = max(S.node_radius(g) for g in geos)
+    pos[:, 2] += rmax + 0.01 * pitch - 0.5 * pitch
     geo = rng.integers(0, n_templates, n).astype(np.int32)
     quat = S.random_quaternions(rng, n)
     objs = S.Objects(pos, np.zeros((n, 3)), np.zeros((n, 3)), quat, np.zeros(n, np.int32), geo)

@@ -152,8 +152,9 @@ enum {
 int fundem_set_profiling(fundem_sim* sim, int on);
 int fundem_kernel_time(fundem_sim* sim, int group, double* ms_total, long long* count);
 /* narrow-phase work since the last call while profiling is on: candidate
-   pairs, node clusters examined, clusters that survived culling, node contacts */
-int fundem_work_counters(fundem_sim* sim, unsigned long long out[4]);
+   pairs, node clusters examined, clusters that survived culling, node
+   contacts, nodes given the exact double-precision predicate */
+int fundem_work_counters(fundem_sim* sim, unsigned long long out[5]);
 
 #ifdef __cplusplus
 }
