@@ -28,7 +28,7 @@ EXPORTS = [
     "fundem_device_view_get", "fundem_num_contacts", "fundem_get_contacts", "fundem_set_contacts",
     "fundem_num_pairs", "fundem_num_bonds", "fundem_get_bonds", "fundem_set_bond_activation",
     "fundem_get_geometry", "fundem_get_grid", "fundem_launch_count", "fundem_set_profiling",
-    "fundem_kernel_time", "fundem_work_counters",
+    "fundem_kernel_time", "fundem_work_counters", "fundem_prefix_sum",
 ]
 TIMERS = {"integrate": 0, "hash": 1, "broad": 2, "narrow_pp": 3, "narrow_pw": 4, "ghost": 5, "reduce": 6}
 
@@ -95,6 +95,7 @@ def lib():
         L.fundem_set_profiling.argtypes = [P, I]
         L.fundem_kernel_time.argtypes = [P, I, C.POINTER(C.c_double), C.POINTER(LL)]
         L.fundem_work_counters.argtypes = [P, C.POINTER(C.c_ulonglong)]
+        L.fundem_prefix_sum.argtypes = [P, P, LL, P]
         _lib = L
     return _lib
 
@@ -131,6 +132,17 @@ def mass_properties(density, origin, spacing, size, sdf):
     _check(lib().fundem_mass_properties(float(density), _d(_f64(origin, 3)), float(spacing), _i(_i32(size)),
                                         _d(_f64(sdf)), _d(m), _d(c), _d(I)), "mass_properties")
     return float(m[0]), c, I
+
+
+def prefix_sum(count, out=None, stream=None):
+    """Inclusive prefix sum of a CUDA int32 tensor through the C ABI
+    (the reference's buildPrefixSum); returns the output tensor."""
+    import torch
+    assert count.is_cuda and count.dtype == torch.int32 and count.is_contiguous()
+    if out is None:
+        out = torch.empty_like(count)
+    _check(lib().fundem_prefix_sum(out.data_ptr(), count.data_ptr(), count.numel(), stream), "prefix_sum")
+    return out
 
 
 def _rot(q, v):

@@ -1540,6 +1540,20 @@ int fundem_kernel_time(fundem_sim* s, int group, double* ms_total, long long* co
     });
 }
 
+int fundem_prefix_sum(int* d_prefix, const int* d_count, long long n, void* stream)
+{
+    if (n < 0 || n > 0x7fffffffLL || (n > 0 && (!d_prefix || !d_count))) return FUNDEM_ERR_ARG;
+    if (n == 0) return FUNDEM_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t ntmp = fd::scan_tmp_size(n);
+    int* tmp = nullptr;
+    if (cudaMallocAsync((void**)&tmp, ntmp * sizeof(int), s) != cudaSuccess) return FUNDEM_ERR_CUDA;
+    fd::scan_inclusive(d_count, d_prefix, n, tmp, s);
+    cudaError_t e = cudaGetLastError();
+    cudaFreeAsync(tmp, s);
+    return e == cudaSuccess ? FUNDEM_OK : FUNDEM_ERR_CUDA;
+}
+
 int fundem_work_counters(fundem_sim* s, unsigned long long out[5])
 {
     if (!s || !out) return FUNDEM_ERR_ARG;

@@ -76,6 +76,7 @@ __device__ __forceinline__ int block_excl_scan(int v, int* total)
     return r;
 }
 
+template <bool INCLUSIVE>
 __global__ void k_scan_tile(const int* in, int* out, long long n, int* tile_sums)
 {
     const long long base = (long long)blockIdx.x * SCAN_TILE + (long long)threadIdx.x * SCAN_ITEMS;
@@ -92,8 +93,9 @@ __global__ void k_scan_tile(const int* in, int* out, long long n, int* tile_sums
 #pragma unroll
     for (int k = 0; k < SCAN_ITEMS; ++k) {
         const long long i = base + k;
+        if (INCLUSIVE) run += v[k];
         if (i < n) out[i] = run;
-        run += v[k];
+        if (!INCLUSIVE) run += v[k];
     }
     if (tile_sums && threadIdx.x == 0) tile_sums[blockIdx.x] = total;
 }
@@ -1068,12 +1070,26 @@ void scan_exclusive(const int* in, int* out, long long n, int* tmp, cudaStream_t
 {
     if (n <= 0) return;
     if (n <= SCAN_TILE) {
-        k_scan_tile<<<1, SCAN_TPB, 0, s>>>(in, out, n, nullptr);
+        k_scan_tile<false><<<1, SCAN_TPB, 0, s>>>(in, out, n, nullptr);
         return;
     }
     const long long tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
     int* sums = tmp;
-    k_scan_tile<<<(unsigned)tiles, SCAN_TPB, 0, s>>>(in, out, n, sums);
+    k_scan_tile<false><<<(unsigned)tiles, SCAN_TPB, 0, s>>>(in, out, n, sums);
+    scan_exclusive(sums, sums, tiles, tmp + tiles, s);
+    k_scan_add<<<(unsigned)tiles, SCAN_TPB, 0, s>>>(out, n, sums);
+}
+
+void scan_inclusive(const int* in, int* out, long long n, int* tmp, cudaStream_t s)
+{
+    if (n <= 0) return;
+    if (n <= SCAN_TILE) {
+        k_scan_tile<true><<<1, SCAN_TPB, 0, s>>>(in, out, n, nullptr);
+        return;
+    }
+    const long long tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+    int* sums = tmp;
+    k_scan_tile<true><<<(unsigned)tiles, SCAN_TPB, 0, s>>>(in, out, n, sums);
     scan_exclusive(sums, sums, tiles, tmp + tiles, s);
     k_scan_add<<<(unsigned)tiles, SCAN_TPB, 0, s>>>(out, n, sums);
 }

@@ -147,5 +147,7 @@ void launch_reduce(ObjDev& P, PairListDev* lists, const int* active, const BondD
 // exclusive scan of n ints (out may alias in); returns needed tmp ints when tmp == nullptr
 size_t scan_tmp_size(long long n);
 void scan_exclusive(const int* in, int* out, long long n, int* tmp, cudaStream_t s);
+// inclusive scan of n ints; tmp as for scan_exclusive
+void scan_inclusive(const int* in, int* out, long long n, int* tmp, cudaStream_t s);
 
 }  // namespace fd

@@ -140,6 +140,13 @@ int fundem_set_bond_activation(fundem_sim* sim, const int* activated);
 int fundem_get_geometry(fundem_sim* sim, int wall, int geo, double* radius, double* inv_mass, double inertia[6],
                         double inv_inertia[6]);
 int fundem_get_grid(fundem_sim* sim, int wall, double minb[3], double maxb[3], double inv_cell[3], int size[3]);
+/* Inclusive prefix sum of n ints in device memory, stream-ordered:
+   d_prefix[i] = d_count[0] + ... + d_count[i].  Replaces buildPrefixSum,
+   kernel/CUDAKernelFunction/myUtility/buildHashStartEnd.cu:139-177 (which
+   runs thrust::inclusive_scan); scratch is taken with cudaMallocAsync on the
+   stream and released after the scan.  stream may be NULL. */
+int fundem_prefix_sum(int* d_prefix, const int* d_count, long long n, void* stream);
+
 /* kernel launches issued by this simulation so far */
 int fundem_launch_count(fundem_sim* sim, long long* n);
 /* CUDA-event timing of kernel groups on the simulation's stream (off by
