@@ -28,7 +28,7 @@ EXPORTS = [
     "fundem_device_view_get", "fundem_num_contacts", "fundem_get_contacts", "fundem_set_contacts",
     "fundem_num_pairs", "fundem_num_bonds", "fundem_get_bonds", "fundem_set_bond_activation",
     "fundem_get_geometry", "fundem_get_grid", "fundem_launch_count", "fundem_set_profiling",
-    "fundem_kernel_time", "fundem_work_counters", "fundem_prefix_sum",
+    "fundem_kernel_time", "fundem_work_counters", "fundem_prefix_sum", "fundem_prefix_sum_noalloc",
 ]
 TIMERS = {"integrate": 0, "hash": 1, "broad": 2, "narrow_pp": 3, "narrow_pw": 4, "ghost": 5, "reduce": 6}
 
@@ -96,6 +96,7 @@ def lib():
         L.fundem_kernel_time.argtypes = [P, I, C.POINTER(C.c_double), C.POINTER(LL)]
         L.fundem_work_counters.argtypes = [P, C.POINTER(C.c_ulonglong)]
         L.fundem_prefix_sum.argtypes = [P, P, LL, P]
+        L.fundem_prefix_sum_noalloc.argtypes = [P, P, LL, P]
         _lib = L
     return _lib
 

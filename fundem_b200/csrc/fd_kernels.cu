@@ -19,8 +19,10 @@
 //   bonds (contactKernel.cu:293-371), one thread per bond
 //   per-particle reduction in a fixed order (no atomics on forces)
 #include "fd_kernels.cuh"
+#include "../../include/fundem_b200.h"
 
 #include <cstdio>
+#include <mutex>
 
 namespace fd {
 
@@ -1189,3 +1191,60 @@ void launch_reduce(ObjDev& P, PairListDev* lists, const int* active, const BondD
 }
 
 }  // namespace fd
+
+// ---------------------------------------------------------------------------
+// Prefix sum without allocation.
+//
+// For callers that cannot allocate device memory when they need the scan:
+// code that runs inside a device-memory budget owned by another allocator
+// (a framework that has reserved the GPU's memory up front, where a
+// cudaMalloc can fail), and code for which cudaMalloc's implicit device-wide
+// synchronisation is not acceptable.  The scratch (one int per 4096-element
+// tile) lives in a fixed device array of this library instead, so the scan
+// is limited to FUNDEM_NOALLOC_SCAN_MAX elements.  Every GPU that loads the
+// library keeps the 16 KiB array until the process exits.
+//
+// The array is shared by all calls on a device and keeps the last call's
+// contents.  Nothing in it needs to start at zero: every tile sum the scan
+// reads is written earlier in the same call.  Calls that overlap on the GPU
+// (concurrent streams) race on the array.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int NOALLOC_TILES = 4096;
+static_assert((long long)NOALLOC_TILES * fd::SCAN_TILE == FUNDEM_NOALLOC_SCAN_MAX, "limit and scratch size differ");
+static __device__ __align__(256) int g_noalloc_scan_scratch[NOALLOC_TILES];
+
+constexpr int NOALLOC_MAX_DEVICES = 256;
+std::mutex g_noalloc_mutex;
+int* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {nullptr};
+
+// device address of the scratch on the current device; looked up once per
+// device (host code only sees a stand-in for the array's address)
+int noalloc_scratch(int** out)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES) return FUNDEM_ERR_CUDA;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        int* p = nullptr;
+        if (cudaGetSymbolAddress((void**)&p, g_noalloc_scan_scratch) != cudaSuccess || !p) return FUNDEM_ERR_CUDA;
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return FUNDEM_OK;
+}
+}  // namespace
+
+extern "C" int fundem_prefix_sum_noalloc(int* d_prefix, const int* d_count, long long n, void* stream)
+{
+    if (n < 0 || (n > 0 && (!d_prefix || !d_count))) return FUNDEM_ERR_ARG;
+    if (n > FUNDEM_NOALLOC_SCAN_MAX) return FUNDEM_ERR_ARG;
+    if (n == 0) return FUNDEM_OK;
+    int* scratch = nullptr;
+    const int r = noalloc_scratch(&scratch);
+    if (r != FUNDEM_OK) return r;
+    // n <= NOALLOC_TILES * SCAN_TILE: the tile sums fit the array and their
+    // own scan is a single tile, which needs no further scratch
+    fd::scan_inclusive(d_count, d_prefix, n, scratch, (cudaStream_t)stream);
+    return cudaGetLastError() == cudaSuccess ? FUNDEM_OK : FUNDEM_ERR_CUDA;
+}

@@ -147,6 +147,21 @@ int fundem_get_grid(fundem_sim* sim, int wall, double minb[3], double maxb[3], d
    stream and released after the scan.  stream may be NULL. */
 int fundem_prefix_sum(int* d_prefix, const int* d_count, long long n, void* stream);
 
+/* The same inclusive prefix sum without any device allocation.  No
+   counterpart in the reference.  For callers that cannot allocate device
+   memory at the point of the call: code working inside a memory budget that
+   another allocator has already reserved (a cudaMalloc there can fail), and
+   code that cannot accept cudaMalloc's implicit device synchronisation.  The
+   scratch is a fixed 16 KiB device array inside this library, held on every
+   GPU that loads it until the process exits, which limits n to
+   FUNDEM_NOALLOC_SCAN_MAX; larger n returns FUNDEM_ERR_ARG.  The first call
+   on a device looks up the array's device address (once per device, on the
+   current device), so make that first call before any stream capture.  The
+   array is shared by all calls on a device: calls that overlap on the GPU
+   race. */
+#define FUNDEM_NOALLOC_SCAN_MAX 16777216LL
+int fundem_prefix_sum_noalloc(int* d_prefix, const int* d_count, long long n, void* stream);
+
 /* kernel launches issued by this simulation so far */
 int fundem_launch_count(fundem_sim* sim, long long* n);
 /* CUDA-event timing of kernel groups on the simulation's stream (off by
