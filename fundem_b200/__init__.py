@@ -361,8 +361,9 @@ class Simulation:
         _check(self.L.fundem_get_grid(self.h, int(wall), _d(mn), _d(mx), _d(inv), _i(sz)), "grid")
         return dict(min=mn, max=mx, inv_cell=inv, size=sz)
 
-    def set_profiling(self, on):
-        _check(self.L.fundem_set_profiling(self.h, int(bool(on))), "set_profiling")
+    def set_profiling(self, on, counters=False):
+        """Kernel-group timers (on) and narrow-phase work counters (counters)."""
+        _check(self.L.fundem_set_profiling(self.h, int(bool(on)) | (2 if counters else 0)), "set_profiling")
 
     def kernel_times(self):
         """{group: (milliseconds, intervals)} since the last call."""

@@ -538,6 +538,7 @@ struct fundem_sim {
     std::string last_error;
     // optional CUDA-event timing of kernel groups (fundem_set_profiling)
     bool profiling = false;
+    bool counters = false;  // narrow-phase work counters (fundem_set_profiling)
     std::vector<cudaEvent_t> tev[FUNDEM_NTIMERS][2];
     void tbegin(int cat)
     {
@@ -604,7 +605,7 @@ struct fundem_sim {
         a.periodic_y = perY;
         a.records = records;
         a.flags = flags.p;
-        a.stats = profiling ? stats.p : nullptr;
+        a.stats = counters ? stats.p : nullptr;
         return a;
     }
 
@@ -1513,7 +1514,9 @@ int fundem_get_grid(fundem_sim* s, int wall, double minb[3], double maxb[3], dou
 int fundem_set_profiling(fundem_sim* s, int on)
 {
     if (!s) return FUNDEM_ERR_ARG;
-    s->profiling = on != 0;
+    if (on & ~(FUNDEM_PROF_TIMERS | FUNDEM_PROF_COUNTERS)) return FUNDEM_ERR_ARG;
+    s->profiling = (on & FUNDEM_PROF_TIMERS) != 0;
+    s->counters = (on & FUNDEM_PROF_COUNTERS) != 0;
     return FUNDEM_OK;
 }
 

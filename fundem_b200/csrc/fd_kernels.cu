@@ -699,6 +699,10 @@ template <int KIND>
 __global__ void __launch_bounds__(NARROW_WARPS * 32, FD_NARROW_MIN_BLOCKS) k_narrow(NarrowArgs n)
 {
     __shared__ unsigned short s_node[NARROW_WARPS][MAX_NODE_QUEUE];
+    // work counters, summed per block and added to the global ones once
+    __shared__ unsigned long long s_stats[5];
+    if (n.a.stats && threadIdx.x < 5) s_stats[threadIdx.x] = 0ull;
+    __syncthreads();
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     const unsigned int lt_mask = (1u << lane) - 1u;
@@ -739,9 +743,9 @@ __global__ void __launch_bounds__(NARROW_WARPS * 32, FD_NARROW_MIN_BLOCKS) k_nar
             }
         }
         if (n.a.stats && lane == 0) {
-            atomicAdd(&n.a.stats[0], 1ull);
-            atomicAdd(&n.a.stats[1], (unsigned long long)min(ncl, MAX_CLUSTERS));
-            atomicAdd(&n.a.stats[2], (unsigned long long)__popcll(keep));
+            atomicAdd(&s_stats[0], 1ull);
+            atomicAdd(&s_stats[1], (unsigned long long)min(ncl, MAX_CLUSTERS));
+            atomicAdd(&s_stats[2], (unsigned long long)__popcll(keep));
         }
         // ---- phase 1a: single-precision filter over the surviving clusters
         // nodes; nodes that may pass the predicate are queued in cluster order
@@ -781,8 +785,8 @@ __global__ void __launch_bounds__(NARROW_WARPS * 32, FD_NARROW_MIN_BLOCKS) k_nar
             total += __popc(m);
         }
         __syncwarp();
-        if (n.a.stats && lane == 0) atomicAdd(&n.a.stats[4], (unsigned long long)ncand);
-        if (n.a.stats && lane == 0) atomicAdd(&n.a.stats[3], (unsigned long long)total);
+        if (n.a.stats && lane == 0) atomicAdd(&s_stats[4], (unsigned long long)ncand);
+        if (n.a.stats && lane == 0) atomicAdd(&s_stats[3], (unsigned long long)total);
         if (total == 0) {
             if (lane < 9) L.pf[(long long)p * 9 + lane] = 0.0;
             if (lane == 0) { L.c_off[p] = 0; L.c_cnt[p] = 0; }
@@ -902,6 +906,10 @@ __global__ void __launch_bounds__(NARROW_WARPS * 32, FD_NARROW_MIN_BLOCKS) k_nar
             L.c_cnt[p] = store ? total : 0;
         }
         __syncwarp();
+    }
+    if (n.a.stats) {
+        __syncthreads();
+        if (threadIdx.x < 5 && s_stats[threadIdx.x]) atomicAdd(&n.a.stats[threadIdx.x], s_stats[threadIdx.x]);
     }
 }
 

@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cstdint>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -97,12 +98,23 @@ public:
     std::set<int64_t> dumpSteps;
     int64_t step = 0;
     bool timingOnly = false;
+    // timing window: wall time between the hooks of steps windowFrom and
+    // windowTo, after a device synchronisation at each end.  No output frame
+    // falls inside when windowTo is below the last step.
+    int64_t windowFrom = 0, windowTo = 0;
+    std::chrono::steady_clock::time_point tFrom, tTo;
     std::string out_;
 
     void addExternalForceTorque(const double time) override
     {
         step += 1;
-        if (timingOnly) return;
+        if (timingOnly) {
+            if (step == windowFrom || step == windowTo) {
+                cudaDeviceSynchronize();
+                (step == windowFrom ? tFrom : tTo) = std::chrono::steady_clock::now();
+            }
+            return;
+        }
         if (step == 1) dumpGeometry();
         if (!dumpSteps.count(step)) return;
         cudaStreamSynchronize(0);
@@ -174,7 +186,7 @@ public:
 int main(int argc, char** argv)
 {
     if (argc < 3) {
-        std::cerr << "usage: ref_driver scenario.bin outdir [timing]\n";
+        std::cerr << "usage: ref_driver scenario.bin outdir [timing [from to]]\n";
         return 2;
     }
     const std::string scen = argv[1], out = argv[2];
@@ -190,6 +202,10 @@ int main(int argc, char** argv)
     const int32_t perX = r.get<int32_t>(), perY = r.get<int32_t>();
     DumpSolver s(out + "/vtu", out);
     s.timingOnly = timing;
+    if (timing && argc > 5) {
+        s.windowFrom = std::atoll(argv[4]);
+        s.windowTo = std::atoll(argv[5]);
+    }
     const int32_t nDump = r.get<int32_t>();
     for (int i = 0; i < nDump; ++i) s.dumpSteps.insert(r.get<int32_t>());
 
@@ -321,6 +337,13 @@ int main(int argc, char** argv)
     meta << "wall_seconds " << std::chrono::duration<double>(t1 - t0).count() << "\n";
     cudaError_t err = cudaGetLastError();
     meta << "cuda_status " << cudaGetErrorString(err) << "\n";
+    if (s.windowTo > s.windowFrom && s.step >= s.windowTo) {
+        const double w = std::chrono::duration<double>(s.tTo - s.tFrom).count();
+        meta << "window_steps " << (s.windowTo - s.windowFrom) << "\n";
+        meta << "window_seconds " << w << "\n";
+        std::cout << "ref_driver: window " << s.windowFrom << ".." << s.windowTo << ": "
+                  << 1e3 * w / double(s.windowTo - s.windowFrom) << " ms/step" << std::endl;
+    }
     std::cout << "ref_driver: " << s.step << " steps, " << std::chrono::duration<double>(t1 - t0).count()
               << " s, " << cudaGetErrorString(err) << std::endl;
     return err == cudaSuccess ? 0 : 1;
