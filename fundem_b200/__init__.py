@@ -28,7 +28,7 @@ EXPORTS = [
     "fundem_device_view_get", "fundem_num_contacts", "fundem_get_contacts", "fundem_set_contacts",
     "fundem_num_pairs", "fundem_num_bonds", "fundem_get_bonds", "fundem_set_bond_activation",
     "fundem_get_geometry", "fundem_get_grid", "fundem_launch_count", "fundem_set_profiling",
-    "fundem_kernel_time", "fundem_work_counters", "fundem_prefix_sum", "fundem_prefix_sum_noalloc",
+    "fundem_kernel_time", "fundem_work_counters", "fundem_prefix_sum", "fundem_prefix_sum_noalloc", "fundem_last_error",
 ]
 TIMERS = {"integrate": 0, "hash": 1, "broad": 2, "narrow_pp": 3, "narrow_pw": 4, "ghost": 5, "reduce": 6}
 
@@ -97,6 +97,8 @@ def lib():
         L.fundem_work_counters.argtypes = [P, C.POINTER(C.c_ulonglong)]
         L.fundem_prefix_sum.argtypes = [P, P, LL, P]
         L.fundem_prefix_sum_noalloc.argtypes = [P, P, LL, P]
+        L.fundem_last_error.restype = C.c_char_p
+        L.fundem_last_error.argtypes = [P]
         _lib = L
     return _lib
 
@@ -158,12 +160,19 @@ class Simulation:
     def __init__(self, device=0, stream=None, precision=FP64, records=True):
         self.L = lib()
         h = C.c_void_p()
-        _check(self.L.fundem_create(C.byref(h), int(device), stream), "create")
+        self._check(self.L.fundem_create(C.byref(h), int(device), stream), "create")
         self.h = h
-        _check(self.L.fundem_set_precision(self.h, int(precision)), "set_precision")
-        _check(self.L.fundem_set_records(self.h, int(bool(records))), "set_records")
+        self._check(self.L.fundem_set_precision(self.h, int(precision)), "set_precision")
+        self._check(self.L.fundem_set_records(self.h, int(bool(records))), "set_records")
         self.gravity = np.array([0.0, 0.0, -9.81])
         self.dt = 1e-6
+
+    def _check(self, r, what=""):
+        if r != 0:
+            h = getattr(self, "h", None)
+            detail = self.L.fundem_last_error(h).decode() if h else ""
+            msg = lib().fundem_status_string(r).decode()
+            raise FundemError(f"{what}: {msg} ({r})" + (f": {detail}" if detail else ""))
 
     def close(self):
         if getattr(self, "h", None):
@@ -220,14 +229,14 @@ class Simulation:
 
     def add_material(self, wall, kn, ks, mu, e):
         i = C.c_int()
-        _check(self.L.fundem_add_material(self.h, int(wall), kn, ks, mu, e, C.byref(i)), "add_material")
+        self._check(self.L.fundem_add_material(self.h, int(wall), kn, ks, mu, e, C.byref(i)), "add_material")
         return i.value
 
     def add_geometry(self, wall, mass, inertia, origin, spacing, size, sdf, nodes):
         i = C.c_int()
         nodes = _f64(nodes)
         inertia = None if inertia is None else _f64(inertia, 6)
-        _check(self.L.fundem_add_geometry(self.h, int(wall), float(mass), _d(inertia), _d(_f64(origin, 3)),
+        self._check(self.L.fundem_add_geometry(self.h, int(wall), float(mass), _d(inertia), _d(_f64(origin, 3)),
                                           float(spacing), _i(_i32(size)), _d(_f64(sdf)), nodes.size // 3,
                                           _d(nodes), C.byref(i)), "add_geometry")
         return i.value
@@ -235,12 +244,12 @@ class Simulation:
     def add_objects(self, wall, pos, vel, angvel, quat, mat, geo):
         pos = _f64(pos)
         n = pos.size // 3
-        _check(self.L.fundem_add_objects(self.h, int(wall), n, _d(pos), _d(_f64(vel, 3 * n)),
+        self._check(self.L.fundem_add_objects(self.h, int(wall), n, _d(pos), _d(_f64(vel, 3 * n)),
                                          _d(_f64(angvel, 3 * n)), _d(_f64(quat, 4 * n)), _i(_i32(mat)),
                                          _i(_i32(geo))), "add_objects")
 
     def set_wall_motion(self, idx, vel, angvel):
-        _check(self.L.fundem_set_wall_motion(self.h, int(idx), _d(_f64(vel, 3)), _d(_f64(angvel, 3))),
+        self._check(self.L.fundem_set_wall_motion(self.h, int(idx), _d(_f64(vel, 3)), _d(_f64(angvel, 3))),
                "set_wall_motion")
 
     def add_bonds(self, master, slave, point, normal, radius, length, young, poisson, tensile=None,
@@ -248,7 +257,7 @@ class Simulation:
         master = _i32(master)
         n = master.size
         z = np.zeros(n)
-        _check(self.L.fundem_add_bonds(self.h, n, _i(master), _i(_i32(slave)), _d(_f64(point, 3 * n)),
+        self._check(self.L.fundem_add_bonds(self.h, n, _i(master), _i(_i32(slave)), _d(_f64(point, 3 * n)),
                                        _d(_f64(normal, 3 * n)), _d(_f64(radius, n)), _d(_f64(length, n)),
                                        _d(_f64(young, n)), _d(_f64(poisson, n)),
                                        _d(_f64(z if tensile is None else tensile, n)),
@@ -256,69 +265,69 @@ class Simulation:
                                        _d(_f64(z if friction is None else friction, n))), "add_bonds")
 
     def set_periodic(self, x, y):
-        _check(self.L.fundem_set_periodic(self.h, int(bool(x)), int(bool(y))), "set_periodic")
+        self._check(self.L.fundem_set_periodic(self.h, int(bool(x)), int(bool(y))), "set_periodic")
 
     def set_records(self, full):
-        _check(self.L.fundem_set_records(self.h, int(bool(full))), "set_records")
+        self._check(self.L.fundem_set_records(self.h, int(bool(full))), "set_records")
 
     # ------------------------------------------------------------------ run
     def setup(self, minb, maxb):
-        _check(self.L.fundem_setup(self.h, _d(_f64(minb, 3)), _d(_f64(maxb, 3))), "setup")
+        self._check(self.L.fundem_setup(self.h, _d(_f64(minb, 3)), _d(_f64(maxb, 3))), "setup")
 
     def detect(self):
-        _check(self.L.fundem_detect(self.h), "detect")
+        self._check(self.L.fundem_detect(self.h), "detect")
 
     def detect_proximity(self, gap):
-        _check(self.L.fundem_detect_proximity(self.h, float(gap)), "detect_proximity")
+        self._check(self.L.fundem_detect_proximity(self.h, float(gap)), "detect_proximity")
 
     def step(self, n=1, dt=None, gravity=None):
         g = _f64(self.gravity if gravity is None else gravity, 3)
-        _check(self.L.fundem_step(self.h, int(n), _d(g), float(self.dt if dt is None else dt)), "step")
+        self._check(self.L.fundem_step(self.h, int(n), _d(g), float(self.dt if dt is None else dt)), "step")
 
     def step_begin(self, dt=None, gravity=None):
         g = _f64(self.gravity if gravity is None else gravity, 3)
-        _check(self.L.fundem_step_begin(self.h, _d(g), float(self.dt if dt is None else dt)), "step_begin")
+        self._check(self.L.fundem_step_begin(self.h, _d(g), float(self.dt if dt is None else dt)), "step_begin")
 
     def step_end(self, dt=None, gravity=None):
         g = _f64(self.gravity if gravity is None else gravity, 3)
-        _check(self.L.fundem_step_end(self.h, _d(g), float(self.dt if dt is None else dt)), "step_end")
+        self._check(self.L.fundem_step_end(self.h, _d(g), float(self.dt if dt is None else dt)), "step_end")
 
     def sync(self):
-        _check(self.L.fundem_sync(self.h), "sync")
+        self._check(self.L.fundem_sync(self.h), "sync")
 
     # ------------------------------------------------------------------ state
     def num(self, wall=False):
         n = C.c_int()
-        _check(self.L.fundem_num_objects(self.h, int(wall), C.byref(n)), "num_objects")
+        self._check(self.L.fundem_num_objects(self.h, int(wall), C.byref(n)), "num_objects")
         return n.value
 
     def state(self, wall=False):
         n = self.num(wall)
         out = {k: np.zeros((n, 3)) for k in ("pos", "vel", "angvel", "force", "torque")}
         out["quat"] = np.zeros((n, 4))
-        _check(self.L.fundem_get_objects(self.h, int(wall), _d(out["pos"]), _d(out["vel"]), _d(out["angvel"]),
+        self._check(self.L.fundem_get_objects(self.h, int(wall), _d(out["pos"]), _d(out["vel"]), _d(out["angvel"]),
                                          _d(out["quat"]), _d(out["force"]), _d(out["torque"])), "get_objects")
         return out
 
     def set_state(self, wall=False, pos=None, vel=None, angvel=None, quat=None, force=None, torque=None):
         n = self.num(wall)
         f = lambda a, k: None if a is None else _f64(a, n * k)
-        _check(self.L.fundem_set_objects(self.h, int(wall), _d(f(pos, 3)), _d(f(vel, 3)), _d(f(angvel, 3)),
+        self._check(self.L.fundem_set_objects(self.h, int(wall), _d(f(pos, 3)), _d(f(vel, 3)), _d(f(angvel, 3)),
                                          _d(f(quat, 4)), _d(f(force, 3)), _d(f(torque, 3))), "set_objects")
 
     def device_view(self, wall=False):
         v = DeviceView()
-        _check(self.L.fundem_device_view_get(self.h, int(wall), C.byref(v)), "device_view")
+        self._check(self.L.fundem_device_view_get(self.h, int(wall), C.byref(v)), "device_view")
         return v
 
     def num_contacts(self, kind=PP):
         n = C.c_longlong()
-        _check(self.L.fundem_num_contacts(self.h, int(kind), C.byref(n)), "num_contacts")
+        self._check(self.L.fundem_num_contacts(self.h, int(kind), C.byref(n)), "num_contacts")
         return n.value
 
     def num_pairs(self, kind=PP):
         n = C.c_longlong()
-        _check(self.L.fundem_num_pairs(self.h, int(kind), C.byref(n)), "num_pairs")
+        self._check(self.L.fundem_num_pairs(self.h, int(kind), C.byref(n)), "num_pairs")
         return n.value
 
     def contacts(self, kind=PP):
@@ -327,50 +336,50 @@ class Simulation:
                  normal=np.zeros((n, 3)), overlap=np.zeros(n), spring=np.zeros((n, 3)), en=np.zeros(n),
                  es=np.zeros(n))
         if n:
-            _check(self.L.fundem_get_contacts(self.h, int(kind), _i(c["master"]), _i(c["slave"]), _d(c["point"]),
+            self._check(self.L.fundem_get_contacts(self.h, int(kind), _i(c["master"]), _i(c["slave"]), _d(c["point"]),
                                               _d(c["normal"]), _d(c["overlap"]), _d(c["spring"]), _d(c["en"]),
                                               _d(c["es"])), "get_contacts")
         return c
 
     def set_contacts(self, kind, node, partner, spring):
         node = _i32(node)
-        _check(self.L.fundem_set_contacts(self.h, int(kind), node.size, _i(node), _i(_i32(partner)),
+        self._check(self.L.fundem_set_contacts(self.h, int(kind), node.size, _i(node), _i(_i32(partner)),
                                           _d(_f64(spring, 3 * node.size))), "set_contacts")
 
     def bonds(self):
         n = C.c_int()
-        _check(self.L.fundem_num_bonds(self.h, C.byref(n)), "num_bonds")
+        self._check(self.L.fundem_num_bonds(self.h, C.byref(n)), "num_bonds")
         n = n.value
         act, pt, en = np.zeros(n, np.int32), np.zeros((n, 3)), np.zeros((n, 6))
         if n:
-            _check(self.L.fundem_get_bonds(self.h, _i(act), _d(pt), _d(en)), "get_bonds")
+            self._check(self.L.fundem_get_bonds(self.h, _i(act), _d(pt), _d(en)), "get_bonds")
         return dict(activated=act, point=pt, un=en[:, 0], us=en[:, 1], ub=en[:, 2], ut=en[:, 3], sn=en[:, 4],
                     ss=en[:, 5])
 
     def set_bond_activation(self, act):
-        _check(self.L.fundem_set_bond_activation(self.h, _i(_i32(act))), "set_bond_activation")
+        self._check(self.L.fundem_set_bond_activation(self.h, _i(_i32(act))), "set_bond_activation")
 
     def geometry(self, geo, wall=False):
         r, im, I, Ii = np.zeros(1), np.zeros(1), np.zeros(6), np.zeros(6)
-        _check(self.L.fundem_get_geometry(self.h, int(wall), int(geo), _d(r), _d(im), _d(I), _d(Ii)), "geometry")
+        self._check(self.L.fundem_get_geometry(self.h, int(wall), int(geo), _d(r), _d(im), _d(I), _d(Ii)), "geometry")
         return dict(radius=float(r[0]), inv_mass=float(im[0]), inertia=I, inv_inertia=Ii)
 
     def grid(self, wall=False):
         mn, mx, inv = np.zeros(3), np.zeros(3), np.zeros(3)
         sz = np.zeros(3, np.int32)
-        _check(self.L.fundem_get_grid(self.h, int(wall), _d(mn), _d(mx), _d(inv), _i(sz)), "grid")
+        self._check(self.L.fundem_get_grid(self.h, int(wall), _d(mn), _d(mx), _d(inv), _i(sz)), "grid")
         return dict(min=mn, max=mx, inv_cell=inv, size=sz)
 
     def set_profiling(self, on, counters=False):
         """Kernel-group timers (on) and narrow-phase work counters (counters)."""
-        _check(self.L.fundem_set_profiling(self.h, int(bool(on)) | (2 if counters else 0)), "set_profiling")
+        self._check(self.L.fundem_set_profiling(self.h, int(bool(on)) | (2 if counters else 0)), "set_profiling")
 
     def kernel_times(self):
         """{group: (milliseconds, intervals)} since the last call."""
         out = {}
         for name, k in TIMERS.items():
             ms, n = C.c_double(), C.c_longlong()
-            _check(self.L.fundem_kernel_time(self.h, k, C.byref(ms), C.byref(n)), "kernel_time")
+            self._check(self.L.fundem_kernel_time(self.h, k, C.byref(ms), C.byref(n)), "kernel_time")
             out[name] = (ms.value, n.value)
         return out
 
@@ -378,15 +387,15 @@ class Simulation:
         """(pairs, clusters examined, clusters kept, node contacts, exact node
         tests) since the last call."""
         a = (C.c_ulonglong * 5)()
-        _check(self.L.fundem_work_counters(self.h, a), "work_counters")
+        self._check(self.L.fundem_work_counters(self.h, a), "work_counters")
         return tuple(int(x) for x in a)
 
     def status_word(self):
         w = C.c_uint()
-        _check(self.L.fundem_status_word(self.h, C.byref(w)), "status_word")
+        self._check(self.L.fundem_status_word(self.h, C.byref(w)), "status_word")
         return w.value
 
     def launch_count(self):
         n = C.c_longlong()
-        _check(self.L.fundem_launch_count(self.h, C.byref(n)), "launch_count")
+        self._check(self.L.fundem_launch_count(self.h, C.byref(n)), "launch_count")
         return n.value

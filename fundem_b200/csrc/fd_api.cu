@@ -228,12 +228,16 @@ struct GeoSetHost {
     DevArray<int> d_lid;
     DevArray<FdCluster> d_clusters;
     std::vector<FdGeo> table;
+    // node key (cluster-order index) of every node, by pool offset of the
+    // geometry plus the node's original local index
+    std::vector<int> key_of;
     double rmax = 0.0, grid_rmax = 0.0;
     bool built = false;
 
     void build(bool wall, cudaStream_t s)
     {
         table.clear();
+        key_of.clear();
         std::vector<double> sdf;
         std::vector<float> sdf32, dist, cellmin;
         std::vector<double3> nodes;
@@ -311,9 +315,11 @@ struct GeoSetHost {
                 cl.count = pr.second;
                 clusters.push_back(cl);
             }
-            for (int k : idx) {
-                nodes.push_back(g.nodes[k]);
-                lid.push_back(k);
+            key_of.resize(t.node_off + idx.size());
+            for (size_t j = 0; j < idx.size(); ++j) {
+                nodes.push_back(g.nodes[idx[j]]);
+                lid.push_back(idx[j]);
+                key_of[t.node_off + idx[j]] = (int)j;
             }
             rmax = std::max(rmax, t.radius);
             grid_rmax = std::max(grid_rmax, t.grid_radius);
@@ -406,7 +412,7 @@ struct ObjHost {
 };
 
 struct PairGen {
-    DevArray<int> pairA, pairB, seg_off, seg_cnt, c_off, c_cnt, c_node, c_slave, counters;
+    DevArray<int> pairA, pairB, seg_off, seg_cnt, c_off, c_cnt, c_node, c_slave, c_k, counters;
     DevArray<double> pf, c_spring, c_point, c_normal, c_overlap, c_en, c_es;
 };
 
@@ -416,6 +422,10 @@ struct PairList {
     int cap_pairs = 0, cap_contacts = 0;
     int n_obj = 0;
     DevArray<int> rev_cnt, rev_off, rev_fill, rev_pair;
+    // slot and pair scratch of the current step only
+    DevArray<int> c_pair, p_hist_cnt;
+    DevArray<double> c_force;
+    DevArray<int4> p_aux;
     bool allocated = false;
 
     void alloc(int nobj, int capp, int capc)
@@ -427,12 +437,15 @@ struct PairList {
         for (PairGen& g : gen) {
             g.pairA.alloc(cap_pairs); g.pairB.alloc(cap_pairs); g.seg_off.alloc(m); g.seg_cnt.alloc(m);
             g.c_off.alloc(cap_pairs); g.c_cnt.alloc(cap_pairs); g.pf.alloc((size_t)cap_pairs * 9);
-            g.c_node.alloc(cap_contacts); g.c_slave.alloc(cap_contacts); g.c_spring.alloc((size_t)cap_contacts * 3);
+            g.c_node.alloc(cap_contacts); g.c_slave.alloc(cap_contacts); g.c_k.alloc(cap_contacts);
+            g.c_spring.alloc((size_t)cap_contacts * 3);
             g.c_point.alloc((size_t)cap_contacts * 3); g.c_normal.alloc((size_t)cap_contacts * 3);
             g.c_overlap.alloc(cap_contacts); g.c_en.alloc(cap_contacts); g.c_es.alloc(cap_contacts);
-            g.counters.alloc(2);
+            g.counters.alloc(3);
         }
         rev_cnt.alloc(m); rev_off.alloc(m); rev_fill.alloc(m); rev_pair.alloc(cap_pairs);
+        c_pair.alloc(cap_contacts); c_force.alloc((size_t)cap_contacts * 9);
+        p_aux.alloc(cap_pairs); p_hist_cnt.alloc(cap_pairs);
         allocated = true;
     }
     void grow(int capp, int capc)
@@ -443,16 +456,20 @@ struct PairList {
                 g.c_cnt.grow(capp, cap_pairs); g.pf.grow((size_t)capp * 9, (size_t)cap_pairs * 9);
             }
             rev_pair.grow(capp, 0);
+            p_aux.grow(capp, 0);
+            p_hist_cnt.grow(capp, 0);
             cap_pairs = capp;
         }
         if (capc > cap_contacts) {
             for (PairGen& g : gen) {
-                g.c_node.grow(capc, cap_contacts); g.c_slave.grow(capc, cap_contacts);
+                g.c_node.grow(capc, cap_contacts); g.c_slave.grow(capc, cap_contacts); g.c_k.grow(capc, cap_contacts);
                 g.c_spring.grow((size_t)capc * 3, (size_t)cap_contacts * 3);
                 g.c_point.grow((size_t)capc * 3, (size_t)cap_contacts * 3);
                 g.c_normal.grow((size_t)capc * 3, (size_t)cap_contacts * 3);
                 g.c_overlap.grow(capc, cap_contacts); g.c_en.grow(capc, cap_contacts); g.c_es.grow(capc, cap_contacts);
             }
+            c_pair.grow(capc, 0);
+            c_force.grow((size_t)capc * 9, 0);
             cap_contacts = capc;
         }
     }
@@ -467,7 +484,8 @@ struct PairList {
         v.o_c_cnt = o.c_cnt.p;
         v.c_node = c.c_node.p; v.c_slave = c.c_slave.p; v.c_spring = c.c_spring.p; v.c_point = c.c_point.p;
         v.c_normal = c.c_normal.p; v.c_overlap = c.c_overlap.p; v.c_en = c.c_en.p; v.c_es = c.c_es.p;
-        v.n_contacts = c.counters.p + 1; v.cap_contacts = cap_contacts;
+        v.n_slots = c.counters.p + 1; v.n_hits = c.counters.p + 2; v.cap_contacts = cap_contacts;
+        v.c_pair = c_pair.p; v.c_k = c.c_k.p; v.o_c_k = o.c_k.p; v.c_force = c_force.p; v.p_aux = p_aux.p; v.p_hist_cnt = p_hist_cnt.p;
         v.o_c_node = o.c_node.p; v.o_c_spring = o.c_spring.p;
         v.rev_cnt = rev_cnt.p; v.rev_off = rev_off.p; v.rev_fill = rev_fill.p; v.rev_pair = rev_pair.p;
         return v;
@@ -511,6 +529,10 @@ struct BondHost {
 // ---------------------------------------------------------------------------
 // the simulation object
 // ---------------------------------------------------------------------------
+// steps between list-capacity checks inside fundem_step (each check
+// synchronises the stream once)
+constexpr int CAPACITY_CHECK = 64;
+
 struct fundem_sim {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -535,6 +557,7 @@ struct fundem_sim {
     std::vector<int> node_base;
     long long n_nodes = 0;
     long long launches = 0;
+    long long hook_steps = 0;  // fundem_step_begin calls, for capacity checks
     std::string last_error;
     // optional CUDA-event timing of kernel groups (fundem_set_profiling)
     bool profiling = false;
@@ -706,7 +729,7 @@ struct fundem_sim {
     }
 
     // hash + detection (+ forces) of one step, LSSolver.h:1201-1215
-    void detect_all(bool with_force, double dt, double probe = 0.0)
+    void detect_all(bool with_force, double dt, double probe = 0.0, bool new_generation = true)
     {
         ObjDev Pv = P.view(), Wv = W.view();
         GeoSetDev G = pgeo.view(), GW = wgeo.view();
@@ -725,7 +748,8 @@ struct fundem_sim {
         }
         tend(FUNDEM_T_HASH);
         int active[FD_NKIND] = {1, 1, 0, 0, 0};
-        for (int k = 0; k < FD_NKIND; ++k) lists[k].cur ^= 1;
+        if (new_generation)
+            for (int k = 0; k < FD_NKIND; ++k) lists[k].cur ^= 1;
         PairListDev Lpp = lists[FD_PP].view();
         tbegin(FUNDEM_T_BROAD);
         fd::launch_broad_pp(Pv, G, T, Lpp, flags.p, probe, stream);
@@ -767,7 +791,10 @@ struct fundem_sim {
             }
             tend(FUNDEM_T_GHOST);
         }
-        if (!with_force) return;
+        if (!with_force) {
+            FD_CUDA(cudaGetLastError());
+            return;
+        }
         tbegin(FUNDEM_T_REDUCE);
         fd::launch_reverse(Pv, Lpp, scan_tmp.p, scan_tmp.n, stream);
         launches += 4;
@@ -784,6 +811,7 @@ struct fundem_sim {
         fd::launch_reduce(Pv, views, active, bd, stream);
         launches++;
         tend(FUNDEM_T_REDUCE);
+        FD_CUDA(cudaGetLastError());
     }
 
     // copy the device state of a set back into its host mirror
@@ -813,6 +841,33 @@ struct fundem_sim {
             const int needp = 2 * c[0] > L.cap_pairs ? 3 * c[0] : 0;
             const int needc = 2 * c[1] > L.cap_contacts ? 3 * c[1] : 0;
             if (needp || needc) L.grow(std::max(needp, L.cap_pairs), std::max(needc, L.cap_contacts));
+        }
+    }
+
+    // detection outside a step: a list that overflowed is grown to the
+    // demand its counters recorded and the detection runs again into the same
+    // generation (same history source).  Overflow bits raised before the call
+    // are kept for fundem_sync.
+    void detect_fit(double probe)
+    {
+        const unsigned int grow_bits = FD_FLAG_PAIR_OVERFLOW | FD_FLAG_CONTACT_OVERFLOW;
+        unsigned int f0 = 0;
+        FD_CUDA(cudaStreamSynchronize(stream));
+        FD_CUDA(cudaMemcpy(&f0, flags.p, sizeof(f0), cudaMemcpyDeviceToHost));
+        for (int attempt = 0;; ++attempt) {
+            if (attempt > 0 || (f0 & grow_bits)) {
+                const unsigned int clear = f0 & ~grow_bits;
+                FD_CUDA(cudaMemcpy(flags.p, &clear, sizeof(clear), cudaMemcpyHostToDevice));
+            }
+            detect_all(false, 0.0, probe, attempt == 0);
+            ensure_capacity();
+            unsigned int f = 0;
+            FD_CUDA(cudaMemcpy(&f, flags.p, sizeof(f), cudaMemcpyDeviceToHost));
+            if (!(f & grow_bits) || attempt == 3) {
+                const unsigned int keep = f | f0;
+                FD_CUDA(cudaMemcpy(flags.p, &keep, sizeof(keep), cudaMemcpyHostToDevice));
+                break;
+            }
         }
     }
 
@@ -1163,8 +1218,7 @@ int fundem_detect(fundem_sim* s)
     if (!s->setup_done) return FUNDEM_ERR_STATE;
     return guard(s, [&] {
         FD_CUDA(cudaSetDevice(s->device));
-        s->detect_all(false, 0.0);
-        s->ensure_capacity();
+        s->detect_fit(0.0);
         s->detected = true;
     });
 }
@@ -1175,8 +1229,7 @@ int fundem_detect_proximity(fundem_sim* s, double gap)
     if (!s->setup_done) return FUNDEM_ERR_STATE;
     return guard(s, [&] {
         FD_CUDA(cudaSetDevice(s->device));
-        s->detect_all(false, 0.0, gap);
-        s->ensure_capacity();
+        s->detect_fit(gap);
     });
 }
 
@@ -1185,6 +1238,7 @@ int fundem_step_begin(fundem_sim* s, const double g[3], double dt)
     if (!s || !g) return FUNDEM_ERR_ARG;
     if (!s->setup_done) return FUNDEM_ERR_STATE;
     return guard(s, [&] {
+        if (++s->hook_steps % CAPACITY_CHECK == 0) s->ensure_capacity();
         s->front(d3(g), dt);
         s->detect_all(true, dt);
     });
@@ -1204,6 +1258,8 @@ int fundem_step(fundem_sim* s, int nsteps, const double g[3], double dt)
     return guard(s, [&] {
         FD_CUDA(cudaSetDevice(s->device));
         for (int k = 0; k < nsteps; ++k) {
+            // list capacities follow the counts every CAPACITY_CHECK steps
+            if (k > 0 && k % CAPACITY_CHECK == 0) s->ensure_capacity();
             s->front(d3(g), dt);
             s->detect_all(true, dt);
             s->back(d3(g), dt);
@@ -1218,6 +1274,7 @@ int fundem_sync(fundem_sim* s)
     unsigned int f = 0;
     int r = guard(s, [&] {
         FD_CUDA(cudaStreamSynchronize(s->stream));
+        if (s->setup_done) s->ensure_capacity();
         FD_CUDA(cudaGetLastError());
         if (s->flags.p) FD_CUDA(cudaMemcpy(&f, s->flags.p, sizeof(unsigned int), cudaMemcpyDeviceToHost));
     });
@@ -1329,10 +1386,10 @@ int fundem_num_contacts(fundem_sim* s, int kind, long long* n)
     PairList& L = s->lists[kind];
     if (!L.allocated) return FUNDEM_OK;
     return guard(s, [&] {
-        int c[2] = {0, 0};
+        int c[3] = {0, 0, 0};
         FD_CUDA(cudaStreamSynchronize(s->stream));
         FD_CUDA(cudaMemcpy(c, L.gen[L.cur].counters.p, sizeof(c), cudaMemcpyDeviceToHost));
-        *n = std::min(c[1], L.cap_contacts);
+        *n = c[1] <= L.cap_contacts ? c[2] : 0;
     });
 }
 
@@ -1343,11 +1400,12 @@ int fundem_get_contacts(fundem_sim* s, int kind, int* node, int* partner, double
     PairList& L = s->lists[kind];
     if (!L.allocated) return FUNDEM_OK;
     return guard(s, [&] {
-        int c[2] = {0, 0};
+        int c[3] = {0, 0, 0};
         FD_CUDA(cudaStreamSynchronize(s->stream));
         PairGen& g = L.gen[L.cur];
         FD_CUDA(cudaMemcpy(c, g.counters.p, sizeof(c), cudaMemcpyDeviceToHost));
-        const size_t n = (size_t)std::min(c[1], L.cap_contacts);
+        // an overflowed list holds no valid contacts (fundem_num_contacts gives 0)
+        const size_t n = (size_t)(c[1] <= L.cap_contacts ? c[1] : 0);
         std::vector<int> hn(n), hs(n);
         std::vector<double> hsp(3 * n), hpt(3 * n), hnm(3 * n), hov(n), hen(n), hes(n);
         if (n) {
@@ -1360,12 +1418,19 @@ int fundem_get_contacts(fundem_sim* s, int kind, int* node, int* partner, double
             FD_CUDA(cudaMemcpy(hen.data(), g.c_en.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
             FD_CUDA(cudaMemcpy(hes.data(), g.c_es.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
         }
-        std::vector<size_t> order(n);
-        std::iota(order.begin(), order.end(), 0);
+        // slots that hold no contact carry node id -1
+        std::vector<size_t> order;
+        order.reserve(n);
+        for (size_t k = 0; k < n; ++k)
+            if (hn[k] >= 0) order.push_back(k);
+        // the caller sized its arrays with fundem_num_contacts
+        if (order.size() != (size_t)c[2])
+            throw std::runtime_error("contact list inconsistent: " + std::to_string(order.size()) + " contacts in " +
+                                     std::to_string(n) + " slots, counter " + std::to_string(c[2]));
         std::sort(order.begin(), order.end(), [&](size_t a, size_t b) {
             return hn[a] != hn[b] ? hn[a] < hn[b] : hs[a] < hs[b];
         });
-        for (size_t k = 0; k < n; ++k) {
+        for (size_t k = 0; k < order.size(); ++k) {
             const size_t j = order[k];
             if (node) node[k] = hn[j];
             if (partner) partner[k] = hs[j];
@@ -1397,13 +1462,19 @@ int fundem_set_contacts(fundem_sim* s, int kind, long long n, const int* node, c
         };
         for (long long k = 0; k < n; ++k)
             if (node[k] < 0 || node[k] >= s->n_nodes) throw std::invalid_argument("node id out of range");
+        // within a pair, slots ascend in node key (the order the detection
+        // writes them in, which the history search relies on)
+        auto key = [&](int nid) {
+            const int o = owner(nid);
+            return s->pgeo.key_of[s->pgeo.table[s->P.geo[o]].node_off + (nid - s->node_base[o])];
+        };
         std::sort(order.begin(), order.end(), [&](size_t a, size_t b) {
             const int oa = owner(node[a]), ob = owner(node[b]);
             if (oa != ob) return oa < ob;
             if (partner[a] != partner[b]) return partner[a] < partner[b];
-            return node[a] < node[b];
+            return key(node[a]) < key(node[b]);
         });
-        std::vector<int> pairA, pairB, c_off, c_cnt, seg_off(np, 0), seg_cnt(np, 0), cn, cs;
+        std::vector<int> pairA, pairB, c_off, c_cnt, seg_off(np, 0), seg_cnt(np, 0), cn, cs, ck;
         std::vector<double> csp;
         for (size_t t = 0; t < order.size(); ++t) {
             const size_t k = order[t];
@@ -1419,6 +1490,7 @@ int fundem_set_contacts(fundem_sim* s, int kind, long long n, const int* node, c
             c_cnt.back()++;
             cn.push_back(node[k]);
             cs.push_back(B);
+            ck.push_back(key(node[k]));
             csp.insert(csp.end(), {spring[3 * k], spring[3 * k + 1], spring[3 * k + 2]});
         }
         L.grow(std::max<int>(L.cap_pairs, (int)pairA.size() * 2), std::max<int>(L.cap_contacts, (int)cn.size() * 2));
@@ -1431,9 +1503,10 @@ int fundem_set_contacts(fundem_sim* s, int kind, long long n, const int* node, c
         g.c_cnt.upload(c_cnt.data(), c_cnt.size(), s->stream);
         g.c_node.upload(cn.data(), cn.size(), s->stream);
         g.c_slave.upload(cs.data(), cs.size(), s->stream);
+        g.c_k.upload(ck.data(), ck.size(), s->stream);
         g.c_spring.upload(csp.data(), csp.size(), s->stream);
-        const int counters[2] = {(int)pairA.size(), (int)cn.size()};
-        g.counters.upload(counters, 2, s->stream);
+        const int counters[3] = {(int)pairA.size(), (int)cn.size(), (int)cn.size()};
+        g.counters.upload(counters, 3, s->stream);
         FD_CUDA(cudaStreamSynchronize(s->stream));
     });
 }
@@ -1566,6 +1639,11 @@ int fundem_work_counters(fundem_sim* s, unsigned long long out[5])
         FD_CUDA(cudaMemcpy(out, s->stats.p, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
         FD_CUDA(cudaMemset(s->stats.p, 0, 8 * sizeof(unsigned long long)));
     });
+}
+
+const char* fundem_last_error(fundem_sim* s)
+{
+    return s ? s->last_error.c_str() : "";
 }
 
 int fundem_launch_count(fundem_sim* s, long long* n)

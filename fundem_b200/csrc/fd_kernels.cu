@@ -685,23 +685,28 @@ __device__ __forceinline__ bool node_filtered(const double3 p, const CullXf& x, 
     return cm > (float)probe;
 }
 
-__device__ __forceinline__ double warp_sum(double v)
-{
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
-#ifndef FD_NARROW_MIN_BLOCKS
-#define FD_NARROW_MIN_BLOCKS 2
+#ifndef FD_SELECT_MIN_BLOCKS
+#define FD_SELECT_MIN_BLOCKS 3
 #endif
+#ifndef FD_CONTACT_MIN_BLOCKS
+#define FD_CONTACT_MIN_BLOCKS 2
+#endif
+
+// ---------------------------------------------------------------------------
+// narrow phase, stage 1: one warp per candidate pair.  The clusters of A's
+// surface nodes are culled against B, the nodes of the surviving clusters are
+// filtered in single precision, and the nodes that may pass the exact
+// predicate become the pair's contact slots (contiguous, in cluster order).
+// The warp also finds the pair in the previous step's list, the history
+// source of its contacts.
+// ---------------------------------------------------------------------------
 template <int KIND>
-__global__ void __launch_bounds__(NARROW_WARPS * 32, FD_NARROW_MIN_BLOCKS) k_narrow(NarrowArgs n)
+__global__ void __launch_bounds__(NARROW_WARPS * 32, FD_SELECT_MIN_BLOCKS) k_select(NarrowArgs n)
 {
     __shared__ unsigned short s_node[NARROW_WARPS][MAX_NODE_QUEUE];
     // work counters, summed per block and added to the global ones once
-    __shared__ unsigned long long s_stats[5];
-    if (n.a.stats && threadIdx.x < 5) s_stats[threadIdx.x] = 0ull;
+    __shared__ unsigned long long s_stats[4];
+    if (n.a.stats && threadIdx.x < 4) s_stats[threadIdx.x] = 0ull;
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
@@ -709,46 +714,35 @@ __global__ void __launch_bounds__(NARROW_WARPS * 32, FD_NARROW_MIN_BLOCKS) k_nar
     PairListDev& L = n.L;
     const int npairs = min(*L.n_pairs, L.cap_pairs);
     const int nwarps = gridDim.x * NARROW_WARPS;
-    const bool periodic = (KIND == FD_PP || KIND == FD_PW) && (n.a.periodic_x || n.a.periodic_y);
     for (int p = blockIdx.x * NARROW_WARPS + wib; p < npairs; p += nwarps) {
         const int A = L.pairA[p];
         const int B = L.pairB[p];
-        const int gA = n.P.geo[A];
-        const FdGeo& GA = n.G.geo[gA];
+        const FdGeo& GA = n.G.geo[n.P.geo[A]];
         const double3 cA = n.P.pos[A];
         const fd_quat qA = n.P.q[A];
         const double3 cB = Slave<KIND>::pos(n, B);
         const fd_quat qB = Slave<KIND>::q(n, B);
         const FdGeo& GB = Slave<KIND>::geo(n, B);
         const GeoSetDev& SB = Slave<KIND>::set(n);
-        const FdGrid& sg = Slave<KIND>::grid(n);
         const double rB = GB.radius;
-        const double rB2 = rB * rB;
-        int3 bcell;
-        decode_cell(Slave<KIND>::hash(n, B), sg.size, bcell);
         const int ncl = GA.clus_count;
         if (ncl > MAX_CLUSTERS) set_flag(n.a.flags, FD_FLAG_CLUSTER_OVERFLOW);
         // ---- cluster culling, one cluster per lane
         unsigned long long keep = 0ull;
         const CullXf xf = cull_transform(qA, cA, qB, cB);
-        {
-            for (int c0 = 0; c0 < min(ncl, MAX_CLUSTERS); c0 += 32) {
-                const int c = c0 + lane;
-                bool k = false;
-                if (c < ncl) {
-                    const FdCluster cl = n.G.clusters[GA.clus_off + c];
-                    k = !cluster_culled<KIND>(cl, xf, GB, SB, rB, n.a.probe);
-                }
-                keep |= ((unsigned long long)__ballot_sync(0xffffffffu, k)) << c0;
+        for (int c0 = 0; c0 < min(ncl, MAX_CLUSTERS); c0 += 32) {
+            const int c = c0 + lane;
+            bool k = false;
+            if (c < ncl) {
+                const FdCluster cl = n.G.clusters[GA.clus_off + c];
+                k = !cluster_culled<KIND>(cl, xf, GB, SB, rB, n.a.probe);
             }
+            keep |= ((unsigned long long)__ballot_sync(0xffffffffu, k)) << c0;
         }
-        if (n.a.stats && lane == 0) {
-            atomicAdd(&s_stats[0], 1ull);
-            atomicAdd(&s_stats[1], (unsigned long long)min(ncl, MAX_CLUSTERS));
-            atomicAdd(&s_stats[2], (unsigned long long)__popcll(keep));
-        }
-        // ---- phase 1a: single-precision filter over the surviving clusters
-        // nodes; nodes that may pass the predicate are queued in cluster order
+        const int kept = __popcll(keep);
+        // ---- single-precision filter over the nodes of the surviving
+        // clusters; nodes that may pass the predicate are queued in cluster
+        // order
         const float perr = 4e-6f * (float)(length3(cA - cB) + GA.radius + rB + GB.spacing);
         int ncand = 0;
         while (keep) {
@@ -764,152 +758,256 @@ __global__ void __launch_bounds__(NARROW_WARPS * 32, FD_NARROW_MIN_BLOCKS) k_nar
             ncand += __popc(m);
         }
         __syncwarp();
-        // ---- phase 1b: the exact predicate on the queued nodes; contacts are
-        // compacted in place (a slot is rewritten only after it was read)
-        int total = 0;
-        for (int b0 = 0; b0 < ncand; b0 += 32) {
-            const int idx = b0 + lane;
-            bool hit = false;
-            int k = 0;
-            if (idx < ncand) {
-                k = s_node[wib][idx];
-                const double3 node = n.G.nodes[GA.node_off + k];
-                const double3 r = xm_rot(qA, node);
-                const double3 gp = mk3(r.x + cA.x, r.y + cA.y, r.z + cA.z);
-                double ov, fx, fy, fz, pv[8];
-                hit = node_predicate<KIND>(gp, bcell, sg, cB, qB, GB, SB.sdf, rB2, n.a.probe, ov, fx, fy, fz, pv);
-            }
-            const unsigned int m = __ballot_sync(0xffffffffu, hit);
-            __syncwarp();
-            if (hit) s_node[wib][total + __popc(m & lt_mask)] = (unsigned short)k;
-            total += __popc(m);
+        if (n.a.stats && lane == 0) {
+            atomicAdd(&s_stats[0], 1ull);
+            atomicAdd(&s_stats[1], (unsigned long long)min(ncl, MAX_CLUSTERS));
+            atomicAdd(&s_stats[2], (unsigned long long)kept);
+            atomicAdd(&s_stats[3], (unsigned long long)ncand);
         }
-        __syncwarp();
-        if (n.a.stats && lane == 0) atomicAdd(&s_stats[4], (unsigned long long)ncand);
-        if (n.a.stats && lane == 0) atomicAdd(&s_stats[3], (unsigned long long)total);
-        if (total == 0) {
-            if (lane < 9) L.pf[(long long)p * 9 + lane] = 0.0;
-            if (lane == 0) { L.c_off[p] = 0; L.c_cnt[p] = 0; }
-            continue;
-        }
+        // ---- contact slots of the pair
         int base = 0;
-        if (lane == 0) base = atomicAdd(L.n_contacts, total);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        const bool store = (base + total <= L.cap_contacts);
-        if (!store) set_flag(n.a.flags, FD_FLAG_CONTACT_OVERFLOW);
-        // ---- history: the same pair in the previous step's list
-        int oc_off = 0, oc_cnt = 0;
-        {
-            const int os = L.o_seg_off[A], on = L.o_seg_cnt[A];
-            int found = -1;
-            for (int k0 = 0; k0 < on && found < 0; k0 += 32) {
-                const int k = k0 + lane;
-                const bool eq = (k < on) && (L.o_pairB[os + k] == B);
-                const unsigned int m = __ballot_sync(0xffffffffu, eq);
-                if (m) found = os + k0 + __ffs(m) - 1;
-            }
-            if (found >= 0) { oc_off = L.o_c_off[found]; oc_cnt = L.o_c_cnt[found]; }
-        }
-        // ---- phase 2: contact geometry, history, force, records
-        double3 accF = mk3(0., 0., 0.), accTA = mk3(0., 0., 0.), accTB = mk3(0., 0., 0.);
-        // force-side state (positions after the periodic wrap, LSSolver.h:1175-1190)
-        double3 ri = cA, rj = cB;
-        if (periodic) {
-            if (n.a.periodic_x) { ri = wrap_x(ri, n.pgrid); if (KIND == FD_PP) rj = wrap_x(rj, n.pgrid); }
-            if (n.a.periodic_y) { ri = wrap_y(ri, n.pgrid); if (KIND == FD_PP) rj = wrap_y(rj, n.pgrid); }
-        }
-        const double3 vi = n.P.vel[A], wi = n.P.angvel[A];
-        const int mi = n.P.mat[A];
-        const double invMi = GA.inv_mass;
-        const double kni = n.M.kn[mi], ksi = n.M.ks[mi], mui = n.M.mu[mi], ei = n.M.e[mi];
-        double3 vj, wj;
-        double kn = 0., ks = 0., effM = 0., mu, res;
-        if (KIND == FD_PW) {
-            vj = n.W.vel[B];
-            wj = n.W.angvel[B];
-            const int mj = n.W.mat[B];
-            mu = fmin(mui, n.MW.mu[mj]);
-            res = fmin(ei, n.MW.e[mj]);
-            if (invMi > 0.) effM = 1. / invMi;
-            kn = kni;
-            ks = ksi;
-        } else {
-            vj = n.P.vel[B];
-            wj = n.P.angvel[B];
-            const double invMj = GB.inv_mass;
-            const int mj = n.P.mat[B];
-            const double knj = n.M.kn[mj], ksj = n.M.ks[mj];
-            if (kni > 0. && knj > 0.) kn = kni * knj / (kni + knj);
-            if (ksi > 0. && ksj > 0.) ks = ksi * ksj / (ksi + ksj);
-            if (invMi > 0. || invMj > 0.) effM = 1. / (invMi + invMj);
-            res = fmin(ei, n.M.e[mj]);
-            mu = fmin(mui, n.M.mu[mj]);
-        }
-        const int node_base = n.P.node_base[A];
-        for (int b0 = 0; b0 < total; b0 += 32) {
-            const int idx = b0 + lane;
-            if (idx < total) {
-                const int pool = GA.node_off + s_node[wib][idx];
-                const double3 node = n.G.nodes[pool];
-                const double3 r = xm_rot(qA, node);
-                const double3 gp = mk3(r.x + cA.x, r.y + cA.y, r.z + cA.z);
-                double ov = 0., fx = 0., fy = 0., fz = 0., pv[8];
-                node_predicate<KIND>(gp, bcell, sg, cB, qB, GB, SB.sdf, rB2, n.a.probe, ov, fx, fy, fz, pv);
-                double3 nrm = fd_gradient_q(fx, fy, fz, pv);
-                nrm = fd_rot(qB, nrm);
-                nrm = fd_normalize(nrm);
-                const double3 pt = gp + (0.5 * ov) * nrm;
-                const int nid = node_base + n.G.node_lid[pool];
-                double3 spring = mk3(0., 0., 0.);
-                for (int j = 0; j < oc_cnt; ++j) {
-                    if (L.o_c_node[oc_off + j] == nid) {
-                        const double* sp = L.o_c_spring + 3ll * (oc_off + j);
-                        spring = mk3(sp[0], sp[1], sp[2]);
-                        break;
-                    }
-                }
-                double3 F = mk3(0., 0., 0.);
-                if (n.with_force) {
-                    const double3 vc = (vi + cross3(wi, pt - ri)) - (vj + cross3(wj, pt - rj));
-                    linear_contact(F, spring, vc, nrm, ov, n.a.dt, kn, ks, mu, res, effM);
-                    accF += F;
-                    accTA += cross3(pt - ri, F);
-                    accTB += cross3(pt - rj, -F);
-                }
-                if (store) {
-                    const long long slot = base + idx;
-                    L.c_node[slot] = nid;
-                    L.c_slave[slot] = B;
-                    L.c_spring[3 * slot + 0] = spring.x;
-                    L.c_spring[3 * slot + 1] = spring.y;
-                    L.c_spring[3 * slot + 2] = spring.z;
-                    if (n.a.records) {
-                        L.c_point[3 * slot + 0] = pt.x;
-                        L.c_point[3 * slot + 1] = pt.y;
-                        L.c_point[3 * slot + 2] = pt.z;
-                        L.c_normal[3 * slot + 0] = nrm.x;
-                        L.c_normal[3 * slot + 1] = nrm.y;
-                        L.c_normal[3 * slot + 2] = nrm.z;
-                        L.c_overlap[slot] = ov;
-                        L.c_en[slot] = 0.5 * ov * ov * kn;
-                        L.c_es[slot] = 0.5 * lengthSq3(spring) * ks;
-                    }
-                }
+        if (ncand > 0) {
+            if (lane == 0) base = atomicAdd(L.n_slots, ncand);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (base + ncand > L.cap_contacts) {
+                if (lane == 0) set_flag(n.a.flags, FD_FLAG_CONTACT_OVERFLOW);
+                base = 0;
+                ncand = 0;
             }
         }
-        const double red[9] = {warp_sum(accF.x), warp_sum(accF.y), warp_sum(accF.z),
-                               warp_sum(accTA.x), warp_sum(accTA.y), warp_sum(accTA.z),
-                               warp_sum(accTB.x), warp_sum(accTB.y), warp_sum(accTB.z)};
-        if (lane < 9) L.pf[(long long)p * 9 + lane] = red[lane];
+        if (ncand > 0) {
+            // history: the same pair in the previous step's list
+            int oc_off = 0, oc_cnt = 0;
+            {
+                const int os = L.o_seg_off[A], on = L.o_seg_cnt[A];
+                int found = -1;
+                for (int k0 = 0; k0 < on && found < 0; k0 += 32) {
+                    const int k = k0 + lane;
+                    const bool eq = (k < on) && (L.o_pairB[os + k] == B);
+                    const unsigned int m = __ballot_sync(0xffffffffu, eq);
+                    if (m) found = os + k0 + __ffs(m) - 1;
+                }
+                if (found >= 0) { oc_off = L.o_c_off[found]; oc_cnt = L.o_c_cnt[found]; }
+            }
+            for (int i = lane; i < ncand; i += 32) {
+                L.c_pair[base + i] = p;
+                L.c_k[base + i] = s_node[wib][i];
+            }
+            if (lane == 0) {
+                int3 bcell;
+                decode_cell(Slave<KIND>::hash(n, B), Slave<KIND>::grid(n).size, bcell);
+                L.p_aux[p] = make_int4(bcell.x, bcell.y, bcell.z, oc_off);
+                L.p_hist_cnt[p] = oc_cnt;
+            }
+        }
         if (lane == 0) {
-            L.c_off[p] = store ? base : 0;
-            L.c_cnt[p] = store ? total : 0;
+            L.c_off[p] = base;
+            L.c_cnt[p] = ncand;
         }
         __syncwarp();
     }
     if (n.a.stats) {
         __syncthreads();
-        if (threadIdx.x < 5 && s_stats[threadIdx.x]) atomicAdd(&n.a.stats[threadIdx.x], s_stats[threadIdx.x]);
+        if (threadIdx.x < 4 && s_stats[threadIdx.x]) {
+            // pairs, clusters, clusters kept, nodes given the exact predicate
+            const int slot[4] = {0, 1, 2, 4};
+            atomicAdd(&n.a.stats[slot[threadIdx.x]], s_stats[threadIdx.x]);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// narrow phase, stage 2: one thread per contact slot.  The exact
+// double-precision node predicate (LSParticleContactDetectionKernel.cu:37-119);
+// for a contact, the normal, the contact point and the history carried over
+// from the previous step (first match on the node, :288-297), then the
+// contact law (contactKernel.cu:46-291).  A slot whose node is not in contact
+// keeps node id -1.  Force and torques go to the slot; stage 3 sums them per
+// pair.
+// ---------------------------------------------------------------------------
+template <int KIND>
+__global__ void __launch_bounds__(TPB, FD_CONTACT_MIN_BLOCKS) k_contact(NarrowArgs n)
+{
+    __shared__ int s_hits;
+    if (threadIdx.x == 0) s_hits = 0;
+    __syncthreads();
+    PairListDev& L = n.L;
+    const int nslots = min(*L.n_slots, L.cap_contacts);
+    const int lane = threadIdx.x & 31;
+    const bool periodic = (KIND == FD_PP || KIND == FD_PW) && (n.a.periodic_x || n.a.periodic_y);
+    const int stride = gridDim.x * blockDim.x;
+    int hits = 0;
+    for (int s0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); s0 < nslots; s0 += stride) {
+        const int s = s0 + lane;
+        bool hit = false;
+        if (s < nslots) {
+            const int p = L.c_pair[s];
+            const int k = L.c_k[s];
+            const int A = L.pairA[p];
+            const int B = L.pairB[p];
+            const int4 aux = L.p_aux[p];
+            const int3 bcell = make_int3(aux.x, aux.y, aux.z);
+            const FdGeo& GA = n.G.geo[n.P.geo[A]];
+            const double3 cA = n.P.pos[A];
+            const fd_quat qA = n.P.q[A];
+            const double3 cB = Slave<KIND>::pos(n, B);
+            const fd_quat qB = Slave<KIND>::q(n, B);
+            const FdGeo& GB = Slave<KIND>::geo(n, B);
+            const GeoSetDev& SB = Slave<KIND>::set(n);
+            const FdGrid& sg = Slave<KIND>::grid(n);
+            const double rB2 = GB.radius * GB.radius;
+            const int pool = GA.node_off + k;
+            const double3 node = n.G.nodes[pool];
+            const double3 r = xm_rot(qA, node);
+            const double3 gp = mk3(r.x + cA.x, r.y + cA.y, r.z + cA.z);
+            double ov = 0., fx = 0., fy = 0., fz = 0., pv[8];
+            hit = node_predicate<KIND>(gp, bcell, sg, cB, qB, GB, SB.sdf, rB2, n.a.probe, ov, fx, fy, fz, pv);
+            int nid = -1;
+            if (hit) {
+                double3 nrm = fd_gradient_q(fx, fy, fz, pv);
+                nrm = fd_rot(qB, nrm);
+                nrm = fd_normalize(nrm);
+                const double3 pt = gp + (0.5 * ov) * nrm;
+                nid = n.P.node_base[A] + n.G.node_lid[pool];
+                double3 spring = mk3(0., 0., 0.);
+                {
+                    // the previous slots of the pair are ascending in node
+                    // key; a node appears at most once per pair
+                    const int oc_off = aux.w, oc_end = aux.w + L.p_hist_cnt[p];
+                    int lo = oc_off, hi = oc_end;
+                    while (lo < hi) {
+                        const int mid = (lo + hi) >> 1;
+                        if (L.o_c_k[mid] < k) lo = mid + 1; else hi = mid;
+                    }
+                    if (lo < oc_end && L.o_c_k[lo] == k && L.o_c_node[lo] == nid) {
+                        const double* sp = L.o_c_spring + 3ll * lo;
+                        spring = mk3(sp[0], sp[1], sp[2]);
+                    }
+                }
+                double kn = 0., ks = 0.;
+                if (n.with_force) {
+                    // force-side state (positions after the periodic wrap,
+                    // LSSolver.h:1175-1190)
+                    double3 ri = cA, rj = cB;
+                    if (periodic) {
+                        if (n.a.periodic_x) { ri = wrap_x(ri, n.pgrid); if (KIND == FD_PP) rj = wrap_x(rj, n.pgrid); }
+                        if (n.a.periodic_y) { ri = wrap_y(ri, n.pgrid); if (KIND == FD_PP) rj = wrap_y(rj, n.pgrid); }
+                    }
+                    const double3 vi = n.P.vel[A], wi = n.P.angvel[A];
+                    const int mi = n.P.mat[A];
+                    const double invMi = GA.inv_mass;
+                    const double kni = n.M.kn[mi], ksi = n.M.ks[mi], mui = n.M.mu[mi], ei = n.M.e[mi];
+                    double3 vj, wj;
+                    double effM = 0., mu, res;
+                    if (KIND == FD_PW) {
+                        vj = n.W.vel[B];
+                        wj = n.W.angvel[B];
+                        const int mj = n.W.mat[B];
+                        mu = fmin(mui, n.MW.mu[mj]);
+                        res = fmin(ei, n.MW.e[mj]);
+                        if (invMi > 0.) effM = 1. / invMi;
+                        kn = kni;
+                        ks = ksi;
+                    } else {
+                        vj = n.P.vel[B];
+                        wj = n.P.angvel[B];
+                        const double invMj = GB.inv_mass;
+                        const int mj = n.P.mat[B];
+                        const double knj = n.M.kn[mj], ksj = n.M.ks[mj];
+                        if (kni > 0. && knj > 0.) kn = kni * knj / (kni + knj);
+                        if (ksi > 0. && ksj > 0.) ks = ksi * ksj / (ksi + ksj);
+                        if (invMi > 0. || invMj > 0.) effM = 1. / (invMi + invMj);
+                        res = fmin(ei, n.M.e[mj]);
+                        mu = fmin(mui, n.M.mu[mj]);
+                    }
+                    const double3 vc = (vi + cross3(wi, pt - ri)) - (vj + cross3(wj, pt - rj));
+                    double3 F = mk3(0., 0., 0.);
+                    linear_contact(F, spring, vc, nrm, ov, n.a.dt, kn, ks, mu, res, effM);
+                    const double3 TA = cross3(pt - ri, F);
+                    const double3 TB = cross3(pt - rj, -F);
+                    double* o = L.c_force + 9ll * s;
+                    o[0] = F.x; o[1] = F.y; o[2] = F.z;
+                    o[3] = TA.x; o[4] = TA.y; o[5] = TA.z;
+                    o[6] = TB.x; o[7] = TB.y; o[8] = TB.z;
+                }
+                L.c_slave[s] = B;
+                L.c_spring[3 * s + 0] = spring.x;
+                L.c_spring[3 * s + 1] = spring.y;
+                L.c_spring[3 * s + 2] = spring.z;
+                if (n.a.records) {
+                    if (!n.with_force) {
+                        const int mi = n.P.mat[A];
+                        kn = n.M.kn[mi];
+                        ks = n.M.ks[mi];
+                        if (KIND != FD_PW) {
+                            const int mj = n.P.mat[B];
+                            const double knj = n.M.kn[mj], ksj = n.M.ks[mj];
+                            kn = (kn > 0. && knj > 0.) ? kn * knj / (kn + knj) : 0.;
+                            ks = (ks > 0. && ksj > 0.) ? ks * ksj / (ks + ksj) : 0.;
+                        }
+                    }
+                    L.c_point[3 * s + 0] = pt.x;
+                    L.c_point[3 * s + 1] = pt.y;
+                    L.c_point[3 * s + 2] = pt.z;
+                    L.c_normal[3 * s + 0] = nrm.x;
+                    L.c_normal[3 * s + 1] = nrm.y;
+                    L.c_normal[3 * s + 2] = nrm.z;
+                    L.c_overlap[s] = ov;
+                    L.c_en[s] = 0.5 * ov * ov * kn;
+                    L.c_es[s] = 0.5 * lengthSq3(spring) * ks;
+                }
+            }
+            L.c_node[s] = nid;
+        }
+        hits += __popc(__ballot_sync(0xffffffffu, hit));
+    }
+    if (lane == 0 && hits) atomicAdd(&s_hits, hits);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_hits) {
+        atomicAdd(L.n_hits, s_hits);
+        if (n.a.stats) atomicAdd(&n.a.stats[3], (unsigned long long)s_hits);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// narrow phase, stage 3: the pair's force and torques summed over its contact
+// slots.  Eight lanes per pair: lane l sums slots l, l + 8, ... in order, then
+// a fixed butterfly combines the lanes, so the result does not depend on
+// where the pair's slots lie.
+// ---------------------------------------------------------------------------
+__global__ void k_pair_sum(PairListDev L, int with_force)
+{
+    const int npairs = min(*L.n_pairs, L.cap_pairs);
+    const int lane = threadIdx.x & 31, grp = lane >> 3, l = lane & 7;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int p0 = warp * 4; p0 < npairs; p0 += nwarps * 4) {
+        const int p = p0 + grp;
+        double acc[9] = {0., 0., 0., 0., 0., 0., 0., 0., 0.};
+        int o = 0, c = 0;
+        if (p < npairs && with_force) {
+            o = L.c_off[p];
+            c = L.c_cnt[p];
+        }
+        for (int j = l; j < c; j += 8) {
+            if (L.c_node[o + j] < 0) continue;
+            const double* f = L.c_force + 9ll * (o + j);
+#pragma unroll
+            for (int t = 0; t < 9; ++t) acc[t] += f[t];
+        }
+#pragma unroll
+        for (int t = 0; t < 9; ++t) {
+            acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], 4);
+            acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], 2);
+            acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], 1);
+        }
+        if (p < npairs) {
+            double* out = L.pf + 9ll * p;
+#pragma unroll
+            for (int t = 0; t < 8; ++t)
+                if (l == t) out[t] = acc[t];
+            if (l == 0) out[8] = acc[8];
+        }
     }
 }
 
@@ -1155,20 +1253,22 @@ void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& 
                    const GeoSetDev& GW, const MatDev& MW, const FdGrid& pgrid, const FdGrid& wgrid,
                    const GhostDev* gh, PairListDev& L, const StepArgs& a, int with_force, cudaStream_t s)
 {
-    cudaMemsetAsync(L.n_contacts, 0, sizeof(int), s);
+    cudaMemsetAsync(L.n_slots, 0, 2 * sizeof(int), s);  // slots and contacts
     NarrowArgs n;
     n.P = P; n.G = G; n.M = M; n.W = W; n.GW = GW; n.MW = MW; n.pgrid = pgrid; n.wgrid = wgrid;
     if (gh) n.gh = *gh; else memset(&n.gh, 0, sizeof(n.gh));
     n.L = L; n.a = a; n.with_force = with_force;
     const long long need = ((long long)L.cap_pairs + NARROW_WARPS - 1) / NARROW_WARPS;
     const int grid = (int)(need < 148 * 24 ? (need > 0 ? need : 1) : 148 * 24);
+    const int cgrid = 148 * 16;
     switch (kind) {
-    case FD_PP: k_narrow<FD_PP><<<grid, NARROW_WARPS * 32, 0, s>>>(n); break;
-    case FD_PW: k_narrow<FD_PW><<<grid, NARROW_WARPS * 32, 0, s>>>(n); break;
-    case FD_GX: k_narrow<FD_GX><<<grid, NARROW_WARPS * 32, 0, s>>>(n); break;
-    case FD_GY: k_narrow<FD_GY><<<grid, NARROW_WARPS * 32, 0, s>>>(n); break;
-    case FD_GXY: k_narrow<FD_GXY><<<grid, NARROW_WARPS * 32, 0, s>>>(n); break;
+    case FD_PP: k_select<FD_PP><<<grid, NARROW_WARPS * 32, 0, s>>>(n); k_contact<FD_PP><<<cgrid, TPB, 0, s>>>(n); break;
+    case FD_PW: k_select<FD_PW><<<grid, NARROW_WARPS * 32, 0, s>>>(n); k_contact<FD_PW><<<cgrid, TPB, 0, s>>>(n); break;
+    case FD_GX: k_select<FD_GX><<<grid, NARROW_WARPS * 32, 0, s>>>(n); k_contact<FD_GX><<<cgrid, TPB, 0, s>>>(n); break;
+    case FD_GY: k_select<FD_GY><<<grid, NARROW_WARPS * 32, 0, s>>>(n); k_contact<FD_GY><<<cgrid, TPB, 0, s>>>(n); break;
+    case FD_GXY: k_select<FD_GXY><<<grid, NARROW_WARPS * 32, 0, s>>>(n); k_contact<FD_GXY><<<cgrid, TPB, 0, s>>>(n); break;
     }
+    k_pair_sum<<<148 * 8, TPB, 0, s>>>(L, with_force);
 }
 
 void launch_reverse(const ObjDev& P, PairListDev& L, int* scan_tmp, size_t, cudaStream_t s)

@@ -23,19 +23,29 @@ struct PairListDev {
     int* o_seg_cnt;
     int* o_c_off;
     int* o_c_cnt;
-    // contacts of the current step
+    // contact slots of the current step: the nodes that passed the
+    // single-precision filter, contiguous per pair; c_node is the global
+    // boundary-node id of a contact and -1 for a slot that is none
     int* c_node;
     int* c_slave;
+    int* c_pair;       // pair of each slot
+    int* c_k;          // node key of each slot: cluster-order index relative to
+                       // the geometry (ascending within a pair)
+    double* c_force;   // 9 per slot: F, torque on A, torque on B (contacts only)
+    int4* p_aux;       // per pair: cell of B (x, y, z), first history slot
+    int* p_hist_cnt;   // per pair: history slots
     double* c_spring;  // 3 per contact
     double* c_point;   // 3 per contact (records)
     double* c_normal;  // 3 per contact (records)
     double* c_overlap; // records
     double* c_en;      // records
     double* c_es;      // records
-    int* n_contacts;   // device counter
-    int cap_contacts;
+    int* n_slots;      // device counter: slots used
+    int* n_hits;       // device counter: contacts (n_slots + 1)
+    int cap_contacts;  // slot capacity
     // previous contacts
     int* o_c_node;
+    int* o_c_k;
     double* o_c_spring;
     // reverse index (pairs grouped by partner B)
     int* rev_cnt;

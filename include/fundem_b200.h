@@ -88,14 +88,17 @@ int fundem_detect(fundem_sim* sim);
    bonds.  No counterpart in the reference. */
 int fundem_detect_proximity(fundem_sim* sim, double gap);
 /* nsteps iterations of the loop body of LSSolver::compute* (LSSolver.h:1097-1107):
-   kick, drift, detection, forces, bonds, kick.  No host synchronisation. */
+   kick, drift, detection, forces, bonds, kick.  The host waits for the
+   stream once every 64 steps, to grow the contact lists ahead of their
+   counts; the reference synchronises every step. */
 int fundem_step(fundem_sim* sim, int nsteps, const double gravity[3], double dt);
 /* one step split at the addExternalForceTorque hook (LSSolver.h:588): after
    step_begin the force/torque arrays hold the step's contact and bond sums;
    the caller may add to them (stream-ordered) before step_end. */
 int fundem_step_begin(fundem_sim* sim, const double gravity[3], double dt);
 int fundem_step_end(fundem_sim* sim, const double gravity[3], double dt);
-/* wait for the stream; returns the accumulated device error status */
+/* wait for the stream and grow the contact lists ahead of their counts;
+   returns the accumulated device error status */
 int fundem_sync(fundem_sim* sim);
 /* record one status word per step into a host ring without stalling */
 int fundem_status_word(fundem_sim* sim, unsigned int* flags);
@@ -161,6 +164,11 @@ int fundem_prefix_sum(int* d_prefix, const int* d_count, long long n, void* stre
    race. */
 #define FUNDEM_NOALLOC_SCAN_MAX 16777216LL
 int fundem_prefix_sum_noalloc(int* d_prefix, const int* d_count, long long n, void* stream);
+
+/* text of the last error a call on this simulation returned (empty when
+   none); valid until the next call on it.  The reference prints such
+   messages to std::cerr instead. */
+const char* fundem_last_error(fundem_sim* sim);
 
 /* kernel launches issued by this simulation so far */
 int fundem_launch_count(fundem_sim* sim, long long* n);
