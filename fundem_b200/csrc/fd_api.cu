@@ -227,6 +227,8 @@ struct GeoSetHost {
     DevArray<double3> d_nodes;
     DevArray<int> d_lid;
     DevArray<FdCluster> d_clusters;
+    DevArray<float4> d_nodes32, d_clus_sphere;
+    DevArray<int2> d_clus_range;
     std::vector<FdGeo> table;
     // node key (cluster-order index) of every node, by pool offset of the
     // geometry plus the node's original local index
@@ -341,6 +343,22 @@ struct GeoSetHost {
         d_lid.upload(lid.data(), lid.size(), s);
         d_clusters.alloc(std::max<size_t>(clusters.size(), 1));
         d_clusters.upload(clusters.data(), clusters.size(), s);
+        // single-precision copies for the culling stages
+        std::vector<float4> n32(nodes.size()), cs32(clusters.size());
+        std::vector<int2> cr(clusters.size());
+        for (size_t k = 0; k < nodes.size(); ++k)
+            n32[k] = make_float4((float)nodes[k].x, (float)nodes[k].y, (float)nodes[k].z, 0.f);
+        for (size_t k = 0; k < clusters.size(); ++k) {
+            const FdCluster& c = clusters[k];
+            cs32[k] = make_float4((float)c.centre.x, (float)c.centre.y, (float)c.centre.z, (float)c.radius);
+            cr[k] = make_int2(c.start, c.count);
+        }
+        d_nodes32.alloc(std::max<size_t>(n32.size(), 1));
+        d_nodes32.upload(n32.data(), n32.size(), s);
+        d_clus_sphere.alloc(std::max<size_t>(cs32.size(), 1));
+        d_clus_sphere.upload(cs32.data(), cs32.size(), s);
+        d_clus_range.alloc(std::max<size_t>(cr.size(), 1));
+        d_clus_range.upload(cr.data(), cr.size(), s);
         FD_CUDA(cudaStreamSynchronize(s));
         built = true;
     }
@@ -357,6 +375,9 @@ struct GeoSetHost {
         v.nodes = d_nodes.p;
         v.node_lid = d_lid.p;
         v.clusters = d_clusters.p;
+        v.nodes32 = d_nodes32.p;
+        v.clus_sphere = d_clus_sphere.p;
+        v.clus_range = d_clus_range.p;
         v.rmax = rmax;
         v.grid_rmax = grid_rmax;
         return v;
@@ -383,6 +404,7 @@ struct ObjHost {
     DevArray<double3> d_pos, d_vel, d_angvel, d_force, d_torque;
     DevArray<fd_quat> d_q;
     DevArray<int> d_mat, d_geo, d_node_base;
+    DevArray<float4> d_rot;
     DevArray<long long> d_hash;
     int n_dev = 0;
     bool dirty = true;
@@ -393,7 +415,7 @@ struct ObjHost {
         const size_t n = pos.size();
         const size_t m = std::max<size_t>(n, 1);
         d_pos.alloc(m); d_vel.alloc(m); d_angvel.alloc(m); d_force.alloc(m); d_torque.alloc(m);
-        d_q.alloc(m); d_mat.alloc(m); d_geo.alloc(m); d_hash.alloc(m); d_node_base.alloc(m);
+        d_q.alloc(m); d_mat.alloc(m); d_geo.alloc(m); d_hash.alloc(m); d_node_base.alloc(m); d_rot.alloc(3 * m);
         d_pos.upload(pos.data(), n, s); d_vel.upload(vel.data(), n, s); d_angvel.upload(angvel.data(), n, s);
         d_force.upload(force.data(), n, s); d_torque.upload(torque.data(), n, s); d_q.upload(q.data(), n, s);
         d_mat.upload(mat.data(), n, s); d_geo.upload(geo.data(), n, s);
@@ -407,6 +429,7 @@ struct ObjHost {
         v.n = n_dev;
         v.pos = d_pos.p; v.vel = d_vel.p; v.angvel = d_angvel.p; v.force = d_force.p; v.torque = d_torque.p;
         v.q = d_q.p; v.mat = d_mat.p; v.geo = d_geo.p; v.hash = d_hash.p; v.node_base = d_node_base.p;
+        v.rot = d_rot.p;
         return v;
     }
 };
@@ -507,9 +530,10 @@ struct CellTable {
 struct Ghost {
     DevArray<double3> pos;
     DevArray<long long> hash;
+    DevArray<int> occ;
     CellTable cells;
     bool active = false;
-    fd::GhostDev view() { return fd::GhostDev{pos.p, hash.p, cells.view()}; }
+    fd::GhostDev view() { return fd::GhostDev{pos.p, hash.p, cells.view(), occ.p}; }
 };
 
 struct BondHost {
@@ -717,6 +741,7 @@ struct fundem_sim {
             if (act[d]) {
                 ghosts[d].pos.alloc(std::max(np, 1));
                 ghosts[d].hash.alloc(std::max(np, 1));
+                ghosts[d].occ.alloc(6);
                 ghosts[d].cells.alloc(pgrid, np);
             }
         }

@@ -154,6 +154,14 @@ __global__ void k_drift(ObjDev O, double dt)
 // ---------------------------------------------------------------------------
 // hashing and the dense cell table (counting sort)
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ void quat_matrix(const fd_quat q, double R[9])
+{
+    const double q0 = q.q0, q1 = q.q1, q2 = q.q2, q3 = q.q3;
+    R[0] = 1.0 - 2.0 * (q2 * q2 + q3 * q3); R[1] = 2.0 * (q1 * q2 - q0 * q3); R[2] = 2.0 * (q1 * q3 + q0 * q2);
+    R[3] = 2.0 * (q1 * q2 + q0 * q3); R[4] = 1.0 - 2.0 * (q1 * q1 + q3 * q3); R[5] = 2.0 * (q2 * q3 - q0 * q1);
+    R[6] = 2.0 * (q1 * q3 - q0 * q2); R[7] = 2.0 * (q2 * q3 + q0 * q1); R[8] = 1.0 - 2.0 * (q1 * q1 + q2 * q2);
+}
+
 __global__ void k_hash_count(ObjDev O, FdGrid g, int* count)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -161,6 +169,13 @@ __global__ void k_hash_count(ObjDev O, FdGrid g, int* count)
     const long long h = fd_hash(O.pos[i], g);
     O.hash[i] = h;
     if (h >= 0 && h < g.num) atomicAdd(&count[h], 1);
+    if (O.rot) {
+        double R[9];
+        quat_matrix(O.q[i], R);
+        O.rot[3 * i + 0] = make_float4((float)R[0], (float)R[1], (float)R[2], 0.f);
+        O.rot[3 * i + 1] = make_float4((float)R[3], (float)R[4], (float)R[5], 0.f);
+        O.rot[3 * i + 2] = make_float4((float)R[6], (float)R[7], (float)R[8], 0.f);
+    }
 }
 
 __global__ void k_scatter(const long long* hash, int n, long long num, const int* start, int* fill, int* sorted)
@@ -222,7 +237,11 @@ __global__ void k_ghost_build(ObjDev P, GhostDev Gh, int kind)
     else if (r.z >= g.maxb.y) { gc.z = g.size.z - 1; out = true; }
     const long long h = out ? fd_lin3(gc.x, gc.y, gc.z, g.size) : -1;
     Gh.hash[i] = h;
-    if (h >= 0 && h < g.num) atomicAdd(&Gh.cells.count[h], 1);
+    if (h >= 0 && h < g.num) {
+        atomicAdd(&Gh.cells.count[h], 1);
+        atomicMin(&Gh.occ[0], gc.x); atomicMin(&Gh.occ[1], gc.y); atomicMin(&Gh.occ[2], gc.z);
+        atomicMax(&Gh.occ[3], gc.x); atomicMax(&Gh.occ[4], gc.y); atomicMax(&Gh.occ[5], gc.z);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -319,37 +338,133 @@ __device__ __forceinline__ bool body_culled(const double3 cA, double rA, const d
     return false;
 }
 
-__global__ void k_broad_pp(ObjDev P, GeoSetDev G, CellTableDev T, PairListDev L, unsigned int* flags, double probe)
+// cells that can hold the centre of a partner of a body of radius r centred
+// at c, when partners have radius at most rp: every partner centre within
+// r + rp of c lies in a cell overlapping [c - r - rp, c + r + rp]
+__device__ __forceinline__ void partner_search_range(double3 c, double reach, const FdGrid& g, int3& lo, int3& hi)
 {
-    const int A = blockIdx.x * blockDim.x + threadIdx.x;
-    if (A >= P.n) return;
-    const double3 cA = P.pos[A];
-    const double rA = G.geo[P.geo[A]].radius;
-    int3 lo, hi;
-    body_search_range(cA, rA * (1.0 + BOUND_REL), T.g, lo, hi);
-    int buf[MAX_CAND];
-    int cnt = 0, total = 0;
-    for (int z = lo.z; z <= hi.z; ++z)
-        for (int y = lo.y; y <= hi.y; ++y)
-            for (int x = lo.x; x <= hi.x; ++x) {
-                const long long h = fd_lin3(x, y, z, T.g.size);
-                const int c = T.count[h];
-                if (c == 0) continue;
-                const int s = T.start[h];
-                for (int k = s; k < s + c; ++k) {
-                    const int B = T.sorted[k];
-                    if (B <= A) continue;
-                    const double3 cB = P.pos[B];
-                    const double3 d = cA - cB;
+    lo.x = cell_index_clamped(c.x - reach, g.minb.x, g.inv.x, g.size.x);
+    lo.y = cell_index_clamped(c.y - reach, g.minb.y, g.inv.y, g.size.y);
+    lo.z = cell_index_clamped(c.z - reach, g.minb.z, g.inv.z, g.size.z);
+    hi.x = cell_index_clamped(c.x + reach, g.minb.x, g.inv.x, g.size.x);
+    hi.y = cell_index_clamped(c.y + reach, g.minb.y, g.inv.y, g.size.y);
+    hi.z = cell_index_clamped(c.z + reach, g.minb.z, g.inv.z, g.size.z);
+}
+
+#ifndef FD_BROAD_LANES
+#define FD_BROAD_LANES 8
+#endif
+constexpr int BROAD_LANES = FD_BROAD_LANES;  // lanes per particle in the cell-table broad phases
+constexpr int BROAD_CAND = 128;              // candidate slots staged per lane group and pass
+
+// Cell-table broad phase, BROAD_LANES lanes per particle A: the lanes read
+// the cells around A, share out the objects in them, test each (partner
+// order B > A for particle pairs, bounding spheres, body-level cull) and
+// emit A's pairs sorted by partner id.  GHOST: partners are the ghost images
+// of a cell table built from ghost positions (no B > A rule; the reach is the
+// partner's SDF grid radius, since ghost pairs have no radius test).
+template <bool GHOST>
+__global__ void __launch_bounds__(TPB) k_broad_cells(ObjDev P, GeoSetDev G, CellTableDev T, const double3* gpos,
+                                                     const int* occ, PairListDev L, unsigned int* flags,
+                                                     double probe)
+{
+    __shared__ int s_list[TPB / BROAD_LANES][MAX_CAND];
+    __shared__ int s_cand[TPB / BROAD_LANES][BROAD_CAND];
+    const unsigned int full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int gl = lane & (BROAD_LANES - 1);
+    const int gbase = lane & ~(BROAD_LANES - 1);
+    const int gb = threadIdx.x / BROAD_LANES;
+    const int A = (blockIdx.x * blockDim.x + threadIdx.x) / BROAD_LANES;
+    const bool valid = A < P.n;
+    double3 cA = mk3(0., 0., 0.);
+    double rA = 0.;
+    int3 lo = make_int3(0, 0, 0), hi = make_int3(-1, -1, -1);
+    if (valid) {
+        cA = P.pos[A];
+        rA = G.geo[P.geo[A]].radius;
+        // above the sphere test's own tolerance (rs * (1 + 2 BOUND_REL))
+        const double reach = (rA + (GHOST ? G.grid_rmax : G.rmax)) * (1.0 + 8.0 * BOUND_REL);
+        partner_search_range(cA, reach, T.g, lo, hi);
+        if (occ) {
+            // only the cells that hold ghost images
+            lo.x = max(lo.x, occ[0]); lo.y = max(lo.y, occ[1]); lo.z = max(lo.z, occ[2]);
+            hi.x = min(hi.x, occ[3]); hi.y = min(hi.y, occ[4]); hi.z = min(hi.z, occ[5]);
+        }
+    }
+    const int nx = max(hi.x - lo.x + 1, 0), ny = max(hi.y - lo.y + 1, 0), nz = max(hi.z - lo.z + 1, 0);
+    const int ncell = nx * ny * nz;
+    const int ncell_max = __reduce_max_sync(full, ncell);
+    int cnt = 0;  // partners that passed (uniform over the lane group)
+    for (int c0 = 0; c0 < ncell_max; c0 += BROAD_LANES) {
+        int cc = 0, cs = 0;
+        const int ci = c0 + gl;
+        if (ci < ncell) {
+            const int x = lo.x + ci % nx, y = lo.y + (ci / nx) % ny, z = lo.z + ci / (nx * ny);
+            const long long h = fd_lin3(x, y, z, T.g.size);
+            cc = T.count[h];
+            if (cc) cs = T.start[h];
+        }
+        // exclusive scan of the cell counts over the lane group
+        int incl = cc;
+#pragma unroll
+        for (int d = 1; d < BROAD_LANES; d <<= 1) {
+            const int y = __shfl_up_sync(full, incl, d, BROAD_LANES);
+            if (gl >= d) incl += y;
+        }
+        const int ex = incl - cc;
+        const int tot = __shfl_sync(full, incl, BROAD_LANES - 1, BROAD_LANES);
+        const int tot_max = __reduce_max_sync(full, tot);
+        for (int f0 = 0; f0 < tot_max; f0 += BROAD_LANES) {
+            // stage the table slots of the next BROAD_CAND candidates
+            if (f0 % BROAD_CAND == 0) {
+                __syncwarp();
+                for (int t = max(ex, f0); t < min(ex + cc, f0 + BROAD_CAND); ++t) s_cand[gb][t - f0] = cs + (t - ex);
+                __syncwarp();
+            }
+            const int f = f0 + gl;
+            bool pass = false;
+            int B = -1;
+            if (valid && f < tot) {
+                B = T.sorted[s_cand[gb][f % BROAD_CAND]];
+                if (GHOST || B > A) {
                     const FdGeo& GB = G.geo[P.geo[B]];
-                    const double rs = rA + GB.radius;
-                    if (lengthSq3(d) > rs * rs * (1.0 + 4.0 * BOUND_REL)) continue;
-                    if (body_culled(cA, rA, cB, P.q[B], GB, G, probe)) continue;
-                    if (cnt < MAX_CAND) buf[cnt++] = B;
-                    ++total;
+                    const double3 cB = GHOST ? gpos[B] : P.pos[B];
+                    const double rs = rA + (GHOST ? GB.grid_radius : GB.radius);
+                    if (lengthSq3(cA - cB) <= rs * rs * (1.0 + 4.0 * BOUND_REL))
+                        pass = !body_culled(cA, rA, cB, P.q[B], GB, G, probe);
                 }
             }
-    emit_pairs(A, buf, cnt, total, L, flags);
+            const unsigned int gm = (__ballot_sync(full, pass) >> gbase) & ((1u << BROAD_LANES) - 1u);
+            if (pass) {
+                const int pos = cnt + __popc(gm & ((1u << gl) - 1u));
+                if (pos < MAX_CAND) s_list[gb][pos] = B;
+            }
+            cnt += __popc(gm);
+        }
+    }
+    __syncwarp();
+    if (valid && cnt > MAX_CAND && gl == 0) set_flag(flags, FD_FLAG_NEIGHBOR_OVERFLOW);
+    const int n = min(cnt, MAX_CAND);
+    int base = 0;
+    if (valid && gl == 0 && n > 0) base = atomicAdd(L.n_pairs, n);
+    base = __shfl_sync(full, base, 0, BROAD_LANES);
+    const bool ok = base + n <= L.cap_pairs;
+    if (valid && n > 0 && !ok && gl == 0) set_flag(flags, FD_FLAG_PAIR_OVERFLOW);
+    if (valid && gl == 0) {
+        L.seg_off[A] = (ok && n > 0) ? base : 0;
+        L.seg_cnt[A] = ok ? n : 0;
+    }
+    // pairs of A in ascending partner order (partners are distinct)
+    if (valid && ok) {
+        for (int e = gl; e < n; e += BROAD_LANES) {
+            const int v = s_list[gb][e];
+            int r = 0;
+            for (int j = 0; j < n; ++j) r += (s_list[gb][j] < v);
+            L.pairA[base + r] = A;
+            L.pairB[base + r] = v;
+        }
+    }
 }
 
 __global__ void k_broad_pw(ObjDev P, GeoSetDev G, ObjDev W, GeoSetDev GW, FdGrid wg, PairListDev L,
@@ -377,38 +492,6 @@ __global__ void k_broad_pw(ObjDev P, GeoSetDev G, ObjDev W, GeoSetDev GW, FdGrid
         if (cnt < MAX_CAND) buf[cnt++] = w;
         ++total;
     }
-    emit_pairs(A, buf, cnt, total, L, flags);
-}
-
-__global__ void k_broad_ghost(ObjDev P, GeoSetDev G, GhostDev Gh, PairListDev L, unsigned int* flags, double probe)
-{
-    const int A = blockIdx.x * blockDim.x + threadIdx.x;
-    if (A >= P.n) return;
-    const double3 cA = P.pos[A];
-    const double rA = G.geo[P.geo[A]].radius;
-    const CellTableDev& T = Gh.cells;
-    int3 lo, hi;
-    body_search_range(cA, rA * (1.0 + BOUND_REL), T.g, lo, hi);
-    int buf[MAX_CAND];
-    int cnt = 0, total = 0;
-    for (int z = lo.z; z <= hi.z; ++z)
-        for (int y = lo.y; y <= hi.y; ++y)
-            for (int x = lo.x; x <= hi.x; ++x) {
-                const long long h = fd_lin3(x, y, z, T.g.size);
-                const int c = T.count[h];
-                if (c == 0) continue;
-                const int s = T.start[h];
-                for (int k = s; k < s + c; ++k) {
-                    const int j = T.sorted[k];
-                    const FdGeo& GB = G.geo[P.geo[j]];
-                    const double rs = rA + GB.grid_radius;
-                    const double3 cj = Gh.pos[j];
-                    if (lengthSq3(cA - cj) > rs * rs * (1.0 + 4.0 * BOUND_REL)) continue;
-                    if (body_culled(cA, rA, cj, P.q[j], GB, G, probe)) continue;
-                    if (cnt < MAX_CAND) buf[cnt++] = j;
-                    ++total;
-                }
-            }
     emit_pairs(A, buf, cnt, total, L, flags);
 }
 
@@ -477,6 +560,7 @@ template <int KIND> struct Slave;
 template <> struct Slave<FD_PP> {
     __device__ static double3 pos(const NarrowArgs& n, int j) { return n.P.pos[j]; }
     __device__ static fd_quat q(const NarrowArgs& n, int j) { return n.P.q[j]; }
+    __device__ static const float4* rot(const NarrowArgs& n, int j) { return n.P.rot + 3ll * j; }
     __device__ static const FdGeo& geo(const NarrowArgs& n, int j) { return n.G.geo[n.P.geo[j]]; }
     __device__ static const GeoSetDev& set(const NarrowArgs& n) { return n.G; }
     __device__ static long long hash(const NarrowArgs& n, int j) { return n.P.hash[j]; }
@@ -486,6 +570,7 @@ template <> struct Slave<FD_PP> {
 template <> struct Slave<FD_PW> {
     __device__ static double3 pos(const NarrowArgs& n, int j) { return n.W.pos[j]; }
     __device__ static fd_quat q(const NarrowArgs& n, int j) { return n.W.q[j]; }
+    __device__ static const float4* rot(const NarrowArgs& n, int j) { return n.W.rot + 3ll * j; }
     __device__ static const FdGeo& geo(const NarrowArgs& n, int j) { return n.GW.geo[n.W.geo[j]]; }
     __device__ static const GeoSetDev& set(const NarrowArgs& n) { return n.GW; }
     __device__ static long long hash(const NarrowArgs& n, int j) { return n.W.hash[j]; }
@@ -495,6 +580,7 @@ template <> struct Slave<FD_PW> {
 struct SlaveGhost {
     __device__ static double3 pos(const NarrowArgs& n, int j) { return n.gh.pos[j]; }
     __device__ static fd_quat q(const NarrowArgs& n, int j) { return n.P.q[j]; }
+    __device__ static const float4* rot(const NarrowArgs& n, int j) { return n.P.rot + 3ll * j; }
     __device__ static const FdGeo& geo(const NarrowArgs& n, int j) { return n.G.geo[n.P.geo[j]]; }
     __device__ static const GeoSetDev& set(const NarrowArgs& n) { return n.G; }
     __device__ static long long hash(const NarrowArgs& n, int j) { return n.gh.hash[j]; }
@@ -553,28 +639,28 @@ struct CullXf {
     float t[3];
 };
 
-__device__ __forceinline__ void quat_matrix(const fd_quat q, double R[9])
+// from the single-precision rotation rows of A and B; the product's
+// relative error (a few 1e-7) is far below the cull margins
+__device__ __forceinline__ CullXf cull_transform(const float4* RA, const float4* RB, const double3 cA,
+                                                 const double3 cB)
 {
-    const double q0 = q.q0, q1 = q.q1, q2 = q.q2, q3 = q.q3;
-    R[0] = 1.0 - 2.0 * (q2 * q2 + q3 * q3); R[1] = 2.0 * (q1 * q2 - q0 * q3); R[2] = 2.0 * (q1 * q3 + q0 * q2);
-    R[3] = 2.0 * (q1 * q2 + q0 * q3); R[4] = 1.0 - 2.0 * (q1 * q1 + q3 * q3); R[5] = 2.0 * (q2 * q3 - q0 * q1);
-    R[6] = 2.0 * (q1 * q3 - q0 * q2); R[7] = 2.0 * (q2 * q3 + q0 * q1); R[8] = 1.0 - 2.0 * (q1 * q1 + q2 * q2);
-}
-
-__device__ __forceinline__ CullXf cull_transform(const fd_quat qA, const double3 cA, const fd_quat qB, const double3 cB)
-{
-    double RA[9], RB[9];
-    quat_matrix(qA, RA);
-    quat_matrix(qB, RB);
+    const float4 a0 = RA[0], a1 = RA[1], a2 = RA[2];
+    const float4 b0 = RB[0], b1 = RB[1], b2 = RB[2];
     CullXf x;
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-            x.m[3 * i + j] = (float)(RB[i] * RA[j] + RB[3 + i] * RA[3 + j] + RB[6 + i] * RA[6 + j]);
-    const double3 d = cA - cB;
-#pragma unroll
-    for (int i = 0; i < 3; ++i) x.t[i] = (float)(RB[i] * d.x + RB[3 + i] * d.y + RB[6 + i] * d.z);
+    // M = RB^T RA
+    x.m[0] = fmaf(b0.x, a0.x, fmaf(b1.x, a1.x, b2.x * a2.x));
+    x.m[1] = fmaf(b0.x, a0.y, fmaf(b1.x, a1.y, b2.x * a2.y));
+    x.m[2] = fmaf(b0.x, a0.z, fmaf(b1.x, a1.z, b2.x * a2.z));
+    x.m[3] = fmaf(b0.y, a0.x, fmaf(b1.y, a1.x, b2.y * a2.x));
+    x.m[4] = fmaf(b0.y, a0.y, fmaf(b1.y, a1.y, b2.y * a2.y));
+    x.m[5] = fmaf(b0.y, a0.z, fmaf(b1.y, a1.z, b2.y * a2.z));
+    x.m[6] = fmaf(b0.z, a0.x, fmaf(b1.z, a1.x, b2.z * a2.x));
+    x.m[7] = fmaf(b0.z, a0.y, fmaf(b1.z, a1.y, b2.z * a2.y));
+    x.m[8] = fmaf(b0.z, a0.z, fmaf(b1.z, a1.z, b2.z * a2.z));
+    const float dx = (float)(cA.x - cB.x), dy = (float)(cA.y - cB.y), dz = (float)(cA.z - cB.z);
+    x.t[0] = fmaf(b0.x, dx, fmaf(b1.x, dy, b2.x * dz));
+    x.t[1] = fmaf(b0.y, dx, fmaf(b1.y, dy, b2.y * dz));
+    x.t[2] = fmaf(b0.z, dx, fmaf(b1.z, dy, b2.z * dz));
     return x;
 }
 
@@ -589,16 +675,16 @@ __device__ __forceinline__ CullXf cull_transform(const fd_quat qA, const double3
 //   * the Lipschitz bound of the trilinear SDF (coarse grids such as plane
 //     walls, where it is tight).
 template <int KIND>
-__device__ __forceinline__ bool cluster_culled(const FdCluster& cl, const CullXf& x, const FdGeo& GB,
+__device__ __forceinline__ bool cluster_culled(const float4 cl, const CullXf& x, const FdGeo& GB,
                                                const GeoSetDev& SB, double rB, double probe)
 {
-    const float cx = (float)cl.centre.x, cy = (float)cl.centre.y, cz = (float)cl.centre.z;
+    const float cx = cl.x, cy = cl.y, cz = cl.z;
     const float px = fmaf(x.m[0], cx, fmaf(x.m[1], cy, fmaf(x.m[2], cz, x.t[0])));
     const float py = fmaf(x.m[3], cx, fmaf(x.m[4], cy, fmaf(x.m[5], cz, x.t[1])));
     const float pz = fmaf(x.m[6], cx, fmaf(x.m[7], cy, fmaf(x.m[8], cz, x.t[2])));
-    const float scale = (float)(rB + cl.radius + GB.spacing);
+    const float scale = (float)rB + cl.w + (float)GB.spacing;
     const float margin = 2e-5f * scale;
-    const float rho = (float)cl.radius + margin;
+    const float rho = cl.w + margin;
     if (Slave<KIND>::radius_test) {
         const float lim = (float)rB + rho;
         if (px * px + py * py + pz * pz > lim * lim) return true;
@@ -648,10 +734,10 @@ __device__ __forceinline__ bool cluster_culled(const FdCluster& cl, const CullXf
 //     value is a convex combination of them).
 // Nodes that pass go to the exact double-precision predicate.
 template <int KIND>
-__device__ __forceinline__ bool node_filtered(const double3 p, const CullXf& x, const FdGeo& GB, const GeoSetDev& SB,
+__device__ __forceinline__ bool node_filtered(const float4 p, const CullXf& x, const FdGeo& GB, const GeoSetDev& SB,
                                               float rB, float perr, double probe)
 {
-    const float cx = (float)p.x, cy = (float)p.y, cz = (float)p.z;
+    const float cx = p.x, cy = p.y, cz = p.z;
     const float px = fmaf(x.m[0], cx, fmaf(x.m[1], cy, fmaf(x.m[2], cz, x.t[0])));
     const float py = fmaf(x.m[3], cx, fmaf(x.m[4], cy, fmaf(x.m[5], cz, x.t[1])));
     const float pz = fmaf(x.m[6], cx, fmaf(x.m[7], cy, fmaf(x.m[8], cz, x.t[2])));
@@ -686,7 +772,7 @@ __device__ __forceinline__ bool node_filtered(const double3 p, const CullXf& x, 
 }
 
 #ifndef FD_SELECT_MIN_BLOCKS
-#define FD_SELECT_MIN_BLOCKS 3
+#define FD_SELECT_MIN_BLOCKS 4
 #endif
 #ifndef FD_CONTACT_MIN_BLOCKS
 #define FD_CONTACT_MIN_BLOCKS 2
@@ -719,9 +805,7 @@ __global__ void __launch_bounds__(NARROW_WARPS * 32, FD_SELECT_MIN_BLOCKS) k_sel
         const int B = L.pairB[p];
         const FdGeo& GA = n.G.geo[n.P.geo[A]];
         const double3 cA = n.P.pos[A];
-        const fd_quat qA = n.P.q[A];
         const double3 cB = Slave<KIND>::pos(n, B);
-        const fd_quat qB = Slave<KIND>::q(n, B);
         const FdGeo& GB = Slave<KIND>::geo(n, B);
         const GeoSetDev& SB = Slave<KIND>::set(n);
         const double rB = GB.radius;
@@ -729,14 +813,11 @@ __global__ void __launch_bounds__(NARROW_WARPS * 32, FD_SELECT_MIN_BLOCKS) k_sel
         if (ncl > MAX_CLUSTERS) set_flag(n.a.flags, FD_FLAG_CLUSTER_OVERFLOW);
         // ---- cluster culling, one cluster per lane
         unsigned long long keep = 0ull;
-        const CullXf xf = cull_transform(qA, cA, qB, cB);
+        const CullXf xf = cull_transform(n.P.rot + 3ll * A, Slave<KIND>::rot(n, B), cA, cB);
         for (int c0 = 0; c0 < min(ncl, MAX_CLUSTERS); c0 += 32) {
             const int c = c0 + lane;
             bool k = false;
-            if (c < ncl) {
-                const FdCluster cl = n.G.clusters[GA.clus_off + c];
-                k = !cluster_culled<KIND>(cl, xf, GB, SB, rB, n.a.probe);
-            }
+            if (c < ncl) k = !cluster_culled<KIND>(n.G.clus_sphere[GA.clus_off + c], xf, GB, SB, rB, n.a.probe);
             keep |= ((unsigned long long)__ballot_sync(0xffffffffu, k)) << c0;
         }
         const int kept = __popcll(keep);
@@ -748,11 +829,11 @@ __global__ void __launch_bounds__(NARROW_WARPS * 32, FD_SELECT_MIN_BLOCKS) k_sel
         while (keep) {
             const int c = __ffsll((long long)keep) - 1;
             keep &= keep - 1ull;
-            const FdCluster cl = n.G.clusters[GA.clus_off + c];
-            const int k = cl.start + lane;
+            const int2 cr = n.G.clus_range[GA.clus_off + c];
+            const int k = cr.x + lane;
             bool cand = false;
-            if (lane < cl.count)
-                cand = !node_filtered<KIND>(n.G.nodes[GA.node_off + k], xf, GB, SB, (float)rB, perr, n.a.probe);
+            if (lane < cr.y)
+                cand = !node_filtered<KIND>(n.G.nodes32[GA.node_off + k], xf, GB, SB, (float)rB, perr, n.a.probe);
             const unsigned int m = __ballot_sync(0xffffffffu, cand);
             if (cand) s_node[wib][ncand + __popc(m & lt_mask)] = (unsigned short)k;
             ncand += __popc(m);
@@ -1228,13 +1309,18 @@ void launch_wrap(ObjDev& P, const FdGrid& g, int dim, cudaStream_t s)
 void launch_ghost_build(const ObjDev& P, GhostDev& Gh, int kind, cudaStream_t s)
 {
     cudaMemsetAsync(Gh.cells.count, 0, sizeof(int) * Gh.cells.g.num, s);
+    // occupied-cell box of the ghost images: empty until the build fills it
+    cudaMemsetAsync(Gh.occ, 0x7f, 3 * sizeof(int), s);
+    cudaMemsetAsync(Gh.occ + 3, 0xff, 3 * sizeof(int), s);
     if (P.n > 0) k_ghost_build<<<nblocks(P.n), TPB, 0, s>>>(P, Gh, kind);
 }
 void launch_broad_pp(const ObjDev& P, const GeoSetDev& G, const CellTableDev& T, PairListDev& L,
                      unsigned int* flags, double probe, cudaStream_t s)
 {
     cudaMemsetAsync(L.n_pairs, 0, sizeof(int), s);
-    if (P.n > 0) k_broad_pp<<<nblocks(P.n), TPB, 0, s>>>(P, G, T, L, flags, probe);
+    if (P.n > 0)
+        k_broad_cells<false><<<nblocks((long long)P.n * BROAD_LANES), TPB, 0, s>>>(P, G, T, nullptr, nullptr, L,
+                                                                                   flags, probe);
 }
 void launch_broad_pw(const ObjDev& P, const GeoSetDev& G, const ObjDev& W, const GeoSetDev& GW,
                      const FdGrid& wg, PairListDev& L, unsigned int* flags, double probe, cudaStream_t s)
@@ -1246,7 +1332,9 @@ void launch_broad_ghost(const ObjDev& P, const GeoSetDev& G, const GhostDev& Gh,
                         unsigned int* flags, double probe, cudaStream_t s)
 {
     cudaMemsetAsync(L.n_pairs, 0, sizeof(int), s);
-    if (P.n > 0) k_broad_ghost<<<nblocks(P.n), TPB, 0, s>>>(P, G, Gh, L, flags, probe);
+    if (P.n > 0)
+        k_broad_cells<true><<<nblocks((long long)P.n * BROAD_LANES), TPB, 0, s>>>(P, G, Gh.cells, Gh.pos, Gh.occ,
+                                                                                  L, flags, probe);
 }
 
 void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& M, const ObjDev& W,

@@ -66,6 +66,8 @@ struct ObjDev {
     int* geo;
     long long* hash;   // cell hash of the current step (-1 when not hashed)
     int* node_base;    // first global boundary node of each object
+    float4* rot;       // 3 per object: rows of the rotation matrix, single
+                       // precision, refreshed at every hashing (culling only)
 };
 
 struct GeoSetDev {
@@ -78,6 +80,9 @@ struct GeoSetDev {
     const double3* nodes;     // cluster order
     const int* node_lid;      // original local index of each node (cluster order)
     const FdCluster* clusters;
+    const float4* nodes32;      // cluster order, single precision (culling only)
+    const float4* clus_sphere;  // per cluster: centre, radius (single precision)
+    const int2* clus_range;     // per cluster: first node, node count
     double rmax;              // largest bounding radius over the set
     double grid_rmax;         // largest grid radius over the set
 };
@@ -101,6 +106,7 @@ struct GhostDev {
     double3* pos;
     long long* hash;
     CellTableDev cells;
+    int* occ;  // box of the cells holding ghost images: min x, y, z, max x, y, z
 };
 
 struct BondDev {
