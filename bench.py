@@ -5,12 +5,18 @@
 
 Workload (default): the scaled, periodic, bonded column -- 262,144
 superellipsoids from 8 templates (32^3 SDFs, 642 surface nodes), periodic in
-x and y, floor wall and a top platen moving at 1 m/s, V-model bonds between
-pairs whose surface gap is below 0.05 of the mean diameter, dt = 5e-7 s,
-FP64.  A step is one pass of the whole timestep (kicks, drift, hashing,
-broad phase, narrow phase + contact law, ghosts, bonds, reduction) over the
-resident state.  Inputs are larger than L2 (state + templates + lists are
-several hundred MB), so no L2 flush is needed between steps.
+x and y, floor wall and a top platen that starts on the bed and moves down
+at 1 m/s, V-model bonds between pairs whose surface gap is below 0.05 of the
+mean diameter, dt = 5e-7 s, FP64.  A step is one pass of the whole timestep
+(kicks, drift, hashing, broad phase, narrow phase + contact law, ghosts,
+bonds, reduction) over the resident state.  The default warm-up (1000 steps)
+puts the timed window in the compression phase.  Inputs are larger than L2
+(state + templates + lists are several hundred MB), so no L2 flush is needed
+between steps.
+
+The `mixed` object compares the mixed-precision mode with FP64 on the same
+workload: two fresh simulations run --error-steps steps, their positions are
+compared, then each runs K timed steps from there.
 
 --impl reference times the CPU restatement of the reference algorithm (the
 reference itself has no CPU code) on a bounded sample of the same workload,
@@ -232,6 +238,11 @@ def run_fundem(args, rank, world, dist):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_val = world * n * args.steps / float(t.item())
 
+    # mixed precision against FP64 on the same workload: two fresh simulations
+    # from the initial state, `error_steps` steps each, positions compared
+    # (minimum image across the periodic seams), then K timed steps each
+    mixed = None if args.no_mixed else mixed_vs_fp64(sc, dev, args, dist, world)
+
     if rank != 0:
         return
     pk, pk_kind = peaks()
@@ -268,6 +279,7 @@ def run_fundem(args, rank, world, dist):
         "narrow_work_per_step": {"pairs": wc[0] / wc_steps, "clusters": wc[1] / wc_steps,
                                  "clusters_kept": wc[2] / wc_steps, "node_contacts": wc[3] / wc_steps,
                                  "exact_node_tests": wc[4] / wc_steps},
+        "mixed": mixed,
         "cpu_baseline": cpu,
         "clocks": clk,
         "gpu_launches": launches,
@@ -275,11 +287,65 @@ def run_fundem(args, rank, world, dist):
     print(json.dumps(line), flush=True)
 
 
+def mixed_vs_fp64(sc, dev, args, dist, world):
+    import torch
+    import fundem_b200 as F
+    n = len(sc.particles)
+    sims = {}
+    for prec in (F.FP64, F.FP32_MIXED):
+        s = F.Simulation.from_scenario(sc, device=dev, precision=prec, records=False)
+        s.detect()
+        s.step(args.error_steps)
+        s.sync()
+        sims[prec] = s
+    a, b = sims[F.FP64].state(), sims[F.FP32_MIXED].state()
+    L = np.array([sc.domain_max[0] - sc.domain_min[0], sc.domain_max[1] - sc.domain_min[1]])
+    d = a["pos"] - b["pos"]
+    for k in range(2):
+        if (sc.periodic_x, sc.periodic_y)[k]:
+            d[:, k] -= L[k] * np.round(d[:, k] / L[k])
+    dx = np.linalg.norm(d, axis=1)
+    rel = dx / np.maximum(np.linalg.norm(a["pos"], axis=1), 1e-300)
+    norm_rel = float(np.linalg.norm(d) / np.linalg.norm(a["pos"]))
+    dq = 1.0 - np.abs(np.sum(a["quat"] * b["quat"], axis=1))
+    ms = {}
+    for prec, s in sims.items():
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0.record()
+        s.step(args.steps)
+        e1.record()
+        torch.cuda.synchronize()
+        s.sync()
+        t = e0.elapsed_time(e1)
+        if dist:
+            tt = torch.tensor([t], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t = float(tt.item())
+        ms[prec] = t / args.steps
+    for s in sims.values():
+        s.close()
+    gate = 1e-5
+    return {"value": world * n / (ms[F.FP32_MIXED] / 1e3), "unit": METRIC, "ms_per_step": ms[F.FP32_MIXED],
+            "fp64_ms_per_step_same_state": ms[F.FP64], "speedup_vs_fp64": ms[F.FP64] / ms[F.FP32_MIXED],
+            "dtype": "f32 contact and bond laws, f64 integration and spring history",
+            "timed_after_steps": args.error_steps,
+            "error_vs_fp64": {"steps": args.error_steps, "normwise_rel_position": norm_rel,
+                              "p99_rel_position": float(np.percentile(rel, 99)), "max_rel_position": float(rel.max()),
+                              "max_abs_position_m": float(dx.max()), "p99_abs_position_m": float(np.percentile(dx, 99)),
+                              "max_quaternion_error": float(dq.max()), "gate_rel_position": gate,
+                              "pass": bool(norm_rel <= gate and np.percentile(rel, 99) <= gate),
+                              "gate_metric": "||X_mixed - X_fp64|| / ||X_fp64|| and the 99th percentile of "
+                                             "|x_mixed - x_fp64| / |x_fp64| over particles"}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
-    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=1000)
     ap.add_argument("--impl", default="fundem", choices=["fundem", "reference"])
     ap.add_argument("--n", type=int, default=262144)
     ap.add_argument("--footprint", type=int, nargs=2, default=[128, 128])
@@ -289,6 +355,9 @@ def main():
     ap.add_argument("--profile", action="store_true",
                     help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision comparison")
+    ap.add_argument("--error-steps", type=int, default=1000,
+                    help="steps before the mixed-precision position error is measured")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))

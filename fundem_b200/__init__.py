@@ -267,6 +267,10 @@ class Simulation:
     def set_periodic(self, x, y):
         self._check(self.L.fundem_set_periodic(self.h, int(bool(x)), int(bool(y))), "set_periodic")
 
+    def set_precision(self, precision):
+        """FP64 (the reference's arithmetic) or FP32_MIXED; may change between steps."""
+        self._check(self.L.fundem_set_precision(self.h, int(precision)), "set_precision")
+
     def set_records(self, full):
         self._check(self.L.fundem_set_records(self.h, int(bool(full))), "set_records")
 

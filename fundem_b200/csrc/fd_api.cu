@@ -561,6 +561,7 @@ struct fundem_sim {
     int device = 0;
     cudaStream_t stream = nullptr;
     int precision = FUNDEM_FP64;
+    bool mixed() const { return precision == FUNDEM_FP32_MIXED; }
     int records = 1;
     MatHost pmat, wmat;
     GeoSetHost pgeo, wgeo;
@@ -780,14 +781,14 @@ struct fundem_sim {
         fd::launch_broad_pp(Pv, G, T, Lpp, flags.p, probe, stream);
         tend(FUNDEM_T_BROAD);
         tbegin(FUNDEM_T_NARROW_PP);
-        fd::launch_narrow(FD_PP, Pv, G, M, Wv, GW, MW, pgrid, wgrid, nullptr, Lpp, a, with_force, stream);
+        fd::launch_narrow(FD_PP, Pv, G, M, Wv, GW, MW, pgrid, wgrid, nullptr, Lpp, a, with_force, mixed(), stream);
         tend(FUNDEM_T_NARROW_PP);
         PairListDev Lpw = lists[FD_PW].view();
         tbegin(FUNDEM_T_BROAD);
         fd::launch_broad_pw(Pv, G, Wv, GW, wgrid, Lpw, flags.p, probe, stream);
         tend(FUNDEM_T_BROAD);
         tbegin(FUNDEM_T_NARROW_PW);
-        fd::launch_narrow(FD_PW, Pv, G, M, Wv, GW, MW, pgrid, wgrid, nullptr, Lpw, a, with_force, stream);
+        fd::launch_narrow(FD_PW, Pv, G, M, Wv, GW, MW, pgrid, wgrid, nullptr, Lpw, a, with_force, mixed(), stream);
         tend(FUNDEM_T_NARROW_PW);
         launches += 4;
         PairListDev Lg[3];
@@ -810,7 +811,7 @@ struct fundem_sim {
                 fd::GhostDev gh = ghosts[d].view();
                 Lg[d] = lists[kinds[d]].view();
                 fd::launch_broad_ghost(Pv, G, gh, Lg[d], flags.p, probe, stream);
-                fd::launch_narrow(kinds[d], Pv, G, M, Wv, GW, MW, pgrid, wgrid, &gh, Lg[d], a, with_force, stream);
+                fd::launch_narrow(kinds[d], Pv, G, M, Wv, GW, MW, pgrid, wgrid, &gh, Lg[d], a, with_force, mixed(), stream);
                 active[kinds[d]] = 1;
                 launches += 2;
             }
@@ -830,10 +831,10 @@ struct fundem_sim {
                 launches += 4;
             }
         fd::BondDev bd = bond_view();
-        if (bd.n > 0) { fd::launch_bonds(Pv, bd, stream); launches++; }
+        if (bd.n > 0) { fd::launch_bonds(Pv, bd, mixed(), stream); launches++; }
         PairListDev views[FD_NKIND];
         for (int k = 0; k < FD_NKIND; ++k) views[k] = lists[k].view();
-        fd::launch_reduce(Pv, views, active, bd, stream);
+        fd::launch_reduce(Pv, views, active, bd, mixed(), stream);
         launches++;
         tend(FUNDEM_T_REDUCE);
         FD_CUDA(cudaGetLastError());

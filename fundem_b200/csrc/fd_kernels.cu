@@ -1093,6 +1093,280 @@ __global__ void k_pair_sum(PairListDev L, int with_force)
 }
 
 // ---------------------------------------------------------------------------
+// Mixed precision (FUNDEM_FP32_MIXED).  The node predicate, the SDF
+// gradient, the contact law, the bond law and the force sums run in single
+// precision with single-precision accumulation; positions, orientations and
+// their integration, and the tangential-spring history, stay in double
+// precision.  Node positions are formed relative to the body centres, so the
+// single-precision quantities are millimetre-scale offsets, never absolute
+// coordinates.
+// ---------------------------------------------------------------------------
+struct v3f {
+    float x, y, z;
+};
+__device__ __forceinline__ v3f mkf(float x, float y, float z) { return v3f{x, y, z}; }
+__device__ __forceinline__ v3f tof(double3 a) { return v3f{(float)a.x, (float)a.y, (float)a.z}; }
+__device__ __forceinline__ double3 tod(v3f a) { return mk3((double)a.x, (double)a.y, (double)a.z); }
+__device__ __forceinline__ v3f operator+(v3f a, v3f b) { return v3f{a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ v3f operator-(v3f a, v3f b) { return v3f{a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ v3f operator-(v3f a) { return v3f{-a.x, -a.y, -a.z}; }
+__device__ __forceinline__ v3f operator*(float s, v3f a) { return v3f{s * a.x, s * a.y, s * a.z}; }
+__device__ __forceinline__ float dotf(v3f a, v3f b) { return fmaf(a.x, b.x, fmaf(a.y, b.y, a.z * b.z)); }
+__device__ __forceinline__ float lenf(v3f a) { return sqrtf(dotf(a, a)); }
+__device__ __forceinline__ v3f crossf(v3f a, v3f b)
+{
+    return v3f{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+// R v and R^T v from the rotation rows
+__device__ __forceinline__ v3f rowsf(float4 r0, float4 r1, float4 r2, v3f v)
+{
+    return v3f{fmaf(r0.x, v.x, fmaf(r0.y, v.y, r0.z * v.z)), fmaf(r1.x, v.x, fmaf(r1.y, v.y, r1.z * v.z)),
+               fmaf(r2.x, v.x, fmaf(r2.y, v.y, r2.z * v.z))};
+}
+__device__ __forceinline__ v3f colsf(float4 r0, float4 r1, float4 r2, v3f v)
+{
+    return v3f{fmaf(r0.x, v.x, fmaf(r1.x, v.y, r2.x * v.z)), fmaf(r0.y, v.x, fmaf(r1.y, v.y, r2.y * v.z)),
+               fmaf(r0.z, v.x, fmaf(r1.z, v.y, r2.z * v.z))};
+}
+constexpr float PI_F = 3.14159265358979f;
+
+// the linear contact law (contactKernel.cuh:4-77) in single precision, with
+// the spring history accumulated in double precision
+__device__ __forceinline__ v3f linear_contact32(double3& spring, v3f vc, v3f n, float delta, float dt, float kn,
+                                                float ks, float mu, float res, float m)
+{
+    if (!(delta > 0.f)) {
+        spring = mk3(0., 0., 0.);
+        return mkf(0.f, 0.f, 0.f);
+    }
+    const float lr = logf(res);
+    const float diss = -lr / sqrtf(lr * lr + PI_F * PI_F);
+    const float cn = 2.f * diss * sqrtf(m * kn);
+    const v3f vn = dotf(vc, n) * n;
+    const v3f fn = (kn * delta) * n - cn * vn;
+    const float cs = 2.f * diss * sqrtf(m * ks);
+    const v3f vs = vc - vn;
+    if (mu > 0.f && ks > 0.f) {
+        // the history itself is kept in double precision: projection onto
+        // the tangent plane, accumulation and the Coulomb rescaling
+        const double3 nd = tod(n), vsd = tod(vs);
+        double3 p1 = spring - dot3(spring, nd) * nd;
+        const double ap1 = length3(p1);
+        if (!fd_is_zero(ap1)) p1 = p1 * (length3(spring) / ap1);
+        spring = p1 + (double)dt * vsd;
+        const v3f sf = -ks * tof(spring) - cs * vs;
+        const float asf = lenf(sf), afn = lenf(fn);
+        if (asf > 1e-20f && asf > mu * afn) {
+            const double scale = (double)(mu * afn) / (double)asf;
+            const double3 sfd = -(double)ks * spring - (double)cs * vsd;
+            spring = (-1.0 / (double)ks) * (scale * sfd + (double)cs * vsd);
+        }
+    } else {
+        spring = mk3(0., 0., 0.);
+    }
+    return fn + (-ks * tof(spring) - cs * vs);
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(TPB, FD_CONTACT_MIN_BLOCKS) k_contact32(NarrowArgs n)
+{
+    __shared__ int s_hits;
+    if (threadIdx.x == 0) s_hits = 0;
+    __syncthreads();
+    PairListDev& L = n.L;
+    float* cf = reinterpret_cast<float*>(L.c_force);
+    const int nslots = min(*L.n_slots, L.cap_contacts);
+    const int lane = threadIdx.x & 31;
+    const bool periodic = (KIND == FD_PP || KIND == FD_PW) && (n.a.periodic_x || n.a.periodic_y);
+    const int stride = gridDim.x * blockDim.x;
+    int hits = 0;
+    for (int s0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); s0 < nslots; s0 += stride) {
+        const int s = s0 + lane;
+        bool hit = false;
+        if (s < nslots) {
+            const int p = L.c_pair[s];
+            const int k = L.c_k[s];
+            const int A = L.pairA[p];
+            const int B = L.pairB[p];
+            const int4 aux = L.p_aux[p];
+            const FdGeo& GA = n.G.geo[n.P.geo[A]];
+            const double3 cA = n.P.pos[A];
+            const double3 cB = Slave<KIND>::pos(n, B);
+            const FdGeo& GB = Slave<KIND>::geo(n, B);
+            const GeoSetDev& SB = Slave<KIND>::set(n);
+            const FdGrid& sg = Slave<KIND>::grid(n);
+            const float4* RB = Slave<KIND>::rot(n, B);
+            const float4 b0 = RB[0], b1 = RB[1], b2 = RB[2];
+            // the rigid transforms in double precision (as in FP64 mode), the
+            // position inside the cell and the SDF interpolation in single
+            const int pool = GA.node_off + k;
+            const double3 rd = xm_rot(n.P.q[A], n.G.nodes[pool]);
+            const double3 gp = mk3(rd.x + cA.x, rd.y + cA.y, rd.z + cA.z);
+            const v3f r = tof(rd);  // node offset from A's centre
+            int3 lo, hi;
+            fd_node_range(gp, sg, lo, hi);
+            float ov = 0.f, fx = 0.f, fy = 0.f, fz = 0.f, pv[8];
+            if (aux.x >= lo.x && aux.x <= hi.x && aux.y >= lo.y && aux.y <= hi.y && aux.z >= lo.z && aux.z <= hi.z) {
+                const double3 rel = mk3(gp.x - cB.x, gp.y - cB.y, gp.z - cB.z);
+                if (!Slave<KIND>::radius_test || xm_len2(rel) <= GB.radius * GB.radius) {
+                    const double3 lp = xm_rrot(rel, Slave<KIND>::q(n, B));
+                    const double gx = (lp.x - GB.origin.x) * GB.inv_spacing;
+                    const double gy = (lp.y - GB.origin.y) * GB.inv_spacing;
+                    const double gz = (lp.z - GB.origin.z) * GB.inv_spacing;
+                    const int i0 = (int)floor(gx), j0 = (int)floor(gy), k0 = (int)floor(gz);
+                    if (i0 >= 0 && j0 >= 0 && k0 >= 0 && i0 < GB.size.x - 1 && j0 < GB.size.y - 1 &&
+                        k0 < GB.size.z - 1) {
+                        fx = (float)(gx - (double)i0);
+                        fy = (float)(gy - (double)j0);
+                        fz = (float)(gz - (double)k0);
+                        const long long sx = GB.size.x, sxy = (long long)GB.size.x * GB.size.y;
+                        const float* S = SB.sdf32 + GB.sdf_off + (long long)k0 * sxy + (long long)j0 * sx + i0;
+                        pv[0] = __ldg(S); pv[1] = __ldg(S + 1); pv[2] = __ldg(S + sx); pv[3] = __ldg(S + sx + 1);
+                        pv[4] = __ldg(S + sxy); pv[5] = __ldg(S + sxy + 1); pv[6] = __ldg(S + sxy + sx);
+                        pv[7] = __ldg(S + sxy + sx + 1);
+                        const float c00 = pv[0] * (1.f - fx) + pv[1] * fx, c10 = pv[2] * (1.f - fx) + pv[3] * fx;
+                        const float c01 = pv[4] * (1.f - fx) + pv[5] * fx, c11 = pv[6] * (1.f - fx) + pv[7] * fx;
+                        ov = -((c00 * (1.f - fy) + c10 * fy) * (1.f - fz) + (c01 * (1.f - fy) + c11 * fy) * fz);
+                        hit = ov >= -(float)n.a.probe;
+                    }
+                }
+            }
+            int nid = -1;
+            if (hit) {
+                // gradient with the x weight truncated as the reference does
+                // (LSParticleContactDetectionKernel.cuh:34)
+                const float wy0 = 1.f - fy, wy1 = fy, wz0 = 1.f - fz, wz1 = fz;
+                const v3f gB = mkf((pv[1] - pv[0]) * wy0 * wz0 + (pv[3] - pv[2]) * wy1 * wz0 +
+                                       (pv[5] - pv[4]) * wy0 * wz1 + (pv[7] - pv[6]) * wy1 * wz1,
+                                   (pv[2] - pv[0]) * wz0 + (pv[6] - pv[4]) * wz1,
+                                   (pv[4] - pv[0]) * wy0 + (pv[6] - pv[2]) * wy1);
+                v3f nrm = rowsf(b0, b1, b2, gB);
+                const float l2 = dotf(nrm, nrm);
+                nrm = l2 > 1e-20f ? rsqrtf(l2) * nrm : mkf(0.f, 0.f, 0.f);
+                const v3f arm = r + (0.5f * ov) * nrm;  // contact point relative to A's centre
+                nid = n.P.node_base[A] + n.G.node_lid[pool];
+                double3 spring = mk3(0., 0., 0.);
+                {
+                    const int oc_off = aux.w, oc_end = aux.w + L.p_hist_cnt[p];
+                    int lo2 = oc_off, hi2 = oc_end;
+                    while (lo2 < hi2) {
+                        const int mid = (lo2 + hi2) >> 1;
+                        if (L.o_c_k[mid] < k) lo2 = mid + 1; else hi2 = mid;
+                    }
+                    if (lo2 < oc_end && L.o_c_k[lo2] == k && L.o_c_node[lo2] == nid) {
+                        const double* sp = L.o_c_spring + 3ll * lo2;
+                        spring = mk3(sp[0], sp[1], sp[2]);
+                    }
+                }
+                const int mi = n.P.mat[A];
+                float kn = 0.f, ks = 0.f;
+                float mu, res, effM = 0.f;
+                const double kni = n.M.kn[mi], ksi = n.M.ks[mi];
+                const double invMi = GA.inv_mass;
+                if (KIND == FD_PW) {
+                    const int mj = n.W.mat[B];
+                    mu = (float)fmin(n.M.mu[mi], n.MW.mu[mj]);
+                    res = (float)fmin(n.M.e[mi], n.MW.e[mj]);
+                    if (invMi > 0.) effM = (float)(1. / invMi);
+                    kn = (float)kni;
+                    ks = (float)ksi;
+                } else {
+                    const int mj = n.P.mat[B];
+                    const double knj = n.M.kn[mj], ksj = n.M.ks[mj], invMj = GB.inv_mass;
+                    if (kni > 0. && knj > 0.) kn = (float)(kni * knj / (kni + knj));
+                    if (ksi > 0. && ksj > 0.) ks = (float)(ksi * ksj / (ksi + ksj));
+                    if (invMi > 0. || invMj > 0.) effM = (float)(1. / (invMi + invMj));
+                    res = (float)fmin(n.M.e[mi], n.M.e[mj]);
+                    mu = (float)fmin(n.M.mu[mi], n.M.mu[mj]);
+                }
+                if (n.with_force) {
+                    double3 ri = cA, rj = cB;
+                    if (periodic) {
+                        if (n.a.periodic_x) { ri = wrap_x(ri, n.pgrid); if (KIND == FD_PP) rj = wrap_x(rj, n.pgrid); }
+                        if (n.a.periodic_y) { ri = wrap_y(ri, n.pgrid); if (KIND == FD_PP) rj = wrap_y(rj, n.pgrid); }
+                    }
+                    const v3f armA = tof(cA - ri) + arm;
+                    const v3f armB = tof(cA - rj) + arm;
+                    const v3f vi = tof(n.P.vel[A]), wi = tof(n.P.angvel[A]);
+                    const v3f vj = tof(KIND == FD_PW ? n.W.vel[B] : n.P.vel[B]);
+                    const v3f wj = tof(KIND == FD_PW ? n.W.angvel[B] : n.P.angvel[B]);
+                    const v3f vc = (vi + crossf(wi, armA)) - (vj + crossf(wj, armB));
+                    const v3f F = linear_contact32(spring, vc, nrm, ov, (float)n.a.dt, kn, ks, mu, res, effM);
+                    const v3f TA = crossf(armA, F);
+                    const v3f TB = crossf(armB, -F);
+                    float* o = cf + 9ll * s;
+                    o[0] = F.x; o[1] = F.y; o[2] = F.z;
+                    o[3] = TA.x; o[4] = TA.y; o[5] = TA.z;
+                    o[6] = TB.x; o[7] = TB.y; o[8] = TB.z;
+                }
+                L.c_slave[s] = B;
+                L.c_spring[3 * s + 0] = spring.x;
+                L.c_spring[3 * s + 1] = spring.y;
+                L.c_spring[3 * s + 2] = spring.z;
+                if (n.a.records) {
+                    L.c_point[3 * s + 0] = cA.x + arm.x;
+                    L.c_point[3 * s + 1] = cA.y + arm.y;
+                    L.c_point[3 * s + 2] = cA.z + arm.z;
+                    L.c_normal[3 * s + 0] = nrm.x;
+                    L.c_normal[3 * s + 1] = nrm.y;
+                    L.c_normal[3 * s + 2] = nrm.z;
+                    L.c_overlap[s] = ov;
+                    L.c_en[s] = 0.5 * (double)ov * (double)ov * (double)kn;
+                    L.c_es[s] = 0.5 * lengthSq3(spring) * (double)ks;
+                }
+            }
+            L.c_node[s] = nid;
+        }
+        hits += __popc(__ballot_sync(0xffffffffu, hit));
+    }
+    if (lane == 0 && hits) atomicAdd(&s_hits, hits);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_hits) {
+        atomicAdd(L.n_hits, s_hits);
+        if (n.a.stats) atomicAdd(&n.a.stats[3], (unsigned long long)s_hits);
+    }
+}
+
+// stage 3 in single precision: eight lanes per pair, as k_pair_sum
+__global__ void k_pair_sum32(PairListDev L, int with_force)
+{
+    const float* cf = reinterpret_cast<const float*>(L.c_force);
+    float* pf = reinterpret_cast<float*>(L.pf);
+    const int npairs = min(*L.n_pairs, L.cap_pairs);
+    const int lane = threadIdx.x & 31, grp = lane >> 3, l = lane & 7;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int p0 = warp * 4; p0 < npairs; p0 += nwarps * 4) {
+        const int p = p0 + grp;
+        float acc[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        int o = 0, c = 0;
+        if (p < npairs && with_force) {
+            o = L.c_off[p];
+            c = L.c_cnt[p];
+        }
+        for (int j = l; j < c; j += 8) {
+            if (L.c_node[o + j] < 0) continue;
+            const float* f = cf + 9ll * (o + j);
+#pragma unroll
+            for (int t = 0; t < 9; ++t) acc[t] += f[t];
+        }
+#pragma unroll
+        for (int t = 0; t < 9; ++t) {
+            acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], 4);
+            acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], 2);
+            acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], 1);
+        }
+        if (p < npairs) {
+            float* out = pf + 9ll * p;
+#pragma unroll
+            for (int t = 0; t < 8; ++t)
+                if (l == t) out[t] = acc[t];
+            if (l == 0) out[8] = acc[8];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // reverse index: pairs grouped by partner B, sorted by A
 // ---------------------------------------------------------------------------
 __global__ void k_rev_count(PairListDev L, int n_obj)
@@ -1190,6 +1464,71 @@ __global__ void k_bonds(ObjDev P, BondDev Bd)
     O[6] = Tj.x; O[7] = Tj.y; O[8] = Tj.z;
 }
 
+// the V-bond (contactKernel.cuh:138-199) in single precision; the frames are
+// rotated with the single-precision rotation rows, the bond vector is formed
+// from the double-precision centre difference plus the rotated offsets
+__global__ void k_bonds32(ObjDev P, BondDev Bd)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= Bd.n) return;
+    double* E = Bd.energy + 6ll * k;
+    float* O = reinterpret_cast<float*>(Bd.out) + 9ll * k;
+    for (int t = 0; t < 9; ++t) O[t] = 0.f;
+    if (Bd.active[k] == 0) {
+        for (int t = 0; t < 6; ++t) E[t] = 0.;
+        return;
+    }
+    const int i = Bd.master[k], j = Bd.slave[k];
+    const float4 a0 = P.rot[3ll * i], a1 = P.rot[3ll * i + 1], a2 = P.rot[3ll * i + 2];
+    const float4 b0 = P.rot[3ll * j], b1 = P.rot[3ll * j + 1], b2 = P.rot[3ll * j + 2];
+    const double3* f = Bd.frames + 8ll * k;
+    const v3f n1i = rowsf(a0, a1, a2, tof(f[0])), n2i = rowsf(a0, a1, a2, tof(f[1])), n3i = rowsf(a0, a1, a2, tof(f[2]));
+    const v3f n1j = rowsf(b0, b1, b2, tof(f[4])), n2j = rowsf(b0, b1, b2, tof(f[5])), n3j = rowsf(b0, b1, b2, tof(f[6]));
+    const double3 ri = P.pos[i], rj = P.pos[j];
+    const v3f oi = rowsf(a0, a1, a2, tof(f[3])), oj = rowsf(b0, b1, b2, tof(f[7]));
+    Bd.point[k] = 0.5 * (ri + rj) + 0.5 * tod(oi + oj);
+    v3f F = mkf(0.f, 0.f, 0.f), Mij = mkf(0.f, 0.f, 0.f), Mji = mkf(0.f, 0.f, 0.f);
+    int act = 1;
+    const v3f rij = tof(ri - rj) + (oi - oj);
+    const float D = lenf(rij);
+    if (D > 1e-20f) {
+        const float B1 = (float)Bd.B[4 * k], B2 = (float)Bd.B[4 * k + 1], B3 = (float)Bd.B[4 * k + 2],
+                    B4 = (float)Bd.B[4 * k + 3];
+        const float R = (float)Bd.radius[k], D0 = (float)Bd.L0[k];
+        const v3f nij = rsqrtf(dotf(rij, rij)) * rij;
+        const v3f e = -nij;
+        const float c11 = dotf(n1i, n1j);
+        E[0] = 0.5 * (double)B1 * (double)(D - D0) * (double)(D - D0);
+        E[1] = (double)(B2 * (0.5f * dotf(n1j - n1i, e) - 0.25f * c11 + 0.75f));
+        E[2] = (double)((0.25f * B2 + B3 + 0.5f * B4) * (c11 + 1.f));
+        E[3] = (double)(-0.5f * B4 * (c11 + dotf(n2i, n2j) + dotf(n3i, n3j) - 1.f));
+        const v3f dn = n1j - n1i;
+        F = (B1 * (D - D0)) * e + (B2 / (2.f * D)) * (dn - dotf(dn, e) * e);
+        const v3f MTB = B3 * crossf(n1j, n1i) - (0.5f * B4) * (crossf(n2j, n2i) + crossf(n3j, n3i));
+        Mij = (-0.5f * B2) * crossf(e, n1i) + MTB;
+        Mji = (0.5f * B2) * crossf(e, n1j) - MTB;
+        const float bnf = dotf(F, nij);
+        const v3f bsf = F - bnf * nij;
+        const float btt = dotf(MTB, nij);
+        const v3f bbt = MTB - btt * nij;
+        const float Ab = R * R * PI_F;
+        const float Ib = Ab * R * R / 4.f;
+        const float Jb = 2.f * Ib;
+        const float sn = -bnf / Ab + lenf(bbt) / Ib * R;
+        const float ss = lenf(bsf) / Ab + fabsf(btt) / Jb * R;
+        E[4] = sn;
+        E[5] = ss;
+        if (Bd.ts[k] > 0. && sn > (float)Bd.ts[k]) act = 0;
+        else if (Bd.coh[k] > 0. && ss > (float)(Bd.coh[k] - Bd.mu[k] * (double)sn)) act = 0;
+    }
+    Bd.active[k] = act;
+    const v3f Ti = Mij + crossf(oi, F);
+    const v3f Tj = Mji + crossf(oj, -F);
+    O[0] = F.x; O[1] = F.y; O[2] = F.z;
+    O[3] = Ti.x; O[4] = Ti.y; O[5] = Ti.z;
+    O[6] = Tj.x; O[7] = Tj.y; O[8] = Tj.z;
+}
+
 // ---------------------------------------------------------------------------
 // per-particle reduction, fixed order
 // ---------------------------------------------------------------------------
@@ -1200,43 +1539,51 @@ struct ReduceArgs {
     BondDev B;
 };
 
-__device__ __forceinline__ double3 ld3(const double* p) { return mk3(p[0], p[1], p[2]); }
-
+// Real = double: FP64 mode; Real = float: mixed mode (pair and bond results
+// stored and summed in single precision)
+template <typename Real>
 __global__ void k_reduce(ReduceArgs r)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= r.P.n) return;
-    double3 F = mk3(0., 0., 0.), T = mk3(0., 0., 0.);
+    Real F[3] = {0, 0, 0}, T[3] = {0, 0, 0};
+    auto add = [](Real* acc, const Real* v, Real sgn) {
+        acc[0] += sgn * v[0];
+        acc[1] += sgn * v[1];
+        acc[2] += sgn * v[2];
+    };
     for (int kind = 0; kind < FD_NKIND; ++kind) {
         if (!r.active[kind]) continue;
         const PairListDev& L = r.L[kind];
+        const Real* pfa = reinterpret_cast<const Real*>(L.pf);
         const int s = L.seg_off[i], c = L.seg_cnt[i];
         for (int k = s; k < s + c; ++k) {
-            const double* pf = L.pf + 9ll * k;
-            F += ld3(pf);
-            T += ld3(pf + 3);
+            const Real* pf = pfa + 9ll * k;
+            add(F, pf, Real(1));
+            add(T, pf + 3, Real(1));
         }
         if (kind == FD_PW) continue;
         const int rs = L.rev_off[i], rc = L.rev_cnt[i];
         for (int e = rs; e < rs + rc; ++e) {
             const int k = L.rev_pair[e];
             if (kind != FD_PP && L.pairA[k] == i) continue;  // a particle against its own ghost
-            const double* pf = L.pf + 9ll * k;
-            F += -ld3(pf);
-            T += ld3(pf + 6);
+            const Real* pf = pfa + 9ll * k;
+            add(F, pf, Real(-1));
+            add(T, pf + 6, Real(1));
         }
     }
     if (r.B.n > 0) {
+        const Real* out = reinterpret_cast<const Real*>(r.B.out);
         for (int e = r.B.plist_off[i]; e < r.B.plist_off[i + 1]; ++e) {
             const int code = r.B.plist[e];
             const int b = code >> 1, side = code & 1;
-            const double* o = r.B.out + 9ll * b;
-            if (side == 0) { F += ld3(o); T += ld3(o + 3); }
-            else { F += -ld3(o); T += ld3(o + 6); }
+            const Real* o = out + 9ll * b;
+            if (side == 0) { add(F, o, Real(1)); add(T, o + 3, Real(1)); }
+            else { add(F, o, Real(-1)); add(T, o + 6, Real(1)); }
         }
     }
-    r.P.force[i] = F;
-    r.P.torque[i] = T;
+    r.P.force[i] = mk3((double)F[0], (double)F[1], (double)F[2]);
+    r.P.torque[i] = mk3((double)T[0], (double)T[1], (double)T[2]);
 }
 
 }  // namespace
@@ -1339,7 +1686,7 @@ void launch_broad_ghost(const ObjDev& P, const GeoSetDev& G, const GhostDev& Gh,
 
 void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& M, const ObjDev& W,
                    const GeoSetDev& GW, const MatDev& MW, const FdGrid& pgrid, const FdGrid& wgrid,
-                   const GhostDev* gh, PairListDev& L, const StepArgs& a, int with_force, cudaStream_t s)
+                   const GhostDev* gh, PairListDev& L, const StepArgs& a, int with_force, bool mixed, cudaStream_t s)
 {
     cudaMemsetAsync(L.n_slots, 0, 2 * sizeof(int), s);  // slots and contacts
     NarrowArgs n;
@@ -1349,14 +1696,22 @@ void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& 
     const long long need = ((long long)L.cap_pairs + NARROW_WARPS - 1) / NARROW_WARPS;
     const int grid = (int)(need < 148 * 24 ? (need > 0 ? need : 1) : 148 * 24);
     const int cgrid = 148 * 16;
+#define FD_NARROW_CASE(K)                                                              \
+    case K:                                                                            \
+        k_select<K><<<grid, NARROW_WARPS * 32, 0, s>>>(n);                             \
+        if (mixed) k_contact32<K><<<cgrid, TPB, 0, s>>>(n);                            \
+        else k_contact<K><<<cgrid, TPB, 0, s>>>(n);                                    \
+        break;
     switch (kind) {
-    case FD_PP: k_select<FD_PP><<<grid, NARROW_WARPS * 32, 0, s>>>(n); k_contact<FD_PP><<<cgrid, TPB, 0, s>>>(n); break;
-    case FD_PW: k_select<FD_PW><<<grid, NARROW_WARPS * 32, 0, s>>>(n); k_contact<FD_PW><<<cgrid, TPB, 0, s>>>(n); break;
-    case FD_GX: k_select<FD_GX><<<grid, NARROW_WARPS * 32, 0, s>>>(n); k_contact<FD_GX><<<cgrid, TPB, 0, s>>>(n); break;
-    case FD_GY: k_select<FD_GY><<<grid, NARROW_WARPS * 32, 0, s>>>(n); k_contact<FD_GY><<<cgrid, TPB, 0, s>>>(n); break;
-    case FD_GXY: k_select<FD_GXY><<<grid, NARROW_WARPS * 32, 0, s>>>(n); k_contact<FD_GXY><<<cgrid, TPB, 0, s>>>(n); break;
+        FD_NARROW_CASE(FD_PP)
+        FD_NARROW_CASE(FD_PW)
+        FD_NARROW_CASE(FD_GX)
+        FD_NARROW_CASE(FD_GY)
+        FD_NARROW_CASE(FD_GXY)
     }
-    k_pair_sum<<<148 * 8, TPB, 0, s>>>(L, with_force);
+#undef FD_NARROW_CASE
+    if (mixed) k_pair_sum32<<<148 * 8, TPB, 0, s>>>(L, with_force);
+    else k_pair_sum<<<148 * 8, TPB, 0, s>>>(L, with_force);
 }
 
 void launch_reverse(const ObjDev& P, PairListDev& L, int* scan_tmp, size_t, cudaStream_t s)
@@ -1371,19 +1726,22 @@ void launch_reverse(const ObjDev& P, PairListDev& L, int* scan_tmp, size_t, cuda
     k_rev_sort<<<nblocks(P.n), TPB, 0, s>>>(L, P.n);
 }
 
-void launch_bonds(const ObjDev& P, BondDev& B, cudaStream_t s)
+void launch_bonds(const ObjDev& P, BondDev& B, bool mixed, cudaStream_t s)
 {
-    if (B.n > 0) k_bonds<<<nblocks(B.n), TPB, 0, s>>>(P, B);
+    if (B.n <= 0) return;
+    if (mixed) k_bonds32<<<nblocks(B.n), TPB, 0, s>>>(P, B);
+    else k_bonds<<<nblocks(B.n), TPB, 0, s>>>(P, B);
 }
 
-void launch_reduce(ObjDev& P, PairListDev* lists, const int* active, const BondDev& B, cudaStream_t s)
+void launch_reduce(ObjDev& P, PairListDev* lists, const int* active, const BondDev& B, bool mixed, cudaStream_t s)
 {
     if (P.n <= 0) return;
     ReduceArgs r;
     r.P = P;
     for (int k = 0; k < FD_NKIND; ++k) { r.L[k] = lists[k]; r.active[k] = active[k]; }
     r.B = B;
-    k_reduce<<<nblocks(P.n), TPB, 0, s>>>(r);
+    if (mixed) k_reduce<float><<<nblocks(P.n), TPB, 0, s>>>(r);
+    else k_reduce<double><<<nblocks(P.n), TPB, 0, s>>>(r);
 }
 
 }  // namespace fd

@@ -155,10 +155,11 @@ void launch_broad_ghost(const ObjDev& P, const GeoSetDev& G, const GhostDev& Gh,
                         unsigned int* flags, double probe, cudaStream_t s);
 void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& M, const ObjDev& W,
                    const GeoSetDev& GW, const MatDev& MW, const FdGrid& pgrid, const FdGrid& wgrid,
-                   const GhostDev* gh, PairListDev& L, const StepArgs& a, int with_force, cudaStream_t s);
+                   const GhostDev* gh, PairListDev& L, const StepArgs& a, int with_force, bool mixed, cudaStream_t s);
 void launch_reverse(const ObjDev& P, PairListDev& L, int* scan_tmp, size_t scan_tmp_ints, cudaStream_t s);
-void launch_bonds(const ObjDev& P, BondDev& B, cudaStream_t s);
-void launch_reduce(ObjDev& P, PairListDev* lists, const int* active, const BondDev& B, cudaStream_t s);
+// mixed: single-precision contact law, bond law and force sums
+void launch_bonds(const ObjDev& P, BondDev& B, bool mixed, cudaStream_t s);
+void launch_reduce(ObjDev& P, PairListDev* lists, const int* active, const BondDev& B, bool mixed, cudaStream_t s);
 
 // exclusive scan of n ints (out may alias in); returns needed tmp ints when tmp == nullptr
 size_t scan_tmp_size(long long n);

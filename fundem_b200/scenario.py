@@ -590,7 +590,7 @@ def bonded_periodic(n=512, n_templates=8, seed=1, footprint=None, pitch=2.4e-3, 
     bp = pairs[sel]
     point = where[sel]
     nb = len(bp)
-    L0 = np.full(nb, 0.1 * 0.5 * d_mean)
+    L0 = np.linalg.norm(objs.pos[bp[:, 0]] - objs.pos[bp[:, 1]], axis=1)  # centre distance
     bonds = Bonds(bp[:, 0].astype(np.int32), bp[:, 1].astype(np.int32), point, normal[sel],
                   np.full(nb, bond_radius_frac * 0.5 * d_mean), L0, np.full(nb, young), np.full(nb, poisson),
                   np.full(nb, tensile), np.zeros(nb), np.zeros(nb))

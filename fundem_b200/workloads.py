@@ -4,8 +4,8 @@
 superellipsoids from 8 templates (semi-axes uniform in [0.8, 1.2] mm,
 exponents in {2, 4}, 32^3 SDFs, 642 nodes), periodic in x and y, on a floor
 wall under a top platen moving down at 1 m/s, dt = 5e-7 s, with V-model bonds
-(E = 1e8 Pa, tensile strength 1e6 Pa) between every pair whose surface gap is
-below 0.05 of the mean diameter.
+(E = 1e8 Pa, tensile strength 1e6 Pa, length = centre distance) between
+every pair whose surface gap is below 0.05 of the mean diameter.
 
 The packing is a jittered lattice whose random orientations are re-drawn,
 and whose remaining overlapping pairs are pushed apart, on the GPU (detection
@@ -100,7 +100,9 @@ def bonded_column(n=262144, footprint=(128, 128), seed=1, pitch=2.42e-3, jitter=
     objs = S.Objects(pos, np.zeros((n, 3)), np.zeros((n, 3)), quat, np.zeros(n, np.int32), geo)
     damping_ratio = 0.3
     e = float(np.exp(-np.pi * damping_ratio / np.sqrt(1 - damping_ratio ** 2)))
-    top = box[2] + 1.0 * pitch
+    # the platen starts 1 um above the highest possible node of the bed, so
+    # the compression begins within the first steps
+    top = float(np.max(pos[:, 2])) + rmax + 1e-6
     ext = float(max(box[0], box[1])) * 1.05
     wall_geos = [S.plane_wall_template(ext), S.plane_wall_template(ext)]
     c = 0.5 * box
@@ -133,7 +135,10 @@ def bonded_column(n=262144, footprint=(128, 128), seed=1, pitch=2.42e-3, jitter=
     sel = order[first]
     nbond = len(sel)
     R = bond_radius_frac * 0.5 * d_mean
-    L0 = np.maximum(-cp["overlap"][sel], 0.02 * d_mean)
+    # bond length: the distance between the two particle centres (the beam
+    # joins the centres; a length of the order of the gap makes the bond's
+    # shear stiffness, which scales as 1/L0^2, far stiffer than the contacts)
+    L0 = np.linalg.norm(sc.particles.pos[a[sel]] - sc.particles.pos[b[sel]], axis=1)
     sim.add_bonds(a[sel], b[sel], cp["point"][sel], cp["normal"][sel], np.full(nbond, R), L0,
                   np.full(nbond, young), np.full(nbond, poisson), np.full(nbond, tensile), np.zeros(nbond),
                   np.zeros(nbond))

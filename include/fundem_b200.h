@@ -43,7 +43,12 @@ const char* fundem_status_string(int status);
    this returns FUNDEM_ERR_CUDA).  stream may be NULL (the legacy stream). */
 int fundem_create(fundem_sim** out, int device, void* stream);
 int fundem_destroy(fundem_sim* sim);
-/* precision of the contact path (FUNDEM_FP64 reproduces the reference) */
+/* precision of the contact path.  FUNDEM_FP64 reproduces the reference.
+   FUNDEM_FP32_MIXED evaluates the node predicate, the SDF gradient, the
+   contact and bond laws and the force sums in single precision; positions,
+   orientations, their integration and the tangential-spring history stay in
+   double precision.  No counterpart in the reference.  May be changed
+   between steps. */
 int fundem_set_precision(fundem_sim* sim, int mode);
 /* when nonzero every step writes full contact records (point, normal,
    overlap, energies); otherwise only node, partner and sliding spring */
