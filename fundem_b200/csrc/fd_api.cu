@@ -444,7 +444,6 @@ struct PairList {
     int cur = 0;
     int cap_pairs = 0, cap_contacts = 0;
     int n_obj = 0;
-    DevArray<int> rev_cnt, rev_off, rev_fill, rev_pair;
     // slot and pair scratch of the current step only
     DevArray<int> c_pair, p_hist_cnt;
     DevArray<double> c_force;
@@ -466,7 +465,6 @@ struct PairList {
             g.c_overlap.alloc(cap_contacts); g.c_en.alloc(cap_contacts); g.c_es.alloc(cap_contacts);
             g.counters.alloc(3);
         }
-        rev_cnt.alloc(m); rev_off.alloc(m); rev_fill.alloc(m); rev_pair.alloc(cap_pairs);
         c_pair.alloc(cap_contacts); c_force.alloc((size_t)cap_contacts * 9);
         p_aux.alloc(cap_pairs); p_hist_cnt.alloc(cap_pairs);
         allocated = true;
@@ -478,7 +476,6 @@ struct PairList {
                 g.pairA.grow(capp, cap_pairs); g.pairB.grow(capp, cap_pairs); g.c_off.grow(capp, cap_pairs);
                 g.c_cnt.grow(capp, cap_pairs); g.pf.grow((size_t)capp * 9, (size_t)cap_pairs * 9);
             }
-            rev_pair.grow(capp, 0);
             p_aux.grow(capp, 0);
             p_hist_cnt.grow(capp, 0);
             cap_pairs = capp;
@@ -510,7 +507,6 @@ struct PairList {
         v.n_slots = c.counters.p + 1; v.n_hits = c.counters.p + 2; v.cap_contacts = cap_contacts;
         v.c_pair = c_pair.p; v.c_k = c.c_k.p; v.o_c_k = o.c_k.p; v.c_force = c_force.p; v.p_aux = p_aux.p; v.p_hist_cnt = p_hist_cnt.p;
         v.o_c_node = o.c_node.p; v.o_c_spring = o.c_spring.p;
-        v.rev_cnt = rev_cnt.p; v.rev_off = rev_off.p; v.rev_fill = rev_fill.p; v.rev_pair = rev_pair.p;
         return v;
     }
 };
@@ -581,6 +577,22 @@ struct fundem_sim {
     DevArray<unsigned long long> stats;  // narrow-phase work counters (profiling only)
     std::vector<int> node_base;
     long long n_nodes = 0;
+    // reverse index over the particle and ghost lists (capacity: their pair
+    // capacities together)
+    DevArray<int> rev_cnt, rev_off, rev_fill, rev_code;
+    fd::RevDev rev_view()
+    {
+        const int np = std::max(P.n(), 1);
+        if (rev_cnt.n < (size_t)np) {
+            rev_cnt.alloc(np); rev_off.alloc(np); rev_fill.alloc(np);
+        }
+        long long cap = 0;
+        for (int k : {FD_PP, FD_GX, FD_GY, FD_GXY})
+            if (lists[k].allocated) cap += lists[k].cap_pairs;
+        cap = std::max<long long>(cap, 16);
+        if (rev_code.n < (size_t)cap) rev_code.alloc((size_t)cap, false);
+        return fd::RevDev{rev_cnt.p, rev_off.p, rev_fill.p, rev_code.p, (int)rev_code.n};
+    }
     long long launches = 0;
     long long hook_steps = 0;  // fundem_step_begin calls, for capacity checks
     std::string last_error;
@@ -822,19 +834,14 @@ struct fundem_sim {
             return;
         }
         tbegin(FUNDEM_T_REDUCE);
-        fd::launch_reverse(Pv, Lpp, scan_tmp.p, scan_tmp.n, stream);
-        launches += 4;
-        for (int d = 0; d < 3; ++d)
-            if (ghosts[d].active) {
-                PairListDev L = lists[FD_GX + d].view();
-                fd::launch_reverse(Pv, L, scan_tmp.p, scan_tmp.n, stream);
-                launches += 4;
-            }
-        fd::BondDev bd = bond_view();
-        if (bd.n > 0) { fd::launch_bonds(Pv, bd, mixed(), stream); launches++; }
         PairListDev views[FD_NKIND];
         for (int k = 0; k < FD_NKIND; ++k) views[k] = lists[k].view();
-        fd::launch_reduce(Pv, views, active, bd, mixed(), stream);
+        fd::RevDev rv = rev_view();
+        fd::launch_reverse(Pv, views, active, rv, scan_tmp.p, scan_tmp.n, stream);
+        launches += 6;
+        fd::BondDev bd = bond_view();
+        if (bd.n > 0) { fd::launch_bonds(Pv, bd, mixed(), stream); launches++; }
+        fd::launch_reduce(Pv, views, active, rv, bd, mixed(), stream);
         launches++;
         tend(FUNDEM_T_REDUCE);
         FD_CUDA(cudaGetLastError());

@@ -1369,36 +1369,71 @@ __global__ void k_pair_sum32(PairListDev L, int with_force)
 // ---------------------------------------------------------------------------
 // reverse index: pairs grouped by partner B, sorted by A
 // ---------------------------------------------------------------------------
-__global__ void k_rev_count(PairListDev L, int n_obj)
+// kinds that have a partner side: particle pairs and the three ghost lists
+// (FD_GX, FD_GY, FD_GXY are consecutive)
+__host__ __device__ constexpr int rev_kind(int k) { return k == 0 ? FD_PP : FD_GX + k - 1; }
+static_assert(FD_GY == FD_GX + 1 && FD_GXY == FD_GX + 2, "ghost kinds are consecutive");
+
+struct RevArgs {
+    PairListDev L[4];
+    int active[4];
+    RevDev R;
+    int n_obj;
+};
+
+// the pair behind a flat index over the active lists
+__device__ __forceinline__ bool rev_locate(const RevArgs& r, int idx, int& k, int& p)
 {
-    const int npairs = min(*L.n_pairs, L.cap_pairs);
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npairs; p += gridDim.x * blockDim.x) {
-        const int B = L.pairB[p];
-        if (B >= 0 && B < n_obj) atomicAdd(&L.rev_cnt[B], 1);
+#pragma unroll
+    for (k = 0; k < 4; ++k) {
+        if (!r.active[k]) continue;
+        const int np = min(*r.L[k].n_pairs, r.L[k].cap_pairs);
+        if (idx < np) { p = idx; return true; }
+        idx -= np;
+    }
+    return false;
+}
+
+__global__ void k_rev_count(RevArgs r)
+{
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x;; idx += gridDim.x * blockDim.x) {
+        int k, p;
+        if (!rev_locate(r, idx, k, p)) return;
+        const int B = r.L[k].pairB[p];
+        if (B >= 0 && B < r.n_obj) atomicAdd(&r.R.cnt[B], 1);
     }
 }
-__global__ void k_rev_fill(PairListDev L, int n_obj)
+__global__ void k_rev_fill(RevArgs r)
 {
-    const int npairs = min(*L.n_pairs, L.cap_pairs);
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npairs; p += gridDim.x * blockDim.x) {
-        const int B = L.pairB[p];
-        if (B >= 0 && B < n_obj) {
-            const int slot = L.rev_off[B] + atomicAdd(&L.rev_fill[B], 1);
-            L.rev_pair[slot] = p;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x;; idx += gridDim.x * blockDim.x) {
+        int k, p;
+        if (!rev_locate(r, idx, k, p)) return;
+        const int B = r.L[k].pairB[p];
+        if (B >= 0 && B < r.n_obj) {
+            const int slot = r.R.off[B] + atomicAdd(&r.R.fill[B], 1);
+            if (slot < r.R.cap) r.R.code[slot] = p * 8 + rev_kind(k);  // pair counts stay below 2^28
         }
     }
 }
-__global__ void k_rev_sort(PairListDev L, int n_obj)
+// deterministic order: by owner, then kind (an owner has one pair per kind
+// with a given partner)
+__global__ void k_rev_sort(RevArgs r)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n_obj) return;
-    int* seg = L.rev_pair + L.rev_off[i];
-    const int cnt = L.rev_cnt[i];
+    if (i >= r.n_obj) return;
+    const int o = r.R.off[i];
+    const int cnt = min(r.R.cnt[i], r.R.cap - o);
+    int* seg = r.R.code + o;
+    auto key = [&](int code) {
+        const int kind = code & 7;
+        const int k = kind == FD_PP ? 0 : kind - FD_GX + 1;
+        return (long long)r.L[k].pairA[code >> 3] * 8 + kind;
+    };
     for (int a = 1; a < cnt; ++a) {
         const int v = seg[a];
-        const int key = L.pairA[v];
+        const long long kv = key(v);
         int b = a - 1;
-        while (b >= 0 && L.pairA[seg[b]] > key) { seg[b + 1] = seg[b]; --b; }
+        while (b >= 0 && key(seg[b]) > kv) { seg[b + 1] = seg[b]; --b; }
         seg[b + 1] = v;
     }
 }
@@ -1536,6 +1571,7 @@ struct ReduceArgs {
     ObjDev P;
     PairListDev L[FD_NKIND];
     int active[FD_NKIND];
+    RevDev R;
     BondDev B;
 };
 
@@ -1552,6 +1588,7 @@ __global__ void k_reduce(ReduceArgs r)
         acc[1] += sgn * v[1];
         acc[2] += sgn * v[2];
     };
+    // pairs the particle owns, kind by kind
     for (int kind = 0; kind < FD_NKIND; ++kind) {
         if (!r.active[kind]) continue;
         const PairListDev& L = r.L[kind];
@@ -1562,12 +1599,16 @@ __global__ void k_reduce(ReduceArgs r)
             add(F, pf, Real(1));
             add(T, pf + 3, Real(1));
         }
-        if (kind == FD_PW) continue;
-        const int rs = L.rev_off[i], rc = L.rev_cnt[i];
+    }
+    // pairs in which it is the partner, by owner
+    {
+        const int rs = r.R.off[i], rc = min(r.R.cnt[i], r.R.cap - rs);
         for (int e = rs; e < rs + rc; ++e) {
-            const int k = L.rev_pair[e];
+            const int code = r.R.code[e];
+            const int kind = code & 7, k = code >> 3;
+            const PairListDev& L = r.L[kind];
             if (kind != FD_PP && L.pairA[k] == i) continue;  // a particle against its own ghost
-            const Real* pf = pfa + 9ll * k;
+            const Real* pf = reinterpret_cast<const Real*>(L.pf) + 9ll * k;
             add(F, pf, Real(-1));
             add(T, pf + 6, Real(1));
         }
@@ -1714,16 +1755,24 @@ void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& 
     else k_pair_sum<<<148 * 8, TPB, 0, s>>>(L, with_force);
 }
 
-void launch_reverse(const ObjDev& P, PairListDev& L, int* scan_tmp, size_t, cudaStream_t s)
+void launch_reverse(const ObjDev& P, PairListDev* lists, const int* active, RevDev& R, int* scan_tmp, size_t,
+                    cudaStream_t s)
 {
     if (P.n <= 0) return;
-    cudaMemsetAsync(L.rev_cnt, 0, sizeof(int) * P.n, s);
-    cudaMemsetAsync(L.rev_fill, 0, sizeof(int) * P.n, s);
+    RevArgs r;
+    for (int k = 0; k < 4; ++k) {
+        r.L[k] = lists[rev_kind(k)];
+        r.active[k] = active[rev_kind(k)];
+    }
+    r.R = R;
+    r.n_obj = P.n;
+    cudaMemsetAsync(R.cnt, 0, sizeof(int) * P.n, s);
+    cudaMemsetAsync(R.fill, 0, sizeof(int) * P.n, s);
     const int g = 148 * 8;
-    k_rev_count<<<g, TPB, 0, s>>>(L, P.n);
-    scan_exclusive(L.rev_cnt, L.rev_off, P.n, scan_tmp, s);
-    k_rev_fill<<<g, TPB, 0, s>>>(L, P.n);
-    k_rev_sort<<<nblocks(P.n), TPB, 0, s>>>(L, P.n);
+    k_rev_count<<<g, TPB, 0, s>>>(r);
+    scan_exclusive(R.cnt, R.off, P.n, scan_tmp, s);
+    k_rev_fill<<<g, TPB, 0, s>>>(r);
+    k_rev_sort<<<nblocks(P.n), TPB, 0, s>>>(r);
 }
 
 void launch_bonds(const ObjDev& P, BondDev& B, bool mixed, cudaStream_t s)
@@ -1733,12 +1782,14 @@ void launch_bonds(const ObjDev& P, BondDev& B, bool mixed, cudaStream_t s)
     else k_bonds<<<nblocks(B.n), TPB, 0, s>>>(P, B);
 }
 
-void launch_reduce(ObjDev& P, PairListDev* lists, const int* active, const BondDev& B, bool mixed, cudaStream_t s)
+void launch_reduce(ObjDev& P, PairListDev* lists, const int* active, const RevDev& R, const BondDev& B, bool mixed,
+                   cudaStream_t s)
 {
     if (P.n <= 0) return;
     ReduceArgs r;
     r.P = P;
     for (int k = 0; k < FD_NKIND; ++k) { r.L[k] = lists[k]; r.active[k] = active[k]; }
+    r.R = R;
     r.B = B;
     if (mixed) k_reduce<float><<<nblocks(P.n), TPB, 0, s>>>(r);
     else k_reduce<double><<<nblocks(P.n), TPB, 0, s>>>(r);

@@ -47,11 +47,17 @@ struct PairListDev {
     int* o_c_node;
     int* o_c_k;
     double* o_c_spring;
-    // reverse index (pairs grouped by partner B)
-    int* rev_cnt;
-    int* rev_off;
-    int* rev_fill;
-    int* rev_pair;
+};
+
+// Reverse index over the particle-particle and ghost lists together: for each
+// particle, the pairs in which it is the partner, as codes pair * 8 + kind,
+// sorted by (owner, kind).
+struct RevDev {
+    int* cnt;
+    int* off;
+    int* fill;
+    int* code;
+    int cap;
 };
 
 struct ObjDev {
@@ -156,10 +162,12 @@ void launch_broad_ghost(const ObjDev& P, const GeoSetDev& G, const GhostDev& Gh,
 void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& M, const ObjDev& W,
                    const GeoSetDev& GW, const MatDev& MW, const FdGrid& pgrid, const FdGrid& wgrid,
                    const GhostDev* gh, PairListDev& L, const StepArgs& a, int with_force, bool mixed, cudaStream_t s);
-void launch_reverse(const ObjDev& P, PairListDev& L, int* scan_tmp, size_t scan_tmp_ints, cudaStream_t s);
+void launch_reverse(const ObjDev& P, PairListDev* lists, const int* active, RevDev& R, int* scan_tmp,
+                    size_t scan_tmp_ints, cudaStream_t s);
 // mixed: single-precision contact law, bond law and force sums
 void launch_bonds(const ObjDev& P, BondDev& B, bool mixed, cudaStream_t s);
-void launch_reduce(ObjDev& P, PairListDev* lists, const int* active, const BondDev& B, bool mixed, cudaStream_t s);
+void launch_reduce(ObjDev& P, PairListDev* lists, const int* active, const RevDev& R, const BondDev& B, bool mixed,
+                   cudaStream_t s);
 
 // exclusive scan of n ints (out may alias in); returns needed tmp ints when tmp == nullptr
 size_t scan_tmp_size(long long n);
