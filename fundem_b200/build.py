@@ -54,6 +54,24 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
+KERNEL_HEADERS = HERE  # the directory holding kernel/LSSolver.h and the value types
+
+
+def build_app(sources, output, include_dirs=(), verbose=False) -> str:
+    """Build an app written against the LSSolver call surface (kernel/LSSolver.h)
+    into an executable linked with libfundem_b200.so: .cpp sources go through
+    the host compiler, .cu sources through nvcc for sm_100a."""
+    build()
+    cmd = [NVCC, *ARCH, "-O2", "-std=c++17", "-I", KERNEL_HEADERS, "-I", os.path.join(ROOT, "include")]
+    for d in include_dirs:
+        cmd += ["-I", d]
+    cmd += list(sources) + ["-L", LIBDIR, "-lfundem_b200", "-Xlinker", "-rpath," + LIBDIR, "-o", output]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.check_call(cmd)
+    return output
+
+
 if __name__ == "__main__":
     build(force="--force" in sys.argv, verbose="-v" in sys.argv)
     print(LIB)

@@ -10,7 +10,7 @@
  * to the reference project).  The reference's own boundary is a set of
  * extern "C" kernel launchers driven by header-only C++ classes; here the
  * launch sequence of one step is owned by the library, and the
- * header-compatible C++ classes (fundem_b200/kernel/*.h) sit on top of these
+ * header-compatible C++ classes (the headers in fundem_b200/kernel/) sit on top of these
  * functions.
  */
 #ifndef FUNDEM_B200_H
