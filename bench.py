@@ -202,12 +202,7 @@ def run_fundem(args, rank, world, dist):
     kt = sim.kernel_times()
     sim.set_profiling(False)
     contacts_end = sim.num_contacts(0) + sim.num_contacts(1) + sum(sim.num_contacts(k) for k in (2, 3, 4))
-    t_max = ms
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
-    value = world * n * args.steps / (t_max / 1e3)
+    t_max, value = aggregate(ms, n, args.steps, world, dist, "cuda")
 
     # end to end through the C ABI with host buffers: upload the state from
     # host memory, run the steps reading back the status word every step,
@@ -232,11 +227,9 @@ def run_fundem(args, rank, world, dist):
     sim.step(wc_steps)
     wc = sim.work_counters()
     sim.set_profiling(False)
-    e2e_val = n * e2e_steps / t_e2e
-    if dist:
-        t = torch.tensor([t_e2e], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_val = world * n * args.steps / float(t.item())
+    e2e_val = 0.0
+    if e2e_steps:
+        _, e2e_val = aggregate(1e3 * t_e2e, n, e2e_steps, world, dist, "cuda")
 
     # mixed precision against FP64 on the same workload: two fresh simulations
     # from the initial state, `error_steps` steps each, positions compared
@@ -285,6 +278,19 @@ def run_fundem(args, rank, world, dist):
         "gpu_launches": launches,
     }
     print(json.dumps(line), flush=True)
+
+
+def aggregate(ms, n, steps, world, dist, device):
+    """Whole-job throughput of `world` replicas of n particles each: the
+    slowest rank's time (a MAX all-reduce, every rank takes part) and
+    world * n * steps / that time, in particle-steps/s."""
+    t_max = ms
+    if dist:
+        import torch
+        t = torch.tensor([float(ms)], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    return t_max, world * n * steps / (t_max / 1e3)
 
 
 def mixed_vs_fp64(sc, dev, args, dist, world):
