@@ -29,6 +29,7 @@ EXPORTS = [
     "fundem_num_pairs", "fundem_num_bonds", "fundem_get_bonds", "fundem_set_bond_activation",
     "fundem_get_geometry", "fundem_get_grid", "fundem_launch_count", "fundem_set_profiling",
     "fundem_kernel_time", "fundem_work_counters", "fundem_prefix_sum", "fundem_prefix_sum_noalloc", "fundem_last_error",
+    "fundem_adjoint_begin", "fundem_adjoint_forward", "fundem_adjoint_backward", "fundem_adjoint_end",
 ]
 TIMERS = {"integrate": 0, "hash": 1, "broad": 2, "narrow_pp": 3, "narrow_pw": 4, "ghost": 5, "reduce": 6}
 
@@ -99,6 +100,10 @@ def lib():
         L.fundem_prefix_sum_noalloc.argtypes = [P, P, LL, P]
         L.fundem_last_error.restype = C.c_char_p
         L.fundem_last_error.argtypes = [P]
+        L.fundem_adjoint_begin.argtypes = [P, I]
+        L.fundem_adjoint_forward.argtypes = [P, I, D, C.c_double]
+        L.fundem_adjoint_backward.argtypes = [P, D, D, D, D]
+        L.fundem_adjoint_end.argtypes = [P]
         _lib = L
     return _lib
 
@@ -230,7 +235,34 @@ class Simulation:
     def add_material(self, wall, kn, ks, mu, e):
         i = C.c_int()
         self._check(self.L.fundem_add_material(self.h, int(wall), kn, ks, mu, e, C.byref(i)), "add_material")
+        if not wall:
+            self._n_pmat = max(getattr(self, "_n_pmat", 0), i.value + 1)
         return i.value
+
+    # ------------------------------------------------------------------ adjoint
+    def adjoint_begin(self, checkpoint_interval=500):
+        """Start recording from the current state (after detect) for reverse-mode
+        gradients; a checkpoint every `checkpoint_interval` steps."""
+        self._check(self.L.fundem_adjoint_begin(self.h, int(checkpoint_interval)), "adjoint_begin")
+
+    def adjoint_forward(self, nsteps, gravity=None, dt=None):
+        g = self.gravity if gravity is None else np.asarray(gravity, float)
+        dt = self.dt if dt is None else float(dt)
+        self._check(self.L.fundem_adjoint_forward(self.h, int(nsteps), _d(_f64(g, 3)), dt), "adjoint_forward")
+
+    def adjoint_backward(self, dl_dpos, dl_dvel):
+        """Gradients of a loss with the given gradients on the final positions
+        and velocities: (d/d initial velocities (n, 3), d/d per particle
+        material (kn, ks, damping ratio, mu) (n_materials, 4))."""
+        n = self.num(False)
+        gv0 = np.zeros((n, 3))
+        gp = np.zeros((getattr(self, "_n_pmat", 1), 4))
+        self._check(self.L.fundem_adjoint_backward(self.h, _d(_f64(dl_dpos, 3 * n)), _d(_f64(dl_dvel, 3 * n)),
+                                                   _d(gv0), _d(gp)), "adjoint_backward")
+        return gv0, gp
+
+    def adjoint_end(self):
+        self._check(self.L.fundem_adjoint_end(self.h), "adjoint_end")
 
     def add_geometry(self, wall, mass, inertia, origin, spacing, size, sdf, nodes):
         i = C.c_int()

@@ -16,8 +16,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libfundem_b200.so")
-SOURCES = ["fd_kernels.cu", "fd_api.cu"]
-HEADERS = ["fd_internal.cuh", "fd_kernels.cuh"]
+SOURCES = ["fd_kernels.cu", "fd_adjoint.cu", "fd_api.cu"]
+HEADERS = ["fd_internal.cuh", "fd_kernels.cuh", "fd_adjoint.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "nvcc")
 # extra compiler definitions, e.g. FUNDEM_NVCC_DEFS="-DFD_NARROW_MIN_BLOCKS=1"

@@ -1,9 +1,12 @@
 // fd_api.cu -- host side of libfundem_b200: template preprocessing, device
 // memory, step orchestration and the C ABI declared in include/fundem_b200.h.
 #include "../../include/fundem_b200.h"
+#include "fd_adjoint.cuh"
 #include "fd_kernels.cuh"
 
 #include <algorithm>
+#include <map>
+#include <tuple>
 #include <cfloat>
 #include <functional>
 #include <cmath>
@@ -444,6 +447,8 @@ struct PairList {
     int cur = 0;
     int cap_pairs = 0, cap_contacts = 0;
     int n_obj = 0;
+    // (node, partner) of the list set_contacts uploaded last, in slot order
+    std::vector<int> up_node, up_partner;
     // slot and pair scratch of the current step only
     DevArray<int> c_pair, p_hist_cnt;
     DevArray<double> c_force;
@@ -553,6 +558,52 @@ struct BondHost {
 // synchronises the stream once)
 constexpr int CAPACITY_CHECK = 64;
 
+// adjoint: per-step records of the contact lists and bonds over one
+// checkpoint segment, the host checkpoints, and the reverse-sweep arrays
+struct AdjTape {
+    int steps = 0;
+    int cap[FD_NKIND] = {0, 0, 0, 0, 0};
+    DevArray<int> ints[FD_NKIND];        // 8 ints per slot per step
+    DevArray<double> dbl[FD_NKIND];      // 13 doubles per slot per step
+    DevArray<int> nslots;                // per step and kind
+    int nbond = 0;
+    DevArray<int> bond_active;           // per step and bond
+    DevArray<double> bond_rij;           // 3 per step and bond
+    fd::AdjRec rec(int k, int t)
+    {
+        fd::AdjRec r{};
+        const long long c = cap[k];
+        int* I = ints[k].p + 8ll * c * t;
+        double* D = dbl[k].p + 13ll * c * t;
+        r.hit = I; r.A = I + c; r.Bp = I + 2 * c; r.B = I + 3 * c; r.geoB = I + 4 * c; r.matB = I + 5 * c;
+        r.nid = I + 6 * c; r.hist = I + 7 * c;
+        r.rel = D; r.vc = D + 3 * c; r.sprev = D + 6 * c; r.qB = D + 9 * c;
+        r.cap = cap[k];
+        return r;
+    }
+    int* ns(int k, int t) { return nslots.p + (long long)t * FD_NKIND + k; }
+};
+
+struct AdjCheckpoint {
+    std::vector<double> pos, vel, angvel, quat, force, torque;
+    std::vector<double> wpos, wvel, wangvel, wquat, wforce, wtorque;
+    std::vector<int> node[FD_NKIND], partner[FD_NKIND];
+    std::vector<double> spring[FD_NKIND];
+    std::vector<int> bond_active;
+};
+
+struct AdjState {
+    bool on = false;
+    int K = 0;
+    double3 g{0, 0, 0};
+    double dt = 0.0;
+    bool dt_set = false;
+    long long steps = 0;
+    std::vector<AdjCheckpoint> ckpt;   // state at the start of each segment
+    std::vector<int> seg_steps;        // steps in each segment
+    AdjCheckpoint final_state;
+};
+
 struct fundem_sim {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -595,6 +646,10 @@ struct fundem_sim {
     }
     long long launches = 0;
     long long hook_steps = 0;  // fundem_step_begin calls, for capacity checks
+    AdjState adj;
+    AdjTape tape;
+    AdjTape* recording = nullptr;  // set while a segment is re-run for the reverse sweep
+    int record_step = 0;
     std::string last_error;
     // optional CUDA-event timing of kernel groups (fundem_set_profiling)
     bool profiling = false;
@@ -657,7 +712,7 @@ struct fundem_sim {
 
     fd::StepArgs step_args(double dt, double probe = 0.0)
     {
-        fd::StepArgs a;
+        fd::StepArgs a{};
         a.dt = dt;
         a.probe = probe;
         a.gravity = make_double3(0, 0, 0);
@@ -793,14 +848,22 @@ struct fundem_sim {
         fd::launch_broad_pp(Pv, G, T, Lpp, flags.p, probe, stream);
         tend(FUNDEM_T_BROAD);
         tbegin(FUNDEM_T_NARROW_PP);
+        a.rec = recording ? recording->rec(FD_PP, record_step) : fd::AdjRec{};
         fd::launch_narrow(FD_PP, Pv, G, M, Wv, GW, MW, pgrid, wgrid, nullptr, Lpp, a, with_force, mixed(), stream);
+        if (recording)
+            FD_CUDA(cudaMemcpyAsync(recording->ns(FD_PP, record_step), Lpp.n_slots, sizeof(int),
+                                    cudaMemcpyDeviceToDevice, stream));
         tend(FUNDEM_T_NARROW_PP);
         PairListDev Lpw = lists[FD_PW].view();
         tbegin(FUNDEM_T_BROAD);
         fd::launch_broad_pw(Pv, G, Wv, GW, wgrid, Lpw, flags.p, probe, stream);
         tend(FUNDEM_T_BROAD);
         tbegin(FUNDEM_T_NARROW_PW);
+        a.rec = recording ? recording->rec(FD_PW, record_step) : fd::AdjRec{};
         fd::launch_narrow(FD_PW, Pv, G, M, Wv, GW, MW, pgrid, wgrid, nullptr, Lpw, a, with_force, mixed(), stream);
+        if (recording)
+            FD_CUDA(cudaMemcpyAsync(recording->ns(FD_PW, record_step), Lpw.n_slots, sizeof(int),
+                                    cudaMemcpyDeviceToDevice, stream));
         tend(FUNDEM_T_NARROW_PW);
         launches += 4;
         PairListDev Lg[3];
@@ -823,7 +886,12 @@ struct fundem_sim {
                 fd::GhostDev gh = ghosts[d].view();
                 Lg[d] = lists[kinds[d]].view();
                 fd::launch_broad_ghost(Pv, G, gh, Lg[d], flags.p, probe, stream);
-                fd::launch_narrow(kinds[d], Pv, G, M, Wv, GW, MW, pgrid, wgrid, &gh, Lg[d], a, with_force, mixed(), stream);
+                a.rec = recording ? recording->rec(kinds[d], record_step) : fd::AdjRec{};
+                fd::launch_narrow(kinds[d], Pv, G, M, Wv, GW, MW, pgrid, wgrid, &gh, Lg[d], a, with_force, mixed(),
+                                  stream);
+                if (recording)
+                    FD_CUDA(cudaMemcpyAsync(recording->ns(kinds[d], record_step), Lg[d].n_slots, sizeof(int),
+                                            cudaMemcpyDeviceToDevice, stream));
                 active[kinds[d]] = 1;
                 launches += 2;
             }
@@ -840,6 +908,10 @@ struct fundem_sim {
         fd::launch_reverse(Pv, views, active, rv, scan_tmp.p, scan_tmp.n, stream);
         launches += 6;
         fd::BondDev bd = bond_view();
+        if (recording && bd.n > 0) {
+            bd.rec_active = recording->bond_active.p + (long long)record_step * bd.n;
+            bd.rec_rij = recording->bond_rij.p + 3ll * record_step * bd.n;
+        }
         if (bd.n > 0) { fd::launch_bonds(Pv, bd, mixed(), stream); launches++; }
         fd::launch_reduce(Pv, views, active, rv, bd, mixed(), stream);
         launches++;
@@ -1537,6 +1609,8 @@ int fundem_set_contacts(fundem_sim* s, int kind, long long n, const int* node, c
         g.c_node.upload(cn.data(), cn.size(), s->stream);
         g.c_slave.upload(cs.data(), cs.size(), s->stream);
         g.c_k.upload(ck.data(), ck.size(), s->stream);
+        L.up_node = cn;
+        L.up_partner = cs;
         g.c_spring.upload(csp.data(), csp.size(), s->stream);
         const int counters[3] = {(int)pairA.size(), (int)cn.size(), (int)cn.size()};
         g.counters.upload(counters, 3, s->stream);
@@ -1687,3 +1761,274 @@ int fundem_launch_count(fundem_sim* s, long long* n)
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// adjoint: checkpoints, segment re-runs with recording, reverse sweep
+// ---------------------------------------------------------------------------
+namespace {
+
+void adj_check(int r)
+{
+    if (r != FUNDEM_OK) throw std::runtime_error(std::string("adjoint: ") + fundem_status_string(r));
+}
+
+void adj_snapshot(fundem_sim* s, AdjCheckpoint& c)
+{
+    int np = 0, nw = 0;
+    adj_check(fundem_num_objects(s, 0, &np));
+    adj_check(fundem_num_objects(s, 1, &nw));
+    auto grab = [&](int wall, int n, std::vector<double>& x, std::vector<double>& v, std::vector<double>& w,
+                    std::vector<double>& q, std::vector<double>& f, std::vector<double>& t) {
+        x.assign(3 * n, 0.0); v.assign(3 * n, 0.0); w.assign(3 * n, 0.0); q.assign(4 * n, 0.0);
+        f.assign(3 * n, 0.0); t.assign(3 * n, 0.0);
+        if (n > 0) adj_check(fundem_get_objects(s, wall, x.data(), v.data(), w.data(), q.data(), f.data(), t.data()));
+    };
+    grab(0, np, c.pos, c.vel, c.angvel, c.quat, c.force, c.torque);
+    grab(1, nw, c.wpos, c.wvel, c.wangvel, c.wquat, c.wforce, c.wtorque);
+    for (int k = 0; k < FD_NKIND; ++k) {
+        long long n = 0;
+        adj_check(fundem_num_contacts(s, k, &n));
+        c.node[k].assign(n, 0); c.partner[k].assign(n, 0); c.spring[k].assign(3 * n, 0.0);
+        if (n > 0)
+            adj_check(fundem_get_contacts(s, k, c.node[k].data(), c.partner[k].data(), nullptr, nullptr, nullptr,
+                                          c.spring[k].data(), nullptr, nullptr));
+    }
+    int nb = 0;
+    adj_check(fundem_num_bonds(s, &nb));
+    c.bond_active.assign(nb, 0);
+    if (nb > 0) adj_check(fundem_get_bonds(s, c.bond_active.data(), nullptr, nullptr));
+}
+
+void adj_restore(fundem_sim* s, AdjCheckpoint& c)
+{
+    if (!c.quat.empty())
+        adj_check(fundem_set_objects(s, 0, c.pos.data(), c.vel.data(), c.angvel.data(), c.quat.data(), c.force.data(),
+                                     c.torque.data()));
+    if (!c.wquat.empty())
+        adj_check(fundem_set_objects(s, 1, c.wpos.data(), c.wvel.data(), c.wangvel.data(), c.wquat.data(),
+                                     c.wforce.data(), c.wtorque.data()));
+    for (int k = 0; k < FD_NKIND; ++k) {
+        if (!s->lists[k].allocated) continue;
+        adj_check(fundem_set_contacts(s, k, (long long)c.node[k].size(), c.node[k].data(), c.partner[k].data(),
+                                      c.spring[k].data()));
+    }
+    if (!c.bond_active.empty()) adj_check(fundem_set_bond_activation(s, c.bond_active.data()));
+}
+
+}  // namespace
+
+extern "C" {
+
+int fundem_adjoint_begin(fundem_sim* s, int checkpoint_interval)
+{
+    if (!s || checkpoint_interval < 1) return FUNDEM_ERR_ARG;
+    if (!s->setup_done || !s->detected) return FUNDEM_ERR_STATE;
+    if (s->precision != FUNDEM_FP64) {
+        s->last_error = "the adjoint differentiates the FP64 path";
+        return FUNDEM_ERR_STATE;
+    }
+    for (const FdGeo& g : s->pgeo.table) {
+        const fd_sym& I = g.inv_inertia;
+        if (I.xx != 0.0 || I.yy != 0.0 || I.zz != 0.0 || I.xy != 0.0 || I.xz != 0.0 || I.yz != 0.0) {
+            s->last_error = "the adjoint differentiates translations only: a particle geometry can rotate";
+            return FUNDEM_ERR_STATE;
+        }
+    }
+    return guard(s, [&] {
+        AdjState& A = s->adj;
+        A = AdjState{};
+        A.on = true;
+        A.K = checkpoint_interval;
+        A.ckpt.emplace_back();
+        adj_snapshot(s, A.ckpt.back());
+        A.seg_steps.push_back(0);
+    });
+}
+
+int fundem_adjoint_forward(fundem_sim* s, int nsteps, const double g[3], double dt)
+{
+    if (!s || !g || nsteps < 0 || !(dt > 0.0)) return FUNDEM_ERR_ARG;
+    AdjState& A = s->adj;
+    if (!A.on) return FUNDEM_ERR_STATE;
+    const double3 gg = make_double3(g[0], g[1], g[2]);
+    if (A.dt_set && (A.dt != dt || A.g.x != gg.x || A.g.y != gg.y || A.g.z != gg.z)) {
+        s->last_error = "the adjoint needs one time step and one gravity over the recording";
+        return FUNDEM_ERR_ARG;
+    }
+    A.g = gg;
+    A.dt = dt;
+    A.dt_set = true;
+    const int r = guard(s, [&] {
+        FD_CUDA(cudaSetDevice(s->device));
+        for (int k = 0; k < nsteps; ++k) {
+            if (A.seg_steps.back() == A.K) {
+                A.ckpt.emplace_back();
+                adj_snapshot(s, A.ckpt.back());
+                A.seg_steps.push_back(0);
+            }
+            if (A.steps % CAPACITY_CHECK == 0) s->ensure_capacity();
+            s->front(gg, dt);
+            s->detect_all(true, dt);
+            s->back(gg, dt);
+            A.seg_steps.back() += 1;
+            A.steps += 1;
+        }
+        FD_CUDA(cudaGetLastError());
+    });
+    if (r != FUNDEM_OK) return r;
+    return fundem_sync(s);
+}
+
+int fundem_adjoint_backward(fundem_sim* s, const double* dl_dpos, const double* dl_dvel, double* dl_dvel0,
+                            double* dl_dparams)
+{
+    if (!s || !dl_dpos || !dl_dvel || !dl_dvel0 || !dl_dparams) return FUNDEM_ERR_ARG;
+    AdjState& A = s->adj;
+    if (!A.on || A.steps == 0) return FUNDEM_ERR_STATE;
+    return guard(s, [&] {
+        FD_CUDA(cudaSetDevice(s->device));
+        adj_snapshot(s, A.final_state);
+        s->ensure_capacity();
+        const int np = s->P.n();
+        const int nmat = (int)s->pmat.kn.size();
+        const int K = A.K;
+        // tape for one segment
+        AdjTape& T = s->tape;
+        T.steps = K;
+        for (int k = 0; k < FD_NKIND; ++k) {
+            T.cap[k] = s->lists[k].allocated ? s->lists[k].cap_contacts : 0;
+            const size_t c = (size_t)std::max(T.cap[k], 1);
+            T.ints[k].alloc(8 * c * K, false);
+            T.dbl[k].alloc(13 * c * K, false);
+        }
+        T.nslots.alloc((size_t)K * FD_NKIND);
+        fd::BondDev bd = s->bond_view();
+        T.nbond = bd.n;
+        T.bond_active.alloc((size_t)std::max(bd.n, 1) * K);
+        T.bond_rij.alloc((size_t)std::max(bd.n, 1) * 3 * K);
+        DevArray<double> xb, vb, vhb, Fb, Feb, pgrad, Sb[2][FD_NKIND];
+        DevArray<double3> dn;
+        xb.alloc(3 * (size_t)np); vb.alloc(3 * (size_t)np); vhb.alloc(3 * (size_t)np);
+        Fb.alloc(3 * (size_t)np); Feb.alloc(3 * (size_t)np); pgrad.alloc(4 * (size_t)std::max(nmat, 1));
+        for (int k = 0; k < FD_NKIND; ++k) {
+            Sb[0][k].alloc(3 * (size_t)std::max(T.cap[k], 1));
+            Sb[1][k].alloc(3 * (size_t)std::max(T.cap[k], 1));
+        }
+        xb.upload(dl_dpos, 3 * (size_t)np, s->stream);
+        vb.upload(dl_dvel, 3 * (size_t)np, s->stream);
+        dn.alloc((size_t)std::max(bd.n, 1));
+        const ObjDev Pv = s->P.view();
+        fd::adj_bond_frames(bd.frames, Pv.q, bd.master, bd.slave, bd.n, dn.p, s->stream);
+        fd::AdjParticles ap{np, Pv.geo, Pv.mat, s->pgeo.view(), xb.p, vb.p, vhb.p, Fb.p, Feb.p, pgrad.p};
+        std::map<std::tuple<int, int, int>, double3> carry;
+        int cur = 0;
+        for (int seg = (int)A.ckpt.size() - 1; seg >= 0; --seg) {
+            const int ns = A.seg_steps[seg];
+            if (ns == 0) continue;
+            adj_restore(s, A.ckpt[seg]);
+            // re-run the segment, recording every step
+            s->recording = &T;
+            for (int t = 0; t < ns; ++t) {
+                s->record_step = t;
+                s->front(A.g, A.dt);
+                s->detect_all(true, A.dt);
+                s->back(A.g, A.dt);
+            }
+            s->recording = nullptr;
+            FD_CUDA(cudaStreamSynchronize(s->stream));
+            unsigned int f = 0;
+            FD_CUDA(cudaMemcpy(&f, s->flags.p, sizeof(f), cudaMemcpyDeviceToHost));
+            if (f & (FD_FLAG_PAIR_OVERFLOW | FD_FLAG_CONTACT_OVERFLOW | FD_FLAG_NEIGHBOR_OVERFLOW))
+                throw std::runtime_error("adjoint: a contact list overflowed while a segment was re-run");
+            // spring adjoints of the segment's last step, from the later segment
+            for (int k = 0; k < FD_NKIND; ++k)
+                FD_CUDA(cudaMemsetAsync(Sb[cur][k].p, 0, Sb[cur][k].n * sizeof(double), s->stream));
+            if (!carry.empty()) {
+                const int t = ns - 1;
+                for (int k = 0; k < FD_NKIND; ++k) {
+                    if (T.cap[k] == 0) continue;
+                    int nsl = 0;
+                    FD_CUDA(cudaMemcpy(&nsl, T.ns(k, t), sizeof(int), cudaMemcpyDeviceToHost));
+                    nsl = std::min(nsl, T.cap[k]);
+                    if (nsl <= 0) continue;
+                    const fd::AdjRec R = T.rec(k, t);
+                    std::vector<int> hit(nsl), nid(nsl), B(nsl);
+                    FD_CUDA(cudaMemcpy(hit.data(), R.hit, sizeof(int) * nsl, cudaMemcpyDeviceToHost));
+                    FD_CUDA(cudaMemcpy(nid.data(), R.nid, sizeof(int) * nsl, cudaMemcpyDeviceToHost));
+                    FD_CUDA(cudaMemcpy(B.data(), R.B, sizeof(int) * nsl, cudaMemcpyDeviceToHost));
+                    std::vector<double> sb(3 * (size_t)nsl, 0.0);
+                    bool any = false;
+                    for (int i = 0; i < nsl; ++i) {
+                        if (!hit[i]) continue;
+                        auto it = carry.find(std::make_tuple(k, nid[i], B[i]));
+                        if (it == carry.end()) continue;
+                        sb[3 * i] = it->second.x; sb[3 * i + 1] = it->second.y; sb[3 * i + 2] = it->second.z;
+                        any = true;
+                    }
+                    if (any)
+                        FD_CUDA(cudaMemcpy(Sb[cur][k].p, sb.data(), sizeof(double) * sb.size(), cudaMemcpyHostToDevice));
+                }
+            }
+            // reverse sweep over the segment
+            for (int t = ns - 1; t >= 0; --t) {
+                fd::adj_force(ap, A.dt, s->stream);
+                const int prv = cur ^ 1;
+                for (int k = 0; k < FD_NKIND; ++k)
+                    FD_CUDA(cudaMemsetAsync(Sb[prv][k].p, 0, Sb[prv][k].n * sizeof(double), s->stream));
+                for (int k = 0; k < FD_NKIND; ++k) {
+                    if (T.cap[k] == 0) continue;
+                    fd::AdjContactArgs c{};
+                    c.rec = T.rec(k, t);
+                    c.nslots = T.ns(k, t);
+                    c.M = s->pmat.view();
+                    c.MW = s->wmat.view();
+                    c.GW = s->wgeo.view();
+                    c.Sb_cur = Sb[cur][k].p;
+                    c.Sb_prev = Sb[prv][k].p;
+                    c.sb_prev_cap = T.cap[k];
+                    c.dt = A.dt;
+                    fd::adj_contacts(ap, c, s->stream);
+                }
+                if (bd.n > 0) {
+                    fd::AdjBondArgs b{bd.n, bd.master, bd.slave, T.bond_active.p + (long long)t * bd.n,
+                                      T.bond_rij.p + 3ll * t * bd.n, bd.B, bd.L0, dn.p};
+                    fd::adj_bonds(ap, b, s->stream);
+                }
+                fd::adj_particles(ap, A.dt, s->stream);
+                cur = prv;
+            }
+            FD_CUDA(cudaGetLastError());
+            // spring adjoints of the restored lists (the state before the
+            // segment), keyed for the earlier segment
+            carry.clear();
+            FD_CUDA(cudaStreamSynchronize(s->stream));
+            for (int k = 0; k < FD_NKIND; ++k) {
+                const PairList& L = s->lists[k];
+                const size_t n = L.up_node.size();
+                if (T.cap[k] == 0 || n == 0) continue;
+                std::vector<double> sb(3 * n);
+                FD_CUDA(cudaMemcpy(sb.data(), Sb[cur][k].p, sizeof(double) * 3 * std::min<size_t>(n, T.cap[k]),
+                                   cudaMemcpyDeviceToHost));
+                for (size_t i = 0; i < std::min<size_t>(n, T.cap[k]); ++i)
+                    if (sb[3 * i] != 0.0 || sb[3 * i + 1] != 0.0 || sb[3 * i + 2] != 0.0)
+                        carry[std::make_tuple(k, L.up_node[i], L.up_partner[i])] =
+                            make_double3(sb[3 * i], sb[3 * i + 1], sb[3 * i + 2]);
+            }
+        }
+        FD_CUDA(cudaStreamSynchronize(s->stream));
+        FD_CUDA(cudaMemcpy(dl_dvel0, vb.p, sizeof(double) * 3 * np, cudaMemcpyDeviceToHost));
+        FD_CUDA(cudaMemcpy(dl_dparams, pgrad.p, sizeof(double) * 4 * nmat, cudaMemcpyDeviceToHost));
+        adj_restore(s, A.final_state);
+        FD_CUDA(cudaStreamSynchronize(s->stream));
+    });
+}
+
+int fundem_adjoint_end(fundem_sim* s)
+{
+    if (!s) return FUNDEM_ERR_ARG;
+    s->adj = AdjState{};
+    return FUNDEM_OK;
+}
+
+}  // extern "C"
+

@@ -951,6 +951,7 @@ __global__ void __launch_bounds__(TPB, FD_CONTACT_MIN_BLOCKS) k_contact(NarrowAr
                 const double3 pt = gp + (0.5 * ov) * nrm;
                 nid = n.P.node_base[A] + n.G.node_lid[pool];
                 double3 spring = mk3(0., 0., 0.);
+                int hist = -1;
                 {
                     // the previous slots of the pair are ascending in node
                     // key; a node appears at most once per pair
@@ -963,7 +964,28 @@ __global__ void __launch_bounds__(TPB, FD_CONTACT_MIN_BLOCKS) k_contact(NarrowAr
                     if (lo < oc_end && L.o_c_k[lo] == k && L.o_c_node[lo] == nid) {
                         const double* sp = L.o_c_spring + 3ll * lo;
                         spring = mk3(sp[0], sp[1], sp[2]);
+                        hist = lo;
                     }
+                }
+                const AdjRec& R = n.a.rec;
+                if (R.hit && s < R.cap) {
+                    R.A[s] = A;
+                    R.B[s] = B;
+                    R.Bp[s] = KIND == FD_PW ? -1 : B;
+                    R.geoB[s] = KIND == FD_PW ? n.W.geo[B] : n.P.geo[B];
+                    R.matB[s] = KIND == FD_PW ? n.W.mat[B] : n.P.mat[B];
+                    R.nid[s] = nid;
+                    R.hist[s] = hist;
+                    R.rel[3 * s + 0] = gp.x - cB.x;
+                    R.rel[3 * s + 1] = gp.y - cB.y;
+                    R.rel[3 * s + 2] = gp.z - cB.z;
+                    R.sprev[3 * s + 0] = spring.x;
+                    R.sprev[3 * s + 1] = spring.y;
+                    R.sprev[3 * s + 2] = spring.z;
+                    R.qB[4 * s + 0] = qB.q0;
+                    R.qB[4 * s + 1] = qB.q1;
+                    R.qB[4 * s + 2] = qB.q2;
+                    R.qB[4 * s + 3] = qB.q3;
                 }
                 double kn = 0., ks = 0.;
                 if (n.with_force) {
@@ -1002,6 +1024,11 @@ __global__ void __launch_bounds__(TPB, FD_CONTACT_MIN_BLOCKS) k_contact(NarrowAr
                         mu = fmin(mui, n.M.mu[mj]);
                     }
                     const double3 vc = (vi + cross3(wi, pt - ri)) - (vj + cross3(wj, pt - rj));
+                    if (R.hit && s < R.cap) {
+                        R.vc[3 * s + 0] = vc.x;
+                        R.vc[3 * s + 1] = vc.y;
+                        R.vc[3 * s + 2] = vc.z;
+                    }
                     double3 F = mk3(0., 0., 0.);
                     linear_contact(F, spring, vc, nrm, ov, n.a.dt, kn, ks, mu, res, effM);
                     const double3 TA = cross3(pt - ri, F);
@@ -1039,6 +1066,7 @@ __global__ void __launch_bounds__(TPB, FD_CONTACT_MIN_BLOCKS) k_contact(NarrowAr
                 }
             }
             L.c_node[s] = nid;
+            if (n.a.rec.hit && s < n.a.rec.cap) n.a.rec.hit[s] = hit ? 1 : 0;
         }
         hits += __popc(__ballot_sync(0xffffffffu, hit));
     }
@@ -1122,11 +1150,6 @@ __device__ __forceinline__ v3f rowsf(float4 r0, float4 r1, float4 r2, v3f v)
 {
     return v3f{fmaf(r0.x, v.x, fmaf(r0.y, v.y, r0.z * v.z)), fmaf(r1.x, v.x, fmaf(r1.y, v.y, r1.z * v.z)),
                fmaf(r2.x, v.x, fmaf(r2.y, v.y, r2.z * v.z))};
-}
-__device__ __forceinline__ v3f colsf(float4 r0, float4 r1, float4 r2, v3f v)
-{
-    return v3f{fmaf(r0.x, v.x, fmaf(r1.x, v.y, r2.x * v.z)), fmaf(r0.y, v.x, fmaf(r1.y, v.y, r2.y * v.z)),
-               fmaf(r0.z, v.x, fmaf(r1.z, v.y, r2.z * v.z))};
 }
 constexpr float PI_F = 3.14159265358979f;
 
@@ -1448,6 +1471,7 @@ __global__ void k_bonds(ObjDev P, BondDev Bd)
     double* E = Bd.energy + 6ll * k;
     double* O = Bd.out + 9ll * k;
     for (int t = 0; t < 9; ++t) O[t] = 0.;
+    if (Bd.rec_active) Bd.rec_active[k] = Bd.active[k] != 0;
     if (Bd.active[k] == 0) {
         for (int t = 0; t < 6; ++t) E[t] = 0.;
         return;
@@ -1464,6 +1488,11 @@ __global__ void k_bonds(ObjDev P, BondDev Bd)
     double3 F = mk3(0., 0., 0.), Mij = mk3(0., 0., 0.), Mji = mk3(0., 0., 0.);
     int act = 1;
     const double3 rij = rbi - rbj;
+    if (Bd.rec_rij) {
+        Bd.rec_rij[3 * k + 0] = rij.x;
+        Bd.rec_rij[3 * k + 1] = rij.y;
+        Bd.rec_rij[3 * k + 2] = rij.z;
+    }
     const double D = length3(rij);
     if (!fd_is_zero(D)) {
         const double B1 = Bd.B[4 * k], B2 = Bd.B[4 * k + 1], B3 = Bd.B[4 * k + 2], B4 = Bd.B[4 * k + 3];

@@ -132,9 +132,31 @@ struct BondDev {
     double* out;           // 9 per bond: F, Ti, Tj
     const int* plist_off;  // per particle (n+1): bonds touching it
     const int* plist;      // bond id * 2 + side
+    int* rec_active;       // adjoint recording (null when off): bond active at the step
+    double* rec_rij;       // 3 per bond: bond vector rb_i - rb_j at the step
+};
+
+// Adjoint recording of one list at one step, one entry per contact slot
+// (null pointers when not recording).  The partner index Bp is the particle
+// that takes the reaction (the image's particle for ghosts, -1 for walls).
+struct AdjRec {
+    int* hit;        // 1 when the slot holds a contact
+    int* A;
+    int* Bp;
+    int* B;          // partner as listed (wall index for walls)
+    int* geoB;       // partner geometry (in the wall set for walls)
+    int* matB;       // partner material (a wall material for walls)
+    int* nid;        // global boundary-node id of the contact
+    int* hist;       // slot of the same contact in the previous step, -1 when none
+    double* rel;     // 3 per slot: contact node minus partner centre, world frame
+    double* vc;      // 3 per slot: relative velocity of A against the partner
+    double* sprev;   // 3 per slot: sliding spring before this step's update
+    double* qB;      // 4 per slot: partner orientation
+    int cap;         // slots the record holds
 };
 
 struct StepArgs {
+    AdjRec rec;      // recording of the list being launched (rec.hit null: off)
     double dt;
     double probe;      // contact when overlap >= -probe (0 in a timestep)
     double3 gravity;

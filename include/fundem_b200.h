@@ -170,6 +170,29 @@ int fundem_prefix_sum(int* d_prefix, const int* d_count, long long n, void* stre
 #define FUNDEM_NOALLOC_SCAN_MAX 16777216LL
 int fundem_prefix_sum_noalloc(int* d_prefix, const int* d_count, long long n, void* stream);
 
+/* Reverse-mode gradients (the adjoint of the FP64 step).  No counterpart in
+   the reference.  Loss gradients on the final state are carried back to the
+   initial velocities and to each particle material's normal stiffness,
+   shear stiffness, damping ratio and friction coefficient.  Contact topology
+   is frozen at each step, as the forward run had it (including each
+   contact's stick or slip and each bond's breakage); orientations are
+   taken as fixed, so every particle geometry must have a zero inverse
+   inertia (as the reference's inverse() gives mm-scale particles).
+   begin: start recording from the current state (after fundem_detect),
+     with a checkpoint every checkpoint_interval steps;
+   forward: run steps (one gravity and time step for the whole recording);
+   backward: dl_dpos, dl_dvel (n*3, the loss gradient on the final positions
+     and velocities) -> dl_dvel0 (n*3) and dl_dparams (4 per particle
+     material: kn, ks, damping ratio, mu).  Each checkpoint segment is re-run
+     once with recording, then swept in reverse; the final state is restored
+     afterwards.
+   end: drop the recording. */
+int fundem_adjoint_begin(fundem_sim* sim, int checkpoint_interval);
+int fundem_adjoint_forward(fundem_sim* sim, int nsteps, const double gravity[3], double dt);
+int fundem_adjoint_backward(fundem_sim* sim, const double* dl_dpos, const double* dl_dvel, double* dl_dvel0,
+                            double* dl_dparams);
+int fundem_adjoint_end(fundem_sim* sim);
+
 /* text of the last error a call on this simulation returned (empty when
    none); valid until the next call on it.  The reference prints such
    messages to std::cerr instead. */
