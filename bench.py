@@ -235,6 +235,12 @@ def run_fundem(args, rank, world, dist):
     # from the initial state, `error_steps` steps each, positions compared
     # (minimum image across the periodic seams), then K timed steps each
     mixed = None if args.no_mixed else mixed_vs_fp64(sc, dev, args, dist, world)
+    adjoint = None
+    if not args.no_adjoint and rank == 0:
+        try:
+            adjoint = adjoint_cost(args, dev)
+        except Exception as exc:  # an auxiliary figure: report, do not fail the run
+            adjoint = {"error": f"{type(exc).__name__}: {exc}"}
 
     if rank != 0:
         return
@@ -273,6 +279,7 @@ def run_fundem(args, rank, world, dist):
                                  "clusters_kept": wc[2] / wc_steps, "node_contacts": wc[3] / wc_steps,
                                  "exact_node_tests": wc[4] / wc_steps},
         "mixed": mixed,
+        "adjoint": adjoint,
         "cpu_baseline": cpu,
         "clocks": clk,
         "gpu_launches": launches,
@@ -347,6 +354,52 @@ def mixed_vs_fp64(sc, dev, args, dist, world):
                                              "|x_mixed - x_fp64| / |x_fp64| over particles"}}
 
 
+def adjoint_cost(args, dev):
+    """Cost of the adjoint against the plain forward run on the adjoint pour
+    (4096 particles, 2 templates, dt = 1e-6 s, a checkpoint every 500 steps).
+    Loss: mean particle height (a packing measure) plus the mean-square
+    displacement of 64 tagged particles."""
+    import fundem_b200 as F
+    from fundem_b200 import workloads
+    sim, sc = workloads.adjoint_pour(n=4096, device=dev)
+    n = len(sc.particles)
+    x0 = sim.state()["pos"].copy()
+    sim.close()
+    steps, K = args.adjoint_steps, 500
+    s = F.Simulation.from_scenario(sc, device=dev, records=False)
+    s.detect()
+    s.sync()
+    t0 = time.perf_counter()
+    s.step(steps)
+    s.sync()
+    t_fwd = time.perf_counter() - t0
+    s.close()
+    s = F.Simulation.from_scenario(sc, device=dev, records=False)
+    s.detect()
+    s.adjoint_begin(K)
+    t0 = time.perf_counter()
+    s.adjoint_forward(steps)
+    t_rec = time.perf_counter() - t0
+    st = s.state()
+    tag = np.arange(0, n, n // 64)[:64]
+    dl_dx = np.zeros((n, 3))
+    dl_dx[:, 2] = 1.0 / n
+    dl_dx[tag] += 2.0 * (st["pos"][tag] - x0[tag]) / len(tag)
+    contacts = s.num_contacts(F.PP) + s.num_contacts(F.PW)
+    t0 = time.perf_counter()
+    gv0, gp = s.adjoint_backward(dl_dx, np.zeros((n, 3)))
+    t_bwd = time.perf_counter() - t0
+    s.adjoint_end()
+    s.close()
+    return {"workload": "adjoint pour: 4096 superellipsoids, 2 templates, six walls, dt 1e-6 s",
+            "steps": steps, "checkpoint_interval": K, "node_contacts_at_end": contacts,
+            "forward_s": t_fwd, "recorded_forward_s": t_rec, "backward_s": t_bwd,
+            "backward_over_forward": t_bwd / t_fwd, "total_over_forward": (t_rec + t_bwd) / t_fwd,
+            "dl_dparams": gp[0].tolist(), "dl_dparams_order": ["kn", "ks", "damping ratio", "mu"],
+            "note": "backward re-runs each checkpoint segment once with recording, then sweeps it in reverse; "
+                    "wall-clock times, the calls synchronise"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -362,6 +415,8 @@ def main():
                     help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision comparison")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint cost measurement")
+    ap.add_argument("--adjoint-steps", type=int, default=2000)
     ap.add_argument("--error-steps", type=int, default=1000,
                     help="steps before the mixed-precision position error is measured")
     args = ap.parse_args()

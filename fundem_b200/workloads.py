@@ -151,3 +151,23 @@ def bonded_column(n=262144, footprint=(128, 128), seed=1, pitch=2.42e-3, jitter=
     info = dict(n=n, templates=n_templates, resampled=moved, bonds=nbond, gap=gap, d_mean=d_mean,
                 footprint=[nx, ny], layers=nz, pitch=pitch)
     return sim, sc, info
+
+
+def adjoint_pour(n=4096, seed=0, n_templates=2, box=(40e-3, 40e-3, 80e-3), pitch=2.8e-3, dt=1e-6,
+                 overlap_tol=2e-6, device=0, log=None):
+    """The adjoint workload: n superellipsoids (the small pour's distributions,
+    2 templates, 32^3 SDFs, 642 nodes) on a jittered lattice in a box of six
+    plane walls, dt = 1e-6 s, orientations re-drawn on the GPU until no
+    overlap exceeds overlap_tol.  Returns (Simulation, Scenario)."""
+    from . import Simulation
+    sc = S.pour(n=n, n_templates=n_templates, seed=seed, box=box, pitch=pitch, dt=dt, explicit_mass=True,
+                resolve=False, name="adjoint_pour")
+    rng = np.random.default_rng(seed + 1)
+    sim = Simulation.from_scenario(sc, device=device, records=True)
+    moved, quat, pos = resolve_on_gpu(sim, sc, rng, tol=overlap_tol, log=log)
+    sc.particles.quat = quat
+    sc.particles.pos = pos
+    sim.set_state(quat=quat, pos=pos)
+    sim.set_records(False)
+    sim.detect()
+    return sim, sc
