@@ -235,6 +235,12 @@ def run_fundem(args, rank, world, dist):
     # from the initial state, `error_steps` steps each, positions compared
     # (minimum image across the periodic seams), then K timed steps each
     mixed = None if args.no_mixed else mixed_vs_fp64(sc, dev, args, dist, world)
+    batched = None
+    if not args.no_batch and rank == 0:
+        try:
+            batched = batched_cost(args, dev)
+        except Exception as exc:  # an auxiliary figure: report, do not fail the run
+            batched = {"error": f"{type(exc).__name__}: {exc}"}
     adjoint = None
     if not args.no_adjoint and rank == 0:
         try:
@@ -280,6 +286,7 @@ def run_fundem(args, rank, world, dist):
                                  "exact_node_tests": wc[4] / wc_steps},
         "mixed": mixed,
         "adjoint": adjoint,
+        "batched": batched,
         "cpu_baseline": cpu,
         "clocks": clk,
         "gpu_launches": launches,
@@ -400,6 +407,45 @@ def adjoint_cost(args, dev):
                     "wall-clock times, the calls synchronise"}
 
 
+def batched_cost(args, dev):
+    """The calibration sweep: args.batch_sims independent pours of uneven size
+    (log-uniform in [500, 20000] particles, per-simulation kn, friction and
+    damping), args.batch_steps steps each, stepped concurrently (one stream per
+    simulation, CUDA-graph chunks of the autotuned length) and one at a time."""
+    from fundem_b200 import batch
+    t0 = time.perf_counter()
+    scs, params = batch.calibration_scenarios(n_sims=args.batch_sims, seed=1)
+    t_build = time.perf_counter() - t0
+    probe = batch.Batch(scs[: min(32, len(scs))], device=dev)
+    chunk, tune = batch.autotune_chunk(probe, candidates=(25, 50, 100, 200), probe_steps=200)
+    probe.close()
+    t0 = time.perf_counter()
+    conc = batch.Batch(scs, device=dev)
+    t_setup = time.perf_counter() - t0
+    particles = conc.particles
+    conc.sync()
+    t0 = time.perf_counter()
+    conc.run_graphs(args.batch_steps, chunk)
+    t_conc = time.perf_counter() - t0
+    conc.close()
+    seq = batch.Batch(scs, device=dev)
+    seq.sync()
+    t0 = time.perf_counter()
+    seq.run_sequential(args.batch_steps)
+    t_seq = time.perf_counter() - t0
+    seq.close()
+    ps = particles * args.batch_steps
+    return {"workload": "calibration sweep: pours of 500-20,000 particles (log-uniform), kn, friction and damping "
+                        "per simulation, the small pour's shapes, fill ratio 0.4, dt 1e-6 s",
+            "simulations": len(scs), "particles": particles, "steps": args.batch_steps,
+            "chunk": chunk, "autotune_s": {str(k): round(v, 4) for k, v in tune.items()},
+            "concurrent_s": t_conc, "sequential_s": t_seq, "speedup": t_seq / t_conc,
+            "concurrent_particle_steps_per_s": ps / t_conc, "sequential_particle_steps_per_s": ps / t_seq,
+            "scenario_build_s": round(t_build, 1), "setup_s": round(t_setup, 1),
+            "note": "one stream per simulation with CUDA-graph chunks (not a single persistent kernel); "
+                    "wall-clock times around synchronised runs"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -417,6 +463,9 @@ def main():
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision comparison")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint cost measurement")
     ap.add_argument("--adjoint-steps", type=int, default=2000)
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched calibration measurement")
+    ap.add_argument("--batch-sims", type=int, default=256)
+    ap.add_argument("--batch-steps", type=int, default=200)
     ap.add_argument("--error-steps", type=int, default=1000,
                     help="steps before the mixed-precision position error is measured")
     args = ap.parse_args()

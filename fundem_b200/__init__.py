@@ -30,6 +30,7 @@ EXPORTS = [
     "fundem_get_geometry", "fundem_get_grid", "fundem_launch_count", "fundem_set_profiling",
     "fundem_kernel_time", "fundem_work_counters", "fundem_prefix_sum", "fundem_prefix_sum_noalloc", "fundem_last_error",
     "fundem_adjoint_begin", "fundem_adjoint_forward", "fundem_adjoint_backward", "fundem_adjoint_end",
+    "fundem_step_graph",
 ]
 TIMERS = {"integrate": 0, "hash": 1, "broad": 2, "narrow_pp": 3, "narrow_pw": 4, "ghost": 5, "reduce": 6}
 
@@ -104,6 +105,7 @@ def lib():
         L.fundem_adjoint_forward.argtypes = [P, I, D, C.c_double]
         L.fundem_adjoint_backward.argtypes = [P, D, D, D, D]
         L.fundem_adjoint_end.argtypes = [P]
+        L.fundem_step_graph.argtypes = [P, I, D, C.c_double]
         _lib = L
     return _lib
 
@@ -192,12 +194,12 @@ class Simulation:
 
     # ------------------------------------------------------------------ build
     @classmethod
-    def from_scenario(cls, sc, device=0, precision=FP64, records=True, setup=True):
+    def from_scenario(cls, sc, device=0, precision=FP64, records=True, setup=True, stream=None):
         """Register a Scenario exactly as the reference API receives it:
         materials, geometries (explicit mass, or density through the
         addParticleCluster centroid handling, LSSolver.h:125-165), particles,
         walls, wall motion, bonds and periodicity."""
-        s = cls(device=device, precision=precision, records=records)
+        s = cls(device=device, stream=stream, precision=precision, records=records)
         for (kn, ks, mu, e) in sc.particle_materials:
             s.add_material(False, kn, ks, mu, e)
         for (mu, e) in sc.wall_materials:
@@ -319,6 +321,13 @@ class Simulation:
     def step(self, n=1, dt=None, gravity=None):
         g = _f64(self.gravity if gravity is None else gravity, 3)
         self._check(self.L.fundem_step(self.h, int(n), _d(g), float(self.dt if dt is None else dt)), "step")
+
+    def step_graph(self, n, dt=None, gravity=None):
+        """n steps recorded once into a CUDA graph and replayed on later calls
+        (for many small simulations on separate streams)."""
+        g = _f64(self.gravity if gravity is None else gravity, 3)
+        self._check(self.L.fundem_step_graph(self.h, int(n), _d(g), float(self.dt if dt is None else dt)),
+                    "step_graph")
 
     def step_begin(self, dt=None, gravity=None):
         g = _f64(self.gravity if gravity is None else gravity, 3)

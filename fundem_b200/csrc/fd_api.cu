@@ -5,6 +5,7 @@
 #include "fd_kernels.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <map>
 #include <tuple>
 #include <cfloat>
@@ -33,6 +34,10 @@ struct CudaError : std::runtime_error {
         if (e_ != cudaSuccess) throw CudaError(std::string(#x) + ": " + cudaGetErrorString(e_));     \
     } while (0)
 
+// bumped by every device (re)allocation of a DevArray: a captured step graph
+// holds raw pointers and is rebuilt when this moves
+std::atomic<unsigned long long> g_alloc_epoch{0};
+
 template <typename T> struct DevArray {
     T* p = nullptr;
     size_t n = 0;
@@ -51,6 +56,7 @@ template <typename T> struct DevArray {
         release();
         n = count;
         if (count == 0) return;
+        g_alloc_epoch.fetch_add(1);
         FD_CUDA(cudaMalloc((void**)&p, sizeof(T) * count));
         if (zero) FD_CUDA(cudaMemset(p, 0, sizeof(T) * count));
     }
@@ -58,6 +64,7 @@ template <typename T> struct DevArray {
     void grow(size_t count, size_t keep)
     {
         if (count <= n) return;
+        g_alloc_epoch.fetch_add(1);
         T* q = nullptr;
         FD_CUDA(cudaMalloc((void**)&q, sizeof(T) * count));
         FD_CUDA(cudaMemset(q, 0, sizeof(T) * count));
@@ -646,6 +653,23 @@ struct fundem_sim {
     }
     long long launches = 0;
     long long hook_steps = 0;  // fundem_step_begin calls, for capacity checks
+    // a captured run of steps (fundem_step_graph)
+    cudaGraphExec_t graph_exec = nullptr;
+    cudaStream_t cap_stream = nullptr;
+    bool capturing = false;
+    int graph_steps = 0;
+    double graph_key[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // gravity, dt, precision, records, counters, periodicity
+    unsigned long long graph_epoch = 0;
+    void drop_graph()
+    {
+        if (graph_exec) cudaGraphExecDestroy(graph_exec);
+        graph_exec = nullptr;
+    }
+    ~fundem_sim()
+    {
+        drop_graph();
+        if (cap_stream) cudaStreamDestroy(cap_stream);
+    }
     AdjState adj;
     AdjTape tape;
     AdjTape* recording = nullptr;  // set while a segment is re-run for the reverse sweep
@@ -657,7 +681,7 @@ struct fundem_sim {
     std::vector<cudaEvent_t> tev[FUNDEM_NTIMERS][2];
     void tbegin(int cat)
     {
-        if (!profiling) return;
+        if (!profiling || capturing) return;
         cudaEvent_t e;
         FD_CUDA(cudaEventCreate(&e));
         FD_CUDA(cudaEventRecord(e, stream));
@@ -665,7 +689,7 @@ struct fundem_sim {
     }
     void tend(int cat)
     {
-        if (!profiling) return;
+        if (!profiling || capturing) return;
         cudaEvent_t e;
         FD_CUDA(cudaEventCreate(&e));
         FD_CUDA(cudaEventRecord(e, stream));
@@ -1370,6 +1394,62 @@ int fundem_step(fundem_sim* s, int nsteps, const double g[3], double dt)
             s->back(d3(g), dt);
         }
         FD_CUDA(cudaGetLastError());
+    });
+}
+
+int fundem_step_graph(fundem_sim* s, int nsteps, const double g[3], double dt)
+{
+    if (!s || !g || nsteps < 1) return FUNDEM_ERR_ARG;
+    if (!s->setup_done) return FUNDEM_ERR_STATE;
+    return guard(s, [&] {
+        FD_CUDA(cudaSetDevice(s->device));
+        // grow the lists ahead of their counts, and make every lazy
+        // allocation of a step, before anything is captured
+        s->ensure_capacity();
+        s->rev_view();
+        const double key[8] = {g[0], g[1], g[2], dt, (double)s->precision, (double)s->records,
+                               (double)s->counters, (double)(s->perX * 2 + s->perY)};
+        bool same = s->graph_exec && s->graph_steps == nsteps && s->graph_epoch == g_alloc_epoch.load();
+        for (int k = 0; k < 8 && same; ++k) same = s->graph_key[k] == key[k];
+        if (!same) {
+            s->drop_graph();
+            if (!s->cap_stream) FD_CUDA(cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking));
+            const cudaStream_t own = s->stream;
+            const unsigned long long epoch = g_alloc_epoch.load();
+            s->stream = s->cap_stream;
+            s->capturing = true;
+            cudaGraph_t graph = nullptr;
+            cudaError_t e = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
+            try {
+                if (e != cudaSuccess) throw CudaError(cudaGetErrorString(e));
+                for (int k = 0; k < nsteps; ++k) {
+                    s->front(d3(g), dt);
+                    s->detect_all(true, dt);
+                    s->back(d3(g), dt);
+                }
+            } catch (...) {
+                cudaStreamEndCapture(s->stream, &graph);
+                if (graph) cudaGraphDestroy(graph);
+                s->stream = own;
+                s->capturing = false;
+                throw;
+            }
+            e = cudaStreamEndCapture(s->stream, &graph);
+            s->stream = own;
+            s->capturing = false;
+            FD_CUDA(e);
+            if (g_alloc_epoch.load() != epoch) {
+                cudaGraphDestroy(graph);
+                throw std::logic_error("a device allocation happened while the steps were captured");
+            }
+            e = cudaGraphInstantiate(&s->graph_exec, graph, 0);
+            cudaGraphDestroy(graph);
+            FD_CUDA(e);
+            s->graph_steps = nsteps;
+            std::copy(key, key + 8, s->graph_key);
+            s->graph_epoch = epoch;
+        }
+        FD_CUDA(cudaGraphLaunch(s->graph_exec, s->stream));
     });
 }
 

@@ -97,6 +97,13 @@ int fundem_detect_proximity(fundem_sim* sim, double gap);
    stream once every 64 steps, to grow the contact lists ahead of their
    counts; the reference synchronises every step. */
 int fundem_step(fundem_sim* sim, int nsteps, const double gravity[3], double dt);
+/* nsteps iterations as fundem_step, recorded once into a CUDA graph and
+   replayed on later calls with the same nsteps, gravity, time step and
+   settings; the graph is recorded again after any list growth or
+   re-setup.  Each call first grows the contact lists ahead of their counts
+   (one stream synchronisation).  For many small simulations on separate
+   streams, whose steps are launch-bound.  No counterpart in the reference. */
+int fundem_step_graph(fundem_sim* sim, int nsteps, const double gravity[3], double dt);
 /* one step split at the addExternalForceTorque hook (LSSolver.h:588): after
    step_begin the force/torque arrays hold the step's contact and bond sums;
    the caller may add to them (stream-ordered) before step_end. */
