@@ -538,10 +538,10 @@ struct CellTable {
 struct Ghost {
     DevArray<double3> pos;
     DevArray<long long> hash;
-    DevArray<int> occ;
+    DevArray<int> occ, searchers, nsearch;
     CellTable cells;
     bool active = false;
-    fd::GhostDev view() { return fd::GhostDev{pos.p, hash.p, cells.view(), occ.p}; }
+    fd::GhostDev view() { return fd::GhostDev{pos.p, hash.p, cells.view(), occ.p, searchers.p, nsearch.p}; }
 };
 
 struct BondHost {
@@ -834,6 +834,8 @@ struct fundem_sim {
                 ghosts[d].pos.alloc(std::max(np, 1));
                 ghosts[d].hash.alloc(std::max(np, 1));
                 ghosts[d].occ.alloc(6);
+                ghosts[d].searchers.alloc(std::max(np, 1));
+                ghosts[d].nsearch.alloc(1);
                 ghosts[d].cells.alloc(pgrid, np);
             }
         }

@@ -363,10 +363,14 @@ constexpr int BROAD_CAND = 128;              // candidate slots staged per lane 
 // emit A's pairs sorted by partner id.  GHOST: partners are the ghost images
 // of a cell table built from ghost positions (no B > A rule; the reach is the
 // partner's SDF grid radius, since ghost pairs have no radius test).
-template <bool GHOST>
+//
+// LIST: only the particles in alist[0 .. *acount) search (the ghost phases
+// list the particles whose search box reaches a ghost image; the others
+// were given empty segments by k_ghost_searchers).
+template <bool GHOST, bool LIST>
 __global__ void __launch_bounds__(TPB) k_broad_cells(ObjDev P, GeoSetDev G, CellTableDev T, const double3* gpos,
-                                                     const int* occ, PairListDev L, unsigned int* flags,
-                                                     double probe)
+                                                     const int* occ, const int* alist, const int* acount,
+                                                     PairListDev L, unsigned int* flags, double probe)
 {
     __shared__ int s_list[TPB / BROAD_LANES][MAX_CAND];
     __shared__ int s_cand[TPB / BROAD_LANES][BROAD_CAND];
@@ -375,8 +379,14 @@ __global__ void __launch_bounds__(TPB) k_broad_cells(ObjDev P, GeoSetDev G, Cell
     const int gl = lane & (BROAD_LANES - 1);
     const int gbase = lane & ~(BROAD_LANES - 1);
     const int gb = threadIdx.x / BROAD_LANES;
-    const int A = (blockIdx.x * blockDim.x + threadIdx.x) / BROAD_LANES;
-    const bool valid = A < P.n;
+    constexpr int GPW = 32 / BROAD_LANES;           // lane groups per warp
+    constexpr int GPB = TPB / BROAD_LANES;          // lane groups per block
+    const int total = LIST ? *acount : P.n;
+    // warp-uniform loop over the warp's groups
+    for (int gw = blockIdx.x * GPB + (gb & ~(GPW - 1)); gw < total; gw += gridDim.x * GPB) {
+    const int gidx = gw + (gb & (GPW - 1));
+    const bool valid = gidx < total;
+    const int A = valid ? (LIST ? alist[gidx] : gidx) : 0;
     double3 cA = mk3(0., 0., 0.);
     double rA = 0.;
     int3 lo = make_int3(0, 0, 0), hi = make_int3(-1, -1, -1);
@@ -464,6 +474,30 @@ __global__ void __launch_bounds__(TPB) k_broad_cells(ObjDev P, GeoSetDev G, Cell
             L.pairA[base + r] = A;
             L.pairB[base + r] = v;
         }
+    }
+    __syncwarp();
+    }
+}
+
+// ghost phases: particles whose search box reaches the cells holding ghost
+// images are listed for k_broad_cells<true, true>; the others get empty
+// segments here
+__global__ void k_ghost_searchers(ObjDev P, GeoSetDev G, FdGrid g, const int* occ, PairListDev L, int* alist,
+                                  int* acount)
+{
+    const int A = blockIdx.x * blockDim.x + threadIdx.x;
+    if (A >= P.n) return;
+    const double rA = G.geo[P.geo[A]].radius;
+    const double reach = (rA + G.grid_rmax) * (1.0 + 8.0 * BOUND_REL);
+    int3 lo, hi;
+    partner_search_range(P.pos[A], reach, g, lo, hi);
+    const bool any = max(lo.x, occ[0]) <= min(hi.x, occ[3]) && max(lo.y, occ[1]) <= min(hi.y, occ[4]) &&
+                     max(lo.z, occ[2]) <= min(hi.z, occ[5]);
+    if (any) {
+        alist[atomicAdd(acount, 1)] = A;
+    } else {
+        L.seg_off[A] = 0;
+        L.seg_cnt[A] = 0;
     }
 }
 
@@ -1736,8 +1770,8 @@ void launch_broad_pp(const ObjDev& P, const GeoSetDev& G, const CellTableDev& T,
 {
     cudaMemsetAsync(L.n_pairs, 0, sizeof(int), s);
     if (P.n > 0)
-        k_broad_cells<false><<<nblocks((long long)P.n * BROAD_LANES), TPB, 0, s>>>(P, G, T, nullptr, nullptr, L,
-                                                                                   flags, probe);
+        k_broad_cells<false, false><<<nblocks((long long)P.n * BROAD_LANES), TPB, 0, s>>>(
+            P, G, T, nullptr, nullptr, nullptr, nullptr, L, flags, probe);
 }
 void launch_broad_pw(const ObjDev& P, const GeoSetDev& G, const ObjDev& W, const GeoSetDev& GW,
                      const FdGrid& wg, PairListDev& L, unsigned int* flags, double probe, cudaStream_t s)
@@ -1749,9 +1783,12 @@ void launch_broad_ghost(const ObjDev& P, const GeoSetDev& G, const GhostDev& Gh,
                         unsigned int* flags, double probe, cudaStream_t s)
 {
     cudaMemsetAsync(L.n_pairs, 0, sizeof(int), s);
-    if (P.n > 0)
-        k_broad_cells<true><<<nblocks((long long)P.n * BROAD_LANES), TPB, 0, s>>>(P, G, Gh.cells, Gh.pos, Gh.occ,
-                                                                                  L, flags, probe);
+    if (P.n <= 0) return;
+    cudaMemsetAsync(Gh.nsearch, 0, sizeof(int), s);
+    k_ghost_searchers<<<nblocks(P.n), TPB, 0, s>>>(P, G, Gh.cells.g, Gh.occ, L, Gh.searchers, Gh.nsearch);
+    const long long groups = std::min<long long>(P.n, 148ll * 8 * (TPB / BROAD_LANES));
+    k_broad_cells<true, true><<<nblocks(groups * BROAD_LANES), TPB, 0, s>>>(
+        P, G, Gh.cells, Gh.pos, Gh.occ, Gh.searchers, Gh.nsearch, L, flags, probe);
 }
 
 void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& M, const ObjDev& W,

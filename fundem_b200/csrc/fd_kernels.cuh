@@ -113,6 +113,8 @@ struct GhostDev {
     long long* hash;
     CellTableDev cells;
     int* occ;  // box of the cells holding ghost images: min x, y, z, max x, y, z
+    int* searchers;  // particles whose search box reaches a ghost image
+    int* nsearch;    // their count
 };
 
 struct BondDev {
