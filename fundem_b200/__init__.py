@@ -30,7 +30,7 @@ EXPORTS = [
     "fundem_get_geometry", "fundem_get_grid", "fundem_launch_count", "fundem_set_profiling",
     "fundem_kernel_time", "fundem_work_counters", "fundem_prefix_sum", "fundem_prefix_sum_noalloc", "fundem_last_error",
     "fundem_adjoint_begin", "fundem_adjoint_forward", "fundem_adjoint_backward", "fundem_adjoint_end",
-    "fundem_step_graph",
+    "fundem_step_graph", "fundem_set_neighbour_list",
 ]
 TIMERS = {"integrate": 0, "hash": 1, "broad": 2, "narrow_pp": 3, "narrow_pw": 4, "ghost": 5, "reduce": 6}
 
@@ -106,6 +106,7 @@ def lib():
         L.fundem_adjoint_backward.argtypes = [P, D, D, D, D]
         L.fundem_adjoint_end.argtypes = [P]
         L.fundem_step_graph.argtypes = [P, I, D, C.c_double]
+        L.fundem_set_neighbour_list.argtypes = [P, I]
         _lib = L
     return _lib
 
@@ -300,6 +301,10 @@ class Simulation:
 
     def set_periodic(self, x, y):
         self._check(self.L.fundem_set_periodic(self.h, int(bool(x)), int(bool(y))), "set_periodic")
+
+    def set_neighbour_list(self, mode):
+        """-1: from the particle count, 0: off, 1: on."""
+        self._check(self.L.fundem_set_neighbour_list(self.h, int(mode)), "set_neighbour_list")
 
     def set_precision(self, precision):
         """FP64 (the reference's arithmetic) or FP32_MIXED; may change between steps."""

@@ -564,6 +564,10 @@ struct BondHost {
 // steps between list-capacity checks inside fundem_step (each check
 // synchronises the stream once)
 constexpr int CAPACITY_CHECK = 64;
+// particle counts from which the particle-particle broad phase keeps a
+// neighbour list, and its skin as a fraction of the largest bounding radius
+constexpr int NL_MIN_PARTICLES = 8192;
+constexpr double NL_SKIN = 0.15;
 
 // adjoint: per-step records of the contact lists and bonds over one
 // checkpoint segment, the host checkpoints, and the reverse-sweep arrays
@@ -635,6 +639,28 @@ struct fundem_sim {
     DevArray<unsigned long long> stats;  // narrow-phase work counters (profiling only)
     std::vector<int> node_base;
     long long n_nodes = 0;
+    // neighbour list of the particle-particle broad phase (large sets only;
+    // small ones search the cell table every step)
+    DevArray<double3> nl_ref;
+    DevArray<int> nl_vis, nl_cnt, nl_list, nl_ctrl;
+    bool use_nl = false;
+    int nl_mode = -1;  // -1: from the particle count, 0: off, 1: on (fundem_set_neighbour_list)
+    // (re)allocate the neighbour list for the current particle count and
+    // request a build at the next detection
+    void configure_nl()
+    {
+        use_nl = nl_mode > 0 || (nl_mode < 0 && P.n() >= NL_MIN_PARTICLES);
+        if (!use_nl) return;
+        const size_t m = std::max(P.n(), 1);
+        nl_ref.alloc(m); nl_vis.alloc(m); nl_cnt.alloc(m); nl_list.alloc(m * fd::NL_MAX, false);
+        nl_ctrl.alloc(4);
+        const int one = 1;
+        FD_CUDA(cudaMemcpy(nl_ctrl.p, &one, sizeof(int), cudaMemcpyHostToDevice));
+    }
+    fd::NlDev nl_view()
+    {
+        return fd::NlDev{nl_ref.p, nl_vis.p, nl_cnt.p, nl_list.p, nl_ctrl.p, NL_SKIN * pgeo.rmax, perX, perY};
+    }
     // reverse index over the particle and ghost lists (capacity: their pair
     // capacities together)
     DevArray<int> rev_cnt, rev_off, rev_fill, rev_code;
@@ -818,6 +844,7 @@ struct fundem_sim {
         pgrid = make_grid(mn, mx, pcell, setup_done ? &pgrid : nullptr);
         wgrid = make_grid(mn, mx, wcell, setup_done ? &wgrid : nullptr);
         ptab.alloc(pgrid, P.n());
+        configure_nl();
         wcount.alloc((size_t)std::max<long long>(wgrid.num, 1));
         const int np = P.n();
         const int nw = W.n();
@@ -871,7 +898,13 @@ struct fundem_sim {
             for (int k = 0; k < FD_NKIND; ++k) lists[k].cur ^= 1;
         PairListDev Lpp = lists[FD_PP].view();
         tbegin(FUNDEM_T_BROAD);
-        fd::launch_broad_pp(Pv, G, T, Lpp, flags.p, probe, stream);
+        if (use_nl) {
+            fd::NlDev nl = nl_view();
+            fd::launch_broad_pp_nl(Pv, G, T, Lpp, nl, flags.p, probe, stream);
+            launches += 2;
+        } else {
+            fd::launch_broad_pp(Pv, G, T, Lpp, flags.p, probe, stream);
+        }
         tend(FUNDEM_T_BROAD);
         tbegin(FUNDEM_T_NARROW_PP);
         a.rec = recording ? recording->rec(FD_PP, record_step) : fd::AdjRec{};
@@ -1113,6 +1146,17 @@ int fundem_set_precision(fundem_sim* s, int mode)
     if (!s || (mode != FUNDEM_FP64 && mode != FUNDEM_FP32_MIXED)) return FUNDEM_ERR_ARG;
     s->precision = mode;
     return FUNDEM_OK;
+}
+
+int fundem_set_neighbour_list(fundem_sim* s, int mode)
+{
+    if (!s || mode < -1 || mode > 1) return FUNDEM_ERR_ARG;
+    s->nl_mode = mode;
+    if (!s->setup_done) return FUNDEM_OK;
+    return guard(s, [&] {
+        FD_CUDA(cudaStreamSynchronize(s->stream));
+        s->configure_nl();
+    });
 }
 
 int fundem_set_records(fundem_sim* s, int full)

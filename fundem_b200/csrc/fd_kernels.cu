@@ -301,41 +301,70 @@ __device__ void emit_pairs(int A, int* buf, int cnt, int total, PairListDev& L, 
 
 constexpr double BOUND_REL = 1e-9;
 
-// Body-level cull of a candidate pair: true when no surface node of a body of
-// radius rA centred at cA can reach a cell of B's SDF grid where the
-// trilinear value can be <= -probe... i.e. no contact (or proximity pair) is
-// possible.  Uses the same exact-conservative bounds as the cluster cull: the
-// grid box, the distance-to-possibly-inside-cells field (probe == 0 only) and
-// the Lipschitz bound of the trilinear SDF.
-__device__ __forceinline__ bool body_culled(const double3 cA, double rA, const double3 cB, const fd_quat qB,
-                                            const FdGeo& GB, const GeoSetDev& SB, double probe)
+// True when no point within `radius` of p (a position in B's body frame, in
+// single precision) can pass the node predicate against B (or, with probe >
+// 0, come within `probe` of B).  Conservative: single-precision evaluation
+// with relative margins far above its rounding (about 1e-7 relative), bounds
+// that hold in exact arithmetic:
+//   * B's bounding sphere (particle pairs: the reference's radius test),
+//   * B's SDF grid box (nodes outside it are never contacts),
+//   * D(v): lower bound on the distance from grid node v to any cell whose
+//     corner minimum is <= 0, 1-Lipschitz in the position,
+//   * the Lipschitz bound of the trilinear SDF (distance-like fields).
+__device__ __forceinline__ bool sphere_culled(float px, float py, float pz, float radius, bool radius_test,
+                                              const FdGeo& GB, const GeoSetDev& SB, double rB, double probe)
 {
-    const double3 lp = fd_rrot(cA - cB, qB);
-    const double3 g = mk3((lp.x - GB.origin.x) * GB.inv_spacing, (lp.y - GB.origin.y) * GB.inv_spacing,
-                          (lp.z - GB.origin.z) * GB.inv_spacing);
-    const double rho = rA * (1.0 + 1e-7) + 1e-12 * (GB.spacing + rA);
-    const double rg = rho * GB.inv_spacing;
-    if (g.x < -rg || g.y < -rg || g.z < -rg) return true;
-    if (g.x > GB.size.x - 1 + rg || g.y > GB.size.y - 1 + rg || g.z > GB.size.z - 1 + rg) return true;
-    if (probe == 0.0) {
-        const int vx = min(max((int)rint(g.x), 0), GB.size.x - 1);
-        const int vy = min(max((int)rint(g.y), 0), GB.size.y - 1);
-        const int vz = min(max((int)rint(g.z), 0), GB.size.z - 1);
-        const double D = (double)__ldg(SB.dist + GB.dist_off + fd_lin3(vx, vy, vz, GB.size));
-        const double3 dv = mk3((g.x - vx) * GB.spacing, (g.y - vy) * GB.spacing, (g.z - vz) * GB.spacing);
-        if (D - length3(dv) > rho) return true;
+    const float scale = (float)rB + radius + (float)GB.spacing;
+    const float margin = 2e-5f * scale;
+    const float rho = radius + margin;
+    if (radius_test) {
+        const float lim = (float)rB + rho;
+        if (px * px + py * py + pz * pz > lim * lim) return true;
     }
-    if (g.x >= 0. && g.y >= 0. && g.z >= 0. && g.x < GB.size.x - 1 && g.y < GB.size.y - 1 && g.z < GB.size.z - 1) {
-        const int i0 = (int)floor(g.x), j0 = (int)floor(g.y), k0 = (int)floor(g.z);
+    const float is = (float)GB.inv_spacing;
+    const float gx = (px - (float)GB.origin.x) * is, gy = (py - (float)GB.origin.y) * is,
+                gz = (pz - (float)GB.origin.z) * is;
+    const float rg = rho * is + 1e-4f;
+    if (gx < -rg || gy < -rg || gz < -rg) return true;
+    if (gx > GB.size.x - 1 + rg || gy > GB.size.y - 1 + rg || gz > GB.size.z - 1 + rg) return true;
+    if (probe == 0.0) {
+        const int vx = min(max(__float2int_rn(gx), 0), GB.size.x - 1);
+        const int vy = min(max(__float2int_rn(gy), 0), GB.size.y - 1);
+        const int vz = min(max(__float2int_rn(gz), 0), GB.size.z - 1);
+        const float D = __ldg(SB.dist + GB.dist_off + fd_lin3(vx, vy, vz, GB.size));
+        const float sp = (float)GB.spacing;
+        const float dx = (gx - vx) * sp, dy = (gy - vy) * sp, dz = (gz - vz) * sp;
+        if (D - sqrtf(dx * dx + dy * dy + dz * dz) > rho) return true;
+    }
+    // the Lipschitz bound only helps where the field is distance-like
+    if (GB.lip < 4.0 && gx >= 0.f && gy >= 0.f && gz >= 0.f && gx < GB.size.x - 1 && gy < GB.size.y - 1 &&
+        gz < GB.size.z - 1) {
+        const int i0 = (int)gx, j0 = (int)gy, k0 = (int)gz;
         const long long sx = GB.size.x, sxy = (long long)GB.size.x * GB.size.y;
-        const double* S = SB.sdf + GB.sdf_off + (long long)k0 * sxy + (long long)j0 * sx + i0;
-        double p[8] = {__ldg(S), __ldg(S + 1), __ldg(S + sx), __ldg(S + sx + 1),
-                       __ldg(S + sxy), __ldg(S + sxy + 1), __ldg(S + sxy + sx), __ldg(S + sxy + sx + 1)};
-        const double phi = xm_trilinear(g.x - i0, g.y - j0, g.z - k0, p);
-        const double bound = GB.lip * rho;
-        if (phi - bound - probe > 1e-7 * (fabs(phi) + bound + probe) + 1e-12 * GB.spacing) return true;
+        const float* S = SB.sdf32 + GB.sdf_off + (long long)k0 * sxy + (long long)j0 * sx + i0;
+        const float fx = gx - i0, fy = gy - j0, fz = gz - k0;
+        const float c00 = __ldg(S) * (1.f - fx) + __ldg(S + 1) * fx;
+        const float c10 = __ldg(S + sx) * (1.f - fx) + __ldg(S + sx + 1) * fx;
+        const float c01 = __ldg(S + sxy) * (1.f - fx) + __ldg(S + sxy + 1) * fx;
+        const float c11 = __ldg(S + sxy + sx) * (1.f - fx) + __ldg(S + sxy + sx + 1) * fx;
+        const float phi = (c00 * (1.f - fy) + c10 * fy) * (1.f - fz) + (c01 * (1.f - fy) + c11 * fy) * fz;
+        const float bound = (float)GB.lip * rho + (float)probe;
+        if (phi - bound > 1e-5f * (fabsf(phi) + bound + (float)GB.spacing)) return true;
     }
     return false;
+}
+
+// Body-level cull of a candidate pair in single precision: A's bounding
+// sphere (radius rA about cA) against B, through B's rotation rows
+__device__ __forceinline__ bool body_culled32(const double3 cA, double rA, const double3 cB, const float4* RB,
+                                              bool radius_test, const FdGeo& GB, const GeoSetDev& SB, double probe)
+{
+    const float4 b0 = RB[0], b1 = RB[1], b2 = RB[2];
+    const float dx = (float)(cA.x - cB.x), dy = (float)(cA.y - cB.y), dz = (float)(cA.z - cB.z);
+    const float px = fmaf(b0.x, dx, fmaf(b1.x, dy, b2.x * dz));
+    const float py = fmaf(b0.y, dx, fmaf(b1.y, dy, b2.y * dz));
+    const float pz = fmaf(b0.z, dx, fmaf(b1.z, dy, b2.z * dz));
+    return sphere_culled(px, py, pz, (float)rA, radius_test, GB, SB, GB.radius, probe);
 }
 
 // cells that can hold the centre of a partner of a body of radius r centred
@@ -357,6 +386,20 @@ __device__ __forceinline__ void partner_search_range(double3 c, double reach, co
 constexpr int BROAD_LANES = FD_BROAD_LANES;  // lanes per particle in the cell-table broad phases
 constexpr int BROAD_CAND = 128;              // candidate slots staged per lane group and pass
 
+// d with its periodic components taken to the nearest image
+__device__ __forceinline__ double3 nl_min_image(double3 d, const NlDev& nl, const FdGrid& g)
+{
+    if (nl.periodic_x) {
+        const double L = g.maxb.x - g.minb.x;
+        d.x -= L * rint(d.x / L);
+    }
+    if (nl.periodic_y) {
+        const double L = g.maxb.y - g.minb.y;
+        d.y -= L * rint(d.y / L);
+    }
+    return d;
+}
+
 // Cell-table broad phase, BROAD_LANES lanes per particle A: the lanes read
 // the cells around A, share out the objects in them, test each (partner
 // order B > A for particle pairs, bounding spheres, body-level cull) and
@@ -367,11 +410,17 @@ constexpr int BROAD_CAND = 128;              // candidate slots staged per lane 
 // LIST: only the particles in alist[0 .. *acount) search (the ghost phases
 // list the particles whose search box reaches a ghost image; the others
 // were given empty segments by k_ghost_searchers).
-template <bool GHOST, bool LIST>
+//
+// NLB: build the neighbour list instead of the pairs (only when a rebuild
+// was requested): the sphere test is widened by the skin, the body-level
+// cull is left to the per-step filter, and each particle's partners go to its
+// fixed slice of the list.
+template <bool GHOST, bool LIST, bool NLB>
 __global__ void __launch_bounds__(TPB) k_broad_cells(ObjDev P, GeoSetDev G, CellTableDev T, const double3* gpos,
                                                      const int* occ, const int* alist, const int* acount,
-                                                     PairListDev L, unsigned int* flags, double probe)
+                                                     PairListDev L, NlDev nl, unsigned int* flags, double probe)
 {
+    if (NLB && nl.ctrl[0] == 0) return;
     __shared__ int s_list[TPB / BROAD_LANES][MAX_CAND];
     __shared__ int s_cand[TPB / BROAD_LANES][BROAD_CAND];
     const unsigned int full = 0xffffffffu;
@@ -394,7 +443,25 @@ __global__ void __launch_bounds__(TPB) k_broad_cells(ObjDev P, GeoSetDev G, Cell
         cA = P.pos[A];
         rA = G.geo[P.geo[A]].radius;
         // above the sphere test's own tolerance (rs * (1 + 2 BOUND_REL))
-        const double reach = (rA + (GHOST ? G.grid_rmax : G.rmax)) * (1.0 + 8.0 * BOUND_REL);
+        const double reach = (rA + (GHOST ? G.grid_rmax : G.rmax)) * (1.0 + 8.0 * BOUND_REL) + (NLB ? nl.skin : 0.0);
+        if (NLB && gl == 0) {
+            nl.ref[A] = cA;
+            nl.vis[A] = P.hash[A] >= 0;
+        }
+        if (NLB) {
+            // periodic directions: the cell range wraps around
+            const int3 s3 = T.g.size;
+            if (nl.periodic_x) {
+                lo.x = (int)floor((cA.x - reach - T.g.minb.x) * T.g.inv.x);
+                hi.x = (int)floor((cA.x + reach - T.g.minb.x) * T.g.inv.x);
+                if (hi.x - lo.x + 1 >= s3.x) { lo.x = 0; hi.x = s3.x - 1; }
+            }
+            if (nl.periodic_y) {
+                lo.y = (int)floor((cA.y - reach - T.g.minb.y) * T.g.inv.y);
+                hi.y = (int)floor((cA.y + reach - T.g.minb.y) * T.g.inv.y);
+                if (hi.y - lo.y + 1 >= s3.y) { lo.y = 0; hi.y = s3.y - 1; }
+            }
+        }
         partner_search_range(cA, reach, T.g, lo, hi);
         if (occ) {
             // only the cells that hold ghost images
@@ -410,7 +477,12 @@ __global__ void __launch_bounds__(TPB) k_broad_cells(ObjDev P, GeoSetDev G, Cell
         int cc = 0, cs = 0;
         const int ci = c0 + gl;
         if (ci < ncell) {
-            const int x = lo.x + ci % nx, y = lo.y + (ci / nx) % ny, z = lo.z + ci / (nx * ny);
+            int x = lo.x + ci % nx, y = lo.y + (ci / nx) % ny;
+            const int z = lo.z + ci / (nx * ny);
+            if (NLB) {
+                x = ((x % T.g.size.x) + T.g.size.x) % T.g.size.x;
+                y = ((y % T.g.size.y) + T.g.size.y) % T.g.size.y;
+            }
             const long long h = fd_lin3(x, y, z, T.g.size);
             cc = T.count[h];
             if (cc) cs = T.start[h];
@@ -440,9 +512,14 @@ __global__ void __launch_bounds__(TPB) k_broad_cells(ObjDev P, GeoSetDev G, Cell
                 if (GHOST || B > A) {
                     const FdGeo& GB = G.geo[P.geo[B]];
                     const double3 cB = GHOST ? gpos[B] : P.pos[B];
-                    const double rs = rA + (GHOST ? GB.grid_radius : GB.radius);
-                    if (lengthSq3(cA - cB) <= rs * rs * (1.0 + 4.0 * BOUND_REL))
-                        pass = !body_culled(cA, rA, cB, P.q[B], GB, G, probe);
+                    if (NLB) {
+                        const double rs = (rA + GB.radius) * (1.0 + 8.0 * BOUND_REL) + nl.skin;
+                        pass = lengthSq3(nl_min_image(cA - cB, nl, T.g)) <= rs * rs;
+                    } else {
+                        const double rs = rA + (GHOST ? GB.grid_radius : GB.radius);
+                        if (lengthSq3(cA - cB) <= rs * rs * (1.0 + 4.0 * BOUND_REL))
+                            pass = !body_culled32(cA, rA, cB, P.rot + 3ll * B, !GHOST, GB, G, probe);
+                    }
                 }
             }
             const unsigned int gm = (__ballot_sync(full, pass) >> gbase) & ((1u << BROAD_LANES) - 1u);
@@ -456,6 +533,20 @@ __global__ void __launch_bounds__(TPB) k_broad_cells(ObjDev P, GeoSetDev G, Cell
     __syncwarp();
     if (valid && cnt > MAX_CAND && gl == 0) set_flag(flags, FD_FLAG_NEIGHBOR_OVERFLOW);
     const int n = min(cnt, MAX_CAND);
+    if (NLB) {
+        static_assert(NL_MAX >= MAX_CAND, "a list slice holds every partner");
+        if (valid) {
+            for (int e = gl; e < n; e += BROAD_LANES) {
+                const int v = s_list[gb][e];
+                int r = 0;
+                for (int j = 0; j < n; ++j) r += (s_list[gb][j] < v);
+                nl.list[(long long)A * NL_MAX + r] = v;
+            }
+            if (gl == 0) nl.cnt[A] = n;
+        }
+        __syncwarp();
+        continue;
+    }
     int base = 0;
     if (valid && gl == 0 && n > 0) base = atomicAdd(L.n_pairs, n);
     base = __shfl_sync(full, base, 0, BROAD_LANES);
@@ -477,6 +568,77 @@ __global__ void __launch_bounds__(TPB) k_broad_cells(ObjDev P, GeoSetDev G, Cell
     }
     __syncwarp();
     }
+}
+
+// neighbour list: request a rebuild when a particle moved more than skin / 2
+// since the last build or changed visibility
+__global__ void k_nl_check(ObjDev P, NlDev nl, FdGrid g)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.n) return;
+    const double h = 0.5 * nl.skin;
+    const bool moved = lengthSq3(nl_min_image(P.pos[i] - nl.ref[i], nl, g)) > h * h;
+    const bool vis = P.hash[i] >= 0;
+    if (moved || vis != (nl.vis[i] != 0)) nl.ctrl[0] = 1;
+}
+
+// the pairs from the neighbour list: the exact sphere test and the
+// body-level cull of the cell search, on the listed partners (ascending, so
+// each particle's pairs come out in partner order)
+__global__ void __launch_bounds__(TPB) k_nl_filter(ObjDev P, GeoSetDev G, PairListDev L, NlDev nl,
+                                                   unsigned int* flags, double probe)
+{
+    constexpr int LN = 8;  // lanes per particle
+    const unsigned int full = 0xffffffffu;
+    const int lane = threadIdx.x & 31, gl = lane & (LN - 1), gbase = lane & ~(LN - 1);
+    const int A = (blockIdx.x * blockDim.x + threadIdx.x) / LN;
+    const bool valid = A < P.n;
+    double3 cA = mk3(0., 0., 0.);
+    double rA = 0.;
+    int cnt = 0;
+    if (valid) {
+        cA = P.pos[A];
+        rA = G.geo[P.geo[A]].radius;
+        cnt = nl.cnt[A];
+    }
+    const int cmax = __reduce_max_sync(full, cnt);
+    // two passes: count the partners that pass, then write them in order
+    unsigned long long passed = 0ull;  // bit e: entry e passed (entries < NL_MAX)
+    for (int e0 = 0; e0 < cmax; e0 += LN) {
+        const int e = e0 + gl;
+        bool pass = false;
+        if (valid && e < cnt) {
+            const int B = nl.list[(long long)A * NL_MAX + e];
+            if (P.hash[B] >= 0) {
+                const FdGeo& GB = G.geo[P.geo[B]];
+                const double3 cB = P.pos[B];
+                const double rs = rA + GB.radius;
+                if (lengthSq3(cA - cB) <= rs * rs * (1.0 + 4.0 * BOUND_REL))
+                    pass = !body_culled32(cA, rA, cB, P.rot + 3ll * B, true, GB, G, probe);
+            }
+        }
+        const unsigned int gm = (__ballot_sync(full, pass) >> gbase) & ((1u << LN) - 1u);
+        passed |= (unsigned long long)gm << e0;
+    }
+    const int n = __popcll(passed);
+    int base = 0;
+    if (valid && gl == 0 && n > 0) base = atomicAdd(L.n_pairs, n);
+    base = __shfl_sync(full, base, 0, LN);
+    const bool ok = base + n <= L.cap_pairs;
+    if (valid && n > 0 && !ok && gl == 0) set_flag(flags, FD_FLAG_PAIR_OVERFLOW);
+    if (valid && gl == 0) {
+        L.seg_off[A] = (ok && n > 0) ? base : 0;
+        L.seg_cnt[A] = ok ? n : 0;
+    }
+    if (valid && ok) {
+        for (int e = gl; e < cnt; e += LN) {
+            if (!((passed >> e) & 1ull)) continue;
+            const int r = __popcll(passed & ((1ull << e) - 1ull));
+            L.pairA[base + r] = A;
+            L.pairB[base + r] = nl.list[(long long)A * NL_MAX + e];
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) nl.ctrl[0] = 0;
 }
 
 // ghost phases: particles whose search box reaches the cells holding ghost
@@ -522,7 +684,7 @@ __global__ void k_broad_pw(ObjDev P, GeoSetDev G, ObjDev W, GeoSetDev GW, FdGrid
         const double rs = rA + GB.grid_radius;
         const double3 cW = W.pos[w];
         if (lengthSq3(cA - cW) > rs * rs * (1.0 + 4.0 * BOUND_REL)) continue;
-        if (body_culled(cA, rA, cW, W.q[w], GB, GW, probe)) continue;
+        if (body_culled32(cA, rA, cW, W.rot + 3ll * w, false, GB, GW, probe)) continue;
         if (cnt < MAX_CAND) buf[cnt++] = w;
         ++total;
     }
@@ -716,44 +878,7 @@ __device__ __forceinline__ bool cluster_culled(const float4 cl, const CullXf& x,
     const float px = fmaf(x.m[0], cx, fmaf(x.m[1], cy, fmaf(x.m[2], cz, x.t[0])));
     const float py = fmaf(x.m[3], cx, fmaf(x.m[4], cy, fmaf(x.m[5], cz, x.t[1])));
     const float pz = fmaf(x.m[6], cx, fmaf(x.m[7], cy, fmaf(x.m[8], cz, x.t[2])));
-    const float scale = (float)rB + cl.w + (float)GB.spacing;
-    const float margin = 2e-5f * scale;
-    const float rho = cl.w + margin;
-    if (Slave<KIND>::radius_test) {
-        const float lim = (float)rB + rho;
-        if (px * px + py * py + pz * pz > lim * lim) return true;
-    }
-    const float is = (float)GB.inv_spacing;
-    const float gx = (px - (float)GB.origin.x) * is, gy = (py - (float)GB.origin.y) * is,
-                gz = (pz - (float)GB.origin.z) * is;
-    const float rg = rho * is + 1e-4f;
-    if (gx < -rg || gy < -rg || gz < -rg) return true;
-    if (gx > GB.size.x - 1 + rg || gy > GB.size.y - 1 + rg || gz > GB.size.z - 1 + rg) return true;
-    if (probe == 0.0) {
-        const int vx = min(max(__float2int_rn(gx), 0), GB.size.x - 1);
-        const int vy = min(max(__float2int_rn(gy), 0), GB.size.y - 1);
-        const int vz = min(max(__float2int_rn(gz), 0), GB.size.z - 1);
-        const float D = __ldg(SB.dist + GB.dist_off + fd_lin3(vx, vy, vz, GB.size));
-        const float sp = (float)GB.spacing;
-        const float dx = (gx - vx) * sp, dy = (gy - vy) * sp, dz = (gz - vz) * sp;
-        if (D - sqrtf(dx * dx + dy * dy + dz * dz) > rho) return true;
-    }
-    // the Lipschitz bound only helps where the field is distance-like
-    if (GB.lip < 4.0 && gx >= 0.f && gy >= 0.f && gz >= 0.f && gx < GB.size.x - 1 && gy < GB.size.y - 1 &&
-        gz < GB.size.z - 1) {
-        const int i0 = (int)gx, j0 = (int)gy, k0 = (int)gz;
-        const long long sx = GB.size.x, sxy = (long long)GB.size.x * GB.size.y;
-        const float* S = SB.sdf32 + GB.sdf_off + (long long)k0 * sxy + (long long)j0 * sx + i0;
-        const float fx = gx - i0, fy = gy - j0, fz = gz - k0;
-        const float c00 = __ldg(S) * (1.f - fx) + __ldg(S + 1) * fx;
-        const float c10 = __ldg(S + sx) * (1.f - fx) + __ldg(S + sx + 1) * fx;
-        const float c01 = __ldg(S + sxy) * (1.f - fx) + __ldg(S + sxy + 1) * fx;
-        const float c11 = __ldg(S + sxy + sx) * (1.f - fx) + __ldg(S + sxy + sx + 1) * fx;
-        const float phi = (c00 * (1.f - fy) + c10 * fy) * (1.f - fz) + (c01 * (1.f - fy) + c11 * fy) * fz;
-        const float bound = (float)GB.lip * rho + (float)probe;
-        if (phi - bound > 1e-5f * (fabsf(phi) + bound + (float)GB.spacing)) return true;
-    }
-    return false;
+    return sphere_culled(px, py, pz, cl.w, Slave<KIND>::radius_test, GB, SB, rB, probe);
 }
 
 // Node filter: true when a node certainly fails the node predicate.  The
@@ -1770,9 +1895,20 @@ void launch_broad_pp(const ObjDev& P, const GeoSetDev& G, const CellTableDev& T,
 {
     cudaMemsetAsync(L.n_pairs, 0, sizeof(int), s);
     if (P.n > 0)
-        k_broad_cells<false, false><<<nblocks((long long)P.n * BROAD_LANES), TPB, 0, s>>>(
-            P, G, T, nullptr, nullptr, nullptr, nullptr, L, flags, probe);
+        k_broad_cells<false, false, false><<<nblocks((long long)P.n * BROAD_LANES), TPB, 0, s>>>(
+            P, G, T, nullptr, nullptr, nullptr, nullptr, L, NlDev{}, flags, probe);
 }
+void launch_broad_pp_nl(const ObjDev& P, const GeoSetDev& G, const CellTableDev& T, PairListDev& L, NlDev& nl,
+                        unsigned int* flags, double probe, cudaStream_t s)
+{
+    cudaMemsetAsync(L.n_pairs, 0, sizeof(int), s);
+    if (P.n <= 0) return;
+    k_nl_check<<<nblocks(P.n), TPB, 0, s>>>(P, nl, T.g);
+    k_broad_cells<false, false, true><<<nblocks((long long)P.n * BROAD_LANES), TPB, 0, s>>>(
+        P, G, T, nullptr, nullptr, nullptr, nullptr, L, nl, flags, probe);
+    k_nl_filter<<<nblocks((long long)P.n * 8), TPB, 0, s>>>(P, G, L, nl, flags, probe);
+}
+
 void launch_broad_pw(const ObjDev& P, const GeoSetDev& G, const ObjDev& W, const GeoSetDev& GW,
                      const FdGrid& wg, PairListDev& L, unsigned int* flags, double probe, cudaStream_t s)
 {
@@ -1787,8 +1923,8 @@ void launch_broad_ghost(const ObjDev& P, const GeoSetDev& G, const GhostDev& Gh,
     cudaMemsetAsync(Gh.nsearch, 0, sizeof(int), s);
     k_ghost_searchers<<<nblocks(P.n), TPB, 0, s>>>(P, G, Gh.cells.g, Gh.occ, L, Gh.searchers, Gh.nsearch);
     const long long groups = std::min<long long>(P.n, 148ll * 8 * (TPB / BROAD_LANES));
-    k_broad_cells<true, true><<<nblocks(groups * BROAD_LANES), TPB, 0, s>>>(
-        P, G, Gh.cells, Gh.pos, Gh.occ, Gh.searchers, Gh.nsearch, L, flags, probe);
+    k_broad_cells<true, true, false><<<nblocks(groups * BROAD_LANES), TPB, 0, s>>>(
+        P, G, Gh.cells, Gh.pos, Gh.occ, Gh.searchers, Gh.nsearch, L, NlDev{}, flags, probe);
 }
 
 void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& M, const ObjDev& W,

@@ -157,6 +157,24 @@ struct AdjRec {
     int cap;         // slots the record holds
 };
 
+// Verlet neighbour list of the particle-particle broad phase: per particle A,
+// up to NL_MAX partners B > A whose centre lay within rA + rB + skin at the
+// last build, ascending, by minimum-image distance in periodic directions
+// (so a particle that wraps keeps the partners it meets on the other side).
+// Rebuilt when a particle moved more than skin / 2 since then (minimum image)
+// or changed visibility (inside or outside the domain).  The per-step filter
+// applies the raw-position tests of the cell search.
+constexpr int NL_MAX = 64;
+struct NlDev {
+    double3* ref;   // positions at the last build
+    int* vis;       // visibility (cell hash >= 0) at the last build
+    int* cnt;       // partners per particle
+    int* list;      // NL_MAX per particle
+    int* ctrl;      // [0]: rebuild requested
+    double skin;
+    int periodic_x, periodic_y;  // distances and displacements by minimum image
+};
+
 struct StepArgs {
     AdjRec rec;      // recording of the list being launched (rec.hit null: off)
     double dt;
@@ -179,6 +197,9 @@ void launch_ghost_build(const ObjDev& P, GhostDev& Gh, int kind, cudaStream_t s)
 // pair lists
 void launch_broad_pp(const ObjDev& P, const GeoSetDev& G, const CellTableDev& T, PairListDev& L,
                      unsigned int* flags, double probe, cudaStream_t s);
+// the same pairs through the neighbour list (check, conditional rebuild, filter)
+void launch_broad_pp_nl(const ObjDev& P, const GeoSetDev& G, const CellTableDev& T, PairListDev& L, NlDev& nl,
+                        unsigned int* flags, double probe, cudaStream_t s);
 void launch_broad_pw(const ObjDev& P, const GeoSetDev& G, const ObjDev& W, const GeoSetDev& GW,
                      const FdGrid& wg, PairListDev& L, unsigned int* flags, double probe, cudaStream_t s);
 void launch_broad_ghost(const ObjDev& P, const GeoSetDev& G, const GhostDev& Gh, PairListDev& L,

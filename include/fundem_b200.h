@@ -50,6 +50,11 @@ int fundem_destroy(fundem_sim* sim);
    double precision.  No counterpart in the reference.  May be changed
    between steps. */
 int fundem_set_precision(fundem_sim* sim, int mode);
+/* neighbour list of the particle-particle broad phase: -1 (default) keeps
+   one from 8192 particles on, 0 searches the cell table every step, 1 keeps
+   one; both give the same pairs.  Takes effect at the next detection.
+   No counterpart in the reference. */
+int fundem_set_neighbour_list(fundem_sim* sim, int mode);
 /* when nonzero every step writes full contact records (point, normal,
    overlap, energies); otherwise only node, partner and sliding spring */
 int fundem_set_records(fundem_sim* sim, int full_records);
