@@ -30,7 +30,7 @@ EXPORTS = [
     "fundem_get_geometry", "fundem_get_grid", "fundem_launch_count", "fundem_set_profiling",
     "fundem_kernel_time", "fundem_work_counters", "fundem_prefix_sum", "fundem_prefix_sum_noalloc", "fundem_last_error",
     "fundem_adjoint_begin", "fundem_adjoint_forward", "fundem_adjoint_backward", "fundem_adjoint_end",
-    "fundem_step_graph", "fundem_set_neighbour_list",
+    "fundem_step_graph", "fundem_set_neighbour_list", "fundem_checkpoint_write", "fundem_checkpoint_read",
 ]
 TIMERS = {"integrate": 0, "hash": 1, "broad": 2, "narrow_pp": 3, "narrow_pw": 4, "ghost": 5, "reduce": 6}
 
@@ -107,6 +107,8 @@ def lib():
         L.fundem_adjoint_end.argtypes = [P]
         L.fundem_step_graph.argtypes = [P, I, D, C.c_double]
         L.fundem_set_neighbour_list.argtypes = [P, I]
+        L.fundem_checkpoint_write.argtypes = [P, C.c_char_p]
+        L.fundem_checkpoint_read.argtypes = [P, C.c_char_p]
         _lib = L
     return _lib
 
@@ -301,6 +303,14 @@ class Simulation:
 
     def set_periodic(self, x, y):
         self._check(self.L.fundem_set_periodic(self.h, int(bool(x)), int(bool(y))), "set_periodic")
+
+    def checkpoint_write(self, path):
+        """Write the state a restart needs (objects, contact history, bonds)."""
+        self._check(self.L.fundem_checkpoint_write(self.h, os.fsencode(path)), "checkpoint_write")
+
+    def checkpoint_read(self, path):
+        """Restore a checkpoint into a simulation with the same setup."""
+        self._check(self.L.fundem_checkpoint_read(self.h, os.fsencode(path)), "checkpoint_read")
 
     def set_neighbour_list(self, mode):
         """-1: from the particle count, 0: off, 1: on."""

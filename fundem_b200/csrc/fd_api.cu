@@ -11,6 +11,7 @@
 #include <cfloat>
 #include <functional>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <numeric>
@@ -2145,6 +2146,112 @@ int fundem_adjoint_backward(fundem_sim* s, const double* dl_dpos, const double* 
         FD_CUDA(cudaMemcpy(dl_dvel0, vb.p, sizeof(double) * 3 * np, cudaMemcpyDeviceToHost));
         FD_CUDA(cudaMemcpy(dl_dparams, pgrad.p, sizeof(double) * 4 * nmat, cudaMemcpyDeviceToHost));
         adj_restore(s, A.final_state);
+        FD_CUDA(cudaStreamSynchronize(s->stream));
+    });
+}
+
+// ---------------------------------------------------------------------------
+// checkpoint files: the state a restart needs, FP64 little-endian
+//   "FDCK" u32 version=1, i32 np, i32 nw, i32 nb,
+//   particles: pos, vel, angvel (3 np each), quat (4 np), force, torque (3 np each)
+//   walls: the same with nw
+//   per kind (5): i64 n, node (n i32), partner (n i32), spring (3n f64)
+//   bonds: activation (nb i32)
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+namespace {
+constexpr uint32_t CKPT_MAGIC = 0x4b434446u;  // "FDCK"
+
+template <typename T> void put(std::FILE* f, const T* p, size_t n)
+{
+    if (n && std::fwrite(p, sizeof(T), n, f) != n) throw std::runtime_error("checkpoint: write failed");
+}
+template <typename T> void get(std::FILE* f, T* p, size_t n)
+{
+    if (n && std::fread(p, sizeof(T), n, f) != n) throw std::runtime_error("checkpoint: file truncated");
+}
+}  // namespace
+
+extern "C" {
+
+int fundem_checkpoint_write(fundem_sim* s, const char* path)
+{
+    if (!s || !path) return FUNDEM_ERR_ARG;
+    if (!s->setup_done) return FUNDEM_ERR_STATE;
+    return guard(s, [&] {
+        AdjCheckpoint c;
+        adj_snapshot(s, c);
+        std::FILE* f = std::fopen(path, "wb");
+        if (!f) throw std::invalid_argument(std::string("cannot open ") + path);
+        try {
+            const uint32_t head[2] = {CKPT_MAGIC, 1u};
+            const int32_t counts[3] = {(int32_t)(c.pos.size() / 3), (int32_t)(c.wpos.size() / 3),
+                                       (int32_t)c.bond_active.size()};
+            put(f, head, 2);
+            put(f, counts, 3);
+            for (auto* v : {&c.pos, &c.vel, &c.angvel, &c.quat, &c.force, &c.torque, &c.wpos, &c.wvel, &c.wangvel,
+                            &c.wquat, &c.wforce, &c.wtorque})
+                put(f, v->data(), v->size());
+            for (int k = 0; k < FD_NKIND; ++k) {
+                const int64_t n = (int64_t)c.node[k].size();
+                put(f, &n, 1);
+                put(f, c.node[k].data(), c.node[k].size());
+                put(f, c.partner[k].data(), c.partner[k].size());
+                put(f, c.spring[k].data(), c.spring[k].size());
+            }
+            put(f, c.bond_active.data(), c.bond_active.size());
+        } catch (...) {
+            std::fclose(f);
+            throw;
+        }
+        if (std::fclose(f) != 0) throw std::runtime_error("checkpoint: write failed");
+    });
+}
+
+int fundem_checkpoint_read(fundem_sim* s, const char* path)
+{
+    if (!s || !path) return FUNDEM_ERR_ARG;
+    if (!s->setup_done) return FUNDEM_ERR_STATE;
+    return guard(s, [&] {
+        std::FILE* f = std::fopen(path, "rb");
+        if (!f) throw std::invalid_argument(std::string("cannot open ") + path);
+        AdjCheckpoint c;
+        try {
+            uint32_t head[2];
+            int32_t counts[3];
+            get(f, head, 2);
+            if (head[0] != CKPT_MAGIC || head[1] != 1u) throw std::invalid_argument("not a checkpoint file");
+            get(f, counts, 3);
+            int np = 0, nw = 0, nb = 0;
+            adj_check(fundem_num_objects(s, 0, &np));
+            adj_check(fundem_num_objects(s, 1, &nw));
+            adj_check(fundem_num_bonds(s, &nb));
+            if (counts[0] != np || counts[1] != nw || counts[2] != nb)
+                throw std::invalid_argument("checkpoint: object or bond counts differ from the simulation");
+            auto rd = [&](std::vector<double>& v, size_t n) { v.resize(n); get(f, v.data(), n); };
+            rd(c.pos, 3 * np); rd(c.vel, 3 * np); rd(c.angvel, 3 * np); rd(c.quat, 4 * np);
+            rd(c.force, 3 * np); rd(c.torque, 3 * np);
+            rd(c.wpos, 3 * nw); rd(c.wvel, 3 * nw); rd(c.wangvel, 3 * nw); rd(c.wquat, 4 * nw);
+            rd(c.wforce, 3 * nw); rd(c.wtorque, 3 * nw);
+            for (int k = 0; k < FD_NKIND; ++k) {
+                int64_t n = 0;
+                get(f, &n, 1);
+                if (n < 0 || n > (int64_t)1 << 31) throw std::invalid_argument("checkpoint: bad contact count");
+                c.node[k].resize(n); c.partner[k].resize(n); c.spring[k].resize(3 * n);
+                get(f, c.node[k].data(), n);
+                get(f, c.partner[k].data(), n);
+                get(f, c.spring[k].data(), 3 * n);
+            }
+            c.bond_active.resize(nb);
+            get(f, c.bond_active.data(), nb);
+        } catch (...) {
+            std::fclose(f);
+            throw;
+        }
+        std::fclose(f);
+        adj_restore(s, c);
+        s->detected = true;
         FD_CUDA(cudaStreamSynchronize(s->stream));
     });
 }

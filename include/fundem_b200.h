@@ -205,6 +205,15 @@ int fundem_adjoint_backward(fundem_sim* sim, const double* dl_dpos, const double
                             double* dl_dparams);
 int fundem_adjoint_end(fundem_sim* sim);
 
+/* Checkpoint files (FP64 binary): object state, the contact history of every
+   list and bond activation, which is all a restart needs besides the setup
+   calls.  read expects a simulation set up with the same materials,
+   geometries, objects and bonds (the counts are checked); a run continued
+   from a checkpoint repeats the uninterrupted run bit for bit.  The
+   reference keeps no restart files (its VTU output is not reloadable). */
+int fundem_checkpoint_write(fundem_sim* sim, const char* path);
+int fundem_checkpoint_read(fundem_sim* sim, const char* path);
+
 /* text of the last error a call on this simulation returned (empty when
    none); valid until the next call on it.  The reference prints such
    messages to std::cerr instead. */
