@@ -8,6 +8,7 @@ missing, the calls raise.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 
 import numpy as np
@@ -31,12 +32,23 @@ EXPORTS = [
     "fundem_kernel_time", "fundem_work_counters", "fundem_prefix_sum", "fundem_prefix_sum_noalloc", "fundem_last_error",
     "fundem_adjoint_begin", "fundem_adjoint_forward", "fundem_adjoint_backward", "fundem_adjoint_end",
     "fundem_step_graph", "fundem_set_neighbour_list", "fundem_checkpoint_write", "fundem_checkpoint_read",
+    "fundem_levelset_grid",
 ]
 TIMERS = {"integrate": 0, "hash": 1, "broad": 2, "narrow_pp": 3, "narrow_pw": 4, "ghost": 5, "reduce": 6}
 
 
 class FundemError(RuntimeError):
     pass
+
+
+class Shape(C.Structure):
+    """fundem_shape: a shape whose signed-distance grid the GPU evaluates."""
+    _fields_ = [("kind", C.c_int), ("positive_inside", C.c_int), ("param", C.c_double * 8),
+                ("n_vertices", C.c_int), ("vertices", C.POINTER(C.c_double)),
+                ("n_triangles", C.c_int), ("triangles", C.POINTER(C.c_int))]
+
+
+SHAPES = {"superellipsoid": 0, "sphere": 1, "box": 2, "cylinder": 3, "mesh": 4}
 
 
 class DeviceView(C.Structure):
@@ -109,6 +121,7 @@ def lib():
         L.fundem_set_neighbour_list.argtypes = [P, I]
         L.fundem_checkpoint_write.argtypes = [P, C.c_char_p]
         L.fundem_checkpoint_read.argtypes = [P, C.c_char_p]
+        L.fundem_levelset_grid.argtypes = [I, P, C.POINTER(Shape), D, C.c_double, IP, D]
         _lib = L
     return _lib
 
@@ -145,6 +158,44 @@ def mass_properties(density, origin, spacing, size, sdf):
     _check(lib().fundem_mass_properties(float(density), _d(_f64(origin, 3)), float(spacing), _i(_i32(size)),
                                         _d(_f64(sdf)), _d(m), _d(c), _d(I)), "mass_properties")
     return float(m[0]), c, I
+
+
+def grid_layout(bbox_min, bbox_max, spacing, padding=2):
+    """Origin and node counts of the grid Base::buildGrid lays over a bounding
+    box (LevelSetObjectGenerator.h:122-183): padded by max(1, padding)
+    spacings, snapped outwards to multiples of the spacing."""
+    h = float(spacing)
+    pad = max(1, int(padding)) * h
+    lo = [h * math.floor((float(a) - pad) / h) for a in bbox_min]
+    hi = [h * math.ceil((float(b) + pad) / h) for b in bbox_max]
+    size = [int(math.floor((b - a) / h + 0.5)) + 1 for a, b in zip(lo, hi)]
+    return np.array(lo), np.array(size, dtype=np.int32)
+
+
+def levelset_grid(kind, param, origin, spacing, size, positive_inside=False, vertices=None, triangles=None,
+                  device=-1, stream=None):
+    """Signed-distance grid of a shape, evaluated on the GPU (Base::buildGrid,
+    LevelSetObjectGenerator.h:122-224).  kind is one of SHAPES; param holds
+    rx, ry, rz, ee, en (superellipsoid), radius (sphere), lx, ly, lz (box),
+    A xyz, B xyz, radius (cylinder); a mesh takes vertices (n, 3) and
+    triangles (m, 3).  Returns the nx*ny*nz values, x fastest."""
+    sh = Shape()
+    sh.kind = SHAPES[kind] if isinstance(kind, str) else int(kind)
+    sh.positive_inside = 1 if positive_inside else 0
+    p = _f64(param) if param is not None else np.zeros(0)
+    for k in range(min(8, p.size)):
+        sh.param[k] = p[k]
+    keep = []
+    if vertices is not None:
+        v, t = _f64(vertices), _i32(triangles)
+        keep += [v, t]
+        sh.n_vertices, sh.vertices = v.size // 3, _d(v)
+        sh.n_triangles, sh.triangles = t.size // 3, _i(t)
+    n = _i32(size)
+    out = np.empty(int(np.prod(n.astype(np.int64))), dtype=np.float64)
+    _check(lib().fundem_levelset_grid(int(device), stream, C.byref(sh), _d(_f64(origin, 3)), float(spacing), _i(n),
+                                      _d(out)), "levelset_grid")
+    return out
 
 
 def prefix_sum(count, out=None, stream=None):

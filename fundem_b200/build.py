@@ -16,7 +16,9 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libfundem_b200.so")
-SOURCES = ["fd_kernels.cu", "fd_adjoint.cu", "fd_api.cu"]
+SOURCES = ["fd_kernels.cu", "fd_adjoint.cu", "fd_api.cu", "fd_levelset.cu"]
+# per-source flags: the grid generator rounds every add and multiply on its own
+SOURCE_FLAGS = {"fd_levelset.cu": ["-fmad=false"]}
 HEADERS = ["fd_internal.cuh", "fd_kernels.cuh", "fd_adjoint.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "nvcc")
@@ -40,7 +42,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     for src in SOURCES:
         obj = os.path.join(LIBDIR, src.replace(".cu", ".o"))
         cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
-               "-I", os.path.join(ROOT, "include"), *EXTRA, "-c", os.path.join(CSRC, src), "-o", obj]
+               "-I", os.path.join(ROOT, "include"), *EXTRA, *SOURCE_FLAGS.get(src, []), "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
             print(" ".join(cmd))

@@ -25,7 +25,12 @@ FUNDEM_HD inline double3 operator-(double3 a, double3 b) { return make_double3(a
 FUNDEM_HD inline double3 operator-(double3 a) { return make_double3(-a.x, -a.y, -a.z); }
 FUNDEM_HD inline double3 operator*(double3 a, double s) { return make_double3(a.x * s, a.y * s, a.z * s); }
 FUNDEM_HD inline double3 operator*(double s, double3 a) { return make_double3(s * a.x, s * a.y, s * a.z); }
-FUNDEM_HD inline double3 operator/(double3 a, double s) { return make_double3(a.x / s, a.y / s, a.z / s); }
+// division by a scalar multiplies by its reciprocal, as the reference's value type does (myVec.h:55-59)
+FUNDEM_HD inline double3 operator/(double3 a, double s)
+{
+    const double inv = 1.0 / s;
+    return make_double3(a.x * inv, a.y * inv, a.z * inv);
+}
 FUNDEM_HD inline double3& operator+=(double3& a, double3 b) { a = a + b; return a; }
 FUNDEM_HD inline double3& operator-=(double3& a, double3 b) { a = a - b; return a; }
 FUNDEM_HD inline double3& operator*=(double3& a, double s) { a = a * s; return a; }

@@ -71,6 +71,32 @@ int fundem_add_geometry(fundem_sim* sim, int wall, double mass, const double ine
 /* mass, centroid and inertia from a density (LSSolver.h:470-586; host) */
 int fundem_mass_properties(double density, const double origin[3], double spacing, const int size[3],
                            const double* sdf, double* mass, double centroid[3], double inertia[6]);
+
+/* Shapes whose signed-distance grid fundem_levelset_grid evaluates on the GPU
+   (the implicit functions of kernel/helper/LevelSetObjectGenerator.h). */
+enum fundem_shape_kind {
+    FUNDEM_SHAPE_SUPERELLIPSOID = 0, /* param: rx, ry, rz, ee, en                    (:1264-1354) */
+    FUNDEM_SHAPE_SPHERE = 1,         /* param: radius                                (:1628-1661) */
+    FUNDEM_SHAPE_BOX = 2,            /* param: lx, ly, lz, centred on the origin      (:1781-1867) */
+    FUNDEM_SHAPE_CYLINDER = 3,       /* param: A xyz, B xyz, radius                  (:2050-2131) */
+    FUNDEM_SHAPE_MESH = 4            /* closed triangle mesh: vertices, triangles    (:888-953) */
+};
+typedef struct fundem_shape {
+    int kind;               /* fundem_shape_kind */
+    int positive_inside;    /* 1: value and gradient negated (the walls' convention) */
+    double param[8];
+    int n_vertices;         /* FUNDEM_SHAPE_MESH: host arrays, xyz per vertex ... */
+    const double* vertices;
+    int n_triangles;        /* ... and three vertex indices per triangle */
+    const int* triangles;
+} fundem_shape;
+/* Base::buildGrid, LevelSetObjectGenerator.h:122-224, evaluated on the GPU:
+   sdf[i + nx (j + ny k)] at origin + (i, j, k) * spacing holds f / |grad f|
+   where |grad f| > 1e-12, else -spacing/2 (f <= 0) or +spacing/2.  sdf is a
+   host array of nx*ny*nz doubles; the call returns when it is filled.
+   device < 0 uses the current device; stream may be NULL. */
+int fundem_levelset_grid(int device, void* stream, const fundem_shape* shape, const double origin[3],
+                         double spacing, const int size[3], double* sdf);
 /* LSSolver::addParticle / addWall, LSSolver.h:88-104, 225-238 (host arrays) */
 int fundem_add_objects(fundem_sim* sim, int wall, int n, const double* pos, const double* vel, const double* angvel,
                        const double* quat, const int* mat, const int* geo);
