@@ -9,6 +9,7 @@
 // the turning phase (1): one line per particle, position, velocity, mass.
 #include <cmath>
 #include <cstdio>
+#include <filesystem>
 #include <cstdlib>
 #include <fstream>
 #include <random>
@@ -21,15 +22,17 @@
 
 struct Drum : public LSSolver {
     explicit Drum(const std::string& dir) : LSSolver(dir) {}
-    void writeState(const std::string& file, const std::vector<double>& mass)
+    bool writeState(const std::string& file, const std::vector<double>& mass)
     {
         const std::vector<double3>& x = getLSParticle().positionHostRef();
         const std::vector<double3>& v = getLSParticle().velocityHostRef();
         std::ofstream f(file);
+        if (!f) return false;
         f.precision(17);
         for (size_t i = 0; i < x.size(); ++i)
             f << x[i].x << ' ' << x[i].y << ' ' << x[i].z << ' ' << v[i].x << ' ' << v[i].y << ' ' << v[i].z << ' '
               << mass[i] << '\n';
+        return bool(f);
     }
 };
 
@@ -40,6 +43,7 @@ int main(int argc, char** argv)
     const double L = 0.5, R = 1.0, density = 1000.0;
     const double3 A = make_double3(-L, 0.0, 0.0), B = make_double3(L, 0.0, 0.0);
 
+    std::filesystem::create_directories(out);
     Drum drum(out);
     drum.addParticleMaterial(6.0e5, 1.8e5, 0.5, 0.5);
     drum.addWallMaterial(0.5, 0.5);
@@ -81,10 +85,10 @@ int main(int argc, char** argv)
     const double3 lo = make_double3(-L, -2.0 * R, -2.0 * R), hi = make_double3(L, 2.0 * R, 2.0 * R);
     const double3 gravity = make_double3(0.0, 0.0, -9.81);
     drum.solve(lo, hi, gravity, 1.0e-4, 1.0, 2, argc, argv);
-    drum.writeState(out + "/state_0.txt", mass);
+    if (!drum.writeState(out + "/state_0.txt", mass)) return 1;
     drum.setFixedAngularVelocityToWall(0, make_double3(pi(), 0.0, 0.0));
     drum.solve(lo, hi, gravity, 1.0e-4, 0.5, 2, argc, argv);
-    drum.writeState(out + "/state_1.txt", mass);
+    if (!drum.writeState(out + "/state_1.txt", mass)) return 1;
     std::printf("particles %zu\n", pack.centers.size());
     return 0;
 }

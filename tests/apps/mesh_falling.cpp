@@ -7,6 +7,7 @@
 //
 // Writes <outdir>/state.txt: one line per particle, position and velocity.
 #include <cstdio>
+#include <filesystem>
 #include <fstream>
 #include <string>
 #include <vector>
@@ -18,14 +19,16 @@
 
 struct Box : public LSSolver {
     explicit Box(const std::string& dir) : LSSolver(dir) {}
-    void writeState(const std::string& file)
+    bool writeState(const std::string& file)
     {
         const std::vector<double3>& x = getLSParticle().positionHostRef();
         const std::vector<double3>& v = getLSParticle().velocityHostRef();
         std::ofstream f(file);
+        if (!f) return false;
         f.precision(17);
         for (size_t i = 0; i < x.size(); ++i)
             f << x[i].x << ' ' << x[i].y << ' ' << x[i].z << ' ' << v[i].x << ' ' << v[i].y << ' ' << v[i].z << '\n';
+        return bool(f);
     }
 };
 
@@ -45,6 +48,7 @@ int main(int argc, char** argv)
     const double d = length(mesh.boundingBoxMax() - mesh.boundingBoxMin());
     const SpherePacking::Pack pack = SpherePacking::buildRegularInBox(lo, hi, 0.5 * d);
 
+    std::filesystem::create_directories(out);
     Box box(out);
     box.addParticleMaterial(6.0e5, 1.8e5, 0.5, 0.8);
     std::vector<double3> zero(pack.centers.size(), make_double3(0, 0, 0));
@@ -62,7 +66,7 @@ int main(int argc, char** argv)
                         wall.vertexPosition(), wall.triangleVertexIndex());
     box.addWall(0.5 * (lo + hi), make_double3(0, 0, 0), make_double3(0, 0, 0), make_quaternion(1, 0, 0, 0), 0, 0);
     box.solve(lo, hi, make_double3(0.0, 0.0, -9.81), 1.0e-4, 0.5, 2, argc, argv);
-    box.writeState(out + "/state.txt");
+    if (!box.writeState(out + "/state.txt")) return 1;
     std::printf("particles %zu\n", pack.centers.size());
     return 0;
 }
