@@ -18,6 +18,7 @@ LIB_PATH = os.path.join(HERE, "_lib", "libfundem_b200.so")
 
 FP64, FP32_MIXED = 0, 1
 PP, PW, GX, GY, GXY = 0, 1, 2, 3, 4
+GR90, GR180, GR270 = 5, 6, 7  # sector images
 
 # every symbol declared in include/fundem_b200.h
 EXPORTS = [
@@ -32,7 +33,7 @@ EXPORTS = [
     "fundem_kernel_time", "fundem_work_counters", "fundem_prefix_sum", "fundem_prefix_sum_noalloc", "fundem_last_error",
     "fundem_adjoint_begin", "fundem_adjoint_forward", "fundem_adjoint_backward", "fundem_adjoint_end",
     "fundem_step_graph", "fundem_set_neighbour_list", "fundem_checkpoint_write", "fundem_checkpoint_read",
-    "fundem_levelset_grid",
+    "fundem_levelset_grid", "fundem_set_periodic_sector",
 ]
 TIMERS = {"integrate": 0, "hash": 1, "broad": 2, "narrow_pp": 3, "narrow_pw": 4, "ghost": 5, "reduce": 6}
 
@@ -122,6 +123,7 @@ def lib():
         L.fundem_checkpoint_write.argtypes = [P, C.c_char_p]
         L.fundem_checkpoint_read.argtypes = [P, C.c_char_p]
         L.fundem_levelset_grid.argtypes = [I, P, C.POINTER(Shape), D, C.c_double, IP, D]
+        L.fundem_set_periodic_sector.argtypes = [P, I]
         _lib = L
     return _lib
 
@@ -282,6 +284,8 @@ class Simulation:
             s.add_bonds(B.master, B.slave, B.point, B.normal, B.radius, B.length, B.young, B.poisson,
                         B.tensile, B.cohesion, B.friction)
         s.set_periodic(sc.periodic_x, sc.periodic_y)
+        if getattr(sc, "periodic_sector", False):
+            s.set_periodic_sector(True)
         s.gravity = np.asarray(sc.gravity, float)
         s.dt = float(sc.dt)
         if setup:
@@ -354,6 +358,11 @@ class Simulation:
 
     def set_periodic(self, x, y):
         self._check(self.L.fundem_set_periodic(self.h, int(bool(x)), int(bool(y))), "set_periodic")
+
+    def set_periodic_sector(self, on=True):
+        """Quarter-sector periodicity about the z axis through the domain's
+        min corner (LSSolver::addPeriodicBoundarySector)."""
+        self._check(self.L.fundem_set_periodic_sector(self.h, int(bool(on))), "set_periodic_sector")
 
     def checkpoint_write(self, path):
         """Write the state a restart needs (objects, contact history, bonds)."""

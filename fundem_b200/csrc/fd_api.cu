@@ -541,8 +541,15 @@ struct Ghost {
     DevArray<long long> hash;
     DevArray<int> occ, searchers, nsearch;
     CellTable cells;
+    // sector images only: orientation, velocity, rotation rows
+    DevArray<fd_quat> q;
+    DevArray<double3> vel;
+    DevArray<float4> rot;
     bool active = false;
-    fd::GhostDev view() { return fd::GhostDev{pos.p, hash.p, cells.view(), occ.p, searchers.p, nsearch.p}; }
+    fd::GhostDev view()
+    {
+        return fd::GhostDev{pos.p, hash.p, cells.view(), occ.p, searchers.p, nsearch.p, q.p, vel.p, rot.p};
+    }
 };
 
 struct BondHost {
@@ -627,13 +634,14 @@ struct fundem_sim {
     ObjHost P, W;
     BondHost bonds;
     bool perX = false, perY = false;
+    bool sector = false;  // quarter-sector periodicity about z through the domain's min corner
     bool geo_dirty = true;
     bool setup_done = false;
     bool detected = false;
     FdGrid pgrid{}, wgrid{};
     CellTable ptab;
     PairList lists[FD_NKIND];
-    Ghost ghosts[3];
+    Ghost ghosts[6];  // X, Y, XY, then the sector images R90, R180, R270
     DevArray<int> scan_tmp;
     DevArray<int> wcount;  // wall-grid histogram (walls are looped over directly)
     DevArray<unsigned int> flags;
@@ -672,7 +680,7 @@ struct fundem_sim {
             rev_cnt.alloc(np); rev_off.alloc(np); rev_fill.alloc(np);
         }
         long long cap = 0;
-        for (int k : {FD_PP, FD_GX, FD_GY, FD_GXY})
+        for (int k : {FD_PP, FD_GX, FD_GY, FD_GXY, FD_GR90, FD_GR180, FD_GR270})
             if (lists[k].allocated) cap += lists[k].cap_pairs;
         cap = std::max<long long>(cap, 16);
         if (rev_code.n < (size_t)cap) rev_code.alloc((size_t)cap, false);
@@ -769,6 +777,7 @@ struct fundem_sim {
         a.gravity = make_double3(0, 0, 0);
         a.periodic_x = perX;
         a.periodic_y = perY;
+        a.sector = sector;
         a.records = records;
         a.flags = flags.p;
         a.stats = counters ? stats.p : nullptr;
@@ -851,14 +860,20 @@ struct fundem_sim {
         const int nw = W.n();
         // capacities (grown after the first detection)
         const int kinds_cap[FD_NKIND] = {std::max(64, 8 * np), std::max(64, np * std::min(nw, 4)),
+                                         std::max(64, np), std::max(64, np), std::max(64, np),
                                          std::max(64, np), std::max(64, np), std::max(64, np)};
         for (int k = 0; k < FD_NKIND; ++k) {
             if (!lists[k].allocated || counts_changed) lists[k].alloc(np, kinds_cap[k], 2 * kinds_cap[k]);
         }
-        const bool act[3] = {perX, perY, perX && perY};
-        for (int d = 0; d < 3; ++d) {
+        const bool act[6] = {perX, perY, perX && perY, sector, sector, sector};
+        for (int d = 0; d < 6; ++d) {
             ghosts[d].active = act[d];
             if (act[d]) {
+                if (d >= 3) {
+                    ghosts[d].q.alloc(std::max(np, 1));
+                    ghosts[d].vel.alloc(std::max(np, 1));
+                    ghosts[d].rot.alloc(3 * std::max(np, 1));
+                }
                 ghosts[d].pos.alloc(std::max(np, 1));
                 ghosts[d].hash.alloc(std::max(np, 1));
                 ghosts[d].occ.alloc(6);
@@ -926,10 +941,12 @@ struct fundem_sim {
                                     cudaMemcpyDeviceToDevice, stream));
         tend(FUNDEM_T_NARROW_PW);
         launches += 4;
-        PairListDev Lg[3];
-        if (perX || perY) {
+        PairListDev Lg[6];
+        if (perX || perY || sector) {
             tbegin(FUNDEM_T_GHOST);
-            const int kinds[3] = {FD_GX, FD_GY, FD_GXY};
+            // PeriodicBoundaryXY2D then PeriodicBoundarySector::updateGhostSpatialGrid
+            // (LSSolver.h:780-784), then the detection of every image set
+            const int kinds[6] = {FD_GX, FD_GY, FD_GXY, FD_GR90, FD_GR180, FD_GR270};
             for (int d = 0; d < 3; ++d) {
                 if (!ghosts[d].active) continue;
                 if (d == 0) { fd::launch_wrap(Pv, pgrid, 0, stream); launches++; }
@@ -941,7 +958,19 @@ struct fundem_sim {
                 fd::launch_cell_table(ghostobj, gh.cells, scan_tmp.p, scan_tmp.n, stream);
                 launches += 3;
             }
-            for (int d = 0; d < 3; ++d) {
+            if (sector) {
+                fd::launch_sector_wrap(Pv, pgrid, stream);
+                fd::GhostDev sv[3] = {ghosts[3].view(), ghosts[4].view(), ghosts[5].view()};
+                fd::launch_sector_images(Pv, sv, stream);
+                launches += 2;
+                for (int d = 3; d < 6; ++d) {
+                    ObjDev ghostobj = Pv;
+                    ghostobj.hash = ghosts[d].hash.p;
+                    fd::launch_cell_table(ghostobj, sv[d - 3].cells, scan_tmp.p, scan_tmp.n, stream);
+                    launches += 2;
+                }
+            }
+            for (int d = 0; d < 6; ++d) {
                 if (!ghosts[d].active) continue;
                 fd::GhostDev gh = ghosts[d].view();
                 Lg[d] = lists[kinds[d]].view();
@@ -1013,13 +1042,33 @@ struct fundem_sim {
     // demand its counters recorded and the detection runs again into the same
     // generation (same history source).  Overflow bits raised before the call
     // are kept for fundem_sync.
+    // Detection that grows the lists and detects again until nothing
+    // overflowed.  The periodic wraps inside a detection move bodies, so a
+    // repeated attempt starts again from the state the first one saw.
     void detect_fit(double probe)
     {
         const unsigned int grow_bits = FD_FLAG_PAIR_OVERFLOW | FD_FLAG_CONTACT_OVERFLOW;
         unsigned int f0 = 0;
         FD_CUDA(cudaStreamSynchronize(stream));
         FD_CUDA(cudaMemcpy(&f0, flags.p, sizeof(f0), cudaMemcpyDeviceToHost));
+        const size_t np = (size_t)P.n();
+        const bool wraps = (perX || perY || sector) && np > 0 && P.n_dev == (int)np;
+        DevArray<double3> keep_pos, keep_vel;
+        DevArray<fd_quat> keep_q;
+        if (wraps) {
+            keep_pos.alloc(np);
+            keep_vel.alloc(np);
+            keep_q.alloc(np);
+            FD_CUDA(cudaMemcpyAsync(keep_pos.p, P.d_pos.p, np * sizeof(double3), cudaMemcpyDeviceToDevice, stream));
+            FD_CUDA(cudaMemcpyAsync(keep_vel.p, P.d_vel.p, np * sizeof(double3), cudaMemcpyDeviceToDevice, stream));
+            FD_CUDA(cudaMemcpyAsync(keep_q.p, P.d_q.p, np * sizeof(fd_quat), cudaMemcpyDeviceToDevice, stream));
+        }
         for (int attempt = 0;; ++attempt) {
+            if (attempt > 0 && wraps) {
+                FD_CUDA(cudaMemcpyAsync(P.d_pos.p, keep_pos.p, np * sizeof(double3), cudaMemcpyDeviceToDevice, stream));
+                FD_CUDA(cudaMemcpyAsync(P.d_vel.p, keep_vel.p, np * sizeof(double3), cudaMemcpyDeviceToDevice, stream));
+                FD_CUDA(cudaMemcpyAsync(P.d_q.p, keep_q.p, np * sizeof(fd_quat), cudaMemcpyDeviceToDevice, stream));
+            }
             if (attempt > 0 || (f0 & grow_bits)) {
                 const unsigned int clear = f0 & ~grow_bits;
                 FD_CUDA(cudaMemcpy(flags.p, &clear, sizeof(clear), cudaMemcpyHostToDevice));
@@ -1381,6 +1430,13 @@ int fundem_set_periodic(fundem_sim* s, int x, int y)
     return FUNDEM_OK;
 }
 
+int fundem_set_periodic_sector(fundem_sim* s, int on)
+{
+    if (!s) return FUNDEM_ERR_ARG;
+    s->sector = on != 0;
+    return FUNDEM_OK;
+}
+
 int fundem_setup(fundem_sim* s, const double mn[3], const double mx[3])
 {
     if (!s || !mn || !mx) return FUNDEM_ERR_ARG;
@@ -1455,7 +1511,7 @@ int fundem_step_graph(fundem_sim* s, int nsteps, const double g[3], double dt)
         s->ensure_capacity();
         s->rev_view();
         const double key[8] = {g[0], g[1], g[2], dt, (double)s->precision, (double)s->records,
-                               (double)s->counters, (double)(s->perX * 2 + s->perY)};
+                               (double)s->counters, (double)(s->sector * 4 + s->perX * 2 + s->perY)};
         bool same = s->graph_exec && s->graph_steps == nsteps && s->graph_epoch == g_alloc_epoch.load();
         for (int k = 0; k < 8 && same; ++k) same = s->graph_key[k] == key[k];
         if (!same) {
@@ -1954,6 +2010,10 @@ int fundem_adjoint_begin(fundem_sim* s, int checkpoint_interval)
         s->last_error = "the adjoint differentiates the FP64 path";
         return FUNDEM_ERR_STATE;
     }
+    if (s->sector) {
+        s->last_error = "the adjoint does not differentiate through the turned images of sector periodicity";
+        return FUNDEM_ERR_STATE;
+    }
     for (const FdGeo& g : s->pgeo.table) {
         const fd_sym& I = g.inv_inertia;
         if (I.xx != 0.0 || I.yy != 0.0 || I.zz != 0.0 || I.xy != 0.0 || I.xz != 0.0 || I.yz != 0.0) {
@@ -2152,10 +2212,11 @@ int fundem_adjoint_backward(fundem_sim* s, const double* dl_dpos, const double* 
 
 // ---------------------------------------------------------------------------
 // checkpoint files: the state a restart needs, FP64 little-endian
-//   "FDCK" u32 version=1, i32 np, i32 nw, i32 nb,
+//   "FDCK" u32 version=2, i32 np, i32 nw, i32 nb,
 //   particles: pos, vel, angvel (3 np each), quat (4 np), force, torque (3 np each)
 //   walls: the same with nw
-//   per kind (5): i64 n, node (n i32), partner (n i32), spring (3n f64)
+//   version 2: i32 number of kinds K (version 1 files hold the first 5)
+//   per kind (K): i64 n, node (n i32), partner (n i32), spring (3n f64)
 //   bonds: activation (nb i32)
 // ---------------------------------------------------------------------------
 }  // extern "C"
@@ -2185,14 +2246,16 @@ int fundem_checkpoint_write(fundem_sim* s, const char* path)
         std::FILE* f = std::fopen(path, "wb");
         if (!f) throw std::invalid_argument(std::string("cannot open ") + path);
         try {
-            const uint32_t head[2] = {CKPT_MAGIC, 1u};
+            const uint32_t head[2] = {CKPT_MAGIC, 2u};
             const int32_t counts[3] = {(int32_t)(c.pos.size() / 3), (int32_t)(c.wpos.size() / 3),
                                        (int32_t)c.bond_active.size()};
+            const int32_t nkind = FD_NKIND;
             put(f, head, 2);
             put(f, counts, 3);
             for (auto* v : {&c.pos, &c.vel, &c.angvel, &c.quat, &c.force, &c.torque, &c.wpos, &c.wvel, &c.wangvel,
                             &c.wquat, &c.wforce, &c.wtorque})
                 put(f, v->data(), v->size());
+            put(f, &nkind, 1);
             for (int k = 0; k < FD_NKIND; ++k) {
                 const int64_t n = (int64_t)c.node[k].size();
                 put(f, &n, 1);
@@ -2221,7 +2284,8 @@ int fundem_checkpoint_read(fundem_sim* s, const char* path)
             uint32_t head[2];
             int32_t counts[3];
             get(f, head, 2);
-            if (head[0] != CKPT_MAGIC || head[1] != 1u) throw std::invalid_argument("not a checkpoint file");
+            if (head[0] != CKPT_MAGIC || (head[1] != 1u && head[1] != 2u))
+                throw std::invalid_argument("not a checkpoint file");
             get(f, counts, 3);
             int np = 0, nw = 0, nb = 0;
             adj_check(fundem_num_objects(s, 0, &np));
@@ -2234,7 +2298,10 @@ int fundem_checkpoint_read(fundem_sim* s, const char* path)
             rd(c.force, 3 * np); rd(c.torque, 3 * np);
             rd(c.wpos, 3 * nw); rd(c.wvel, 3 * nw); rd(c.wangvel, 3 * nw); rd(c.wquat, 4 * nw);
             rd(c.wforce, 3 * nw); rd(c.wtorque, 3 * nw);
-            for (int k = 0; k < FD_NKIND; ++k) {
+            int32_t nkind = 5;
+            if (head[1] == 2u) get(f, &nkind, 1);
+            if (nkind < 0 || nkind > FD_NKIND) throw std::invalid_argument("checkpoint: bad number of kinds");
+            for (int k = 0; k < nkind; ++k) {
                 int64_t n = 0;
                 get(f, &n, 1);
                 if (n < 0 || n > (int64_t)1 << 31) throw std::invalid_argument("checkpoint: bad contact count");

@@ -33,7 +33,10 @@ enum FdFlag : unsigned int {
 };
 
 // kinds of pair lists
-enum FdKind { FD_PP = 0, FD_PW = 1, FD_GX = 2, FD_GY = 3, FD_GXY = 4, FD_NKIND = 5 };
+// (GR90, GR180, GR270: the images of sector periodicity, turned about the z
+// axis through the domain's min corner)
+enum FdKind { FD_PP = 0, FD_PW = 1, FD_GX = 2, FD_GY = 3, FD_GXY = 4, FD_GR90 = 5, FD_GR180 = 6, FD_GR270 = 7,
+              FD_NKIND = 8 };
 
 struct __align__(16) fd_quat { double q0, q1, q2, q3; };
 struct fd_sym { double xx, yy, zz, xy, xz, yz; };

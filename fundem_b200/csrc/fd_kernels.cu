@@ -213,20 +213,12 @@ __global__ void k_wrap(ObjDev P, FdGrid g, int dim)
     P.pos[i] = dim == 0 ? wrap_x(P.pos[i], g) : wrap_y(P.pos[i], g);
 }
 
-__global__ void k_ghost_build(ObjDev P, GhostDev Gh, int kind)
+// calculateGhostHashKernel, including its z test against maxBound.y (:236):
+// an image outside the domain is hashed into the clamped boundary cell, an
+// image inside it is not a ghost
+__device__ __forceinline__ void image_hash(GhostDev& Gh, int i, double3 r)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.n) return;
     const FdGrid& g = Gh.cells.g;
-    const double3 p = P.pos[i];
-    const double3 ox = mk3(g.maxb.x - g.minb.x, 0., 0.), oy = mk3(0., g.maxb.y - g.minb.y, 0.);
-    const int3 c = fd_cell_of(p, g);
-    double3 r = p;
-    if (kind == FD_GX && c.x == 0) r = r + ox;
-    if (kind == FD_GY && c.y == 0) r = r + oy;
-    if (kind == FD_GXY && c.x == 0 && c.y == 0) r = r + (ox + oy);
-    Gh.pos[i] = r;
-    // calculateGhostHashKernel, including its z test against maxBound.y (:236)
     int3 gc = fd_cell_of(r, g);
     bool out = false;
     if (r.x < g.minb.x) { gc.x = 0; out = true; }
@@ -242,6 +234,150 @@ __global__ void k_ghost_build(ObjDev P, GhostDev Gh, int kind)
         atomicMin(&Gh.occ[0], gc.x); atomicMin(&Gh.occ[1], gc.y); atomicMin(&Gh.occ[2], gc.z);
         atomicMax(&Gh.occ[3], gc.x); atomicMax(&Gh.occ[4], gc.y); atomicMax(&Gh.occ[5], gc.z);
     }
+}
+
+__global__ void k_ghost_build(ObjDev P, GhostDev Gh, int kind)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.n) return;
+    const FdGrid& g = Gh.cells.g;
+    const double3 p = P.pos[i];
+    const double3 ox = mk3(g.maxb.x - g.minb.x, 0., 0.), oy = mk3(0., g.maxb.y - g.minb.y, 0.);
+    const int3 c = fd_cell_of(p, g);
+    double3 r = p;
+    if (kind == FD_GX && c.x == 0) r = r + ox;
+    if (kind == FD_GY && c.y == 0) r = r + oy;
+    if (kind == FD_GXY && c.x == 0 && c.y == 0) r = r + (ox + oy);
+    Gh.pos[i] = r;
+    image_hash(Gh, i, r);
+}
+
+// ---------------------------------------------------------------------------
+// sector periodicity, mySpatialGrid.cu:58-85, 154-213 (PeriodicBoundary.h:
+// 319-425): the quarter sector x >= min.x, y >= min.y repeats under quarter
+// turns about the z axis through the domain's min corner
+// ---------------------------------------------------------------------------
+// rotateVector, myVec.h:143-182 (device branch): v turned by the angle |om|
+// about om, v + (sin t / t) om x v + ((1 - cos t) / t^2) om x (om x v)
+__device__ __forceinline__ double3 turn_vec(double3 v, double3 om)
+{
+    const double th2 = dot3(om, om);
+    if (fd_is_zero(th2)) {
+        const double3 oxv = cross3(om, v), oo = cross3(om, oxv);
+        return v + oxv + 0.5 * oo;
+    }
+    const double inv = rsqrt(th2);
+    const double th = th2 * inv;
+    double sn, cs;
+    sincos(th, &sn, &cs);
+    const double A = sn * inv, B = (1.0 - cs) * (inv * inv);
+    const double3 oxv = cross3(om, v), oo = cross3(om, oxv);
+    return v + A * oxv + B * oo;
+}
+// rotateQuaternion, myQua.h:131-180: the turn about om times q, normalised
+__device__ __forceinline__ fd_quat turn_quat(fd_quat q, double3 om)
+{
+    const double th2 = om.x * om.x + om.y * om.y + om.z * om.z;
+    if (fd_is_zero(th2)) return q;
+    const double th = sqrt(th2);
+    const double inv = 1.0 / th;
+    const double ux = om.x * inv, uy = om.y * inv, uz = om.z * inv;
+    const double half = 0.5 * th;
+    const double c = cos(half), sn = sin(half);
+    const double r0 = c, r1 = sn * ux, r2 = sn * uy, r3 = sn * uz;
+    fd_quat o;
+    o.q0 = r0 * q.q0 - r1 * q.q1 - r2 * q.q2 - r3 * q.q3;
+    o.q1 = r0 * q.q1 + r1 * q.q0 + r2 * q.q3 - r3 * q.q2;
+    o.q2 = r0 * q.q2 - r1 * q.q3 + r2 * q.q0 + r3 * q.q1;
+    o.q3 = r0 * q.q3 + r1 * q.q2 - r2 * q.q1 + r3 * q.q0;
+    return fd_normalize_q(o);
+}
+// velocity, position about the min corner and orientation turned by a about z
+__device__ __forceinline__ void sector_turn(double3& v, double3& p, fd_quat& q, double3 mn, double a)
+{
+    const double3 om = mk3(0., 0., a);
+    v = turn_vec(v, om);
+    p = mn + turn_vec(p - mn, om);
+    q = turn_quat(q, om);
+}
+
+// position and velocity of a body as the sector wrap of this step leaves
+// them: the reference computes particle and wall contact forces after that
+// wrap from contacts detected before it, so the force side of those contacts
+// sees the turned body
+__device__ __forceinline__ void sector_fold(double3& p, double3& v, double3 mn)
+{
+    if (p.x < mn.x && p.y >= mn.y) {
+        const double3 om = mk3(0., 0., -0.5 * PI_D);
+        v = turn_vec(v, om);
+        p = mn + turn_vec(p - mn, om);
+    }
+    if (p.y < mn.y && p.x >= mn.x) {
+        const double3 om = mk3(0., 0., 0.5 * PI_D);
+        v = turn_vec(v, om);
+        p = mn + turn_vec(p - mn, om);
+    }
+}
+
+// a body that left through the x face comes back through the y face turned
+// by -90 degrees, and one that left through the y face by +90 degrees
+__global__ void k_sector_wrap(ObjDev P, double3 mn)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.n) return;
+    double3 v = P.vel[i], p = P.pos[i];
+    fd_quat q = P.q[i];
+    bool turned = false;
+    if (p.x < mn.x && p.y >= mn.y) { sector_turn(v, p, q, mn, -0.5 * PI_D); turned = true; }
+    if (p.y < mn.y && p.x >= mn.x) { sector_turn(v, p, q, mn, 0.5 * PI_D); turned = true; }
+    P.vel[i] = v;
+    P.pos[i] = p;
+    P.q[i] = q;
+    if (turned && P.rot) {
+        // the single-precision rotation rows of this step follow the turn
+        double R[9];
+        quat_matrix(q, R);
+        P.rot[3 * i + 0] = make_float4((float)R[0], (float)R[1], (float)R[2], 0.f);
+        P.rot[3 * i + 1] = make_float4((float)R[3], (float)R[4], (float)R[5], 0.f);
+        P.rot[3 * i + 2] = make_float4((float)R[6], (float)R[7], (float)R[8], 0.f);
+    }
+}
+
+__device__ __forceinline__ void image_store(GhostDev& Gh, int i, double3 p, double3 v, fd_quat q)
+{
+    Gh.pos[i] = p;
+    Gh.vel[i] = v;
+    Gh.q[i] = q;
+    double R[9];
+    quat_matrix(q, R);
+    Gh.rot[3 * i + 0] = make_float4((float)R[0], (float)R[1], (float)R[2], 0.f);
+    Gh.rot[3 * i + 1] = make_float4((float)R[3], (float)R[4], (float)R[5], 0.f);
+    Gh.rot[3 * i + 2] = make_float4((float)R[6], (float)R[7], (float)R[8], 0.f);
+    image_hash(Gh, i, p);
+}
+
+// images turned by +90 degrees (bodies in the first cell row in y), -90
+// degrees (first cell column in x) and 180 degrees (the corner cell); every
+// other image is a copy of its body
+__global__ void k_sector_images(ObjDev P, GhostDev R90, GhostDev R180, GhostDev R270)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.n) return;
+    const FdGrid& g = R90.cells.g;
+    const double3 p = P.pos[i], v = P.vel[i];
+    const fd_quat q = P.q[i];
+    const int3 c = fd_cell_of(p, g);
+    const bool row0 = c.y == 0, col0 = c.x == 0;
+    double3 pa = p, va = v;
+    fd_quat qa = q;
+    if (row0) sector_turn(va, pa, qa, g.minb, 0.5 * PI_D);
+    image_store(R90, i, pa, va, qa);
+    pa = p; va = v; qa = q;
+    if (row0 && col0) sector_turn(va, pa, qa, g.minb, PI_D);
+    image_store(R180, i, pa, va, qa);
+    pa = p; va = v; qa = q;
+    if (col0) sector_turn(va, pa, qa, g.minb, -0.5 * PI_D);
+    image_store(R270, i, pa, va, qa);
 }
 
 // ---------------------------------------------------------------------------
@@ -417,7 +553,7 @@ __device__ __forceinline__ double3 nl_min_image(double3 d, const NlDev& nl, cons
 // fixed slice of the list.
 template <bool GHOST, bool LIST, bool NLB>
 __global__ void __launch_bounds__(TPB) k_broad_cells(ObjDev P, GeoSetDev G, CellTableDev T, const double3* gpos,
-                                                     const int* occ, const int* alist, const int* acount,
+                                                     const float4* grot, const int* occ, const int* alist, const int* acount,
                                                      PairListDev L, NlDev nl, unsigned int* flags, double probe)
 {
     if (NLB && nl.ctrl[0] == 0) return;
@@ -518,7 +654,8 @@ __global__ void __launch_bounds__(TPB) k_broad_cells(ObjDev P, GeoSetDev G, Cell
                     } else {
                         const double rs = rA + (GHOST ? GB.grid_radius : GB.radius);
                         if (lengthSq3(cA - cB) <= rs * rs * (1.0 + 4.0 * BOUND_REL))
-                            pass = !body_culled32(cA, rA, cB, P.rot + 3ll * B, !GHOST, GB, G, probe);
+                            pass = !body_culled32(cA, rA, cB, (GHOST && grot ? grot : P.rot) + 3ll * B, !GHOST,
+                                                  GB, G, probe);
                     }
                 }
             }
@@ -755,6 +892,7 @@ struct NarrowArgs {
 template <int KIND> struct Slave;
 template <> struct Slave<FD_PP> {
     __device__ static double3 pos(const NarrowArgs& n, int j) { return n.P.pos[j]; }
+    __device__ static double3 vel(const NarrowArgs& n, int j) { return n.P.vel[j]; }
     __device__ static fd_quat q(const NarrowArgs& n, int j) { return n.P.q[j]; }
     __device__ static const float4* rot(const NarrowArgs& n, int j) { return n.P.rot + 3ll * j; }
     __device__ static const FdGeo& geo(const NarrowArgs& n, int j) { return n.G.geo[n.P.geo[j]]; }
@@ -765,6 +903,7 @@ template <> struct Slave<FD_PP> {
 };
 template <> struct Slave<FD_PW> {
     __device__ static double3 pos(const NarrowArgs& n, int j) { return n.W.pos[j]; }
+    __device__ static double3 vel(const NarrowArgs& n, int j) { return n.W.vel[j]; }
     __device__ static fd_quat q(const NarrowArgs& n, int j) { return n.W.q[j]; }
     __device__ static const float4* rot(const NarrowArgs& n, int j) { return n.W.rot + 3ll * j; }
     __device__ static const FdGeo& geo(const NarrowArgs& n, int j) { return n.GW.geo[n.W.geo[j]]; }
@@ -773,10 +912,18 @@ template <> struct Slave<FD_PW> {
     __device__ static const FdGrid& grid(const NarrowArgs& n) { return n.wgrid; }
     static constexpr bool radius_test = false;
 };
+// ghost images: translated images share their body's orientation and
+// velocity; sector images carry their own.  The angular velocity is always
+// the body's own, as in addGhostLevelSetParticleContactForceTorqueKernel
+// (contactKernel.cu:262), which does not turn it with the image.
 struct SlaveGhost {
     __device__ static double3 pos(const NarrowArgs& n, int j) { return n.gh.pos[j]; }
-    __device__ static fd_quat q(const NarrowArgs& n, int j) { return n.P.q[j]; }
-    __device__ static const float4* rot(const NarrowArgs& n, int j) { return n.P.rot + 3ll * j; }
+    __device__ static double3 vel(const NarrowArgs& n, int j) { return n.gh.vel ? n.gh.vel[j] : n.P.vel[j]; }
+    __device__ static fd_quat q(const NarrowArgs& n, int j) { return n.gh.q ? n.gh.q[j] : n.P.q[j]; }
+    __device__ static const float4* rot(const NarrowArgs& n, int j)
+    {
+        return (n.gh.rot ? n.gh.rot : n.P.rot) + 3ll * j;
+    }
     __device__ static const FdGeo& geo(const NarrowArgs& n, int j) { return n.G.geo[n.P.geo[j]]; }
     __device__ static const GeoSetDev& set(const NarrowArgs& n) { return n.G; }
     __device__ static long long hash(const NarrowArgs& n, int j) { return n.gh.hash[j]; }
@@ -1155,14 +1302,19 @@ __global__ void __launch_bounds__(TPB, FD_CONTACT_MIN_BLOCKS) k_contact(NarrowAr
                         if (n.a.periodic_x) { ri = wrap_x(ri, n.pgrid); if (KIND == FD_PP) rj = wrap_x(rj, n.pgrid); }
                         if (n.a.periodic_y) { ri = wrap_y(ri, n.pgrid); if (KIND == FD_PP) rj = wrap_y(rj, n.pgrid); }
                     }
-                    const double3 vi = n.P.vel[A], wi = n.P.angvel[A];
+                    double3 vi = n.P.vel[A], vjs = Slave<KIND>::vel(n, B);
+                    const double3 wi = n.P.angvel[A];
+                    if ((KIND == FD_PP || KIND == FD_PW) && n.a.sector) {
+                        sector_fold(ri, vi, n.pgrid.minb);
+                        if (KIND == FD_PP) sector_fold(rj, vjs, n.pgrid.minb);
+                    }
                     const int mi = n.P.mat[A];
                     const double invMi = GA.inv_mass;
                     const double kni = n.M.kn[mi], ksi = n.M.ks[mi], mui = n.M.mu[mi], ei = n.M.e[mi];
                     double3 vj, wj;
                     double effM = 0., mu, res;
                     if (KIND == FD_PW) {
-                        vj = n.W.vel[B];
+                        vj = vjs;
                         wj = n.W.angvel[B];
                         const int mj = n.W.mat[B];
                         mu = fmin(mui, n.MW.mu[mj]);
@@ -1171,7 +1323,7 @@ __global__ void __launch_bounds__(TPB, FD_CONTACT_MIN_BLOCKS) k_contact(NarrowAr
                         kn = kni;
                         ks = ksi;
                     } else {
-                        vj = n.P.vel[B];
+                        vj = vjs;
                         wj = n.P.angvel[B];
                         const double invMj = GB.inv_mass;
                         const int mj = n.P.mat[B];
@@ -1467,10 +1619,15 @@ __global__ void __launch_bounds__(TPB, FD_CONTACT_MIN_BLOCKS) k_contact32(Narrow
                         if (n.a.periodic_x) { ri = wrap_x(ri, n.pgrid); if (KIND == FD_PP) rj = wrap_x(rj, n.pgrid); }
                         if (n.a.periodic_y) { ri = wrap_y(ri, n.pgrid); if (KIND == FD_PP) rj = wrap_y(rj, n.pgrid); }
                     }
+                    double3 vid = n.P.vel[A], vjd = Slave<KIND>::vel(n, B);
+                    if ((KIND == FD_PP || KIND == FD_PW) && n.a.sector) {
+                        sector_fold(ri, vid, n.pgrid.minb);
+                        if (KIND == FD_PP) sector_fold(rj, vjd, n.pgrid.minb);
+                    }
                     const v3f armA = tof(cA - ri) + arm;
                     const v3f armB = tof(cA - rj) + arm;
-                    const v3f vi = tof(n.P.vel[A]), wi = tof(n.P.angvel[A]);
-                    const v3f vj = tof(KIND == FD_PW ? n.W.vel[B] : n.P.vel[B]);
+                    const v3f vi = tof(vid), wi = tof(n.P.angvel[A]);
+                    const v3f vj = tof(vjd);
                     const v3f wj = tof(KIND == FD_PW ? n.W.angvel[B] : n.P.angvel[B]);
                     const v3f vc = (vi + crossf(wi, armA)) - (vj + crossf(wj, armB));
                     const v3f F = linear_contact32(spring, vc, nrm, ov, (float)n.a.dt, kn, ks, mu, res, effM);
@@ -1551,14 +1708,16 @@ __global__ void k_pair_sum32(PairListDev L, int with_force)
 // ---------------------------------------------------------------------------
 // reverse index: pairs grouped by partner B, sorted by A
 // ---------------------------------------------------------------------------
-// kinds that have a partner side: particle pairs and the three ghost lists
-// (FD_GX, FD_GY, FD_GXY are consecutive)
+// kinds that have a partner side: particle pairs and the six ghost lists
+// (FD_GX .. FD_GR270 are consecutive)
+constexpr int REV_LISTS = 7;
 __host__ __device__ constexpr int rev_kind(int k) { return k == 0 ? FD_PP : FD_GX + k - 1; }
-static_assert(FD_GY == FD_GX + 1 && FD_GXY == FD_GX + 2, "ghost kinds are consecutive");
+static_assert(FD_GR270 == FD_GX + 5 && FD_NKIND == FD_GR270 + 1, "ghost kinds are consecutive and last");
+static_assert(FD_NKIND <= 8, "a reverse-index code keeps the kind in 3 bits");
 
 struct RevArgs {
-    PairListDev L[4];
-    int active[4];
+    PairListDev L[REV_LISTS];
+    int active[REV_LISTS];
     RevDev R;
     int n_obj;
 };
@@ -1567,7 +1726,7 @@ struct RevArgs {
 __device__ __forceinline__ bool rev_locate(const RevArgs& r, int idx, int& k, int& p)
 {
 #pragma unroll
-    for (k = 0; k < 4; ++k) {
+    for (k = 0; k < REV_LISTS; ++k) {
         if (!r.active[k]) continue;
         const int np = min(*r.L[k].n_pairs, r.L[k].cap_pairs);
         if (idx < np) { p = idx; return true; }
@@ -1890,13 +2049,27 @@ void launch_ghost_build(const ObjDev& P, GhostDev& Gh, int kind, cudaStream_t s)
     cudaMemsetAsync(Gh.occ + 3, 0xff, 3 * sizeof(int), s);
     if (P.n > 0) k_ghost_build<<<nblocks(P.n), TPB, 0, s>>>(P, Gh, kind);
 }
+void launch_sector_wrap(ObjDev& P, const FdGrid& g, cudaStream_t s)
+{
+    if (P.n > 0) k_sector_wrap<<<nblocks(P.n), TPB, 0, s>>>(P, g.minb);
+}
+void launch_sector_images(const ObjDev& P, GhostDev* R, cudaStream_t s)
+{
+    for (int d = 0; d < 3; ++d) {
+        cudaMemsetAsync(R[d].cells.count, 0, sizeof(int) * R[d].cells.g.num, s);
+        cudaMemsetAsync(R[d].occ, 0x7f, 3 * sizeof(int), s);
+        cudaMemsetAsync(R[d].occ + 3, 0xff, 3 * sizeof(int), s);
+    }
+    if (P.n > 0) k_sector_images<<<nblocks(P.n), TPB, 0, s>>>(P, R[0], R[1], R[2]);
+}
+
 void launch_broad_pp(const ObjDev& P, const GeoSetDev& G, const CellTableDev& T, PairListDev& L,
                      unsigned int* flags, double probe, cudaStream_t s)
 {
     cudaMemsetAsync(L.n_pairs, 0, sizeof(int), s);
     if (P.n > 0)
         k_broad_cells<false, false, false><<<nblocks((long long)P.n * BROAD_LANES), TPB, 0, s>>>(
-            P, G, T, nullptr, nullptr, nullptr, nullptr, L, NlDev{}, flags, probe);
+            P, G, T, nullptr, nullptr, nullptr, nullptr, nullptr, L, NlDev{}, flags, probe);
 }
 void launch_broad_pp_nl(const ObjDev& P, const GeoSetDev& G, const CellTableDev& T, PairListDev& L, NlDev& nl,
                         unsigned int* flags, double probe, cudaStream_t s)
@@ -1905,7 +2078,7 @@ void launch_broad_pp_nl(const ObjDev& P, const GeoSetDev& G, const CellTableDev&
     if (P.n <= 0) return;
     k_nl_check<<<nblocks(P.n), TPB, 0, s>>>(P, nl, T.g);
     k_broad_cells<false, false, true><<<nblocks((long long)P.n * BROAD_LANES), TPB, 0, s>>>(
-        P, G, T, nullptr, nullptr, nullptr, nullptr, L, nl, flags, probe);
+        P, G, T, nullptr, nullptr, nullptr, nullptr, nullptr, L, nl, flags, probe);
     k_nl_filter<<<nblocks((long long)P.n * 8), TPB, 0, s>>>(P, G, L, nl, flags, probe);
 }
 
@@ -1924,7 +2097,7 @@ void launch_broad_ghost(const ObjDev& P, const GeoSetDev& G, const GhostDev& Gh,
     k_ghost_searchers<<<nblocks(P.n), TPB, 0, s>>>(P, G, Gh.cells.g, Gh.occ, L, Gh.searchers, Gh.nsearch);
     const long long groups = std::min<long long>(P.n, 148ll * 8 * (TPB / BROAD_LANES));
     k_broad_cells<true, true, false><<<nblocks(groups * BROAD_LANES), TPB, 0, s>>>(
-        P, G, Gh.cells, Gh.pos, Gh.occ, Gh.searchers, Gh.nsearch, L, NlDev{}, flags, probe);
+        P, G, Gh.cells, Gh.pos, Gh.rot, Gh.occ, Gh.searchers, Gh.nsearch, L, NlDev{}, flags, probe);
 }
 
 void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& M, const ObjDev& W,
@@ -1951,6 +2124,15 @@ void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& 
         FD_NARROW_CASE(FD_GX)
         FD_NARROW_CASE(FD_GY)
         FD_NARROW_CASE(FD_GXY)
+    case FD_GR90:
+    case FD_GR180:
+    case FD_GR270:
+        // the sector images differ from the translated ones only in the state
+        // the ghost traits read, so they share the ghost kernels
+        k_select<FD_GX><<<grid, NARROW_WARPS * 32, 0, s>>>(n);
+        if (mixed) k_contact32<FD_GX><<<cgrid, TPB, 0, s>>>(n);
+        else k_contact<FD_GX><<<cgrid, TPB, 0, s>>>(n);
+        break;
     }
 #undef FD_NARROW_CASE
     if (mixed) k_pair_sum32<<<148 * 8, TPB, 0, s>>>(L, with_force);
@@ -1962,7 +2144,7 @@ void launch_reverse(const ObjDev& P, PairListDev* lists, const int* active, RevD
 {
     if (P.n <= 0) return;
     RevArgs r;
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < REV_LISTS; ++k) {
         r.L[k] = lists[rev_kind(k)];
         r.active[k] = active[rev_kind(k)];
     }

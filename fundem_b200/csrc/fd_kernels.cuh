@@ -115,6 +115,12 @@ struct GhostDev {
     int* occ;  // box of the cells holding ghost images: min x, y, z, max x, y, z
     int* searchers;  // particles whose search box reaches a ghost image
     int* nsearch;    // their count
+    // sector images only (null for the translated X/Y images, which share the
+    // particle's orientation and velocity): orientation, velocity and the
+    // single-precision rotation rows of each image
+    fd_quat* q;
+    double3* vel;
+    float4* rot;
 };
 
 struct BondDev {
@@ -181,6 +187,7 @@ struct StepArgs {
     double probe;      // contact when overlap >= -probe (0 in a timestep)
     double3 gravity;
     int periodic_x, periodic_y;
+    int sector;      // sector periodicity (the force side of particle and wall contacts folds bodies)
     int records;
     unsigned int* flags;
     unsigned long long* stats;  // optional: pairs, clusters, clusters kept, contacts (narrow kernels)
@@ -193,6 +200,10 @@ void launch_hash_count(const ObjDev& O, CellTableDev& T, cudaStream_t s);
 void launch_cell_table(ObjDev& O, CellTableDev& T, int* scan_tmp, size_t scan_tmp_ints, cudaStream_t s);
 void launch_wrap(ObjDev& P, const FdGrid& g, int dim, cudaStream_t s);
 void launch_ghost_build(const ObjDev& P, GhostDev& Gh, int kind, cudaStream_t s);
+// sector periodicity: turn bodies that left the quarter sector back in, then
+// build the three turned image sets (R90, R180, R270)
+void launch_sector_wrap(ObjDev& P, const FdGrid& g, cudaStream_t s);
+void launch_sector_images(const ObjDev& P, GhostDev* R, cudaStream_t s);
 
 // pair lists
 void launch_broad_pp(const ObjDev& P, const GeoSetDev& G, const CellTableDev& T, PairListDev& L,

@@ -198,14 +198,12 @@ public:
 
     void addPeriodicBoundaryXD() { perX_ = true; report(fundem_set_periodic(sim_, perX_, perY_), "periodic"); }
     void addPeriodicBoundaryYD() { perY_ = true; report(fundem_set_periodic(sim_, perX_, perY_), "periodic"); }
-    void addPeriodicBoundarySector()
-    {
-        std::cerr << "[LSSolver] addPeriodicBoundarySector: sector periodicity is not available" << std::endl;
-    }
+    void addPeriodicBoundarySector() { report(fundem_set_periodic_sector(sim_, 1), "addPeriodicBoundarySector"); }
     void removePeriodicBoundary()
     {
         perX_ = perY_ = false;
         report(fundem_set_periodic(sim_, 0, 0), "removePeriodicBoundary");
+        report(fundem_set_periodic_sector(sim_, 0), "removePeriodicBoundary");
     }
 
     // ---------------------------------------------------------------- run

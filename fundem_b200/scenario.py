@@ -282,6 +282,9 @@ class Scenario:
     bonds: Bonds = field(default_factory=Bonds.empty)
     periodic_x: bool = False
     periodic_y: bool = False
+    # quarter-sector periodicity about the z axis through domain_min
+    # (LSSolver::addPeriodicBoundarySector)
+    periodic_sector: bool = False
     name: str = "scenario"
 
     def copy(self) -> "Scenario":

@@ -33,7 +33,8 @@ typedef enum {
 
 enum { FUNDEM_FP64 = 0, FUNDEM_FP32_MIXED = 1 };
 /* contact list kinds */
-enum { FUNDEM_PP = 0, FUNDEM_PW = 1, FUNDEM_GX = 2, FUNDEM_GY = 3, FUNDEM_GXY = 4 };
+enum { FUNDEM_PP = 0, FUNDEM_PW = 1, FUNDEM_GX = 2, FUNDEM_GY = 3, FUNDEM_GXY = 4,
+       FUNDEM_GR90 = 5, FUNDEM_GR180 = 6, FUNDEM_GR270 = 7 /* sector images */ };
 
 const char* fundem_version(void);
 const char* fundem_status_string(int status);
@@ -111,6 +112,15 @@ int fundem_add_bonds(fundem_sim* sim, int n, const int* master, const int* slave
                      const double* poisson, const double* tensile, const double* cohesion, const double* friction);
 /* addPeriodicBoundaryXD / YD / removePeriodicBoundary, LSSolver.h:384-414 */
 int fundem_set_periodic(fundem_sim* sim, int x, int y);
+/* addPeriodicBoundarySector / removePeriodicBoundary, LSSolver.h:410-424
+   (PeriodicBoundary.h:319-425): the quarter sector x >= min.x, y >= min.y
+   of the domain repeats under quarter turns about the z axis through the
+   domain's min corner.  A body leaving through one face comes back through
+   the other, turned; bodies next to the faces meet images turned by +90, 180
+   and -90 degrees (contact kinds 5, 6, 7).  As in the reference, an image's
+   angular velocity is its body's, not turned, and a contact's reaction goes
+   to the body unturned.  Takes effect at the next fundem_setup. */
+int fundem_set_periodic_sector(fundem_sim* sim, int on);
 
 /* LSSolver::upload, LSSolver.h:692-703: domain and grids, template tables,
    device state.  May be called again (multi-phase runs): state already on

@@ -317,7 +317,8 @@ struct orc_world {
     obj_set P, W;
     contacts PP, PW;
     ghost_t GX, GY, GXY;
-    int perX, perY;
+    ghost_t R90, R180, R270; /* sector images, PeriodicBoundary.h:319-425 */
+    int perX, perY, sector;
     bonds_t B;
 };
 
@@ -353,6 +354,7 @@ void orc_destroy(orc_world* w)
     free_obj(&w->P); free_obj(&w->W);
     free_contacts(&w->PP); free_contacts(&w->PW);
     free_ghost(&w->GX); free_ghost(&w->GY); free_ghost(&w->GXY);
+    free_ghost(&w->R90); free_ghost(&w->R180); free_ghost(&w->R270);
     bonds_t* b = &w->B;
     free(b->master); free(b->slave); free(b->active); free(b->point); free(b->radius);
     free(b->L0); free(b->B1); free(b->B2); free(b->B3); free(b->B4); free(b->ts); free(b->coh);
@@ -614,6 +616,7 @@ int orc_add_bond(orc_world* w, int master, int slave, const double point[3],
 }
 
 void orc_set_periodic(orc_world* w, int x, int y) { w->perX = x ? 1 : 0; w->perY = y ? 1 : 0; }
+void orc_set_sector(orc_world* w, int on) { w->sector = on ? 1 : 0; }
 
 /* spatialGrid::set, mySpatialGrid.h:212-240 */
 static void grid_set(grid_t* g, d3 minb, d3 maxb, double cell)
@@ -707,6 +710,11 @@ int orc_setup(orc_world* w, const double minb[3], const double maxb[3])
     else w->GY.active = 0;
     if (w->perX && w->perY) ghost_init(&w->GXY, &w->P);
     else w->GXY.active = 0;
+    ghost_t* sec[3] = {&w->R90, &w->R180, &w->R270};
+    for (int d = 0; d < 3; ++d) {
+        if (w->sector) ghost_init(sec[d], &w->P);
+        else sec[d]->active = 0;
+    }
     return 0;
 }
 
@@ -1202,6 +1210,91 @@ static void ghost_grid(ghost_t* gh)
     }
     build_start_end(gh->n, gh->hash_value, gh->hash_index, &gh->g);
 }
+/* rotateVector, myVec.h:143-182 (host branch): v rotated by the angle |om|
+   about om, exp([om]x) v = v + (sin t / t) om x v + ((1 - cos t) / t^2) om x (om x v) */
+static d3 rot_by_omega(d3 v, d3 om)
+{
+    const double th2 = dot(om, om);
+    if (is_zero(th2)) {
+        const d3 oxv = cross(om, v), oo = cross(om, oxv);
+        return add(add(v, oxv), mul(oo, 0.5));
+    }
+    const double inv = 1.0 / sqrt(th2);
+    const double th = th2 * inv;
+    const double sn = sin(th), cs = cos(th);
+    const double A = sn * inv, B = (1.0 - cs) * (inv * inv);
+    const d3 oxv = cross(om, v), oo = cross(om, oxv);
+    return add(add(v, mul(oxv, A)), mul(oo, B));
+}
+/* rotateQuaternion, myQua.h:131-180: r(om) * q (Hamilton product), normalised */
+static qt rot_quat_by_omega(qt q, d3 om)
+{
+    const double th2 = om.x * om.x + om.y * om.y + om.z * om.z;
+    if (is_zero(th2)) return q;
+    const double th = sqrt(th2);
+    const double inv = 1.0 / th;
+    const double ux = om.x * inv, uy = om.y * inv, uz = om.z * inv;
+    const double half = 0.5 * th;
+    const double c = cos(half), sn = sin(half);
+    const double r0 = c, r1 = sn * ux, r2 = sn * uy, r3 = sn * uz;
+    qt o;
+    o.q0 = r0 * q.q0 - r1 * q.q1 - r2 * q.q2 - r3 * q.q3;
+    o.q1 = r0 * q.q1 + r1 * q.q0 + r2 * q.q3 - r3 * q.q2;
+    o.q2 = r0 * q.q2 - r1 * q.q3 + r2 * q.q0 + r3 * q.q1;
+    o.q3 = r0 * q.q3 + r1 * q.q2 - r2 * q.q1 + r3 * q.q0;
+    return normalizeq(o);
+}
+/* velocity, position about the domain's min corner, and orientation of a body
+   turned by the angle a about z */
+static void sector_turn(d3* v, d3* p, qt* q, d3 mn, double a)
+{
+    const d3 om = v3(0., 0., a);
+    *v = rot_by_omega(*v, om);
+    *p = add(mn, rot_by_omega(sub(*p, mn), om));
+    *q = rot_quat_by_omega(*q, om);
+}
+/* updateVelocityPositionOrientationOutOfSectorKernel, mySpatialGrid.cu:58-85:
+   a body that left the quarter sector x >= min.x, y >= min.y through one face
+   comes back through the other */
+static void sector_wrap(obj_set* P)
+{
+    const d3 mn = P->g.minb;
+    for (int i = 0; i < P->n; ++i) {
+        d3 v = P->vel[i], p = P->pos[i];
+        qt q = P->q[i];
+        if (p.x < mn.x && p.y >= mn.y) sector_turn(&v, &p, &q, mn, -0.5 * PI);
+        if (p.y < mn.y && p.x >= mn.x) sector_turn(&v, &p, &q, mn, 0.5 * PI);
+        P->vel[i] = v;
+        P->pos[i] = p;
+        P->q[i] = q;
+    }
+}
+/* calculateSectorGhostVelocityPositionOrientationKernel, mySpatialGrid.cu:154-213:
+   images turned by +90 degrees (bodies in the first cell row in y), -90
+   degrees (first cell column in x) and 180 degrees (the corner cell); every
+   other image is a copy of the body */
+static void sector_images(orc_world* w)
+{
+    const obj_set* P = &w->P;
+    const grid_t* g = &P->g;
+    for (int i = 0; i < P->n; ++i) {
+        const d3 p = P->pos[i], v = P->vel[i];
+        const qt q = P->q[i];
+        ghost_t* im[3] = {&w->R90, &w->R180, &w->R270};
+        for (int d = 0; d < 3; ++d) { im[d]->pos[i] = p; im[d]->vel[i] = v; im[d]->q[i] = q; }
+        int c[3];
+        cellpos(p, g->minb, g->inv, c);
+        if (c[1] == 0) {
+            sector_turn(&w->R90.vel[i], &w->R90.pos[i], &w->R90.q[i], g->minb, 0.5 * PI);
+            if (c[0] == 0) {
+                sector_turn(&w->R270.vel[i], &w->R270.pos[i], &w->R270.q[i], g->minb, -0.5 * PI);
+                sector_turn(&w->R180.vel[i], &w->R180.pos[i], &w->R180.q[i], g->minb, PI);
+            }
+        } else if (c[0] == 0) {
+            sector_turn(&w->R270.vel[i], &w->R270.pos[i], &w->R270.q[i], g->minb, -0.5 * PI);
+        }
+    }
+}
 static void update_ghost_grids(orc_world* w)
 {
     obj_set* P = &w->P;
@@ -1217,6 +1310,14 @@ static void update_ghost_grids(orc_world* w)
         memcpy(gh->q, P->q, sizeof(qt) * P->n);
         memcpy(gh->vel, P->vel, sizeof(d3) * P->n);
     }
+    /* PeriodicBoundarySector::updateGhostSpatialGrid, PeriodicBoundary.h:351-383 */
+    if (w->sector) {
+        sector_wrap(P);
+        sector_images(w);
+        ghost_grid(&w->R90);
+        ghost_grid(&w->R180);
+        ghost_grid(&w->R270);
+    }
 }
 
 static void detect_pp(orc_world* w)
@@ -1231,8 +1332,8 @@ static void detect_pw(orc_world* w)
 }
 static void detect_ghosts(orc_world* w)
 {
-    ghost_t* list[3] = {&w->GX, &w->GY, &w->GXY};
-    for (int d = 0; d < 3; ++d) {
+    ghost_t* list[6] = {&w->GX, &w->GY, &w->GXY, &w->R90, &w->R180, &w->R270};
+    for (int d = 0; d < 6; ++d) {
         ghost_t* gh = list[d];
         if (!gh->active) continue;
         detect_ctx cx = {&w->P, gh->pos, gh->q, w->P.geo, gh->hash_index, &gh->g, &w->P.geos, 0};
@@ -1249,7 +1350,7 @@ int orc_initial_detect(orc_world* w)
     update_grid(&w->W);
     detect_pp(w);
     detect_pw(w);
-    if (w->perX || w->perY) {
+    if (w->perX || w->perY || w->sector) {
         update_ghost_grids(w);
         detect_ghosts(w);
     }
@@ -1273,7 +1374,7 @@ int orc_detect_and_force(orc_world* w, double dt)
     update_grid(&w->W);
     detect_pp(w);
     detect_pw(w);
-    if (w->perX || w->perY) {
+    if (w->perX || w->perY || w->sector) {
         update_ghost_grids(w);
         detect_ghosts(w);
     }
@@ -1283,6 +1384,9 @@ int orc_detect_and_force(orc_world* w, double dt)
     if (w->GX.active) run_contact_forces(w, &w->GX.c, ORC_GX, &w->GX, dt);
     if (w->GY.active) run_contact_forces(w, &w->GY.c, ORC_GY, &w->GY, dt);
     if (w->GXY.active) run_contact_forces(w, &w->GXY.c, ORC_GXY, &w->GXY, dt);
+    if (w->R90.active) run_contact_forces(w, &w->R90.c, ORC_GR90, &w->R90, dt);
+    if (w->R180.active) run_contact_forces(w, &w->R180.c, ORC_GR180, &w->R180, dt);
+    if (w->R270.active) run_contact_forces(w, &w->R270.c, ORC_GR270, &w->R270, dt);
     bond_forces(w);
     return 0;
 }
@@ -1358,6 +1462,9 @@ static contacts* kind_list(orc_world* w, int kind)
     case ORC_GX: return &w->GX.c;
     case ORC_GY: return &w->GY.c;
     case ORC_GXY: return &w->GXY.c;
+    case ORC_GR90: return &w->R90.c;
+    case ORC_GR180: return &w->R180.c;
+    case ORC_GR270: return &w->R270.c;
     }
     return NULL;
 }

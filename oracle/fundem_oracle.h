@@ -31,7 +31,7 @@ extern "C" {
 typedef struct orc_world orc_world;
 
 /* contact list kinds */
-enum { ORC_PP = 0, ORC_PW = 1, ORC_GX = 2, ORC_GY = 3, ORC_GXY = 4 };
+enum { ORC_PP = 0, ORC_PW = 1, ORC_GX = 2, ORC_GY = 3, ORC_GXY = 4, ORC_GR90 = 5, ORC_GR180 = 6, ORC_GR270 = 7 };
 
 orc_world* orc_create(void);
 void orc_destroy(orc_world* w);
@@ -57,6 +57,8 @@ int orc_add_bond(orc_world* w, int master, int slave, const double point[3],
                  const double normal[3], double radius, double L0, double E, double nu,
                  double tensile, double cohesion, double mu);
 void orc_set_periodic(orc_world* w, int x, int y);
+/* addPeriodicBoundarySector / removePeriodicBoundary, LSSolver.h:410-424 */
+void orc_set_sector(orc_world* w, int on);
 int orc_setup(orc_world* w, const double minb[3], const double maxb[3]);
 
 /* pre-loop detection (LSSolver.h:1093-1096 and the periodic variants) */

@@ -21,6 +21,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libfundem_oracle.so")
 
 PP, PW, GX, GY, GXY = 0, 1, 2, 3, 4
+GR90, GR180, GR270 = 5, 6, 7
 
 _lib = None
 
@@ -53,6 +54,7 @@ def lib():
         L.orc_add_bond.argtypes = [P, C.c_int, C.c_int, D, D, C.c_double, C.c_double, C.c_double,
                                    C.c_double, C.c_double, C.c_double, C.c_double]
         L.orc_set_periodic.argtypes = [P, C.c_int, C.c_int]
+        L.orc_set_sector.argtypes = [P, C.c_int]
         L.orc_setup.argtypes = [P, D, D]
         L.orc_initial_detect.argtypes = [P]
         L.orc_step.argtypes = [P, D, C.c_double]
@@ -211,6 +213,7 @@ class OracleWorld:
                            float(B.radius[k]), float(B.length[k]), float(B.young[k]), float(B.poisson[k]),
                            float(B.tensile[k]), float(B.cohesion[k]), float(B.friction[k]))
         L.orc_set_periodic(w, int(sc.periodic_x), int(sc.periodic_y))
+        L.orc_set_sector(w, int(getattr(sc, "periodic_sector", False)))
         o.gravity = np.asarray(sc.gravity, float)
         o.dt = float(sc.dt)
         if setup:

@@ -154,6 +154,13 @@ public:
         w.arr(fetch(B.Ut(), nB));
         w.arr(fetch(B.maxNormalStress(), nB));
         w.arr(fetch(B.maxShearStress(), nB));
+        // the sector images' lists, after the bonds, only when sector periodicity is on
+        PeriodicBoundarySector& ps = PeriodicBoundarySector_;
+        if (ps.ativateFlag_) {
+            dump_contacts(w, ps.R90_.ghostSolidInteraction_);
+            dump_contacts(w, ps.R180_.ghostSolidInteraction_);
+            dump_contacts(w, ps.R270_.ghostSolidInteraction_);
+        }
     }
 
     void dumpGeometry()
@@ -322,7 +329,8 @@ int main(int argc, char** argv)
         const double ts = r.get<double>(), coh = r.get<double>(), mu = r.get<double>();
         s.addBondedInteraction(m, sl, pt, nm, R, L0, E, nu, ts, coh, mu);
     }
-    if (perX) s.addPeriodicBoundaryXD();
+    if (perX & 1) s.addPeriodicBoundaryXD();
+    if (perX & 2) s.addPeriodicBoundarySector();
     if (perY) s.addPeriodicBoundaryYD();
 
     // numStep = size_t(Tmax/dt) + 1 and the loop runs numStep + 1 times

@@ -13,6 +13,8 @@ import numpy as np
 MAGIC = 0x43534446
 VERSION = 1
 KINDS = ("pp", "pw", "gx", "gy", "gxy")
+# the sector images' lists follow the bonds in a dump, when the run has them
+SECTOR_KINDS = ("gr90", "gr180", "gr270")
 
 
 class _W:
@@ -47,7 +49,9 @@ def write_reference_scenario(sc, path, n_steps, dump_steps=()):
     w.f64(*sc.gravity)
     w.f64(sc.dt)
     w.i64(n_steps)
-    w.i32(int(sc.periodic_x), int(sc.periodic_y))
+    # periodicity flags; bit 1 of the first one asks for sector periodicity
+    # (kept inside the x flag so that scenario files without it are unchanged)
+    w.i32(int(sc.periodic_x) | (2 if getattr(sc, "periodic_sector", False) else 0), int(sc.periodic_y))
     w.i32(len(dump_steps))
     for s in dump_steps:
         w.i32(s)
@@ -140,16 +144,22 @@ def read_dump(path):
     d["torque"] = r.arr("<f8", 3 * nP, (nP, 3))
     d["wall_pos"] = r.arr("<f8", 3 * nW, (nW, 3))
     d["wall_quat"] = r.arr("<f8", 4 * nW, (nW, 4))
-    for k in KINDS:
+
+    def contacts():
         n, = r.get("q")
-        c = dict(master=r.arr("<i4", n), slave=r.arr("<i4", n), point=r.arr("<f8", 3 * n, (n, 3)),
-                 normal=r.arr("<f8", 3 * n, (n, 3)), overlap=r.arr("<f8", n), spring=r.arr("<f8", 3 * n, (n, 3)),
-                 en=r.arr("<f8", n), es=r.arr("<f8", n))
-        d[k] = c
+        return dict(master=r.arr("<i4", n), slave=r.arr("<i4", n), point=r.arr("<f8", 3 * n, (n, 3)),
+                    normal=r.arr("<f8", 3 * n, (n, 3)), overlap=r.arr("<f8", n), spring=r.arr("<f8", 3 * n, (n, 3)),
+                    en=r.arr("<f8", n), es=r.arr("<f8", n))
+
+    for k in KINDS:
+        d[k] = contacts()
     nb, = r.get("q")
     d["bonds"] = dict(activated=r.arr("<i4", nb), point=r.arr("<f8", 3 * nb, (nb, 3)), un=r.arr("<f8", nb),
                       us=r.arr("<f8", nb), ub=r.arr("<f8", nb), ut=r.arr("<f8", nb), sn=r.arr("<f8", nb),
                       ss=r.arr("<f8", nb))
+    if r.o < len(r.b):
+        for k in SECTOR_KINDS:
+            d[k] = contacts()
     return d
 
 

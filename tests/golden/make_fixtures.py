@@ -82,7 +82,9 @@ def collect(src, cases):
             steps.append(s)
             for k in ("pos", "vel", "angvel", "quat", "force", "torque", "wall_pos", "wall_quat"):
                 out[f"s{s}_{k}"] = dump[k]
-            for kind in SIO.KINDS:
+            for kind in SIO.KINDS + SIO.SECTOR_KINDS:
+                if kind not in dump:
+                    continue
                 for k, v in dump[kind].items():
                     out[f"s{s}_{kind}_{k}"] = v
             for k, v in dump["bonds"].items():

@@ -9,6 +9,10 @@ arranged so every code path sees work:
   centre sits above the domain (invisible as a contact target).
 * `periodic`: a column periodic in x and y on a floor wall with a moving top
   platen and V-model bonds between near neighbours.
+* `sector`: a quarter-sector pile periodic about the z axis through the
+  domain's min corner (addPeriodicBoundarySector), cm-scale rotating bodies
+  on a floor wall; one body starts just outside the x face, so the first
+  step turns it back into the sector.
 * `pour_mm`: mm-scale config-0 shapes (the inverse inertia falls under the
   1e-30 determinant threshold and is zero).
 * `sphere`: the sphere-on-plane case of the reference's test app.
@@ -101,6 +105,34 @@ def periodic(seed=5, nx=4, ny=4, nz=3, grid_n=16, level=2):
                       periodic_x=True, periodic_y=True, name="periodic")
 
 
+def sector(seed=11, nx=4, ny=4, nz=2, grid_n=16, level=2):
+    rng = np.random.default_rng(seed)
+    geos = S.superellipsoid_templates(rng, 2, lo=8e-3, hi=12e-3, n=grid_n, level=level, density=2500.0,
+                                      explicit_mass=True)
+    pitch = 2 * max(S.node_radius(x) for x in geos) * 0.72
+    n = nx * ny * nz
+    box = np.array([nx, ny, nz]) * pitch
+    pos = S.lattice_positions(rng, n, np.zeros(3), box + 1e-9, pitch, 0.03 * pitch)
+    pos[:, 2] += 0.2 * pitch
+    # one body above the pile, just outside the x face
+    pos[0] = [-0.05 * pitch, 1.5 * pitch, box[2] + 0.4 * pitch]
+    # one body close to the axis, where it meets its own half-turned image
+    pos[nx * ny, :2] = 0.3 * pitch
+    geo = rng.integers(0, 2, n).astype(np.int32)
+    objs = S.Objects(pos, rng.normal(0, 0.2, (n, 3)), rng.normal(0, 10.0, (n, 3)), S.random_quaternions(rng, n),
+                     np.zeros(n, np.int32), geo)
+    ext = float(max(box[0], box[1])) * 2.2
+    wall_geos = [S.plane_wall_template(ext)]
+    walls = S.Objects(np.array([[0.5 * box[0], 0.5 * box[1], 0.15 * pitch]]), np.zeros((1, 3)), np.zeros((1, 3)),
+                      np.array([S.WALL_QUAT["+z"]]), np.zeros(1, np.int32), np.array([0], np.int32))
+    dom_lo = np.array([0.0, 0.0, -0.1 * pitch])
+    dom_hi = np.array([box[0], box[1], box[2] + 0.8 * pitch])
+    return S.Scenario(domain_min=dom_lo, domain_max=dom_hi, gravity=np.array([0.0, 0.0, -9.81]), dt=2e-5,
+                      particle_materials=[(2e4, 1.6e4, 0.5, 0.5)], wall_materials=[(0.5, 0.5)],
+                      particle_geometries=geos, wall_geometries=wall_geos, particles=objs, walls=walls,
+                      periodic_sector=True, name="sector")
+
+
 def pour_mm(seed=0, n=64, grid_n=32, level=3):
     sc = S.pour(n=n, n_templates=4, seed=seed, box=(11e-3, 11e-3, 11e-3), pitch=2.7e-3, jitter=0.05e-3,
                 init_speed=0.0, grid_n=grid_n, level=level, resolve=True, name="pour_mm")
@@ -114,7 +146,8 @@ def sphere():
     return S.sphere_on_plane()
 
 
-CASES = {"cluster": cluster, "periodic": periodic, "pour_mm": pour_mm, "sphere": sphere}
+CASES = {"cluster": cluster, "periodic": periodic, "pour_mm": pour_mm, "sphere": sphere, "sector": sector}
 # in-loop steps the reference runs per case and the steps it dumps
 REF_STEPS = {"cluster": (40, [1, 2, 3, 10, 11, 39, 40]), "periodic": (40, [1, 2, 3, 10, 11, 39, 40]),
+             "sector": (40, [1, 2, 3, 10, 11, 39, 40]),
              "pour_mm": (20, [1, 2, 3, 19, 20]), "sphere": (10000, [1, 2, 4500, 4550, 4600, 4650, 4700, 9000, 10000])}
