@@ -62,6 +62,11 @@ public:
     const std::vector<double3>& forceHostRef() { download(); return force_; }
     const std::vector<double3>& torqueHostRef() { download(); return torque_; }
     const std::vector<quaternion>& orientationHostRef() { download(); return q_; }
+    // the copies made by the last download(), without another transfer
+    const std::vector<double3>& positionHost() const { return pos_; }
+    const std::vector<double3>& velocityHost() const { return vel_; }
+    const std::vector<double3>& angularVelocityHost() const { return angvel_; }
+    const std::vector<quaternion>& orientationHost() const { return q_; }
 
 private:
     void refresh() const

@@ -7,10 +7,10 @@
 // device pointers of getLSParticle().
 //
 // Invalid input is reported on std::cerr and the call is skipped, as in the
-// reference.  Differences: solve() writes one particle VTU file per frame
-// (centres, velocities, angular velocities; the reference also writes the
-// surface mesh and contacts), and addPeriodicBoundarySector is not
-// available (the sector periodicity is not part of this library).
+// reference.  solve() writes the reference's frame files (LSSolver.h:717-744):
+// particle and wall surface meshes, particle centres, particle and wall
+// contacts and bonds, as VTK XML files (VTUWriter.h).  Contact lists are in
+// canonical (node, partner) order, which the reference does not fix.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -26,6 +26,7 @@
 #include "LSParticle.h"
 #include "SolidInteraction.h"
 #include "VBondedInteraction.h"
+#include "VTUWriter.h"
 
 class LSSolver {
 public:
@@ -39,7 +40,10 @@ public:
             std::cerr << "[LSSolver] cannot use CUDA device " << device << ": " << fundem_status_string(r)
                       << std::endl;
             sim_ = nullptr;
+            return;
         }
+        // every step keeps contact points, normals and energies for the frames
+        fundem_set_records(sim_, 1);
     }
     virtual ~LSSolver()
     {
@@ -63,11 +67,10 @@ public:
                              const std::vector<double3>& boundaryNodePosition,
                              const std::vector<int3>& boundaryNodeConnectivity)
     {
-        (void)boundaryNodeConnectivity;  // surface mesh: output only in the reference
         const double I[6] = {inertiaTensor.xx, inertiaTensor.yy, inertiaTensor.zz,
                              inertiaTensor.xy, inertiaTensor.xz, inertiaTensor.yz};
         addGeometry(false, mass, I, gridNodeOrigin, gridNodeSpacing, gridNodeSize, gridNodeSignedDistance,
-                    boundaryNodePosition, "addParticleGeometry");
+                    boundaryNodePosition, boundaryNodeConnectivity, "addParticleGeometry");
     }
 
     void addParticle(const double3 position, const double3 velocity, const double3 angularVelocity,
@@ -93,7 +96,6 @@ public:
                             const std::vector<double3>& boundaryNodePosition,
                             const std::vector<int3>& boundaryNodeConnectivity)
     {
-        (void)boundaryNodeConnectivity;
         const size_t n = position.size();
         if (velocity.size() != n || angularVelocity.size() != n || orientation.size() != n) {
             std::cerr << "[LSSolver] addParticleCluster: array sizes differ" << std::endl;
@@ -108,7 +110,7 @@ public:
         std::vector<double3> nodes(boundaryNodePosition);
         for (double3& p : nodes) p = p - cen;
         const int geo = addGeometry(false, mass, I, gridNodeOrigin - cen, gridNodeSpacing, gridNodeSize,
-                                    gridNodeSignedDistance, nodes, "addParticleCluster");
+                                    gridNodeSignedDistance, nodes, boundaryNodeConnectivity, "addParticleCluster");
         if (geo < 0) return;
         for (size_t i = 0; i < n; ++i)
             addParticle(position[i] + rotateVectorByQuaternion(orientation[i], cen), velocity[i],
@@ -127,17 +129,17 @@ public:
                          const std::vector<double3>& boundaryNodePosition,
                          const std::vector<int3>& boundaryNodeConnectivity)
     {
-        (void)boundaryNodeConnectivity;
         const double I[6] = {0, 0, 0, 0, 0, 0};
         addGeometry(true, 0.0, I, gridNodeOrigin, gridNodeSpacing, gridNodeSize, gridNodeSignedDistance,
-                    boundaryNodePosition, "addWallGeometry");
+                    boundaryNodePosition, boundaryNodeConnectivity, "addWallGeometry");
     }
 
     void addWall(const double3 position, const double3 velocity, const double3 angularVelocity,
                  const quaternion orientation, const int materialID, const int geometryID)
     {
-        report(fundem_add_objects(sim_, 1, 1, &position.x, &velocity.x, &angularVelocity.x, &orientation.q0,
-                                  &materialID, &geometryID), "addWall");
+        if (report(fundem_add_objects(sim_, 1, 1, &position.x, &velocity.x, &angularVelocity.x, &orientation.q0,
+                                      &materialID, &geometryID), "addWall"))
+            wallGeo_.push_back(geometryID);
     }
 
     void moveLSParticle(const size_t index, const double3 offSet)
@@ -171,9 +173,12 @@ public:
                               const double tensileStrength = 0., const double cohesion = 0.,
                               const double frictionCoefficient = 0.)
     {
-        report(fundem_add_bonds(sim_, 1, &masterObjectID, &slaveObjectID, &bondPoint.x, &bondNormal.x, &radius,
-                                &initialLength, &YoungsModulus, &poissonRatio, &tensileStrength, &cohesion,
-                                &frictionCoefficient), "addBondedInteraction");
+        if (report(fundem_add_bonds(sim_, 1, &masterObjectID, &slaveObjectID, &bondPoint.x, &bondNormal.x, &radius,
+                                    &initialLength, &YoungsModulus, &poissonRatio, &tensileStrength, &cohesion,
+                                    &frictionCoefficient), "addBondedInteraction")) {
+            bondMaster_.push_back(masterObjectID);
+            bondSlave_.push_back(slaveObjectID);
+        }
     }
 
     // one bond per current particle-particle node contact (LSSolver.h:347-380)
@@ -188,7 +193,8 @@ public:
         const std::vector<double3> point = I.contactPointHostRef();
         const std::vector<double3> normal = I.contactNormalHostRef();
         std::vector<int> nodeBase(particleGeo_.size() + 1, 0);
-        for (size_t i = 0; i < particleGeo_.size(); ++i) nodeBase[i + 1] = nodeBase[i] + geoNodes_[particleGeo_[i]];
+        for (size_t i = 0; i < particleGeo_.size(); ++i)
+            nodeBase[i + 1] = nodeBase[i] + (int)geoNodes_[particleGeo_[i]].size();
         for (size_t k = 0; k < node.size(); ++k) {
             const int i = (int)(std::upper_bound(nodeBase.begin(), nodeBase.end(), node[k]) - nodeBase.begin()) - 1;
             addBondedInteraction(i, slave[k], point[k], normal[k], radius, initialLength, YoungsModulus,
@@ -273,7 +279,8 @@ private:
     }
 
     int addGeometry(bool wall, double mass, const double I[6], double3 origin, double spacing, int3 size,
-                    const std::vector<double>& sdf, const std::vector<double3>& nodes, const char* what)
+                    const std::vector<double>& sdf, const std::vector<double3>& nodes,
+                    const std::vector<int3>& triangles, const char* what)
     {
         const int sz[3] = {size.x, size.y, size.z};
         if ((long long)sdf.size() != (long long)size.x * size.y * size.z) {
@@ -284,51 +291,159 @@ private:
         if (!report(fundem_add_geometry(sim_, wall, mass, I, &origin.x, spacing, sz, sdf.data(), (int)nodes.size(),
                                         nodes.empty() ? nullptr : &nodes[0].x, &id), what))
             return -1;
-        if (!wall) {
-            if ((int)geoNodes_.size() <= id) geoNodes_.resize(id + 1, 0);
-            geoNodes_[id] = (int)nodes.size();
-        }
+        // body-frame nodes and triangles of the template, for the frames
+        std::vector<std::vector<double3>>& N = wall ? wallGeoNodes_ : geoNodes_;
+        std::vector<std::vector<int3>>& T = wall ? wallGeoTris_ : geoTris_;
+        if ((int)N.size() <= id) { N.resize(id + 1); T.resize(id + 1); }
+        N[id] = nodes;
+        T[id] = triangles;
         return id;
     }
 
-    // one VTU file of particle centres per frame, in <dir>_phase<k>/LSParticle/
+    // the frame files of LSSolver::output (LSSolver.h:717-744), in
+    // <dir>_phase<k>/LSParticle, LSParticleInteraction, Wall and
+    // LSParticle-WallInteraction
     void output(size_t iFrame, size_t iStep, double time)
     {
         const std::string dir = dir_ + "_phase" + std::to_string(phase_);
-        const std::string sub = dir + "/LSParticle";
-        mkdir(dir.c_str(), 0755);
-        mkdir(sub.c_str(), 0755);
-        char name[64];
-        std::snprintf(name, sizeof(name), "/LSParticle_%04zu.vtu", iFrame);
+        const std::string dP = dir + "/LSParticle", dPI = dir + "/LSParticleInteraction", dW = dir + "/Wall",
+                          dWI = dir + "/LSParticle-WallInteraction";
+        for (const std::string& d : {dir, dP, dPI, dW, dWI}) mkdir(d.c_str(), 0755);
+        char num[16];
+        std::snprintf(num, sizeof(num), "_%04zu.vtu", iFrame);
+        bool ok = true;
         LSParticle_.download();
-        const std::vector<double3>& x = LSParticle_.positionHostRef();
-        const std::vector<double3>& v = LSParticle_.velocityHostRef();
-        const std::vector<double3>& w = LSParticle_.angularVelocityHostRef();
-        std::ofstream f(sub + name);
-        if (!f) {
-            std::cerr << "[LSSolver] cannot write " << sub + name << std::endl;
-            return;
+        Wall_.download();
+        ok &= writeMesh(dP + "/LSObjectMesh" + num, LSParticle_, particleGeo_, geoNodes_, geoTris_, time, iStep);
+        ok &= writeCentres(dP + "/Particle" + num, time, iStep);
+        ok &= writeContacts(dPI + "/LSInteraction" + num, FUNDEM_PP, time, iStep);
+        ok &= writeBonds(dPI + "/VBondedInteraction" + num, time, iStep);
+        ok &= writeMesh(dW + "/LSObjectMesh" + num, Wall_, wallGeo_, wallGeoNodes_, wallGeoTris_, time, iStep);
+        ok &= writeContacts(dWI + "/LSInteraction" + num, FUNDEM_PW, time, iStep);
+        if (!ok) std::cerr << "[LSSolver] cannot write the frame files in " << dir << std::endl;
+    }
+
+    static void put3(std::vector<float>& a, double3 v)
+    {
+        a.push_back(float(v.x));
+        a.push_back(float(v.y));
+        a.push_back(float(v.z));
+    }
+
+    // surface meshes of a set: nodes in the world frame with the body's
+    // velocity there, triangles, and the body index of each node
+    bool writeMesh(const std::string& file, const LSParticle& set, const std::vector<int>& objGeo,
+                   const std::vector<std::vector<double3>>& nodes, const std::vector<std::vector<int3>>& tris,
+                   double time, size_t step)
+    {
+        const std::vector<double3>& x = set.positionHost();
+        if (x.empty()) return true;
+        const std::vector<double3>& v = set.velocityHost();
+        const std::vector<double3>& w = set.angularVelocityHost();
+        const std::vector<quaternion>& q = set.orientationHost();
+        std::vector<float> points, vel;
+        std::vector<int32_t> id, conn, offs;
+        std::vector<uint8_t> types;
+        int32_t base = 0;
+        for (size_t i = 0; i < x.size() && i < objGeo.size(); ++i) {
+            const int g = objGeo[i];
+            for (const double3& b : nodes[g]) {
+                const double3 p = x[i] + rotateVectorByQuaternion(q[i], b);
+                put3(points, p);
+                put3(vel, v[i] + cross(w[i], p - x[i]));
+                id.push_back((int32_t)i);
+            }
+            for (const int3& t : tris[g]) {
+                conn.push_back(base + t.x);
+                conn.push_back(base + t.y);
+                conn.push_back(base + t.z);
+                offs.push_back((int32_t)conn.size());
+                types.push_back(5);  // triangle
+            }
+            base += (int32_t)nodes[g].size();
         }
-        f << "<?xml version=\"1.0\"?>\n<VTKFile type=\"UnstructuredGrid\" version=\"0.1\">\n<UnstructuredGrid>\n";
-        f << "<FieldData><DataArray type=\"Float64\" Name=\"TIME\" NumberOfTuples=\"1\" format=\"ascii\">" << time
-          << "</DataArray><DataArray type=\"Int64\" Name=\"STEP\" NumberOfTuples=\"1\" format=\"ascii\">" << iStep
-          << "</DataArray></FieldData>\n";
-        f << "<Piece NumberOfPoints=\"" << x.size() << "\" NumberOfCells=\"0\">\n<Points>\n"
-          << "<DataArray type=\"Float64\" NumberOfComponents=\"3\" format=\"ascii\">\n";
-        f.precision(17);
-        for (const double3& p : x) f << p.x << ' ' << p.y << ' ' << p.z << '\n';
-        f << "</DataArray>\n</Points>\n<PointData>\n";
-        auto vec = [&](const char* nm, const std::vector<double3>& a) {
-            f << "<DataArray type=\"Float64\" Name=\"" << nm << "\" NumberOfComponents=\"3\" format=\"ascii\">\n";
-            for (const double3& p : a) f << p.x << ' ' << p.y << ' ' << p.z << '\n';
-            f << "</DataArray>\n";
-        };
-        vec("velocity", v);
-        vec("angularVelocity", w);
-        f << "</PointData>\n<Cells>\n<DataArray type=\"Int32\" Name=\"connectivity\" format=\"ascii\"></DataArray>\n"
-          << "<DataArray type=\"Int32\" Name=\"offsets\" format=\"ascii\"></DataArray>\n"
-          << "<DataArray type=\"UInt8\" Name=\"types\" format=\"ascii\"></DataArray>\n</Cells>\n"
-          << "</Piece>\n</UnstructuredGrid>\n</VTKFile>\n";
+        return fundem_vtu::write(file, time, (long long)step, points, conn, offs, types,
+                                 {fundem_vtu::array("particleID", 1, id), fundem_vtu::array("velocity", 3, vel)});
+    }
+
+    bool writeCentres(const std::string& file, double time, size_t step)
+    {
+        const std::vector<double3>& x = LSParticle_.positionHost();
+        if (x.empty()) return true;
+        const std::vector<double3>& v = LSParticle_.velocityHost();
+        const std::vector<double3>& w = LSParticle_.angularVelocityHost();
+        const std::vector<quaternion>& q = LSParticle_.orientationHost();
+        std::vector<float> points, vel, ang, ori;
+        for (size_t i = 0; i < x.size(); ++i) {
+            put3(points, x[i]);
+            put3(vel, v[i]);
+            put3(ang, w[i]);
+            for (double c : {q[i].q0, q[i].q1, q[i].q2, q[i].q3}) ori.push_back(float(c));
+        }
+        return fundem_vtu::write(file, time, (long long)step, points, {}, {}, {},
+                                 {fundem_vtu::array("velocity", 3, vel), fundem_vtu::array("angularVelocity", 3, ang),
+                                  fundem_vtu::array("orientation", 4, ori)});
+    }
+
+    // node contacts of one list as vertices: point, normal, direction of the
+    // sliding spring and the two elastic energies
+    bool writeContacts(const std::string& file, int kind, double time, size_t step)
+    {
+        long long n = 0;
+        if (!report(fundem_num_contacts(sim_, kind, &n), "output")) return false;
+        std::vector<int> node(n), partner(n);
+        std::vector<double> point(3 * n), normal(3 * n), overlap(n), spring(3 * n), en(n), es(n);
+        if (n > 0 && !report(fundem_get_contacts(sim_, kind, node.data(), partner.data(), point.data(), normal.data(),
+                                                 overlap.data(), spring.data(), en.data(), es.data()), "output"))
+            return false;
+        std::vector<float> pts, nrm, dir, fen, fes;
+        std::vector<int32_t> conn, offs;
+        std::vector<uint8_t> types;
+        for (long long k = 0; k < n; ++k) {
+            put3(pts, make_double3(point[3 * k], point[3 * k + 1], point[3 * k + 2]));
+            put3(nrm, make_double3(normal[3 * k], normal[3 * k + 1], normal[3 * k + 2]));
+            put3(dir, normalize(make_double3(spring[3 * k], spring[3 * k + 1], spring[3 * k + 2])));
+            fen.push_back(float(en[k]));
+            fes.push_back(float(es[k]));
+            conn.push_back((int32_t)k);
+            offs.push_back((int32_t)k + 1);
+            types.push_back(1);  // vertex
+        }
+        return fundem_vtu::write(file, time, (long long)step, pts, conn, offs, types,
+                                 {fundem_vtu::array("contactNormal", 3, nrm), fundem_vtu::array("slidingDirection", 3, dir),
+                                  fundem_vtu::array("normalElasticEnergy", 1, fen),
+                                  fundem_vtu::array("slidingElasticEnergy", 1, fes)});
+    }
+
+    bool writeBonds(const std::string& file, double time, size_t step)
+    {
+        int n = 0;
+        if (!report(fundem_num_bonds(sim_, &n), "output")) return false;
+        if (n == 0) return true;
+        std::vector<int> act(n);
+        std::vector<double> point(3 * n), e(6 * n);
+        if (!report(fundem_get_bonds(sim_, act.data(), point.data(), e.data()), "output")) return false;
+        std::vector<float> pts;
+        std::vector<float> f[6];
+        std::vector<int32_t> conn, offs, mid, sid, a32;
+        std::vector<uint8_t> types;
+        for (int k = 0; k < n; ++k) {
+            put3(pts, make_double3(point[3 * k], point[3 * k + 1], point[3 * k + 2]));
+            for (int c = 0; c < 6; ++c) f[c].push_back(float(e[6 * k + c]));
+            mid.push_back(k < (int)bondMaster_.size() ? bondMaster_[k] : -1);
+            sid.push_back(k < (int)bondSlave_.size() ? bondSlave_[k] : -1);
+            a32.push_back(act[k]);
+            conn.push_back(k);
+            offs.push_back(k + 1);
+            types.push_back(1);
+        }
+        return fundem_vtu::write(
+            file, time, (long long)step, pts, conn, offs, types,
+            {fundem_vtu::array("masterObjectID", 1, mid), fundem_vtu::array("slaveObjectID", 1, sid),
+             fundem_vtu::array("activated", 1, a32), fundem_vtu::array("normalElasticEnergy", 1, f[0]),
+             fundem_vtu::array("shearElasticEnergy", 1, f[1]), fundem_vtu::array("bendingElasticEnergy", 1, f[2]),
+             fundem_vtu::array("torsionElasticEnergy", 1, f[3]), fundem_vtu::array("maxNormalStress", 1, f[4]),
+             fundem_vtu::array("maxShearStress", 1, f[5])});
     }
 
     std::string dir_;
@@ -338,8 +453,10 @@ private:
     fundem_sim* sim_ = nullptr;
     int phase_ = 0;
     bool perX_ = false, perY_ = false;
-    std::vector<int> geoNodes_;     // boundary nodes per particle geometry
-    std::vector<int> particleGeo_;  // geometry of each particle
+    std::vector<std::vector<double3>> geoNodes_, wallGeoNodes_;  // body-frame nodes per geometry
+    std::vector<std::vector<int3>> geoTris_, wallGeoTris_;       // surface triangles per geometry
+    std::vector<int> particleGeo_, wallGeo_;                      // geometry of each particle and wall
+    std::vector<int> bondMaster_, bondSlave_;                     // bodies of each bond
     std::vector<double3> wallVel_, wallAng_;
     LSParticle LSParticle_;
     LSParticle Wall_;

@@ -142,6 +142,39 @@ def test_drum_app(tmp_path, fundem):
         if phase == 1:
             assert Lx > 0.2 * rigid, (Lx, rigid)
         print(f"phase {phase}: L_x {Lx:.3f}, rigid co-rotation {rigid:.3f}")
+    _check_drum_frames(tmp_path / "drum_phase2", _state(out / "state_1.txt"))
+
+
+def _check_drum_frames(d, state):
+    """The last frame of the turning phase, as LSSolver::solve writes it: the
+    particles' surface meshes and centres, the drum's mesh, and the particle
+    and wall contacts."""
+    import vtu_read as V
+    last = sorted(os.listdir(d / "LSParticle"))[-1][-8:]  # NNNN.vtu
+    centres = V.read(d / "LSParticle" / ("Particle_" + last))
+    assert centres["n_points"] == len(state)
+    assert np.allclose(centres["points"], state[:, :3], rtol=0, atol=1e-6)
+    assert np.allclose(centres["point_data"]["velocity"], state[:, 3:6], rtol=1e-6, atol=1e-6)
+    assert centres["point_data"]["orientation"].shape == (len(state), 4)
+    mesh = V.read(d / "LSParticle" / ("LSObjectMesh_" + last))
+    # subdivision level 3: 642 nodes and 1280 triangles per particle
+    assert mesh["n_points"] == 642 * len(state) and mesh["n_cells"] == 1280 * len(state)
+    assert np.all(mesh["types"] == 5) and mesh["offsets"][-1] == 3 * mesh["n_cells"]
+    pid = mesh["point_data"]["particleID"]
+    assert np.array_equal(pid, np.repeat(np.arange(len(state)), 642))
+    # every node lies within its body's reach of the body's centre
+    reach = np.linalg.norm(mesh["points"] - centres["points"][pid], axis=1)
+    assert reach.max() < 0.3 and reach.min() > 0.0
+    wall = V.read(d / "Wall" / ("LSObjectMesh_" + last))
+    # 96 segments, 2 axial segments: 3 rings and 2 cap centres; 2 x 96 x 2 side and 2 x 96 cap triangles
+    assert wall["n_points"] == 3 * 96 + 2 and wall["n_cells"] == 4 * 96 + 2 * 96
+    for sub in ("LSParticleInteraction", "LSParticle-WallInteraction"):
+        c = V.read(d / sub / ("LSInteraction_" + last))
+        assert c["n_points"] > 0, sub
+        n = c["point_data"]["contactNormal"]
+        assert np.allclose(np.linalg.norm(n, axis=1), 1.0, atol=1e-5), sub
+        assert np.all(np.hypot(c["points"][:, 1], c["points"][:, 2]) < 1.0 + 1e-3), sub
+        assert np.all(c["point_data"]["normalElasticEnergy"] >= 0), sub
 
 
 def test_mesh_falling_app(tmp_path, fundem):
