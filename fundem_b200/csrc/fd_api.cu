@@ -35,9 +35,18 @@ struct CudaError : std::runtime_error {
         if (e_ != cudaSuccess) throw CudaError(std::string(#x) + ": " + cudaGetErrorString(e_));     \
     } while (0)
 
-// bumped by every device (re)allocation of a DevArray: a captured step graph
-// holds raw pointers and is rebuilt when this moves
+// A captured step graph holds raw device pointers and is rebuilt when one of
+// its simulation's arrays was (re)allocated since the capture.  Allocations
+// made inside a call on a simulation (guard() sets t_sim_epoch) bump that
+// simulation's counter; any other allocation bumps the global counter, which
+// every graph also checks.
 std::atomic<unsigned long long> g_alloc_epoch{0};
+thread_local unsigned long long* t_sim_epoch = nullptr;
+inline void bump_alloc_epoch()
+{
+    if (t_sim_epoch) ++*t_sim_epoch;
+    else g_alloc_epoch.fetch_add(1);
+}
 
 template <typename T> struct DevArray {
     T* p = nullptr;
@@ -57,7 +66,7 @@ template <typename T> struct DevArray {
         release();
         n = count;
         if (count == 0) return;
-        g_alloc_epoch.fetch_add(1);
+        bump_alloc_epoch();
         FD_CUDA(cudaMalloc((void**)&p, sizeof(T) * count));
         if (zero) FD_CUDA(cudaMemset(p, 0, sizeof(T) * count));
     }
@@ -65,7 +74,7 @@ template <typename T> struct DevArray {
     void grow(size_t count, size_t keep)
     {
         if (count <= n) return;
-        g_alloc_epoch.fetch_add(1);
+        bump_alloc_epoch();
         T* q = nullptr;
         FD_CUDA(cudaMalloc((void**)&q, sizeof(T) * count));
         FD_CUDA(cudaMemset(q, 0, sizeof(T) * count));
@@ -693,8 +702,10 @@ struct fundem_sim {
     cudaStream_t cap_stream = nullptr;
     bool capturing = false;
     int graph_steps = 0;
+    int graph_unchecked = 0;  // steps replayed since the last capacity check
+    unsigned long long alloc_epoch = 0;  // device (re)allocations of this simulation
     double graph_key[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // gravity, dt, precision, records, counters, periodicity
-    unsigned long long graph_epoch = 0;
+    unsigned long long graph_epoch = 0, graph_gepoch = 0;
     void drop_graph()
     {
         if (graph_exec) cudaGraphExecDestroy(graph_exec);
@@ -1107,6 +1118,12 @@ struct fundem_sim {
 namespace {
 int guard(fundem_sim* s, const std::function<void()>& f)
 {
+    // allocations inside the call belong to this simulation
+    struct EpochScope {
+        unsigned long long* prev;
+        explicit EpochScope(unsigned long long* e) : prev(t_sim_epoch) { if (e) t_sim_epoch = e; }
+        ~EpochScope() { t_sim_epoch = prev; }
+    } scope(s ? &s->alloc_epoch : nullptr);
     try {
         f();
         return FUNDEM_OK;
@@ -1506,19 +1523,28 @@ int fundem_step_graph(fundem_sim* s, int nsteps, const double g[3], double dt)
     if (!s->setup_done) return FUNDEM_ERR_STATE;
     return guard(s, [&] {
         FD_CUDA(cudaSetDevice(s->device));
-        // grow the lists ahead of their counts, and make every lazy
-        // allocation of a step, before anything is captured
-        s->ensure_capacity();
-        s->rev_view();
         const double key[8] = {g[0], g[1], g[2], dt, (double)s->precision, (double)s->records,
                                (double)s->counters, (double)(s->sector * 4 + s->perX * 2 + s->perY)};
-        bool same = s->graph_exec && s->graph_steps == nsteps && s->graph_epoch == g_alloc_epoch.load();
-        for (int k = 0; k < 8 && same; ++k) same = s->graph_key[k] == key[k];
-        if (!same) {
+        auto reusable = [&] {
+            bool same = s->graph_exec && s->graph_steps == nsteps && s->graph_epoch == s->alloc_epoch &&
+                        s->graph_gepoch == g_alloc_epoch.load();
+            for (int k = 0; k < 8 && same; ++k) same = s->graph_key[k] == key[k];
+            return same;
+        };
+        // grow the lists ahead of their counts every CAPACITY_CHECK steps, as
+        // fundem_step does, and always before a capture (which also makes
+        // every lazy allocation of a step first)
+        if (!reusable() || s->graph_unchecked >= CAPACITY_CHECK) {
+            s->ensure_capacity();
+            s->rev_view();
+            s->graph_unchecked = 0;
+        }
+        s->graph_unchecked += nsteps;
+        if (!reusable()) {
             s->drop_graph();
             if (!s->cap_stream) FD_CUDA(cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking));
             const cudaStream_t own = s->stream;
-            const unsigned long long epoch = g_alloc_epoch.load();
+            const unsigned long long epoch = s->alloc_epoch, gepoch = g_alloc_epoch.load();
             s->stream = s->cap_stream;
             s->capturing = true;
             cudaGraph_t graph = nullptr;
@@ -1541,7 +1567,7 @@ int fundem_step_graph(fundem_sim* s, int nsteps, const double g[3], double dt)
             s->stream = own;
             s->capturing = false;
             FD_CUDA(e);
-            if (g_alloc_epoch.load() != epoch) {
+            if (s->alloc_epoch != epoch || g_alloc_epoch.load() != gepoch) {
                 cudaGraphDestroy(graph);
                 throw std::logic_error("a device allocation happened while the steps were captured");
             }
@@ -1551,6 +1577,7 @@ int fundem_step_graph(fundem_sim* s, int nsteps, const double g[3], double dt)
             s->graph_steps = nsteps;
             std::copy(key, key + 8, s->graph_key);
             s->graph_epoch = epoch;
+            s->graph_gepoch = gepoch;
         }
         FD_CUDA(cudaGraphLaunch(s->graph_exec, s->stream));
     });
