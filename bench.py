@@ -280,6 +280,7 @@ def run_fundem(args, rank, world, dist):
     nar_bytes = BYTES_PARTICLE_STEP * n + BYTES_CONTACT_STEP * 0.5 * (contacts + contacts_end)
     achieved = nar_bytes / (nar_avg / 1e3) / 1e9 if nar_avg > 0 else None
     step_bytes = BYTES_PARTICLE_STEP * n + BYTES_CONTACT_STEP * 0.5 * (contacts + contacts_end) + BYTES_BOND_STEP * nbonds
+    traffic_per_pair = profiled_traffic_per_pair()
     cpu = None
     if world == 1 and not args.no_cpu:
         cpu = cpu_baseline(seconds=args.cpu_seconds, n=args.cpu_sample)
@@ -299,7 +300,10 @@ def run_fundem(args, rank, world, dist):
                         "(fundem_step_graph) followed by a read of the status word, state downloaded"},
         "graph": graph,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk, "unit": "GB/s",
-                     "frac": (achieved / pk) if achieved else None, "traffic": None,
+                     "frac": (achieved / pk) if achieved else None,
+                     "traffic": (traffic_per_pair * pairs) if traffic_per_pair else None,
+                     "traffic_source": TRAFFIC_PROFILE + " (ncu DRAM bytes per candidate pair x pairs)"
+                     if traffic_per_pair else None,
                      "kernel": "k_narrow<PP> (narrow phase + contact law)", "peak_source": pk_kind,
                      "kernel_ms": nar_avg, "algorithmic_bytes": nar_bytes,
                      "step_achieved_gbs": step_bytes / (t_max / args.steps / 1e3) / 1e9},
@@ -319,6 +323,22 @@ def run_fundem(args, rank, world, dist):
 
 
 GRAPH_CHUNK = 50  # steps per CUDA graph in the graph-replay measurement
+# ncu summary holding the narrow phase's DRAM bytes per candidate pair
+TRAFFIC_PROFILE = "profiles/narrow_pp_traffic_bonded_column_65k.md"
+
+
+def profiled_traffic_per_pair():
+    """DRAM bytes per candidate pair of the particle-particle narrow phase,
+    from the committed ncu summary (None when it is absent)."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), TRAFFIC_PROFILE)
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_pair"):
+                    return float(line.split("=")[1])
+    except OSError:
+        pass
+    return None
 
 
 def aggregate(ms, n, steps, world, dist, device):
