@@ -2110,8 +2110,10 @@ void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& 
     if (gh) n.gh = *gh; else memset(&n.gh, 0, sizeof(n.gh));
     n.L = L; n.a = a; n.with_force = with_force;
     const long long need = ((long long)L.cap_pairs + NARROW_WARPS - 1) / NARROW_WARPS;
-    const int grid = (int)(need < 148 * 24 ? (need > 0 ? need : 1) : 148 * 24);
-    const int cgrid = 148 * 16;
+    // grid-stride kernels: one resident wave at most (the pair and slot
+    // counts are known only on the device)
+    const int grid = (int)(need < 148 * FD_SELECT_MIN_BLOCKS ? (need > 0 ? need : 1) : 148 * FD_SELECT_MIN_BLOCKS);
+    const int cgrid = 148 * 4;
 #define FD_NARROW_CASE(K)                                                              \
     case K:                                                                            \
         k_select<K><<<grid, NARROW_WARPS * 32, 0, s>>>(n);                             \
@@ -2135,8 +2137,8 @@ void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& 
         break;
     }
 #undef FD_NARROW_CASE
-    if (mixed) k_pair_sum32<<<148 * 8, TPB, 0, s>>>(L, with_force);
-    else k_pair_sum<<<148 * 8, TPB, 0, s>>>(L, with_force);
+    if (mixed) k_pair_sum32<<<148 * 4, TPB, 0, s>>>(L, with_force);
+    else k_pair_sum<<<148 * 4, TPB, 0, s>>>(L, with_force);
 }
 
 void launch_reverse(const ObjDev& P, PairListDev* lists, const int* active, RevDev& R, int* scan_tmp, size_t,
