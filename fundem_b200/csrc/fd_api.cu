@@ -697,19 +697,27 @@ struct fundem_sim {
     }
     long long launches = 0;
     long long hook_steps = 0;  // fundem_step_begin calls, for capacity checks
-    // a captured run of steps (fundem_step_graph)
-    cudaGraphExec_t graph_exec = nullptr;
+    // Captured runs of steps (fundem_step_graph).  A capture fixes which of
+    // the two list generations each step writes and reads its history from,
+    // so there is one graph per generation the run starts on: for an odd
+    // number of steps the starting generation alternates between calls.
+    struct StepGraph {
+        cudaGraphExec_t exec = nullptr;
+        int steps = 0;
+        double key[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // gravity, dt, precision, records, counters, periodicity
+        unsigned long long epoch = 0, gepoch = 0;  // allocation counters at the capture
+    };
+    StepGraph graphs[2];
     cudaStream_t cap_stream = nullptr;
     bool capturing = false;
-    int graph_steps = 0;
     int graph_unchecked = 0;  // steps replayed since the last capacity check
     unsigned long long alloc_epoch = 0;  // device (re)allocations of this simulation
-    double graph_key[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // gravity, dt, precision, records, counters, periodicity
-    unsigned long long graph_epoch = 0, graph_gepoch = 0;
     void drop_graph()
     {
-        if (graph_exec) cudaGraphExecDestroy(graph_exec);
-        graph_exec = nullptr;
+        for (StepGraph& g : graphs) {
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+            g.exec = nullptr;
+        }
     }
     ~fundem_sim()
     {
@@ -1525,23 +1533,25 @@ int fundem_step_graph(fundem_sim* s, int nsteps, const double g[3], double dt)
         FD_CUDA(cudaSetDevice(s->device));
         const double key[8] = {g[0], g[1], g[2], dt, (double)s->precision, (double)s->records,
                                (double)s->counters, (double)(s->sector * 4 + s->perX * 2 + s->perY)};
-        auto reusable = [&] {
-            bool same = s->graph_exec && s->graph_steps == nsteps && s->graph_epoch == s->alloc_epoch &&
-                        s->graph_gepoch == g_alloc_epoch.load();
-            for (int k = 0; k < 8 && same; ++k) same = s->graph_key[k] == key[k];
+        auto reusable = [&](const fundem_sim::StepGraph& G) {
+            bool same = G.exec && G.steps == nsteps && G.epoch == s->alloc_epoch && G.gepoch == g_alloc_epoch.load();
+            for (int k = 0; k < 8 && same; ++k) same = G.key[k] == key[k];
             return same;
         };
         // grow the lists ahead of their counts every CAPACITY_CHECK steps, as
         // fundem_step does, and always before a capture (which also makes
         // every lazy allocation of a step first)
-        if (!reusable() || s->graph_unchecked >= CAPACITY_CHECK) {
+        if (!reusable(s->graphs[s->lists[FD_PP].cur]) || s->graph_unchecked >= CAPACITY_CHECK) {
             s->ensure_capacity();
             s->rev_view();
             s->graph_unchecked = 0;
         }
         s->graph_unchecked += nsteps;
-        if (!reusable()) {
-            s->drop_graph();
+        // the generation the run starts on (all lists flip together)
+        fundem_sim::StepGraph& G = s->graphs[s->lists[FD_PP].cur];
+        if (!reusable(G)) {
+            if (G.exec) cudaGraphExecDestroy(G.exec);
+            G.exec = nullptr;
             if (!s->cap_stream) FD_CUDA(cudaStreamCreateWithFlags(&s->cap_stream, cudaStreamNonBlocking));
             const cudaStream_t own = s->stream;
             const unsigned long long epoch = s->alloc_epoch, gepoch = g_alloc_epoch.load();
@@ -1571,15 +1581,23 @@ int fundem_step_graph(fundem_sim* s, int nsteps, const double g[3], double dt)
                 cudaGraphDestroy(graph);
                 throw std::logic_error("a device allocation happened while the steps were captured");
             }
-            e = cudaGraphInstantiate(&s->graph_exec, graph, 0);
+            e = cudaGraphInstantiate(&G.exec, graph, 0);
             cudaGraphDestroy(graph);
             FD_CUDA(e);
-            s->graph_steps = nsteps;
-            std::copy(key, key + 8, s->graph_key);
-            s->graph_epoch = epoch;
-            s->graph_gepoch = gepoch;
+            G.steps = nsteps;
+            std::copy(key, key + 8, G.key);
+            G.epoch = epoch;
+            G.gepoch = gepoch;
+            // capturing flipped the host's generation index nsteps times
+            // without running a step; put it back so the launch below
+            // starts from the generation it was captured for
+            if (nsteps & 1)
+                for (int k = 0; k < FD_NKIND; ++k) s->lists[k].cur ^= 1;
         }
-        FD_CUDA(cudaGraphLaunch(s->graph_exec, s->stream));
+        FD_CUDA(cudaGraphLaunch(G.exec, s->stream));
+        // the launch leaves the newest lists in the generation nsteps flips on
+        if (nsteps & 1)
+            for (int k = 0; k < FD_NKIND; ++k) s->lists[k].cur ^= 1;
     });
 }
 

@@ -38,3 +38,29 @@ def test_step_graph_matches_step(fundem):
     assert np.array_equal(g.state()["pos"], p.state()["pos"])
     assert g.num_contacts(fundem.PP) == p.num_contacts(fundem.PP)
     g.close(); p.close()
+
+
+@pytest.mark.parametrize("chunks", [(1,) * 12, (3, 1, 3, 5), (2, 1, 1, 8)])
+def test_step_graph_odd_lengths_and_mixed_calls(fundem, chunks):
+    """Graphs of odd length alternate the contact-list generation they start
+    on, and plain steps may come between replays: every sequence equals the
+    same number of plain steps bit for bit."""
+    from fundem_b200 import workloads
+    sim, sc, info = workloads.bonded_column(n=2048, footprint=(16, 16), seed=2)
+    sim.close()
+    g = fundem.Simulation.from_scenario(sc, records=False)
+    p = fundem.Simulation.from_scenario(sc, records=False)
+    g.detect(); p.detect()
+    total = 0
+    for i, c in enumerate(chunks):
+        g.step_graph(c)
+        if i % 2 == 1:
+            g.step(1)  # a plain step between replays flips the generation too
+            total += 1
+        total += c
+    p.step(total)
+    g.sync(); p.sync()
+    assert np.array_equal(g.state()["pos"], p.state()["pos"])
+    for k in (fundem.PP, fundem.PW):
+        assert g.num_contacts(k) == p.num_contacts(k)
+    g.close(); p.close()
