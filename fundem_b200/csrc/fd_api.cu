@@ -37,9 +37,9 @@ struct CudaError : std::runtime_error {
 
 // Copies and fills issued on the legacy default stream are not ordered with
 // a simulation stream created non-blocking (as PyTorch's streams are), and
-// cudaMemset and device-to-device or host-to-device cudaMemcpy may return
-// before they finish: the library waits for the legacy stream right after
-// them, before the simulation stream uses the memory.
+// cudaMemset and device-to-device cudaMemcpy may return before they finish.
+// The array allocations below, which know no stream, wait for the legacy
+// stream after them; everything else goes on the simulation's stream.
 inline cudaError_t after_legacy(cudaError_t e) { return e != cudaSuccess ? e : cudaStreamSynchronize(cudaStreamLegacy); }
 
 // A captured step graph holds raw device pointers and is rebuilt when one of
@@ -680,7 +680,7 @@ struct fundem_sim {
         nl_ref.alloc(m); nl_vis.alloc(m); nl_cnt.alloc(m); nl_list.alloc(m * fd::NL_MAX, false);
         nl_ctrl.alloc(4);
         const int one = 1;
-        FD_CUDA(after_legacy(cudaMemcpy(nl_ctrl.p, &one, sizeof(int), cudaMemcpyHostToDevice)));
+        FD_CUDA(cudaMemcpyAsync(nl_ctrl.p, &one, sizeof(int), cudaMemcpyHostToDevice, stream));
     }
     fd::NlDev nl_view()
     {
@@ -1097,7 +1097,7 @@ struct fundem_sim {
             }
             if (attempt > 0 || (f0 & grow_bits)) {
                 const unsigned int clear = f0 & ~grow_bits;
-                FD_CUDA(after_legacy(cudaMemcpy(flags.p, &clear, sizeof(clear), cudaMemcpyHostToDevice)));
+                FD_CUDA(cudaMemcpyAsync(flags.p, &clear, sizeof(clear), cudaMemcpyHostToDevice, stream));
             }
             detect_all(false, 0.0, probe, attempt == 0);
             ensure_capacity();
@@ -1105,7 +1105,7 @@ struct fundem_sim {
             FD_CUDA(cudaMemcpy(&f, flags.p, sizeof(f), cudaMemcpyDeviceToHost));
             if (!(f & grow_bits) || attempt == 3) {
                 const unsigned int keep = f | f0;
-                FD_CUDA(after_legacy(cudaMemcpy(flags.p, &keep, sizeof(keep), cudaMemcpyHostToDevice)));
+                FD_CUDA(cudaMemcpyAsync(flags.p, &keep, sizeof(keep), cudaMemcpyHostToDevice, stream));
                 break;
             }
         }
@@ -1891,7 +1891,7 @@ int fundem_set_bond_activation(fundem_sim* s, const int* activated)
         const size_t n = B.master.size();
         std::memcpy(B.active.data(), activated, sizeof(int) * n);
         if (B.n_dev == (int)n && !B.dirty && n > 0)
-            FD_CUDA(after_legacy(cudaMemcpy(B.d_active.p, activated, sizeof(int) * n, cudaMemcpyHostToDevice)));
+            FD_CUDA(cudaMemcpyAsync(B.d_active.p, activated, sizeof(int) * n, cudaMemcpyHostToDevice, s->stream));
     });
 }
 
@@ -1979,7 +1979,7 @@ int fundem_work_counters(fundem_sim* s, unsigned long long out[5])
     return guard(s, [&] {
         FD_CUDA(cudaStreamSynchronize(s->stream));
         FD_CUDA(cudaMemcpy(out, s->stats.p, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
-        FD_CUDA(after_legacy(cudaMemset(s->stats.p, 0, 8 * sizeof(unsigned long long))));
+        FD_CUDA(cudaMemsetAsync(s->stats.p, 0, 8 * sizeof(unsigned long long), s->stream));
     });
 }
 
@@ -2205,7 +2205,8 @@ int fundem_adjoint_backward(fundem_sim* s, const double* dl_dpos, const double* 
                         any = true;
                     }
                     if (any)
-                        FD_CUDA(after_legacy(cudaMemcpy(Sb[cur][k].p, sb.data(), sizeof(double) * sb.size(), cudaMemcpyHostToDevice)));
+                        FD_CUDA(cudaMemcpyAsync(Sb[cur][k].p, sb.data(), sizeof(double) * sb.size(),
+                                                cudaMemcpyHostToDevice, s->stream));
                 }
             }
             // reverse sweep over the segment
