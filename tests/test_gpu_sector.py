@@ -151,3 +151,26 @@ def test_sector_trajectory_vs_reference(fundem):
             assert np.array_equal(keys(canonical(g.contacts(ki))),
                                   keys(canonical(golden_contacts(gold, s, kind)))), (s, kind)
     g.sync()
+
+
+def test_sector_neighbour_list_and_mixed(fundem):
+    """With sector periodicity the neighbour list (forced on at this size)
+    gives the cell search's steps bit for bit, bodies turned by the wrap
+    included; the mixed-precision path follows FP64 closely."""
+    def run(nl, precision):
+        g = fundem.Simulation.from_scenario(PC.sector())
+        g.set_neighbour_list(nl)
+        g.set_precision(precision)
+        g.detect()
+        g.step(40)
+        g.sync()
+        st = g.state()
+        c = g.contacts(0)
+        g.close()
+        return st, c
+    cell, c_cell = run(0, fundem.FP64)
+    nl, c_nl = run(1, fundem.FP64)
+    assert np.array_equal(cell["pos"], nl["pos"]) and np.array_equal(cell["vel"], nl["vel"])
+    assert np.array_equal(keys(canonical(c_cell)), keys(canonical(c_nl)))
+    mixed, _ = run(0, fundem.FP32_MIXED)
+    assert rel_err(mixed["pos"], cell["pos"]) < 1e-6
