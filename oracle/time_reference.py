@@ -11,7 +11,8 @@ the hooks of steps 20 and STEPS - 10, after a device synchronisation at each
 end; no output frame falls in that window (the reference writes VTU frames
 at the start and end of solve).  The scenario and the reference's VTU output
 go to a scratch directory under /tmp, removed afterwards; a JSON summary goes
-to gpurun_out/ when that directory exists, else to the current directory.
+to the directory named by the environment variable FUNDEM_TIMING_OUT, else to
+the current directory.
 
 Measurement infrastructure: needs a GPU and oracle/_ref/ref_driver built by
 oracle/Makefile from the reference sources.
@@ -70,7 +71,7 @@ def main():
     res = dict(particles=n, footprint=[fx, fy], info=info, fundem_ms_per_step=ours, reference_ms_per_step=ref,
                reference_window=[20, steps_ref - 10], ratio=ref / ours)
     print(json.dumps(res), flush=True)
-    dst = os.path.join(ROOT, "gpurun_out") if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else "."
+    dst = os.environ.get("FUNDEM_TIMING_OUT", ".")
     with open(os.path.join(dst, f"reference_timing_{n}.json"), "w") as f:
         json.dump(res, f, default=str)
     return r.returncode

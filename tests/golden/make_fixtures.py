@@ -103,8 +103,8 @@ def collect(src, cases):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("mode", choices=["run", "collect", "sha"])
-    ap.add_argument("--out", default="gpurun_out/ref")
-    ap.add_argument("--src", default="gpurun_out/ref")
+    ap.add_argument("--out", default="ref_dumps")
+    ap.add_argument("--src", default="ref_dumps")
     ap.add_argument("--cases", nargs="*", default=list(PC.CASES))
     a = ap.parse_args()
     if a.mode == "run":
