@@ -124,3 +124,34 @@ def test_adjoint_refuses_rotating_bodies(fundem):
     with pytest.raises(fundem.FundemError):
         s.adjoint_begin(10)
     s.close()
+
+
+def test_checkpoint_interval_autotuner(fundem):
+    """The autotuner times forward + backward for several checkpoint
+    intervals and picks one; the gradients do not depend on the interval,
+    since each segment's re-run repeats the forward run (they agree to
+    rounding: the reverse sweep adds to particles with atomics)."""
+    from fundem_b200 import autotune, workloads
+    sim, sc, info = workloads.bonded_column(n=512, footprint=(8, 8), seed=11)
+    sim.close()
+    rng = np.random.default_rng(5)
+    w = rng.standard_normal((512, 3))
+    u = rng.standard_normal((512, 3)) * 1e-3
+
+    def make():
+        s = fundem.Simulation.from_scenario(sc, records=False)
+        s.detect()
+        return s
+
+    best, times = autotune.checkpoint_interval(make, 40, w, u, candidates=(5, 10, 20, 40))
+    assert best in (5, 10, 20, 40) and set(times) == {5, 10, 20, 40}
+    grads = []
+    for k in (5, 40):
+        s = make()
+        s.adjoint_begin(k)
+        s.adjoint_forward(40)
+        grads.append(s.adjoint_backward(w, u))
+        s.adjoint_end()
+        s.close()
+    for a, b in zip(grads[0], grads[1]):
+        assert np.abs(a - b).max() <= 1e-10 * np.abs(b).max()
