@@ -1415,13 +1415,17 @@ __global__ void k_pair_sum(PairListDev L, int with_force)
 #pragma unroll
             for (int t = 0; t < 9; ++t) acc[t] += f[t];
         }
+        // pairs without contact slots keep no sum: k_reduce skips them by
+        // their slot count
+        if (__any_sync(0xffffffffu, c > 0)) {
 #pragma unroll
-        for (int t = 0; t < 9; ++t) {
-            acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], 4);
-            acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], 2);
-            acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], 1);
+            for (int t = 0; t < 9; ++t) {
+                acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], 4);
+                acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], 2);
+                acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], 1);
+            }
         }
-        if (p < npairs) {
+        if (p < npairs && c > 0) {
             double* out = L.pf + 9ll * p;
 #pragma unroll
             for (int t = 0; t < 8; ++t)
@@ -1689,13 +1693,15 @@ __global__ void k_pair_sum32(PairListDev L, int with_force)
 #pragma unroll
             for (int t = 0; t < 9; ++t) acc[t] += f[t];
         }
+        if (__any_sync(0xffffffffu, c > 0)) {
 #pragma unroll
-        for (int t = 0; t < 9; ++t) {
-            acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], 4);
-            acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], 2);
-            acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], 1);
+            for (int t = 0; t < 9; ++t) {
+                acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], 4);
+                acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], 2);
+                acc[t] += __shfl_xor_sync(0xffffffffu, acc[t], 1);
+            }
         }
-        if (p < npairs) {
+        if (p < npairs && c > 0) {
             float* out = pf + 9ll * p;
 #pragma unroll
             for (int t = 0; t < 8; ++t)
@@ -1942,6 +1948,7 @@ __global__ void k_reduce(ReduceArgs r)
         const Real* pfa = reinterpret_cast<const Real*>(L.pf);
         const int s = L.seg_off[i], c = L.seg_cnt[i];
         for (int k = s; k < s + c; ++k) {
+            if (L.c_cnt[k] == 0) continue;  // no contact slot, no sum kept
             const Real* pf = pfa + 9ll * k;
             add(F, pf, Real(1));
             add(T, pf + 3, Real(1));
@@ -1955,6 +1962,7 @@ __global__ void k_reduce(ReduceArgs r)
             const int kind = code & 7, k = code >> 3;
             const PairListDev& L = r.L[kind];
             if (kind != FD_PP && L.pairA[k] == i) continue;  // a particle against its own ghost
+            if (L.c_cnt[k] == 0) continue;
             const Real* pf = reinterpret_cast<const Real*>(L.pf) + 9ll * k;
             add(F, pf, Real(-1));
             add(T, pf + 6, Real(1));
