@@ -1747,7 +1747,8 @@ __global__ void k_rev_count(RevArgs r)
         int k, p;
         if (!rev_locate(r, idx, k, p)) return;
         const int B = r.L[k].pairB[p];
-        if (B >= 0 && B < r.n_obj) atomicAdd(&r.R.cnt[B], 1);
+        // only pairs with contact slots carry a force to the partner
+        if (B >= 0 && B < r.n_obj && r.L[k].c_cnt[p] > 0) atomicAdd(&r.R.cnt[B], 1);
     }
 }
 __global__ void k_rev_fill(RevArgs r)
@@ -1756,7 +1757,7 @@ __global__ void k_rev_fill(RevArgs r)
         int k, p;
         if (!rev_locate(r, idx, k, p)) return;
         const int B = r.L[k].pairB[p];
-        if (B >= 0 && B < r.n_obj) {
+        if (B >= 0 && B < r.n_obj && r.L[k].c_cnt[p] > 0) {
             const int slot = r.R.off[B] + atomicAdd(&r.R.fill[B], 1);
             if (slot < r.R.cap) r.R.code[slot] = p * 8 + rev_kind(k);  // pair counts stay below 2^28
         }
