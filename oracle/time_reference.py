@@ -1,10 +1,12 @@
 """Time the reference's own CUDA build against this library on one workload.
 
     python oracle/time_reference.py N FX FY [STEPS]
+    python oracle/time_reference.py pour [STEPS]
 
 Builds the bonded periodic column with N particles on an FX x FY footprint
-(fundem_b200.workloads.bonded_column, on the GPU), times 100 steps of this
-library from that state, then writes the same scenario for the reference
+(fundem_b200.workloads.bonded_column, on the GPU), or the 1,000-particle
+pour in a box of six walls (fundem_b200.scenario.pour, the small pour's
+shape), times 100 steps of this library (1,000 for the pour) from that state, then writes the same scenario for the reference
 (oracle.scenario_io.write_reference_scenario) and runs oracle/_ref/ref_driver
 in timing mode over STEPS steps.  The driver reports the wall time between
 the hooks of steps 20 and STEPS - 10, after a device synchronisation at each
@@ -34,20 +36,31 @@ def main():
     from fundem_b200 import workloads
     from oracle import scenario_io
 
-    n, fx, fy = int(sys.argv[1]), int(sys.argv[2]), int(sys.argv[3])
-    steps_ref = int(sys.argv[4]) if len(sys.argv) > 4 else 50
-    sim, sc, info = workloads.bonded_column(n=n, footprint=(fx, fy), seed=1)
+    if sys.argv[1] == "pour":
+        import fundem_b200 as F
+        from fundem_b200 import scenario as S
+        sc = S.pour(n=1000, n_templates=4, seed=0)
+        n, fx, fy, info = 1000, 0, 0, {"workload": "pour"}
+        steps_ref = int(sys.argv[2]) if len(sys.argv) > 2 else 2000
+        sim = F.Simulation.from_scenario(sc)
+        sim.detect()
+        ours_steps = 1000
+    else:
+        n, fx, fy = int(sys.argv[1]), int(sys.argv[2]), int(sys.argv[3])
+        steps_ref = int(sys.argv[4]) if len(sys.argv) > 4 else 50
+        sim, sc, info = workloads.bonded_column(n=n, footprint=(fx, fy), seed=1)
+        ours_steps = 100
     sim.set_records(False)
     sim.step(20)
     sim.sync()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    sim.step(100)
+    sim.step(ours_steps)
     e1.record()
     torch.cuda.synchronize()
     sim.sync()
-    ours = e0.elapsed_time(e1) / 100
-    print(f"fundem_b200: {ours:.4f} ms/step at n={n} (steps 20..120)", flush=True)
+    ours = e0.elapsed_time(e1) / ours_steps
+    print(f"fundem_b200: {ours:.4f} ms/step at n={n} (steps 20..{20 + ours_steps})", flush=True)
     sim.close()
     torch.cuda.empty_cache()
 
