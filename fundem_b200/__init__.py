@@ -17,6 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libfundem_b200.so")
 
 FP64, FP32_MIXED = 0, 1
+INERTIA_REFERENCE, INERTIA_PHYSICAL = 0, 1
 PP, PW, GX, GY, GXY = 0, 1, 2, 3, 4
 GR90, GR180, GR270 = 5, 6, 7  # sector images
 
@@ -33,7 +34,7 @@ EXPORTS = [
     "fundem_kernel_time", "fundem_work_counters", "fundem_prefix_sum", "fundem_prefix_sum_noalloc", "fundem_last_error",
     "fundem_adjoint_begin", "fundem_adjoint_forward", "fundem_adjoint_backward", "fundem_adjoint_end",
     "fundem_step_graph", "fundem_set_neighbour_list", "fundem_checkpoint_write", "fundem_checkpoint_read",
-    "fundem_levelset_grid", "fundem_set_periodic_sector",
+    "fundem_levelset_grid", "fundem_set_periodic_sector", "fundem_set_inertia_mode",
 ]
 TIMERS = {"integrate": 0, "hash": 1, "broad": 2, "narrow_pp": 3, "narrow_pw": 4, "ghost": 5, "reduce": 6}
 
@@ -124,6 +125,7 @@ def lib():
         L.fundem_checkpoint_read.argtypes = [P, C.c_char_p]
         L.fundem_levelset_grid.argtypes = [I, P, C.POINTER(Shape), D, C.c_double, IP, D]
         L.fundem_set_periodic_sector.argtypes = [P, I]
+        L.fundem_set_inertia_mode.argtypes = [P, I]
         _lib = L
     return _lib
 
@@ -286,6 +288,8 @@ class Simulation:
         s.set_periodic(sc.periodic_x, sc.periodic_y)
         if getattr(sc, "periodic_sector", False):
             s.set_periodic_sector(True)
+        if getattr(sc, "inertia", "reference") == "physical":
+            s.set_inertia_mode(INERTIA_PHYSICAL)
         s.gravity = np.asarray(sc.gravity, float)
         s.dt = float(sc.dt)
         if setup:
@@ -363,6 +367,12 @@ class Simulation:
         """Quarter-sector periodicity about the z axis through the domain's
         min corner (LSSolver::addPeriodicBoundarySector)."""
         self._check(self.L.fundem_set_periodic_sector(self.h, int(bool(on))), "set_periodic_sector")
+
+    def set_inertia_mode(self, mode):
+        """INERTIA_REFERENCE (the reference's inverse(): zero when
+        |det I| < 1e-30) or INERTIA_PHYSICAL (scale-aware); takes effect at
+        the next setup."""
+        self._check(self.L.fundem_set_inertia_mode(self.h, int(mode)), "set_inertia_mode")
 
     def checkpoint_write(self, path):
         """Write the state a restart needs (objects, contact history, bonds)."""

@@ -114,13 +114,23 @@ struct HostGeo {
     std::vector<double3> nodes;
 };
 
-// inverse with the |det| < 1e-30 -> zero rule of myMat.h:163-194
-fd_sym host_inverse(const fd_sym& A)
+// Inverse of a symmetric 3x3 matrix by cofactors.  FUNDEM_INERTIA_REFERENCE
+// keeps the absolute |det| < 1e-30 -> zero rule of myMat.h:163-194, under
+// which mm-scale bodies (det of order 1e-34) never turn.
+// FUNDEM_INERTIA_PHYSICAL tests the determinant against the cube of the
+// largest diagonal entry instead, so only a matrix singular to 1e-12 relative
+// (no mass, a line or point body) gives zero, at any length scale.
+fd_sym host_inverse(const fd_sym& A, int mode = FUNDEM_INERTIA_REFERENCE)
 {
     const double det = A.xx * (A.yy * A.zz - A.yz * A.yz) + A.xy * (A.yz * A.xz - A.xy * A.zz) +
                        A.xz * (A.xy * A.yz - A.yy * A.xz);
     fd_sym r{0, 0, 0, 0, 0, 0};
-    if (std::fabs(det) < 1e-30) return r;
+    if (mode == FUNDEM_INERTIA_PHYSICAL) {
+        const double m = std::max(std::fabs(A.xx), std::max(std::fabs(A.yy), std::fabs(A.zz)));
+        if (!(m > 0.0) || !(std::fabs(det) > 1e-12 * m * m * m)) return r;
+    } else if (std::fabs(det) < 1e-30) {
+        return r;
+    }
     const double di = 1.0 / det;
     r.xx = (A.yy * A.zz - A.yz * A.yz) * di;
     r.yy = (A.xx * A.zz - A.xz * A.xz) * di;
@@ -263,7 +273,7 @@ struct GeoSetHost {
     double rmax = 0.0, grid_rmax = 0.0;
     bool built = false;
 
-    void build(bool wall, cudaStream_t s)
+    void build(bool wall, int inertia_mode, cudaStream_t s)
     {
         table.clear();
         key_of.clear();
@@ -315,7 +325,7 @@ struct GeoSetHost {
             const double mass = wall ? 0.0 : g.mass;
             t.inv_mass = mass > 0.0 ? 1.0 / mass : 0.0;
             t.inertia = mass > 0.0 ? g.inertia : fd_sym{0, 0, 0, 0, 0, 0};
-            t.inv_inertia = host_inverse(t.inertia);
+            t.inv_inertia = host_inverse(t.inertia, inertia_mode);
             // clusters
             std::vector<int> idx(g.nodes.size());
             std::iota(idx.begin(), idx.end(), 0);
@@ -651,6 +661,7 @@ struct fundem_sim {
     BondHost bonds;
     bool perX = false, perY = false;
     bool sector = false;  // quarter-sector periodicity about z through the domain's min corner
+    int inertia_mode = FUNDEM_INERTIA_REFERENCE;
     bool geo_dirty = true;
     bool setup_done = false;
     bool detected = false;
@@ -859,8 +870,8 @@ struct fundem_sim {
     {
         FD_CUDA(cudaSetDevice(device));
         if (geo_dirty) {
-            pgeo.build(false, stream);
-            wgeo.build(true, stream);
+            pgeo.build(false, inertia_mode, stream);
+            wgeo.build(true, inertia_mode, stream);
             pmat.upload(stream);
             wmat.upload(stream);
             geo_dirty = false;
@@ -1469,6 +1480,16 @@ int fundem_set_periodic_sector(fundem_sim* s, int on)
     return FUNDEM_OK;
 }
 
+int fundem_set_inertia_mode(fundem_sim* s, int mode)
+{
+    if (!s || (mode != FUNDEM_INERTIA_REFERENCE && mode != FUNDEM_INERTIA_PHYSICAL)) return FUNDEM_ERR_ARG;
+    if (mode != s->inertia_mode) {
+        s->inertia_mode = mode;
+        s->geo_dirty = true;
+    }
+    return FUNDEM_OK;
+}
+
 int fundem_setup(fundem_sim* s, const double mn[3], const double mx[3])
 {
     if (!s || !mn || !mx) return FUNDEM_ERR_ARG;
@@ -1906,7 +1927,7 @@ int fundem_get_geometry(fundem_sim* s, int wall, int geo, double* radius, double
     for (const double3& p : g.nodes) r = std::max(r, host_len(p));
     const double mass = wall ? 0.0 : g.mass;
     const fd_sym I = mass > 0.0 ? g.inertia : fd_sym{0, 0, 0, 0, 0, 0};
-    const fd_sym Ii = host_inverse(I);
+    const fd_sym Ii = host_inverse(I, s->inertia_mode);
     if (radius) *radius = r;
     if (inv_mass) *inv_mass = mass > 0.0 ? 1.0 / mass : 0.0;
     if (inertia) { inertia[0] = I.xx; inertia[1] = I.yy; inertia[2] = I.zz; inertia[3] = I.xy; inertia[4] = I.xz; inertia[5] = I.yz; }

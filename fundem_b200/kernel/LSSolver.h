@@ -212,6 +212,17 @@ public:
         report(fundem_set_periodic_sector(sim_, 0), "removePeriodicBoundary");
     }
 
+    // Not in the reference: physical = true inverts every particle inertia
+    // that is not singular relative to its own scale, so millimetre bodies
+    // turn under contact torques; false (default) keeps inverse()'s
+    // |det| < 1e-30 -> zero rule (myMat.h:163-194).  Applies from the next
+    // solve().
+    void usePhysicalInertia(const bool physical)
+    {
+        report(fundem_set_inertia_mode(sim_, physical ? FUNDEM_INERTIA_PHYSICAL : FUNDEM_INERTIA_REFERENCE),
+               "usePhysicalInertia");
+    }
+
     // ---------------------------------------------------------------- run
     // the loop of LSSolver::compute* (LSSolver.h:440-467, 1091-1229):
     // numStep = Tmax / dt + 1, iStep = 0 .. numStep inclusive

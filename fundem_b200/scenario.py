@@ -285,6 +285,9 @@ class Scenario:
     # quarter-sector periodicity about the z axis through domain_min
     # (LSSolver::addPeriodicBoundarySector)
     periodic_sector: bool = False
+    # inverse-inertia rule: "reference" (|det I| < 1e-30 gives zero, so
+    # mm-scale bodies never turn) or "physical" (scale-aware)
+    inertia: str = "reference"
     name: str = "scenario"
 
     def copy(self) -> "Scenario":

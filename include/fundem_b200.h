@@ -32,6 +32,8 @@ typedef enum {
 } fundem_status;
 
 enum { FUNDEM_FP64 = 0, FUNDEM_FP32_MIXED = 1 };
+/* inverse-inertia rule of the particle geometries */
+enum { FUNDEM_INERTIA_REFERENCE = 0, FUNDEM_INERTIA_PHYSICAL = 1 };
 /* contact list kinds */
 enum { FUNDEM_PP = 0, FUNDEM_PW = 1, FUNDEM_GX = 2, FUNDEM_GY = 3, FUNDEM_GXY = 4,
        FUNDEM_GR90 = 5, FUNDEM_GR180 = 6, FUNDEM_GR270 = 7 /* sector images */ };
@@ -121,6 +123,15 @@ int fundem_set_periodic(fundem_sim* sim, int x, int y);
    angular velocity is its body's, not turned, and a contact's reaction goes
    to the body unturned.  Takes effect at the next fundem_setup. */
 int fundem_set_periodic_sector(fundem_sim* sim, int on);
+/* inverse inertia of the particle geometries.  FUNDEM_INERTIA_REFERENCE
+   (default) keeps inverse() of myMat.h:163-194, which gives zero when
+   |det I| < 1e-30: bodies of millimetre scale (det of order 1e-34) then
+   never change their angular velocity.  FUNDEM_INERTIA_PHYSICAL inverts
+   every matrix that is not singular relative to its own scale
+   (|det I| > 1e-12 max(|Ixx|, |Iyy|, |Izz|)^3), so such bodies turn under
+   contact torques.  No counterpart in the reference.  Takes effect at the
+   next fundem_setup. */
+int fundem_set_inertia_mode(fundem_sim* sim, int mode);
 
 /* LSSolver::upload, LSSolver.h:692-703: domain and grids, template tables,
    device state.  May be called again (multi-phase runs): state already on

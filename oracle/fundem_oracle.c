@@ -207,13 +207,22 @@ static sm rot_tensor(qt q, sm I)
     r.yz = r1x * g + r1y * h + r1z * i;
     return r;
 }
-/* inverse with the |det| < 1e-30 -> zero quirk, myMat.h:163-194 */
-static sm inverse_sm(sm A)
+/* inverse with the |det| < 1e-30 -> zero quirk, myMat.h:163-194; with
+   physical != 0 the determinant is tested against the cube of the largest
+   diagonal entry (1e-12 relative) instead, the project's scale-aware rule */
+static sm inverse_sm_mode(sm A, int physical)
 {
     const double det = A.xx * (A.yy * A.zz - A.yz * A.yz) + A.xy * (A.yz * A.xz - A.xy * A.zz) +
                        A.xz * (A.xy * A.yz - A.yy * A.xz);
     sm r = {0, 0, 0, 0, 0, 0};
-    if (fabs(det) < 1e-30) return r;
+    if (physical) {
+        double m = fabs(A.xx);
+        if (fabs(A.yy) > m) m = fabs(A.yy);
+        if (fabs(A.zz) > m) m = fabs(A.zz);
+        if (!(m > 0.0) || !(fabs(det) > 1e-12 * m * m * m)) return r;
+    } else if (fabs(det) < 1e-30) {
+        return r;
+    }
     const double di = 1.0 / det;
     r.xx = (A.yy * A.zz - A.yz * A.yz) * di;
     r.yy = (A.xx * A.zz - A.xz * A.xz) * di;
@@ -223,6 +232,7 @@ static sm inverse_sm(sm A)
     r.yz = -(A.xx * A.yz - A.xz * A.xy) * di;
     return r;
 }
+static sm inverse_sm(sm A) { return inverse_sm_mode(A, 0); }
 void orc_inverse_sym(const double in[6], double out[6])
 {
     sm a = {in[0], in[1], in[2], in[3], in[4], in[5]};
@@ -319,6 +329,7 @@ struct orc_world {
     ghost_t GX, GY, GXY;
     ghost_t R90, R180, R270; /* sector images, PeriodicBoundary.h:319-425 */
     int perX, perY, sector;
+    int physical_inertia; /* 0: the reference's inverse() rule */
     bonds_t B;
 };
 
@@ -418,7 +429,7 @@ int orc_add_geometry(orc_world* w, int wall, double mass, const double inertia[6
     }
     g->inv_mass[k] = mass > 0.0 ? 1.0 / mass : 0.0;
     g->inertia[k] = I;
-    g->inv_inertia[k] = inverse_sm(I);
+    g->inv_inertia[k] = inverse_sm_mode(I, wall ? 0 : w->physical_inertia);
     g->origin[k] = v3(origin[0], origin[1], origin[2]);
     g->inv_spacing[k] = 1.0 / spacing;
     g->size[3 * k] = size[0]; g->size[3 * k + 1] = size[1]; g->size[3 * k + 2] = size[2];
@@ -617,6 +628,14 @@ int orc_add_bond(orc_world* w, int master, int slave, const double point[3],
 
 void orc_set_periodic(orc_world* w, int x, int y) { w->perX = x ? 1 : 0; w->perY = y ? 1 : 0; }
 void orc_set_sector(orc_world* w, int on) { w->sector = on ? 1 : 0; }
+
+/* inverse-inertia rule: 0 the reference's, 1 scale-aware; recomputes the
+   particle geometries already added */
+void orc_set_inertia_mode(orc_world* w, int physical)
+{
+    w->physical_inertia = physical ? 1 : 0;
+    for (int k = 0; k < w->P.geos.n; ++k) w->P.geos.inv_inertia[k] = inverse_sm_mode(w->P.geos.inertia[k], w->physical_inertia);
+}
 
 /* spatialGrid::set, mySpatialGrid.h:212-240 */
 static void grid_set(grid_t* g, d3 minb, d3 maxb, double cell)

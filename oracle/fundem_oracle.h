@@ -59,6 +59,7 @@ int orc_add_bond(orc_world* w, int master, int slave, const double point[3],
 void orc_set_periodic(orc_world* w, int x, int y);
 /* addPeriodicBoundarySector / removePeriodicBoundary, LSSolver.h:410-424 */
 void orc_set_sector(orc_world* w, int on);
+void orc_set_inertia_mode(orc_world* w, int physical);
 int orc_setup(orc_world* w, const double minb[3], const double maxb[3]);
 
 /* pre-loop detection (LSSolver.h:1093-1096 and the periodic variants) */

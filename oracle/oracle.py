@@ -55,6 +55,7 @@ def lib():
                                    C.c_double, C.c_double, C.c_double, C.c_double]
         L.orc_set_periodic.argtypes = [P, C.c_int, C.c_int]
         L.orc_set_sector.argtypes = [P, C.c_int]
+        L.orc_set_inertia_mode.argtypes = [P, C.c_int]
         L.orc_setup.argtypes = [P, D, D]
         L.orc_initial_detect.argtypes = [P]
         L.orc_step.argtypes = [P, D, C.c_double]
@@ -214,6 +215,7 @@ class OracleWorld:
                            float(B.tensile[k]), float(B.cohesion[k]), float(B.friction[k]))
         L.orc_set_periodic(w, int(sc.periodic_x), int(sc.periodic_y))
         L.orc_set_sector(w, int(getattr(sc, "periodic_sector", False)))
+        L.orc_set_inertia_mode(w, int(getattr(sc, "inertia", "reference") == "physical"))
         o.gravity = np.asarray(sc.gravity, float)
         o.dt = float(sc.dt)
         if setup:
