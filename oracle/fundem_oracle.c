@@ -977,16 +977,23 @@ static d3 sliding_spring(d3 prev, d3 sv, d3 n, d3 fn, double mu, double k, doubl
     }
     return spring;
 }
+/* 0: the reference's single-precision square roots in the damping terms
+   (contactKernel.cuh:51, 53, 58); 1: double precision, a smooth variant for
+   finite-difference checks of derivatives (test use only) */
+static int g_sqrt64 = 0;
+void orc_set_damping_sqrt64(int on) { g_sqrt64 = on ? 1 : 0; }
+static inline double damp_sqrt(double x) { return g_sqrt64 ? sqrt(x) : (double)sqrtf((float)x); }
+
 static void linear_contact(d3* F, d3* spring, d3 vc, d3 n, double delta, double dt, double kn,
                            double ks, double mu, double res, double m)
 {
     if (delta > 0.) {
         const double lr = log(res);
-        const double diss = -lr / (double)sqrtf((float)(lr * lr + PI * PI));
-        const double cn = 2. * diss * (double)sqrtf((float)(m * kn));
+        const double diss = -lr / damp_sqrt(lr * lr + PI * PI);
+        const double cn = 2. * diss * damp_sqrt(m * kn);
         const d3 vn = mul(n, dot(vc, n));
         const d3 fn = sub(mul(n, kn * delta), mul(vn, cn));
-        const double cs = 2. * diss * (double)sqrtf((float)(m * ks));
+        const double cs = 2. * diss * damp_sqrt(m * ks);
         const d3 vs = sub(vc, vn);
         *spring = sliding_spring(*spring, vs, n, fn, mu, ks, cs, dt);
         const d3 fs = sub(mul(*spring, -ks), mul(vs, cs));

@@ -60,6 +60,8 @@ void orc_set_periodic(orc_world* w, int x, int y);
 /* addPeriodicBoundarySector / removePeriodicBoundary, LSSolver.h:410-424 */
 void orc_set_sector(orc_world* w, int on);
 void orc_set_inertia_mode(orc_world* w, int physical);
+/* damping square roots: 0 single precision as the reference, 1 double (test use) */
+void orc_set_damping_sqrt64(int on);
 int orc_setup(orc_world* w, const double minb[3], const double maxb[3]);
 
 /* pre-loop detection (LSSolver.h:1093-1096 and the periodic variants) */

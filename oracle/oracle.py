@@ -56,6 +56,7 @@ def lib():
         L.orc_set_periodic.argtypes = [P, C.c_int, C.c_int]
         L.orc_set_sector.argtypes = [P, C.c_int]
         L.orc_set_inertia_mode.argtypes = [P, C.c_int]
+        L.orc_set_damping_sqrt64.argtypes = [C.c_int]
         L.orc_setup.argtypes = [P, D, D]
         L.orc_initial_detect.argtypes = [P]
         L.orc_step.argtypes = [P, D, C.c_double]
