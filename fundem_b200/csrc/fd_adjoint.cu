@@ -152,9 +152,10 @@ template <typename T> __device__ __forceinline__ T vdot(const V3<T>& a, const V3
 constexpr int NDIR = 13;  // rel 3, vc 3, sprev 3, kn, ks, diss, mu
 using D13 = Dual<NDIR>;
 
-__device__ bool contact_dual(const V3<D13>& rel, const V3<D13>& vc, const V3<D13>& sprev, const D13& kn,
+__device__ bool contact_dual(const V3<D13>& rel, V3<D13> vc, const V3<D13>& sprev, const D13& kn,
                              const D13& ks, const D13& diss, const D13& mu, double m, double dt, const FdGeo& GB,
-                             const double* sdf, const double qB[4], V3<D13>& F, V3<D13>& snew)
+                             const double* sdf, const double qB[4], const double3 wA, const double3 wB,
+                             V3<D13>& F, V3<D13>& snew)
 {
     // rotation matrix of the partner (rows: world <- body)
     const double q0 = qB[0], q1 = qB[1], q2 = qB[2], q3 = qB[3];
@@ -189,6 +190,20 @@ __device__ bool contact_dual(const V3<D13>& rel, const V3<D13>& vc, const V3<D13
     const D13 nl = dsqrt(vdot(nw, nw));
     if (!(nl.v > 0.0)) return false;
     const V3<D13> n = V3<D13>{nw.x / nl, nw.y / nl, nw.z / nl};
+    // The contact point is the node moved by n overlap / 2
+    // (LSParticleContactDetectionKernel.cu:268-281), so with turning bodies
+    // the velocity wA x (c - rA) - wB x (c - rB) moves with the point:
+    // its derivative adds wA x dh - wB x (drel + dh), h = n overlap / 2.
+    if (wA.x != 0.0 || wA.y != 0.0 || wA.z != 0.0 || wB.x != 0.0 || wB.y != 0.0 || wB.z != 0.0) {
+        const D13 half = ov * 0.5;
+        V3<D13> dh = scale(half, n), dr = rel;
+        dh.x.v = dh.y.v = dh.z.v = 0.0;  // derivative parts only
+        dr.x.v = dr.y.v = dr.z.v = 0.0;
+        const V3<D13> drh = dr + dh;
+        vc.x = vc.x + (dh.z * wA.y - dh.y * wA.z) - (drh.z * wB.y - drh.y * wB.z);
+        vc.y = vc.y + (dh.x * wA.z - dh.z * wA.x) - (drh.x * wB.z - drh.z * wB.x);
+        vc.z = vc.z + (dh.y * wA.x - dh.x * wA.y) - (drh.y * wB.x - drh.x * wB.y);
+    }
     F = V3<D13>{D13(0.0), D13(0.0), D13(0.0)};
     snew = F;
     if (!(ov.v > 0.0)) return true;
@@ -282,11 +297,16 @@ __global__ void __launch_bounds__(ADJ_TPB) k_adj_contact(AdjParticles a, AdjCont
     const FdGeo& GB = wall ? c.GW.geo[R.geoB[s]] : a.G.geo[R.geoB[s]];
     const double* sdf = wall ? c.GW.sdf : a.G.sdf;
     const double qB[4] = {R.qB[4 * s], R.qB[4 * s + 1], R.qB[4 * s + 2], R.qB[4 * s + 3]};
+    const double3 wA = a.angvel[A], wB = wall ? c.wall_angvel[R.B[s]] : a.angvel[Bp];
     V3<D13> F, snew;
-    if (!contact_dual(rel, vc, sprev, dkn, dks, ddiss, dmu, m, c.dt, GB, sdf, qB, F, snew)) return;
+    if (!contact_dual(rel, vc, sprev, dkn, dks, ddiss, dmu, m, c.dt, GB, sdf, qB, wA, wB, F, snew)) return;
+    // A contact with a particle's own periodic image has no reaction
+    // (contactKernel.cu:207-291), and its node offset and relative velocity
+    // do not move with the particle.
+    const bool react = !wall && Bp != A;
     // output adjoints: force on A (and its reaction), new spring
     double fb[3] = {a.Fb[3 * A], a.Fb[3 * A + 1], a.Fb[3 * A + 2]};
-    if (!wall) {
+    if (react) {
         fb[0] -= a.Fb[3 * Bp];
         fb[1] -= a.Fb[3 * Bp + 1];
         fb[2] -= a.Fb[3 * Bp + 2];
@@ -298,9 +318,11 @@ __global__ void __launch_bounds__(ADJ_TPB) k_adj_contact(AdjParticles a, AdjCont
         g[k] = fb[0] * F.x.d[k] + fb[1] * F.y.d[k] + fb[2] * F.z.d[k] + sb[0] * snew.x.d[k] +
                sb[1] * snew.y.d[k] + sb[2] * snew.z.d[k];
     // positions (the node offset is fixed: d rel / d x_A = I, d rel / d x_B = -I)
-    atomic_add3(a.xb + 3 * A, g[0], g[1], g[2]);
-    atomic_add3(a.vhb + 3 * A, g[3], g[4], g[5]);
-    if (!wall) {
+    if (wall || react) {
+        atomic_add3(a.xb + 3 * A, g[0], g[1], g[2]);
+        atomic_add3(a.vhb + 3 * A, g[3], g[4], g[5]);
+    }
+    if (react) {
         atomic_add3(a.xb + 3 * Bp, -g[0], -g[1], -g[2]);
         atomic_add3(a.vhb + 3 * Bp, -g[3], -g[4], -g[5]);
     }
@@ -332,8 +354,7 @@ __global__ void k_adj_bond(AdjParticles a, AdjBondArgs b)
     if (!(D.v > 1.0e-20)) return;
     const double B1 = b.B[4 * k], B2 = b.B[4 * k + 1], D0 = b.L0[k];
     const V3<D3> e{-(r.x / D), -(r.y / D), -(r.z / D)};
-    const double3 dn = b.dn[k];
-    const V3<D3> dnv{D3(dn.x), D3(dn.y), D3(dn.z)};
+    const V3<D3> dnv{D3(b.dn[3 * k]), D3(b.dn[3 * k + 1]), D3(b.dn[3 * k + 2])};
     const D3 dne = vdot(dnv, e);
     const D3 c1 = B1 * (D + (-D0));
     const D3 c2 = B2 / (2.0 * D);
@@ -359,18 +380,6 @@ __global__ void k_adj_particle(AdjParticles a, double dt)
     }
 }
 
-// the bond frame difference n1j - n1i in the world, from the recorded body
-// frames and the (fixed) orientations
-__global__ void k_adj_bond_frames(const double3* frames, const fd_quat* q, const int* master, const int* slave,
-                                  int n, double3* dn)
-{
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    const double3 n1i = fd_rot(q[master[k]], frames[8ll * k]);
-    const double3 n1j = fd_rot(q[slave[k]], frames[8ll * k + 4]);
-    dn[k] = n1j - n1i;
-}
-
 }  // namespace
 
 void adj_force(const AdjParticles& a, double dt, cudaStream_t s)
@@ -388,11 +397,6 @@ void adj_bonds(const AdjParticles& a, const AdjBondArgs& b, cudaStream_t s)
 void adj_particles(const AdjParticles& a, double dt, cudaStream_t s)
 {
     if (a.n > 0) k_adj_particle<<<(a.n + 255) / 256, 256, 0, s>>>(a, dt);
-}
-void adj_bond_frames(const double3* frames, const fd_quat* q, const int* master, const int* slave, int n, double3* dn,
-                     cudaStream_t s)
-{
-    if (n > 0) k_adj_bond_frames<<<(n + 255) / 256, 256, 0, s>>>(frames, q, master, slave, n, dn);
 }
 
 }  // namespace fd

@@ -9,6 +9,7 @@ struct AdjParticles {
     int n;
     const int* geo;
     const int* mat;
+    const double3* angvel;  // constant over the run: the bodies do not turn
     GeoSetDev G;
     double* xb;     // adjoint of the positions
     double* vb;     // adjoint of the velocities at the step's end
@@ -24,6 +25,7 @@ struct AdjContactArgs {
     MatDev M;              // particle materials
     MatDev MW;             // wall materials
     GeoSetDev GW;          // wall geometries
+    const double3* wall_angvel;  // prescribed wall angular velocities
     const double* Sb_cur;  // spring adjoints of this step's slots
     double* Sb_prev;       // spring adjoints of the previous step's slots (accumulated)
     int sb_prev_cap;
@@ -38,14 +40,12 @@ struct AdjBondArgs {
     const double* rij;     // recorded at the step
     const double* B;       // 4 per bond
     const double* L0;
-    const double3* dn;     // n1j - n1i, world frame
+    const double* dn;      // 3 per bond: n1j - n1i in the world frame, recorded at the step
 };
 
 void adj_force(const AdjParticles& a, double dt, cudaStream_t s);
 void adj_contacts(const AdjParticles& a, const AdjContactArgs& c, cudaStream_t s);
 void adj_bonds(const AdjParticles& a, const AdjBondArgs& b, cudaStream_t s);
 void adj_particles(const AdjParticles& a, double dt, cudaStream_t s);
-void adj_bond_frames(const double3* frames, const fd_quat* q, const int* master, const int* slave, int n, double3* dn,
-                     cudaStream_t s);
 
 }  // namespace fd

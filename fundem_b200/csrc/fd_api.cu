@@ -614,6 +614,7 @@ struct AdjTape {
     int nbond = 0;
     DevArray<int> bond_active;           // per step and bond
     DevArray<double> bond_rij;           // 3 per step and bond
+    DevArray<double> bond_dn;            // 3 per step and bond: n1j - n1i
     fd::AdjRec rec(int k, int t)
     {
         fd::AdjRec r{};
@@ -1037,6 +1038,7 @@ struct fundem_sim {
         if (recording && bd.n > 0) {
             bd.rec_active = recording->bond_active.p + (long long)record_step * bd.n;
             bd.rec_rij = recording->bond_rij.p + 3ll * record_step * bd.n;
+            bd.rec_dn = recording->bond_dn.p + 3ll * record_step * bd.n;
         }
         if (bd.n > 0) { fd::launch_bonds(Pv, bd, mixed(), stream); launches++; }
         fd::launch_reduce(Pv, views, active, rv, bd, mixed(), stream);
@@ -2166,8 +2168,8 @@ int fundem_adjoint_backward(fundem_sim* s, const double* dl_dpos, const double* 
         T.nbond = bd.n;
         T.bond_active.alloc((size_t)std::max(bd.n, 1) * K);
         T.bond_rij.alloc((size_t)std::max(bd.n, 1) * 3 * K);
+        T.bond_dn.alloc((size_t)std::max(bd.n, 1) * 3 * K);
         DevArray<double> xb, vb, vhb, Fb, Feb, pgrad, Sb[2][FD_NKIND];
-        DevArray<double3> dn;
         xb.alloc(3 * (size_t)np); vb.alloc(3 * (size_t)np); vhb.alloc(3 * (size_t)np);
         Fb.alloc(3 * (size_t)np); Feb.alloc(3 * (size_t)np); pgrad.alloc(4 * (size_t)std::max(nmat, 1));
         for (int k = 0; k < FD_NKIND; ++k) {
@@ -2176,10 +2178,8 @@ int fundem_adjoint_backward(fundem_sim* s, const double* dl_dpos, const double* 
         }
         xb.upload(dl_dpos, 3 * (size_t)np, s->stream);
         vb.upload(dl_dvel, 3 * (size_t)np, s->stream);
-        dn.alloc((size_t)std::max(bd.n, 1));
         const ObjDev Pv = s->P.view();
-        fd::adj_bond_frames(bd.frames, Pv.q, bd.master, bd.slave, bd.n, dn.p, s->stream);
-        fd::AdjParticles ap{np, Pv.geo, Pv.mat, s->pgeo.view(), xb.p, vb.p, vhb.p, Fb.p, Feb.p, pgrad.p};
+        fd::AdjParticles ap{np, Pv.geo, Pv.mat, Pv.angvel, s->pgeo.view(), xb.p, vb.p, vhb.p, Fb.p, Feb.p, pgrad.p};
         std::map<std::tuple<int, int, int>, double3> carry;
         int cur = 0;
         for (int seg = (int)A.ckpt.size() - 1; seg >= 0; --seg) {
@@ -2244,6 +2244,7 @@ int fundem_adjoint_backward(fundem_sim* s, const double* dl_dpos, const double* 
                     c.M = s->pmat.view();
                     c.MW = s->wmat.view();
                     c.GW = s->wgeo.view();
+                    c.wall_angvel = s->W.view().angvel;
                     c.Sb_cur = Sb[cur][k].p;
                     c.Sb_prev = Sb[prv][k].p;
                     c.sb_prev_cap = T.cap[k];
@@ -2252,7 +2253,7 @@ int fundem_adjoint_backward(fundem_sim* s, const double* dl_dpos, const double* 
                 }
                 if (bd.n > 0) {
                     fd::AdjBondArgs b{bd.n, bd.master, bd.slave, T.bond_active.p + (long long)t * bd.n,
-                                      T.bond_rij.p + 3ll * t * bd.n, bd.B, bd.L0, dn.p};
+                                      T.bond_rij.p + 3ll * t * bd.n, bd.B, bd.L0, T.bond_dn.p + 3ll * t * bd.n};
                     fd::adj_bonds(ap, b, s->stream);
                 }
                 fd::adj_particles(ap, A.dt, s->stream);

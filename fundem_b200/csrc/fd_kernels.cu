@@ -1817,6 +1817,9 @@ __global__ void k_bonds(ObjDev P, BondDev Bd)
         Bd.rec_rij[3 * k + 0] = rij.x;
         Bd.rec_rij[3 * k + 1] = rij.y;
         Bd.rec_rij[3 * k + 2] = rij.z;
+        Bd.rec_dn[3 * k + 0] = n1j.x - n1i.x;
+        Bd.rec_dn[3 * k + 1] = n1j.y - n1i.y;
+        Bd.rec_dn[3 * k + 2] = n1j.z - n1i.z;
     }
     const double D = length3(rij);
     if (!fd_is_zero(D)) {

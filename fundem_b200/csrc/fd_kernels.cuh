@@ -142,6 +142,7 @@ struct BondDev {
     const int* plist;      // bond id * 2 + side
     int* rec_active;       // adjoint recording (null when off): bond active at the step
     double* rec_rij;       // 3 per bond: bond vector rb_i - rb_j at the step
+    double* rec_dn;        // 3 per bond: frame difference n1j - n1i at the step
 };
 
 // Adjoint recording of one list at one step, one entry per contact slot
