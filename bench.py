@@ -420,38 +420,48 @@ def adjoint_cost(args, dev):
     x0 = sim.state()["pos"].copy()
     sim.close()
     steps, K = args.adjoint_steps, 500
-    s = F.Simulation.from_scenario(sc, device=dev, records=False)
-    s.detect()
-    s.sync()
-    t0 = time.perf_counter()
-    s.step(steps)
-    s.sync()
-    t_fwd = time.perf_counter() - t0
-    s.close()
-    s = F.Simulation.from_scenario(sc, device=dev, records=False)
-    s.detect()
-    s.adjoint_begin(K)
-    t0 = time.perf_counter()
-    s.adjoint_forward(steps)
-    t_rec = time.perf_counter() - t0
-    st = s.state()
-    tag = np.arange(0, n, n // 64)[:64]
-    dl_dx = np.zeros((n, 3))
-    dl_dx[:, 2] = 1.0 / n
-    dl_dx[tag] += 2.0 * (st["pos"][tag] - x0[tag]) / len(tag)
-    contacts = s.num_contacts(F.PP) + s.num_contacts(F.PW)
-    t0 = time.perf_counter()
-    gv0, gp = s.adjoint_backward(dl_dx, np.zeros((n, 3)))
-    t_bwd = time.perf_counter() - t0
-    s.adjoint_end()
-    s.close()
-    return {"workload": "adjoint pour: 4096 superellipsoids, 2 templates, six walls, dt 1e-6 s",
-            "steps": steps, "checkpoint_interval": K, "node_contacts_at_end": contacts,
-            "forward_s": t_fwd, "recorded_forward_s": t_rec, "backward_s": t_bwd,
-            "backward_over_forward": t_bwd / t_fwd, "total_over_forward": (t_rec + t_bwd) / t_fwd,
-            "dl_dparams": gp[0].tolist(), "dl_dparams_order": ["kn", "ks", "damping ratio", "mu"],
-            "note": "backward re-runs each checkpoint segment once with recording, then sweeps it in reverse; "
-                    "wall-clock times, the calls synchronise"}
+
+    def run(precision):
+        s = F.Simulation.from_scenario(sc, device=dev, records=False)
+        s.set_precision(precision)
+        s.detect()
+        s.sync()
+        t0 = time.perf_counter()
+        s.step(steps)
+        s.sync()
+        t_fwd = time.perf_counter() - t0
+        s.close()
+        s = F.Simulation.from_scenario(sc, device=dev, records=False)
+        s.set_precision(precision)
+        s.detect()
+        s.adjoint_begin(K)
+        t0 = time.perf_counter()
+        s.adjoint_forward(steps)
+        t_rec = time.perf_counter() - t0
+        st = s.state()
+        tag = np.arange(0, n, n // 64)[:64]
+        dl_dx = np.zeros((n, 3))
+        dl_dx[:, 2] = 1.0 / n
+        dl_dx[tag] += 2.0 * (st["pos"][tag] - x0[tag]) / len(tag)
+        contacts = s.num_contacts(F.PP) + s.num_contacts(F.PW)
+        t0 = time.perf_counter()
+        gv0, gp = s.adjoint_backward(dl_dx, np.zeros((n, 3)))
+        t_bwd = time.perf_counter() - t0
+        s.adjoint_end()
+        s.close()
+        return {"node_contacts_at_end": contacts, "forward_s": t_fwd, "recorded_forward_s": t_rec,
+                "backward_s": t_bwd, "backward_over_forward": t_bwd / t_fwd,
+                "total_over_forward": (t_rec + t_bwd) / t_fwd, "dl_dparams": gp[0].tolist()}
+
+    out = {"workload": "adjoint pour: 4096 superellipsoids, 2 templates, six walls, dt 1e-6 s",
+           "steps": steps, "checkpoint_interval": K}
+    out.update(run(F.FP64))
+    out["fp32_mixed"] = run(F.FP32_MIXED)
+    out["dl_dparams_order"] = ["kn", "ks", "damping ratio", "mu"]
+    out["note"] = ("backward re-runs each checkpoint segment once with recording, then sweeps it in reverse; "
+                   "wall-clock times, the calls synchronise; fp32_mixed: the FP32_MIXED step and its adjoint "
+                   "(the recorded single-precision run swept with double-precision Jacobians)")
+    return out
 
 
 def batched_cost(args, dev):

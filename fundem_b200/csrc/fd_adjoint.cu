@@ -32,91 +32,100 @@ namespace {
 constexpr int ADJ_TPB = 128;
 
 // ---------------------------------------------------------------------------
-// forward-mode dual numbers with N derivative directions
+// forward-mode dual numbers with N derivative directions over the scalar type
+// T (double for the FP64 step, float for the mixed-precision one); scalar
+// operands are doubles converted to T
 // ---------------------------------------------------------------------------
-template <int N>
+template <int N, typename T = double>
 struct Dual {
-    double v;
-    double d[N];
+    T v;
+    T d[N];
     __device__ Dual() {}
-    __device__ Dual(double x) : v(x)
+    __device__ Dual(double x) : v((T)x)
     {
 #pragma unroll
-        for (int i = 0; i < N; ++i) d[i] = 0.0;
+        for (int i = 0; i < N; ++i) d[i] = T(0);
     }
     __device__ static Dual var(double x, int i)
     {
         Dual r(x);
-        r.d[i] = 1.0;
+        r.d[i] = T(1);
         return r;
     }
 };
-template <int N> __device__ __forceinline__ Dual<N> operator+(const Dual<N>& a, const Dual<N>& b)
+template <int N, typename T> __device__ __forceinline__ Dual<N, T> operator+(const Dual<N, T>& a, const Dual<N, T>& b)
 {
-    Dual<N> r;
+    Dual<N, T> r;
     r.v = a.v + b.v;
 #pragma unroll
     for (int i = 0; i < N; ++i) r.d[i] = a.d[i] + b.d[i];
     return r;
 }
-template <int N> __device__ __forceinline__ Dual<N> operator-(const Dual<N>& a, const Dual<N>& b)
+template <int N, typename T> __device__ __forceinline__ Dual<N, T> operator-(const Dual<N, T>& a, const Dual<N, T>& b)
 {
-    Dual<N> r;
+    Dual<N, T> r;
     r.v = a.v - b.v;
 #pragma unroll
     for (int i = 0; i < N; ++i) r.d[i] = a.d[i] - b.d[i];
     return r;
 }
-template <int N> __device__ __forceinline__ Dual<N> operator-(const Dual<N>& a)
+template <int N, typename T> __device__ __forceinline__ Dual<N, T> operator-(const Dual<N, T>& a)
 {
-    Dual<N> r;
+    Dual<N, T> r;
     r.v = -a.v;
 #pragma unroll
     for (int i = 0; i < N; ++i) r.d[i] = -a.d[i];
     return r;
 }
-template <int N> __device__ __forceinline__ Dual<N> operator*(const Dual<N>& a, const Dual<N>& b)
+template <int N, typename T> __device__ __forceinline__ Dual<N, T> operator*(const Dual<N, T>& a, const Dual<N, T>& b)
 {
-    Dual<N> r;
+    Dual<N, T> r;
     r.v = a.v * b.v;
 #pragma unroll
     for (int i = 0; i < N; ++i) r.d[i] = a.d[i] * b.v + a.v * b.d[i];
     return r;
 }
-template <int N> __device__ __forceinline__ Dual<N> operator*(const Dual<N>& a, double s)
+template <int N, typename T> __device__ __forceinline__ Dual<N, T> operator*(const Dual<N, T>& a, double sd)
 {
-    Dual<N> r;
+    const T s = (T)sd;
+    Dual<N, T> r;
     r.v = a.v * s;
 #pragma unroll
     for (int i = 0; i < N; ++i) r.d[i] = a.d[i] * s;
     return r;
 }
-template <int N> __device__ __forceinline__ Dual<N> operator*(double s, const Dual<N>& a) { return a * s; }
-template <int N> __device__ __forceinline__ Dual<N> operator/(const Dual<N>& a, const Dual<N>& b)
+template <int N, typename T> __device__ __forceinline__ Dual<N, T> operator*(double s, const Dual<N, T>& a)
 {
-    Dual<N> r;
-    const double ib = 1.0 / b.v;
+    return a * s;
+}
+template <int N, typename T> __device__ __forceinline__ Dual<N, T> operator/(const Dual<N, T>& a, const Dual<N, T>& b)
+{
+    Dual<N, T> r;
+    const T ib = T(1) / b.v;
     r.v = a.v * ib;
 #pragma unroll
     for (int i = 0; i < N; ++i) r.d[i] = (a.d[i] - r.v * b.d[i]) * ib;
     return r;
 }
-template <int N> __device__ __forceinline__ Dual<N> operator/(double a, const Dual<N>& b)
+template <int N, typename T> __device__ __forceinline__ Dual<N, T> operator/(double a, const Dual<N, T>& b)
 {
-    return Dual<N>(a) / b;
+    return Dual<N, T>(a) / b;
 }
-template <int N> __device__ __forceinline__ Dual<N> operator+(const Dual<N>& a, double s)
+template <int N, typename T> __device__ __forceinline__ Dual<N, T> operator+(const Dual<N, T>& a, double s)
 {
-    Dual<N> r = a;
-    r.v += s;
+    Dual<N, T> r = a;
+    r.v += (T)s;
     return r;
 }
-template <int N> __device__ __forceinline__ Dual<N> operator-(double s, const Dual<N>& a) { return (-a) + s; }
-template <int N> __device__ __forceinline__ Dual<N> dsqrt(const Dual<N>& a)
+template <int N, typename T> __device__ __forceinline__ Dual<N, T> operator-(double s, const Dual<N, T>& a)
 {
-    Dual<N> r;
+    return (-a) + s;
+}
+template <int N, typename T> __device__ __forceinline__ Dual<N, T> dsqrt(const Dual<N, T>& a)
+{
+    Dual<N, T> r;
     r.v = sqrt(a.v);
-    const double g = r.v > 0.0 ? 0.5 / r.v : 0.0;
+    const T g = r.v > T(0) ? T(0.5) / r.v : T(0);
 #pragma unroll
     for (int i = 0; i < N; ++i) r.d[i] = a.d[i] * g;
     return r;
@@ -150,13 +159,18 @@ template <typename T> __device__ __forceinline__ T vdot(const V3<T>& a, const V3
 // recorded state falls in.
 // ---------------------------------------------------------------------------
 constexpr int NDIR = 13;  // rel 3, vc 3, sprev 3, kn, ks, diss, mu
-using D13 = Dual<NDIR>;
 
-__device__ bool contact_dual(const V3<D13>& rel, V3<D13> vc, const V3<D13>& sprev, const D13& kn,
-                             const D13& ks, const D13& diss, const D13& mu, double m, double dt, const FdGeo& GB,
-                             const double* sdf, const double qB[4], const double3 wA, const double3 wB,
-                             V3<D13>& F, V3<D13>& snew)
+// T is the scalar type of the duals (the launches use double).  The cell and
+// the position inside it come from the recorded double-precision node
+// offset, as in the forward kernels.
+template <typename T>
+__device__ bool contact_dual(const V3<Dual<NDIR, T>>& rel, const double3 reld, V3<Dual<NDIR, T>> vc,
+                             const V3<Dual<NDIR, T>>& sprev, const Dual<NDIR, T>& kn, const Dual<NDIR, T>& ks,
+                             const Dual<NDIR, T>& diss, const Dual<NDIR, T>& mu, double m, double dt,
+                             const FdGeo& GB, const T* sdf, const double qB[4], const double3 wA, const double3 wB,
+                             V3<Dual<NDIR, T>>& F, V3<Dual<NDIR, T>>& snew)
 {
+    using D13 = Dual<NDIR, T>;
     // rotation matrix of the partner (rows: world <- body)
     const double q0 = qB[0], q1 = qB[1], q2 = qB[2], q3 = qB[3];
     const double R[9] = {1.0 - 2.0 * (q2 * q2 + q3 * q3), 2.0 * (q1 * q2 - q0 * q3), 2.0 * (q1 * q3 + q0 * q2),
@@ -169,12 +183,18 @@ __device__ bool contact_dual(const V3<D13>& rel, V3<D13> vc, const V3<D13>& spre
     const D13 gx = (lx + (-GB.origin.x)) * GB.inv_spacing;
     const D13 gy = (ly + (-GB.origin.y)) * GB.inv_spacing;
     const D13 gz = (lz + (-GB.origin.z)) * GB.inv_spacing;
-    const int i0 = (int)floor(gx.v), j0 = (int)floor(gy.v), k0 = (int)floor(gz.v);
+    const double gxd = (reld.x * R[0] + reld.y * R[3] + reld.z * R[6] + (-GB.origin.x)) * GB.inv_spacing;
+    const double gyd = (reld.x * R[1] + reld.y * R[4] + reld.z * R[7] + (-GB.origin.y)) * GB.inv_spacing;
+    const double gzd = (reld.x * R[2] + reld.y * R[5] + reld.z * R[8] + (-GB.origin.z)) * GB.inv_spacing;
+    const int i0 = (int)floor(gxd), j0 = (int)floor(gyd), k0 = (int)floor(gzd);
     if (i0 < 0 || j0 < 0 || k0 < 0 || i0 >= GB.size.x - 1 || j0 >= GB.size.y - 1 || k0 >= GB.size.z - 1)
         return false;
-    const D13 fx = gx + (-(double)i0), fy = gy + (-(double)j0), fz = gz + (-(double)k0);
+    D13 fx = gx, fy = gy, fz = gz;
+    fx.v = (T)(gxd - (double)i0);
+    fy.v = (T)(gyd - (double)j0);
+    fz.v = (T)(gzd - (double)k0);
     const long long sx = GB.size.x, sxy = (long long)GB.size.x * GB.size.y;
-    const double* S = sdf + GB.sdf_off + (long long)k0 * sxy + (long long)j0 * sx + i0;
+    const T* S = sdf + GB.sdf_off + (long long)k0 * sxy + (long long)j0 * sx + i0;
     const double p[8] = {S[0], S[1], S[sx], S[sx + 1], S[sxy], S[sxy + 1], S[sxy + sx], S[sxy + sx + 1]};
     const D13 ux = 1.0 - fx, uy = 1.0 - fy, uz = 1.0 - fz;
     const D13 phi = ((p[0] * ux + p[1] * fx) * uy + (p[2] * ux + p[3] * fx) * fy) * uz +
@@ -257,8 +277,10 @@ __global__ void k_adj_force(AdjParticles a, double dt)
 }
 
 // the contacts of one list at one step
+template <typename T>
 __global__ void __launch_bounds__(ADJ_TPB) k_adj_contact(AdjParticles a, AdjContactArgs c)
 {
+    using D13 = Dual<NDIR, T>;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     const int nslots = min(*c.nslots, c.rec.cap);
     if (s >= nslots || !c.rec.hit[s]) return;
@@ -295,11 +317,15 @@ __global__ void __launch_bounds__(ADJ_TPB) k_adj_contact(AdjParticles a, AdjCont
     V3<D13> sprev{D13::var(R.sprev[3 * s], 6), D13::var(R.sprev[3 * s + 1], 7), D13::var(R.sprev[3 * s + 2], 8)};
     const D13 dkn = D13::var(kn, 9), dks = D13::var(ks, 10), ddiss = D13::var(diss, 11), dmu = D13::var(mu, 12);
     const FdGeo& GB = wall ? c.GW.geo[R.geoB[s]] : a.G.geo[R.geoB[s]];
-    const double* sdf = wall ? c.GW.sdf : a.G.sdf;
+    const T* sdf;
+    if constexpr (sizeof(T) == sizeof(double)) sdf = wall ? c.GW.sdf : a.G.sdf;
+    else sdf = wall ? c.GW.sdf32 : a.G.sdf32;
     const double qB[4] = {R.qB[4 * s], R.qB[4 * s + 1], R.qB[4 * s + 2], R.qB[4 * s + 3]};
     const double3 wA = a.angvel[A], wB = wall ? c.wall_angvel[R.B[s]] : a.angvel[Bp];
     V3<D13> F, snew;
-    if (!contact_dual(rel, vc, sprev, dkn, dks, ddiss, dmu, m, c.dt, GB, sdf, qB, wA, wB, F, snew)) return;
+    const double3 reld = make_double3(R.rel[3 * s], R.rel[3 * s + 1], R.rel[3 * s + 2]);
+    if (!contact_dual<T>(rel, reld, vc, sprev, dkn, dks, ddiss, dmu, m, c.dt, GB, sdf, qB, wA, wB, F, snew))
+        return;
     // A contact with a particle's own periodic image has no reaction
     // (contactKernel.cu:207-291), and its node offset and relative velocity
     // do not move with the particle.
@@ -315,8 +341,8 @@ __global__ void __launch_bounds__(ADJ_TPB) k_adj_contact(AdjParticles a, AdjCont
     double g[NDIR];
 #pragma unroll
     for (int k = 0; k < NDIR; ++k)
-        g[k] = fb[0] * F.x.d[k] + fb[1] * F.y.d[k] + fb[2] * F.z.d[k] + sb[0] * snew.x.d[k] +
-               sb[1] * snew.y.d[k] + sb[2] * snew.z.d[k];
+        g[k] = fb[0] * (double)F.x.d[k] + fb[1] * (double)F.y.d[k] + fb[2] * (double)F.z.d[k] +
+               sb[0] * (double)snew.x.d[k] + sb[1] * (double)snew.y.d[k] + sb[2] * (double)snew.z.d[k];
     // positions (the node offset is fixed: d rel / d x_A = I, d rel / d x_B = -I)
     if (wall || react) {
         atomic_add3(a.xb + 3 * A, g[0], g[1], g[2]);
@@ -343,11 +369,12 @@ __global__ void __launch_bounds__(ADJ_TPB) k_adj_contact(AdjParticles a, AdjCont
 
 // the bonds at one step: force F(r) on the master, -F on the slave, with the
 // body frames fixed (no rotation)
+template <typename T>
 __global__ void k_adj_bond(AdjParticles a, AdjBondArgs b)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= b.n || !b.active[k]) return;
-    using D3 = Dual<3>;
+    using D3 = Dual<3, T>;
     const int i = b.master[k], j = b.slave[k];
     const V3<D3> r{D3::var(b.rij[3 * k], 0), D3::var(b.rij[3 * k + 1], 1), D3::var(b.rij[3 * k + 2], 2)};
     const D3 D = dsqrt(vdot(r, r));
@@ -362,7 +389,7 @@ __global__ void k_adj_bond(AdjParticles a, AdjBondArgs b)
     const double fb[3] = {a.Fb[3 * i] - a.Fb[3 * j], a.Fb[3 * i + 1] - a.Fb[3 * j + 1], a.Fb[3 * i + 2] - a.Fb[3 * j + 2]};
     double g[3];
 #pragma unroll
-    for (int t = 0; t < 3; ++t) g[t] = fb[0] * F.x.d[t] + fb[1] * F.y.d[t] + fb[2] * F.z.d[t];
+    for (int t = 0; t < 3; ++t) g[t] = fb[0] * (double)F.x.d[t] + fb[1] * (double)F.y.d[t] + fb[2] * (double)F.z.d[t];
     atomic_add3(a.xb + 3 * i, g[0], g[1], g[2]);
     atomic_add3(a.xb + 3 * j, -g[0], -g[1], -g[2]);
 }
@@ -386,13 +413,16 @@ void adj_force(const AdjParticles& a, double dt, cudaStream_t s)
 {
     if (a.n > 0) k_adj_force<<<(a.n + 255) / 256, 256, 0, s>>>(a, dt);
 }
+// Both precisions of the step are swept with double-precision Jacobians: the
+// single-precision evaluation of a contact's Jacobian gave non-finite
+// gradients on a 4,096-particle pour, where contacts separate from the walls.
 void adj_contacts(const AdjParticles& a, const AdjContactArgs& c, cudaStream_t s)
 {
-    if (c.rec.cap > 0) k_adj_contact<<<(c.rec.cap + ADJ_TPB - 1) / ADJ_TPB, ADJ_TPB, 0, s>>>(a, c);
+    if (c.rec.cap > 0) k_adj_contact<double><<<(c.rec.cap + ADJ_TPB - 1) / ADJ_TPB, ADJ_TPB, 0, s>>>(a, c);
 }
 void adj_bonds(const AdjParticles& a, const AdjBondArgs& b, cudaStream_t s)
 {
-    if (b.n > 0) k_adj_bond<<<(b.n + 255) / 256, 256, 0, s>>>(a, b);
+    if (b.n > 0) k_adj_bond<double><<<(b.n + 255) / 256, 256, 0, s>>>(a, b);
 }
 void adj_particles(const AdjParticles& a, double dt, cudaStream_t s)
 {

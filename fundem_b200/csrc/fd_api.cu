@@ -644,6 +644,7 @@ struct AdjState {
     double3 g{0, 0, 0};
     double dt = 0.0;
     bool dt_set = false;
+    int precision = FUNDEM_FP64;       // of the recorded run: its re-runs and Jacobians use it
     long long steps = 0;
     std::vector<AdjCheckpoint> ckpt;   // state at the start of each segment
     std::vector<int> seg_steps;        // steps in each segment
@@ -2081,10 +2082,6 @@ int fundem_adjoint_begin(fundem_sim* s, int checkpoint_interval)
 {
     if (!s || checkpoint_interval < 1) return FUNDEM_ERR_ARG;
     if (!s->setup_done || !s->detected) return FUNDEM_ERR_STATE;
-    if (s->precision != FUNDEM_FP64) {
-        s->last_error = "the adjoint differentiates the FP64 path";
-        return FUNDEM_ERR_STATE;
-    }
     if (s->sector) {
         s->last_error = "the adjoint does not differentiate through the turned images of sector periodicity";
         return FUNDEM_ERR_STATE;
@@ -2100,6 +2097,7 @@ int fundem_adjoint_begin(fundem_sim* s, int checkpoint_interval)
         AdjState& A = s->adj;
         A = AdjState{};
         A.on = true;
+        A.precision = s->precision;
         A.K = checkpoint_interval;
         A.ckpt.emplace_back();
         adj_snapshot(s, A.ckpt.back());
@@ -2116,6 +2114,10 @@ int fundem_adjoint_forward(fundem_sim* s, int nsteps, const double g[3], double 
     if (A.dt_set && (A.dt != dt || A.g.x != gg.x || A.g.y != gg.y || A.g.z != gg.z)) {
         s->last_error = "the adjoint needs one time step and one gravity over the recording";
         return FUNDEM_ERR_ARG;
+    }
+    if (s->precision != A.precision) {
+        s->last_error = "the precision changed since fundem_adjoint_begin";
+        return FUNDEM_ERR_STATE;
     }
     A.g = gg;
     A.dt = dt;
@@ -2147,6 +2149,10 @@ int fundem_adjoint_backward(fundem_sim* s, const double* dl_dpos, const double* 
     if (!s || !dl_dpos || !dl_dvel || !dl_dvel0 || !dl_dparams) return FUNDEM_ERR_ARG;
     AdjState& A = s->adj;
     if (!A.on || A.steps == 0) return FUNDEM_ERR_STATE;
+    if (s->precision != A.precision) {
+        s->last_error = "the precision changed since fundem_adjoint_begin";
+        return FUNDEM_ERR_STATE;
+    }
     return guard(s, [&] {
         FD_CUDA(cudaSetDevice(s->device));
         adj_snapshot(s, A.final_state);

@@ -1584,6 +1584,7 @@ __global__ void __launch_bounds__(TPB, FD_CONTACT_MIN_BLOCKS) k_contact32(Narrow
                 const v3f arm = r + (0.5f * ov) * nrm;  // contact point relative to A's centre
                 nid = n.P.node_base[A] + n.G.node_lid[pool];
                 double3 spring = mk3(0., 0., 0.);
+                int hist = -1;
                 {
                     const int oc_off = aux.w, oc_end = aux.w + L.p_hist_cnt[p];
                     int lo2 = oc_off, hi2 = oc_end;
@@ -1594,7 +1595,29 @@ __global__ void __launch_bounds__(TPB, FD_CONTACT_MIN_BLOCKS) k_contact32(Narrow
                     if (lo2 < oc_end && L.o_c_k[lo2] == k && L.o_c_node[lo2] == nid) {
                         const double* sp = L.o_c_spring + 3ll * lo2;
                         spring = mk3(sp[0], sp[1], sp[2]);
+                        hist = lo2;
                     }
+                }
+                const AdjRec& R = n.a.rec;
+                if (R.hit && s < R.cap) {
+                    const fd_quat qB = Slave<KIND>::q(n, B);
+                    R.A[s] = A;
+                    R.B[s] = B;
+                    R.Bp[s] = KIND == FD_PW ? -1 : B;
+                    R.geoB[s] = KIND == FD_PW ? n.W.geo[B] : n.P.geo[B];
+                    R.matB[s] = KIND == FD_PW ? n.W.mat[B] : n.P.mat[B];
+                    R.nid[s] = nid;
+                    R.hist[s] = hist;
+                    R.rel[3 * s + 0] = gp.x - cB.x;
+                    R.rel[3 * s + 1] = gp.y - cB.y;
+                    R.rel[3 * s + 2] = gp.z - cB.z;
+                    R.sprev[3 * s + 0] = spring.x;
+                    R.sprev[3 * s + 1] = spring.y;
+                    R.sprev[3 * s + 2] = spring.z;
+                    R.qB[4 * s + 0] = qB.q0;
+                    R.qB[4 * s + 1] = qB.q1;
+                    R.qB[4 * s + 2] = qB.q2;
+                    R.qB[4 * s + 3] = qB.q3;
                 }
                 const int mi = n.P.mat[A];
                 float kn = 0.f, ks = 0.f;
@@ -1634,6 +1657,11 @@ __global__ void __launch_bounds__(TPB, FD_CONTACT_MIN_BLOCKS) k_contact32(Narrow
                     const v3f vj = tof(vjd);
                     const v3f wj = tof(KIND == FD_PW ? n.W.angvel[B] : n.P.angvel[B]);
                     const v3f vc = (vi + crossf(wi, armA)) - (vj + crossf(wj, armB));
+                    if (R.hit && s < R.cap) {
+                        R.vc[3 * s + 0] = vc.x;
+                        R.vc[3 * s + 1] = vc.y;
+                        R.vc[3 * s + 2] = vc.z;
+                    }
                     const v3f F = linear_contact32(spring, vc, nrm, ov, (float)n.a.dt, kn, ks, mu, res, effM);
                     const v3f TA = crossf(armA, F);
                     const v3f TB = crossf(armB, -F);
@@ -1659,6 +1687,7 @@ __global__ void __launch_bounds__(TPB, FD_CONTACT_MIN_BLOCKS) k_contact32(Narrow
                 }
             }
             L.c_node[s] = nid;
+            if (n.a.rec.hit && s < n.a.rec.cap) n.a.rec.hit[s] = hit ? 1 : 0;
         }
         hits += __popc(__ballot_sync(0xffffffffu, hit));
     }
@@ -1866,6 +1895,7 @@ __global__ void k_bonds32(ObjDev P, BondDev Bd)
     double* E = Bd.energy + 6ll * k;
     float* O = reinterpret_cast<float*>(Bd.out) + 9ll * k;
     for (int t = 0; t < 9; ++t) O[t] = 0.f;
+    if (Bd.rec_active) Bd.rec_active[k] = Bd.active[k] != 0;
     if (Bd.active[k] == 0) {
         for (int t = 0; t < 6; ++t) E[t] = 0.;
         return;
@@ -1882,6 +1912,14 @@ __global__ void k_bonds32(ObjDev P, BondDev Bd)
     v3f F = mkf(0.f, 0.f, 0.f), Mij = mkf(0.f, 0.f, 0.f), Mji = mkf(0.f, 0.f, 0.f);
     int act = 1;
     const v3f rij = tof(ri - rj) + (oi - oj);
+    if (Bd.rec_rij) {
+        Bd.rec_rij[3 * k + 0] = rij.x;
+        Bd.rec_rij[3 * k + 1] = rij.y;
+        Bd.rec_rij[3 * k + 2] = rij.z;
+        Bd.rec_dn[3 * k + 0] = n1j.x - n1i.x;
+        Bd.rec_dn[3 * k + 1] = n1j.y - n1i.y;
+        Bd.rec_dn[3 * k + 2] = n1j.z - n1i.z;
+    }
     const float D = lenf(rij);
     if (D > 1e-20f) {
         const float B1 = (float)Bd.B[4 * k], B2 = (float)Bd.B[4 * k + 1], B3 = (float)Bd.B[4 * k + 2],

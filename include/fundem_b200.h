@@ -229,14 +229,18 @@ int fundem_prefix_sum(int* d_prefix, const int* d_count, long long n, void* stre
 #define FUNDEM_NOALLOC_SCAN_MAX 16777216LL
 int fundem_prefix_sum_noalloc(int* d_prefix, const int* d_count, long long n, void* stream);
 
-/* Reverse-mode gradients (the adjoint of the FP64 step).  No counterpart in
-   the reference.  Loss gradients on the final state are carried back to the
+/* Reverse-mode gradients (the adjoint of the step, in the precision set when
+   the recording begins: FP64, or FP32_MIXED, whose recorded single-precision
+   run is swept with double-precision contact and bond Jacobians; the
+   precision may not change while recording).  No counterpart in the reference.  Loss gradients on the final state are carried back to the
    initial velocities and to each particle material's normal stiffness,
    shear stiffness, damping ratio and friction coefficient.  Contact topology
    is frozen at each step, as the forward run had it (including each
    contact's stick or slip and each bond's breakage); orientations are
    taken as fixed, so every particle geometry must have a zero inverse
-   inertia (as the reference's inverse() gives mm-scale particles).
+   inertia (as the reference's inverse() gives mm-scale particles); constant
+   angular velocities of particles and prescribed ones of walls enter the
+   contact velocities.  Sector periodicity is not differentiated.
    begin: start recording from the current state (after fundem_detect),
      with a checkpoint every checkpoint_interval steps;
    forward: run steps (one gravity and time step for the whole recording);
