@@ -2163,8 +2163,16 @@ int fundem_adjoint_backward(fundem_sim* s, const double* dl_dpos, const double* 
         // tape for one segment
         AdjTape& T = s->tape;
         T.steps = K;
+        // lists the step fills: particle pairs, walls, and the ghost
+        // directions in use (the adjoint refuses sector periodicity); the
+        // others keep no tape and are skipped by the sweep
+        bool used[FD_NKIND] = {};
+        used[FD_PP] = used[FD_PW] = true;
+        used[FD_GX] = s->ghosts[0].active;
+        used[FD_GY] = s->ghosts[1].active;
+        used[FD_GXY] = s->ghosts[2].active;
         for (int k = 0; k < FD_NKIND; ++k) {
-            T.cap[k] = s->lists[k].allocated ? s->lists[k].cap_contacts : 0;
+            T.cap[k] = (used[k] && s->lists[k].allocated) ? s->lists[k].cap_contacts : 0;
             const size_t c = (size_t)std::max(T.cap[k], 1);
             T.ints[k].alloc(8 * c * K, false);
             T.dbl[k].alloc(13 * c * K, false);
