@@ -107,3 +107,52 @@ def test_tangent_matches_central_differences(oracle_mod, smooth_damping, case):
     Lp, Lm = loss(_with(sc, dv=h * r)), loss(_with(sc, dv=-h * r))
     central = (Lp - Lm) / (2 * h)
     assert abs(D[4] - central) <= 1e-6 * abs(central) + 1e-9, (D[4], central)
+
+
+def test_tangent_two_materials(oracle_mod, smooth_damping):
+    """The 48-body cluster with two particle materials (harmonic-mean
+    stiffness and minimum friction and restitution between them), five
+    walls and bodies spinning at about 20 rad/s, made translating: all eight
+    material gradients against central differences (relative step 1e-6)
+    within 1e-4 relative (observed 2e-5 at most, on the smallest ones)."""
+    from oracle import tangent
+    sc = copy.deepcopy(PC.cluster())
+    for g in sc.particle_geometries:
+        if g.density is not None:  # the template registered through a density
+            g.density = None
+            g.mass = 1.5e-3
+        g.inertia = np.zeros(6)
+    sc.wall_materials = [(0.9, 0.95)] * len(sc.wall_materials)
+    assert len(sc.particle_materials) == 2 and set(np.unique(sc.particles.mat)) == {0, 1}
+    n = len(sc.particles)
+    rng = np.random.default_rng(2)
+    w = rng.standard_normal((n, 3))
+    u = rng.standard_normal((n, 3)) * 1e-3
+    tr = tangent.TangentRun(sc)
+    tr.step(T)
+    D = tr.directional(w, u)
+    tr.close()
+
+    def loss(s2):
+        o = oracle_mod.OracleWorld.from_scenario(s2)
+        o.initial_detect()
+        o.step(T)
+        st = o.state()
+        o.close()
+        return float(np.sum(w * st["pos"]) + np.sum(u * st["vel"]))
+
+    for m in range(2):
+        kn, ks, mu, e = sc.particle_materials[m]
+        for k, x0 in enumerate((kn, ks, _zeta(e), mu)):
+            def moved(x):
+                s2 = copy.deepcopy(sc)
+                a = list(s2.particle_materials[m])
+                if k == 2:
+                    a[3] = float(np.exp(-np.pi * x / np.sqrt(1.0 - x * x)))
+                else:
+                    a[(0, 1, None, 2)[k]] = x
+                s2.particle_materials[m] = tuple(a)
+                return s2
+            h = 1e-6 * x0
+            central = (loss(moved(x0 + h)) - loss(moved(x0 - h))) / (2 * h)
+            assert abs(D[4 * m + k] - central) <= 1e-4 * abs(central), (m, k, D[4 * m + k], central)
