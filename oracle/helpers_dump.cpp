@@ -24,6 +24,9 @@
 //   PH name x0 y0 z0 x1 y1 z1 r                    buildHexInBox
 //   PB name x0 y0 z0 x1 y1 z1 n rmin rmax seed attempts   random packing in a box
 //   PC name ax ay az bx by bz R n rmin rmax seed attempts  random packing in a cylinder
+//   QR name x0 y0 z0 x1 y1 z1 r                    SpherePack::buildRegularInBox (kernel/Packing.h)
+//   QH name x0 y0 z0 x1 y1 z1 r                    SpherePack::buildHexInBox
+//   QB name x0 y0 z0 x1 y1 z1 n rmin rmax seed attempts   SpherePack::buildNonOverlappingInBox_LargeFirst
 // Shapes write name/vertices, name/triangles and, unless `nogrid`, the grid of
 // buildGridByResolution(res, pad): name/origin, name/size, name/spacing,
 // name/sdf.  Packings write name/centers and name/radii.
@@ -40,6 +43,7 @@
 #include "kernel/helper/LevelSetObjectGenerator.h"
 #include "kernel/helper/OBJLoader.h"
 #include "kernel/helper/SpherePackingGenerator.h"
+#include "kernel/Packing.h"
 
 namespace {
 
@@ -165,6 +169,26 @@ int run(bool grid, int argc, char** argv)
                                ? SpherePacking::buildNonOverlappingInBox_LargeFirst(a, b, n, rmin, rmax, seed, attempts)
                                : SpherePacking::buildNonOverlappingInCylinder_LargeFirst(a, b, R, n, rmin, rmax, seed,
                                                                                          attempts));
+        } else if (kind == "QR" || kind == "QH" || kind == "QB") {
+            double3 a, b;
+            in >> a.x >> a.y >> a.z >> b.x >> b.y >> b.z;
+            SpherePack p;
+            if (kind == "QB") {
+                double rmin, rmax;
+                int n, attempts;
+                uint32_t seed;
+                in >> n >> rmin >> rmax >> seed >> attempts;
+                p.buildNonOverlappingInBox_LargeFirst(a, b, n, rmin, rmax, seed, attempts);
+            } else {
+                double r;
+                in >> r;
+                if (kind == "QR") p.buildRegularInBox(a, b, r);
+                else p.buildHexInBox(a, b, r);
+            }
+            SpherePacking::Pack q;
+            q.centers = p.centers;
+            q.radii = p.radii;
+            put_pack(name, q);
         } else {
             std::cerr << "helpers_dump: unknown case kind " << kind << std::endl;
             return 2;

@@ -47,6 +47,11 @@ PR regular 0.0 0.0 0.0 1.0 1.0 3.0 0.1
 PH hex 0.0 0.0 0.0 1.0 1.0 1.0 0.07
 PB box_random 0.0 0.0 0.0 1.0 1.0 2.0 300 0.03 0.08 12345 2000
 PC drum_random -1.0 0.0 0.0 1.0 0.0 0.0 2.0 500 0.1 0.3 12345 2000
+QR pack_regular 0.0 0.0 0.0 1.0 1.0 3.0 0.1
+QH pack_hex -0.5 0.0 0.2 1.0 1.3 1.0 0.07
+QB pack_random 1.0 2.0 3.0 0.0 0.0 0.0 400 0.02 0.09 777 500
+QB pack_crowded 0.0 0.0 0.0 0.5 0.5 0.5 2000 0.03 0.05 12345 200
+QB pack_thin 0.0 0.0 0.0 2.0 2.0 0.05 50 0.03 0.04 3 100
 """
 
 

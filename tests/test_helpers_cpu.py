@@ -58,10 +58,11 @@ def _records(exe, golden, mode):
 
 @needs_gxx
 def test_meshes_and_packings_bit_exact(dump_exe, golden):
-    """Surface meshes of every shape (vertex order included), the OBJ mesh and
-    all four packings equal the reference's, bit for bit."""
+    """Surface meshes of every shape (vertex order included), the OBJ mesh,
+    the four SpherePacking:: packings and the five SpherePack (kernel/Packing.h)
+    packings equal the reference's, bit for bit."""
     rec = _records(dump_exe, golden, "nogrid")
-    assert len(rec) == 32
+    assert len(rec) == 42
     for k, v in rec.items():
         assert v.dtype == golden[k].dtype and v.shape == golden[k].shape, k
         assert np.array_equal(v, golden[k]), k
