@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "../../include/fundem_b200.h"
+#include "CUDAKernelFunction/myUtility/myFileEdit.h"
 #include "CUDAKernelFunction/myUtility/myMat.h"
 #include "CUDAKernelFunction/myUtility/myQua.h"
 #include "CUDAKernelFunction/myUtility/myVec.h"
