@@ -11,6 +11,7 @@
 
 #include "../../include/fundem_b200.h"
 #include "CUDAKernelFunction/myUtility/myFileEdit.h"
+#include "CUDAKernelFunction/myUtility/myHostDeviceArray.h"
 #include "CUDAKernelFunction/myUtility/myMat.h"
 #include "CUDAKernelFunction/myUtility/myQua.h"
 #include "CUDAKernelFunction/myUtility/myVec.h"
