@@ -278,35 +278,125 @@ class TangentRun:
 
     def _contacts(self, kind, c, P, W, dvh, dF):
         nd = self.nd
-        m = len(c["master"])
-        if m == 0:
+        S = self._contact_setup(kind, c, P, W)
+        if S is None:
             return ({}, c["spring"], np.zeros((nd, 0, 3)))
-        A = self.node_pid[c["master"]]
-        j = c["slave"].astype(np.int64)
-        wall = kind == O.PW
-        ghost = kind in self.shift
-        point, normal, overlap = c["point"], c["normal"], c["overlap"]
-        gp = point - normal * (0.5 * overlap)[:, None]
-        if wall:
-            rj, vj, wj, qB = W["pos"][j], W["vel"][j], W["angvel"][j], W["quat"][j]
-            G, geoB = self.wgeo, self.wall_geo[j]
-        else:
-            rj, vj, wj, qB = P["pos"][j], P["vel"][j], P["angvel"][j], P["quat"][j]
-            if ghost:
-                rj = rj + self.shift[kind]
-            G, geoB = self.pgeo, self.geo[j]
-        # a contact with a particle's own periodic image has no reaction
-        react = np.zeros(m, bool) if wall else (j != A) if ghost else np.ones(m, bool)
-        ri, vi, wi = P["pos"][A], P["vel"][A], P["angvel"][A]
+        A, j, wall, react, m = S.A, S.j, S.wall, S.react, S.m
         # rel = gp - r_B: derivative dx_A - dx_B (zero for a particle's own
         # image); walls do not move with the parameters
-        rel = v3(gp - rj, self.dx[:, A, :] - (0.0 if wall else self.dx[:, j, :]))
-        # the partner's SDF at the node
-        R = rotation(qB)
+        rel = v3(S.gp - S.rj, self.dx[:, A, :] - (0.0 if wall else self.dx[:, j, :]))
+        vc = v3(S.vc_val, dvh[:, A, :] - (0.0 if wall else dvh[:, j, :]))
+        pad = np.zeros((nd - self.np_dirs, m))
+        Kn = Dual(S.kn, np.vstack([S.w_kn, pad]))
+        Ks = Dual(S.ks, np.vstack([S.w_ks, pad]))
+        Diss = Dual(S.diss, np.vstack([S.w_diss, pad]))
+        Mu = Dual(S.mu, np.vstack([S.w_mu, pad]))
+        # the previous spring: first match of (node, partner) in the previous list
+        _, spr_prev, dS_prev = self.lists[kind]
+        has, hc = S.hist >= 0, np.where(S.hist >= 0, S.hist, 0)
+        sp_val = np.where(has[:, None], spr_prev[hc] if len(spr_prev) else 0.0, 0.0)
+        sp_der = np.where(has[None, :, None], dS_prev[:, hc, :] if dS_prev.shape[1] else 0.0, 0.0)
+        F, snew, ok = self._contact_eval(S, rel, vc, v3(sp_val, sp_der), Kn, Ks, Diss, Mu)
+        Fd = np.where(ok[None, :, None], F.derivs(), 0.0)
+        Sd = np.where(ok[None, :, None], snew.derivs(), 0.0)
+        Sv = np.where(ok[:, None], snew.value(), 0.0)
+        scale = max(float(np.abs(c["spring"]).max()), 1e-300)
+        self.max_spring_dev = max(self.max_spring_dev, float(np.abs(Sv - c["spring"]).max()) / scale)
+        np.add.at(dF, (slice(None), A), Fd)
+        if not wall:
+            np.add.at(dF, (slice(None), j[react]), -Fd[:, react])
+        return (self._keys(c), c["spring"], Sd)
+
+    class _Contacts:
+        """Values of one contact list at one step (see _contact_setup)."""
+
+    def _contact_setup(self, kind, c, P, W):
+        """Partners, state values, effective parameters and their weights on
+        the material parameter directions (4 per material: kn, ks, damping
+        ratio, friction), and history slots of the contacts of list `kind`
+        (contactKernel.cu:46-291)."""
+        m = len(c["master"])
+        if m == 0:
+            return None
+        S = TangentRun._Contacts()
+        S.m, S.kind = m, kind
+        S.A = A = self.node_pid[c["master"]]
+        S.j = j = c["slave"].astype(np.int64)
+        S.wall = wall = kind == O.PW
+        ghost = kind in self.shift
+        point, normal, overlap = c["point"], c["normal"], c["overlap"]
+        S.overlap = overlap
+        S.gp = point - normal * (0.5 * overlap)[:, None]
+        if wall:
+            rj, vj, S.wj, S.qB = W["pos"][j], W["vel"][j], W["angvel"][j], W["quat"][j]
+            S.G, S.geoB = self.wgeo, self.wall_geo[j]
+        else:
+            rj, vj, S.wj, S.qB = P["pos"][j], P["vel"][j], P["angvel"][j], P["quat"][j]
+            if ghost:
+                rj = rj + self.shift[kind]
+            S.G, S.geoB = self.pgeo, self.geo[j]
+        S.rj = rj
+        # a contact with a particle's own periodic image has no reaction
+        S.react = np.zeros(m, bool) if wall else (j != A) if ghost else np.ones(m, bool)
+        ri, vi = P["pos"][A], P["vel"][A]
+        S.wi = P["angvel"][A]
+        S.vc_val = (vi + np.cross(S.wi, point - ri)) - (vj + np.cross(S.wj, point - rj))
+        # effective parameters and their weights on the material directions
+        mi = self.mat[A]
+        kni, ksi, mui, ei = self.kn[mi], self.ks[mi], self.mu[mi], self.e[mi]
+        im_i = self.inv_mass[A]
+        w = [np.zeros((self.np_dirs, m)) for _ in range(4)]
+        cols = np.arange(m)
+        if wall:
+            mw = self.wall_mat[j]
+            kn, ks = kni, ksi
+            mu = np.minimum(mui, self.wmu[mw])
+            res = np.minimum(ei, self.we[mw])
+            meff = np.where(im_i > 0, 1.0 / np.where(im_i > 0, im_i, 1.0), 0.0)
+            w[0][4 * mi, cols] = 1.0
+            w[1][4 * mi + 1, cols] = 1.0
+            own_e, own_mu = ei <= self.we[mw], mui <= self.wmu[mw]
+            w[2][4 * mi[own_e] + 2, cols[own_e]] = 1.0
+            w[3][4 * mi[own_mu] + 3, cols[own_mu]] = 1.0
+        else:
+            mj = self.mat[j]
+            knj, ksj = self.kn[mj], self.ks[mj]
+            okn, oks = (kni > 0) & (knj > 0), (ksi > 0) & (ksj > 0)
+            skn, sks = np.where(okn, kni + knj, 1.0), np.where(oks, ksi + ksj, 1.0)
+            kn = np.where(okn, kni * knj / skn, 0.0)
+            ks = np.where(oks, ksi * ksj / sks, 0.0)
+            np.add.at(w[0], (4 * mi, cols), np.where(okn, knj * knj / skn ** 2, 0.0))
+            np.add.at(w[0], (4 * mj, cols), np.where(okn, kni * kni / skn ** 2, 0.0))
+            np.add.at(w[1], (4 * mi + 1, cols), np.where(oks, ksj * ksj / sks ** 2, 0.0))
+            np.add.at(w[1], (4 * mj + 1, cols), np.where(oks, ksi * ksi / sks ** 2, 0.0))
+            im_j = self.inv_mass[j]
+            ssum = im_i + im_j
+            meff = np.where((im_i > 0) | (im_j > 0), 1.0 / np.where(ssum != 0, ssum, 1.0), 0.0)
+            res = np.minimum(ei, self.e[mj])
+            mu = np.minimum(mui, self.mu[mj])
+            w[2][4 * np.where(ei <= self.e[mj], mi, mj) + 2, cols] = 1.0
+            w[3][4 * np.where(mui <= self.mu[mj], mi, mj) + 3, cols] = 1.0
+        S.kn = np.broadcast_to(np.asarray(kn, float), (m,)).copy()
+        S.ks = np.broadcast_to(np.asarray(ks, float), (m,)).copy()
+        S.diss = _diss(res)
+        S.mu = np.asarray(mu, float)
+        S.meff = meff
+        S.w_kn, S.w_ks, S.w_diss, S.w_mu = w
+        keys = self.lists[kind][0]
+        S.hist = np.array([keys.get((int(a), int(b)), -1) for a, b in zip(c["master"], c["slave"])], np.int64)
+        return S
+
+    def _contact_eval(self, S, rel, vc, sprev, Kn, Ks, Diss, Mu):
+        """Force on A and new sliding spring of each contact as duals of the
+        seeded node offset `rel`, contact velocity `vc` (its dependence on the
+        contact point is added here), previous spring and parameters; also
+        the mask of contacts that carry a force."""
+        R = rotation(S.qB)
         lx = rel.x * R[:, 0, 0] + rel.y * R[:, 1, 0] + rel.z * R[:, 2, 0]
         ly = rel.x * R[:, 0, 1] + rel.y * R[:, 1, 1] + rel.z * R[:, 2, 1]
         lz = rel.x * R[:, 0, 2] + rel.y * R[:, 1, 2] + rel.z * R[:, 2, 2]
-        org, ih, sz, off = G.origin[geoB], G.inv_h[geoB], G.size[geoB], G.off[geoB]
+        G = S.G
+        org, ih, sz, off = G.origin[S.geoB], G.inv_h[S.geoB], G.size[S.geoB], G.off[S.geoB]
         gx, gy, gz = (lx - org[:, 0]) * ih, (ly - org[:, 1]) * ih, (lz - org[:, 2]) * ih
         i0 = np.floor(gx.v).astype(np.int64)
         j0 = np.floor(gy.v).astype(np.int64)
@@ -323,7 +413,7 @@ class TangentRun:
         phi = ((p[0] * ux + p[1] * fx) * uy + (p[2] * ux + p[3] * fx) * fy) * uz + \
               ((p[4] * ux + p[5] * fx) * uy + (p[6] * ux + p[7] * fx) * fy) * fz
         ov = -phi
-        dev = np.abs(ov.v - overlap) / np.maximum(np.abs(overlap), 1e-300)
+        dev = np.abs(ov.v - S.overlap) / np.maximum(np.abs(S.overlap), 1e-300)
         self.max_overlap_dev = max(self.max_overlap_dev, float(np.max(np.where(inside, dev, 0.0))))
         # gradient with the x weight truncated to the cell's x = 0 face
         ggx = (p[1] - p[0]) * (uy * uz) + (p[3] - p[2]) * (fy * uz) + (p[5] - p[4]) * (uy * fz) + \
@@ -340,64 +430,9 @@ class TangentRun:
         h = n.scale(0.5 * ov)
         hd = V3(deriv(h.x.d), deriv(h.y.d), deriv(h.z.d))
         reld = V3(deriv(rel.x.d), deriv(rel.y.d), deriv(rel.z.d))
-        vc_val = (vi + np.cross(wi, point - ri)) - (vj + np.cross(wj, point - rj))
-        vc = v3(vc_val, dvh[:, A, :] - (0.0 if wall else dvh[:, j, :]))
-        vc = vc + cross_const(wi, hd) - cross_const(wj, reld + hd)
-        # effective parameters and the directions their derivatives go to
-        mi = self.mat[A]
-        kni, ksi, mui, ei = self.kn[mi], self.ks[mi], self.mu[mi], self.e[mi]
-        im_i = self.inv_mass[A]
-        dkn, dks, ddiss, dmu = (np.zeros((nd, m)) for _ in range(4))
-        cols = np.arange(m)
-        if wall:
-            mw = self.wall_mat[j]
-            kn, ks = kni, ksi
-            mu = np.minimum(mui, self.wmu[mw])
-            res = np.minimum(ei, self.we[mw])
-            meff = np.where(im_i > 0, 1.0 / np.where(im_i > 0, im_i, 1.0), 0.0)
-            dkn[4 * mi, cols] = 1.0
-            dks[4 * mi + 1, cols] = 1.0
-            own_e, own_mu = ei <= self.we[mw], mui <= self.wmu[mw]
-            ddiss[4 * mi[own_e] + 2, cols[own_e]] = 1.0
-            dmu[4 * mi[own_mu] + 3, cols[own_mu]] = 1.0
-        else:
-            mj = self.mat[j]
-            knj, ksj = self.kn[mj], self.ks[mj]
-            okn, oks = (kni > 0) & (knj > 0), (ksi > 0) & (ksj > 0)
-            skn, sks = np.where(okn, kni + knj, 1.0), np.where(oks, ksi + ksj, 1.0)
-            kn = np.where(okn, kni * knj / skn, 0.0)
-            ks = np.where(oks, ksi * ksj / sks, 0.0)
-            np.add.at(dkn, (4 * mi, cols), np.where(okn, knj * knj / skn ** 2, 0.0))
-            np.add.at(dkn, (4 * mj, cols), np.where(okn, kni * kni / skn ** 2, 0.0))
-            np.add.at(dks, (4 * mi + 1, cols), np.where(oks, ksj * ksj / sks ** 2, 0.0))
-            np.add.at(dks, (4 * mj + 1, cols), np.where(oks, ksi * ksi / sks ** 2, 0.0))
-            im_j = self.inv_mass[j]
-            ssum = im_i + im_j
-            meff = np.where((im_i > 0) | (im_j > 0), 1.0 / np.where(ssum != 0, ssum, 1.0), 0.0)
-            res = np.minimum(ei, self.e[mj])
-            mu = np.minimum(mui, self.mu[mj])
-            ddiss[4 * np.where(ei <= self.e[mj], mi, mj) + 2, cols] = 1.0
-            dmu[4 * np.where(mui <= self.mu[mj], mi, mj) + 3, cols] = 1.0
-        Kn, Ks = Dual(np.asarray(kn, float), dkn), Dual(np.asarray(ks, float), dks)
-        Diss, Mu = Dual(_diss(res), ddiss), Dual(np.asarray(mu, float), dmu)
-        # the previous spring: first match of (node, partner) in the previous list
-        keys, spr_prev, dS_prev = self.lists[kind]
-        hist = np.array([keys.get((int(a), int(b)), -1) for a, b in zip(c["master"], c["slave"])], np.int64)
-        has = hist >= 0
-        hc = np.where(has, hist, 0)
-        sp_val = np.where(has[:, None], spr_prev[hc] if len(spr_prev) else 0.0, 0.0)
-        sp_der = np.where(has[None, :, None], dS_prev[:, hc, :] if dS_prev.shape[1] else 0.0, 0.0)
-        F, snew = self._law(v3(sp_val, sp_der), vc, n, ov, Kn, Ks, Diss, Mu, meff, float(self.sc.dt))
-        ok = inside & (ov.v > 0.0)
-        Fd = np.where(ok[None, :, None], F.derivs(), 0.0)
-        Sd = np.where(ok[None, :, None], snew.derivs(), 0.0)
-        Sv = np.where(ok[:, None], snew.value(), 0.0)
-        scale = max(float(np.abs(c["spring"]).max()), 1e-300)
-        self.max_spring_dev = max(self.max_spring_dev, float(np.abs(Sv - c["spring"]).max()) / scale)
-        np.add.at(dF, (slice(None), A), Fd)
-        if not wall:
-            np.add.at(dF, (slice(None), j[react]), -Fd[:, react])
-        return (self._keys(c), c["spring"], Sd)
+        vc = vc + cross_const(S.wi, hd) - cross_const(S.wj, reld + hd)
+        F, snew = self._law(sprev, vc, n, ov, Kn, Ks, Diss, Mu, S.meff, float(self.sc.dt))
+        return F, snew, inside & (ov.v > 0.0)
 
     @staticmethod
     def _law(sprev, vc, n, ov, kn, ks, diss, mu, m, dt):
