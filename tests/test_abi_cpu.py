@@ -58,3 +58,27 @@ def test_mass_properties_host_matches_oracle(fundem, oracle_mod):
     b = oracle_mod.mass_properties(2500.0, g.origin, g.spacing, g.size, g.sdf)
     assert a[0] == b[0]
     assert np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2])
+
+
+@pytest.mark.parametrize("lang", ["c", "c++"])
+def test_header_is_plain_c(tmp_path, lang):
+    """include/fundem_b200.h compiles on its own as C99 and as C++17: plain
+    types, extern "C" linkage, no library types in the signatures."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc" if lang == "c" else "g++")
+    if cc is None:
+        pytest.skip("no host compiler")
+    src = tmp_path / ("probe.c" if lang == "c" else "probe.cpp")
+    src.write_text('#include "fundem_b200.h"\nint probe(void) { return FUNDEM_OK + FUNDEM_INERTIA_PHYSICAL; }\n')
+    std = "-std=c99" if lang == "c" else "-std=c++17"
+    subprocess.check_call([cc, std, "-Wall", "-Werror", "-pedantic", "-fsyntax-only", "-I",
+                           os.path.join(ROOT, "include"), str(src)])
+
+
+def test_null_simulation_is_an_argument_error(fundem):
+    L = fundem.lib()
+    assert L.fundem_set_inertia_mode(None, 0) == 1
+    assert L.fundem_set_periodic_sector(None, 1) == 1
+    assert L.fundem_set_precision(None, 0) == 1
+    assert L.fundem_adjoint_begin(None, 10) == 1
