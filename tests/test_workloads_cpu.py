@@ -65,3 +65,17 @@ def test_calibration_sweep():
         (k, ks, m, e), = sc.particle_materials
         assert k == p["kn"] and ks == 0.8 * k and m == p["mu"]
         assert abs(_zeta(e) - p["damping_ratio"]) < 1e-12
+
+
+def test_bonded_column_parameters():
+    """The benchmark's bonded periodic column (built on the device, so only
+    its parameters are checked here): 262,144 particles from 8 templates,
+    dt = 5e-7 s, bond modulus 1e8 Pa, tensile strength 1e6 Pa, bonds where
+    the surface gap is below 0.05 of the mean diameter, a 1 m/s platen."""
+    import inspect
+    from fundem_b200 import workloads
+    d = {k: v.default for k, v in inspect.signature(workloads.bonded_column).parameters.items()}
+    assert d["n"] == 262144 and d["n_templates"] == 8 and d["dt"] == 5e-7
+    assert d["young"] == 1e8 and d["tensile"] == 1e6 and d["gap_frac"] == 0.05 and d["platen_speed"] == 1.0
+    a = {k: v.default for k, v in inspect.signature(workloads.adjoint_pour).parameters.items()}
+    assert a["n"] == 4096 and a["n_templates"] == 2 and a["dt"] == 1e-6
