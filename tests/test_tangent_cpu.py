@@ -190,3 +190,40 @@ def test_reverse_reference_adjoint_matches_tangent(oracle_mod, case):
     rr.close()
     got = np.concatenate([gp.ravel(), [float(np.sum(gv0 * d)) for d in dirs]])
     assert np.all(np.abs(got - ref) <= 1e-12 * np.abs(ref) + 1e-15 * np.abs(ref).max()), (got, ref)
+
+
+def test_autograd_wrapper_with_the_reference_adjoint(oracle_mod):
+    """The torch.autograd wrapper of the adjoint (tests/adjoint_autograd.py)
+    over the CPU reference adjoint: a loss that is nonlinear in the final
+    state (mean height plus the kinetic-energy-like sum of squared final
+    velocities) differentiated by loss.backward() gives the material and
+    initial-velocity gradients of the forward-mode derivative along the
+    same directions."""
+    import torch
+    from oracle import tangent
+    import adjoint_autograd as AG
+    sc = copy.deepcopy(PC.periodic())
+    for g in sc.particle_geometries:
+        g.inertia = np.zeros(6)
+    sc.wall_materials = [(0.9, 0.95)]
+    n, steps = len(sc.particles), 20
+    v0 = torch.tensor(sc.particles.vel, dtype=torch.float64, requires_grad=True)
+    params = torch.tensor(AG.material_parameters(sc), dtype=torch.float64, requires_grad=True)
+    x, v = AG.DEMRun.apply(v0, params, AG.OracleBackend(sc), steps)
+    loss = x[:, 2].mean() + 1e-2 * (v * v).sum()
+    loss.backward()
+    # the same derivative, direction by direction, with the loss gradient at
+    # the final state
+    rng = np.random.default_rng(9)
+    r = rng.standard_normal((n, 3))
+    tr = tangent.TangentRun(sc, [r])
+    tr.step(steps)
+    st = tr.o.state()
+    dl_dx = np.zeros((n, 3))
+    dl_dx[:, 2] = 1.0 / n
+    D = tr.directional(dl_dx, 2e-2 * st["vel"])
+    tr.close()
+    got = np.concatenate([params.grad.numpy().ravel(), [float(np.sum(v0.grad.numpy() * r))]])
+    # same run (the restitution coefficient passes through the damping ratio)
+    assert np.abs(st["pos"] - x.detach().numpy()).max() <= 1e-14 * np.abs(st["pos"]).max()
+    assert np.all(np.abs(got - D) <= 1e-10 * np.abs(D) + 1e-14 * np.abs(D).max()), (got, D)
