@@ -227,3 +227,16 @@ def test_autograd_wrapper_with_the_reference_adjoint(oracle_mod):
     # same run (the restitution coefficient passes through the damping ratio)
     assert np.abs(st["pos"] - x.detach().numpy()).max() <= 1e-14 * np.abs(st["pos"]).max()
     assert np.all(np.abs(got - D) <= 1e-10 * np.abs(D) + 1e-14 * np.abs(D).max()), (got, D)
+
+
+def test_reference_derivatives_refuse_what_they_do_not_differentiate():
+    """Rotating bodies and sector images are outside the frozen-topology
+    translation model both references (and the GPU adjoint) differentiate."""
+    from oracle import reverse, tangent
+    with pytest.raises(AssertionError):
+        tangent.TangentRun(PC.periodic())          # cm bodies: nonzero inverse inertia
+    sc = copy.deepcopy(PC.sector())
+    for g in sc.particle_geometries:
+        g.inertia = np.zeros(6)
+    with pytest.raises(AssertionError):
+        reverse.ReverseRun(sc)
