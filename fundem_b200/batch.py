@@ -10,6 +10,11 @@ on the batch itself.
 counts log-uniform in [500, 20000], per-simulation kn log-uniform in
 [5e3, 5e4], friction uniform in [0.2, 0.8] and damping ratio uniform in
 [0.1, 0.5], the small pour's shapes, in boxes sized for a fill ratio of 0.4.
+
+Over several GPUs (one process per GPU), `shard` splits the simulations
+whole, largest first, and `run_sharded` runs each rank's share and gathers
+the per-simulation results on every rank; the simulations exchange nothing
+while they run.
 """
 from __future__ import annotations
 
@@ -113,3 +118,49 @@ def autotune_chunk(batch, candidates=(25, 50, 100, 200), probe_steps=200):
         times[c] = time.perf_counter() - t0
     best = min(times, key=times.get)
     return best, times
+
+
+def shard(costs, world):
+    """Indices of the simulations each of `world` ranks runs: whole
+    simulations, the costliest first, each to the rank with the least work
+    so far (ties to the lowest rank).  Deterministic, so every rank computes
+    the same split."""
+    costs = np.asarray(costs, float)
+    order = sorted(range(len(costs)), key=lambda i: (-costs[i], i))
+    load = [0.0] * world
+    parts = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        parts[r].append(i)
+        load[r] += costs[i]
+    return [sorted(p) for p in parts]
+
+
+def run_sharded(scenarios, steps, chunk, rank, world, dist=None, device=0, summary=None, batch_cls=None):
+    """Run `steps` steps of this rank's share of `scenarios` (cost: particles
+    x steps) as one Batch in graph chunks of `chunk` steps, and return
+    {simulation index: summary(simulation)} for every simulation, gathered
+    from all ranks (torch.distributed all_gather_object when `dist` is given
+    and world > 1).  The default summary is the final mean particle height."""
+    batch_cls = Batch if batch_cls is None else batch_cls
+    if summary is None:
+        def summary(sim):
+            return float(sim.state()["pos"][:, 2].mean())
+    mine = shard([len(sc.particles) * steps for sc in scenarios], world)[rank]
+    local = {}
+    if mine:
+        b = batch_cls([scenarios[i] for i in mine], device=device)
+        try:
+            b.run_graphs(steps, chunk)
+            for i, sim in zip(mine, b.sims):
+                local[i] = summary(sim)
+        finally:
+            b.close()
+    if dist is None or world == 1:
+        return local
+    parts = [None] * world
+    dist.all_gather_object(parts, local)
+    out = {}
+    for p in parts:
+        out.update(p)
+    return out
