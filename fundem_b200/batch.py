@@ -73,10 +73,15 @@ class Batch:
         import torch
         self.streams = [torch.cuda.Stream(device=device) for _ in scenarios]
         self.sims = []
-        for sc, st in zip(scenarios, self.streams):
-            s = Simulation.from_scenario(sc, device=device, records=False, stream=st.cuda_stream)
-            s.detect()
-            self.sims.append(s)
+        try:
+            for sc, st in zip(scenarios, self.streams):
+                s = Simulation.from_scenario(sc, device=device, records=False, stream=st.cuda_stream)
+                self.sims.append(s)
+                s.detect()
+        except BaseException:
+            # release what was built before the failure
+            self.close()
+            raise
         self.particles = sum(s.num(False) for s in self.sims)
 
     def run_graphs(self, steps, chunk):
@@ -148,19 +153,29 @@ def run_sharded(scenarios, steps, chunk, rank, world, dist=None, device=0, summa
             return float(sim.state()["pos"][:, 2].mean())
     mine = shard([len(sc.particles) * steps for sc in scenarios], world)[rank]
     local = {}
-    if mine:
-        b = batch_cls([scenarios[i] for i in mine], device=device)
-        try:
-            b.run_graphs(steps, chunk)
-            for i, sim in zip(mine, b.sims):
-                local[i] = summary(sim)
-        finally:
-            b.close()
+    error = None
+    try:
+        if mine:
+            b = batch_cls([scenarios[i] for i in mine], device=device)
+            try:
+                b.run_graphs(steps, chunk)
+                for i, sim in zip(mine, b.sims):
+                    local[i] = summary(sim)
+            finally:
+                b.close()
+    except Exception as exc:
+        if dist is None or world == 1:
+            raise
+        # every rank still takes part in the gather, then all raise together
+        error = f"rank {rank}: {type(exc).__name__}: {exc}"
     if dist is None or world == 1:
         return local
     parts = [None] * world
-    dist.all_gather_object(parts, local)
+    dist.all_gather_object(parts, {"error": error, "results": local})
+    errors = [p["error"] for p in parts if p["error"]]
+    if errors:
+        raise RuntimeError("sharded run failed: " + "; ".join(errors))
     out = {}
     for p in parts:
-        out.update(p)
+        out.update(p["results"])
     return out

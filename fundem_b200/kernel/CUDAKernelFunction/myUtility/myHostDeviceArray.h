@@ -1,17 +1,23 @@
-// HostDeviceArray1D<T>, CUDA_CHECK and debug_dump_device_array with the names,
-// members and behaviour of the reference's kernel/CUDAKernelFunction/
-// myUtility/myHostDeviceArray.h, which LSParticle.h includes, so hooks and
-// apps that keep their own per-object arrays this way build unchanged.  The
-// library itself keeps its device state elsewhere; this is a container for
-// the caller.
+// Caller-side container of the LSSolver call surface: a host std::vector with
+// a device mirror, under the names an app written against the reference's
+// LSParticle.h can reach (HostDeviceArray1D<T>, CUDA_CHECK,
+// check_cuda_error, debug_dump_device_array).  The library keeps its own
+// device state elsewhere; this header serves apps and hooks that keep extra
+// per-object arrays.
 //
-// A host vector and a device copy: the device side is allocated
-// stream-ordered (cudaMallocAsync / cudaFreeAsync on the given stream, or
-// cudaFree for the synchronous release and on destruction), copies are
-// stream-ordered, and a host-to-device copy reallocates when the sizes
-// differ.  Not copyable; movable.
+// Design:
+//   * the device side is one block with a logical size and a capacity; a
+//     request that fits the capacity reuses the block, a larger one replaces
+//     it (stream-ordered cudaMallocAsync / cudaFreeAsync on the caller's
+//     stream), so repeated host-to-device copies of a list that shrinks and
+//     grows again do not churn the allocator;
+//   * every CUDA call goes through CUDA_CHECK, which throws std::runtime_error;
+//   * the destructor and moves release without checking (the runtime may be
+//     shutting down) and never throw.
+// Not copyable; movable.
 #pragma once
 #include <cstddef>
+#include <sstream>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -19,159 +25,174 @@
 
 #include <cuda_runtime.h>
 
+// Throws std::runtime_error naming the failed call, its source location and
+// the runtime's description of the error.
 inline void check_cuda_error(cudaError_t result, const char* func, const char* file, int line)
 {
     if (result == cudaSuccess) return;
-    throw std::runtime_error(std::string("CUDA Error at ") + file + ":" + std::to_string(line) + " / " + func + ": " +
-                             cudaGetErrorString(result));
+    std::ostringstream msg;
+    msg << func << " failed with " << cudaGetErrorName(result) << " (" << cudaGetErrorString(result) << "), "
+        << file << " line " << line;
+    throw std::runtime_error(msg.str());
 }
 
 #define CUDA_CHECK(val) check_cuda_error((val), #val, __FILE__, __LINE__)
 
 #ifndef NDEBUG
-#include <iomanip>
 #include <iostream>
-// Prints the first n values of a device array after the stream (or the whole
-// device, for stream 0) has finished.
+
+namespace hda_detail {
+template <typename T>
+inline void print_element(std::ostream& os, const T& v) { os << v; }
+inline void print_element(std::ostream& os, const double3& v) { os << v.x << ' ' << v.y << ' ' << v.z; }
+inline void print_element(std::ostream& os, const int3& v) { os << v.x << ' ' << v.y << ' ' << v.z; }
+}  // namespace hda_detail
+
+// Debug aid: waits for `stream` (the whole device for stream 0), copies the
+// first n elements of a device array back and prints one per line,
+// "name[i] value".  Compiled out with NDEBUG.
 template <typename T>
 void debug_dump_device_array(const T* d_ptr, std::size_t n, const char* name, cudaStream_t stream = 0)
 {
-    if (n == 0) return;
+    if (n == 0 || d_ptr == nullptr) return;
     CUDA_CHECK(stream == 0 ? cudaDeviceSynchronize() : cudaStreamSynchronize(stream));
     std::vector<T> h(n);
     CUDA_CHECK(cudaMemcpy(h.data(), d_ptr, n * sizeof(T), cudaMemcpyDeviceToHost));
-    std::cout << "[DEBUG] " << name << " (first " << n << " values):\n";
-    for (std::size_t i = 0; i < n; ++i) std::cout << "  [" << i << "] = " << h[i] << "\n";
-}
-
-template <>
-inline void debug_dump_device_array<double3>(const double3* d_ptr, std::size_t n, const char* name,
-                                            cudaStream_t stream)
-{
-    if (n == 0) return;
-    CUDA_CHECK(stream == 0 ? cudaDeviceSynchronize() : cudaStreamSynchronize(stream));
-    std::vector<double3> h(n);
-    cudaMemcpyAsync(h.data(), d_ptr, n * sizeof(double3), cudaMemcpyDeviceToHost, stream);
-    cudaStreamSynchronize(stream);
-    std::cout << name << ":\n";
-    std::ios saved(nullptr);
-    saved.copyfmt(std::cout);
-    std::cout << std::scientific << std::setprecision(3);
-    for (std::size_t i = 0; i < n; ++i)
-        std::cout << "  [" << i << "] = (" << h[i].x << ", " << h[i].y << ", " << h[i].z << ")\n";
-    std::cout.copyfmt(saved);
+    std::ostringstream out;
+    for (std::size_t i = 0; i < n; ++i) {
+        out << name << '[' << i << "] ";
+        hda_detail::print_element(out, h[i]);
+        out << '\n';
+    }
+    std::cout << out.str() << std::flush;
 }
 #endif
 
 template <typename T>
 struct HostDeviceArray1D
 {
-private:
-    std::vector<T> h_data;
-    size_t d_size{0};
-
 public:
-    T* d_ptr{nullptr};
+    T* d_ptr{nullptr};  // device block (null when nothing is allocated)
 
 private:
-    // for the destructor and moves: no error checks, the runtime may be
-    // shutting down
-    void dropDevice() noexcept
+    std::vector<T> host_;
+    std::size_t dev_count_{0};     // logical device size
+    std::size_t dev_capacity_{0};  // elements the block can hold
+
+    void forget() noexcept
+    {
+        d_ptr = nullptr;
+        dev_count_ = 0;
+        dev_capacity_ = 0;
+    }
+    void free_unchecked() noexcept
     {
         if (d_ptr) (void)cudaFree(d_ptr);
-        d_ptr = nullptr;
-        d_size = 0;
+        forget();
+    }
+    // device block of at least n elements, size n; contents undefined
+    void reserve_device(std::size_t n, cudaStream_t stream)
+    {
+        if (n > dev_capacity_ || d_ptr == nullptr) {
+            if (d_ptr) CUDA_CHECK(cudaFreeAsync(d_ptr, stream));
+            forget();
+            if (n > 0) CUDA_CHECK(cudaMallocAsync(reinterpret_cast<void**>(&d_ptr), n * sizeof(T), stream));
+            dev_capacity_ = n;
+        }
+        dev_count_ = n;
     }
 
 public:
     HostDeviceArray1D() = default;
-    ~HostDeviceArray1D() { dropDevice(); }
+    ~HostDeviceArray1D() { free_unchecked(); }
     HostDeviceArray1D(const HostDeviceArray1D&) = delete;
     HostDeviceArray1D& operator=(const HostDeviceArray1D&) = delete;
-    HostDeviceArray1D(HostDeviceArray1D&& other) noexcept { *this = std::move(other); }
+    HostDeviceArray1D(HostDeviceArray1D&& other) noexcept
+        : d_ptr(std::exchange(other.d_ptr, nullptr)),
+          host_(std::move(other.host_)),
+          dev_count_(std::exchange(other.dev_count_, 0)),
+          dev_capacity_(std::exchange(other.dev_capacity_, 0))
+    {
+        other.host_.clear();
+    }
     HostDeviceArray1D& operator=(HostDeviceArray1D&& other) noexcept
     {
-        if (this != &other) {
-            dropDevice();
-            h_data = std::move(other.h_data);
-            d_ptr = std::exchange(other.d_ptr, nullptr);
-            d_size = std::exchange(other.d_size, 0);
-        }
+        if (this == &other) return *this;
+        free_unchecked();
+        d_ptr = std::exchange(other.d_ptr, nullptr);
+        dev_count_ = std::exchange(other.dev_count_, 0);
+        dev_capacity_ = std::exchange(other.dev_capacity_, 0);
+        host_ = std::move(other.host_);
+        other.host_.clear();
         return *this;
     }
 
-    size_t hostSize() const { return h_data.size(); }
-    size_t deviceSize() const { return d_size; }
-    double deviceMemoryGB() const { return (double)d_size * sizeof(T) / (1024.0 * 1024.0 * 1024.0); }
+    // sizes
+    std::size_t hostSize() const { return host_.size(); }
+    std::size_t deviceSize() const { return dev_count_; }
+    double deviceMemoryGB() const { return double(dev_count_ * sizeof(T)) / double(1ull << 30); }
 
+    // device block
     void releaseDevice(cudaStream_t stream)
     {
-        if (d_ptr) cudaFreeAsync(d_ptr, stream);
-        d_ptr = nullptr;
-        d_size = 0;
+        T* p = d_ptr;
+        forget();
+        if (p) CUDA_CHECK(cudaFreeAsync(p, stream));
     }
-
     void releaseDeviceSync()
     {
-        if (d_ptr) cudaFree(d_ptr);
-        d_ptr = nullptr;
-        d_size = 0;
+        T* p = d_ptr;
+        forget();
+        if (p) CUDA_CHECK(cudaFree(p));
+    }
+    // n elements on the device, zeroed unless zeroFill is false (stream-ordered)
+    void allocateDevice(std::size_t n, cudaStream_t stream, bool zeroFill = true)
+    {
+        reserve_device(n, stream);
+        if (zeroFill && n > 0) CUDA_CHECK(cudaMemsetAsync(d_ptr, 0, n * sizeof(T), stream));
     }
 
-    // n elements on the device (any previous allocation released first),
-    // zeroed unless zeroFill is false
-    void allocateDevice(size_t n, cudaStream_t stream, bool zeroFill = true)
+    // host vector
+    void pushHost(const T& value) { host_.push_back(value); }
+    // inserts before index; an index at or past the end appends
+    void insertHost(std::size_t index, const T& value)
     {
-        if (d_ptr) releaseDevice(stream);
-        d_size = n;
-        if (n == 0) return;
-        cudaMallocAsync((void**)&d_ptr, n * sizeof(T), stream);
-        if (zeroFill) cudaMemsetAsync(d_ptr, 0, n * sizeof(T), stream);
+        host_.insert(host_.begin() + static_cast<std::ptrdiff_t>(index < host_.size() ? index : host_.size()), value);
     }
+    // an index past the end changes nothing
+    void eraseHost(std::size_t index)
+    {
+        if (index < host_.size()) host_.erase(host_.begin() + static_cast<std::ptrdiff_t>(index));
+    }
+    void clearHost() { host_.clear(); }
+    void reserveHost(std::size_t n) { host_.reserve(n); }
+    void resizeHost(std::size_t n) { host_.resize(n); }
+    const std::vector<T>& hostRef() const { return host_; }
+    void setHost(const std::vector<T>& values) { host_ = values; }
 
-    void pushHost(const T& value) { h_data.push_back(value); }
-    // inserts before index; at or past the end it appends
-    void insertHost(size_t index, const T& value)
-    {
-        if (index >= h_data.size()) h_data.push_back(value);
-        else h_data.insert(h_data.begin() + (std::ptrdiff_t)index, value);
-    }
-    // no-op past the end
-    void eraseHost(size_t index)
-    {
-        if (index < h_data.size()) h_data.erase(h_data.begin() + (std::ptrdiff_t)index);
-    }
-    void clearHost() { h_data.clear(); }
-    void reserveHost(size_t n) { h_data.reserve(n); }
-    void resizeHost(size_t n) { h_data.resize(n); }
-    const std::vector<T>& hostRef() const { return h_data; }
-    void setHost(const std::vector<T>& values) { h_data = values; }
-
-    // the host vector to the device, reallocating (not zeroed) when the
-    // sizes differ
+    // transfers (stream-ordered; the host side is complete once the stream
+    // reaches the copy)
+    // host vector -> device; the device size becomes the host size
     void copyHostToDevice(cudaStream_t stream)
     {
-        const size_t n = h_data.size();
-        if (n != d_size || d_ptr == nullptr) allocateDevice(n, stream, false);
-        if (n > 0) cudaMemcpyAsync(d_ptr, h_data.data(), n * sizeof(T), cudaMemcpyHostToDevice, stream);
+        reserve_device(host_.size(), stream);
+        if (!host_.empty())
+            CUDA_CHECK(cudaMemcpyAsync(d_ptr, host_.data(), host_.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
     }
-
-    // the device array to the host vector (resized to the device size);
-    // complete once the stream reaches it
+    // device -> host vector, resized to the device size
     void copyDeviceToHost(cudaStream_t stream)
     {
-        if (d_size == 0 || d_ptr == nullptr) return;
-        if (h_data.size() != d_size) h_data.resize(d_size);
-        cudaMemcpyAsync(h_data.data(), d_ptr, d_size * sizeof(T), cudaMemcpyDeviceToHost, stream);
+        if (d_ptr == nullptr || dev_count_ == 0) return;
+        host_.resize(dev_count_);
+        CUDA_CHECK(cudaMemcpyAsync(host_.data(), d_ptr, dev_count_ * sizeof(T), cudaMemcpyDeviceToHost, stream));
     }
-
-    // a synchronous device-to-host copy, returned by value
+    // synchronous device -> host copy; returns the refreshed host vector
     std::vector<T> getHostCopy()
     {
-        if (d_size > 0 && d_ptr) {
-            if (h_data.size() != d_size) h_data.resize(d_size);
-            cudaMemcpy(h_data.data(), d_ptr, d_size * sizeof(T), cudaMemcpyDeviceToHost);
+        if (d_ptr != nullptr && dev_count_ > 0) {
+            host_.resize(dev_count_);
+            CUDA_CHECK(cudaMemcpy(host_.data(), d_ptr, dev_count_ * sizeof(T), cudaMemcpyDeviceToHost));
         }
-        return h_data;
+        return host_;
     }
 };

@@ -1,126 +1,165 @@
-// OBJLoader:: -- reads the vertices and faces of a Wavefront OBJ file into the
-// arrays TriangleMeshParticle::setMesh takes, with the names and behaviour of
-// the reference's kernel/helper/OBJLoader.h: relative file names resolve
-// against the executable's directory, face tokens may carry /vt/vn parts,
-// negative indices count back from the last vertex, polygons become triangle
-// fans from their first corner, and a malformed file yields empty arrays and
-// false.
+// OBJLoader::loadOBJMesh -- reads the vertices and faces of a Wavefront OBJ
+// file into the arrays TriangleMeshParticle::setMesh takes.  The entry point
+// keeps the reference's name and argument list (kernel/helper/OBJLoader.h,
+// called as in apps/tutorial/LSParticleFalling.cpp:57); the parser is this
+// project's own.
+//
+// Accepted input:
+//   * "v x y z" lines (vertices) and "f a b c ..." lines (faces); every other
+//     line ("vn", "vt", "o", "g", "usemtl", comments after '#') is skipped;
+//   * a face corner is "i", "i/t", "i//n" or "i/t/n"; only i is used;
+//     i > 0 counts from the first vertex (1-based), i < 0 back from the last
+//     vertex read so far;
+//   * a polygon of k corners becomes the k - 2 triangles of a fan from its
+//     first corner.
+// A relative file name is taken from the running executable's directory
+// (argv[0]); an absolute one as it is.  On a malformed file the arrays are
+// left empty, a message naming the line goes to std::cerr, and the call
+// returns false.  With verbose, the counts go to std::cout.
 #pragma once
+#include <cerrno>
+#include <cstdlib>
 #include <filesystem>
 #include <fstream>
 #include <iostream>
-#include <sstream>
-#include <stdexcept>
 #include <string>
 #include <vector>
 
 #include <vector_functions.h>
 #include <vector_types.h>
 
-// directory of the running executable, from argv[0] (OBJLoader.h:22-33)
-inline std::filesystem::path getExecutableDirectory(const char* argv0)
-{
-    if (argv0 == nullptr) return std::filesystem::current_path();
-    std::filesystem::path exe(argv0);
-    if (exe.is_relative()) exe = std::filesystem::absolute(exe);
-    return std::filesystem::weakly_canonical(exe).parent_path();
-}
-
-// an absolute name is kept; a relative one is taken from the executable's directory
-inline std::string resolvePathFromExecutable(const std::string& filename, const char* argv0)
-{
-    const std::filesystem::path p(filename);
-    if (p.is_absolute()) return p.string();
-    return (getExecutableDirectory(argv0) / p).string();
-}
-
 namespace OBJLoader
 {
-
-inline std::string trim(const std::string& s)
+namespace detail
 {
-    const size_t a = s.find_first_not_of(" \t\r\n");
-    if (a == std::string::npos) return "";
-    const size_t b = s.find_last_not_of(" \t\r\n");
-    return s.substr(a, b - a + 1);
+
+// A read position within one line.
+struct Cursor {
+    const char* p;
+    const char* end;
+
+    static bool space(char c) { return c == ' ' || c == '\t' || c == '\r' || c == '\n' || c == '\v' || c == '\f'; }
+    void skip_space()
+    {
+        while (p < end && space(*p)) ++p;
+    }
+    bool at_end()
+    {
+        skip_space();
+        return p >= end || *p == '#';
+    }
+    // the next whitespace-delimited word
+    std::string word()
+    {
+        skip_space();
+        const char* a = p;
+        while (p < end && !space(*p)) ++p;
+        return std::string(a, p);
+    }
+    bool number(double& out)
+    {
+        const std::string w = word();
+        if (w.empty()) return false;
+        char* stop = nullptr;
+        errno = 0;
+        out = std::strtod(w.c_str(), &stop);
+        return stop == w.c_str() + w.size() && errno != ERANGE;
+    }
+};
+
+// the vertex part of a face corner, as a 0-based index; false when the
+// corner is malformed or names no vertex read so far
+inline bool corner_index(const std::string& corner, long long nvert, int& out)
+{
+    const std::string head = corner.substr(0, corner.find('/'));
+    if (head.empty()) return false;
+    char* stop = nullptr;
+    errno = 0;
+    const long long i = std::strtoll(head.c_str(), &stop, 10);
+    if (stop != head.c_str() + head.size() || errno == ERANGE || i == 0) return false;
+    const long long z = i > 0 ? i - 1 : nvert + i;
+    if (z < 0 || z >= nvert) return false;
+    out = static_cast<int>(z);
+    return true;
 }
 
-inline bool startsWith(const std::string& s, const std::string& prefix)
+inline std::filesystem::path locate(const std::string& filename, int argc, char** argv)
 {
-    return s.compare(0, prefix.size(), prefix) == 0;
+    const std::filesystem::path name(filename);
+    if (name.is_absolute()) return name;
+    std::filesystem::path base = std::filesystem::current_path();
+    if (argc > 0 && argv != nullptr && argv[0] != nullptr) {
+        std::error_code ec;
+        const std::filesystem::path exe = std::filesystem::weakly_canonical(std::filesystem::absolute(argv[0]), ec);
+        if (!ec) base = exe.parent_path();
+    }
+    return base / name;
 }
 
-// the vertex index of a face token "v", "v/vt", "v//vn" or "v/vt/vn"
-inline int parseOBJVertexIndex(const std::string& token)
+// parses the stream; on failure returns false with the line number and reason
+inline bool parse(std::istream& in, std::vector<double3>& vertices, std::vector<int3>& faces, std::size_t& line_no,
+                  std::string& why)
 {
-    if (token.empty()) throw std::runtime_error("Empty face token in OBJ.");
-    const std::string head = token.substr(0, token.find('/'));
-    if (head.empty()) throw std::runtime_error("Invalid OBJ face token: " + token);
-    return std::stoi(head);
+    std::string line;
+    std::vector<int> poly;
+    line_no = 0;
+    while (std::getline(in, line)) {
+        ++line_no;
+        Cursor c{line.data(), line.data() + line.size()};
+        if (c.at_end()) continue;
+        const std::string tag = c.word();
+        if (tag == "v") {
+            double x, y, z;
+            if (!c.number(x) || !c.number(y) || !c.number(z)) {
+                why = "vertex needs three numbers";
+                return false;
+            }
+            vertices.push_back(make_double3(x, y, z));
+        } else if (tag == "f") {
+            poly.clear();
+            while (!c.at_end()) {
+                int id = 0;
+                const std::string corner = c.word();
+                if (!corner_index(corner, static_cast<long long>(vertices.size()), id)) {
+                    why = "bad face corner '" + corner + "'";
+                    return false;
+                }
+                poly.push_back(id);
+            }
+            if (poly.size() < 3) {
+                why = "face with fewer than three corners";
+                return false;
+            }
+            for (std::size_t k = 2; k < poly.size(); ++k) faces.push_back(make_int3(poly[0], poly[k - 1], poly[k]));
+        }
+    }
+    return true;
 }
 
-// 1-based from the start, or negative from the end of the vertices read so far
-inline int convertOBJIndexToZeroBased(const int objIndex, const int numVertices)
-{
-    if (objIndex > 0) return objIndex - 1;
-    if (objIndex < 0) return numVertices + objIndex;
-    throw std::runtime_error("OBJ index cannot be zero.");
-}
+}  // namespace detail
 
 inline bool loadOBJMesh(const std::string& filename, std::vector<double3>& vertices, std::vector<int3>& faces,
                         const int argc, char** argv, const bool verbose = true)
 {
     vertices.clear();
     faces.clear();
-    const char* argv0 = (argc > 0 && argv != nullptr) ? argv[0] : nullptr;
-    const std::string path = resolvePathFromExecutable(filename, argv0);
+    const std::filesystem::path path = detail::locate(filename, argc, argv);
     std::ifstream in(path);
-    if (!in.is_open()) {
-        std::cerr << "[OBJLoader] Failed to open file: " << path << std::endl;
+    if (!in) {
+        std::cerr << "OBJLoader: cannot open " << path.string() << std::endl;
         return false;
     }
-    std::string line;
-    size_t lineNumber = 0;
-    try {
-        while (std::getline(in, line)) {
-            ++lineNumber;
-            line = trim(line);
-            if (line.empty() || line[0] == '#') continue;
-            if (startsWith(line, "v ")) {
-                std::istringstream ss(line.substr(2));
-                double x, y, z;
-                ss >> x >> y >> z;
-                if (ss.fail()) throw std::runtime_error("Failed to parse vertex at line " + std::to_string(lineNumber));
-                vertices.push_back(make_double3(x, y, z));
-            } else if (startsWith(line, "f ")) {
-                std::istringstream ss(line.substr(2));
-                std::vector<int> corner;
-                std::string token;
-                const int nv = (int)vertices.size();
-                while (ss >> token) {
-                    const int id = convertOBJIndexToZeroBased(parseOBJVertexIndex(token), nv);
-                    if (id < 0 || id >= nv)
-                        throw std::runtime_error("Face index out of range at line " + std::to_string(lineNumber));
-                    corner.push_back(id);
-                }
-                if (corner.size() < 3)
-                    throw std::runtime_error("Face has fewer than 3 vertices at line " + std::to_string(lineNumber));
-                for (size_t k = 1; k + 1 < corner.size(); ++k)
-                    faces.push_back(make_int3(corner[0], corner[k], corner[k + 1]));
-            }
-        }
-    } catch (const std::exception& e) {
-        std::cerr << "[OBJLoader] Error while reading " << path << " at line " << lineNumber << ": " << e.what()
-                  << std::endl;
+    std::size_t line_no = 0;
+    std::string why;
+    if (!detail::parse(in, vertices, faces, line_no, why)) {
+        std::cerr << "OBJLoader: " << path.string() << ":" << line_no << ": " << why << std::endl;
         vertices.clear();
         faces.clear();
         return false;
     }
-    if (verbose) {
-        std::cout << "[OBJLoader] Loaded OBJ: " << path << std::endl;
-        std::cout << "  Num vertices = " << vertices.size() << std::endl;
-        std::cout << "  Num faces    = " << faces.size() << std::endl;
-    }
+    if (verbose)
+        std::cout << "OBJLoader: " << path.string() << ": " << vertices.size() << " vertices, " << faces.size()
+                  << " triangles" << std::endl;
     return true;
 }
 

@@ -83,3 +83,44 @@ def test_run_sharded_two_ranks():
         assert sorted(res[r]) == list(range(40))
         assert all(res[r][i] == pytest.approx(want[i], rel=0, abs=1e-15) for i in range(40))
     assert res[0] == res[1]
+
+
+class _FailingBatch(_Batch):
+    """A stand-in whose construction fails on rank 1 (a simulation that
+    cannot be built there)."""
+
+    def __init__(self, scenarios, device=0):
+        import torch.distributed as dist
+        if dist.get_rank() == 1:
+            raise ValueError("no room for the batch")
+        super().__init__(scenarios, device)
+
+
+def _rank_failing(rank, world, port, out):
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    from fundem_b200 import batch
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=__import__("datetime").timedelta(seconds=60))
+    try:
+        scs, _ = batch.calibration_scenarios(n_sims=12, seed=3)
+        try:
+            batch.run_sharded(scs, 10, 5, rank, world, dist=dist, batch_cls=_FailingBatch)
+            out[rank] = "returned"
+        except RuntimeError as exc:
+            out[rank] = str(exc)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_run_sharded_failure_reaches_every_rank():
+    """A rank whose batch fails still joins the gather; every rank then raises
+    the same error instead of waiting for the process-group timeout."""
+    port = 29700 + os.getpid() % 1000
+    with mp.Manager() as m:
+        out = m.dict()
+        mp.spawn(_rank_failing, args=(2, port, out), nprocs=2, join=True)
+        res = dict(out)
+    for r in (0, 1):
+        assert "rank 1: ValueError: no room for the batch" in res[r]

@@ -7,10 +7,12 @@ import subprocess
 
 import pytest
 
+from oracle.refpath import reference_path
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 APPS = os.path.join(ROOT, "tests", "apps")
 CUDA_INC = "/usr/local/cuda/include"
-REF_APP = os.path.join("/root/reference", "apps", "test", "LSSphereBouncing.cpp")
+REF_APP = reference_path("apps", "test", "LSSphereBouncing.cpp")
 
 
 def _syntax(src, extra=()):
@@ -25,7 +27,7 @@ def test_own_app_compiles():
     _syntax(os.path.join(APPS, "sphere_drop.cpp"))
 
 
-@pytest.mark.skipif(not os.path.exists(REF_APP) or shutil.which("g++") is None,
+@pytest.mark.skipif(REF_APP is None or shutil.which("g++") is None,
                     reason="reference sources not present")
 def test_reference_app_compiles_unchanged():
     """The reference's own sphere-bouncing app, as it lies in the reference

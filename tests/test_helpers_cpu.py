@@ -12,13 +12,15 @@ import subprocess
 import numpy as np
 import pytest
 
+from oracle.refpath import reference_path, reference_root
+
 from golden import make_helper_fixtures as MF
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 APPS = os.path.join(ROOT, "tests", "apps")
 CUDA_INC = "/usr/local/cuda/include"
-REF_ROOT = "/root/reference"
-REF_TUTORIAL = os.path.join(REF_ROOT, "apps", "tutorial")
+REF_ROOT = reference_root()
+REF_TUTORIAL = reference_path("apps", "tutorial")
 
 needs_gxx = pytest.mark.skipif(shutil.which("g++") is None, reason="no host compiler")
 
@@ -103,7 +105,7 @@ def test_grid_layout_matches(golden, fundem):
         assert golden[name + "/spacing"][0] == h
 
 
-@pytest.mark.skipif(not os.path.exists(os.path.join(REF_ROOT, "kernel", "helper")), reason="reference sources absent")
+@pytest.mark.skipif(REF_ROOT is None, reason="reference sources absent")
 @needs_gxx
 def test_fixtures_reproduce_from_reference(tmp_path, golden):
     """The committed fixtures are what the reference's helpers produce now."""
@@ -151,7 +153,7 @@ int main(int argc, char** argv) {
         assert line.split()[1:] == ["0", "0", "0"], line
 
 
-@pytest.mark.skipif(not os.path.isdir(REF_TUTORIAL) or shutil.which("g++") is None,
+@pytest.mark.skipif(REF_TUTORIAL is None or shutil.which("g++") is None,
                     reason="reference sources not present")
 @pytest.mark.parametrize("app", ["LSParticleFalling.cpp", "LSParticleRolling.cpp"])
 def test_reference_tutorials_compile_unchanged(app):

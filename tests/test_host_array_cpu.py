@@ -9,8 +9,10 @@ import subprocess
 
 import pytest
 
+from oracle.refpath import reference_path
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF_KERNEL = os.path.join("/root/reference", "kernel")
+REF_KERNEL = reference_path("kernel")
 SRC = os.path.join(ROOT, "tests", "apps", "host_array_check.cpp")
 CUDA = "/usr/local/cuda"
 
@@ -30,5 +32,5 @@ def test_host_side(tmp_path):
     ours = _run(tmp_path, os.path.join(ROOT, "fundem_b200", "kernel"), "ours")
     assert "insert host 7 device 0 gb 0.000: 0 1.5 -1 3 4.5 6 9 ptr 0\n" in ours
     assert "moved-from host 0 " in ours and "moved-to host 3 " in ours
-    if os.path.isdir(REF_KERNEL):
+    if REF_KERNEL and os.path.isdir(REF_KERNEL):
         assert ours == _run(tmp_path, REF_KERNEL, "ref")
