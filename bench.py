@@ -29,6 +29,7 @@ steps / the slowest rank's time.
 from __future__ import annotations
 
 import argparse
+import faulthandler
 import json
 import os
 import subprocess
@@ -54,51 +55,119 @@ def log(*a):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clock, power and clock-event reasons sampled during the timed
+    region: NVML in a thread every 5 ms (the region can be a few tens of
+    milliseconds), or nvidia-smi every 200 ms where NVML is missing."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
+               0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown"}
 
-    def __init__(self, index):
+    def __init__(self, index, period_s=0.005):
         self.index = index
-        self.samples = []
+        self.period = period_s
+        self.samples = []   # (sm_mhz, max_mhz, power_w, reason bits)
         self.proc = None
+        self.nvml = None
+        self._stop = threading.Event()
+
+    def _nvml_handle(self):
+        """The NVML handle of CUDA device `index`, matched by UUID (NVML and
+        CUDA may number devices differently), else by index."""
+        import pynvml
+        pynvml.nvmlInit()
+        want = None
+        try:
+            import torch
+            want = str(torch.cuda.get_device_properties(self.index).uuid).lower()
+        except Exception:
+            pass
+        if want:
+            for i in range(pynvml.nvmlDeviceGetCount()):
+                h = pynvml.nvmlDeviceGetHandleByIndex(i)
+                u = pynvml.nvmlDeviceGetUUID(h)
+                u = (u.decode() if isinstance(u, bytes) else str(u)).lower()
+                if u.endswith(want):
+                    return pynvml, h
+        return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
 
     def start(self):
+        try:
+            self.nvml, h = self._nvml_handle()
+            self.thread = threading.Thread(target=self._poll_nvml, args=(h,), daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread = threading.Thread(target=self._read_smi, daemon=True)
             self.thread.start()
         except Exception:
             self.proc = None
 
-    def _read(self):
+    def _poll_nvml(self, h):
+        N = self.nvml
+        mx = N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM)
+        get_reasons = getattr(N, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            N.nvmlDeviceGetCurrentClocksThrottleReasons
+        while not self._stop.is_set():
+            try:
+                self.samples.append((float(N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)), float(mx),
+                                     N.nvmlDeviceGetPowerUsage(h) / 1e3, int(get_reasons(h))))
+            except Exception:
+                pass
+            time.sleep(self.period)
+
+    def _read_smi(self):
+        names = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20, "sw_power_cap": 0x4}
         for line in self.proc.stdout:
-            self.samples.append([x.strip() for x in line.split(",")])
+            s = [x.strip() for x in line.split(",")]
+            if len(s) < 9 or not s[1].replace(".", "").isdigit():
+                continue
+            bits = 0
+            for k, nm in enumerate(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")):
+                if "Active" in s[5 + k] and "Not" not in s[5 + k]:
+                    bits |= names[nm]
+            pw = float(s[3]) if s[3].replace(".", "").isdigit() else float("nan")
+            self.samples.append((float(s[1]), float(s[2]), pw, bits))
 
     def stop(self):
-        if not self.proc:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        sm = [float(s[1]) for s in self.samples if len(s) >= 9 and s[1].replace(".", "").isdigit()]
-        mx = [float(s[2]) for s in self.samples if len(s) >= 9 and s[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        self._stop.set()
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if getattr(self, "thread", None):
+            self.thread.join(timeout=5)
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0,
+                    "source": "nvml" if self.nvml else ("nvidia-smi" if self.proc else "unavailable")}
+        sm = [x[0] for x in self.samples]
         reasons = set()
-        for s in self.samples:
-            if len(s) < 9:
-                continue
-            for k, nm in enumerate(names):
-                if "Active" in s[5 + k] and "Not" not in s[5 + k]:
+        for x in self.samples:
+            for bit, nm in self.REASONS.items():
+                if x[3] & bit:
                     reasons.add(nm)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.samples)}
+        return {"sm_mhz": float(np.median(sm)), "sm_min_mhz": float(min(sm)), "sm_max_mhz": max(x[1] for x in self.samples),
+                "power_w_max": float(np.nanmax([x[2] for x in self.samples])), "reasons": sorted(reasons),
+                "samples": len(self.samples), "source": "nvml" if self.nvml else "nvidia-smi"}
+
+
+def pinned_like(a):
+    """A copy of a numpy array in page-locked host memory."""
+    import torch
+    t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+    out = t.numpy()  # shares the tensor's memory and keeps the tensor alive
+    out[...] = a
+    return out
 
 
 def peaks():
@@ -163,52 +232,66 @@ def run_fundem(args, rank, world, dist):
 
     build.build()
     dev = int(os.environ.get("LOCAL_RANK", 0))
+
+    def log0(*a):
+        if rank == 0:
+            log(*a)
     torch.cuda.set_device(dev)
     t_build = time.perf_counter()
     sim, sc, info = workloads.bonded_column(n=args.n, footprint=tuple(args.footprint), seed=1 + rank, device=dev,
-                                            log=log if rank == 0 else None)
+                                            settle_steps=args.settle_steps, log=log if rank == 0 else None)
     t_build = time.perf_counter() - t_build
     n = info["n"]
     g = np.asarray(sc.gravity, float)
     dt = sc.dt
+    log0(f"workload built in {t_build:.1f} s; {args.warmup} warm-up steps")
     sim.step(args.warmup)
     sim.sync()
     pairs = sim.num_pairs(0)
     contacts = sim.num_contacts(0) + sim.num_contacts(1) + sum(sim.num_contacts(k) for k in (2, 3, 4))
     nbonds = int(sim.bonds()["activated"].sum())
-    sim.set_profiling(True)
-    sim.kernel_times()
     l0 = sim.launch_count()
     clocks = ClockSampler(dev)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     clocks.start()
+    time.sleep(0.02)  # the sampler's first reading precedes the region
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if args.profile:
         torch.cuda.profiler.start()
+    # the headline: K plain steps, no kernel timers
     e0.record()
     sim.step(args.steps)
     e1.record()
     torch.cuda.synchronize()
     if args.profile:
         torch.cuda.profiler.stop()
+    clk = clocks.stop()
     sim.sync()
     if dist:
         dist.barrier()
     ms = e0.elapsed_time(e1)
-    clk = clocks.stop()
     launches = sim.launch_count() - l0
-    kt = sim.kernel_times()
-    sim.set_profiling(False)
     contacts_end = sim.num_contacts(0) + sim.num_contacts(1) + sum(sim.num_contacts(k) for k in (2, 3, 4))
     t_max, value = aggregate(ms, n, args.steps, world, dist, "cuda")
+    log0(f"timed: {ms / args.steps:.4f} ms/step, clocks {clk}")
+    # the same K steps again with the kernel-group timers on (CUDA events on
+    # the simulation's stream around each group): per-kernel times and the
+    # roofline's launch duration
+    sim.set_profiling(True)
+    sim.kernel_times()
+    sim.step(args.steps)
+    sim.sync()
+    kt = sim.kernel_times()
+    sim.set_profiling(False)
 
-    # end to end through the C ABI with host buffers: upload the state from
-    # host memory, run the steps reading back the status word every step,
+    # end to end through the C ABI with host buffers in pinned memory: upload
+    # the state, run the steps reading back the status word every step,
     # download the state
     st = sim.state()
-    host = {k: np.ascontiguousarray(v) for k, v in st.items()}
+    host = {k: pinned_like(v) for k, v in st.items()}
+    back = {k: pinned_like(v) for k, v in st.items()}
     state_bytes = sum(v.nbytes for v in host.values())
     e2e_steps = 0 if args.no_e2e else args.steps
     if e2e_steps:
@@ -222,9 +305,10 @@ def run_fundem(args, rank, world, dist):
     for _ in range(e2e_steps):
         sim.step_graph(1)
         sim.status_word()
-    out = sim.state()
+    sim.state(out=back)
     sim.sync()
     t_e2e = time.perf_counter() - t0
+    log0(f"end to end: {t_e2e:.4f} s")
     # narrow-phase work counters, on a few extra steps outside the timed regions
     wc_steps = 10
     sim.set_profiling(False, counters=True)
@@ -270,6 +354,12 @@ def run_fundem(args, rank, world, dist):
         except Exception as exc:  # an auxiliary figure: report, do not fail the run
             adjoint = {"error": f"{type(exc).__name__}: {exc}"}
 
+    ref_gpu = None
+    if rank == 0 and world == 1 and not args.no_reference_gpu:
+        try:
+            ref_gpu = reference_gpu_time(sc, args)
+        except Exception as exc:  # an auxiliary figure: report, do not fail the run
+            ref_gpu = {"error": f"{type(exc).__name__}: {exc}"}
     if rank != 0:
         return
     pk, pk_kind = peaks()
@@ -293,7 +383,15 @@ def run_fundem(args, rank, world, dist):
                    "bonds": info["bonds"], "periodic": "xy", "precision": "fp64",
                    "footprint": info["footprint"], "layers": info["layers"],
                    "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}",
-                   "pairs": pairs, "node_contacts": contacts, "setup_s": round(t_build, 1)},
+                   "pairs": pairs, "node_contacts": contacts, "node_contacts_end": contacts_end,
+                   "active_bonds": nbonds, "setup_s": round(t_build, 1),
+                   "settle": {"steps": info["settle_steps"], "dt": info["settle_dt"],
+                              "peak_speed_m_s": info["settle_peak_speed"], "settled": info["settled"],
+                              "kinetic_energy_j": info["settle_kinetic_energy"],
+                              "kinetic_energy_peak_j": info["settle_kinetic_energy_peak"],
+                              "coordination": info["coordination"],
+                              "node_contacts": info["settled_node_contacts"]},
+                   "timed_from": "the settled, bonded bed with the platen released (workloads.bonded_column)"},
         "e2e": {"value": e2e_val, "unit": METRIC, "h2d_bytes_per_step": state_bytes / args.steps,
                 "d2h_bytes_per_step": 4 + state_bytes / args.steps,
                 "note": "state uploaded from host arrays, each step a one-step CUDA-graph replay "
@@ -309,6 +407,9 @@ def run_fundem(args, rank, world, dist):
                      "step_achieved_gbs": step_bytes / (t_max / args.steps / 1e3) / 1e9},
         "contact_updates_per_s": world * 0.5 * (contacts + contacts_end) * args.steps / (t_max / 1e3),
         "kernel_ms_per_step": {k: v[0] / max(args.steps, 1) for k, v in kt.items()},
+        "kernel_timing": "a second pass of K steps right after the headline, with CUDA-event timers on the "
+                         "simulation's stream around each kernel group",
+        "reference_gpu": ref_gpu,
         "narrow_work_per_step": {"pairs": wc[0] / wc_steps, "clusters": wc[1] / wc_steps,
                                  "clusters_kept": wc[2] / wc_steps, "node_contacts": wc[3] / wc_steps,
                                  "exact_node_tests": wc[4] / wc_steps},
@@ -339,6 +440,43 @@ def profiled_traffic_per_pair():
     except OSError:
         pass
     return None
+
+
+def reference_gpu_time(sc, args):
+    """The reference's own CUDA build (oracle/_ref/ref_driver: its LSSolver and
+    kernels compiled from its sources, no change) on the same settled state,
+    same B200: wall time between the solver hooks of two steps, after a
+    device synchronisation at each end, with no output frame between them
+    (the reference writes frames at the start and end of a solve).  The
+    reference starts without the tangential-spring history of the settle."""
+    import shutil
+    import tempfile
+    from oracle import scenario_io
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+    if not os.path.exists(exe):
+        return {"unavailable": "oracle/_ref/ref_driver not built (needs the reference sources)"}
+    steps_ref, lo = args.reference_gpu_steps, 10
+    out = tempfile.mkdtemp(prefix="fundem_ref_")
+    try:
+        path = os.path.join(out, "scenario.bin")
+        scenario_io.write_reference_scenario(sc, path, steps_ref)
+        t0 = time.time()
+        r = subprocess.run([exe, path, out, "timing", str(lo), str(steps_ref - 5), "exit"], capture_output=True,
+                           text=True, timeout=args.reference_gpu_timeout)
+        wall = time.time() - t0
+        if r.returncode != 0:
+            return {"error": f"ref_driver exit {r.returncode}: {r.stderr[-300:]}"}
+        meta = {}
+        with open(os.path.join(out, "meta.txt")) as f:
+            for line in f:
+                k, v = line.split(None, 1)
+                meta[k] = v.strip()
+    finally:
+        shutil.rmtree(out, ignore_errors=True)
+    ms = 1e3 * float(meta["window_seconds"]) / float(meta["window_steps"])
+    n = len(sc.particles)
+    return {"ms_per_step": ms, "value": n / (ms / 1e3), "unit": METRIC, "window_steps": [lo, steps_ref - 5],
+            "wall_s": round(wall, 1), "what": "the reference's CUDA build, same scenario and state, same GPU"}
 
 
 def aggregate(ms, n, steps, world, dist, device):
@@ -511,6 +649,7 @@ def batched_cost(args, dev):
 
 
 def main():
+    faulthandler.enable()
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
@@ -528,6 +667,11 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint cost measurement")
     ap.add_argument("--adjoint-steps", type=int, default=2000)
     ap.add_argument("--no-batch", action="store_true", help="skip the batched calibration measurement")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's own CUDA build on the same state")
+    ap.add_argument("--reference-gpu-steps", type=int, default=30)
+    ap.add_argument("--reference-gpu-timeout", type=float, default=400.0)
+    ap.add_argument("--settle-steps", type=int, default=24000, help="most settling steps of the workload")
     ap.add_argument("--batch-sims", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=200)
     ap.add_argument("--error-steps", type=int, default=1000,

@@ -431,12 +431,22 @@ class Simulation:
         self._check(self.L.fundem_num_objects(self.h, int(wall), C.byref(n)), "num_objects")
         return n.value
 
-    def state(self, wall=False):
+    def state(self, wall=False, out=None):
+        """Object state as host arrays; `out` may supply the six arrays
+        (C-contiguous float64, (n, 3) and (n, 4) for quat), for example in
+        page-locked memory, and is filled in place."""
         n = self.num(wall)
-        out = {k: np.zeros((n, 3)) for k in ("pos", "vel", "angvel", "force", "torque")}
-        out["quat"] = np.zeros((n, 4))
-        self._check(self.L.fundem_get_objects(self.h, int(wall), _d(out["pos"]), _d(out["vel"]), _d(out["angvel"]),
-                                         _d(out["quat"]), _d(out["force"]), _d(out["torque"])), "get_objects")
+        if out is None:
+            out = {k: np.zeros((n, 3)) for k in ("pos", "vel", "angvel", "force", "torque")}
+            out["quat"] = np.zeros((n, 4))
+        else:
+            for k, v in out.items():
+                if not (v.dtype == np.float64 and v.flags.c_contiguous and v.shape == (n, 4 if k == "quat" else 3)):
+                    raise ValueError(f"state(out=...): {k} must be a C-contiguous float64 array of shape "
+                                     f"({n}, {4 if k == 'quat' else 3})")
+        self._check(self.L.fundem_get_objects(self.h, int(wall), _d(out.get("pos")), _d(out.get("vel")),
+                                              _d(out.get("angvel")), _d(out.get("quat")), _d(out.get("force")),
+                                              _d(out.get("torque"))), "get_objects")
         return out
 
     def set_state(self, wall=False, pos=None, vel=None, angvel=None, quat=None, force=None, torque=None):

@@ -1558,14 +1558,31 @@ __global__ void __launch_bounds__(TPB, FD_CONTACT_MIN_BLOCKS) k_contact32(Narrow
                         fy = (float)(gy - (double)j0);
                         fz = (float)(gz - (double)k0);
                         const long long sx = GB.size.x, sxy = (long long)GB.size.x * GB.size.y;
-                        const float* S = SB.sdf32 + GB.sdf_off + (long long)k0 * sxy + (long long)j0 * sx + i0;
-                        pv[0] = __ldg(S); pv[1] = __ldg(S + 1); pv[2] = __ldg(S + sx); pv[3] = __ldg(S + sx + 1);
-                        pv[4] = __ldg(S + sxy); pv[5] = __ldg(S + sxy + 1); pv[6] = __ldg(S + sxy + sx);
-                        pv[7] = __ldg(S + sxy + sx + 1);
-                        const float c00 = pv[0] * (1.f - fx) + pv[1] * fx, c10 = pv[2] * (1.f - fx) + pv[3] * fx;
-                        const float c01 = pv[4] * (1.f - fx) + pv[5] * fx, c11 = pv[6] * (1.f - fx) + pv[7] * fx;
-                        ov = -((c00 * (1.f - fy) + c10 * fy) * (1.f - fz) + (c01 * (1.f - fy) + c11 * fy) * fz);
-                        hit = ov >= -(float)n.a.probe;
+                        const long long c0 = GB.sdf_off + (long long)k0 * sxy + (long long)j0 * sx + i0;
+                        if (KIND == FD_PW) {
+                            // wall grids are coarse (a plane wall is one cell
+                            // the size of the domain, corner values of tenths
+                            // of a metre): single-precision interpolation
+                            // there would carry errors of 1e-8 m, so the
+                            // (few) wall contacts interpolate in double
+                            const double* S = SB.sdf + c0;
+                            double pd[8] = {__ldg(S), __ldg(S + 1), __ldg(S + sx), __ldg(S + sx + 1), __ldg(S + sxy),
+                                            __ldg(S + sxy + 1), __ldg(S + sxy + sx), __ldg(S + sxy + sx + 1)};
+                            const double ovd = -xm_trilinear(gx - (double)i0, gy - (double)j0, gz - (double)k0, pd);
+#pragma unroll
+                            for (int c = 0; c < 8; ++c) pv[c] = (float)pd[c];
+                            ov = (float)ovd;
+                            hit = ovd >= -n.a.probe;
+                        } else {
+                            const float* S = SB.sdf32 + c0;
+                            pv[0] = __ldg(S); pv[1] = __ldg(S + 1); pv[2] = __ldg(S + sx); pv[3] = __ldg(S + sx + 1);
+                            pv[4] = __ldg(S + sxy); pv[5] = __ldg(S + sxy + 1); pv[6] = __ldg(S + sxy + sx);
+                            pv[7] = __ldg(S + sxy + sx + 1);
+                            const float c00 = pv[0] * (1.f - fx) + pv[1] * fx, c10 = pv[2] * (1.f - fx) + pv[3] * fx;
+                            const float c01 = pv[4] * (1.f - fx) + pv[5] * fx, c11 = pv[6] * (1.f - fx) + pv[7] * fx;
+                            ov = -((c00 * (1.f - fy) + c10 * fy) * (1.f - fz) + (c01 * (1.f - fy) + c11 * fy) * fz);
+                            hit = ov >= -(float)n.a.probe;
+                        }
                     }
                 }
             }

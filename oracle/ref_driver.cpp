@@ -98,6 +98,7 @@ public:
     std::set<int64_t> dumpSteps;
     int64_t step = 0;
     bool timingOnly = false;
+    bool exitAfterWindow = false;  // timing mode: stop once the window is measured
     // timing window: wall time between the hooks of steps windowFrom and
     // windowTo, after a device synchronisation at each end.  No output frame
     // falls inside when windowTo is below the last step.
@@ -112,6 +113,21 @@ public:
             if (step == windowFrom || step == windowTo) {
                 cudaDeviceSynchronize();
                 (step == windowFrom ? tFrom : tTo) = std::chrono::steady_clock::now();
+            }
+            if (exitAfterWindow && step == windowTo && windowTo > windowFrom) {
+                // the window is all a timing run needs: report it and leave
+                // before the remaining steps and the closing frame output
+                const double w = std::chrono::duration<double>(tTo - tFrom).count();
+                const cudaError_t err = cudaGetLastError();
+                std::ofstream meta(out_ + "/meta.txt");
+                meta << "steps " << step << "\n";
+                meta << "cuda_status " << cudaGetErrorString(err) << "\n";
+                meta << "window_steps " << (windowTo - windowFrom) << "\n";
+                meta << "window_seconds " << w << "\n";
+                meta.close();
+                std::cout << "ref_driver: window " << windowFrom << ".." << windowTo << ": "
+                          << 1e3 * w / double(windowTo - windowFrom) << " ms/step" << std::endl;
+                std::_Exit(err == cudaSuccess ? 0 : 1);
             }
             return;
         }
@@ -193,7 +209,7 @@ public:
 int main(int argc, char** argv)
 {
     if (argc < 3) {
-        std::cerr << "usage: ref_driver scenario.bin outdir [timing [from to]]\n";
+        std::cerr << "usage: ref_driver scenario.bin outdir [timing [from to [exit]]]\n";
         return 2;
     }
     const std::string scen = argv[1], out = argv[2];
@@ -212,6 +228,7 @@ int main(int argc, char** argv)
     if (timing && argc > 5) {
         s.windowFrom = std::atoll(argv[4]);
         s.windowTo = std::atoll(argv[5]);
+        s.exitAfterWindow = argc > 6 && std::string(argv[6]) == "exit";
     }
     const int32_t nDump = r.get<int32_t>();
     for (int i = 0; i < nDump; ++i) s.dumpSteps.insert(r.get<int32_t>());

@@ -29,7 +29,7 @@ T, K = 50, 16
 @pytest.fixture(scope="module", params=[11, 12, 13, 14])
 def setup(fundem, request):
     from fundem_b200 import workloads
-    sim, sc, info = workloads.bonded_column(n=512, footprint=(8, 8), seed=request.param)
+    sim, sc, info = workloads.bonded_column(n=512, footprint=(8, 8), seed=request.param, settle_steps=0)
     sim.close()
     # walls with more friction and restitution than the particles: the
     # particle-wall contacts then take mu = min(...) and e = min(...) from the
@@ -132,7 +132,7 @@ def test_checkpoint_interval_autotuner(fundem):
     since each segment's re-run repeats the forward run (they agree to
     rounding: the reverse sweep adds to particles with atomics)."""
     from fundem_b200 import autotune, workloads
-    sim, sc, info = workloads.bonded_column(n=512, footprint=(8, 8), seed=11)
+    sim, sc, info = workloads.bonded_column(n=512, footprint=(8, 8), seed=11, settle_steps=0)
     sim.close()
     rng = np.random.default_rng(5)
     w = rng.standard_normal((512, 3))
@@ -174,7 +174,7 @@ def _turning_column():
     particles spin at about 20 rad/s (zero inverse inertia keeps it) and the
     floor turns about z at 5 rad/s."""
     from fundem_b200 import workloads
-    sim, sc, info = workloads.bonded_column(n=512, footprint=(8, 8), seed=12)
+    sim, sc, info = workloads.bonded_column(n=512, footprint=(8, 8), seed=12, settle_steps=0)
     sim.close()
     sc.wall_materials = [(0.7, 0.9)]
     rng = np.random.default_rng(12)
@@ -236,7 +236,7 @@ def test_mixed_precision_adjoint(fundem, oracle_mod):
     forward and backward differences of kn differ by 13% there)."""
     from oracle import tangent
     from fundem_b200 import workloads
-    sim, sc, info = workloads.bonded_column(n=512, footprint=(8, 8), seed=11)
+    sim, sc, info = workloads.bonded_column(n=512, footprint=(8, 8), seed=11, settle_steps=0)
     sim.close()
     sc.wall_materials = [(0.7, 0.9)]
     n = len(sc.particles)

@@ -24,7 +24,7 @@ def test_graph_chunks_match_sequential(fundem):
 
 def test_step_graph_matches_step(fundem):
     from fundem_b200 import workloads
-    sim, sc, info = workloads.bonded_column(n=2048, footprint=(16, 16), seed=2)
+    sim, sc, info = workloads.bonded_column(n=2048, footprint=(16, 16), seed=2, settle_steps=0)
     sim.close()
     import torch
     st = torch.cuda.Stream()
@@ -46,7 +46,7 @@ def test_step_graph_odd_lengths_and_mixed_calls(fundem, chunks):
     on, and plain steps may come between replays: every sequence equals the
     same number of plain steps bit for bit."""
     from fundem_b200 import workloads
-    sim, sc, info = workloads.bonded_column(n=2048, footprint=(16, 16), seed=2)
+    sim, sc, info = workloads.bonded_column(n=2048, footprint=(16, 16), seed=2, settle_steps=0)
     sim.close()
     g = fundem.Simulation.from_scenario(sc, records=False)
     p = fundem.Simulation.from_scenario(sc, records=False)

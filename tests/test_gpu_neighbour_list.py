@@ -13,7 +13,7 @@ pytestmark = pytest.mark.gpu
 
 def test_neighbour_list_matches_cell_search(fundem):
     from fundem_b200 import workloads
-    sim, sc, info = workloads.bonded_column(n=4096, footprint=(32, 16), seed=4)
+    sim, sc, info = workloads.bonded_column(n=4096, footprint=(32, 16), seed=4, settle_steps=0)
     sim.close()
     runs = {}
     for mode in (0, 1):
