@@ -245,8 +245,10 @@ def run_fundem(args, rank, world, dist):
     g = np.asarray(sc.gravity, float)
     dt = sc.dt
     log0(f"workload built in {t_build:.1f} s; {args.warmup} warm-up steps")
+    sim.set_pair_cache(args.pair_cache, args.pair_skin)
     sim.step(args.warmup)
     sim.sync()
+    pc0 = sim.pair_cache_stats()
     pairs = sim.num_pairs(0)
     contacts = sim.num_contacts(0) + sim.num_contacts(1) + sum(sim.num_contacts(k) for k in (2, 3, 4))
     nbonds = int(sim.bonds()["activated"].sum())
@@ -273,6 +275,7 @@ def run_fundem(args, rank, world, dist):
         dist.barrier()
     ms = e0.elapsed_time(e1)
     launches = sim.launch_count() - l0
+    pc1 = sim.pair_cache_stats()
     contacts_end = sim.num_contacts(0) + sim.num_contacts(1) + sum(sim.num_contacts(k) for k in (2, 3, 4))
     t_max, value = aggregate(ms, n, args.steps, world, dist, "cuda")
     log0(f"timed: {ms / args.steps:.4f} ms/step, clocks {clk}")
@@ -406,6 +409,11 @@ def run_fundem(args, rank, world, dist):
                      "kernel_ms": nar_avg, "algorithmic_bytes": nar_bytes,
                      "step_achieved_gbs": step_bytes / (t_max / args.steps / 1e3) / 1e9},
         "contact_updates_per_s": world * 0.5 * (contacts + contacts_end) * args.steps / (t_max / 1e3),
+        "pair_cache": {"skin_m": pc1[2], "rebuilds_in_timed_steps": pc1[0] - pc0[0],
+                       "timed_steps": pc1[1] - pc0[1],
+                       "note": "candidate pairs and contact slots of the particle-particle list kept between "
+                               "rebuilds (a particle drifting half the skin rebuilds them); the exact FP64 "
+                               "node predicate runs on every slot every step"},
         "kernel_ms_per_step": {k: v[0] / max(args.steps, 1) for k, v in kt.items()},
         "kernel_timing": "a second pass of K steps right after the headline, with CUDA-event timers on the "
                          "simulation's stream around each kernel group",
@@ -672,6 +680,9 @@ def main():
     ap.add_argument("--reference-gpu-steps", type=int, default=30)
     ap.add_argument("--reference-gpu-timeout", type=float, default=400.0)
     ap.add_argument("--settle-steps", type=int, default=24000, help="most settling steps of the workload")
+    ap.add_argument("--pair-cache", type=int, default=-1, choices=[-1, 0, 1],
+                    help="pair cache of the particle-particle list: -1 library default, 0 off, 1 on")
+    ap.add_argument("--pair-skin", type=float, default=0.0, help="pair-cache skin in metres (0: default)")
     ap.add_argument("--batch-sims", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=200)
     ap.add_argument("--error-steps", type=int, default=1000,

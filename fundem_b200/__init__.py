@@ -35,6 +35,7 @@ EXPORTS = [
     "fundem_adjoint_begin", "fundem_adjoint_forward", "fundem_adjoint_backward", "fundem_adjoint_end",
     "fundem_step_graph", "fundem_set_neighbour_list", "fundem_checkpoint_write", "fundem_checkpoint_read",
     "fundem_levelset_grid", "fundem_set_periodic_sector", "fundem_set_inertia_mode",
+    "fundem_set_pair_cache", "fundem_pair_cache_stats",
 ]
 TIMERS = {"integrate": 0, "hash": 1, "broad": 2, "narrow_pp": 3, "narrow_pw": 4, "ghost": 5, "reduce": 6}
 
@@ -126,6 +127,8 @@ def lib():
         L.fundem_levelset_grid.argtypes = [I, P, C.POINTER(Shape), D, C.c_double, IP, D]
         L.fundem_set_periodic_sector.argtypes = [P, I]
         L.fundem_set_inertia_mode.argtypes = [P, I]
+        L.fundem_set_pair_cache.argtypes = [P, I, C.c_double]
+        L.fundem_pair_cache_stats.argtypes = [P, C.POINTER(LL), C.POINTER(LL), C.POINTER(C.c_double)]
         _lib = L
     return _lib
 
@@ -385,6 +388,17 @@ class Simulation:
     def set_neighbour_list(self, mode):
         """-1: from the particle count, 0: off, 1: on."""
         self._check(self.L.fundem_set_neighbour_list(self.h, int(mode)), "set_neighbour_list")
+
+    def set_pair_cache(self, mode, skin=0.0):
+        """Pair cache of the particle-particle list: mode -1 (default, from
+        8192 particles), 0 off, 1 on; skin <= 0 takes the default skin."""
+        self._check(self.L.fundem_set_pair_cache(self.h, int(mode), float(skin)), "set_pair_cache")
+
+    def pair_cache_stats(self):
+        """(rebuilds, steps run with the cache, skin in metres)."""
+        r, n, sk = C.c_longlong(), C.c_longlong(), C.c_double()
+        self._check(self.L.fundem_pair_cache_stats(self.h, C.byref(r), C.byref(n), C.byref(sk)), "pair_cache_stats")
+        return r.value, n.value, sk.value
 
     def set_precision(self, precision):
         """FP64 (the reference's arithmetic) or FP32_MIXED; may change between steps."""

@@ -539,6 +539,7 @@ struct PairList {
         PairListDev v;
         v.pairA = c.pairA.p; v.pairB = c.pairB.p; v.seg_off = c.seg_off.p; v.seg_cnt = c.seg_cnt.p;
         v.c_off = c.c_off.p; v.c_cnt = c.c_cnt.p; v.pf = c.pf.p; v.n_pairs = c.counters.p; v.cap_pairs = cap_pairs;
+        v.o_pairA = o.pairA.p; v.o_counters = o.counters.p;
         v.o_pairB = o.pairB.p; v.o_seg_off = o.seg_off.p; v.o_seg_cnt = o.seg_cnt.p; v.o_c_off = o.c_off.p;
         v.o_c_cnt = o.c_cnt.p;
         v.c_node = c.c_node.p; v.c_slave = c.c_slave.p; v.c_spring = c.c_spring.p; v.c_point = c.c_point.p;
@@ -602,6 +603,11 @@ constexpr int CAPACITY_CHECK = 64;
 // neighbour list, and its skin as a fraction of the largest bounding radius
 constexpr int NL_MIN_PARTICLES = 8192;
 constexpr double NL_SKIN = 0.15;
+// pair cache (fundem_set_pair_cache): default skin as a fraction of the
+// largest particle bounding radius, and the particle count from which the
+// default mode keeps the cache
+constexpr double PC_SKIN = 0.01;
+constexpr int PC_MIN_PARTICLES = 8192;
 
 // adjoint: per-step records of the contact lists and bonds over one
 // checkpoint segment, the host checkpoints, and the reverse-sweep arrays
@@ -697,7 +703,45 @@ struct fundem_sim {
     }
     fd::NlDev nl_view()
     {
-        return fd::NlDev{nl_ref.p, nl_vis.p, nl_cnt.p, nl_list.p, nl_ctrl.p, NL_SKIN * pgeo.rmax, perX, perY};
+        return fd::NlDev{nl_ref.p, nl_vis.p, nl_cnt.p, nl_list.p, nl_ctrl.p, NL_SKIN * pgeo.rmax, perX, perY, 0.0};
+    }
+    // pair cache of the particle-particle list (fundem_set_pair_cache): the
+    // pairs and contact slots of a rebuild step are kept while no particle
+    // drifts more than half the skin; each step still runs the exact
+    // predicate on every slot
+    DevArray<double3> pc_ref_pos;
+    DevArray<fd_quat> pc_ref_q;
+    DevArray<int> pc_ref_vis, pc_ctrl;
+    int pc_mode = -1;          // -1: from the particle count, 0: off, 1: on
+    double pc_skin_set = 0.0;  // <= 0: PC_SKIN * the largest bounding radius
+    bool pc_on = false;
+    bool pc_force = true;      // the next cached step rebuilds
+    long long pc_steps = 0;    // steps run with the cache
+    void configure_pc()
+    {
+        pc_on = pc_mode > 0 || (pc_mode < 0 && P.n() >= PC_MIN_PARTICLES);
+        pc_force = true;
+        drop_graph();
+        if (!pc_on) return;
+        const size_t m = std::max(P.n(), 1);
+        pc_ref_pos.alloc(m); pc_ref_q.alloc(m); pc_ref_vis.alloc(m);
+        pc_ctrl.alloc(4);
+    }
+    double pc_skin() const { return pc_skin_set > 0.0 ? pc_skin_set : PC_SKIN * pgeo.rmax; }
+    // the adjoint records and re-runs full detections
+    bool pc_active() const { return pc_on && !adj.on && recording == nullptr && pc_ctrl.p != nullptr; }
+    fd::PairCacheDev pc_view()
+    {
+        return fd::PairCacheDev{pc_ref_pos.p, pc_ref_q.p, pc_ref_vis.p, pc_ctrl.p, pc_skin(), 2.0 * pgeo.rmax};
+    }
+    // before steps (outside any stream capture): a pending forced rebuild is
+    // written to the device flag
+    void pc_prepare()
+    {
+        if (!pc_active() || !pc_force) return;
+        const int one = 1;
+        FD_CUDA(cudaMemcpyAsync(pc_ctrl.p, &one, sizeof(int), cudaMemcpyHostToDevice, stream));
+        pc_force = false;
     }
     // reverse index over the particle and ghost lists (capacity: their pair
     // capacities together)
@@ -894,6 +938,7 @@ struct fundem_sim {
         wgrid = make_grid(mn, mx, wcell, setup_done ? &wgrid : nullptr);
         ptab.alloc(pgrid, P.n());
         configure_nl();
+        configure_pc();
         wcount.alloc((size_t)std::max<long long>(wgrid.num, 1));
         const int np = P.n();
         const int nw = W.n();
@@ -952,18 +997,43 @@ struct fundem_sim {
         if (new_generation)
             for (int k = 0; k < FD_NKIND; ++k) lists[k].cur ^= 1;
         PairListDev Lpp = lists[FD_PP].view();
+        // pair cache: steps only (a detection outside a step lists the exact
+        // pairs and slots, and the next cached step rebuilds)
+        const bool pc = with_force && probe == 0.0 && pc_active();
+        fd::PairCacheDev pcv{};
+        if (pc) {
+            pcv = pc_view();
+            fd::launch_pair_cache_check(Pv, pcv, stream);
+            launches += 1;
+            pc_steps += 1;
+        } else if (pc_on) {
+            pc_force = true;
+        }
         tbegin(FUNDEM_T_BROAD);
         if (use_nl) {
             fd::NlDev nl = nl_view();
-            fd::launch_broad_pp_nl(Pv, G, T, Lpp, nl, flags.p, probe, stream);
+            nl.pair_skin = pc ? pcv.skin : 0.0;
+            fd::launch_broad_pp_nl(Pv, G, T, Lpp, nl, flags.p, probe, stream, pc ? pcv.ctrl : nullptr);
             launches += 2;
         } else {
-            fd::launch_broad_pp(Pv, G, T, Lpp, flags.p, probe, stream);
+            fd::launch_broad_pp(Pv, G, T, Lpp, flags.p, probe, stream, pc ? pcv.skin : 0.0, pc ? pcv.ctrl : nullptr);
         }
         tend(FUNDEM_T_BROAD);
         tbegin(FUNDEM_T_NARROW_PP);
         a.rec = recording ? recording->rec(FD_PP, record_step) : fd::AdjRec{};
-        fd::launch_narrow(FD_PP, Pv, G, M, Wv, GW, MW, pgrid, wgrid, nullptr, Lpp, a, with_force, mixed(), stream);
+        {
+            fd::StepArgs ap = a;
+            if (pc) {
+                ap.skin = pcv.skin;
+                ap.gate = pcv.ctrl;
+                launches += 1;  // the carry
+            }
+            fd::launch_narrow(FD_PP, Pv, G, M, Wv, GW, MW, pgrid, wgrid, nullptr, Lpp, ap, with_force, mixed(), stream);
+        }
+        if (pc) {
+            fd::launch_pair_cache_commit(Pv, pcv, Lpp, stream);
+            launches += 1;
+        }
         if (recording)
             FD_CUDA(cudaMemcpyAsync(recording->ns(FD_PP, record_step), Lpp.n_slots, sizeof(int),
                                     cudaMemcpyDeviceToDevice, stream));
@@ -1074,7 +1144,10 @@ struct fundem_sim {
             FD_CUDA(cudaMemcpy(c, L.gen[L.cur].counters.p, sizeof(c), cudaMemcpyDeviceToHost));
             const int needp = 2 * c[0] > L.cap_pairs ? 3 * c[0] : 0;
             const int needc = 2 * c[1] > L.cap_contacts ? 3 * c[1] : 0;
-            if (needp || needc) L.grow(std::max(needp, L.cap_pairs), std::max(needc, L.cap_contacts));
+            if (needp || needc) {
+                L.grow(std::max(needp, L.cap_pairs), std::max(needc, L.cap_contacts));
+                if (k == FD_PP) pc_force = true;  // the slot-to-pair map is not kept by a growth
+            }
         }
     }
 
@@ -1252,6 +1325,33 @@ int fundem_set_neighbour_list(fundem_sim* s, int mode)
     return guard(s, [&] {
         FD_CUDA(cudaStreamSynchronize(s->stream));
         s->configure_nl();
+    });
+}
+
+int fundem_set_pair_cache(fundem_sim* s, int mode, double skin)
+{
+    if (!s || mode < -1 || mode > 1 || !(skin >= 0.0)) return FUNDEM_ERR_ARG;
+    s->pc_mode = mode;
+    s->pc_skin_set = skin;
+    if (!s->setup_done) return FUNDEM_OK;
+    return guard(s, [&] {
+        FD_CUDA(cudaStreamSynchronize(s->stream));
+        s->configure_pc();
+    });
+}
+
+int fundem_pair_cache_stats(fundem_sim* s, long long* rebuilds, long long* steps, double* skin)
+{
+    if (!s) return FUNDEM_ERR_ARG;
+    return guard(s, [&] {
+        int c[2] = {0, 0};
+        if (s->pc_ctrl.p) {
+            FD_CUDA(cudaStreamSynchronize(s->stream));
+            FD_CUDA(cudaMemcpy(c, s->pc_ctrl.p, sizeof(c), cudaMemcpyDeviceToHost));
+        }
+        if (rebuilds) *rebuilds = c[1];
+        if (steps) *steps = s->pc_on ? s->pc_steps : 0;
+        if (skin) *skin = s->pc_on ? s->pc_skin() : 0.0;
     });
 }
 
@@ -1527,6 +1627,7 @@ int fundem_step_begin(fundem_sim* s, const double g[3], double dt)
     if (!s->setup_done) return FUNDEM_ERR_STATE;
     return guard(s, [&] {
         if (++s->hook_steps % CAPACITY_CHECK == 0) s->ensure_capacity();
+        s->pc_prepare();
         s->front(d3(g), dt);
         s->detect_all(true, dt);
     });
@@ -1548,6 +1649,7 @@ int fundem_step(fundem_sim* s, int nsteps, const double g[3], double dt)
         for (int k = 0; k < nsteps; ++k) {
             // list capacities follow the counts every CAPACITY_CHECK steps
             if (k > 0 && k % CAPACITY_CHECK == 0) s->ensure_capacity();
+            s->pc_prepare();
             s->front(d3(g), dt);
             s->detect_all(true, dt);
             s->back(d3(g), dt);
@@ -1563,7 +1665,8 @@ int fundem_step_graph(fundem_sim* s, int nsteps, const double g[3], double dt)
     return guard(s, [&] {
         FD_CUDA(cudaSetDevice(s->device));
         const double key[8] = {g[0], g[1], g[2], dt, (double)s->precision, (double)s->records,
-                               (double)s->counters, (double)(s->sector * 4 + s->perX * 2 + s->perY)};
+                               (double)s->counters,
+                               (double)(s->pc_active() * 8 + s->sector * 4 + s->perX * 2 + s->perY)};
         auto reusable = [&](const fundem_sim::StepGraph& G) {
             bool same = G.exec && G.steps == nsteps && G.epoch == s->alloc_epoch && G.gepoch == g_alloc_epoch.load();
             for (int k = 0; k < 8 && same; ++k) same = G.key[k] == key[k];
@@ -1625,6 +1728,7 @@ int fundem_step_graph(fundem_sim* s, int nsteps, const double g[3], double dt)
             if (nsteps & 1)
                 for (int k = 0; k < FD_NKIND; ++k) s->lists[k].cur ^= 1;
         }
+        s->pc_prepare();
         FD_CUDA(cudaGraphLaunch(G.exec, s->stream));
         // the launch leaves the newest lists in the generation nsteps flips on
         if (nsteps & 1)
@@ -1695,6 +1799,7 @@ int fundem_set_objects(fundem_sim* s, int wall, const double* pos, const double*
     if (!s) return FUNDEM_ERR_ARG;
     ObjHost& O = wall ? s->W : s->P;
     return guard(s, [&] {
+        s->pc_force = true;  // the pair cache rebuilds at the next step
         const size_t n = O.n();
         const bool dev = (O.n_dev == (int)n) && !O.dirty && n > 0;
         auto put = [&](void* ddst, void* hdst, const double* src, size_t bytes) {
@@ -1816,6 +1921,7 @@ int fundem_set_contacts(fundem_sim* s, int kind, long long n, const int* node, c
     if (!s->setup_done) return FUNDEM_ERR_STATE;
     PairList& L = s->lists[kind];
     return guard(s, [&] {
+        s->pc_force = true;  // the pair cache rebuilds at the next step
         // group by (particle of node, partner); the list becomes the current
         // generation so the next detection reads it as history
         const int np = s->P.n();
@@ -2097,6 +2203,7 @@ int fundem_adjoint_begin(fundem_sim* s, int checkpoint_interval)
         AdjState& A = s->adj;
         A = AdjState{};
         A.on = true;
+        s->pc_force = true;  // the adjoint runs full detections; the cache rebuilds afterwards
         A.precision = s->precision;
         A.K = checkpoint_interval;
         A.ckpt.emplace_back();
@@ -2366,6 +2473,7 @@ int fundem_checkpoint_read(fundem_sim* s, const char* path)
     if (!s || !path) return FUNDEM_ERR_ARG;
     if (!s->setup_done) return FUNDEM_ERR_STATE;
     return guard(s, [&] {
+        s->pc_force = true;  // the pair cache rebuilds at the next step
         std::FILE* f = std::fopen(path, "rb");
         if (!f) throw std::invalid_argument(std::string("cannot open ") + path);
         AdjCheckpoint c;
@@ -2416,6 +2524,7 @@ int fundem_adjoint_end(fundem_sim* s)
 {
     if (!s) return FUNDEM_ERR_ARG;
     s->adj = AdjState{};
+    s->pc_force = true;
     return FUNDEM_OK;
 }
 

@@ -551,11 +551,17 @@ __device__ __forceinline__ double3 nl_min_image(double3 d, const NlDev& nl, cons
 // was requested): the sphere test is widened by the skin, the body-level
 // cull is left to the per-step filter, and each particle's partners go to its
 // fixed slice of the list.
+//
+// skin (pair cache): partners within rA + rB + skin are listed and the
+// body-level cull treats A's sphere as skin larger; gate: the kernel runs
+// only when *gate != 0 (null: always).
 template <bool GHOST, bool LIST, bool NLB>
 __global__ void __launch_bounds__(TPB) k_broad_cells(ObjDev P, GeoSetDev G, CellTableDev T, const double3* gpos,
                                                      const float4* grot, const int* occ, const int* alist, const int* acount,
-                                                     PairListDev L, NlDev nl, unsigned int* flags, double probe)
+                                                     PairListDev L, NlDev nl, unsigned int* flags, double probe,
+                                                     double skin, const int* gate)
 {
+    if (gate && *gate == 0) return;
     if (NLB && nl.ctrl[0] == 0) return;
     __shared__ int s_list[TPB / BROAD_LANES][MAX_CAND];
     __shared__ int s_cand[TPB / BROAD_LANES][BROAD_CAND];
@@ -579,7 +585,7 @@ __global__ void __launch_bounds__(TPB) k_broad_cells(ObjDev P, GeoSetDev G, Cell
         cA = P.pos[A];
         rA = G.geo[P.geo[A]].radius;
         // above the sphere test's own tolerance (rs * (1 + 2 BOUND_REL))
-        const double reach = (rA + (GHOST ? G.grid_rmax : G.rmax)) * (1.0 + 8.0 * BOUND_REL) + (NLB ? nl.skin : 0.0);
+        const double reach = (rA + (GHOST ? G.grid_rmax : G.rmax)) * (1.0 + 8.0 * BOUND_REL) + (NLB ? nl.skin : skin);
         if (NLB && gl == 0) {
             nl.ref[A] = cA;
             nl.vis[A] = P.hash[A] >= 0;
@@ -652,10 +658,10 @@ __global__ void __launch_bounds__(TPB) k_broad_cells(ObjDev P, GeoSetDev G, Cell
                         const double rs = (rA + GB.radius) * (1.0 + 8.0 * BOUND_REL) + nl.skin;
                         pass = lengthSq3(nl_min_image(cA - cB, nl, T.g)) <= rs * rs;
                     } else {
-                        const double rs = rA + (GHOST ? GB.grid_radius : GB.radius);
+                        const double rs = rA + (GHOST ? GB.grid_radius : GB.radius) + skin;
                         if (lengthSq3(cA - cB) <= rs * rs * (1.0 + 4.0 * BOUND_REL))
-                            pass = !body_culled32(cA, rA, cB, (GHOST && grot ? grot : P.rot) + 3ll * B, !GHOST,
-                                                  GB, G, probe);
+                            pass = !body_culled32(cA, rA + skin, cB, (GHOST && grot ? grot : P.rot) + 3ll * B,
+                                                  !GHOST, GB, G, probe);
                     }
                 }
             }
@@ -709,11 +715,13 @@ __global__ void __launch_bounds__(TPB) k_broad_cells(ObjDev P, GeoSetDev G, Cell
 
 // neighbour list: request a rebuild when a particle moved more than skin / 2
 // since the last build or changed visibility
-__global__ void k_nl_check(ObjDev P, NlDev nl, FdGrid g)
+__global__ void k_nl_check(ObjDev P, NlDev nl, FdGrid g, const int* gate)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.n) return;
-    const double h = 0.5 * nl.skin;
+    if (i >= P.n || (gate && *gate == 0)) return;
+    // with the pair cache, partners within rA + rB + pair_skin must stay
+    // listed: the list is rebuilt before any particle moves (skin - pair_skin) / 2
+    const double h = 0.5 * (nl.skin - nl.pair_skin);
     const bool moved = lengthSq3(nl_min_image(P.pos[i] - nl.ref[i], nl, g)) > h * h;
     const bool vis = P.hash[i] >= 0;
     if (moved || vis != (nl.vis[i] != 0)) nl.ctrl[0] = 1;
@@ -723,8 +731,9 @@ __global__ void k_nl_check(ObjDev P, NlDev nl, FdGrid g)
 // body-level cull of the cell search, on the listed partners (ascending, so
 // each particle's pairs come out in partner order)
 __global__ void __launch_bounds__(TPB) k_nl_filter(ObjDev P, GeoSetDev G, PairListDev L, NlDev nl,
-                                                   unsigned int* flags, double probe)
+                                                   unsigned int* flags, double probe, const int* gate)
 {
+    if (gate && *gate == 0) return;
     constexpr int LN = 8;  // lanes per particle
     const unsigned int full = 0xffffffffu;
     const int lane = threadIdx.x & 31, gl = lane & (LN - 1), gbase = lane & ~(LN - 1);
@@ -749,9 +758,9 @@ __global__ void __launch_bounds__(TPB) k_nl_filter(ObjDev P, GeoSetDev G, PairLi
             if (P.hash[B] >= 0) {
                 const FdGeo& GB = G.geo[P.geo[B]];
                 const double3 cB = P.pos[B];
-                const double rs = rA + GB.radius;
+                const double rs = rA + GB.radius + nl.pair_skin;
                 if (lengthSq3(cA - cB) <= rs * rs * (1.0 + 4.0 * BOUND_REL))
-                    pass = !body_culled32(cA, rA, cB, P.rot + 3ll * B, true, GB, G, probe);
+                    pass = !body_culled32(cA, rA + nl.pair_skin, cB, P.rot + 3ll * B, true, GB, G, probe);
             }
         }
         const unsigned int gm = (__ballot_sync(full, pass) >> gbase) & ((1u << LN) - 1u);
@@ -776,6 +785,87 @@ __global__ void __launch_bounds__(TPB) k_nl_filter(ObjDev P, GeoSetDev G, PairLi
         }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) nl.ctrl[0] = 0;
+}
+
+// ---------------------------------------------------------------------------
+// pair cache of the particle-particle list (see PairCacheDev)
+// ---------------------------------------------------------------------------
+// flag a rebuild when a particle drifted by more than skin / 2 since the last
+// build or changed visibility
+__global__ void k_pc_check(ObjDev P, PairCacheDev c)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.n || c.ctrl[0] != 0) return;
+    if (c.ctrl[2] != 0) {
+        // the last build overflowed its lists: build again
+        c.ctrl[0] = 1;
+        return;
+    }
+    const double3 d = P.pos[i] - c.ref_pos[i];
+    // 2 sin(theta / 2) = 2 |vector part of q conj(q0)|: the chord a unit
+    // lever arm sweeps under the rotation since the build
+    const fd_quat q = P.q[i], r = c.ref_q[i];
+    const double vx = r.q0 * q.q1 - q.q0 * r.q1 - (q.q2 * r.q3 - q.q3 * r.q2);
+    const double vy = r.q0 * q.q2 - q.q0 * r.q2 - (q.q3 * r.q1 - q.q1 * r.q3);
+    const double vz = r.q0 * q.q3 - q.q0 * r.q3 - (q.q1 * r.q2 - q.q2 * r.q1);
+    const double chord = 2.0 * sqrt(vx * vx + vy * vy + vz * vz);
+    const double drift = sqrt(lengthSq3(d)) + c.reach * chord;
+    // a little below skin / 2, so that the two drifts of a pair stay below
+    // the single-precision skin the culling stages use
+    const bool vis = P.hash[i] >= 0;
+    if (!(drift <= 0.5 * c.skin * (1.0 - 1e-6)) || vis != (c.ref_vis[i] != 0)) c.ctrl[0] = 1;
+}
+
+// a step without a rebuild: this step's pairs and slots are the previous
+// step's, carried over; each pair's history is its own slots of the previous
+// step, and its partner's cell is taken from this step's hash
+__global__ void k_pc_carry(PairListDev L, ObjDev P, FdGrid g, const int* gate)
+{
+    if (*gate != 0) return;
+    const int npairs = min(L.o_counters[0], L.cap_pairs);
+    const int nslots = min(L.o_counters[1], L.cap_contacts);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t0 == 0) {
+        *L.n_pairs = L.o_counters[0];
+        *L.n_slots = L.o_counters[1];
+    }
+    for (long long i = t0; i < P.n; i += stride) {
+        L.seg_off[i] = L.o_seg_off[i];
+        L.seg_cnt[i] = L.o_seg_cnt[i];
+    }
+    for (long long p = t0; p < npairs; p += stride) {
+        const int B = L.o_pairB[p];
+        const int off = L.o_c_off[p], cnt = L.o_c_cnt[p];
+        L.pairA[p] = L.o_pairA[p];
+        L.pairB[p] = B;
+        L.c_off[p] = off;
+        L.c_cnt[p] = cnt;
+        if (cnt > 0) {
+            int3 bc;
+            decode_cell(P.hash[B], g.size, bc);
+            L.p_aux[p] = make_int4(bc.x, bc.y, bc.z, off);
+            L.p_hist_cnt[p] = cnt;
+        }
+    }
+    for (long long k = t0; k < nslots; k += stride) L.c_k[k] = L.o_c_k[k];
+}
+
+// after the particle-particle narrow phase of a rebuild step: its state is the
+// new reference; the flag is cleared for the next step
+__global__ void k_pc_commit(ObjDev P, PairCacheDev c, PairListDev L)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.n || c.ctrl[0] == 0) return;
+    c.ref_pos[i] = P.pos[i];
+    c.ref_q[i] = P.q[i];
+    c.ref_vis[i] = P.hash[i] >= 0;
+    if (i == 0) {
+        c.ctrl[1] += 1;
+        // a build whose pairs or slots did not fit is not kept: the next
+        // step builds again (the host grows the lists at its next check)
+        c.ctrl[2] = (*L.n_pairs > L.cap_pairs || *L.n_slots > L.cap_contacts) ? 1 : 0;
+    }
 }
 
 // ghost phases: particles whose search box reaches the cells holding ghost
@@ -1071,10 +1161,21 @@ __device__ __forceinline__ bool node_filtered(const float4 p, const CullXf& x, c
         const float slack = (float)GB.lip * perr + 1e-5f * (fabsf(phi) + (float)GB.spacing);
         return phi - (float)probe > slack;
     }
-    if (fx < ge || fy < ge || fz < ge || fx > 1.f - ge || fy > 1.f - ge || fz > 1.f - ge) return false;
-    const float cm = __ldg(SB.cellmin + GB.cellmin_off +
-                           ((long long)k0 * (GB.size.y - 1) + j0) * (GB.size.x - 1) + i0);
-    return cm > (float)probe;
+    // the trilinear value anywhere the node can be (within ge of its
+    // single-precision position, in grid units) is at least the smallest
+    // corner minimum over the cells that box touches (one to a few cells:
+    // two per axis where the node is within ge of a cell face)
+    const int ilo = max((int)floorf(gx - ge), 0), ihi = min((int)floorf(gx + ge), GB.size.x - 2);
+    const int jlo = max((int)floorf(gy - ge), 0), jhi = min((int)floorf(gy + ge), GB.size.y - 2);
+    const int klo = max((int)floorf(gz - ge), 0), khi = min((int)floorf(gz + ge), GB.size.z - 2);
+    if (ihi - ilo > 2 || jhi - jlo > 2 || khi - klo > 2) return false;  // a margin of more than a cell: keep
+    const long long rx = GB.size.x - 1, rxy = (long long)(GB.size.y - 1) * (GB.size.x - 1);
+    const float* CM = SB.cellmin + GB.cellmin_off;
+    for (int k = klo; k <= khi; ++k)
+        for (int j = jlo; j <= jhi; ++j)
+            for (int i = ilo; i <= ihi; ++i)
+                if (__ldg(CM + k * rxy + j * rx + i) <= (float)probe) return false;
+    return true;
 }
 
 #ifndef FD_SELECT_MIN_BLOCKS
@@ -1092,9 +1193,15 @@ __device__ __forceinline__ bool node_filtered(const float4 p, const CullXf& x, c
 // The warp also finds the pair in the previous step's list, the history
 // source of its contacts.
 // ---------------------------------------------------------------------------
+//
+// With the pair cache (n.a.gate non-null) the kernel runs only on rebuild
+// steps, and every culling margin is widened by the skin n.a.skin: a cluster
+// is kept when it may come within reach of B after moves of up to the skin,
+// a node is slotted when it may pass the predicate after such moves.
 template <int KIND>
 __global__ void __launch_bounds__(NARROW_WARPS * 32, FD_SELECT_MIN_BLOCKS) k_select(NarrowArgs n)
 {
+    if (n.a.gate && *n.a.gate == 0) return;
     __shared__ unsigned short s_node[NARROW_WARPS][MAX_NODE_QUEUE];
     // work counters, summed per block and added to the global ones once
     __shared__ unsigned long long s_stats[4];
@@ -1123,14 +1230,18 @@ __global__ void __launch_bounds__(NARROW_WARPS * 32, FD_SELECT_MIN_BLOCKS) k_sel
         for (int c0 = 0; c0 < min(ncl, MAX_CLUSTERS); c0 += 32) {
             const int c = c0 + lane;
             bool k = false;
-            if (c < ncl) k = !cluster_culled<KIND>(n.G.clus_sphere[GA.clus_off + c], xf, GB, SB, rB, n.a.probe);
+            if (c < ncl) {
+                float4 cl = n.G.clus_sphere[GA.clus_off + c];
+                cl.w += (float)n.a.skin;
+                k = !cluster_culled<KIND>(cl, xf, GB, SB, rB, n.a.probe);
+            }
             keep |= ((unsigned long long)__ballot_sync(0xffffffffu, k)) << c0;
         }
         const int kept = __popcll(keep);
         // ---- single-precision filter over the nodes of the surviving
         // clusters; nodes that may pass the predicate are queued in cluster
         // order
-        const float perr = 4e-6f * (float)(length3(cA - cB) + GA.radius + rB + GB.spacing);
+        const float perr = 4e-6f * (float)(length3(cA - cB) + GA.radius + rB + GB.spacing) + (float)n.a.skin;
         int ncand = 0;
         while (keep) {
             const int c = __ffsll((long long)keep) - 1;
@@ -2131,22 +2242,31 @@ void launch_sector_images(const ObjDev& P, GhostDev* R, cudaStream_t s)
 }
 
 void launch_broad_pp(const ObjDev& P, const GeoSetDev& G, const CellTableDev& T, PairListDev& L,
-                     unsigned int* flags, double probe, cudaStream_t s)
+                     unsigned int* flags, double probe, cudaStream_t s, double skin, const int* gate)
 {
     cudaMemsetAsync(L.n_pairs, 0, sizeof(int), s);
     if (P.n > 0)
         k_broad_cells<false, false, false><<<nblocks((long long)P.n * BROAD_LANES), TPB, 0, s>>>(
-            P, G, T, nullptr, nullptr, nullptr, nullptr, nullptr, L, NlDev{}, flags, probe);
+            P, G, T, nullptr, nullptr, nullptr, nullptr, nullptr, L, NlDev{}, flags, probe, skin, gate);
 }
 void launch_broad_pp_nl(const ObjDev& P, const GeoSetDev& G, const CellTableDev& T, PairListDev& L, NlDev& nl,
-                        unsigned int* flags, double probe, cudaStream_t s)
+                        unsigned int* flags, double probe, cudaStream_t s, const int* gate)
 {
     cudaMemsetAsync(L.n_pairs, 0, sizeof(int), s);
     if (P.n <= 0) return;
-    k_nl_check<<<nblocks(P.n), TPB, 0, s>>>(P, nl, T.g);
+    k_nl_check<<<nblocks(P.n), TPB, 0, s>>>(P, nl, T.g, gate);
     k_broad_cells<false, false, true><<<nblocks((long long)P.n * BROAD_LANES), TPB, 0, s>>>(
-        P, G, T, nullptr, nullptr, nullptr, nullptr, nullptr, L, nl, flags, probe);
-    k_nl_filter<<<nblocks((long long)P.n * 8), TPB, 0, s>>>(P, G, L, nl, flags, probe);
+        P, G, T, nullptr, nullptr, nullptr, nullptr, nullptr, L, nl, flags, probe, 0.0, gate);
+    k_nl_filter<<<nblocks((long long)P.n * 8), TPB, 0, s>>>(P, G, L, nl, flags, probe, gate);
+}
+void launch_pair_cache_check(const ObjDev& P, const PairCacheDev& c, cudaStream_t s)
+{
+    if (P.n > 0) k_pc_check<<<nblocks(P.n), TPB, 0, s>>>(P, c);
+}
+void launch_pair_cache_commit(const ObjDev& P, const PairCacheDev& c, const PairListDev& L, cudaStream_t s)
+{
+    if (P.n > 0) k_pc_commit<<<nblocks(P.n), TPB, 0, s>>>(P, c, L);
+    cudaMemsetAsync(c.ctrl, 0, sizeof(int), s);
 }
 
 void launch_broad_pw(const ObjDev& P, const GeoSetDev& G, const ObjDev& W, const GeoSetDev& GW,
@@ -2164,7 +2284,7 @@ void launch_broad_ghost(const ObjDev& P, const GeoSetDev& G, const GhostDev& Gh,
     k_ghost_searchers<<<nblocks(P.n), TPB, 0, s>>>(P, G, Gh.cells.g, Gh.occ, L, Gh.searchers, Gh.nsearch);
     const long long groups = std::min<long long>(P.n, 148ll * 8 * (TPB / BROAD_LANES));
     k_broad_cells<true, true, false><<<nblocks(groups * BROAD_LANES), TPB, 0, s>>>(
-        P, G, Gh.cells, Gh.pos, Gh.rot, Gh.occ, Gh.searchers, Gh.nsearch, L, NlDev{}, flags, probe);
+        P, G, Gh.cells, Gh.pos, Gh.rot, Gh.occ, Gh.searchers, Gh.nsearch, L, NlDev{}, flags, probe, 0.0, nullptr);
 }
 
 void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& M, const ObjDev& W,
@@ -2184,6 +2304,7 @@ void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& 
 #define FD_NARROW_CASE(K)                                                              \
     case K:                                                                            \
         k_select<K><<<grid, NARROW_WARPS * 32, 0, s>>>(n);                             \
+        if (a.gate) k_pc_carry<<<148 * 8, TPB, 0, s>>>(L, P, pgrid, a.gate);          \
         if (mixed) k_contact32<K><<<cgrid, TPB, 0, s>>>(n);                            \
         else k_contact<K><<<cgrid, TPB, 0, s>>>(n);                                    \
         break;

@@ -18,6 +18,8 @@ struct PairListDev {
     int* n_pairs;      // device counter
     int cap_pairs;
     // previous step (history source)
+    int* o_pairA;
+    int* o_counters;   // previous step's counters: pairs, slots, contacts
     int* o_pairB;
     int* o_seg_off;
     int* o_seg_cnt;
@@ -180,6 +182,29 @@ struct NlDev {
     int* ctrl;      // [0]: rebuild requested
     double skin;
     int periodic_x, periodic_y;  // distances and displacements by minimum image
+    double pair_skin;   // positional skin of the pair cache (0 without it): the
+                        // list is rebuilt once a particle moved (skin - pair_skin) / 2
+};
+
+// Pair cache of the particle-particle list.  The candidate pairs and the
+// nodes that may pass the node predicate (the contact slots) are built with
+// every culling margin widened by a positional skin, and kept while no
+// particle has drifted by more than skin / 2 since that build: the drift of
+// particle i is |c_i - c_i0| + 2 r_max * 2 sin(theta_i / 2), theta_i its
+// rotation since the build, which bounds how far any node of a pair can move
+// in its partner's body frame (pairs stay listed, nodes stay slotted, while
+// the two drifts sum to less than the skin).  Every step still runs the
+// exact double-precision predicate on every slot, so the contacts are the
+// ones a full detection gives.  ctrl[0]: rebuild this step (set by the check
+// or by the host), ctrl[1]: rebuilds so far, ctrl[2]: the last build
+// overflowed its lists (the next step builds again).
+struct PairCacheDev {
+    double3* ref_pos;   // positions at the last build
+    fd_quat* ref_q;     // orientations at the last build
+    int* ref_vis;       // visibility (hashed) at the last build
+    int* ctrl;
+    double skin;
+    double reach;       // 2 r_max: lever arm of a rotation in the drift bound
 };
 
 struct StepArgs {
@@ -190,6 +215,8 @@ struct StepArgs {
     int periodic_x, periodic_y;
     int sector;      // sector periodicity (the force side of particle and wall contacts folds bodies)
     int records;
+    double skin;       // positional skin of the culling stages (the pair cache; 0 without it)
+    const int* gate;   // pair cache: the selection runs only when *gate != 0 (null: always)
     unsigned int* flags;
     unsigned long long* stats;  // optional: pairs, clusters, clusters kept, contacts (narrow kernels)
 };
@@ -206,16 +233,26 @@ void launch_ghost_build(const ObjDev& P, GhostDev& Gh, int kind, cudaStream_t s)
 void launch_sector_wrap(ObjDev& P, const FdGrid& g, cudaStream_t s);
 void launch_sector_images(const ObjDev& P, GhostDev* R, cudaStream_t s);
 
-// pair lists
+// pair lists.  skin widens the sphere tests and the body-level cull (the pair
+// cache); with gate non-null the kernels run only when *gate != 0
 void launch_broad_pp(const ObjDev& P, const GeoSetDev& G, const CellTableDev& T, PairListDev& L,
-                     unsigned int* flags, double probe, cudaStream_t s);
+                     unsigned int* flags, double probe, cudaStream_t s, double skin = 0.0,
+                     const int* gate = nullptr);
 // the same pairs through the neighbour list (check, conditional rebuild, filter)
 void launch_broad_pp_nl(const ObjDev& P, const GeoSetDev& G, const CellTableDev& T, PairListDev& L, NlDev& nl,
-                        unsigned int* flags, double probe, cudaStream_t s);
+                        unsigned int* flags, double probe, cudaStream_t s, const int* gate = nullptr);
+// pair cache: flag a rebuild when a particle drifted by more than skin / 2
+// (or changed visibility); after the particle-particle narrow phase, keep
+// the state of a rebuild step as the new reference and clear the flag
+void launch_pair_cache_check(const ObjDev& P, const PairCacheDev& c, cudaStream_t s);
+void launch_pair_cache_commit(const ObjDev& P, const PairCacheDev& c, const PairListDev& L, cudaStream_t s);
 void launch_broad_pw(const ObjDev& P, const GeoSetDev& G, const ObjDev& W, const GeoSetDev& GW,
                      const FdGrid& wg, PairListDev& L, unsigned int* flags, double probe, cudaStream_t s);
 void launch_broad_ghost(const ObjDev& P, const GeoSetDev& G, const GhostDev& Gh, PairListDev& L,
                         unsigned int* flags, double probe, cudaStream_t s);
+// a.gate non-null (particle-particle list under the pair cache): on steps
+// without a rebuild the selection is skipped and the previous step's pairs
+// and slots are carried into this step's list
 void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& M, const ObjDev& W,
                    const GeoSetDev& GW, const MatDev& MW, const FdGrid& pgrid, const FdGrid& wgrid,
                    const GhostDev* gh, PairListDev& L, const StepArgs& a, int with_force, bool mixed, cudaStream_t s);

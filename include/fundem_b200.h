@@ -58,6 +58,25 @@ int fundem_set_precision(fundem_sim* sim, int mode);
    one; both give the same pairs.  Takes effect at the next detection.
    No counterpart in the reference. */
 int fundem_set_neighbour_list(fundem_sim* sim, int mode);
+/* Pair cache of the particle-particle list.  The reference detects every
+   step from scratch (count and write passes, LSParticleContactDetectionKernel.cu:4-305,
+   after a fresh hash and sort).  With the cache, the candidate pairs and the
+   nodes that may pass the node predicate (the contact slots) are built with
+   every culling margin widened by a positional skin, and kept while no
+   particle has drifted by more than half the skin since that build (drift:
+   centre displacement plus twice the largest bounding radius times the
+   chord of its rotation); a particle that changes visibility, a periodic
+   wrap, a list growth or a state change through this API rebuilds them.
+   Every step still evaluates the exact double-precision predicate on every
+   slot, so the contacts are those a full detection gives.  mode -1 (default)
+   keeps the cache from 8192 particles on, 0 never, 1 always; skin <= 0
+   picks 0.01 times the largest particle bounding radius.  The adjoint's
+   recording runs full detections.  Takes effect at the next step.
+   No counterpart in the reference. */
+int fundem_set_pair_cache(fundem_sim* sim, int mode, double skin);
+/* rebuilds of the pair cache and steps run with it since setup, and the skin
+   in use (zeros when the cache is off) */
+int fundem_pair_cache_stats(fundem_sim* sim, long long* rebuilds, long long* steps, double* skin);
 /* when nonzero every step writes full contact records (point, normal,
    overlap, energies); otherwise only node, partner and sliding spring */
 int fundem_set_records(fundem_sim* sim, int full_records);

@@ -16,8 +16,14 @@ arranged so every code path sees work:
 * `pour_mm`: mm-scale config-0 shapes (the inverse inertia falls under the
   1e-30 determinant threshold and is zero).
 * `sphere`: the sphere-on-plane case of the reference's test app.
+* `pour1000`: the small pour as configured (1,000 superellipsoids from 4
+  templates, 32^3 grids, 642 nodes, six plane walls of a 20 x 20 x 40 mm box,
+  seed 0), its lattice pulled 3% towards the box centre and given small
+  random velocities, so that contacts start at once.
 """
 from __future__ import annotations
+
+import copy
 
 import numpy as np
 
@@ -146,8 +152,29 @@ def sphere():
     return S.sphere_on_plane()
 
 
-CASES = {"cluster": cluster, "periodic": periodic, "pour_mm": pour_mm, "sphere": sphere, "sector": sector}
+_POUR0 = {}
+
+
+def pour_config0():
+    """The small pour exactly as configured (scenario.pour() defaults).  Its
+    host-side overlap resolution takes tens of seconds, so it is built once
+    per process; each call returns an independent copy."""
+    if "sc" not in _POUR0:
+        _POUR0["sc"] = S.pour()
+    return copy.deepcopy(_POUR0["sc"])
+
+
+def pour1000(seed=0):
+    sc = pour_config0()
+    sc.name = "pour1000"
+    _compress(sc.particles, np.array([10e-3, 10e-3, 20e-3]), 0.97)
+    sc.particles.vel[:] = np.random.default_rng(seed).normal(0, 0.02, (len(sc.particles), 3))
+    return sc
+
+
+CASES = {"cluster": cluster, "periodic": periodic, "pour_mm": pour_mm, "sphere": sphere, "sector": sector,
+         "pour1000": pour1000}
 # in-loop steps the reference runs per case and the steps it dumps
 REF_STEPS = {"cluster": (40, [1, 2, 3, 10, 11, 39, 40]), "periodic": (40, [1, 2, 3, 10, 11, 39, 40]),
              "sector": (40, [1, 2, 3, 10, 11, 39, 40]),
-             "pour_mm": (20, [1, 2, 3, 19, 20]), "sphere": (10000, [1, 2, 4500, 4550, 4600, 4650, 4700, 9000, 10000])}
+             "pour_mm": (20, [1, 2, 3, 19, 20]), "pour1000": (20, [1, 2, 10, 11, 19, 20]), "sphere": (10000, [1, 2, 4500, 4550, 4600, 4650, 4700, 9000, 10000])}

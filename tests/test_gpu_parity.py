@@ -15,7 +15,7 @@ import parity_cases as PC
 pytestmark = pytest.mark.gpu
 
 KINDS = ("pp", "pw", "gx", "gy", "gxy")
-CASES = ["cluster", "periodic", "pour_mm"]
+CASES = ["cluster", "periodic", "pour_mm", "pour1000"]
 
 
 def _pair(fundem, oracle_mod, name):

@@ -170,7 +170,7 @@ def _rebuild_and_check(name):
     return g
 
 
-@pytest.mark.parametrize("name", ["cluster", "periodic", "pour_mm", "sector"])
+@pytest.mark.parametrize("name", ["cluster", "periodic", "pour_mm", "sector", "pour1000"])
 def test_oracle_geometry_matches_reference(oracle_mod, name):
     g = _rebuild_and_check(name)
     w = oracle_mod.OracleWorld.from_scenario(PC.CASES[name]())
@@ -211,7 +211,7 @@ def _oracle_at(oracle_mod, name, g, step):
     return w
 
 
-@pytest.mark.parametrize("name", ["cluster", "periodic", "pour_mm", "sector"])
+@pytest.mark.parametrize("name", ["cluster", "periodic", "pour_mm", "sector", "pour1000"])
 def test_oracle_detection_bit_exact_vs_reference(oracle_mod, name):
     """From the reference's exact state at step s, the oracle's detection
     reproduces the reference's contact set and overlaps bit for bit (the
@@ -245,7 +245,7 @@ def test_oracle_detection_bit_exact_vs_reference(oracle_mod, name):
     assert checked > 0
 
 
-@pytest.mark.parametrize("name", ["cluster", "pour_mm"])
+@pytest.mark.parametrize("name", ["cluster", "pour_mm", "pour1000"])
 def test_oracle_overlaps_bitwise_from_reference_state(oracle_mod, name):
     """Detection from the reference's dumped positions at step s (no
     integration in between): overlaps agree bit for bit."""
