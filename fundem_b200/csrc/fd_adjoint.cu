@@ -411,22 +411,22 @@ __global__ void k_adj_particle(AdjParticles a, double dt)
 
 void adj_force(const AdjParticles& a, double dt, cudaStream_t s)
 {
-    if (a.n > 0) k_adj_force<<<(a.n + 255) / 256, 256, 0, s>>>(a, dt);
+    if (a.n > 0) { k_adj_force<<<(a.n + 255) / 256, 256, 0, s>>>(a, dt); count_launch(); }
 }
 // Both precisions of the step are swept with double-precision Jacobians: the
 // single-precision evaluation of a contact's Jacobian gave non-finite
 // gradients on a 4,096-particle pour, where contacts separate from the walls.
 void adj_contacts(const AdjParticles& a, const AdjContactArgs& c, cudaStream_t s)
 {
-    if (c.rec.cap > 0) k_adj_contact<double><<<(c.rec.cap + ADJ_TPB - 1) / ADJ_TPB, ADJ_TPB, 0, s>>>(a, c);
+    if (c.rec.cap > 0) { k_adj_contact<double><<<(c.rec.cap + ADJ_TPB - 1) / ADJ_TPB, ADJ_TPB, 0, s>>>(a, c); count_launch(); }
 }
 void adj_bonds(const AdjParticles& a, const AdjBondArgs& b, cudaStream_t s)
 {
-    if (b.n > 0) k_adj_bond<double><<<(b.n + 255) / 256, 256, 0, s>>>(a, b);
+    if (b.n > 0) { k_adj_bond<double><<<(b.n + 255) / 256, 256, 0, s>>>(a, b); count_launch(); }
 }
 void adj_particles(const AdjParticles& a, double dt, cudaStream_t s)
 {
-    if (a.n > 0) k_adj_particle<<<(a.n + 255) / 256, 256, 0, s>>>(a, dt);
+    if (a.n > 0) { k_adj_particle<<<(a.n + 255) / 256, 256, 0, s>>>(a, dt); count_launch(); }
 }
 
 }  // namespace fd

@@ -484,7 +484,7 @@ struct PairList {
     // (node, partner) of the list set_contacts uploaded last, in slot order
     std::vector<int> up_node, up_partner;
     // slot and pair scratch of the current step only
-    DevArray<int> c_pair, p_hist_cnt;
+    DevArray<int> c_pair, c_hit, p_hist_cnt;
     DevArray<double> c_force;
     DevArray<int4> p_aux;
     bool allocated = false;
@@ -504,7 +504,7 @@ struct PairList {
             g.c_overlap.alloc(cap_contacts); g.c_en.alloc(cap_contacts); g.c_es.alloc(cap_contacts);
             g.counters.alloc(3);
         }
-        c_pair.alloc(cap_contacts); c_force.alloc((size_t)cap_contacts * 9);
+        c_pair.alloc(cap_contacts); c_hit.alloc(cap_contacts, false); c_force.alloc((size_t)cap_contacts * 9);
         p_aux.alloc(cap_pairs); p_hist_cnt.alloc(cap_pairs);
         allocated = true;
     }
@@ -528,6 +528,7 @@ struct PairList {
                 g.c_overlap.grow(capc, cap_contacts); g.c_en.grow(capc, cap_contacts); g.c_es.grow(capc, cap_contacts);
             }
             c_pair.grow(capc, 0);
+            c_hit.grow(capc, 0);
             c_force.grow((size_t)capc * 9, 0);
             cap_contacts = capc;
         }
@@ -545,7 +546,7 @@ struct PairList {
         v.c_node = c.c_node.p; v.c_slave = c.c_slave.p; v.c_spring = c.c_spring.p; v.c_point = c.c_point.p;
         v.c_normal = c.c_normal.p; v.c_overlap = c.c_overlap.p; v.c_en = c.c_en.p; v.c_es = c.c_es.p;
         v.n_slots = c.counters.p + 1; v.n_hits = c.counters.p + 2; v.cap_contacts = cap_contacts;
-        v.c_pair = c_pair.p; v.c_k = c.c_k.p; v.o_c_k = o.c_k.p; v.c_force = c_force.p; v.p_aux = p_aux.p; v.p_hist_cnt = p_hist_cnt.p;
+        v.c_pair = c_pair.p; v.c_hit = c_hit.p; v.c_k = c.c_k.p; v.o_c_k = o.c_k.p; v.c_force = c_force.p; v.p_aux = p_aux.p; v.p_hist_cnt = p_hist_cnt.p;
         v.o_c_node = o.c_node.p; v.o_c_spring = o.c_spring.p;
         return v;
     }
@@ -985,12 +986,10 @@ struct fundem_sim {
         tbegin(FUNDEM_T_HASH);
         fd::launch_hash_count(Pv, T, stream);
         fd::launch_cell_table(Pv, T, scan_tmp.p, scan_tmp.n, stream);
-        launches += 3;
         // wall hash (visibility and cell for the node test)
         if (W.n_dev > 0) {
             CellTableDev wt{wgrid, wcount.p, nullptr, nullptr, nullptr};
             fd::launch_hash_count(Wv, wt, stream);
-            launches += 1;
         }
         tend(FUNDEM_T_HASH);
         int active[FD_NKIND] = {1, 1, 0, 0, 0};
@@ -1004,7 +1003,6 @@ struct fundem_sim {
         if (pc) {
             pcv = pc_view();
             fd::launch_pair_cache_check(Pv, pcv, stream);
-            launches += 1;
             pc_steps += 1;
         } else if (pc_on) {
             pc_force = true;
@@ -1014,7 +1012,6 @@ struct fundem_sim {
             fd::NlDev nl = nl_view();
             nl.pair_skin = pc ? pcv.skin : 0.0;
             fd::launch_broad_pp_nl(Pv, G, T, Lpp, nl, flags.p, probe, stream, pc ? pcv.ctrl : nullptr);
-            launches += 2;
         } else {
             fd::launch_broad_pp(Pv, G, T, Lpp, flags.p, probe, stream, pc ? pcv.skin : 0.0, pc ? pcv.ctrl : nullptr);
         }
@@ -1026,13 +1023,11 @@ struct fundem_sim {
             if (pc) {
                 ap.skin = pcv.skin;
                 ap.gate = pcv.ctrl;
-                launches += 1;  // the carry
             }
             fd::launch_narrow(FD_PP, Pv, G, M, Wv, GW, MW, pgrid, wgrid, nullptr, Lpp, ap, with_force, mixed(), stream);
         }
         if (pc) {
             fd::launch_pair_cache_commit(Pv, pcv, Lpp, stream);
-            launches += 1;
         }
         if (recording)
             FD_CUDA(cudaMemcpyAsync(recording->ns(FD_PP, record_step), Lpp.n_slots, sizeof(int),
@@ -1049,7 +1044,6 @@ struct fundem_sim {
             FD_CUDA(cudaMemcpyAsync(recording->ns(FD_PW, record_step), Lpw.n_slots, sizeof(int),
                                     cudaMemcpyDeviceToDevice, stream));
         tend(FUNDEM_T_NARROW_PW);
-        launches += 4;
         PairListDev Lg[6];
         if (perX || perY || sector) {
             tbegin(FUNDEM_T_GHOST);
@@ -1058,25 +1052,22 @@ struct fundem_sim {
             const int kinds[6] = {FD_GX, FD_GY, FD_GXY, FD_GR90, FD_GR180, FD_GR270};
             for (int d = 0; d < 3; ++d) {
                 if (!ghosts[d].active) continue;
-                if (d == 0) { fd::launch_wrap(Pv, pgrid, 0, stream); launches++; }
-                if (d == 1) { fd::launch_wrap(Pv, pgrid, 1, stream); launches++; }
+                if (d == 0) fd::launch_wrap(Pv, pgrid, 0, stream);
+                if (d == 1) fd::launch_wrap(Pv, pgrid, 1, stream);
                 fd::GhostDev gh = ghosts[d].view();
                 fd::launch_ghost_build(Pv, gh, kinds[d], stream);
                 ObjDev ghostobj = Pv;
                 ghostobj.hash = ghosts[d].hash.p;
                 fd::launch_cell_table(ghostobj, gh.cells, scan_tmp.p, scan_tmp.n, stream);
-                launches += 3;
             }
             if (sector) {
                 fd::launch_sector_wrap(Pv, pgrid, stream);
                 fd::GhostDev sv[3] = {ghosts[3].view(), ghosts[4].view(), ghosts[5].view()};
                 fd::launch_sector_images(Pv, sv, stream);
-                launches += 2;
                 for (int d = 3; d < 6; ++d) {
                     ObjDev ghostobj = Pv;
                     ghostobj.hash = ghosts[d].hash.p;
                     fd::launch_cell_table(ghostobj, sv[d - 3].cells, scan_tmp.p, scan_tmp.n, stream);
-                    launches += 2;
                 }
             }
             for (int d = 0; d < 6; ++d) {
@@ -1091,7 +1082,6 @@ struct fundem_sim {
                     FD_CUDA(cudaMemcpyAsync(recording->ns(kinds[d], record_step), Lg[d].n_slots, sizeof(int),
                                             cudaMemcpyDeviceToDevice, stream));
                 active[kinds[d]] = 1;
-                launches += 2;
             }
             tend(FUNDEM_T_GHOST);
         }
@@ -1104,16 +1094,15 @@ struct fundem_sim {
         for (int k = 0; k < FD_NKIND; ++k) views[k] = lists[k].view();
         fd::RevDev rv = rev_view();
         fd::launch_reverse(Pv, views, active, rv, scan_tmp.p, scan_tmp.n, stream);
-        launches += 6;
         fd::BondDev bd = bond_view();
         if (recording && bd.n > 0) {
             bd.rec_active = recording->bond_active.p + (long long)record_step * bd.n;
             bd.rec_rij = recording->bond_rij.p + 3ll * record_step * bd.n;
             bd.rec_dn = recording->bond_dn.p + 3ll * record_step * bd.n;
         }
-        if (bd.n > 0) { fd::launch_bonds(Pv, bd, mixed(), stream); launches++; }
+        if (bd.n > 0) fd::launch_bonds(Pv, bd, mixed(), stream);
         fd::launch_reduce(Pv, views, active, rv, bd, mixed(), stream);
-        launches++;
+
         tend(FUNDEM_T_REDUCE);
         FD_CUDA(cudaGetLastError());
     }
@@ -1206,14 +1195,13 @@ struct fundem_sim {
         fd::launch_drift(Pv, dt, stream);
         fd::launch_drift(Wv, dt, stream);
         tend(FUNDEM_T_INTEGRATE);
-        launches += 3;
     }
     void back(double3 g, double dt)
     {
         tbegin(FUNDEM_T_INTEGRATE);
         fd::launch_kick(P.view(), pgeo.view(), g, 0.5 * dt, stream);
         tend(FUNDEM_T_INTEGRATE);
-        launches++;
+
     }
 };
 
@@ -1226,6 +1214,11 @@ int guard(fundem_sim* s, const std::function<void()>& f)
         explicit EpochScope(unsigned long long* e) : prev(t_sim_epoch) { if (e) t_sim_epoch = e; }
         ~EpochScope() { t_sim_epoch = prev; }
     } scope(s ? &s->alloc_epoch : nullptr);
+    // kernels launched inside the call are counted for this simulation
+    struct CountScope {
+        explicit CountScope(long long* c) { fd::set_launch_counter(c); }
+        ~CountScope() { fd::set_launch_counter(nullptr); }
+    } counting(s ? &s->launches : nullptr);
     try {
         f();
         return FUNDEM_OK;

@@ -1184,6 +1184,11 @@ __device__ __forceinline__ bool node_filtered(const float4 p, const CullXf& x, c
 #ifndef FD_CONTACT_MIN_BLOCKS
 #define FD_CONTACT_MIN_BLOCKS 2
 #endif
+// the predicate pass of the contact kernels: latency-bound gathers, so as
+// many resident warps as fit without spilling
+#ifndef FD_PROBE_MIN_BLOCKS
+#define FD_PROBE_MIN_BLOCKS 4
+#endif
 
 // ---------------------------------------------------------------------------
 // narrow phase, stage 1: one warp per candidate pair.  The clusters of A's
@@ -1323,22 +1328,21 @@ __global__ void __launch_bounds__(NARROW_WARPS * 32, FD_SELECT_MIN_BLOCKS) k_sel
 // keeps node id -1.  Force and torques go to the slot; stage 3 sums them per
 // pair.
 // ---------------------------------------------------------------------------
-template <int KIND>
-__global__ void __launch_bounds__(TPB, FD_CONTACT_MIN_BLOCKS) k_contact(NarrowArgs n)
+template <int KIND, int PASS>
+__global__ void __launch_bounds__(TPB, PASS == 0 ? FD_PROBE_MIN_BLOCKS : FD_CONTACT_MIN_BLOCKS) k_contact(NarrowArgs n)
 {
-    __shared__ int s_hits;
-    if (threadIdx.x == 0) s_hits = 0;
-    __syncthreads();
     PairListDev& L = n.L;
-    const int nslots = min(*L.n_slots, L.cap_contacts);
+    // pass 0: every slot; pass 1: the slots pass 0 listed as contacts
+    const int nitems = PASS == 0 ? min(*L.n_slots, L.cap_contacts) : min(*L.n_hits, L.cap_contacts);
     const int lane = threadIdx.x & 31;
     const bool periodic = (KIND == FD_PP || KIND == FD_PW) && (n.a.periodic_x || n.a.periodic_y);
     const int stride = gridDim.x * blockDim.x;
     int hits = 0;
-    for (int s0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); s0 < nslots; s0 += stride) {
-        const int s = s0 + lane;
+    for (int s0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); s0 < nitems; s0 += stride) {
+        const int t = s0 + lane;
+        const int s = (PASS == 1 && t < nitems) ? L.c_hit[t] : t;
         bool hit = false;
-        if (s < nslots) {
+        if (t < nitems) {
             const int p = L.c_pair[s];
             const int k = L.c_k[s];
             const int A = L.pairA[p];
@@ -1361,7 +1365,7 @@ __global__ void __launch_bounds__(TPB, FD_CONTACT_MIN_BLOCKS) k_contact(NarrowAr
             double ov = 0., fx = 0., fy = 0., fz = 0., pv[8];
             hit = node_predicate<KIND>(gp, bcell, sg, cB, qB, GB, SB.sdf, rB2, n.a.probe, ov, fx, fy, fz, pv);
             int nid = -1;
-            if (hit) {
+            if (PASS == 1 && hit) {
                 double3 nrm = fd_gradient_q(fx, fy, fz, pv);
                 nrm = fd_rot(qB, nrm);
                 nrm = fd_normalize(nrm);
@@ -1487,17 +1491,26 @@ __global__ void __launch_bounds__(TPB, FD_CONTACT_MIN_BLOCKS) k_contact(NarrowAr
                     L.c_es[s] = 0.5 * lengthSq3(spring) * ks;
                 }
             }
-            L.c_node[s] = nid;
-            if (n.a.rec.hit && s < n.a.rec.cap) n.a.rec.hit[s] = hit ? 1 : 0;
+            if (PASS == 1) {
+                L.c_node[s] = nid;
+            } else {
+                if (!hit) L.c_node[s] = -1;
+                if (n.a.rec.hit && s < n.a.rec.cap) n.a.rec.hit[s] = hit ? 1 : 0;
+            }
         }
-        hits += __popc(__ballot_sync(0xffffffffu, hit));
+        if (PASS == 0) {
+            // contacts are listed for pass 1, one atomic per warp
+            const unsigned int m = __ballot_sync(0xffffffffu, hit);
+            if (m) {
+                int base = 0;
+                if (lane == 0) base = atomicAdd(L.n_hits, __popc(m));
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (hit) L.c_hit[base + __popc(m & ((1u << lane) - 1u))] = s;
+                hits += __popc(m);
+            }
+        }
     }
-    if (lane == 0 && hits) atomicAdd(&s_hits, hits);
-    __syncthreads();
-    if (threadIdx.x == 0 && s_hits) {
-        atomicAdd(L.n_hits, s_hits);
-        if (n.a.stats) atomicAdd(&n.a.stats[3], (unsigned long long)s_hits);
-    }
+    if (PASS == 0 && n.a.stats && lane == 0 && hits) atomicAdd(&n.a.stats[3], (unsigned long long)hits);
 }
 
 // ---------------------------------------------------------------------------
@@ -1616,23 +1629,22 @@ __device__ __forceinline__ v3f linear_contact32(double3& spring, v3f vc, v3f n, 
     return fn + (-ks * tof(spring) - cs * vs);
 }
 
-template <int KIND>
-__global__ void __launch_bounds__(TPB, FD_CONTACT_MIN_BLOCKS) k_contact32(NarrowArgs n)
+template <int KIND, int PASS>
+__global__ void __launch_bounds__(TPB, PASS == 0 ? FD_PROBE_MIN_BLOCKS : FD_CONTACT_MIN_BLOCKS) k_contact32(NarrowArgs n)
 {
-    __shared__ int s_hits;
-    if (threadIdx.x == 0) s_hits = 0;
-    __syncthreads();
     PairListDev& L = n.L;
     float* cf = reinterpret_cast<float*>(L.c_force);
-    const int nslots = min(*L.n_slots, L.cap_contacts);
+    // pass 0: every slot; pass 1: the slots pass 0 listed as contacts
+    const int nitems = PASS == 0 ? min(*L.n_slots, L.cap_contacts) : min(*L.n_hits, L.cap_contacts);
     const int lane = threadIdx.x & 31;
     const bool periodic = (KIND == FD_PP || KIND == FD_PW) && (n.a.periodic_x || n.a.periodic_y);
     const int stride = gridDim.x * blockDim.x;
     int hits = 0;
-    for (int s0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); s0 < nslots; s0 += stride) {
-        const int s = s0 + lane;
+    for (int s0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); s0 < nitems; s0 += stride) {
+        const int t = s0 + lane;
+        const int s = (PASS == 1 && t < nitems) ? L.c_hit[t] : t;
         bool hit = false;
-        if (s < nslots) {
+        if (t < nitems) {
             const int p = L.c_pair[s];
             const int k = L.c_k[s];
             const int A = L.pairA[p];
@@ -1698,7 +1710,7 @@ __global__ void __launch_bounds__(TPB, FD_CONTACT_MIN_BLOCKS) k_contact32(Narrow
                 }
             }
             int nid = -1;
-            if (hit) {
+            if (PASS == 1 && hit) {
                 // gradient with the x weight truncated as the reference does
                 // (LSParticleContactDetectionKernel.cuh:34)
                 const float wy0 = 1.f - fy, wy1 = fy, wz0 = 1.f - fz, wz1 = fz;
@@ -1814,17 +1826,26 @@ __global__ void __launch_bounds__(TPB, FD_CONTACT_MIN_BLOCKS) k_contact32(Narrow
                     L.c_es[s] = 0.5 * lengthSq3(spring) * (double)ks;
                 }
             }
-            L.c_node[s] = nid;
-            if (n.a.rec.hit && s < n.a.rec.cap) n.a.rec.hit[s] = hit ? 1 : 0;
+            if (PASS == 1) {
+                L.c_node[s] = nid;
+            } else {
+                if (!hit) L.c_node[s] = -1;
+                if (n.a.rec.hit && s < n.a.rec.cap) n.a.rec.hit[s] = hit ? 1 : 0;
+            }
         }
-        hits += __popc(__ballot_sync(0xffffffffu, hit));
+        if (PASS == 0) {
+            // contacts are listed for pass 1, one atomic per warp
+            const unsigned int m = __ballot_sync(0xffffffffu, hit);
+            if (m) {
+                int base = 0;
+                if (lane == 0) base = atomicAdd(L.n_hits, __popc(m));
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (hit) L.c_hit[base + __popc(m & ((1u << lane) - 1u))] = s;
+                hits += __popc(m);
+            }
+        }
     }
-    if (lane == 0 && hits) atomicAdd(&s_hits, hits);
-    __syncthreads();
-    if (threadIdx.x == 0 && s_hits) {
-        atomicAdd(L.n_hits, s_hits);
-        if (n.a.stats) atomicAdd(&n.a.stats[3], (unsigned long long)s_hits);
-    }
+    if (PASS == 0 && n.a.stats && lane == 0 && hits) atomicAdd(&n.a.stats[3], (unsigned long long)hits);
 }
 
 // stage 3 in single precision: eight lanes per pair, as k_pair_sum
@@ -2154,6 +2175,19 @@ __global__ void k_reduce(ReduceArgs r)
 
 }  // namespace
 
+// kernel launches are counted into the counter the calling thread set
+// (fundem_launch_count); none when it set none
+thread_local long long* t_launch_counter = nullptr;
+void set_launch_counter(long long* c) { t_launch_counter = c; }
+void count_launch()
+{
+    if (t_launch_counter) ++*t_launch_counter;
+}
+static inline void note_launch()
+{
+    if (t_launch_counter) ++*t_launch_counter;
+}
+
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
@@ -2172,52 +2206,52 @@ void scan_exclusive(const int* in, int* out, long long n, int* tmp, cudaStream_t
 {
     if (n <= 0) return;
     if (n <= SCAN_TILE) {
-        k_scan_tile<false><<<1, SCAN_TPB, 0, s>>>(in, out, n, nullptr);
+        k_scan_tile<false><<<1, SCAN_TPB, 0, s>>>(in, out, n, nullptr); note_launch();
         return;
     }
     const long long tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
     int* sums = tmp;
-    k_scan_tile<false><<<(unsigned)tiles, SCAN_TPB, 0, s>>>(in, out, n, sums);
+    k_scan_tile<false><<<(unsigned)tiles, SCAN_TPB, 0, s>>>(in, out, n, sums); note_launch();
     scan_exclusive(sums, sums, tiles, tmp + tiles, s);
-    k_scan_add<<<(unsigned)tiles, SCAN_TPB, 0, s>>>(out, n, sums);
+    k_scan_add<<<(unsigned)tiles, SCAN_TPB, 0, s>>>(out, n, sums); note_launch();
 }
 
 void scan_inclusive(const int* in, int* out, long long n, int* tmp, cudaStream_t s)
 {
     if (n <= 0) return;
     if (n <= SCAN_TILE) {
-        k_scan_tile<true><<<1, SCAN_TPB, 0, s>>>(in, out, n, nullptr);
+        k_scan_tile<true><<<1, SCAN_TPB, 0, s>>>(in, out, n, nullptr); note_launch();
         return;
     }
     const long long tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
     int* sums = tmp;
-    k_scan_tile<true><<<(unsigned)tiles, SCAN_TPB, 0, s>>>(in, out, n, sums);
+    k_scan_tile<true><<<(unsigned)tiles, SCAN_TPB, 0, s>>>(in, out, n, sums); note_launch();
     scan_exclusive(sums, sums, tiles, tmp + tiles, s);
-    k_scan_add<<<(unsigned)tiles, SCAN_TPB, 0, s>>>(out, n, sums);
+    k_scan_add<<<(unsigned)tiles, SCAN_TPB, 0, s>>>(out, n, sums); note_launch();
 }
 
 void launch_kick(const ObjDev& P, const GeoSetDev& G, double3 gravity, double h, cudaStream_t s)
 {
-    if (P.n > 0) k_kick<<<nblocks(P.n), TPB, 0, s>>>(P, G, gravity, h);
+    if (P.n > 0) { k_kick<<<nblocks(P.n), TPB, 0, s>>>(P, G, gravity, h); note_launch(); }
 }
 void launch_drift(const ObjDev& O, double dt, cudaStream_t s)
 {
-    if (O.n > 0) k_drift<<<nblocks(O.n), TPB, 0, s>>>(O, dt);
+    if (O.n > 0) { k_drift<<<nblocks(O.n), TPB, 0, s>>>(O, dt); note_launch(); }
 }
 void launch_hash_count(const ObjDev& O, CellTableDev& T, cudaStream_t s)
 {
     cudaMemsetAsync(T.count, 0, sizeof(int) * T.g.num, s);
-    if (O.n > 0) k_hash_count<<<nblocks(O.n), TPB, 0, s>>>(O, T.g, T.count);
+    if (O.n > 0) { k_hash_count<<<nblocks(O.n), TPB, 0, s>>>(O, T.g, T.count); note_launch(); }
 }
 void launch_cell_table(ObjDev& O, CellTableDev& T, int* scan_tmp, size_t, cudaStream_t s)
 {
     scan_exclusive(T.count, T.start, T.g.num, scan_tmp, s);
     cudaMemsetAsync(T.fill, 0, sizeof(int) * T.g.num, s);
-    if (O.n > 0) k_scatter<<<nblocks(O.n), TPB, 0, s>>>(O.hash, O.n, T.g.num, T.start, T.fill, T.sorted);
+    if (O.n > 0) { k_scatter<<<nblocks(O.n), TPB, 0, s>>>(O.hash, O.n, T.g.num, T.start, T.fill, T.sorted); note_launch(); }
 }
 void launch_wrap(ObjDev& P, const FdGrid& g, int dim, cudaStream_t s)
 {
-    if (P.n > 0) k_wrap<<<nblocks(P.n), TPB, 0, s>>>(P, g, dim);
+    if (P.n > 0) { k_wrap<<<nblocks(P.n), TPB, 0, s>>>(P, g, dim); note_launch(); }
 }
 void launch_ghost_build(const ObjDev& P, GhostDev& Gh, int kind, cudaStream_t s)
 {
@@ -2225,11 +2259,11 @@ void launch_ghost_build(const ObjDev& P, GhostDev& Gh, int kind, cudaStream_t s)
     // occupied-cell box of the ghost images: empty until the build fills it
     cudaMemsetAsync(Gh.occ, 0x7f, 3 * sizeof(int), s);
     cudaMemsetAsync(Gh.occ + 3, 0xff, 3 * sizeof(int), s);
-    if (P.n > 0) k_ghost_build<<<nblocks(P.n), TPB, 0, s>>>(P, Gh, kind);
+    if (P.n > 0) { k_ghost_build<<<nblocks(P.n), TPB, 0, s>>>(P, Gh, kind); note_launch(); }
 }
 void launch_sector_wrap(ObjDev& P, const FdGrid& g, cudaStream_t s)
 {
-    if (P.n > 0) k_sector_wrap<<<nblocks(P.n), TPB, 0, s>>>(P, g.minb);
+    if (P.n > 0) { k_sector_wrap<<<nblocks(P.n), TPB, 0, s>>>(P, g.minb); note_launch(); }
 }
 void launch_sector_images(const ObjDev& P, GhostDev* R, cudaStream_t s)
 {
@@ -2238,34 +2272,36 @@ void launch_sector_images(const ObjDev& P, GhostDev* R, cudaStream_t s)
         cudaMemsetAsync(R[d].occ, 0x7f, 3 * sizeof(int), s);
         cudaMemsetAsync(R[d].occ + 3, 0xff, 3 * sizeof(int), s);
     }
-    if (P.n > 0) k_sector_images<<<nblocks(P.n), TPB, 0, s>>>(P, R[0], R[1], R[2]);
+    if (P.n > 0) { k_sector_images<<<nblocks(P.n), TPB, 0, s>>>(P, R[0], R[1], R[2]); note_launch(); }
 }
 
 void launch_broad_pp(const ObjDev& P, const GeoSetDev& G, const CellTableDev& T, PairListDev& L,
                      unsigned int* flags, double probe, cudaStream_t s, double skin, const int* gate)
 {
     cudaMemsetAsync(L.n_pairs, 0, sizeof(int), s);
-    if (P.n > 0)
+    if (P.n > 0) {
         k_broad_cells<false, false, false><<<nblocks((long long)P.n * BROAD_LANES), TPB, 0, s>>>(
             P, G, T, nullptr, nullptr, nullptr, nullptr, nullptr, L, NlDev{}, flags, probe, skin, gate);
+        note_launch();
+    }
 }
 void launch_broad_pp_nl(const ObjDev& P, const GeoSetDev& G, const CellTableDev& T, PairListDev& L, NlDev& nl,
                         unsigned int* flags, double probe, cudaStream_t s, const int* gate)
 {
     cudaMemsetAsync(L.n_pairs, 0, sizeof(int), s);
     if (P.n <= 0) return;
-    k_nl_check<<<nblocks(P.n), TPB, 0, s>>>(P, nl, T.g, gate);
+    k_nl_check<<<nblocks(P.n), TPB, 0, s>>>(P, nl, T.g, gate); note_launch();
     k_broad_cells<false, false, true><<<nblocks((long long)P.n * BROAD_LANES), TPB, 0, s>>>(
-        P, G, T, nullptr, nullptr, nullptr, nullptr, nullptr, L, nl, flags, probe, 0.0, gate);
-    k_nl_filter<<<nblocks((long long)P.n * 8), TPB, 0, s>>>(P, G, L, nl, flags, probe, gate);
+        P, G, T, nullptr, nullptr, nullptr, nullptr, nullptr, L, nl, flags, probe, 0.0, gate); note_launch();
+    k_nl_filter<<<nblocks((long long)P.n * 8), TPB, 0, s>>>(P, G, L, nl, flags, probe, gate); note_launch();
 }
 void launch_pair_cache_check(const ObjDev& P, const PairCacheDev& c, cudaStream_t s)
 {
-    if (P.n > 0) k_pc_check<<<nblocks(P.n), TPB, 0, s>>>(P, c);
+    if (P.n > 0) { k_pc_check<<<nblocks(P.n), TPB, 0, s>>>(P, c); note_launch(); }
 }
 void launch_pair_cache_commit(const ObjDev& P, const PairCacheDev& c, const PairListDev& L, cudaStream_t s)
 {
-    if (P.n > 0) k_pc_commit<<<nblocks(P.n), TPB, 0, s>>>(P, c, L);
+    if (P.n > 0) { k_pc_commit<<<nblocks(P.n), TPB, 0, s>>>(P, c, L); note_launch(); }
     cudaMemsetAsync(c.ctrl, 0, sizeof(int), s);
 }
 
@@ -2273,7 +2309,7 @@ void launch_broad_pw(const ObjDev& P, const GeoSetDev& G, const ObjDev& W, const
                      const FdGrid& wg, PairListDev& L, unsigned int* flags, double probe, cudaStream_t s)
 {
     cudaMemsetAsync(L.n_pairs, 0, sizeof(int), s);
-    if (P.n > 0) k_broad_pw<<<nblocks(P.n), TPB, 0, s>>>(P, G, W, GW, wg, L, flags, probe);
+    if (P.n > 0) { k_broad_pw<<<nblocks(P.n), TPB, 0, s>>>(P, G, W, GW, wg, L, flags, probe); note_launch(); }
 }
 void launch_broad_ghost(const ObjDev& P, const GeoSetDev& G, const GhostDev& Gh, PairListDev& L,
                         unsigned int* flags, double probe, cudaStream_t s)
@@ -2281,10 +2317,10 @@ void launch_broad_ghost(const ObjDev& P, const GeoSetDev& G, const GhostDev& Gh,
     cudaMemsetAsync(L.n_pairs, 0, sizeof(int), s);
     if (P.n <= 0) return;
     cudaMemsetAsync(Gh.nsearch, 0, sizeof(int), s);
-    k_ghost_searchers<<<nblocks(P.n), TPB, 0, s>>>(P, G, Gh.cells.g, Gh.occ, L, Gh.searchers, Gh.nsearch);
+    k_ghost_searchers<<<nblocks(P.n), TPB, 0, s>>>(P, G, Gh.cells.g, Gh.occ, L, Gh.searchers, Gh.nsearch); note_launch();
     const long long groups = std::min<long long>(P.n, 148ll * 8 * (TPB / BROAD_LANES));
     k_broad_cells<true, true, false><<<nblocks(groups * BROAD_LANES), TPB, 0, s>>>(
-        P, G, Gh.cells, Gh.pos, Gh.rot, Gh.occ, Gh.searchers, Gh.nsearch, L, NlDev{}, flags, probe, 0.0, nullptr);
+        P, G, Gh.cells, Gh.pos, Gh.rot, Gh.occ, Gh.searchers, Gh.nsearch, L, NlDev{}, flags, probe, 0.0, nullptr); note_launch();
 }
 
 void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& M, const ObjDev& W,
@@ -2303,10 +2339,15 @@ void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& 
     const int cgrid = 148 * 4;
 #define FD_NARROW_CASE(K)                                                              \
     case K:                                                                            \
-        k_select<K><<<grid, NARROW_WARPS * 32, 0, s>>>(n);                             \
-        if (a.gate) k_pc_carry<<<148 * 8, TPB, 0, s>>>(L, P, pgrid, a.gate);          \
-        if (mixed) k_contact32<K><<<cgrid, TPB, 0, s>>>(n);                            \
-        else k_contact<K><<<cgrid, TPB, 0, s>>>(n);                                    \
+        k_select<K><<<grid, NARROW_WARPS * 32, 0, s>>>(n); note_launch();                             \
+        if (a.gate) { k_pc_carry<<<148 * 8, TPB, 0, s>>>(L, P, pgrid, a.gate); note_launch(); }          \
+        if (mixed) {                                                                   \
+            k_contact32<K, 0><<<cgrid, TPB, 0, s>>>(n); note_launch();                                \
+            k_contact32<K, 1><<<cgrid, TPB, 0, s>>>(n); note_launch();                                \
+        } else {                                                                       \
+            k_contact<K, 0><<<cgrid, TPB, 0, s>>>(n); note_launch();                                  \
+            k_contact<K, 1><<<cgrid, TPB, 0, s>>>(n); note_launch();                                  \
+        }                                                                              \
         break;
     switch (kind) {
         FD_NARROW_CASE(FD_PP)
@@ -2319,14 +2360,19 @@ void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& 
     case FD_GR270:
         // the sector images differ from the translated ones only in the state
         // the ghost traits read, so they share the ghost kernels
-        k_select<FD_GX><<<grid, NARROW_WARPS * 32, 0, s>>>(n);
-        if (mixed) k_contact32<FD_GX><<<cgrid, TPB, 0, s>>>(n);
-        else k_contact<FD_GX><<<cgrid, TPB, 0, s>>>(n);
+        k_select<FD_GX><<<grid, NARROW_WARPS * 32, 0, s>>>(n); note_launch();
+        if (mixed) {
+            k_contact32<FD_GX, 0><<<cgrid, TPB, 0, s>>>(n); note_launch();
+            k_contact32<FD_GX, 1><<<cgrid, TPB, 0, s>>>(n); note_launch();
+        } else {
+            k_contact<FD_GX, 0><<<cgrid, TPB, 0, s>>>(n); note_launch();
+            k_contact<FD_GX, 1><<<cgrid, TPB, 0, s>>>(n); note_launch();
+        }
         break;
     }
 #undef FD_NARROW_CASE
-    if (mixed) k_pair_sum32<<<148 * 4, TPB, 0, s>>>(L, with_force);
-    else k_pair_sum<<<148 * 4, TPB, 0, s>>>(L, with_force);
+    if (mixed) { k_pair_sum32<<<148 * 4, TPB, 0, s>>>(L, with_force); note_launch(); }
+    else k_pair_sum<<<148 * 4, TPB, 0, s>>>(L, with_force); note_launch();
 }
 
 void launch_reverse(const ObjDev& P, PairListDev* lists, const int* active, RevDev& R, int* scan_tmp, size_t,
@@ -2343,17 +2389,17 @@ void launch_reverse(const ObjDev& P, PairListDev* lists, const int* active, RevD
     cudaMemsetAsync(R.cnt, 0, sizeof(int) * P.n, s);
     cudaMemsetAsync(R.fill, 0, sizeof(int) * P.n, s);
     const int g = 148 * 8;
-    k_rev_count<<<g, TPB, 0, s>>>(r);
+    k_rev_count<<<g, TPB, 0, s>>>(r); note_launch();
     scan_exclusive(R.cnt, R.off, P.n, scan_tmp, s);
-    k_rev_fill<<<g, TPB, 0, s>>>(r);
-    k_rev_sort<<<nblocks(P.n), TPB, 0, s>>>(r);
+    k_rev_fill<<<g, TPB, 0, s>>>(r); note_launch();
+    k_rev_sort<<<nblocks(P.n), TPB, 0, s>>>(r); note_launch();
 }
 
 void launch_bonds(const ObjDev& P, BondDev& B, bool mixed, cudaStream_t s)
 {
     if (B.n <= 0) return;
-    if (mixed) k_bonds32<<<nblocks(B.n), TPB, 0, s>>>(P, B);
-    else k_bonds<<<nblocks(B.n), TPB, 0, s>>>(P, B);
+    if (mixed) { k_bonds32<<<nblocks(B.n), TPB, 0, s>>>(P, B); note_launch(); }
+    else k_bonds<<<nblocks(B.n), TPB, 0, s>>>(P, B); note_launch();
 }
 
 void launch_reduce(ObjDev& P, PairListDev* lists, const int* active, const RevDev& R, const BondDev& B, bool mixed,
@@ -2365,8 +2411,8 @@ void launch_reduce(ObjDev& P, PairListDev* lists, const int* active, const RevDe
     for (int k = 0; k < FD_NKIND; ++k) { r.L[k] = lists[k]; r.active[k] = active[k]; }
     r.R = R;
     r.B = B;
-    if (mixed) k_reduce<float><<<nblocks(P.n), TPB, 0, s>>>(r);
-    else k_reduce<double><<<nblocks(P.n), TPB, 0, s>>>(r);
+    if (mixed) { k_reduce<float><<<nblocks(P.n), TPB, 0, s>>>(r); note_launch(); }
+    else k_reduce<double><<<nblocks(P.n), TPB, 0, s>>>(r); note_launch();
 }
 
 }  // namespace fd

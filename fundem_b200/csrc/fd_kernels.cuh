@@ -31,6 +31,8 @@ struct PairListDev {
     int* c_node;
     int* c_slave;
     int* c_pair;       // pair of each slot
+    int* c_hit;        // slots holding a contact, listed by the predicate pass
+                       // for the contact-law pass (n_hits of them)
     int* c_k;          // node key of each slot: cluster-order index relative to
                        // the geometry (ascending within a pair)
     double* c_force;   // 9 per slot: F, torque on A, torque on B (contacts only)
@@ -262,6 +264,13 @@ void launch_reverse(const ObjDev& P, PairListDev* lists, const int* active, RevD
 void launch_bonds(const ObjDev& P, BondDev& B, bool mixed, cudaStream_t s);
 void launch_reduce(ObjDev& P, PairListDev* lists, const int* active, const RevDev& R, const BondDev& B, bool mixed,
                    cudaStream_t s);
+
+// Kernel launches of the calling thread are counted into *c (null: not
+// counted); the library points it at the calling simulation's counter for
+// the duration of each call.  count_launch() counts one launch made
+// elsewhere (the adjoint kernels).
+void set_launch_counter(long long* c);
+void count_launch();
 
 // exclusive scan of n ints (out may alias in); returns needed tmp ints when tmp == nullptr
 size_t scan_tmp_size(long long n);
