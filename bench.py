@@ -613,47 +613,80 @@ def adjoint_cost(args, dev):
 def batched_cost(args, dev):
     """The calibration sweep: args.batch_sims independent pours of uneven size
     (log-uniform in [500, 20000] particles, per-simulation kn, friction and
-    damping), args.batch_steps steps each, stepped concurrently (one stream per
-    simulation, CUDA-graph chunks of the autotuned length) and one at a time."""
+    damping), args.batch_steps steps each, run tiled into one simulation (one
+    launch per stage of the timestep over all simulations, per-simulation
+    material blocks and wall groups) and one at a time; then the adjoint of a
+    tiled subset against its forward run."""
+    import torch
+    import fundem_b200 as F
     from fundem_b200 import batch
     t0 = time.perf_counter()
     scs, params = batch.calibration_scenarios(n_sims=args.batch_sims, seed=1)
     t_build = time.perf_counter() - t0
-    probe = batch.Batch(scs[: min(32, len(scs))], device=dev)
-    chunk, tune = batch.autotune_chunk(probe, candidates=(25, 50, 100, 200), probe_steps=200)
-    probe.close()
     t0 = time.perf_counter()
-    conc = batch.Batch(scs, device=dev)
+    tb = batch.TiledBatch(scs, device=dev)
     t_setup = time.perf_counter() - t0
-    particles = conc.particles
-    conc.sync()
-    # the first chunk records every simulation's graph: set-up, timed apart
-    t0 = time.perf_counter()
-    conc.run_graphs(chunk, chunk)
-    t_record = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    conc.run_graphs(args.batch_steps, chunk)
-    t_conc = time.perf_counter() - t0
-    conc.close()
+    particles = tb.particles
+    tb.run(args.batch_warmup)  # untimed: list growth and the first cache builds
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    tb.sim.step(args.batch_steps)
+    e1.record()
+    torch.cuda.synchronize()
+    tb.sync()
+    t_tiled = e0.elapsed_time(e1) / 1e3
+    launches = tb.sim.launch_count()
+    tb.close()
     seq = batch.Batch(scs, device=dev)
     seq.sync()
-    seq.run_sequential(chunk)  # the same warm-up steps, untimed
+    seq.run_sequential(args.batch_warmup)  # the same warm-up steps, untimed
     t0 = time.perf_counter()
     seq.run_sequential(args.batch_steps)
     t_seq = time.perf_counter() - t0
     seq.close()
     ps = particles * args.batch_steps
-    return {"workload": "calibration sweep: pours of 500-20,000 particles (log-uniform), kn, friction and damping "
-                        "per simulation, the small pour's shapes, fill ratio 0.4, dt 1e-6 s",
-            "simulations": len(scs), "particles": particles, "steps": args.batch_steps,
-            "chunk": chunk, "autotune_s": {str(k): round(v, 4) for k, v in tune.items()},
-            "concurrent_s": t_conc, "sequential_s": t_seq, "speedup": t_seq / t_conc,
-            "concurrent_particle_steps_per_s": ps / t_conc, "sequential_particle_steps_per_s": ps / t_seq,
-            "scenario_build_s": round(t_build, 1), "setup_s": round(t_setup, 1),
-            "graph_record_s": round(t_record, 3),
-            "note": "one stream per simulation with CUDA-graph chunks (not a single persistent kernel); "
-                    "wall-clock times around synchronised runs; both runs start after the same warm-up "
-                    "chunk, which for the concurrent run records the graphs (graph_record_s)"}
+    out = {"workload": "calibration sweep: pours of 500-20,000 particles (log-uniform), kn, friction and damping "
+                       "per simulation, the small pour's shapes, fill ratio 0.4, dt 1e-6 s",
+           "simulations": len(scs), "particles": particles, "steps": args.batch_steps,
+           "warmup_steps": args.batch_warmup,
+           "tiled_s": t_tiled, "sequential_s": t_seq, "speedup": t_seq / t_tiled,
+           "tiled_particle_steps_per_s": ps / t_tiled, "sequential_particle_steps_per_s": ps / t_seq,
+           "scenario_build_s": round(t_build, 1), "tiled_setup_s": round(t_setup, 1),
+           "note": "tiled: every simulation in its own region of one Simulation, one launch per stage for all "
+                   "(CUDA events); sequential: the same simulations stepped one after another with plain launches "
+                   "(wall clock around synchronised runs)"}
+    # the adjoint of a tiled subset: per-simulation parameter gradients from one backward sweep
+    try:
+        sub = scs[: args.batch_adjoint_sims]
+        steps, K = args.batch_adjoint_steps, max(args.batch_adjoint_steps // 4, 1)
+        t2 = batch.TiledBatch(sub, device=dev)
+        n = t2.particles
+        t2.sim.sync()
+        t0 = time.perf_counter()
+        t2.sim.step(steps)
+        t2.sim.sync()
+        t_fwd = time.perf_counter() - t0
+        t2.close()
+        t2 = batch.TiledBatch(sub, device=dev)
+        t2.sim.adjoint_begin(K)
+        t0 = time.perf_counter()
+        t2.sim.adjoint_forward(steps)
+        t_rec = time.perf_counter() - t0
+        dl_dx = np.zeros((n, 3))
+        dl_dx[:, 2] = 1.0 / n            # loss: mean particle height of every simulation together
+        t0 = time.perf_counter()
+        gv0, gp = t2.sim.adjoint_backward(dl_dx, np.zeros((n, 3)))
+        t_bwd = time.perf_counter() - t0
+        t2.sim.adjoint_end()
+        t2.close()
+        out["adjoint"] = {"simulations": len(sub), "particles": n, "steps": steps, "checkpoint_interval": K,
+                          "forward_s": t_fwd, "recorded_forward_s": t_rec, "backward_s": t_bwd,
+                          "total_over_forward": (t_rec + t_bwd) / t_fwd,
+                          "dl_dkn_first_sims": [float(g[0]) for g in gp[:4]]}
+    except Exception as exc:  # an auxiliary figure: report, do not fail the run
+        out["adjoint"] = {"error": f"{type(exc).__name__}: {exc}"}
+    return out
 
 
 def main():
@@ -685,6 +718,9 @@ def main():
     ap.add_argument("--pair-skin", type=float, default=0.0, help="pair-cache skin in metres (0: default)")
     ap.add_argument("--batch-sims", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=200)
+    ap.add_argument("--batch-warmup", type=int, default=50)
+    ap.add_argument("--batch-adjoint-sims", type=int, default=32)
+    ap.add_argument("--batch-adjoint-steps", type=int, default=200)
     ap.add_argument("--error-steps", type=int, default=1000,
                     help="steps before the mixed-precision position error is measured")
     args = ap.parse_args()

@@ -35,7 +35,7 @@ EXPORTS = [
     "fundem_adjoint_begin", "fundem_adjoint_forward", "fundem_adjoint_backward", "fundem_adjoint_end",
     "fundem_step_graph", "fundem_set_neighbour_list", "fundem_checkpoint_write", "fundem_checkpoint_read",
     "fundem_levelset_grid", "fundem_set_periodic_sector", "fundem_set_inertia_mode",
-    "fundem_set_pair_cache", "fundem_pair_cache_stats",
+    "fundem_set_pair_cache", "fundem_pair_cache_stats", "fundem_set_wall_groups", "fundem_hash_sort",
 ]
 TIMERS = {"integrate": 0, "hash": 1, "broad": 2, "narrow_pp": 3, "narrow_pw": 4, "ghost": 5, "reduce": 6}
 
@@ -128,6 +128,8 @@ def lib():
         L.fundem_set_periodic_sector.argtypes = [P, I]
         L.fundem_set_inertia_mode.argtypes = [P, I]
         L.fundem_set_pair_cache.argtypes = [P, I, C.c_double]
+        L.fundem_set_wall_groups.argtypes = [P, I, IP, IP]
+        L.fundem_hash_sort.argtypes = [P, I, LL, P, P, P]
         L.fundem_pair_cache_stats.argtypes = [P, C.POINTER(LL), C.POINTER(LL), C.POINTER(C.c_double)]
         _lib = L
     return _lib
@@ -203,6 +205,13 @@ def levelset_grid(kind, param, origin, spacing, size, positive_inside=False, ver
     _check(lib().fundem_levelset_grid(int(device), stream, C.byref(sh), _d(_f64(origin, 3)), float(spacing), _i(n),
                                       _d(out)), "levelset_grid")
     return out
+
+
+def hash_sort(d_hash_ptr, n, num_cells, d_sorted_ptr, d_sorted_hash_ptr=None, stream=None):
+    """fundem_hash_sort on device pointers (ints): stable order of 64-bit cell
+    hashes, those outside [0, num_cells) last."""
+    _check(lib().fundem_hash_sort(C.c_void_p(d_hash_ptr), int(n), int(num_cells), C.c_void_p(d_sorted_ptr),
+                                  C.c_void_p(d_sorted_hash_ptr) if d_sorted_hash_ptr else None, stream), "hash_sort")
 
 
 def prefix_sum(count, out=None, stream=None):
@@ -393,6 +402,12 @@ class Simulation:
         """Pair cache of the particle-particle list: mode -1 (default, from
         8192 particles), 0 off, 1 on; skin <= 0 takes the default skin."""
         self._check(self.L.fundem_set_pair_cache(self.h, int(mode), float(skin)), "set_pair_cache")
+
+    def set_wall_groups(self, first, count):
+        """Per particle, the first wall and the wall count it may meet (a
+        batch of simulations tiled into one); empty arrays remove them."""
+        first, count = _i32(first), _i32(count)
+        self._check(self.L.fundem_set_wall_groups(self.h, int(first.size), _i(first), _i(count)), "set_wall_groups")
 
     def pair_cache_stats(self):
         """(rebuilds, steps run with the cache, skin in metres)."""

@@ -1,10 +1,15 @@
 """Batched calibration: many independent simulations of uneven size on one GPU.
 
-Each simulation has its own CUDA stream and steps in chunks recorded once
-into a CUDA graph (fundem_step_graph), so the launch-bound steps of small
-simulations overlap on the device instead of queueing behind one another.
-The chunk length comes from `autotune_chunk`, which times candidate lengths
-on the batch itself.
+`TiledBatch` places every simulation in its own region of space inside one
+Simulation (`tile`): each stage of the timestep is then one launch over all
+simulations' particles, with the per-simulation parameters as a block of
+materials (simulation i uses material i) and per-particle wall groups (each
+particle meets only its own simulation's walls).  The adjoint of the tiled
+run gives every simulation's parameter gradients at once.
+
+`Batch` is the alternative with one CUDA stream per simulation, stepping in
+chunks recorded once into a CUDA graph (fundem_step_graph); the chunk length
+comes from `autotune_chunk`, which times candidate lengths on the batch.
 
 `calibration_scenarios` builds the calibration sweep: pours with particle
 counts log-uniform in [500, 20000], per-simulation kn log-uniform in
@@ -64,6 +69,117 @@ def calibration_scenarios(n_sims=256, seed=1, n_min=500, n_max=20000, fill=0.4, 
         params.append(dict(n=n, kn=float(kn[i]), mu=float(mu[i]), damping_ratio=float(zeta[i]),
                            fill=float(n * vp / np.prod(hi))))
     return scenarios, params
+
+
+def tile(scenarios, gap=5e-3):
+    """One scenario holding every simulation of `scenarios`, each in its own
+    region of space, so that one launch per stage of the timestep serves all
+    of them.  Simulation i keeps its particles, walls and materials (its
+    particle and wall materials become material i of the tiled scenario: the
+    per-simulation parameter block), moved by an offset on a square layout in
+    x and y whose pitch exceeds any simulation's box plus its walls' extent,
+    so that no particle of one simulation comes within reach of another's
+    particles or walls.  The shape templates, gravity and time step must be
+    shared.  Returns (scenario, layout) with layout holding per simulation
+    the particle range, the wall range and the offset."""
+    n = len(scenarios)
+    if n == 0:
+        raise ValueError("no simulations to tile")
+    s0 = scenarios[0]
+    for sc in scenarios:
+        if sc.particle_geometries is not s0.particle_geometries and len(sc.particle_geometries) != len(
+                s0.particle_geometries):
+            raise ValueError("tiled simulations share their shape templates")
+        if not (np.array_equal(sc.gravity, s0.gravity) and sc.dt == s0.dt):
+            raise ValueError("tiled simulations share gravity and time step")
+        if sc.periodic_x or sc.periodic_y or getattr(sc, "periodic_sector", False) or len(sc.bonds):
+            raise ValueError("tiling takes non-periodic simulations without bonds")
+        if len(sc.particle_materials) != 1 or len(sc.wall_materials) != 1:
+            raise ValueError("each tiled simulation has one particle and one wall material")
+    # reach of a simulation around its own domain: its walls' SDF boxes
+    reach = []
+    for sc in scenarios:
+        ext = max([float(np.max(g.size - 1) * g.spacing) for g in sc.wall_geometries], default=0.0)
+        reach.append(0.5 * ext)
+    span = np.array([sc.domain_max - sc.domain_min for sc in scenarios])
+    pitch = float(np.max(span[:, :2].max(axis=1) + 2.0 * np.array(reach))) + gap
+    ncol = int(np.ceil(np.sqrt(n)))
+    offsets = np.zeros((n, 3))
+    for i, sc in enumerate(scenarios):
+        offsets[i] = [(i % ncol) * pitch, (i // ncol) * pitch, 0.0] - sc.domain_min
+    pos, vel, angvel, quat, mat, geo = [], [], [], [], [], []
+    wpos, wvel, wangvel, wquat, wmat, wgeo = [], [], [], [], [], []
+    wall_geos, pmat, wmatl, motion = [], [], [], []
+    prange, wrange = [], []
+    np_, nw_ = 0, 0
+    for i, sc in enumerate(scenarios):
+        P, W = sc.particles, sc.walls
+        pos.append(P.pos + offsets[i]); vel.append(P.vel); angvel.append(P.angvel); quat.append(P.quat)
+        mat.append(np.full(len(P), i, np.int32)); geo.append(np.asarray(P.geo, np.int32))
+        wpos.append(W.pos + offsets[i]); wvel.append(W.vel); wangvel.append(W.angvel); wquat.append(W.quat)
+        wmat.append(np.full(len(W), i, np.int32)); wgeo.append(np.asarray(W.geo, np.int32) + len(wall_geos))
+        for (idx, v, w) in sc.wall_motion:
+            motion.append((nw_ + idx, v, w))
+        wall_geos.extend(sc.wall_geometries)
+        pmat.append(sc.particle_materials[0]); wmatl.append(sc.wall_materials[0])
+        prange.append((np_, len(P))); wrange.append((nw_, len(W)))
+        np_ += len(P); nw_ += len(W)
+    lo = np.min([sc.domain_min + offsets[i] for i, sc in enumerate(scenarios)], axis=0)
+    hi = np.max([sc.domain_max + offsets[i] for i, sc in enumerate(scenarios)], axis=0)
+    cat = np.concatenate
+    tiled = S.Scenario(domain_min=lo, domain_max=hi, gravity=s0.gravity, dt=s0.dt, particle_materials=pmat,
+                       wall_materials=wmatl, particle_geometries=s0.particle_geometries, wall_geometries=wall_geos,
+                       particles=S.Objects(cat(pos), cat(vel), cat(angvel), cat(quat), cat(mat), cat(geo)),
+                       walls=S.Objects(cat(wpos), cat(wvel), cat(wangvel), cat(wquat), cat(wmat), cat(wgeo)),
+                       wall_motion=motion, name=f"tiled_{n}")
+    layout = {"particles": prange, "walls": wrange, "offsets": offsets, "pitch": pitch, "columns": ncol}
+    return tiled, layout
+
+
+class TiledBatch:
+    """Independent simulations tiled into one Simulation (see `tile`): every
+    kernel of a step runs once for all of them, over the per-simulation
+    material blocks and the per-particle wall groups."""
+
+    def __init__(self, scenarios, device=0, precision=0, gap=5e-3):
+        self.scenario, self.layout = tile(scenarios, gap=gap)
+        self.sim = Simulation.from_scenario(self.scenario, device=device, precision=precision, records=False,
+                                            setup=False)
+        first = np.concatenate([np.full(n, w0, np.int32) for (_, n), (w0, _) in
+                                zip(self.layout["particles"], self.layout["walls"])])
+        count = np.concatenate([np.full(n, nw, np.int32) for (_, n), (_, nw) in
+                                zip(self.layout["particles"], self.layout["walls"])])
+        self.sim.set_wall_groups(first, count)
+        self.sim.setup(self.scenario.domain_min, self.scenario.domain_max)
+        self.sim.detect()
+        self.particles = len(self.scenario.particles)
+
+    def run(self, steps, graph_chunk=0):
+        if graph_chunk:
+            done = 0
+            while done < steps:
+                k = min(graph_chunk, steps - done)
+                self.sim.step_graph(k)
+                done += k
+        else:
+            self.sim.step(steps)
+        self.sim.sync()
+
+    def states(self):
+        """Per simulation, its state in its own coordinates."""
+        st = self.sim.state()
+        out = []
+        for i, (p0, n) in enumerate(self.layout["particles"]):
+            d = {k: v[p0:p0 + n].copy() for k, v in st.items()}
+            d["pos"] -= self.layout["offsets"][i]
+            out.append(d)
+        return out
+
+    def sync(self):
+        self.sim.sync()
+
+    def close(self):
+        self.sim.close()
 
 
 class Batch:

@@ -552,16 +552,60 @@ struct PairList {
     }
 };
 
+// a grid with more cells than this (and than 4 per object) keeps a hash table
+// of its occupied cells instead of a dense one
+constexpr long long DENSE_CELLS = 1ll << 22;
+
 struct CellTable {
     FdGrid g{};
-    DevArray<int> count, start, fill, sorted;
+    bool hashed = false;
+    DevArray<int> count, start, fill, sorted, idx_b, bcount, bscan;
+    DevArray<unsigned long long> skey, key_b, hkey;
+    DevArray<int2> hval;
+    unsigned long long hmask = 0;
+    int cap = 0;
     void alloc(const FdGrid& grid, int nobj)
     {
         g = grid;
-        count.alloc((size_t)g.num); start.alloc((size_t)g.num); fill.alloc((size_t)g.num);
-        sorted.alloc(std::max(nobj, 1));
+        const size_t m = (size_t)std::max(nobj, 1);
+        hashed = g.num > std::max<long long>(4ll * (long long)m, DENSE_CELLS);
+        if (hashed) {
+            size_t H = 1024;
+            while (H < 2 * m) H <<= 1;
+            hkey.alloc(H, false);
+            hval.alloc(H, false);
+            hmask = H - 1;
+            count.release();
+            start.release();
+            fill.release();
+        } else {
+            count.alloc((size_t)std::max<long long>(g.num, 1));
+            start.alloc((size_t)std::max<long long>(g.num, 1), false);
+            fill.alloc((size_t)std::max<long long>(g.num, 1), false);
+            hkey.release();
+            hval.release();
+            hmask = 0;
+        }
+        sorted.alloc(m);
+        skey.alloc(m, false);
+        key_b.alloc(m, false);
+        idx_b.alloc(m, false);
+        size_t bc = 0, bs = 0;
+        fd::radix_sort_scratch((int)m, bc, bs);
+        bcount.alloc(bc, false);
+        bscan.alloc(bs, false);
+        cap = (int)m;
     }
-    CellTableDev view() { return CellTableDev{g, count.p, start.p, fill.p, sorted.p}; }
+    CellTableDev view()
+    {
+        CellTableDev v{};
+        v.g = g;
+        v.hashed = hashed ? 1 : 0;
+        v.count = count.p; v.start = start.p; v.fill = fill.p; v.hkey = hkey.p; v.hval = hval.p; v.hmask = hmask;
+        v.sorted = sorted.p; v.skey = skey.p; v.key_b = key_b.p; v.idx_b = idx_b.p;
+        v.bcount = bcount.p; v.bscan_tmp = bscan.p; v.nobj_cap = cap;
+        return v;
+    }
 };
 
 struct Ghost {
@@ -679,7 +723,6 @@ struct fundem_sim {
     PairList lists[FD_NKIND];
     Ghost ghosts[6];  // X, Y, XY, then the sector images R90, R180, R270
     DevArray<int> scan_tmp;
-    DevArray<int> wcount;  // wall-grid histogram (walls are looped over directly)
     DevArray<unsigned int> flags;
     DevArray<unsigned long long> stats;  // narrow-phase work counters (profiling only)
     std::vector<int> node_base;
@@ -706,6 +749,9 @@ struct fundem_sim {
     {
         return fd::NlDev{nl_ref.p, nl_vis.p, nl_cnt.p, nl_list.p, nl_ctrl.p, NL_SKIN * pgeo.rmax, perX, perY, 0.0};
     }
+    // per particle: first wall and wall count it may meet (fundem_set_wall_groups)
+    std::vector<int2> wall_groups;
+    DevArray<int2> d_wall_groups;
     // pair cache of the particle-particle list (fundem_set_pair_cache): the
     // pairs and contact slots of a rebuild step are kept while no particle
     // drifts more than half the skin; each step still runs the exact
@@ -940,7 +986,12 @@ struct fundem_sim {
         ptab.alloc(pgrid, P.n());
         configure_nl();
         configure_pc();
-        wcount.alloc((size_t)std::max<long long>(wgrid.num, 1));
+        if (!wall_groups.empty()) {
+            if ((int)wall_groups.size() != P.n())
+                throw std::invalid_argument("wall groups: one entry per particle is needed");
+            d_wall_groups.alloc(wall_groups.size(), false);
+            d_wall_groups.upload(wall_groups, stream);
+        }
         const int np = P.n();
         const int nw = W.n();
         // capacities (grown after the first detection)
@@ -983,30 +1034,28 @@ struct fundem_sim {
         fd::MatDev M = pmat.view(), MW = wmat.view();
         fd::StepArgs a = step_args(dt, probe);
         CellTableDev T = ptab.view();
-        tbegin(FUNDEM_T_HASH);
-        fd::launch_hash_count(Pv, T, stream);
-        fd::launch_cell_table(Pv, T, scan_tmp.p, scan_tmp.n, stream);
-        // wall hash (visibility and cell for the node test)
-        if (W.n_dev > 0) {
-            CellTableDev wt{wgrid, wcount.p, nullptr, nullptr, nullptr};
-            fd::launch_hash_count(Wv, wt, stream);
-        }
-        tend(FUNDEM_T_HASH);
-        int active[FD_NKIND] = {1, 1, 0, 0, 0};
-        if (new_generation)
-            for (int k = 0; k < FD_NKIND; ++k) lists[k].cur ^= 1;
-        PairListDev Lpp = lists[FD_PP].view();
         // pair cache: steps only (a detection outside a step lists the exact
         // pairs and slots, and the next cached step rebuilds)
         const bool pc = with_force && probe == 0.0 && pc_active();
         fd::PairCacheDev pcv{};
+        if (pc) pcv = pc_view();
+        tbegin(FUNDEM_T_HASH);
+        fd::launch_hash(Pv, pgrid, stream);
         if (pc) {
-            pcv = pc_view();
             fd::launch_pair_cache_check(Pv, pcv, stream);
             pc_steps += 1;
         } else if (pc_on) {
             pc_force = true;
         }
+        // with the cache, the particle table serves only rebuild steps
+        fd::launch_cell_table(Pv, T, scan_tmp.p, scan_tmp.n, stream, pc ? pcv.ctrl : nullptr);
+        // wall hash (visibility and cell for the node test)
+        if (W.n_dev > 0) fd::launch_hash(Wv, wgrid, stream);
+        tend(FUNDEM_T_HASH);
+        int active[FD_NKIND] = {1, 1, 0, 0, 0};
+        if (new_generation)
+            for (int k = 0; k < FD_NKIND; ++k) lists[k].cur ^= 1;
+        PairListDev Lpp = lists[FD_PP].view();
         tbegin(FUNDEM_T_BROAD);
         if (use_nl) {
             fd::NlDev nl = nl_view();
@@ -1035,7 +1084,8 @@ struct fundem_sim {
         tend(FUNDEM_T_NARROW_PP);
         PairListDev Lpw = lists[FD_PW].view();
         tbegin(FUNDEM_T_BROAD);
-        fd::launch_broad_pw(Pv, G, Wv, GW, wgrid, Lpw, flags.p, probe, stream);
+        fd::launch_broad_pw(Pv, G, Wv, GW, wgrid, Lpw, flags.p, probe, stream,
+                            wall_groups.empty() ? nullptr : d_wall_groups.p);
         tend(FUNDEM_T_BROAD);
         tbegin(FUNDEM_T_NARROW_PW);
         a.rec = recording ? recording->rec(FD_PW, record_step) : fd::AdjRec{};
@@ -1345,6 +1395,30 @@ int fundem_pair_cache_stats(fundem_sim* s, long long* rebuilds, long long* steps
         if (rebuilds) *rebuilds = c[1];
         if (steps) *steps = s->pc_on ? s->pc_steps : 0;
         if (skin) *skin = s->pc_on ? s->pc_skin() : 0.0;
+    });
+}
+
+int fundem_set_wall_groups(fundem_sim* s, int n, const int* first, const int* count)
+{
+    if (!s || n < 0 || (n > 0 && (!first || !count))) return FUNDEM_ERR_ARG;
+    if (n > 0 && n != s->P.n()) {
+        s->last_error = "wall groups: one entry per particle is needed";
+        return FUNDEM_ERR_ARG;
+    }
+    const int nw = s->W.n();
+    for (int i = 0; i < n; ++i)
+        if (first[i] < 0 || count[i] < 0 || first[i] + count[i] > nw) {
+            s->last_error = "wall groups: a range reaches past the walls";
+            return FUNDEM_ERR_ARG;
+        }
+    return guard(s, [&] {
+        s->wall_groups.resize(n);
+        for (int i = 0; i < n; ++i) s->wall_groups[i] = make_int2(first[i], count[i]);
+        if (s->setup_done && n > 0) {
+            s->d_wall_groups.alloc(n, false);
+            s->d_wall_groups.upload(s->wall_groups, s->stream);
+        }
+        s->drop_graph();
     });
 }
 
@@ -2090,6 +2164,32 @@ int fundem_prefix_sum(int* d_prefix, const int* d_count, long long n, void* stre
     int* tmp = nullptr;
     if (cudaMallocAsync((void**)&tmp, ntmp * sizeof(int), s) != cudaSuccess) return FUNDEM_ERR_CUDA;
     fd::scan_inclusive(d_count, d_prefix, n, tmp, s);
+    cudaError_t e = cudaGetLastError();
+    cudaFreeAsync(tmp, s);
+    return e == cudaSuccess ? FUNDEM_OK : FUNDEM_ERR_CUDA;
+}
+
+int fundem_hash_sort(const long long* d_hash, int n, long long num_cells, int* d_sorted, long long* d_sorted_hash,
+                     void* stream)
+{
+    if (n < 0 || num_cells < 0 || (n > 0 && (!d_hash || !d_sorted))) return FUNDEM_ERR_ARG;
+    if (n == 0) return FUNDEM_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    size_t bc = 0, bs = 0;
+    fd::radix_sort_scratch(n, bc, bs);
+    // one block of scratch: sorted keys, second key buffer, second index
+    // buffer, block counts and their scan temporary
+    const size_t bytes = sizeof(unsigned long long) * 2 * (size_t)n + sizeof(int) * ((size_t)n + bc + bs) + 256;
+    char* tmp = nullptr;
+    if (cudaMallocAsync((void**)&tmp, bytes, s) != cudaSuccess) return FUNDEM_ERR_CUDA;
+    unsigned long long* okey = reinterpret_cast<unsigned long long*>(tmp);
+    unsigned long long* key_b = okey + n;
+    int* idx_b = reinterpret_cast<int*>(key_b + n);
+    int* bcount = idx_b + n;
+    int* bscan = bcount + bc;
+    fd::radix_sort_keys(d_hash, n, num_cells, okey, d_sorted, key_b, idx_b, bcount, bscan, s);
+    if (d_sorted_hash)
+        cudaMemcpyAsync(d_sorted_hash, okey, sizeof(long long) * (size_t)n, cudaMemcpyDeviceToDevice, s);
     cudaError_t e = cudaGetLastError();
     cudaFreeAsync(tmp, s);
     return e == cudaSuccess ? FUNDEM_OK : FUNDEM_ERR_CUDA;

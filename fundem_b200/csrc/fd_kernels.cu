@@ -21,6 +21,7 @@
 #include "fd_kernels.cuh"
 #include "../../include/fundem_b200.h"
 
+#include <algorithm>
 #include <cstdio>
 #include <mutex>
 
@@ -79,8 +80,9 @@ __device__ __forceinline__ int block_excl_scan(int v, int* total)
 }
 
 template <bool INCLUSIVE>
-__global__ void k_scan_tile(const int* in, int* out, long long n, int* tile_sums)
+__global__ void k_scan_tile(const int* in, int* out, long long n, int* tile_sums, const int* gate)
 {
+    if (gate && *gate == 0) return;
     const long long base = (long long)blockIdx.x * SCAN_TILE + (long long)threadIdx.x * SCAN_ITEMS;
     int v[SCAN_ITEMS];
     int s = 0;
@@ -102,8 +104,9 @@ __global__ void k_scan_tile(const int* in, int* out, long long n, int* tile_sums
     if (tile_sums && threadIdx.x == 0) tile_sums[blockIdx.x] = total;
 }
 
-__global__ void k_scan_add(int* out, long long n, const int* tile_off)
+__global__ void k_scan_add(int* out, long long n, const int* tile_off, const int* gate)
 {
+    if (gate && *gate == 0) return;
     const long long i = (long long)blockIdx.x * SCAN_TILE + threadIdx.x;
     const int add = tile_off[blockIdx.x];
 #pragma unroll
@@ -162,13 +165,12 @@ __device__ __forceinline__ void quat_matrix(const fd_quat q, double R[9])
     R[6] = 2.0 * (q1 * q3 - q0 * q2); R[7] = 2.0 * (q2 * q3 + q0 * q1); R[8] = 1.0 - 2.0 * (q1 * q1 + q2 * q2);
 }
 
-__global__ void k_hash_count(ObjDev O, FdGrid g, int* count)
+__global__ void k_hash(ObjDev O, FdGrid g)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= O.n) return;
     const long long h = fd_hash(O.pos[i], g);
     O.hash[i] = h;
-    if (h >= 0 && h < g.num) atomicAdd(&count[h], 1);
     if (O.rot) {
         double R[9];
         quat_matrix(O.q[i], R);
@@ -178,14 +180,176 @@ __global__ void k_hash_count(ObjDev O, FdGrid g, int* count)
     }
 }
 
-__global__ void k_scatter(const long long* hash, int n, long long num, const int* start, int* fill, int* sorted)
+// ---------------------------------------------------------------------------
+// stable LSD radix sort of 64-bit cell keys, 8 bits per pass over the bits a
+// key can use: per block a digit histogram, an exclusive scan of the counts
+// (digit-major, so equal digits keep block order), then a scatter that ranks
+// each key within its block by warp (match of equal digits) and by lane
+// ---------------------------------------------------------------------------
+constexpr int RS_TPB = 256;
+constexpr int RS_RADIX = 256;
+constexpr unsigned long long RS_NONE = ~0ull;  // key of an object in no cell
+
+__global__ void k_rs_keys(const long long* hash, int n, long long num, unsigned long long* key, int* idx,
+                          const int* gate)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || (gate && *gate == 0)) return;
+    const long long h = hash[i];
+    key[i] = (h >= 0 && h < num) ? (unsigned long long)h : RS_NONE;
+    idx[i] = i;
+}
+
+__global__ void __launch_bounds__(RS_TPB) k_rs_hist(const unsigned long long* key, int n, int shift, int* bcount,
+                                                   int nblk, const int* gate)
+{
+    if (gate && *gate == 0) return;
+    __shared__ int h[RS_RADIX];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const int i = blockIdx.x * RS_TPB + threadIdx.x;
+    if (i < n) atomicAdd(&h[(key[i] >> shift) & (RS_RADIX - 1)], 1);
+    __syncthreads();
+    bcount[(long long)threadIdx.x * nblk + blockIdx.x] = h[threadIdx.x];
+}
+
+__global__ void __launch_bounds__(RS_TPB) k_rs_scatter(const unsigned long long* key, const int* idx, int n, int shift,
+                                                      const int* boff, int nblk, unsigned long long* okey, int* oidx,
+                                                      const int* gate)
+{
+    if (gate && *gate == 0) return;
+    constexpr int NW = RS_TPB / 32;
+    __shared__ int wcnt[NW][RS_RADIX];
+    for (int d = threadIdx.x; d < NW * RS_RADIX; d += RS_TPB) (&wcnt[0][0])[d] = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int i = blockIdx.x * RS_TPB + threadIdx.x;
+    const bool valid = i < n;
+    const unsigned long long k = valid ? key[i] : 0ull;
+    const int digit = valid ? (int)((k >> shift) & (RS_RADIX - 1)) : RS_RADIX;
+    const unsigned int peers = __match_any_sync(0xffffffffu, digit);
+    const int rank = __popc(peers & ((1u << lane) - 1u));
+    if (valid && lane == __ffs(peers) - 1) wcnt[w][digit] = __popc(peers);
+    __syncthreads();
+    if (valid) {
+        int pos = boff[(long long)digit * nblk + blockIdx.x] + rank;
+        for (int v = 0; v < w; ++v) pos += wcnt[v][digit];
+        okey[pos] = k;
+        oidx[pos] = idx[i];
+    }
+}
+
+// dense table: objects per cell (atomic count), slots by an atomic scatter,
+// then each cell's slots put in ascending object index, so the table equals
+// the one a stable sort of the hashes gives
+__global__ void k_cell_count(const long long* hash, int n, long long num, int* count)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const long long h = hash[i];
+    if (h >= 0 && h < num) atomicAdd(&count[h], 1);
+}
+__global__ void k_cell_scatter(const long long* hash, int n, long long num, const int* start, int* fill, int* sorted)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const long long h = hash[i];
     if (h < 0 || h >= num) return;
-    const int slot = start[h] + atomicAdd(&fill[h], 1);
-    sorted[slot] = i;
+    sorted[start[h] + atomicAdd(&fill[h], 1)] = i;
+}
+__global__ void k_cell_order(long long num, const int* count, const int* start, int* sorted)
+{
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= num) return;
+    const int m = count[c];
+    if (m < 2) return;
+    int* seg = sorted + start[c];
+    for (int a = 1; a < m; ++a) {
+        const int v = seg[a];
+        int b = a - 1;
+        while (b >= 0 && seg[b] > v) {
+            seg[b + 1] = seg[b];
+            --b;
+        }
+        seg[b + 1] = v;
+    }
+}
+
+// runs of equal keys are the cells
+__global__ void k_cells_dense(const unsigned long long* key, int n, long long num, int* count, int* start)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const unsigned long long k = key[i];
+    if (k >= (unsigned long long)num || (i > 0 && key[i - 1] == k)) return;
+    int e = i + 1;
+    while (e < n && key[e] == k) ++e;
+    start[k] = i;
+    count[k] = e - i;
+}
+
+__global__ void k_hkey_clear(unsigned long long* hkey, unsigned long long n, const int* gate)
+{
+    const unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || (gate && *gate == 0)) return;
+    hkey[i] = RS_NONE;
+}
+
+__device__ __forceinline__ unsigned long long cell_slot_hash(unsigned long long k)
+{
+    // splitmix64 finaliser
+    k ^= k >> 30;
+    k *= 0xbf58476d1ce4e5b9ull;
+    k ^= k >> 27;
+    k *= 0x94d049bb133111ebull;
+    k ^= k >> 31;
+    return k;
+}
+
+__global__ void k_cells_hashed(const unsigned long long* key, int n, long long num, unsigned long long* hkey,
+                               int2* hval, unsigned long long hmask, unsigned int* flags, const int* gate)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || (gate && *gate == 0)) return;
+    const unsigned long long k = key[i];
+    if (k >= (unsigned long long)num || (i > 0 && key[i - 1] == k)) return;
+    int e = i + 1;
+    while (e < n && key[e] == k) ++e;
+    unsigned long long slot = cell_slot_hash(k) & hmask;
+    // the table holds at least twice as many slots as there are objects, so
+    // an empty slot is always found; the probe count is bounded all the same
+    for (unsigned long long probe = 0; probe <= hmask; ++probe) {
+        const unsigned long long prev = atomicCAS(&hkey[slot], RS_NONE, k);
+        if (prev == RS_NONE || prev == k) {
+            hval[slot] = make_int2(i, e - i);
+            return;
+        }
+        slot = (slot + 1) & hmask;
+    }
+    set_flag(flags, FD_FLAG_INDEX);
+}
+
+// objects in cell h: their count, and the first of their slots in *first
+__device__ __forceinline__ int cell_lookup(const CellTableDev& T, long long h, int& first)
+{
+    if (!T.hashed) {
+        const int c = T.count[h];
+        if (c) first = T.start[h];
+        return c;
+    }
+    const unsigned long long k = (unsigned long long)h;
+    unsigned long long slot = cell_slot_hash(k) & T.hmask;
+    for (unsigned long long probe = 0; probe <= T.hmask; ++probe) {
+        const unsigned long long kk = T.hkey[slot];
+        if (kk == k) {
+            const int2 v = T.hval[slot];
+            first = v.x;
+            return v.y;
+        }
+        if (kk == RS_NONE) return 0;
+        slot = (slot + 1) & T.hmask;
+    }
+    return 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -230,7 +394,6 @@ __device__ __forceinline__ void image_hash(GhostDev& Gh, int i, double3 r)
     const long long h = out ? fd_lin3(gc.x, gc.y, gc.z, g.size) : -1;
     Gh.hash[i] = h;
     if (h >= 0 && h < g.num) {
-        atomicAdd(&Gh.cells.count[h], 1);
         atomicMin(&Gh.occ[0], gc.x); atomicMin(&Gh.occ[1], gc.y); atomicMin(&Gh.occ[2], gc.z);
         atomicMax(&Gh.occ[3], gc.x); atomicMax(&Gh.occ[4], gc.y); atomicMax(&Gh.occ[5], gc.z);
     }
@@ -626,8 +789,7 @@ __global__ void __launch_bounds__(TPB) k_broad_cells(ObjDev P, GeoSetDev G, Cell
                 y = ((y % T.g.size.y) + T.g.size.y) % T.g.size.y;
             }
             const long long h = fd_lin3(x, y, z, T.g.size);
-            cc = T.count[h];
-            if (cc) cs = T.start[h];
+            cc = cell_lookup(T, h, cs);
         }
         // exclusive scan of the cell counts over the lane group
         int incl = cc;
@@ -890,8 +1052,11 @@ __global__ void k_ghost_searchers(ObjDev P, GeoSetDev G, FdGrid g, const int* oc
     }
 }
 
+// wall_range (null: every wall): per particle, the first wall and the number
+// of walls it can meet (the walls of its own simulation in a batch of
+// simulations tiled into one)
 __global__ void k_broad_pw(ObjDev P, GeoSetDev G, ObjDev W, GeoSetDev GW, FdGrid wg, PairListDev L,
-                           unsigned int* flags, double probe)
+                           unsigned int* flags, double probe, const int2* wall_range)
 {
     const int A = blockIdx.x * blockDim.x + threadIdx.x;
     if (A >= P.n) return;
@@ -901,7 +1066,9 @@ __global__ void k_broad_pw(ObjDev P, GeoSetDev G, ObjDev W, GeoSetDev GW, FdGrid
     body_search_range(cA, rA * (1.0 + BOUND_REL), wg, lo, hi);
     int buf[MAX_CAND];
     int cnt = 0, total = 0;
-    for (int w = 0; w < W.n; ++w) {
+    const int2 wr = wall_range ? wall_range[A] : make_int2(0, W.n);
+    const int wend = min(wr.x + wr.y, W.n);
+    for (int w = max(wr.x, 0); w < wend; ++w) {
         const long long h = W.hash[w];
         if (h < 0 || h >= wg.num) continue;
         int3 c;
@@ -2202,32 +2369,32 @@ size_t scan_tmp_size(long long n)
     return total + 1;
 }
 
-void scan_exclusive(const int* in, int* out, long long n, int* tmp, cudaStream_t s)
+void scan_exclusive(const int* in, int* out, long long n, int* tmp, cudaStream_t s, const int* gate)
 {
     if (n <= 0) return;
     if (n <= SCAN_TILE) {
-        k_scan_tile<false><<<1, SCAN_TPB, 0, s>>>(in, out, n, nullptr); note_launch();
+        k_scan_tile<false><<<1, SCAN_TPB, 0, s>>>(in, out, n, nullptr, gate); note_launch();
         return;
     }
     const long long tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
     int* sums = tmp;
-    k_scan_tile<false><<<(unsigned)tiles, SCAN_TPB, 0, s>>>(in, out, n, sums); note_launch();
-    scan_exclusive(sums, sums, tiles, tmp + tiles, s);
-    k_scan_add<<<(unsigned)tiles, SCAN_TPB, 0, s>>>(out, n, sums); note_launch();
+    k_scan_tile<false><<<(unsigned)tiles, SCAN_TPB, 0, s>>>(in, out, n, sums, gate); note_launch();
+    scan_exclusive(sums, sums, tiles, tmp + tiles, s, gate);
+    k_scan_add<<<(unsigned)tiles, SCAN_TPB, 0, s>>>(out, n, sums, gate); note_launch();
 }
 
 void scan_inclusive(const int* in, int* out, long long n, int* tmp, cudaStream_t s)
 {
     if (n <= 0) return;
     if (n <= SCAN_TILE) {
-        k_scan_tile<true><<<1, SCAN_TPB, 0, s>>>(in, out, n, nullptr); note_launch();
+        k_scan_tile<true><<<1, SCAN_TPB, 0, s>>>(in, out, n, nullptr, nullptr); note_launch();
         return;
     }
     const long long tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
     int* sums = tmp;
-    k_scan_tile<true><<<(unsigned)tiles, SCAN_TPB, 0, s>>>(in, out, n, sums); note_launch();
+    k_scan_tile<true><<<(unsigned)tiles, SCAN_TPB, 0, s>>>(in, out, n, sums, nullptr); note_launch();
     scan_exclusive(sums, sums, tiles, tmp + tiles, s);
-    k_scan_add<<<(unsigned)tiles, SCAN_TPB, 0, s>>>(out, n, sums); note_launch();
+    k_scan_add<<<(unsigned)tiles, SCAN_TPB, 0, s>>>(out, n, sums, nullptr); note_launch();
 }
 
 void launch_kick(const ObjDev& P, const GeoSetDev& G, double3 gravity, double h, cudaStream_t s)
@@ -2238,16 +2405,62 @@ void launch_drift(const ObjDev& O, double dt, cudaStream_t s)
 {
     if (O.n > 0) { k_drift<<<nblocks(O.n), TPB, 0, s>>>(O, dt); note_launch(); }
 }
-void launch_hash_count(const ObjDev& O, CellTableDev& T, cudaStream_t s)
+void launch_hash(const ObjDev& O, const FdGrid& g, cudaStream_t s)
 {
-    cudaMemsetAsync(T.count, 0, sizeof(int) * T.g.num, s);
-    if (O.n > 0) { k_hash_count<<<nblocks(O.n), TPB, 0, s>>>(O, T.g, T.count); note_launch(); }
+    if (O.n > 0) { k_hash<<<nblocks(O.n), TPB, 0, s>>>(O, g); note_launch(); }
 }
-void launch_cell_table(ObjDev& O, CellTableDev& T, int* scan_tmp, size_t, cudaStream_t s)
+void radix_sort_scratch(int n, size_t& bcount_ints, size_t& bscan_ints)
 {
+    const long long nblk = std::max<long long>((n + RS_TPB - 1) / RS_TPB, 1);
+    bcount_ints = (size_t)(RS_RADIX * nblk);
+    bscan_ints = scan_tmp_size((long long)bcount_ints);
+}
+void radix_sort_keys(const long long* keys, int n, long long num_keys, unsigned long long* out_key, int* out_idx,
+                     unsigned long long* key_b, int* idx_b, int* bcount, int* bscan_tmp, cudaStream_t s,
+                     const int* gate)
+{
+    if (n <= 0) return;
+    // bits a key can use; keys of objects in no cell sort after every cell
+    int bits = 1;
+    while (bits < 64 && ((unsigned long long)num_keys >> bits) != 0ull) ++bits;
+    const int passes = (bits + 7) / 8;
+    const int nblk = (n + RS_TPB - 1) / RS_TPB;
+    // the last pass writes (out_key, out_idx)
+    unsigned long long* kb[2] = {out_key, key_b};
+    int* ib[2] = {out_idx, idx_b};
+    int src = passes & 1;
+    k_rs_keys<<<nblocks(n), TPB, 0, s>>>(keys, n, num_keys, kb[src], ib[src], gate); note_launch();
+    for (int p = 0; p < passes; ++p) {
+        const int shift = 8 * p;
+        k_rs_hist<<<nblk, RS_TPB, 0, s>>>(kb[src], n, shift, bcount, nblk, gate); note_launch();
+        scan_exclusive(bcount, bcount, (long long)RS_RADIX * nblk, bscan_tmp, s, gate);
+        k_rs_scatter<<<nblk, RS_TPB, 0, s>>>(kb[src], ib[src], n, shift, bcount, nblk, kb[src ^ 1], ib[src ^ 1], gate);
+        note_launch();
+        src ^= 1;
+    }
+}
+void launch_cell_table(ObjDev& O, CellTableDev& T, int* scan_tmp, size_t, cudaStream_t s, const int* gate)
+{
+    if (O.n <= 0) return;
+    if (T.hashed) {
+        // sparse grids: radix sort of the keys, runs into a hash table
+        radix_sort_keys(O.hash, O.n, T.g.num, T.skey, T.sorted, T.key_b, T.idx_b, T.bcount, T.bscan_tmp, s, gate);
+        if (gate) {
+            k_hkey_clear<<<nblocks((long long)T.hmask + 1), TPB, 0, s>>>(T.hkey, T.hmask + 1, gate); note_launch();
+        } else {
+            cudaMemsetAsync(T.hkey, 0xff, sizeof(unsigned long long) * (T.hmask + 1), s);
+        }
+        k_cells_hashed<<<nblocks(O.n), TPB, 0, s>>>(T.skey, O.n, T.g.num, T.hkey, T.hval, T.hmask, nullptr, gate);
+        note_launch();
+        return;
+    }
+    // dense grids: count, scan, scatter, then each cell in object order
+    cudaMemsetAsync(T.count, 0, sizeof(int) * T.g.num, s);
+    k_cell_count<<<nblocks(O.n), TPB, 0, s>>>(O.hash, O.n, T.g.num, T.count); note_launch();
     scan_exclusive(T.count, T.start, T.g.num, scan_tmp, s);
     cudaMemsetAsync(T.fill, 0, sizeof(int) * T.g.num, s);
-    if (O.n > 0) { k_scatter<<<nblocks(O.n), TPB, 0, s>>>(O.hash, O.n, T.g.num, T.start, T.fill, T.sorted); note_launch(); }
+    k_cell_scatter<<<nblocks(O.n), TPB, 0, s>>>(O.hash, O.n, T.g.num, T.start, T.fill, T.sorted); note_launch();
+    k_cell_order<<<nblocks(T.g.num), TPB, 0, s>>>(T.g.num, T.count, T.start, T.sorted); note_launch();
 }
 void launch_wrap(ObjDev& P, const FdGrid& g, int dim, cudaStream_t s)
 {
@@ -2255,7 +2468,6 @@ void launch_wrap(ObjDev& P, const FdGrid& g, int dim, cudaStream_t s)
 }
 void launch_ghost_build(const ObjDev& P, GhostDev& Gh, int kind, cudaStream_t s)
 {
-    cudaMemsetAsync(Gh.cells.count, 0, sizeof(int) * Gh.cells.g.num, s);
     // occupied-cell box of the ghost images: empty until the build fills it
     cudaMemsetAsync(Gh.occ, 0x7f, 3 * sizeof(int), s);
     cudaMemsetAsync(Gh.occ + 3, 0xff, 3 * sizeof(int), s);
@@ -2268,7 +2480,6 @@ void launch_sector_wrap(ObjDev& P, const FdGrid& g, cudaStream_t s)
 void launch_sector_images(const ObjDev& P, GhostDev* R, cudaStream_t s)
 {
     for (int d = 0; d < 3; ++d) {
-        cudaMemsetAsync(R[d].cells.count, 0, sizeof(int) * R[d].cells.g.num, s);
         cudaMemsetAsync(R[d].occ, 0x7f, 3 * sizeof(int), s);
         cudaMemsetAsync(R[d].occ + 3, 0xff, 3 * sizeof(int), s);
     }
@@ -2306,10 +2517,11 @@ void launch_pair_cache_commit(const ObjDev& P, const PairCacheDev& c, const Pair
 }
 
 void launch_broad_pw(const ObjDev& P, const GeoSetDev& G, const ObjDev& W, const GeoSetDev& GW,
-                     const FdGrid& wg, PairListDev& L, unsigned int* flags, double probe, cudaStream_t s)
+                     const FdGrid& wg, PairListDev& L, unsigned int* flags, double probe, cudaStream_t s,
+                     const int2* wall_range)
 {
     cudaMemsetAsync(L.n_pairs, 0, sizeof(int), s);
-    if (P.n > 0) { k_broad_pw<<<nblocks(P.n), TPB, 0, s>>>(P, G, W, GW, wg, L, flags, probe); note_launch(); }
+    if (P.n > 0) { k_broad_pw<<<nblocks(P.n), TPB, 0, s>>>(P, G, W, GW, wg, L, flags, probe, wall_range); note_launch(); }
 }
 void launch_broad_ghost(const ObjDev& P, const GeoSetDev& G, const GhostDev& Gh, PairListDev& L,
                         unsigned int* flags, double probe, cudaStream_t s)

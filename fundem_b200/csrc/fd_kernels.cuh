@@ -104,12 +104,31 @@ struct MatDev {
     const double* e;
 };
 
+// Cell table of one object set (hashGrid of buildHashStartEnd.cu:69-137).
+// The objects' 64-bit cell keys are sorted by a stable LSD radix sort (so
+// each cell lists its objects in ascending index, as the reference's stable
+// thrust::sort_by_key does); the runs of equal keys are the cells.  A grid of
+// few cells keeps a dense start/count table over all cells; a grid of many
+// cells (dense would be large next to the object count) keeps an
+// open-addressing hash table of its occupied cells instead.
 struct CellTableDev {
     FdGrid g;
-    int* count;
-    int* start;
-    int* fill;
-    int* sorted;   // object index per slot
+    int hashed;                 // 0: dense table, 1: hash table of occupied cells
+    int* count;                 // dense: objects per cell
+    int* start;                 // dense: first slot of each cell (valid where count > 0)
+    int* fill;                  // dense: scatter counters
+    unsigned long long* hkey;   // hashed: cell key per table slot (~0: empty)
+    int2* hval;                 // hashed: (first slot, objects) per table slot
+    unsigned long long hmask;   // hashed: table size - 1 (a power of two)
+    int* sorted;                // object index per slot, by cell key
+    unsigned long long* skey;   // cell key per slot (~0 for objects in no cell, last)
+    // sort scratch: the second key/index buffers, per-block digit counts and
+    // their scan's temporary
+    unsigned long long* key_b;
+    int* idx_b;
+    int* bcount;
+    int* bscan_tmp;
+    int nobj_cap;               // objects the scratch holds
 };
 
 struct GhostDev {
@@ -226,8 +245,22 @@ struct StepArgs {
 // integration and hashing
 void launch_kick(const ObjDev& P, const GeoSetDev& G, double3 gravity, double h, cudaStream_t s);
 void launch_drift(const ObjDev& O, double dt, cudaStream_t s);
-void launch_hash_count(const ObjDev& O, CellTableDev& T, cudaStream_t s);
-void launch_cell_table(ObjDev& O, CellTableDev& T, int* scan_tmp, size_t scan_tmp_ints, cudaStream_t s);
+// cell hash of each object (-1 outside the grid) and its single-precision
+// rotation rows
+void launch_hash(const ObjDev& O, const FdGrid& g, cudaStream_t s);
+// the cell table from the objects' hashes (O.hash); with gate non-null a
+// hash-table build runs only when *gate != 0 (the pair cache's rebuild flag)
+void launch_cell_table(ObjDev& O, CellTableDev& T, int* scan_tmp, size_t scan_tmp_ints, cudaStream_t s,
+                       const int* gate = nullptr);
+// stable sort of n 64-bit keys (key 0 .. num_keys - 1, or negative: last) on
+// the stream: out_idx gets the permutation, out_key the sorted keys (~0 for
+// the negative ones).  Scratch: key_b (n), idx_b (n), bcount and bscan_tmp
+// sized by radix_sort_scratch.
+void radix_sort_keys(const long long* keys, int n, long long num_keys, unsigned long long* out_key, int* out_idx,
+                     unsigned long long* key_b, int* idx_b, int* bcount, int* bscan_tmp, cudaStream_t s,
+                     const int* gate = nullptr);
+// ints needed for bcount and bscan_tmp for n keys
+void radix_sort_scratch(int n, size_t& bcount_ints, size_t& bscan_ints);
 void launch_wrap(ObjDev& P, const FdGrid& g, int dim, cudaStream_t s);
 void launch_ghost_build(const ObjDev& P, GhostDev& Gh, int kind, cudaStream_t s);
 // sector periodicity: turn bodies that left the quarter sector back in, then
@@ -248,8 +281,11 @@ void launch_broad_pp_nl(const ObjDev& P, const GeoSetDev& G, const CellTableDev&
 // the state of a rebuild step as the new reference and clear the flag
 void launch_pair_cache_check(const ObjDev& P, const PairCacheDev& c, cudaStream_t s);
 void launch_pair_cache_commit(const ObjDev& P, const PairCacheDev& c, const PairListDev& L, cudaStream_t s);
+// wall_range (null: every wall): per particle, the first wall and the wall
+// count it may meet (a batch of simulations tiled into one)
 void launch_broad_pw(const ObjDev& P, const GeoSetDev& G, const ObjDev& W, const GeoSetDev& GW,
-                     const FdGrid& wg, PairListDev& L, unsigned int* flags, double probe, cudaStream_t s);
+                     const FdGrid& wg, PairListDev& L, unsigned int* flags, double probe, cudaStream_t s,
+                     const int2* wall_range = nullptr);
 void launch_broad_ghost(const ObjDev& P, const GeoSetDev& G, const GhostDev& Gh, PairListDev& L,
                         unsigned int* flags, double probe, cudaStream_t s);
 // a.gate non-null (particle-particle list under the pair cache): on steps
@@ -274,7 +310,7 @@ void count_launch();
 
 // exclusive scan of n ints (out may alias in); returns needed tmp ints when tmp == nullptr
 size_t scan_tmp_size(long long n);
-void scan_exclusive(const int* in, int* out, long long n, int* tmp, cudaStream_t s);
+void scan_exclusive(const int* in, int* out, long long n, int* tmp, cudaStream_t s, const int* gate = nullptr);
 // inclusive scan of n ints; tmp as for scan_exclusive
 void scan_inclusive(const int* in, int* out, long long n, int* tmp, cudaStream_t s);
 

@@ -77,6 +77,13 @@ int fundem_set_pair_cache(fundem_sim* sim, int mode, double skin);
 /* rebuilds of the pair cache and steps run with it since setup, and the skin
    in use (zeros when the cache is off) */
 int fundem_pair_cache_stats(fundem_sim* sim, long long* rebuilds, long long* steps, double* skin);
+/* Wall groups for a batch of independent simulations tiled into one: for each
+   particle (n = the particle count), the first wall and the number of walls
+   it may meet; the particle-wall broad phase then tests only those walls
+   instead of every wall (the reference tests every wall in the particle's
+   wall-cell neighbourhood, LSParticleContactDetectionKernel.cu:307-429).
+   n = 0 removes the groups.  No counterpart in the reference. */
+int fundem_set_wall_groups(fundem_sim* sim, int n, const int* first, const int* count);
 /* when nonzero every step writes full contact records (point, normal,
    overlap, energies); otherwise only node, partner and sliding spring */
 int fundem_set_records(fundem_sim* sim, int full_records);
@@ -232,6 +239,19 @@ int fundem_get_grid(fundem_sim* sim, int wall, double minb[3], double maxb[3], d
    runs thrust::inclusive_scan); scratch is taken with cudaMallocAsync on the
    stream and released after the scan.  stream may be NULL. */
 int fundem_prefix_sum(int* d_prefix, const int* d_count, long long n, void* stream);
+
+/* Stable sort of object cell hashes, device arrays, stream-ordered:
+   d_sorted receives the permutation that orders d_hash ascending, objects of
+   equal hash in ascending index, and hashes outside [0, num_cells) (the
+   reference's -1 for objects outside the grid) last; d_sorted_hash (may be
+   NULL) receives the sorted hashes, -1 for those.  Replaces the sort of
+   buildHashStartEnd, kernel/CUDAKernelFunction/myUtility/buildHashStartEnd.cu:69-137
+   (thrust::sort_by_key on int32 hashes); here the hashes are 64-bit, so grids
+   of more than 2^31 cells work.  An LSD radix sort, 8 bits per pass over the
+   bits num_cells needs; scratch is taken with cudaMallocAsync on the stream
+   and released after the sort.  stream may be NULL. */
+int fundem_hash_sort(const long long* d_hash, int n, long long num_cells, int* d_sorted, long long* d_sorted_hash,
+                     void* stream);
 
 /* The same inclusive prefix sum without any device allocation.  No
    counterpart in the reference.  For callers that cannot allocate device
