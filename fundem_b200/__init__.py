@@ -36,6 +36,7 @@ EXPORTS = [
     "fundem_step_graph", "fundem_set_neighbour_list", "fundem_checkpoint_write", "fundem_checkpoint_read",
     "fundem_levelset_grid", "fundem_set_periodic_sector", "fundem_set_inertia_mode",
     "fundem_set_pair_cache", "fundem_pair_cache_stats", "fundem_set_wall_groups", "fundem_hash_sort",
+    "fundem_adjoint_backward_rot",
 ]
 TIMERS = {"integrate": 0, "hash": 1, "broad": 2, "narrow_pp": 3, "narrow_pw": 4, "ghost": 5, "reduce": 6}
 
@@ -119,6 +120,7 @@ def lib():
         L.fundem_adjoint_begin.argtypes = [P, I]
         L.fundem_adjoint_forward.argtypes = [P, I, D, C.c_double]
         L.fundem_adjoint_backward.argtypes = [P, D, D, D, D]
+        L.fundem_adjoint_backward_rot.argtypes = [P, D, D, D, D, D, D, D]
         L.fundem_adjoint_end.argtypes = [P]
         L.fundem_step_graph.argtypes = [P, I, D, C.c_double]
         L.fundem_set_neighbour_list.argtypes = [P, I]
@@ -336,6 +338,20 @@ class Simulation:
         self._check(self.L.fundem_adjoint_backward(self.h, _d(_f64(dl_dpos, 3 * n)), _d(_f64(dl_dvel, 3 * n)),
                                                    _d(gv0), _d(gp)), "adjoint_backward")
         return gv0, gp
+
+    def adjoint_backward_rot(self, dl_dpos, dl_dvel, dl_dquat=None, dl_dangvel=None):
+        """As adjoint_backward, with loss gradients on the final orientations
+        (n, 4) and angular velocities (n, 3) of turning bodies: returns
+        (d/d initial velocities, d/d initial angular velocities, d/d per
+        particle material)."""
+        n = self.num(False)
+        gv0, gw0 = np.zeros((n, 3)), np.zeros((n, 3))
+        gp = np.zeros((getattr(self, "_n_pmat", 1), 4))
+        q = None if dl_dquat is None else _f64(dl_dquat, 4 * n)
+        w = None if dl_dangvel is None else _f64(dl_dangvel, 3 * n)
+        self._check(self.L.fundem_adjoint_backward_rot(self.h, _d(_f64(dl_dpos, 3 * n)), _d(_f64(dl_dvel, 3 * n)),
+                                                       _d(q), _d(w), _d(gv0), _d(gw0), _d(gp)), "adjoint_backward_rot")
+        return gv0, gw0, gp
 
     def adjoint_end(self):
         self._check(self.L.fundem_adjoint_end(self.h), "adjoint_end")

@@ -9,7 +9,7 @@ struct AdjParticles {
     int n;
     const int* geo;
     const int* mat;
-    const double3* angvel;  // constant over the run: the bodies do not turn
+    const double3* angvel;  // without turning bodies: constant over the run
     GeoSetDev G;
     double* xb;     // adjoint of the positions
     double* vb;     // adjoint of the velocities at the step's end
@@ -17,10 +17,26 @@ struct AdjParticles {
     double* Fb;     // adjoint of the step's forces
     double* Feb;    // adjoint of the forces reaching the next step's first half-kick
     double* pgrad;  // 4 per particle material: kn, ks, damping ratio, mu
+    // turning bodies (rot = 1: some particle geometry has a nonzero inverse
+    // inertia).  Per particle and step the record holds 10 doubles:
+    // orientation (4), angular velocity (3), torque (3); pr_prev at the step's
+    // start (the previous step's end), pr_cur after the step's drift
+    // (orientation), first half-kick (angular velocity at force time) and
+    // forces (torque)
+    int rot;
+    const double* pr_prev;
+    const double* pr_cur;
+    double* qb;     // 4 per particle: adjoint of the orientation
+    double* wb;     // adjoint of the angular velocity at the step's end
+    double* whb;    // adjoint of the angular velocity at force time
+    double* Tb;     // adjoint of the step's torques
+    double* Teb;    // adjoint of the torques reaching the next step's first half-kick
 };
+constexpr int ADJ_PREC = 10;  // doubles per particle and step in the record
 
 struct AdjContactArgs {
     AdjRec rec;            // the list at this step
+    double3 period;        // domain lengths in x and y (periodic wrap codes)
     const int* nslots;     // slots of the list at this step
     MatDev M;              // particle materials
     MatDev MW;             // wall materials
@@ -47,5 +63,9 @@ void adj_force(const AdjParticles& a, double dt, cudaStream_t s);
 void adj_contacts(const AdjParticles& a, const AdjContactArgs& c, cudaStream_t s);
 void adj_bonds(const AdjParticles& a, const AdjBondArgs& b, cudaStream_t s);
 void adj_particles(const AdjParticles& a, double dt, cudaStream_t s);
+// the record of turning bodies: orientation and angular velocity (after a
+// drift), torque (after the forces), or all three (a segment's start)
+void adj_record_rot(const ObjDev& P, double* dst, int what, cudaStream_t s);
+enum { ADJ_REC_QW = 1, ADJ_REC_T = 2 };
 
 }  // namespace fd

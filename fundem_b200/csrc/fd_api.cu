@@ -659,8 +659,9 @@ constexpr int PC_MIN_PARTICLES = 8192;
 struct AdjTape {
     int steps = 0;
     int cap[FD_NKIND] = {0, 0, 0, 0, 0};
-    DevArray<int> ints[FD_NKIND];        // 8 ints per slot per step
-    DevArray<double> dbl[FD_NKIND];      // 13 doubles per slot per step
+    DevArray<int> ints[FD_NKIND];        // 9 ints per slot per step
+    DevArray<double> dbl[FD_NKIND];      // 16 doubles per slot per step
+    DevArray<double> prot;               // turning bodies: ADJ_PREC per particle and step, K + 1 steps
     DevArray<int> nslots;                // per step and kind
     int nbond = 0;
     DevArray<int> bond_active;           // per step and bond
@@ -670,11 +671,11 @@ struct AdjTape {
     {
         fd::AdjRec r{};
         const long long c = cap[k];
-        int* I = ints[k].p + 8ll * c * t;
-        double* D = dbl[k].p + 13ll * c * t;
+        int* I = ints[k].p + 9ll * c * t;
+        double* D = dbl[k].p + 16ll * c * t;
         r.hit = I; r.A = I + c; r.Bp = I + 2 * c; r.B = I + 3 * c; r.geoB = I + 4 * c; r.matB = I + 5 * c;
-        r.nid = I + 6 * c; r.hist = I + 7 * c;
-        r.rel = D; r.vc = D + 3 * c; r.sprev = D + 6 * c; r.qB = D + 9 * c;
+        r.nid = I + 6 * c; r.hist = I + 7 * c; r.wrap = I + 8 * c;
+        r.rel = D; r.vc = D + 3 * c; r.sprev = D + 6 * c; r.qB = D + 9 * c; r.arm = D + 13 * c;
         r.cap = cap[k];
         return r;
     }
@@ -775,6 +776,16 @@ struct fundem_sim {
         pc_ctrl.alloc(4);
     }
     double pc_skin() const { return pc_skin_set > 0.0 ? pc_skin_set : PC_SKIN * pgeo.rmax; }
+    // some particle geometry has a nonzero inverse inertia: its bodies turn,
+    // and the adjoint differentiates orientations and angular velocities
+    bool adj_turning() const
+    {
+        for (const FdGeo& g : pgeo.table) {
+            const fd_sym& I = g.inv_inertia;
+            if (I.xx != 0.0 || I.yy != 0.0 || I.zz != 0.0 || I.xy != 0.0 || I.xz != 0.0 || I.yz != 0.0) return true;
+        }
+        return false;
+    }
     // the adjoint records and re-runs full detections
     bool pc_active() const { return pc_on && !adj.on && recording == nullptr && pc_ctrl.p != nullptr; }
     fd::PairCacheDev pc_view()
@@ -2285,12 +2296,10 @@ int fundem_adjoint_begin(fundem_sim* s, int checkpoint_interval)
         s->last_error = "the adjoint does not differentiate through the turned images of sector periodicity";
         return FUNDEM_ERR_STATE;
     }
-    for (const FdGeo& g : s->pgeo.table) {
-        const fd_sym& I = g.inv_inertia;
-        if (I.xx != 0.0 || I.yy != 0.0 || I.zz != 0.0 || I.xy != 0.0 || I.xz != 0.0 || I.yz != 0.0) {
-            s->last_error = "the adjoint differentiates translations only: a particle geometry can rotate";
-            return FUNDEM_ERR_STATE;
-        }
+    if (s->adj_turning() && !s->bonds.master.empty()) {
+        s->last_error = "the adjoint differentiates bonds between bodies that do not turn only: a particle "
+                        "geometry can rotate and the run has bonds";
+        return FUNDEM_ERR_STATE;
     }
     return guard(s, [&] {
         AdjState& A = s->adj;
@@ -2346,6 +2355,12 @@ int fundem_adjoint_forward(fundem_sim* s, int nsteps, const double g[3], double 
 int fundem_adjoint_backward(fundem_sim* s, const double* dl_dpos, const double* dl_dvel, double* dl_dvel0,
                             double* dl_dparams)
 {
+    return fundem_adjoint_backward_rot(s, dl_dpos, dl_dvel, nullptr, nullptr, dl_dvel0, nullptr, dl_dparams);
+}
+
+int fundem_adjoint_backward_rot(fundem_sim* s, const double* dl_dpos, const double* dl_dvel, const double* dl_dquat,
+                                const double* dl_dangvel, double* dl_dvel0, double* dl_dangvel0, double* dl_dparams)
+{
     if (!s || !dl_dpos || !dl_dvel || !dl_dvel0 || !dl_dparams) return FUNDEM_ERR_ARG;
     AdjState& A = s->adj;
     if (!A.on || A.steps == 0) return FUNDEM_ERR_STATE;
@@ -2374,8 +2389,8 @@ int fundem_adjoint_backward(fundem_sim* s, const double* dl_dpos, const double* 
         for (int k = 0; k < FD_NKIND; ++k) {
             T.cap[k] = (used[k] && s->lists[k].allocated) ? s->lists[k].cap_contacts : 0;
             const size_t c = (size_t)std::max(T.cap[k], 1);
-            T.ints[k].alloc(8 * c * K, false);
-            T.dbl[k].alloc(13 * c * K, false);
+            T.ints[k].alloc(9 * c * K, false);
+            T.dbl[k].alloc(16 * c * K, false);
         }
         T.nslots.alloc((size_t)K * FD_NKIND);
         fd::BondDev bd = s->bond_view();
@@ -2386,6 +2401,17 @@ int fundem_adjoint_backward(fundem_sim* s, const double* dl_dpos, const double* 
         DevArray<double> xb, vb, vhb, Fb, Feb, pgrad, Sb[2][FD_NKIND];
         xb.alloc(3 * (size_t)np); vb.alloc(3 * (size_t)np); vhb.alloc(3 * (size_t)np);
         Fb.alloc(3 * (size_t)np); Feb.alloc(3 * (size_t)np); pgrad.alloc(4 * (size_t)std::max(nmat, 1));
+        // turning bodies: orientation and angular-velocity adjoints and the
+        // per-step record of orientations, angular velocities and torques
+        const bool rot = s->adj_turning();
+        DevArray<double> qb, wb, whb, Tb, Teb;
+        if (rot) {
+            qb.alloc(4 * (size_t)np); wb.alloc(3 * (size_t)np); whb.alloc(3 * (size_t)np);
+            Tb.alloc(3 * (size_t)np); Teb.alloc(3 * (size_t)np);
+            T.prot.alloc((size_t)fd::ADJ_PREC * np * (K + 1), false);
+            if (dl_dquat) qb.upload(dl_dquat, 4 * (size_t)np, s->stream);
+            if (dl_dangvel) wb.upload(dl_dangvel, 3 * (size_t)np, s->stream);
+        }
         for (int k = 0; k < FD_NKIND; ++k) {
             Sb[0][k].alloc(3 * (size_t)std::max(T.cap[k], 1));
             Sb[1][k].alloc(3 * (size_t)std::max(T.cap[k], 1));
@@ -2393,7 +2419,9 @@ int fundem_adjoint_backward(fundem_sim* s, const double* dl_dpos, const double* 
         xb.upload(dl_dpos, 3 * (size_t)np, s->stream);
         vb.upload(dl_dvel, 3 * (size_t)np, s->stream);
         const ObjDev Pv = s->P.view();
-        fd::AdjParticles ap{np, Pv.geo, Pv.mat, Pv.angvel, s->pgeo.view(), xb.p, vb.p, vhb.p, Fb.p, Feb.p, pgrad.p};
+        fd::AdjParticles ap{np, Pv.geo, Pv.mat, Pv.angvel, s->pgeo.view(), xb.p, vb.p, vhb.p, Fb.p, Feb.p, pgrad.p,
+                            rot ? 1 : 0, nullptr, nullptr, qb.p, wb.p, whb.p, Tb.p, Teb.p};
+        const size_t prs = (size_t)fd::ADJ_PREC * np;  // record doubles per step
         std::map<std::tuple<int, int, int>, double3> carry;
         int cur = 0;
         for (int seg = (int)A.ckpt.size() - 1; seg >= 0; --seg) {
@@ -2402,11 +2430,14 @@ int fundem_adjoint_backward(fundem_sim* s, const double* dl_dpos, const double* 
             adj_restore(s, A.ckpt[seg]);
             // re-run the segment, recording every step
             s->recording = &T;
+            if (rot) fd::adj_record_rot(s->P.view(), T.prot.p, fd::ADJ_REC_QW | fd::ADJ_REC_T, s->stream);
             for (int t = 0; t < ns; ++t) {
                 s->record_step = t;
                 s->front(A.g, A.dt);
+                if (rot) fd::adj_record_rot(s->P.view(), T.prot.p + prs * (t + 1), fd::ADJ_REC_QW, s->stream);
                 s->detect_all(true, A.dt);
                 s->back(A.g, A.dt);
+                if (rot) fd::adj_record_rot(s->P.view(), T.prot.p + prs * (t + 1), fd::ADJ_REC_T, s->stream);
             }
             s->recording = nullptr;
             FD_CUDA(cudaStreamSynchronize(s->stream));
@@ -2446,6 +2477,10 @@ int fundem_adjoint_backward(fundem_sim* s, const double* dl_dpos, const double* 
             }
             // reverse sweep over the segment
             for (int t = ns - 1; t >= 0; --t) {
+                if (rot) {
+                    ap.pr_prev = T.prot.p + prs * t;
+                    ap.pr_cur = T.prot.p + prs * (t + 1);
+                }
                 fd::adj_force(ap, A.dt, s->stream);
                 const int prv = cur ^ 1;
                 for (int k = 0; k < FD_NKIND; ++k)
@@ -2454,6 +2489,7 @@ int fundem_adjoint_backward(fundem_sim* s, const double* dl_dpos, const double* 
                     if (T.cap[k] == 0) continue;
                     fd::AdjContactArgs c{};
                     c.rec = T.rec(k, t);
+                    c.period = make_double3(s->pgrid.maxb.x - s->pgrid.minb.x, s->pgrid.maxb.y - s->pgrid.minb.y, 0.0);
                     c.nslots = T.ns(k, t);
                     c.M = s->pmat.view();
                     c.MW = s->wmat.view();
@@ -2493,6 +2529,10 @@ int fundem_adjoint_backward(fundem_sim* s, const double* dl_dpos, const double* 
         }
         FD_CUDA(cudaStreamSynchronize(s->stream));
         FD_CUDA(cudaMemcpy(dl_dvel0, vb.p, sizeof(double) * 3 * np, cudaMemcpyDeviceToHost));
+        if (dl_dangvel0) {
+            if (rot) FD_CUDA(cudaMemcpy(dl_dangvel0, wb.p, sizeof(double) * 3 * np, cudaMemcpyDeviceToHost));
+            else std::fill(dl_dangvel0, dl_dangvel0 + 3 * (size_t)np, 0.0);
+        }
         FD_CUDA(cudaMemcpy(dl_dparams, pgrad.p, sizeof(double) * 4 * nmat, cudaMemcpyDeviceToHost));
         adj_restore(s, A.final_state);
         FD_CUDA(cudaStreamSynchronize(s->stream));

@@ -370,6 +370,16 @@ __device__ __forceinline__ double3 wrap_y(double3 p, const FdGrid& g)
     return p;
 }
 
+// periodic shifts of the force-side centres ri, rj against the detection-side
+// cA, cB (-1, 0 or 1 period per axis), as one code for the adjoint's record
+__device__ __forceinline__ int wrap_code(double3 cA, double3 ri, double3 cB, double3 rj, const FdGrid& g)
+{
+    const double Lx = g.maxb.x - g.minb.x, Ly = g.maxb.y - g.minb.y;
+    auto sh = [](double d, double L) { return d > 0.5 * L ? 1 : (d < -0.5 * L ? -1 : 0); };
+    return (sh(ri.x - cA.x, Lx) + 1) + 3 * (sh(ri.y - cA.y, Ly) + 1) + 9 * (sh(rj.x - cB.x, Lx) + 1) +
+           27 * (sh(rj.y - cB.y, Ly) + 1);
+}
+
 __global__ void k_wrap(ObjDev P, FdGrid g, int dim)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1574,6 +1584,10 @@ __global__ void __launch_bounds__(TPB, PASS == 0 ? FD_PROBE_MIN_BLOCKS : FD_CONT
                     R.qB[4 * s + 1] = qB.q1;
                     R.qB[4 * s + 2] = qB.q2;
                     R.qB[4 * s + 3] = qB.q3;
+                    R.arm[3 * s + 0] = r.x;
+                    R.arm[3 * s + 1] = r.y;
+                    R.arm[3 * s + 2] = r.z;
+                    R.wrap[s] = 13 + 27;  // no shift unless the force side records one
                 }
                 double kn = 0., ks = 0.;
                 if (n.with_force) {
@@ -1621,6 +1635,7 @@ __global__ void __launch_bounds__(TPB, PASS == 0 ? FD_PROBE_MIN_BLOCKS : FD_CONT
                         R.vc[3 * s + 0] = vc.x;
                         R.vc[3 * s + 1] = vc.y;
                         R.vc[3 * s + 2] = vc.z;
+                        R.wrap[s] = wrap_code(cA, ri, cB, rj, n.pgrid);
                     }
                     double3 F = mk3(0., 0., 0.);
                     linear_contact(F, spring, vc, nrm, ov, n.a.dt, kn, ks, mu, res, effM);
@@ -1925,6 +1940,10 @@ __global__ void __launch_bounds__(TPB, PASS == 0 ? FD_PROBE_MIN_BLOCKS : FD_CONT
                     R.qB[4 * s + 1] = qB.q1;
                     R.qB[4 * s + 2] = qB.q2;
                     R.qB[4 * s + 3] = qB.q3;
+                    R.arm[3 * s + 0] = rd.x;
+                    R.arm[3 * s + 1] = rd.y;
+                    R.arm[3 * s + 2] = rd.z;
+                    R.wrap[s] = 13 + 27;  // no shift unless the force side records one
                 }
                 const int mi = n.P.mat[A];
                 float kn = 0.f, ks = 0.f;
@@ -1968,6 +1987,7 @@ __global__ void __launch_bounds__(TPB, PASS == 0 ? FD_PROBE_MIN_BLOCKS : FD_CONT
                         R.vc[3 * s + 0] = vc.x;
                         R.vc[3 * s + 1] = vc.y;
                         R.vc[3 * s + 2] = vc.z;
+                        R.wrap[s] = wrap_code(cA, ri, cB, rj, n.pgrid);
                     }
                     const v3f F = linear_contact32(spring, vc, nrm, ov, (float)n.a.dt, kn, ks, mu, res, effM);
                     const v3f TA = crossf(armA, F);

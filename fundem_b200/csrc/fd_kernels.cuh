@@ -184,6 +184,9 @@ struct AdjRec {
     double* vc;      // 3 per slot: relative velocity of A against the partner
     double* sprev;   // 3 per slot: sliding spring before this step's update
     double* qB;      // 4 per slot: partner orientation
+    double* arm;     // 3 per slot: contact node minus A's centre, world frame
+    int* wrap;       // per slot: periodic shifts of the force-side centres,
+                     // (sAx + 1) + 3 (sAy + 1) + 9 (sBx + 1) + 27 (sBy + 1)
     int cap;         // slots the record holds
 };
 

@@ -276,10 +276,12 @@ int fundem_prefix_sum_noalloc(int* d_prefix, const int* d_count, long long n, vo
    shear stiffness, damping ratio and friction coefficient.  Contact topology
    is frozen at each step, as the forward run had it (including each
    contact's stick or slip and each bond's breakage); orientations are
-   taken as fixed, so every particle geometry must have a zero inverse
-   inertia (as the reference's inverse() gives mm-scale particles); constant
-   angular velocities of particles and prescribed ones of walls enter the
-   contact velocities.  Sector periodicity is not differentiated.
+   differentiated when a particle geometry has a nonzero inverse inertia
+   (fundem_adjoint_backward_rot takes loss gradients on them); otherwise
+   they are fixed, and constant angular velocities of particles and
+   prescribed ones of walls enter the contact velocities.  Bonds are
+   differentiated between bodies that do not turn.  Sector periodicity is not
+   differentiated.
    begin: start recording from the current state (after fundem_detect),
      with a checkpoint every checkpoint_interval steps;
    forward: run steps (one gravity and time step for the whole recording);
@@ -294,6 +296,20 @@ int fundem_adjoint_forward(fundem_sim* sim, int nsteps, const double gravity[3],
 int fundem_adjoint_backward(fundem_sim* sim, const double* dl_dpos, const double* dl_dvel, double* dl_dvel0,
                             double* dl_dparams);
 int fundem_adjoint_end(fundem_sim* sim);
+/* fundem_adjoint_backward with turning bodies: dl_dquat (n*4) and dl_dangvel
+   (n*3) carry the loss gradient on the final orientations and angular
+   velocities (either may be NULL: zero), dl_dangvel0 (n*3, may be NULL)
+   receives the gradient with respect to the initial angular velocities.
+   The reverse sweep differentiates the world-frame inertia of the half
+   kick (particleIntegrationKernel.cu:3-32), the quaternion Euler step with
+   its normalisation (myQua.h:77-93), the lever arms of the contact torques
+   and the contact velocity (contactKernel.cu:104, 120-123) and the partner's
+   orientation in the SDF lookup and the normal.  Runs with bonds between
+   turning bodies are refused at fundem_adjoint_begin.  No counterpart in
+   the reference. */
+int fundem_adjoint_backward_rot(fundem_sim* sim, const double* dl_dpos, const double* dl_dvel,
+                                const double* dl_dquat, const double* dl_dangvel, double* dl_dvel0,
+                                double* dl_dangvel0, double* dl_dparams);
 
 /* Checkpoint files (FP64 binary): object state, the contact history of every
    list and bond activation, which is all a restart needs besides the setup
