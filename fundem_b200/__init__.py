@@ -36,7 +36,7 @@ EXPORTS = [
     "fundem_step_graph", "fundem_set_neighbour_list", "fundem_checkpoint_write", "fundem_checkpoint_read",
     "fundem_levelset_grid", "fundem_set_periodic_sector", "fundem_set_inertia_mode",
     "fundem_set_pair_cache", "fundem_pair_cache_stats", "fundem_set_wall_groups", "fundem_hash_sort",
-    "fundem_adjoint_backward_rot",
+    "fundem_adjoint_backward_rot", "fundem_contact_view_get", "fundem_bond_view_get",
 ]
 TIMERS = {"integrate": 0, "hash": 1, "broad": 2, "narrow_pp": 3, "narrow_pw": 4, "ghost": 5, "reduce": 6}
 

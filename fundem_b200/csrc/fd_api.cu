@@ -750,6 +750,16 @@ struct fundem_sim {
     {
         return fd::NlDev{nl_ref.p, nl_vis.p, nl_cnt.p, nl_list.p, nl_ctrl.p, NL_SKIN * pgeo.rmax, perX, perY, 0.0};
     }
+    // contiguous views handed out by fundem_contact_view_get / fundem_bond_view_get
+    struct ContactView {
+        DevArray<long long> keys;
+        DevArray<int> order, idx_b, bcount, bscan, master, slave;
+        DevArray<unsigned long long> skey, key_b;
+        DevArray<double> point, normal, overlap, en, es, spring;
+    };
+    ContactView cviews[FD_NKIND];
+    DevArray<double> bview_B, bview_energy;
+    DevArray<double3> bview_frames;
     // per particle: first wall and wall count it may meet (fundem_set_wall_groups)
     std::vector<int2> wall_groups;
     DevArray<int2> d_wall_groups;
@@ -1430,6 +1440,73 @@ int fundem_set_wall_groups(fundem_sim* s, int n, const int* first, const int* co
             s->d_wall_groups.upload(s->wall_groups, s->stream);
         }
         s->drop_graph();
+    });
+}
+
+int fundem_contact_view_get(fundem_sim* s, int kind, fundem_contact_view* out)
+{
+    if (!s || !out || kind < 0 || kind >= FD_NKIND) return FUNDEM_ERR_ARG;
+    *out = fundem_contact_view{};
+    PairList& L = s->lists[kind];
+    if (!s->setup_done || !L.allocated) return FUNDEM_OK;
+    return guard(s, [&] {
+        int c[3] = {0, 0, 0};
+        FD_CUDA(cudaStreamSynchronize(s->stream));
+        FD_CUDA(cudaMemcpy(c, L.gen[L.cur].counters.p, sizeof(c), cudaMemcpyDeviceToHost));
+        const long long n = c[1] <= L.cap_contacts ? c[2] : 0;
+        const size_t cap = (size_t)std::max(L.cap_contacts, 1);
+        auto& V = s->cviews[kind];
+        if (V.keys.n < cap) {
+            V.keys.alloc(cap, false); V.order.alloc(cap, false); V.idx_b.alloc(cap, false);
+            V.skey.alloc(cap, false); V.key_b.alloc(cap, false);
+            size_t bc = 0, bs = 0;
+            fd::radix_sort_scratch((int)cap, bc, bs);
+            V.bcount.alloc(bc, false); V.bscan.alloc(bs, false);
+            V.master.alloc(cap, false); V.slave.alloc(cap, false); V.overlap.alloc(cap, false);
+            V.en.alloc(cap, false); V.es.alloc(cap, false);
+            V.point.alloc(3 * cap, false); V.normal.alloc(3 * cap, false); V.spring.alloc(3 * cap, false);
+        }
+        fd::ContactViewDev v{V.point.p, V.normal.p, V.overlap.p, V.en.p, V.es.p, V.spring.p, V.master.p, V.slave.p};
+        const long long max_key = (s->n_nodes + 1) << 32;
+        fd::launch_contact_view(L.view(), V.keys.p, V.order.p, V.skey.p, V.key_b.p, V.idx_b.p, V.bcount.p, V.bscan.p,
+                                n, max_key, v, s->stream);
+        FD_CUDA(cudaStreamSynchronize(s->stream));
+        FD_CUDA(cudaGetLastError());
+        out->point = V.point.p; out->normal = V.normal.p; out->overlap = V.overlap.p;
+        out->normal_energy = V.en.p; out->sliding_energy = V.es.p; out->spring = V.spring.p;
+        out->master = V.master.p; out->slave = V.slave.p; out->n = n;
+    });
+}
+
+int fundem_bond_view_get(fundem_sim* s, fundem_bond_view* out)
+{
+    if (!s || !out) return FUNDEM_ERR_ARG;
+    *out = fundem_bond_view{};
+    if (!s->setup_done) return FUNDEM_OK;
+    return guard(s, [&] {
+        fd::BondDev bd = s->bond_view();
+        const size_t m = (size_t)std::max(bd.n, 1);
+        if (s->bview_B.n < 4 * m) {
+            s->bview_B.alloc(4 * m, false);
+            s->bview_energy.alloc(6 * m, false);
+            s->bview_frames.alloc(8 * m, false);
+        }
+        fd::BondViewDev v{};
+        for (int t = 0; t < 4; ++t) v.B[t] = s->bview_B.p + t * m;
+        for (int t = 0; t < 6; ++t) v.energy[t] = s->bview_energy.p + t * m;
+        for (int t = 0; t < 8; ++t) v.frames[t] = s->bview_frames.p + t * m;
+        fd::launch_bond_view(bd, v, s->stream);
+        FD_CUDA(cudaStreamSynchronize(s->stream));
+        FD_CUDA(cudaGetLastError());
+        BondHost& B = s->bonds;
+        out->master = B.d_master.p; out->slave = B.d_slave.p; out->activated = B.d_active.p;
+        out->center_point = (double*)B.d_point.p; out->radius = B.d_radius.p; out->initial_length = B.d_L0.p;
+        out->B1 = v.B[0]; out->B2 = v.B[1]; out->B3 = v.B[2]; out->B4 = v.B[3];
+        out->Un = v.energy[0]; out->Us = v.energy[1]; out->Ub = v.energy[2]; out->Ut = v.energy[3];
+        out->max_normal_stress = v.energy[4]; out->max_shear_stress = v.energy[5];
+        out->tensile_strength = B.d_ts.p; out->cohesion = B.d_coh.p; out->friction = B.d_mu.p;
+        for (int t = 0; t < 8; ++t) out->frames[t] = (double*)v.frames[t];
+        out->n = bd.n;
     });
 }
 

@@ -2376,6 +2376,43 @@ static inline void note_launch()
 }
 
 // ---------------------------------------------------------------------------
+// contiguous views of a contact list and of the bonds (the device arrays the
+// reference's SolidInteraction and VBondedInteraction getters return)
+// ---------------------------------------------------------------------------
+__global__ void k_view_keys(PairListDev L, long long* key)
+{
+    const int nslots = min(*L.n_slots, L.cap_contacts);
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < L.cap_contacts; s += gridDim.x * blockDim.x) {
+        const int node = s < nslots ? L.c_node[s] : -1;
+        key[s] = node >= 0 ? ((long long)node << 32) | (unsigned int)L.c_slave[s] : -1ll;
+    }
+}
+__global__ void k_view_gather(PairListDev L, const int* order, long long n, ContactViewDev v)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int s = order[i];
+        v.master[i] = L.c_node[s];
+        v.slave[i] = L.c_slave[s];
+        for (int d = 0; d < 3; ++d) {
+            v.point[3 * i + d] = L.c_point[3 * s + d];
+            v.normal[3 * i + d] = L.c_normal[3 * s + d];
+            v.spring[3 * i + d] = L.c_spring[3 * s + d];
+        }
+        v.overlap[i] = L.c_overlap[s];
+        v.en[i] = L.c_en[s];
+        v.es[i] = L.c_es[s];
+    }
+}
+__global__ void k_bond_view(BondDev B, BondViewDev v)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= B.n) return;
+    for (int t = 0; t < 4; ++t) v.B[t][k] = B.B[4 * k + t];
+    for (int t = 0; t < 6; ++t) v.energy[t][k] = B.energy[6 * k + t];
+    for (int t = 0; t < 8; ++t) v.frames[t][k] = B.frames[8 * k + t];
+}
+
+// ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
 size_t scan_tmp_size(long long n)
@@ -2632,6 +2669,20 @@ void launch_bonds(const ObjDev& P, BondDev& B, bool mixed, cudaStream_t s)
     if (B.n <= 0) return;
     if (mixed) { k_bonds32<<<nblocks(B.n), TPB, 0, s>>>(P, B); note_launch(); }
     else k_bonds<<<nblocks(B.n), TPB, 0, s>>>(P, B); note_launch();
+}
+
+void launch_contact_view(const PairListDev& L, long long* keys, int* order, unsigned long long* skey,
+                         unsigned long long* key_b, int* idx_b, int* bcount, int* bscan, long long n,
+                         long long max_key, const ContactViewDev& v, cudaStream_t s)
+{
+    if (L.cap_contacts <= 0) return;
+    k_view_keys<<<148 * 4, TPB, 0, s>>>(L, keys); note_launch();
+    radix_sort_keys(keys, L.cap_contacts, max_key, skey, order, key_b, idx_b, bcount, bscan, s);
+    if (n > 0) { k_view_gather<<<148 * 4, TPB, 0, s>>>(L, order, n, v); note_launch(); }
+}
+void launch_bond_view(const BondDev& B, const BondViewDev& v, cudaStream_t s)
+{
+    if (B.n > 0) { k_bond_view<<<nblocks(B.n), TPB, 0, s>>>(B, v); note_launch(); }
 }
 
 void launch_reduce(ObjDev& P, PairListDev* lists, const int* active, const RevDev& R, const BondDev& B, bool mixed,

@@ -245,6 +245,24 @@ struct StepArgs {
     unsigned long long* stats;  // optional: pairs, clusters, clusters kept, contacts (narrow kernels)
 };
 
+// contiguous copy of a list's contacts, in (node, partner) order
+struct ContactViewDev {
+    double* point;     // 3 per contact
+    double* normal;    // 3 per contact
+    double* overlap;
+    double* en;
+    double* es;
+    double* spring;    // 3 per contact
+    int* master;       // global boundary node
+    int* slave;        // partner
+};
+// the bonds' interleaved per-bond parameters and state as one array per field
+struct BondViewDev {
+    double* B[4];       // B1 .. B4
+    double* energy[6];  // Un, Us, Ub, Ut, maximum normal stress, maximum shear stress
+    double3* frames[8]; // master n1 n2 n3 point, slave n1 n2 n3 point (body frames)
+};
+
 // integration and hashing
 void launch_kick(const ObjDev& P, const GeoSetDev& G, double3 gravity, double h, cudaStream_t s);
 void launch_drift(const ObjDev& O, double dt, cudaStream_t s);
@@ -303,6 +321,12 @@ void launch_reverse(const ObjDev& P, PairListDev* lists, const int* active, RevD
 void launch_bonds(const ObjDev& P, BondDev& B, bool mixed, cudaStream_t s);
 void launch_reduce(ObjDev& P, PairListDev* lists, const int* active, const RevDev& R, const BondDev& B, bool mixed,
                    cudaStream_t s);
+// the n contacts of a list (keys and sort scratch of the list's slot
+// capacity; max_key bounds node << 32 | partner) into the view
+void launch_contact_view(const PairListDev& L, long long* keys, int* order, unsigned long long* skey,
+                         unsigned long long* key_b, int* idx_b, int* bcount, int* bscan, long long n,
+                         long long max_key, const ContactViewDev& v, cudaStream_t s);
+void launch_bond_view(const BondDev& B, const BondViewDev& v, cudaStream_t s);
 
 // Kernel launches of the calling thread are counted into *c (null: not
 // counted); the library points it at the calling simulation's counter for

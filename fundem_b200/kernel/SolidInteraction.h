@@ -40,7 +40,26 @@ public:
     const std::vector<double> contactOverlapHostRef() { download(); return overlap_; }
     const std::vector<double3> slidingSpringHostRef() { download(); return spring_; }
 
+    // device pointers (kernel/SolidInteraction.h:323-330 of the reference):
+    // contiguous copies of the list's contacts in (node, partner) order, a
+    // read-only snapshot refreshed by each call, valid until the next step
+    double3* contactPoint() { return reinterpret_cast<double3*>(view().point); }
+    double3* contactNormal() { return reinterpret_cast<double3*>(view().normal); }
+    double* contactOverlap() { return view().overlap; }
+    double* normalElasticEnergy() { return view().normal_energy; }
+    double* slidingElasticEnergy() { return view().sliding_energy; }
+    double3* slidingSpring() { return reinterpret_cast<double3*>(view().spring); }
+    int* masterID() { return view().master; }
+    int* slaveID() { return view().slave; }
+
 private:
+    fundem_contact_view view()
+    {
+        fundem_contact_view v{};
+        if (sim_) fundem_detail::check(fundem_contact_view_get(sim_, kind_, &v), "contact_view_get");
+        return v;
+    }
+
     fundem_sim* sim_ = nullptr;
     int kind_;
     std::vector<int> master_, slave_;

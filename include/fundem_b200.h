@@ -218,6 +218,46 @@ int fundem_device_view_get(fundem_sim* sim, int wall, fundem_device_view* out);
 int fundem_num_contacts(fundem_sim* sim, int kind, long long* n);
 int fundem_get_contacts(fundem_sim* sim, int kind, int* node, int* partner, double* point, double* normal,
                         double* overlap, double* spring, double* en, double* es);
+/* Device pointers of one list's contacts, as SolidInteraction's getters hand
+   them out (contactPoint(), contactNormal(), contactOverlap(),
+   normalElasticEnergy(), slidingElasticEnergy(), slidingSpring(),
+   masterID(), slaveID(), numPair_device(): kernel/SolidInteraction.h:323-334):
+   the contacts are copied into contiguous arrays owned by the simulation, in
+   (node, partner) order, n of them.  A read-only snapshot: valid until the
+   next step or view call on the simulation; point, normal, overlap and the
+   energies are filled for steps run with full records. */
+typedef struct {
+    double* point;           /* 3 per contact */
+    double* normal;          /* 3 per contact */
+    double* overlap;
+    double* normal_energy;
+    double* sliding_energy;
+    double* spring;          /* 3 per contact */
+    int* master;             /* global boundary-node index */
+    int* slave;              /* partner object */
+    long long n;
+} fundem_contact_view;
+int fundem_contact_view_get(fundem_sim* sim, int kind, fundem_contact_view* out);
+/* Device pointers of the bonds, as VBondedInteraction's getters hand them out
+   (kernel/VBondedInteraction.h:452-485): ids, activation, centre point,
+   radius and initial length point at the library's own arrays; the
+   beam stiffnesses, energies, stresses and body-frame vectors are copied
+   into one array per field.  The copies are a snapshot, valid until the
+   next step or view call. */
+typedef struct {
+    int* master;
+    int* slave;
+    int* activated;
+    double* center_point;    /* 3 per bond */
+    double* radius;
+    double* initial_length;
+    double *B1, *B2, *B3, *B4;
+    double *Un, *Us, *Ub, *Ut, *max_normal_stress, *max_shear_stress;
+    double *tensile_strength, *cohesion, *friction;
+    double* frames[8];       /* 3 per bond: master n1 n2 n3 point, slave n1 n2 n3 point (body frames) */
+    int n;
+} fundem_bond_view;
+int fundem_bond_view_get(fundem_sim* sim, fundem_bond_view* out);
 /* replace the history (previous step's list) of one kind */
 int fundem_set_contacts(fundem_sim* sim, int kind, long long n, const int* node, const int* partner,
                         const double* spring);

@@ -55,3 +55,17 @@ def test_hook_force_cancels_gravity(app):
     assert abs(v[2] + 0.5 * g * dt) < 1e-12
     assert abs(v[0]) < 1e-15 and abs(v[1]) < 1e-15
     assert abs(x[2] - (h0 - steps * dt * 0.5 * g * dt)) < 1e-12
+
+
+def test_device_getters_from_a_hook(tmp_path):
+    """SolidInteraction's and VBondedInteraction's device getters
+    (contactPoint(), masterID(), slaveID(), slidingSpring(),
+    contactOverlap(), activated(), B1(), Un(), the bond frames, ...) read
+    inside an addExternalForceTorque hook hold the same contacts and bonds as
+    the host getters (tests/apps/view_check.cpp), at every step."""
+    from fundem_b200 import build
+    exe = build.build_app([os.path.join(APPS, "view_check.cpp")], str(tmp_path / "view_check"))
+    r = subprocess.run([exe, str(tmp_path / "out")], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.split()[-3:-1] == ["views", "ok"]
+    assert int(r.stdout.split()[-1]) > 100
