@@ -16,6 +16,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <filesystem>
 #include <fstream>
 #include <iostream>
 #include <sstream>
@@ -229,8 +230,6 @@ public:
     void solve(const double3 minDomain, const double3 maxDomain, const double3 gravity, const double timeStep,
                const double maximumTime, const size_t numFrame, const int argc, char** argv)
     {
-        (void)argc;
-        (void)argv;
         if (!sim_) return;
         if (!(timeStep > 0.0) || !(maximumTime > 0.0) || !(minDomain.x < maxDomain.x) ||
             !(minDomain.y < maxDomain.y) || !(minDomain.z < maxDomain.z)) {
@@ -238,6 +237,8 @@ public:
             return;
         }
         phase_ += 1;
+        resolveDir(argc > 0 ? argv[0] : nullptr);
+        clearFrames();
         if (!report(fundem_setup(sim_, &minDomain.x, &maxDomain.x), "solve: setup")) return;
         LSParticle_.bind(sim_, maxGPUThread_);
         Wall_.bind(sim_, maxGPUThread_);
@@ -309,6 +310,45 @@ private:
         N[id] = nodes;
         T[id] = triangles;
         return id;
+    }
+
+    // a relative output name lives beside the executable: under the nearest
+    // ancestor directory named "build", else in the executable's own
+    // directory (LSSolver.h:615-644); an absolute name is kept
+    void resolveDir(const char* exe)
+    {
+        namespace fs = std::filesystem;
+        const fs::path name(dir_);
+        if (name.is_absolute()) return;
+        if (exe == nullptr) {
+            dir_ = (fs::current_path() / name).string();
+            return;
+        }
+        const fs::path here = fs::weakly_canonical(fs::absolute(fs::path(exe))).parent_path();
+        fs::path base = here;
+        for (fs::path d = here; !d.empty(); d = d.parent_path()) {
+            if (d.filename() == "build") {
+                base = d;
+                break;
+            }
+            if (d == d.parent_path()) break;
+        }
+        dir_ = (base / name).string();
+    }
+
+    // frames of an earlier run of the same phase are removed before the
+    // first frame is written (LSSolver.h:678-690)
+    void clearFrames()
+    {
+        namespace fs = std::filesystem;
+        const std::string dir = dir_ + "_phase" + std::to_string(phase_);
+        for (const char* sub : {"/LSParticle", "/LSParticleInteraction", "/Wall", "/LSParticle-WallInteraction"}) {
+            std::error_code ec;
+            const fs::path d(dir + sub);
+            if (!fs::is_directory(d, ec)) continue;
+            for (const fs::directory_entry& e : fs::directory_iterator(d, ec))
+                if (e.is_regular_file(ec) && e.path().extension() == ".vtu") fs::remove(e.path(), ec);
+        }
     }
 
     // the frame files of LSSolver::output (LSSolver.h:717-744), in

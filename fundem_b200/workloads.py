@@ -266,11 +266,16 @@ def bonded_column(n=262144, footprint=(128, 128), seed=1, pitch=2.42e-3, jitter=
 
 
 def adjoint_pour(n=4096, seed=0, n_templates=2, box=(40e-3, 40e-3, 80e-3), pitch=2.8e-3, dt=1e-6,
-                 overlap_tol=2e-6, device=0, log=None):
+                 overlap_tol=2e-6, settle_steps=0, settle_dt=5e-6, settle_ke_frac=1e-3, device=0, log=None):
     """The adjoint workload: n superellipsoids (the small pour's distributions,
     2 templates, 32^3 SDFs, 642 nodes) on a jittered lattice in a box of six
     plane walls, dt = 1e-6 s, orientations re-drawn on the GPU until no
-    overlap exceeds overlap_tol.  Returns (Simulation, Scenario)."""
+    overlap exceeds overlap_tol.  With settle_steps > 0 the lattice is then
+    poured (the library's own steps under gravity at settle_dt, untimed)
+    until its kinetic energy falls below settle_ke_frac of the fall's peak
+    or settle_steps, and the scenario carries the settled state, so that a
+    window started from it is full of particle and wall contacts.  Returns
+    (Simulation, Scenario)."""
     from . import Simulation
     sc = S.pour(n=n, n_templates=n_templates, seed=seed, box=box, pitch=pitch, dt=dt, explicit_mass=True,
                 resolve=False, name="adjoint_pour")
@@ -282,4 +287,11 @@ def adjoint_pour(n=4096, seed=0, n_templates=2, box=(40e-3, 40e-3, 80e-3), pitch
     sim.set_state(quat=quat, pos=pos)
     sim.set_records(False)
     sim.detect()
+    if settle_steps > 0:
+        masses = np.array([g.mass for g in sc.particle_geometries])[sc.particles.geo]
+        rec = settle(sim, masses, settle_dt, settle_steps, ke_frac=settle_ke_frac, log=log)
+        st = sim.state()
+        sc.particles.pos, sc.particles.vel = st["pos"].copy(), st["vel"].copy()
+        sc.particles.angvel, sc.particles.quat = st["angvel"].copy(), st["quat"].copy()
+        sc.settle = {k: rec[k] for k in ("steps", "dt", "settled", "kinetic_energy", "kinetic_energy_peak")}
     return sim, sc

@@ -40,6 +40,7 @@ class ReverseRun(TangentRun):
 
     def __init__(self, sc):
         super().__init__(sc, [])
+        assert not self.turning, "the reverse reference differentiates translating bodies only"
         self.tape = []
 
     def _step(self):
@@ -79,7 +80,7 @@ class ReverseRun(TangentRun):
         sprev = seed(sp_val, 6)
         par = [Dual(v, np.broadcast_to(eye[:, 9 + k][:, None], (nd, m)).copy())
                for k, v in enumerate((S.kn, S.ks, S.diss, S.mu))]
-        F, snew, ok = self._contact_eval(S, rel, vc, sprev, *par)
+        F, snew, ok, _, _ = self._contact_eval(S, rel, vc, sprev, *par)
         J = np.concatenate([F.derivs(), snew.derivs()], axis=2)  # (13, m, 6)
         J[:, ~ok, :] = 0.0
         return {"kind": kind, "A": S.A, "j": S.j, "wall": S.wall, "react": S.react, "hist": S.hist, "J": J,

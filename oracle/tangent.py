@@ -12,13 +12,19 @@ derivatives of positions, velocities, forces and sliding springs along a set
 of directions: one material's kn, ks, damping ratio or friction coefficient,
 or a change of the initial velocities.  The derivative is the one an adjoint
 of the frozen-topology step computes: the contact lists, history links,
-stick/slip branches and bond breakage of each step are the oracle's, and
-bodies translate only (zero inverse inertia; a constant angular velocity is
-allowed and enters the contact velocity).
+stick/slip branches and bond breakage of each step are the oracle's.
+Bodies may turn (nonzero inverse inertia): orientations, angular velocities
+and torques then carry derivatives too, through the world-frame inertia of
+the kicks, the normalised quaternion step and the lever arms of the contact
+torques; runs with turning bodies have no bonds (the GPU adjoint refuses
+that combination as well).
 
 Equations, following the reference step (LSSolver.h:1033-1107):
   v_h     = v_n + (F_n / m + g) dt / 2          (skipped when 1/m is zero)
+  w_h     = w_n + I_w^-1 (T_n - w_n x I_w w_n) dt / 2,  I_w = R(q_n) I R(q_n)^T
+            (particleIntegrationKernel.cu:3-32, myMat.h:107-158)
   x_{n+1} = x_n + v_h dt
+  q_{n+1} = normalise(q_n + (0, w_h dt / 2) (x) q_n)   (myQua.h:77-93)
   contacts (contactKernel.cu:46-291, contactKernel.cuh:4-77): for a node of
     A at gp inside partner B (centre r_B, orientation q_B),
       rel = gp - r_B, local = R(q_B)^T rel, trilinear SDF value phi and the
@@ -27,10 +33,13 @@ Equations, following the reference step (LSSolver.h:1033-1107):
       overlap = -phi, contact point c = gp + n overlap / 2
       (LSParticleContactDetectionKernel.cu:268-281),
       v_c = v_A + w_A x (c - r_A) - v_B - w_B x (c - r_B),
-      linear spring-dashpot normal force, sliding spring with Coulomb limit;
+      linear spring-dashpot normal force, sliding spring with Coulomb limit,
+      torques (c - r_A) x F on A and (c - r_B) x (-F) on B, where the node
+      gp = x_A + R(q_A) node moves with A's orientation;
   bonds (contactKernel.cuh:138-199): F = B1 (D - L0) e
     + B2 / (2 D) (dn - (dn . e) e), e = -(rb_i - rb_j) / D;
-  v_{n+1} = v_h + (F_{n+1} / m + g) dt / 2.
+  v_{n+1} = v_h + (F_{n+1} / m + g) dt / 2,  w_{n+1} likewise from T_{n+1}
+            at q_{n+1}.
 The damping ratio comes from the restitution coefficient as the reference
 forms it (contactKernel.cuh:49-51), in double precision here.  The effective
 parameters of a contact (harmonic-mean stiffness, minimum friction and
@@ -169,6 +178,61 @@ def rotation(q):
     return R
 
 
+def dquat(q, dq):
+    """Quaternions (n, 4) with derivatives (ND, n, 4) as four duals."""
+    return [Dual(q[:, c], dq[:, :, c]) for c in range(4)]
+
+
+def drotation(qd):
+    """Rotation matrix (rows of duals) of dual unit quaternions, as rotation()."""
+    q0, q1, q2, q3 = qd
+    return [[1.0 - 2.0 * (q2 * q2 + q3 * q3), 2.0 * (q1 * q2 - q0 * q3), 2.0 * (q1 * q3 + q0 * q2)],
+            [2.0 * (q1 * q2 + q0 * q3), 1.0 - 2.0 * (q1 * q1 + q3 * q3), 2.0 * (q2 * q3 - q0 * q1)],
+            [2.0 * (q1 * q3 - q0 * q2), 2.0 * (q2 * q3 + q0 * q1), 1.0 - 2.0 * (q1 * q1 + q2 * q2)]]
+
+
+def matvec(M, a):
+    return V3(M[0][0] * a.x + M[0][1] * a.y + M[0][2] * a.z,
+              M[1][0] * a.x + M[1][1] * a.y + M[1][2] * a.z,
+              M[2][0] * a.x + M[2][1] * a.y + M[2][2] * a.z)
+
+
+def vcross(a, b):
+    """a x b for two V3s."""
+    return V3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x)
+
+
+def sym3(I6):
+    """Symmetric tensors stored (xx, yy, zz, xy, xz, yz), (n, 6) -> (n, 3, 3)."""
+    I6 = np.asarray(I6, float).reshape(-1, 6)
+    xx, yy, zz, xy, xz, yz = I6.T
+    return np.stack([np.stack([xx, xy, xz], 1), np.stack([xy, yy, yz], 1), np.stack([xz, yz, zz], 1)], 1)
+
+
+def world_tensor(R, I):
+    """R I R^T for a dual rotation R and constant tensors I (n, 3, 3)."""
+    T = [[sum(R[a][c] * I[:, c, d] for c in range(3)) for d in range(3)] for a in range(3)]
+    return [[sum(T[a][d] * R[b][d] for d in range(3)) for b in range(3)] for a in range(3)]
+
+
+def dquat_integrate(qd, w, dt):
+    """The quaternion step of myQua.h:77-93 on duals: q + (0, w dt / 2) (x) q,
+    normalised."""
+    q0, q1, q2, q3 = qd
+    vx, vy, vz = w.x * (0.5 * dt), w.y * (0.5 * dt), w.z * (0.5 * dt)
+    s0 = q0 + ((-q1) * vx - q2 * vy - q3 * vz)
+    s1 = q1 + (q0 * vx + q3 * vy - q2 * vz)
+    s2 = q2 + ((-q3) * vx + q0 * vy + q1 * vz)
+    s3 = q3 + (q2 * vx - q1 * vy + q0 * vz)
+    inv = 1.0 / dsqrt(s0 * s0 + s1 * s1 + s2 * s2 + s3 * s3)
+    return [s0 * inv, s1 * inv, s2 * inv, s3 * inv]
+
+
+def _stack(parts):
+    """Derivatives of a list of duals, stacked on a last axis: (ND, n, k)."""
+    return np.stack([p.d for p in parts], axis=2)
+
+
 class _GeoTable:
     """SDF grids of a geometry set, concatenated."""
 
@@ -190,14 +254,16 @@ class TangentRun:
     """The oracle's run of a scenario with derivatives along
     4 * (particle materials) parameter directions (kn, ks, damping ratio and
     friction of each material, in that order) followed by one direction per
-    initial-velocity change in `vel_dirs` (each an (N, 3) array).
+    initial-velocity change in `vel_dirs` (each an (N, 3) array), then one
+    per initial angular-velocity change in `angvel_dirs`.
 
-    After step(T), directional(dl_dpos, dl_dvel) gives d L / d direction for
-    L = sum(dl_dpos * x_T) + sum(dl_dvel * v_T): the four material gradients
-    and the projections of d L / d v_0 on the velocity directions, which an
-    adjoint gives in one backward sweep."""
+    After step(T), directional(dl_dpos, dl_dvel, dl_dquat, dl_dangvel) gives
+    d L / d direction for L = sum(dl_dpos * x_T) + sum(dl_dvel * v_T)
+    + sum(dl_dquat * q_T) + sum(dl_dangvel * w_T): the four material
+    gradients and the projections of d L / d v_0 and d L / d w_0 on the
+    directions, which an adjoint gives in one backward sweep."""
 
-    def __init__(self, sc, vel_dirs=()):
+    def __init__(self, sc, vel_dirs=(), angvel_dirs=()):
         assert not getattr(sc, "periodic_sector", False), "sector images are not differentiated"
         self.sc = sc
         self.o = OracleWorld.from_scenario(sc)
@@ -212,8 +278,13 @@ class TangentRun:
         counts = np.array([len(geos[g]["nodes"]) for g in self.geo])
         self.node_pid = np.repeat(np.arange(n), counts)
         self.inv_mass = np.array([self.o.geometry(int(g))["inv_mass"] for g in self.geo])
-        for g in range(len(geos)):
-            assert not np.any(self.o.geometry(g)["inv_inertia"]), "bodies must translate only"
+        gp = [self.o.geometry(g) for g in range(len(geos))]
+        self.inertia = sym3([g["inertia"] for g in gp])
+        self.inv_inertia = sym3([g["inv_inertia"] for g in gp])
+        self.turning = bool(np.any(self.inv_inertia[np.unique(self.geo)]))
+        assert not (self.turning and len(sc.bonds)), "bonds between turning bodies are not differentiated"
+        # body-frame node offsets, indexed by global boundary-node index
+        self.node_local = np.concatenate([np.asarray(geos[g]["nodes"], float).reshape(-1, 3) for g in self.geo])
         # materials as the oracle stores them (orc_add_material's clamps)
         pm = np.array(sc.particle_materials, float).reshape(-1, 4)
         self.kn = np.where(pm[:, 0] > 0, pm[:, 0], 0.0)
@@ -227,12 +298,18 @@ class TangentRun:
         self.wall_mat = np.asarray(sc.walls.mat, np.int64)
         self.nmat = len(pm)
         self.np_dirs = 4 * self.nmat
-        self.nd = nd = self.np_dirs + len(vel_dirs)
+        self.nd = nd = self.np_dirs + len(vel_dirs) + len(angvel_dirs)
         self.dx = np.zeros((nd, n, 3))
         self.dv = np.zeros((nd, n, 3))
+        self.dw = np.zeros((nd, n, 3))
+        self.dq = np.zeros((nd, n, 4))
         for k, r in enumerate(vel_dirs):
             self.dv[self.np_dirs + k] = np.asarray(r, float).reshape(n, 3)
+        for k, r in enumerate(angvel_dirs):
+            self.dw[self.np_dirs + len(vel_dirs) + k] = np.asarray(r, float).reshape(n, 3)
         self.dF = np.zeros((nd, n, 3))
+        self.dT = np.zeros((nd, n, 3))
+        self.max_quat_dev = 0.0     # recomputed orientations against the oracle's
         grid = self.o.grid()
         span = grid["max"] - grid["min"]
         # ghost images sit one period above the domain (ghost_positions)
@@ -259,33 +336,70 @@ class TangentRun:
         for _ in range(steps):
             self._step()
 
+    def _kick_w(self, st, dq, dw, dT, h):
+        """Derivative of the angular half-kick w + I_w^-1 (T - w x I_w w) h,
+        I_w = R(q) I R(q)^T (particleIntegrationKernel.cu:3-32), at the
+        state `st`; bodies with zero inverse mass take no kick."""
+        if not self.turning:
+            return dw
+        R = drotation(dquat(st["quat"], dq))
+        w = v3(st["angvel"], dw)
+        Iw = world_tensor(R, self.inertia[self.geo])
+        Ii = world_tensor(R, self.inv_inertia[self.geo])
+        acc = matvec(Ii, v3(st["torque"], dT) - vcross(w, matvec(Iw, w)))
+        kicked = (self.inv_mass != 0.0)[None, :, None]
+        return np.where(kicked, dw + h * acc.derivs(), dw)
+
     def _step(self):
         o, dt = self.o, float(self.sc.dt)
         kick = np.where(self.inv_mass != 0.0, 0.5 * dt * self.inv_mass, 0.0)[None, :, None]
+        st0 = o.state() if self.turning else None
         dvh = self.dv + self.dF * kick
+        dwh = self._kick_w(st0, self.dq, self.dw, self.dT, 0.5 * dt)
         self.dx = self.dx + dvh * dt
         o.front()
+        if self.turning:
+            st1 = o.state()
+            qn = dquat_integrate(dquat(st0["quat"], self.dq), v3(st1["angvel"], dwh), dt)
+            self.dq = _stack(qn)
+            qv = np.stack([c.v for c in qn], axis=1)
+            self.max_quat_dev = max(self.max_quat_dev, float(np.abs(qv - st1["quat"]).max()))
         active = o.bonds()["activated"].copy() if len(self.bond_L0) else np.zeros(0, np.int32)
         o.detect_and_force()
         P, W = o.state(), o.state(wall=True)
         dF = np.zeros_like(self.dF)
-        self.lists = {kind: self._contacts(kind, o.contacts(kind), P, W, dvh, dF) for kind in self.kinds}
+        dT = np.zeros_like(self.dT)
+        self.lists = {kind: self._contacts(kind, o.contacts(kind), P, W, dvh, dwh, dF, dT) for kind in self.kinds}
         if len(self.bond_L0):
             self._bonds(active, P, dF)
         o.half_kick()
         self.dv = dvh + dF * kick
+        self.dw = self._kick_w(P, self.dq, dwh, dT, 0.5 * dt)
         self.dF = dF
+        self.dT = dT
 
-    def _contacts(self, kind, c, P, W, dvh, dF):
+    def _contacts(self, kind, c, P, W, dvh, dwh, dF, dT):
         nd = self.nd
         S = self._contact_setup(kind, c, P, W)
         if S is None:
             return ({}, c["spring"], np.zeros((nd, 0, 3)))
         A, j, wall, react, m = S.A, S.j, S.wall, S.react, S.m
-        # rel = gp - r_B: derivative dx_A - dx_B (zero for a particle's own
-        # image); walls do not move with the parameters
-        rel = v3(S.gp - S.rj, self.dx[:, A, :] - (0.0 if wall else self.dx[:, j, :]))
-        vc = v3(S.vc_val, dvh[:, A, :] - (0.0 if wall else dvh[:, j, :]))
+        # the node's offset from A's centre, R(q_A) node, turns with A
+        RA = drotation(dquat(P["quat"][A], self.dq[:, A, :]))
+        armA = matvec(RA, v3(self.node_local[c["master"]], np.zeros((nd, m, 3))))
+        S.armA_d = armA.derivs()
+        # partner orientation: particles (and their images) turn, walls do not
+        S.dqB = np.zeros((nd, m, 4)) if wall else self.dq[:, j, :]
+        # rel = gp - r_B: derivative dx_A + d(R(q_A) node) - dx_B (dx terms
+        # cancel for a particle's own image); walls do not move with the
+        # parameters
+        rel = v3(S.gp - S.rj, self.dx[:, A, :] - (0.0 if wall else self.dx[:, j, :]) + S.armA_d)
+        dvc = dvh[:, A, :] - (0.0 if wall else dvh[:, j, :])
+        if self.turning:
+            dvc = dvc + np.cross(dwh[:, A, :], (S.point - S.ri)[None])
+            if not wall:
+                dvc = dvc - np.cross(dwh[:, j, :], (S.point - S.rj)[None])
+        vc = v3(S.vc_val, dvc)
         pad = np.zeros((nd - self.np_dirs, m))
         Kn = Dual(S.kn, np.vstack([S.w_kn, pad]))
         Ks = Dual(S.ks, np.vstack([S.w_ks, pad]))
@@ -296,8 +410,13 @@ class TangentRun:
         has, hc = S.hist >= 0, np.where(S.hist >= 0, S.hist, 0)
         sp_val = np.where(has[:, None], spr_prev[hc] if len(spr_prev) else 0.0, 0.0)
         sp_der = np.where(has[None, :, None], dS_prev[:, hc, :] if dS_prev.shape[1] else 0.0, 0.0)
-        F, snew, ok = self._contact_eval(S, rel, vc, v3(sp_val, sp_der), Kn, Ks, Diss, Mu)
+        F, snew, ok, TA, TB = self._contact_eval(S, rel, vc, v3(sp_val, sp_der), Kn, Ks, Diss, Mu)
         Fd = np.where(ok[None, :, None], F.derivs(), 0.0)
+        if self.turning:
+            np.add.at(dT, (slice(None), A), np.where(ok[None, :, None], TA, 0.0))
+            if not wall:
+                TBd = np.where(ok[None, :, None], TB, 0.0)
+                np.add.at(dT, (slice(None), j[react]), TBd[:, react])
         Sd = np.where(ok[None, :, None], snew.derivs(), 0.0)
         Sv = np.where(ok[:, None], snew.value(), 0.0)
         scale = max(float(np.abs(c["spring"]).max()), 1e-300)
@@ -336,9 +455,11 @@ class TangentRun:
                 rj = rj + self.shift[kind]
             S.G, S.geoB = self.pgeo, self.geo[j]
         S.rj = rj
+        S.point = point
         # a contact with a particle's own periodic image has no reaction
         S.react = np.zeros(m, bool) if wall else (j != A) if ghost else np.ones(m, bool)
         ri, vi = P["pos"][A], P["vel"][A]
+        S.ri = ri
         S.wi = P["angvel"][A]
         S.vc_val = (vi + np.cross(S.wi, point - ri)) - (vj + np.cross(S.wj, point - rj))
         # effective parameters and their weights on the material directions
@@ -390,11 +511,16 @@ class TangentRun:
         """Force on A and new sliding spring of each contact as duals of the
         seeded node offset `rel`, contact velocity `vc` (its dependence on the
         contact point is added here), previous spring and parameters; also
-        the mask of contacts that carry a force."""
-        R = rotation(S.qB)
-        lx = rel.x * R[:, 0, 0] + rel.y * R[:, 1, 0] + rel.z * R[:, 2, 0]
-        ly = rel.x * R[:, 0, 1] + rel.y * R[:, 1, 1] + rel.z * R[:, 2, 1]
-        lz = rel.x * R[:, 0, 2] + rel.y * R[:, 1, 2] + rel.z * R[:, 2, 2]
+        the mask of contacts that carry a force and the derivatives of the
+        torques on A and B (None when no body turns)."""
+        if self.turning:
+            R = drotation(dquat(S.qB, S.dqB))
+        else:
+            Rc = rotation(S.qB)
+            R = [[Rc[:, a, b] for b in range(3)] for a in range(3)]
+        lx = rel.x * R[0][0] + rel.y * R[1][0] + rel.z * R[2][0]
+        ly = rel.x * R[0][1] + rel.y * R[1][1] + rel.z * R[2][1]
+        lz = rel.x * R[0][2] + rel.y * R[1][2] + rel.z * R[2][2]
         G = S.G
         org, ih, sz, off = G.origin[S.geoB], G.inv_h[S.geoB], G.size[S.geoB], G.off[S.geoB]
         gx, gy, gz = (lx - org[:, 0]) * ih, (ly - org[:, 1]) * ih, (lz - org[:, 2]) * ih
@@ -420,9 +546,9 @@ class TangentRun:
               (p[7] - p[6]) * (fy * fz)
         ggy = (p[2] - p[0]) * uz + (p[6] - p[4]) * fz
         ggz = (p[4] - p[0]) * uy + (p[6] - p[2]) * fy
-        nw = V3(ggx * R[:, 0, 0] + ggy * R[:, 0, 1] + ggz * R[:, 0, 2],
-                ggx * R[:, 1, 0] + ggy * R[:, 1, 1] + ggz * R[:, 1, 2],
-                ggx * R[:, 2, 0] + ggy * R[:, 2, 1] + ggz * R[:, 2, 2])
+        nw = V3(ggx * R[0][0] + ggy * R[0][1] + ggz * R[0][2],
+                ggx * R[1][0] + ggy * R[1][1] + ggz * R[1][2],
+                ggx * R[2][0] + ggy * R[2][1] + ggz * R[2][2])
         nl = dsqrt(nw.dot(nw))
         n = V3(nw.x / nl, nw.y / nl, nw.z / nl)
         # contact velocity: c - r_A moves with n overlap / 2, c - r_B with rel
@@ -430,9 +556,19 @@ class TangentRun:
         h = n.scale(0.5 * ov)
         hd = V3(deriv(h.x.d), deriv(h.y.d), deriv(h.z.d))
         reld = V3(deriv(rel.x.d), deriv(rel.y.d), deriv(rel.z.d))
+        if getattr(S, "armA_d", None) is not None:
+            vc = vc + cross_const(S.wi, v3(np.zeros((S.m, 3)), S.armA_d))
         vc = vc + cross_const(S.wi, hd) - cross_const(S.wj, reld + hd)
         F, snew = self._law(sprev, vc, n, ov, Kn, Ks, Diss, Mu, S.meff, float(self.sc.dt))
-        return F, snew, inside & (ov.v > 0.0)
+        TA = TB = None
+        if self.turning:
+            # lever arms c - r_A and c - r_B: values from the oracle's contact
+            # point, derivatives through the node's turn, rel and n ov / 2
+            armA = v3(S.point - S.ri, S.armA_d + h.derivs())
+            armB = v3(S.point - S.rj, rel.derivs() + h.derivs())
+            TA = vcross(armA, F).derivs()
+            TB = vcross(armB, F.scale(-1.0)).derivs()
+        return F, snew, inside & (ov.v > 0.0), TA, TB
 
     @staticmethod
     def _law(sprev, vc, n, ov, kn, ks, diss, mu, m, dt):
@@ -484,9 +620,15 @@ class TangentRun:
         np.add.at(dF, (slice(None), j), -Fd)
 
     # -- results --------------------------------------------------------------
-    def directional(self, dl_dpos, dl_dvel):
-        """d L / d direction for L = sum(dl_dpos * x_T) + sum(dl_dvel * v_T)."""
-        return np.einsum("dnc,nc->d", self.dx, dl_dpos) + np.einsum("dnc,nc->d", self.dv, dl_dvel)
+    def directional(self, dl_dpos, dl_dvel, dl_dquat=None, dl_dangvel=None):
+        """d L / d direction for L = sum(dl_dpos * x_T) + sum(dl_dvel * v_T)
+        + sum(dl_dquat * q_T) + sum(dl_dangvel * w_T)."""
+        out = np.einsum("dnc,nc->d", self.dx, dl_dpos) + np.einsum("dnc,nc->d", self.dv, dl_dvel)
+        if dl_dquat is not None:
+            out = out + np.einsum("dnc,nc->d", self.dq, dl_dquat)
+        if dl_dangvel is not None:
+            out = out + np.einsum("dnc,nc->d", self.dw, dl_dangvel)
+        return out
 
     def close(self):
         self.o.close()
