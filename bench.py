@@ -345,7 +345,13 @@ def run_fundem(args, rank, world, dist):
     # (minimum image across the periodic seams), then K timed steps each
     mixed = None if args.no_mixed else mixed_vs_fp64(sc, dev, args, dist, world)
     batched = None
-    if not args.no_batch and rank == 0:
+    if not args.no_batch and world > 1:
+        # every rank takes part (the sweep is split across them)
+        try:
+            batched = batched_sharded(args, rank, world, dist, dev)
+        except Exception as exc:  # an auxiliary figure: report, do not fail the run
+            batched = {"error": f"{type(exc).__name__}: {exc}"}
+    elif not args.no_batch and rank == 0:
         try:
             batched = batched_cost(args, dev)
         except Exception as exc:  # an auxiliary figure: report, do not fail the run
@@ -420,7 +426,9 @@ def run_fundem(args, rank, world, dist):
         "reference_gpu": ref_gpu,
         "narrow_work_per_step": {"pairs": wc[0] / wc_steps, "clusters": wc[1] / wc_steps,
                                  "clusters_kept": wc[2] / wc_steps, "node_contacts": wc[3] / wc_steps,
-                                 "exact_node_tests": wc[4] / wc_steps},
+                                 "exact_node_tests": wc[4] / wc_steps,
+                                 "cached_slots_tested": wc[5] / wc_steps,
+                                 "cached_slots_skipped_by_bound": wc[6] / wc_steps},
         "mixed": mixed,
         "adjoint": adjoint,
         "batched": batched,
@@ -701,6 +709,43 @@ def batched_cost(args, dev):
     except Exception as exc:  # an auxiliary figure: report, do not fail the run
         out["adjoint"] = {"error": f"{type(exc).__name__}: {exc}"}
     return out
+
+
+def batched_sharded(args, rank, world, dist, dev):
+    """The calibration sweep split across the ranks: whole simulations per
+    GPU, the costliest first (batch.shard by particles x steps); each rank
+    tiles its share into one simulation and runs args.batch_warmup untimed
+    and args.batch_steps timed steps.  The ranks exchange nothing while they
+    run; the results and each rank's device time (CUDA events) are gathered
+    at the end, and the job's time is the slowest rank's."""
+    import torch
+    from fundem_b200 import batch
+    scs, _ = batch.calibration_scenarios(n_sims=args.batch_sims, seed=1)
+
+    def timer():
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+
+        def stop():
+            e1.record()
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) / 1e3
+        return stop
+    res, secs, parts = batch.run_sharded_tiled(scs, args.batch_steps, rank, world, dist=dist, device=dev,
+                                               warmup=args.batch_warmup, timer=timer)
+    total = sum(len(sc.particles) for sc in scs)
+    t = max(secs)
+    return {"workload": "calibration sweep split across GPUs: whole simulations per rank, largest first, each "
+                        "rank's share tiled into one simulation",
+            "simulations": len(scs), "particles": total, "steps": args.batch_steps,
+            "warmup_steps": args.batch_warmup, "ranks": world,
+            "simulations_per_rank": [len(p) for p in parts],
+            "particles_per_rank": [int(sum(len(scs[i].particles) for i in p)) for p in parts],
+            "seconds_per_rank": secs, "job_s": t, "particle_steps_per_s": total * args.batch_steps / t,
+            "results_gathered": len(res),
+            "note": "strong scaling of a fixed sweep; no exchange while running (the per-simulation results "
+                    "are gathered once at the end)"}
 
 
 def main():

@@ -31,7 +31,7 @@ EXPORTS = [
     "fundem_device_view_get", "fundem_num_contacts", "fundem_get_contacts", "fundem_set_contacts",
     "fundem_num_pairs", "fundem_num_bonds", "fundem_get_bonds", "fundem_set_bond_activation",
     "fundem_get_geometry", "fundem_get_grid", "fundem_launch_count", "fundem_set_profiling",
-    "fundem_kernel_time", "fundem_work_counters", "fundem_prefix_sum", "fundem_prefix_sum_noalloc", "fundem_last_error",
+    "fundem_kernel_time", "fundem_work_counters", "fundem_slot_counters", "fundem_prefix_sum", "fundem_prefix_sum_noalloc", "fundem_last_error",
     "fundem_adjoint_begin", "fundem_adjoint_forward", "fundem_adjoint_backward", "fundem_adjoint_end",
     "fundem_step_graph", "fundem_set_neighbour_list", "fundem_checkpoint_write", "fundem_checkpoint_read",
     "fundem_levelset_grid", "fundem_set_periodic_sector", "fundem_set_inertia_mode",
@@ -113,6 +113,7 @@ def lib():
         L.fundem_set_profiling.argtypes = [P, I]
         L.fundem_kernel_time.argtypes = [P, I, C.POINTER(C.c_double), C.POINTER(LL)]
         L.fundem_work_counters.argtypes = [P, C.POINTER(C.c_ulonglong)]
+        L.fundem_slot_counters.argtypes = [P, C.POINTER(C.c_ulonglong)]
         L.fundem_prefix_sum.argtypes = [P, P, LL, P]
         L.fundem_prefix_sum_noalloc.argtypes = [P, P, LL, P]
         L.fundem_last_error.restype = C.c_char_p
@@ -570,10 +571,14 @@ class Simulation:
 
     def work_counters(self):
         """(pairs, clusters examined, clusters kept, node contacts, exact node
-        tests) since the last call."""
+        tests of the selection, slots given the exact predicate by the cached
+        predicate pass, slots it skipped by the slot bound) since the last
+        call."""
+        b = (C.c_ulonglong * 2)()
+        self._check(self.L.fundem_slot_counters(self.h, b), "slot_counters")
         a = (C.c_ulonglong * 5)()
         self._check(self.L.fundem_work_counters(self.h, a), "work_counters")
-        return tuple(int(x) for x in a)
+        return tuple(int(x) for x in a) + tuple(int(x) for x in b)
 
     def status_word(self):
         w = C.c_uint()

@@ -295,3 +295,48 @@ def run_sharded(scenarios, steps, chunk, rank, world, dist=None, device=0, summa
     for p in parts:
         out.update(p["results"])
     return out
+
+
+def run_sharded_tiled(scenarios, steps, rank, world, dist=None, device=0, warmup=0, timer=None, tiled_cls=None):
+    """This rank's share of `scenarios` (shard, by particles x steps) tiled
+    into one simulation (TiledBatch: one launch per stage for the whole
+    share): `warmup` untimed steps, then `steps` steps bracketed by
+    timer() calls when a timer is given (a callable returning a stop
+    callable that returns seconds).  The ranks exchange nothing while they
+    run; at the end the final mean particle height of every simulation and
+    each rank's seconds are gathered (all_gather_object).  Returns
+    ({simulation index: mean height}, [seconds per rank], [indices per
+    rank]).  A rank whose share fails still joins the gather, and every rank
+    then raises."""
+    tiled_cls = TiledBatch if tiled_cls is None else tiled_cls
+    parts = shard([len(sc.particles) * steps for sc in scenarios], world)
+    mine = parts[rank]
+    local, secs, error = {}, 0.0, None
+    try:
+        if mine:
+            tb = tiled_cls([scenarios[i] for i in mine], device=device)
+            try:
+                if warmup:
+                    tb.run(warmup)
+                stop = timer() if timer else None
+                tb.run(steps)
+                secs = stop() if stop else 0.0
+                for i, st in zip(mine, tb.states()):
+                    local[i] = float(st["pos"][:, 2].mean())
+            finally:
+                tb.close()
+    except Exception as exc:
+        if dist is None or world == 1:
+            raise
+        error = f"rank {rank}: {type(exc).__name__}: {exc}"
+    if dist is None or world == 1:
+        return local, [secs], parts
+    got = [None] * world
+    dist.all_gather_object(got, {"error": error, "results": local, "seconds": secs})
+    errors = [g["error"] for g in got if g["error"]]
+    if errors:
+        raise RuntimeError("sharded run failed: " + "; ".join(errors))
+    out = {}
+    for g in got:
+        out.update(g["results"])
+    return out, [g["seconds"] for g in got], parts

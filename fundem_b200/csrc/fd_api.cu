@@ -485,6 +485,7 @@ struct PairList {
     std::vector<int> up_node, up_partner;
     // slot and pair scratch of the current step only
     DevArray<int> c_pair, c_hit, p_hist_cnt;
+    DevArray<float> c_phi0;  // pair cache: slot bounds of the last rebuild
     DevArray<double> c_force;
     DevArray<int4> p_aux;
     bool allocated = false;
@@ -505,6 +506,7 @@ struct PairList {
             g.counters.alloc(3);
         }
         c_pair.alloc(cap_contacts); c_hit.alloc(cap_contacts, false); c_force.alloc((size_t)cap_contacts * 9);
+        c_phi0.alloc(cap_contacts, false);
         p_aux.alloc(cap_pairs); p_hist_cnt.alloc(cap_pairs);
         allocated = true;
     }
@@ -529,6 +531,7 @@ struct PairList {
             }
             c_pair.grow(capc, 0);
             c_hit.grow(capc, 0);
+            c_phi0.grow(capc, 0);  // rewritten by the rebuild a grow forces
             c_force.grow((size_t)capc * 9, 0);
             cap_contacts = capc;
         }
@@ -548,6 +551,7 @@ struct PairList {
         v.n_slots = c.counters.p + 1; v.n_hits = c.counters.p + 2; v.cap_contacts = cap_contacts;
         v.c_pair = c_pair.p; v.c_hit = c_hit.p; v.c_k = c.c_k.p; v.o_c_k = o.c_k.p; v.c_force = c_force.p; v.p_aux = p_aux.p; v.p_hist_cnt = p_hist_cnt.p;
         v.o_c_node = o.c_node.p; v.o_c_spring = o.c_spring.p;
+        v.c_phi0 = c_phi0.p;
         return v;
     }
 };
@@ -770,6 +774,7 @@ struct fundem_sim {
     DevArray<double3> pc_ref_pos;
     DevArray<fd_quat> pc_ref_q;
     DevArray<int> pc_ref_vis, pc_ctrl;
+    DevArray<float> pc_drift;
     int pc_mode = -1;          // -1: from the particle count, 0: off, 1: on
     double pc_skin_set = 0.0;  // <= 0: PC_SKIN * the largest bounding radius
     bool pc_on = false;
@@ -783,6 +788,7 @@ struct fundem_sim {
         if (!pc_on) return;
         const size_t m = std::max(P.n(), 1);
         pc_ref_pos.alloc(m); pc_ref_q.alloc(m); pc_ref_vis.alloc(m);
+        pc_drift.alloc(m, false);
         pc_ctrl.alloc(4);
     }
     double pc_skin() const { return pc_skin_set > 0.0 ? pc_skin_set : PC_SKIN * pgeo.rmax; }
@@ -800,7 +806,11 @@ struct fundem_sim {
     bool pc_active() const { return pc_on && !adj.on && recording == nullptr && pc_ctrl.p != nullptr; }
     fd::PairCacheDev pc_view()
     {
-        return fd::PairCacheDev{pc_ref_pos.p, pc_ref_q.p, pc_ref_vis.p, pc_ctrl.p, pc_skin(), 2.0 * pgeo.rmax};
+        // lever arms of a rotation: a body's nodes (at most r_max from its
+        // centre) and a node inside a partner's SDF grid (at most the grid
+        // radius from the partner's centre)
+        const double reach = std::max(2.0 * pgeo.rmax, pgeo.grid_rmax);
+        return fd::PairCacheDev{pc_ref_pos.p, pc_ref_q.p, pc_ref_vis.p, pc_ctrl.p, pc_drift.p, pc_skin(), reach};
     }
     // before steps (outside any stream capture): a pending forced rebuild is
     // written to the device flag
@@ -1093,6 +1103,7 @@ struct fundem_sim {
             if (pc) {
                 ap.skin = pcv.skin;
                 ap.gate = pcv.ctrl;
+                ap.drift = pcv.drift;
             }
             fd::launch_narrow(FD_PP, Pv, G, M, Wv, GW, MW, pgrid, wgrid, nullptr, Lpp, ap, with_force, mixed(), stream);
         }
@@ -2291,6 +2302,16 @@ int fundem_work_counters(fundem_sim* s, unsigned long long out[5])
         FD_CUDA(cudaStreamSynchronize(s->stream));
         FD_CUDA(cudaMemcpy(out, s->stats.p, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
         FD_CUDA(cudaMemsetAsync(s->stats.p, 0, 8 * sizeof(unsigned long long), s->stream));
+    });
+}
+
+int fundem_slot_counters(fundem_sim* s, unsigned long long out[2])
+{
+    if (!s || !out) return FUNDEM_ERR_ARG;
+    if (!s->stats.p) { out[0] = out[1] = 0; return FUNDEM_OK; }
+    return guard(s, [&] {
+        FD_CUDA(cudaStreamSynchronize(s->stream));
+        FD_CUDA(cudaMemcpy(out, s->stats.p + 5, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
     });
 }
 

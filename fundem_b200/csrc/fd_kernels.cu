@@ -275,19 +275,6 @@ __global__ void k_cell_order(long long num, const int* count, const int* start, 
     }
 }
 
-// runs of equal keys are the cells
-__global__ void k_cells_dense(const unsigned long long* key, int n, long long num, int* count, int* start)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const unsigned long long k = key[i];
-    if (k >= (unsigned long long)num || (i > 0 && key[i - 1] == k)) return;
-    int e = i + 1;
-    while (e < n && key[e] == k) ++e;
-    start[k] = i;
-    count[k] = e - i;
-}
-
 __global__ void k_hkey_clear(unsigned long long* hkey, unsigned long long n, const int* gate)
 {
     const unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -967,12 +954,7 @@ __global__ void __launch_bounds__(TPB) k_nl_filter(ObjDev P, GeoSetDev G, PairLi
 __global__ void k_pc_check(ObjDev P, PairCacheDev c)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.n || c.ctrl[0] != 0) return;
-    if (c.ctrl[2] != 0) {
-        // the last build overflowed its lists: build again
-        c.ctrl[0] = 1;
-        return;
-    }
+    if (i >= P.n) return;
     const double3 d = P.pos[i] - c.ref_pos[i];
     // 2 sin(theta / 2) = 2 |vector part of q conj(q0)|: the chord a unit
     // lever arm sweeps under the rotation since the build
@@ -982,6 +964,14 @@ __global__ void k_pc_check(ObjDev P, PairCacheDev c)
     const double vz = r.q0 * q.q3 - q.q0 * r.q3 - (q.q1 * r.q2 - q.q2 * r.q1);
     const double chord = 2.0 * sqrt(vx * vx + vy * vy + vz * vz);
     const double drift = sqrt(lengthSq3(d)) + c.reach * chord;
+    // every particle's bound, for the slot test of the predicate pass
+    c.drift[i] = __double2float_ru(drift);
+    if (c.ctrl[0] != 0) return;
+    if (c.ctrl[2] != 0) {
+        // the last build overflowed its lists: build again
+        c.ctrl[0] = 1;
+        return;
+    }
     // a little below skin / 2, so that the two drifts of a pair stay below
     // the single-precision skin the culling stages use
     const bool vis = P.hash[i] >= 0;
@@ -1514,12 +1504,36 @@ __global__ void __launch_bounds__(TPB, PASS == 0 ? FD_PROBE_MIN_BLOCKS : FD_CONT
     const int lane = threadIdx.x & 31;
     const bool periodic = (KIND == FD_PP || KIND == FD_PW) && (n.a.periodic_x || n.a.periodic_y);
     const int stride = gridDim.x * blockDim.x;
+    // pair cache (particle-particle list, predicate pass): a carried step
+    // tests the slot bound, a rebuild step stores it
+    const bool cache = KIND == FD_PP && PASS == 0 && n.a.gate != nullptr && L.c_phi0 != nullptr &&
+                       n.a.drift != nullptr;
+    const bool carried = cache && *n.a.gate == 0;
+    const bool slot_test = carried;
+    const bool phi0_store = cache && !carried;
     int hits = 0;
     for (int s0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); s0 < nitems; s0 += stride) {
         const int t = s0 + lane;
+        bool continue_slot = false;
         const int s = (PASS == 1 && t < nitems) ? L.c_hit[t] : t;
         bool hit = false;
-        if (t < nitems) {
+        if (slot_test && t < nitems) {
+            const int p = L.c_pair[s];
+            const int A = L.pairA[p];
+            const int B = L.pairB[p];
+            // a step that carries the pair cache skips a slot whose node was
+            // outside B at the rebuild by more than the SDF can change under
+            // both bodies' drift since: |grad phi| <= lip (trilinear bound),
+            // and the node's offset in B's frame moved by at most the sum of
+            // the drift bounds
+            const float lip = __double2float_ru(Slave<KIND>::geo(n, B).lip);
+            const float bound = __fmul_ru(lip, __fadd_ru(n.a.drift[A], n.a.drift[B]));
+            if (L.c_phi0[s] > __fadd_ru(bound, 1e-12f)) {
+                L.c_node[s] = -1;
+                continue_slot = true;
+            }
+        }
+        if (t < nitems && !continue_slot) {
             const int p = L.c_pair[s];
             const int k = L.c_k[s];
             const int A = L.pairA[p];
@@ -1539,8 +1553,11 @@ __global__ void __launch_bounds__(TPB, PASS == 0 ? FD_PROBE_MIN_BLOCKS : FD_CONT
             const double3 node = n.G.nodes[pool];
             const double3 r = xm_rot(qA, node);
             const double3 gp = mk3(r.x + cA.x, r.y + cA.y, r.z + cA.z);
-            double ov = 0., fx = 0., fy = 0., fz = 0., pv[8];
+            // an overlap the predicate did not reach stays +inf (a slot that
+            // is never skipped)
+            double ov = PASS == 0 ? __longlong_as_double(0x7ff0000000000000ll) : 0., fx = 0., fy = 0., fz = 0., pv[8];
             hit = node_predicate<KIND>(gp, bcell, sg, cB, qB, GB, SB.sdf, rB2, n.a.probe, ov, fx, fy, fz, pv);
+            if (phi0_store) L.c_phi0[s] = __double2float_rd(-ov);
             int nid = -1;
             if (PASS == 1 && hit) {
                 double3 nrm = fd_gradient_q(fx, fy, fz, pv);
@@ -1679,6 +1696,13 @@ __global__ void __launch_bounds__(TPB, PASS == 0 ? FD_PROBE_MIN_BLOCKS : FD_CONT
                 if (!hit) L.c_node[s] = -1;
                 if (n.a.rec.hit && s < n.a.rec.cap) n.a.rec.hit[s] = hit ? 1 : 0;
             }
+        }
+        if (cache && n.a.stats) {
+            // slots given the exact predicate, slots the bound skipped
+            const unsigned int tested = __ballot_sync(0xffffffffu, t < nitems && !continue_slot);
+            const unsigned int skipped = __ballot_sync(0xffffffffu, continue_slot);
+            if (lane == 0 && tested) atomicAdd(&n.a.stats[5], (unsigned long long)__popc(tested));
+            if (lane == 0 && skipped) atomicAdd(&n.a.stats[6], (unsigned long long)__popc(skipped));
         }
         if (PASS == 0) {
             // contacts are listed for pass 1, one atomic per warp
@@ -2640,8 +2664,12 @@ void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& 
         break;
     }
 #undef FD_NARROW_CASE
-    if (mixed) { k_pair_sum32<<<148 * 4, TPB, 0, s>>>(L, with_force); note_launch(); }
-    else k_pair_sum<<<148 * 4, TPB, 0, s>>>(L, with_force); note_launch();
+    if (mixed) {
+        k_pair_sum32<<<148 * 4, TPB, 0, s>>>(L, with_force);
+    } else {
+        k_pair_sum<<<148 * 4, TPB, 0, s>>>(L, with_force);
+    }
+    note_launch();
 }
 
 void launch_reverse(const ObjDev& P, PairListDev* lists, const int* active, RevDev& R, int* scan_tmp, size_t,
@@ -2667,8 +2695,12 @@ void launch_reverse(const ObjDev& P, PairListDev* lists, const int* active, RevD
 void launch_bonds(const ObjDev& P, BondDev& B, bool mixed, cudaStream_t s)
 {
     if (B.n <= 0) return;
-    if (mixed) { k_bonds32<<<nblocks(B.n), TPB, 0, s>>>(P, B); note_launch(); }
-    else k_bonds<<<nblocks(B.n), TPB, 0, s>>>(P, B); note_launch();
+    if (mixed) {
+        k_bonds32<<<nblocks(B.n), TPB, 0, s>>>(P, B);
+    } else {
+        k_bonds<<<nblocks(B.n), TPB, 0, s>>>(P, B);
+    }
+    note_launch();
 }
 
 void launch_contact_view(const PairListDev& L, long long* keys, int* order, unsigned long long* skey,
@@ -2694,8 +2726,12 @@ void launch_reduce(ObjDev& P, PairListDev* lists, const int* active, const RevDe
     for (int k = 0; k < FD_NKIND; ++k) { r.L[k] = lists[k]; r.active[k] = active[k]; }
     r.R = R;
     r.B = B;
-    if (mixed) { k_reduce<float><<<nblocks(P.n), TPB, 0, s>>>(r); note_launch(); }
-    else k_reduce<double><<<nblocks(P.n), TPB, 0, s>>>(r); note_launch();
+    if (mixed) {
+        k_reduce<float><<<nblocks(P.n), TPB, 0, s>>>(r);
+    } else {
+        k_reduce<double><<<nblocks(P.n), TPB, 0, s>>>(r);
+    }
+    note_launch();
 }
 
 }  // namespace fd

@@ -47,6 +47,9 @@ struct PairListDev {
     int* n_slots;      // device counter: slots used
     int* n_hits;       // device counter: contacts (n_slots + 1)
     int cap_contacts;  // slot capacity
+    float* c_phi0;     // pair cache: per slot, the node's signed distance to the
+                       // partner at the last rebuild (rounded down; -inf when
+                       // the predicate stopped before the distance)
     // previous contacts
     int* o_c_node;
     int* o_c_k;
@@ -227,8 +230,10 @@ struct PairCacheDev {
     fd_quat* ref_q;     // orientations at the last build
     int* ref_vis;       // visibility (hashed) at the last build
     int* ctrl;
+    float* drift;       // per particle: the drift bound since the last build (rounded up)
     double skin;
-    double reach;       // 2 r_max: lever arm of a rotation in the drift bound
+    double reach;       // largest lever arm of a rotation in the drift bound:
+                        // 2 r_max, or a larger SDF-grid radius
 };
 
 struct StepArgs {
@@ -241,6 +246,7 @@ struct StepArgs {
     int records;
     double skin;       // positional skin of the culling stages (the pair cache; 0 without it)
     const int* gate;   // pair cache: the selection runs only when *gate != 0 (null: always)
+    const float* drift;  // pair cache: per-particle drift bounds (see PairCacheDev)
     unsigned int* flags;
     unsigned long long* stats;  // optional: pairs, clusters, clusters kept, contacts (narrow kernels)
 };

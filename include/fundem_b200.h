@@ -384,6 +384,12 @@ int fundem_kernel_time(fundem_sim* sim, int group, double* ms_total, long long* 
    candidate pairs, node clusters examined, clusters that survived culling,
    node contacts, nodes given the exact double-precision predicate */
 int fundem_work_counters(fundem_sim* sim, unsigned long long out[5]);
+/* pair-cache work of the particle-particle predicate pass since the last
+   fundem_work_counters call (which resets these too): slots given the exact
+   predicate, and slots of carried steps skipped because the node was outside
+   the partner at the last rebuild by more than the SDF's Lipschitz bound
+   times both bodies' drift since (such a slot cannot hold a contact) */
+int fundem_slot_counters(fundem_sim* sim, unsigned long long out[2]);
 
 #ifdef __cplusplus
 }

@@ -124,3 +124,62 @@ def test_run_sharded_failure_reaches_every_rank():
         res = dict(out)
     for r in (0, 1):
         assert "rank 1: ValueError: no room for the batch" in res[r]
+
+
+class _Tiled:
+    """Stands in for batch.TiledBatch on the CPU: every step lowers each
+    particle by 1 micrometre."""
+
+    def __init__(self, scenarios, device=0):
+        self.pos = [np.array(sc.particles.pos, float) for sc in scenarios]
+
+    def run(self, steps):
+        self.pos = [p - np.array([0.0, 0.0, 1e-6 * steps]) for p in self.pos]
+
+    def states(self):
+        return [{"pos": p} for p in self.pos]
+
+    def close(self):
+        self.pos = []
+
+
+def _rank_tiled(rank, world, port, out):
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    from fundem_b200 import batch
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=__import__("datetime").timedelta(seconds=60))
+    try:
+        scs, _ = batch.calibration_scenarios(n_sims=40, seed=3)
+
+        def timer():
+            return lambda: 0.25 + rank       # seconds of this rank's timed steps
+        res, secs, parts = batch.run_sharded_tiled(scs, 50, rank, world, dist=dist, warmup=10, timer=timer,
+                                                   tiled_cls=_Tiled)
+        out[rank] = (res, secs, parts)
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_run_sharded_tiled_two_ranks():
+    """Each rank tiles its share into one stand-in simulation; every rank
+    ends with every simulation's result, the split, and both ranks'
+    timings (the bench takes the maximum)."""
+    port = 29800 + os.getpid() % 1000
+    with mp.Manager() as m:
+        out = m.dict()
+        mp.spawn(_rank_tiled, args=(2, port, out), nprocs=2, join=True)
+        res = dict(out)
+    sys.path.insert(0, ROOT)
+    from fundem_b200 import batch
+    scs, _ = batch.calibration_scenarios(n_sims=40, seed=3)
+    want = {i: float(sc.particles.pos[:, 2].mean() - 60e-6) for i, sc in enumerate(scs)}
+    parts = batch.shard([len(sc.particles) * 50 for sc in scs], 2)
+    for r in (0, 1):
+        got, secs, p = res[r]
+        assert sorted(got) == list(range(40))
+        assert all(got[i] == pytest.approx(want[i], rel=0, abs=1e-15) for i in range(40))
+        assert secs == [0.25, 1.25] and p == parts
+    assert res[0] == res[1]
