@@ -621,10 +621,14 @@ struct Ghost {
     DevArray<fd_quat> q;
     DevArray<double3> vel;
     DevArray<float4> rot;
+    // translated images under the pair cache: which particles have an image
+    DevArray<unsigned char> live;
     bool active = false;
-    fd::GhostDev view()
+    // live: null unless the pair cache covers this image set
+    fd::GhostDev view(bool with_live = false)
     {
-        return fd::GhostDev{pos.p, hash.p, cells.view(), occ.p, searchers.p, nsearch.p, q.p, vel.p, rot.p};
+        return fd::GhostDev{pos.p, hash.p, cells.view(), occ.p, searchers.p, nsearch.p, q.p, vel.p, rot.p,
+                            with_live ? live.p : nullptr};
     }
 };
 
@@ -789,7 +793,7 @@ struct fundem_sim {
         const size_t m = std::max(P.n(), 1);
         pc_ref_pos.alloc(m); pc_ref_q.alloc(m); pc_ref_vis.alloc(m);
         pc_drift.alloc(m, false);
-        pc_ctrl.alloc(4);
+        pc_ctrl.alloc(8);
     }
     double pc_skin() const { return pc_skin_set > 0.0 ? pc_skin_set : PC_SKIN * pgeo.rmax; }
     // some particle geometry has a nonzero inverse inertia: its bodies turn,
@@ -1043,6 +1047,7 @@ struct fundem_sim {
                 }
                 ghosts[d].pos.alloc(std::max(np, 1));
                 ghosts[d].hash.alloc(std::max(np, 1));
+                if (d < 3) ghosts[d].live.alloc(std::max(np, 1));
                 ghosts[d].occ.alloc(6);
                 ghosts[d].searchers.alloc(std::max(np, 1));
                 ghosts[d].nsearch.alloc(1);
@@ -1127,6 +1132,11 @@ struct fundem_sim {
                                     cudaMemcpyDeviceToDevice, stream));
         tend(FUNDEM_T_NARROW_PW);
         PairListDev Lg[6];
+        // the translated image sets share the pair cache (not with sector
+        // periodicity): their pairs and slots are kept with the particle
+        // pairs', and a wrap or an image in a clamped cell rebuilds them
+        const bool pcg = pc && !sector;
+        int* gctrl = pcg ? pcv.ctrl : nullptr;
         if (perX || perY || sector) {
             tbegin(FUNDEM_T_GHOST);
             // PeriodicBoundaryXY2D then PeriodicBoundarySector::updateGhostSpatialGrid
@@ -1134,13 +1144,18 @@ struct fundem_sim {
             const int kinds[6] = {FD_GX, FD_GY, FD_GXY, FD_GR90, FD_GR180, FD_GR270};
             for (int d = 0; d < 3; ++d) {
                 if (!ghosts[d].active) continue;
-                if (d == 0) fd::launch_wrap(Pv, pgrid, 0, stream);
-                if (d == 1) fd::launch_wrap(Pv, pgrid, 1, stream);
-                fd::GhostDev gh = ghosts[d].view();
-                fd::launch_ghost_build(Pv, gh, kinds[d], stream);
+                if (d == 0) fd::launch_wrap(Pv, pgrid, 0, stream, gctrl);
+                if (d == 1) fd::launch_wrap(Pv, pgrid, 1, stream, gctrl);
+                fd::GhostDev gh = ghosts[d].view(pcg);
+                fd::launch_ghost_build(Pv, gh, kinds[d], stream, pcg ? pcv.skin : 0.0, gctrl);
+            }
+            if (pcg) fd::launch_ghost_gate(gctrl, stream);
+            for (int d = 0; d < 3; ++d) {
+                if (!ghosts[d].active) continue;
+                fd::GhostDev gh = ghosts[d].view(pcg);
                 ObjDev ghostobj = Pv;
                 ghostobj.hash = ghosts[d].hash.p;
-                fd::launch_cell_table(ghostobj, gh.cells, scan_tmp.p, scan_tmp.n, stream);
+                fd::launch_cell_table(ghostobj, gh.cells, scan_tmp.p, scan_tmp.n, stream, pcg ? gctrl + 5 : nullptr);
             }
             if (sector) {
                 fd::launch_sector_wrap(Pv, pgrid, stream);
@@ -1154,11 +1169,21 @@ struct fundem_sim {
             }
             for (int d = 0; d < 6; ++d) {
                 if (!ghosts[d].active) continue;
-                fd::GhostDev gh = ghosts[d].view();
+                const bool cached = pcg && d < 3;
+                fd::GhostDev gh = ghosts[d].view(cached);
                 Lg[d] = lists[kinds[d]].view();
-                fd::launch_broad_ghost(Pv, G, gh, Lg[d], flags.p, probe, stream);
-                a.rec = recording ? recording->rec(kinds[d], record_step) : fd::AdjRec{};
-                fd::launch_narrow(kinds[d], Pv, G, M, Wv, GW, MW, pgrid, wgrid, &gh, Lg[d], a, with_force, mixed(),
+                fd::StepArgs ag = a;
+                if (cached) {
+                    ag.skin = pcv.skin;
+                    ag.gate = gctrl + 5;
+                    ag.noskin = gctrl + 6;
+                    ag.drift = pcv.drift;
+                    fd::launch_broad_ghost(Pv, G, gh, Lg[d], flags.p, probe, stream, pcv.skin, gctrl + 5, gctrl + 6);
+                } else {
+                    fd::launch_broad_ghost(Pv, G, gh, Lg[d], flags.p, probe, stream);
+                }
+                ag.rec = recording ? recording->rec(kinds[d], record_step) : fd::AdjRec{};
+                fd::launch_narrow(kinds[d], Pv, G, M, Wv, GW, MW, pgrid, wgrid, &gh, Lg[d], ag, with_force, mixed(),
                                   stream);
                 if (recording)
                     FD_CUDA(cudaMemcpyAsync(recording->ns(kinds[d], record_step), Lg[d].n_slots, sizeof(int),
@@ -1166,6 +1191,13 @@ struct fundem_sim {
                 active[kinds[d]] = 1;
             }
             tend(FUNDEM_T_GHOST);
+        }
+        if (pc) {
+            PairListDev gl[3];
+            int ng = 0;
+            for (int d = 0; d < 3 && pcg; ++d)
+                if (ghosts[d].active) gl[ng++] = Lg[d];
+            fd::launch_pair_cache_end(pcv, gl, ng, stream);
         }
         if (!with_force) {
             FD_CUDA(cudaGetLastError());
@@ -1217,7 +1249,8 @@ struct fundem_sim {
             const int needc = 2 * c[1] > L.cap_contacts ? 3 * c[1] : 0;
             if (needp || needc) {
                 L.grow(std::max(needp, L.cap_pairs), std::max(needc, L.cap_contacts));
-                if (k == FD_PP) pc_force = true;  // the slot-to-pair map is not kept by a growth
+                // the slot-to-pair map of a cached list is not kept by a growth
+                if (k == FD_PP || k == FD_GX || k == FD_GY || k == FD_GXY) pc_force = true;
             }
         }
     }

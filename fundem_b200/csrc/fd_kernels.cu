@@ -367,36 +367,53 @@ __device__ __forceinline__ int wrap_code(double3 cA, double3 ri, double3 cB, dou
            27 * (sh(rj.y - cB.y, Ly) + 1);
 }
 
-__global__ void k_wrap(ObjDev P, FdGrid g, int dim)
+__global__ void k_wrap(ObjDev P, FdGrid g, int dim, int* ctrl)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.n) return;
-    P.pos[i] = dim == 0 ? wrap_x(P.pos[i], g) : wrap_y(P.pos[i], g);
+    const double3 p0 = P.pos[i];
+    const double3 p1 = dim == 0 ? wrap_x(p0, g) : wrap_y(p0, g);
+    P.pos[i] = p1;
+    // under the pair cache a wrap changes which particles have images: the
+    // ghost lists of this step are built afresh, and every list at the next
+    if (ctrl && (p1.x != p0.x || p1.y != p0.y)) {
+        ctrl[4] = 1;
+        ctrl[7] = 1;
+    }
 }
 
 // calculateGhostHashKernel, including its z test against maxBound.y (:236):
 // an image outside the domain is hashed into the clamped boundary cell, an
 // image inside it is not a ghost
-__device__ __forceinline__ void image_hash(GhostDev& Gh, int i, double3 r)
+// Returns the directions (bit 0 x, 1 y, 2 z) in which the image lies
+// outside the domain.
+__device__ __forceinline__ int image_hash(GhostDev& Gh, int i, double3 r)
 {
     const FdGrid& g = Gh.cells.g;
     int3 gc = fd_cell_of(r, g);
-    bool out = false;
-    if (r.x < g.minb.x) { gc.x = 0; out = true; }
-    else if (r.x >= g.maxb.x) { gc.x = g.size.x - 1; out = true; }
-    if (r.y < g.minb.y) { gc.y = 0; out = true; }
-    else if (r.y >= g.maxb.y) { gc.y = g.size.y - 1; out = true; }
-    if (r.z < g.minb.z) { gc.z = 0; out = true; }
-    else if (r.z >= g.maxb.y) { gc.z = g.size.z - 1; out = true; }
+    int outm = 0;
+    if (r.x < g.minb.x) { gc.x = 0; outm |= 1; }
+    else if (r.x >= g.maxb.x) { gc.x = g.size.x - 1; outm |= 1; }
+    if (r.y < g.minb.y) { gc.y = 0; outm |= 2; }
+    else if (r.y >= g.maxb.y) { gc.y = g.size.y - 1; outm |= 2; }
+    if (r.z < g.minb.z) { gc.z = 0; outm |= 4; }
+    else if (r.z >= g.maxb.y) { gc.z = g.size.z - 1; outm |= 4; }
+    const bool out = outm != 0;
     const long long h = out ? fd_lin3(gc.x, gc.y, gc.z, g.size) : -1;
     Gh.hash[i] = h;
     if (h >= 0 && h < g.num) {
         atomicMin(&Gh.occ[0], gc.x); atomicMin(&Gh.occ[1], gc.y); atomicMin(&Gh.occ[2], gc.z);
         atomicMax(&Gh.occ[3], gc.x); atomicMax(&Gh.occ[4], gc.y); atomicMax(&Gh.occ[5], gc.z);
     }
+    return outm;
 }
 
-__global__ void k_ghost_build(ObjDev P, GhostDev Gh, int kind)
+// The image of a particle in the first cell column (row, or both) sits one
+// period beyond the domain.  Under the pair cache (ctrl non-null) the
+// particles within ext_skin of that band get images as well, so that a
+// rebuild lists the pairs of every particle that can gain an image before
+// the next rebuild; Gh.live marks the particles that have one now.
+__global__ void k_ghost_build(ObjDev P, GhostDev Gh, int kind, double ext_skin, int* ctrl)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.n) return;
@@ -404,12 +421,58 @@ __global__ void k_ghost_build(ObjDev P, GhostDev Gh, int kind)
     const double3 p = P.pos[i];
     const double3 ox = mk3(g.maxb.x - g.minb.x, 0., 0.), oy = mk3(0., g.maxb.y - g.minb.y, 0.);
     const int3 c = fd_cell_of(p, g);
+    const bool bx = ctrl && (p.x - g.minb.x) * g.inv.x < 1.0 + ext_skin * g.inv.x * 1.01;
+    const bool by = ctrl && (p.y - g.minb.y) * g.inv.y < 1.0 + ext_skin * g.inv.y * 1.01;
+    bool live = false, ext = false;
+    if (kind == FD_GX) { live = c.x == 0; ext = live || bx; }
+    if (kind == FD_GY) { live = c.y == 0; ext = live || by; }
+    if (kind == FD_GXY) { live = c.x == 0 && c.y == 0; ext = live || ((c.x == 0 || bx) && (c.y == 0 || by)); }
     double3 r = p;
-    if (kind == FD_GX && c.x == 0) r = r + ox;
-    if (kind == FD_GY && c.y == 0) r = r + oy;
-    if (kind == FD_GXY && c.x == 0 && c.y == 0) r = r + (ox + oy);
+    if (ext) {
+        if (kind == FD_GX) r = r + ox;
+        if (kind == FD_GY) r = r + oy;
+        if (kind == FD_GXY) r = r + (ox + oy);
+    }
     Gh.pos[i] = r;
-    image_hash(Gh, i, r);
+    if (Gh.live) Gh.live[i] = live ? 1 : 0;
+    const int outm = image_hash(Gh, i, r);
+    if (ctrl && ext) {
+        // outside the domain across the translation only: its cell is the
+        // natural one in the other directions, and candidacy follows the
+        // geometry; otherwise (a clamped cell) this step is built uncached
+        const int along = kind == FD_GX ? 1 : kind == FD_GY ? 2 : 3;
+        if (outm & ~along) {
+            ctrl[4] = 1;
+            ctrl[7] = 1;
+        }
+    }
+}
+
+__global__ void k_ghost_gate(int* ctrl)
+{
+    ctrl[5] = (ctrl[0] != 0 || ctrl[4] != 0) ? 1 : 0;
+    ctrl[6] = ctrl[4];
+}
+
+// end of a cached step
+struct GhostCounts {
+    int* n_pairs[3];
+    int* n_slots[3];
+    int cap_pairs[3];
+    int cap_contacts[3];
+    int n;
+};
+__global__ void k_pc_end(int* ctrl, GhostCounts gc)
+{
+    if (ctrl[5] != 0)
+        for (int k = 0; k < gc.n; ++k)
+            if (*gc.n_pairs[k] > gc.cap_pairs[k] || *gc.n_slots[k] > gc.cap_contacts[k]) ctrl[7] = 1;
+    ctrl[3] = ctrl[7];
+    ctrl[7] = 0;
+    ctrl[0] = 0;
+    ctrl[4] = 0;
+    ctrl[5] = 0;
+    ctrl[6] = 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -719,9 +782,10 @@ template <bool GHOST, bool LIST, bool NLB>
 __global__ void __launch_bounds__(TPB) k_broad_cells(ObjDev P, GeoSetDev G, CellTableDev T, const double3* gpos,
                                                      const float4* grot, const int* occ, const int* alist, const int* acount,
                                                      PairListDev L, NlDev nl, unsigned int* flags, double probe,
-                                                     double skin, const int* gate)
+                                                     double skin, const int* gate, const int* noskin)
 {
     if (gate && *gate == 0) return;
+    if (noskin && *noskin) skin = 0.0;
     if (NLB && nl.ctrl[0] == 0) return;
     __shared__ int s_list[TPB / BROAD_LANES][MAX_CAND];
     __shared__ int s_cand[TPB / BROAD_LANES][BROAD_CAND];
@@ -967,8 +1031,9 @@ __global__ void k_pc_check(ObjDev P, PairCacheDev c)
     // every particle's bound, for the slot test of the predicate pass
     c.drift[i] = __double2float_ru(drift);
     if (c.ctrl[0] != 0) return;
-    if (c.ctrl[2] != 0) {
-        // the last build overflowed its lists: build again
+    if (c.ctrl[2] != 0 || c.ctrl[3] != 0) {
+        // the last build overflowed its lists, or the last step asked for a
+        // rebuild: build again
         c.ctrl[0] = 1;
         return;
     }
@@ -981,7 +1046,7 @@ __global__ void k_pc_check(ObjDev P, PairCacheDev c)
 // a step without a rebuild: this step's pairs and slots are the previous
 // step's, carried over; each pair's history is its own slots of the previous
 // step, and its partner's cell is taken from this step's hash
-__global__ void k_pc_carry(PairListDev L, ObjDev P, FdGrid g, const int* gate)
+__global__ void k_pc_carry(PairListDev L, int n_obj, const long long* hash, FdGrid g, const int* gate)
 {
     if (*gate != 0) return;
     const int npairs = min(L.o_counters[0], L.cap_pairs);
@@ -992,7 +1057,7 @@ __global__ void k_pc_carry(PairListDev L, ObjDev P, FdGrid g, const int* gate)
         *L.n_pairs = L.o_counters[0];
         *L.n_slots = L.o_counters[1];
     }
-    for (long long i = t0; i < P.n; i += stride) {
+    for (long long i = t0; i < n_obj; i += stride) {
         L.seg_off[i] = L.o_seg_off[i];
         L.seg_cnt[i] = L.o_seg_cnt[i];
     }
@@ -1005,7 +1070,7 @@ __global__ void k_pc_carry(PairListDev L, ObjDev P, FdGrid g, const int* gate)
         L.c_cnt[p] = cnt;
         if (cnt > 0) {
             int3 bc;
-            decode_cell(P.hash[B], g.size, bc);
+            decode_cell(hash[B], g.size, bc);
             L.p_aux[p] = make_int4(bc.x, bc.y, bc.z, off);
             L.p_hist_cnt[p] = cnt;
         }
@@ -1034,12 +1099,13 @@ __global__ void k_pc_commit(ObjDev P, PairCacheDev c, PairListDev L)
 // images are listed for k_broad_cells<true, true>; the others get empty
 // segments here
 __global__ void k_ghost_searchers(ObjDev P, GeoSetDev G, FdGrid g, const int* occ, PairListDev L, int* alist,
-                                  int* acount)
+                                  int* acount, double skin, const int* gate, const int* noskin)
 {
     const int A = blockIdx.x * blockDim.x + threadIdx.x;
-    if (A >= P.n) return;
+    if (A >= P.n || (gate && *gate == 0)) return;
+    if (noskin && *noskin) skin = 0.0;
     const double rA = G.geo[P.geo[A]].radius;
-    const double reach = (rA + G.grid_rmax) * (1.0 + 8.0 * BOUND_REL);
+    const double reach = (rA + G.grid_rmax) * (1.0 + 8.0 * BOUND_REL) + skin;
     int3 lo, hi;
     partner_search_range(P.pos[A], reach, g, lo, hi);
     const bool any = max(lo.x, occ[0]) <= min(hi.x, occ[3]) && max(lo.y, occ[1]) <= min(hi.y, occ[4]) &&
@@ -1385,6 +1451,7 @@ __global__ void __launch_bounds__(NARROW_WARPS * 32, FD_SELECT_MIN_BLOCKS) k_sel
     PairListDev& L = n.L;
     const int npairs = min(*L.n_pairs, L.cap_pairs);
     const int nwarps = gridDim.x * NARROW_WARPS;
+    const double skin = (n.a.noskin && *n.a.noskin) ? 0.0 : n.a.skin;
     for (int p = blockIdx.x * NARROW_WARPS + wib; p < npairs; p += nwarps) {
         const int A = L.pairA[p];
         const int B = L.pairB[p];
@@ -1404,7 +1471,7 @@ __global__ void __launch_bounds__(NARROW_WARPS * 32, FD_SELECT_MIN_BLOCKS) k_sel
             bool k = false;
             if (c < ncl) {
                 float4 cl = n.G.clus_sphere[GA.clus_off + c];
-                cl.w += (float)n.a.skin;
+                cl.w += (float)skin;
                 k = !cluster_culled<KIND>(cl, xf, GB, SB, rB, n.a.probe);
             }
             keep |= ((unsigned long long)__ballot_sync(0xffffffffu, k)) << c0;
@@ -1413,7 +1480,7 @@ __global__ void __launch_bounds__(NARROW_WARPS * 32, FD_SELECT_MIN_BLOCKS) k_sel
         // ---- single-precision filter over the nodes of the surviving
         // clusters; nodes that may pass the predicate are queued in cluster
         // order
-        const float perr = 4e-6f * (float)(length3(cA - cB) + GA.radius + rB + GB.spacing) + (float)n.a.skin;
+        const float perr = 4e-6f * (float)(length3(cA - cB) + GA.radius + rB + GB.spacing) + (float)skin;
         int ncand = 0;
         while (keep) {
             const int c = __ffsll((long long)keep) - 1;
@@ -1504,33 +1571,43 @@ __global__ void __launch_bounds__(TPB, PASS == 0 ? FD_PROBE_MIN_BLOCKS : FD_CONT
     const int lane = threadIdx.x & 31;
     const bool periodic = (KIND == FD_PP || KIND == FD_PW) && (n.a.periodic_x || n.a.periodic_y);
     const int stride = gridDim.x * blockDim.x;
-    // pair cache (particle-particle list, predicate pass): a carried step
-    // tests the slot bound, a rebuild step stores it
-    const bool cache = KIND == FD_PP && PASS == 0 && n.a.gate != nullptr && L.c_phi0 != nullptr &&
+    // pair cache (particle-particle and translated ghost lists, predicate
+    // pass): a carried step tests the slot bound, a rebuild step stores it.
+    // A translated ghost list under the cache also holds the pairs of
+    // particles that have no image this step: their slots hold no contact.
+    constexpr bool TRANSLATED = KIND == FD_GX || KIND == FD_GY || KIND == FD_GXY;
+    const bool cache = (KIND == FD_PP || TRANSLATED) && PASS == 0 && n.a.gate != nullptr && L.c_phi0 != nullptr &&
                        n.a.drift != nullptr;
     const bool carried = cache && *n.a.gate == 0;
     const bool slot_test = carried;
     const bool phi0_store = cache && !carried;
+    const bool live_test = TRANSLATED && PASS == 0 && n.gh.live != nullptr;
     int hits = 0;
     for (int s0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); s0 < nitems; s0 += stride) {
         const int t = s0 + lane;
         bool continue_slot = false;
         const int s = (PASS == 1 && t < nitems) ? L.c_hit[t] : t;
         bool hit = false;
-        if (slot_test && t < nitems) {
+        if ((slot_test || live_test) && t < nitems) {
             const int p = L.c_pair[s];
             const int A = L.pairA[p];
             const int B = L.pairB[p];
-            // a step that carries the pair cache skips a slot whose node was
-            // outside B at the rebuild by more than the SDF can change under
-            // both bodies' drift since: |grad phi| <= lip (trilinear bound),
-            // and the node's offset in B's frame moved by at most the sum of
-            // the drift bounds
-            const float lip = __double2float_ru(Slave<KIND>::geo(n, B).lip);
-            const float bound = __fmul_ru(lip, __fadd_ru(n.a.drift[A], n.a.drift[B]));
-            if (L.c_phi0[s] > __fadd_ru(bound, 1e-12f)) {
+            if (live_test && !n.gh.live[B]) {
                 L.c_node[s] = -1;
+                if (phi0_store) L.c_phi0[s] = __int_as_float(0xff800000);  // -inf: never skipped
                 continue_slot = true;
+            } else if (slot_test) {
+                // a step that carries the pair cache skips a slot whose node
+                // was outside B at the rebuild by more than the SDF can change
+                // under both bodies' drift since: |grad phi| <= lip (trilinear
+                // bound), and the node's offset in B's frame moved by at most
+                // the sum of the drift bounds (an image moves with its body)
+                const float lip = __double2float_ru(Slave<KIND>::geo(n, B).lip);
+                const float bound = __fmul_ru(lip, __fadd_ru(n.a.drift[A], n.a.drift[B]));
+                if (L.c_phi0[s] > __fadd_ru(bound, 1e-12f)) {
+                    L.c_node[s] = -1;
+                    continue_slot = true;
+                }
             }
         }
         if (t < nitems && !continue_slot) {
@@ -2543,16 +2620,21 @@ void launch_cell_table(ObjDev& O, CellTableDev& T, int* scan_tmp, size_t, cudaSt
     k_cell_scatter<<<nblocks(O.n), TPB, 0, s>>>(O.hash, O.n, T.g.num, T.start, T.fill, T.sorted); note_launch();
     k_cell_order<<<nblocks(T.g.num), TPB, 0, s>>>(T.g.num, T.count, T.start, T.sorted); note_launch();
 }
-void launch_wrap(ObjDev& P, const FdGrid& g, int dim, cudaStream_t s)
+void launch_wrap(ObjDev& P, const FdGrid& g, int dim, cudaStream_t s, int* ctrl)
 {
-    if (P.n > 0) { k_wrap<<<nblocks(P.n), TPB, 0, s>>>(P, g, dim); note_launch(); }
+    if (P.n > 0) { k_wrap<<<nblocks(P.n), TPB, 0, s>>>(P, g, dim, ctrl); note_launch(); }
 }
-void launch_ghost_build(const ObjDev& P, GhostDev& Gh, int kind, cudaStream_t s)
+void launch_ghost_build(const ObjDev& P, GhostDev& Gh, int kind, cudaStream_t s, double ext_skin, int* ctrl)
 {
     // occupied-cell box of the ghost images: empty until the build fills it
     cudaMemsetAsync(Gh.occ, 0x7f, 3 * sizeof(int), s);
     cudaMemsetAsync(Gh.occ + 3, 0xff, 3 * sizeof(int), s);
-    if (P.n > 0) { k_ghost_build<<<nblocks(P.n), TPB, 0, s>>>(P, Gh, kind); note_launch(); }
+    if (P.n > 0) { k_ghost_build<<<nblocks(P.n), TPB, 0, s>>>(P, Gh, kind, ext_skin, ctrl); note_launch(); }
+}
+void launch_ghost_gate(int* ctrl, cudaStream_t s)
+{
+    k_ghost_gate<<<1, 1, 0, s>>>(ctrl);
+    note_launch();
 }
 void launch_sector_wrap(ObjDev& P, const FdGrid& g, cudaStream_t s)
 {
@@ -2573,7 +2655,7 @@ void launch_broad_pp(const ObjDev& P, const GeoSetDev& G, const CellTableDev& T,
     cudaMemsetAsync(L.n_pairs, 0, sizeof(int), s);
     if (P.n > 0) {
         k_broad_cells<false, false, false><<<nblocks((long long)P.n * BROAD_LANES), TPB, 0, s>>>(
-            P, G, T, nullptr, nullptr, nullptr, nullptr, nullptr, L, NlDev{}, flags, probe, skin, gate);
+            P, G, T, nullptr, nullptr, nullptr, nullptr, nullptr, L, NlDev{}, flags, probe, skin, gate, nullptr);
         note_launch();
     }
 }
@@ -2584,7 +2666,8 @@ void launch_broad_pp_nl(const ObjDev& P, const GeoSetDev& G, const CellTableDev&
     if (P.n <= 0) return;
     k_nl_check<<<nblocks(P.n), TPB, 0, s>>>(P, nl, T.g, gate); note_launch();
     k_broad_cells<false, false, true><<<nblocks((long long)P.n * BROAD_LANES), TPB, 0, s>>>(
-        P, G, T, nullptr, nullptr, nullptr, nullptr, nullptr, L, nl, flags, probe, 0.0, gate); note_launch();
+        P, G, T, nullptr, nullptr, nullptr, nullptr, nullptr, L, nl, flags, probe, 0.0, gate, nullptr);
+    note_launch();
     k_nl_filter<<<nblocks((long long)P.n * 8), TPB, 0, s>>>(P, G, L, nl, flags, probe, gate); note_launch();
 }
 void launch_pair_cache_check(const ObjDev& P, const PairCacheDev& c, cudaStream_t s)
@@ -2594,7 +2677,19 @@ void launch_pair_cache_check(const ObjDev& P, const PairCacheDev& c, cudaStream_
 void launch_pair_cache_commit(const ObjDev& P, const PairCacheDev& c, const PairListDev& L, cudaStream_t s)
 {
     if (P.n > 0) { k_pc_commit<<<nblocks(P.n), TPB, 0, s>>>(P, c, L); note_launch(); }
-    cudaMemsetAsync(c.ctrl, 0, sizeof(int), s);
+}
+void launch_pair_cache_end(const PairCacheDev& c, const PairListDev* ghost_lists, int n_ghost_lists, cudaStream_t s)
+{
+    GhostCounts gc{};
+    gc.n = std::min(n_ghost_lists, 3);
+    for (int k = 0; k < gc.n; ++k) {
+        gc.n_pairs[k] = ghost_lists[k].n_pairs;
+        gc.n_slots[k] = ghost_lists[k].n_slots;
+        gc.cap_pairs[k] = ghost_lists[k].cap_pairs;
+        gc.cap_contacts[k] = ghost_lists[k].cap_contacts;
+    }
+    k_pc_end<<<1, 1, 0, s>>>(c.ctrl, gc);
+    note_launch();
 }
 
 void launch_broad_pw(const ObjDev& P, const GeoSetDev& G, const ObjDev& W, const GeoSetDev& GW,
@@ -2605,15 +2700,20 @@ void launch_broad_pw(const ObjDev& P, const GeoSetDev& G, const ObjDev& W, const
     if (P.n > 0) { k_broad_pw<<<nblocks(P.n), TPB, 0, s>>>(P, G, W, GW, wg, L, flags, probe, wall_range); note_launch(); }
 }
 void launch_broad_ghost(const ObjDev& P, const GeoSetDev& G, const GhostDev& Gh, PairListDev& L,
-                        unsigned int* flags, double probe, cudaStream_t s)
+                        unsigned int* flags, double probe, cudaStream_t s, double skin, const int* gate,
+                        const int* noskin)
 {
     cudaMemsetAsync(L.n_pairs, 0, sizeof(int), s);
     if (P.n <= 0) return;
     cudaMemsetAsync(Gh.nsearch, 0, sizeof(int), s);
-    k_ghost_searchers<<<nblocks(P.n), TPB, 0, s>>>(P, G, Gh.cells.g, Gh.occ, L, Gh.searchers, Gh.nsearch); note_launch();
+    k_ghost_searchers<<<nblocks(P.n), TPB, 0, s>>>(P, G, Gh.cells.g, Gh.occ, L, Gh.searchers, Gh.nsearch, skin,
+                                                    gate, noskin);
+    note_launch();
     const long long groups = std::min<long long>(P.n, 148ll * 8 * (TPB / BROAD_LANES));
     k_broad_cells<true, true, false><<<nblocks(groups * BROAD_LANES), TPB, 0, s>>>(
-        P, G, Gh.cells, Gh.pos, Gh.rot, Gh.occ, Gh.searchers, Gh.nsearch, L, NlDev{}, flags, probe, 0.0, nullptr); note_launch();
+        P, G, Gh.cells, Gh.pos, Gh.rot, Gh.occ, Gh.searchers, Gh.nsearch, L, NlDev{}, flags, probe, skin, gate,
+        noskin);
+    note_launch();
 }
 
 void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& M, const ObjDev& W,
@@ -2633,7 +2733,10 @@ void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& 
 #define FD_NARROW_CASE(K)                                                              \
     case K:                                                                            \
         k_select<K><<<grid, NARROW_WARPS * 32, 0, s>>>(n); note_launch();                             \
-        if (a.gate) { k_pc_carry<<<148 * 8, TPB, 0, s>>>(L, P, pgrid, a.gate); note_launch(); }          \
+        if (a.gate) {                                                                  \
+            k_pc_carry<<<148 * 8, TPB, 0, s>>>(L, P.n, gh ? gh->hash : P.hash, pgrid, a.gate);        \
+            note_launch();                                                             \
+        }                                                                              \
         if (mixed) {                                                                   \
             k_contact32<K, 0><<<cgrid, TPB, 0, s>>>(n); note_launch();                                \
             k_contact32<K, 1><<<cgrid, TPB, 0, s>>>(n); note_launch();                                \

@@ -147,6 +147,10 @@ struct GhostDev {
     fd_quat* q;
     double3* vel;
     float4* rot;
+    // translated images under the pair cache: 1 where the particle has an
+    // image this step (the images of a rebuild also cover the particles
+    // within the skin of the image band, whose pairs the cache keeps)
+    unsigned char* live;
 };
 
 struct BondDev {
@@ -229,6 +233,13 @@ struct PairCacheDev {
     double3* ref_pos;   // positions at the last build
     fd_quat* ref_q;     // orientations at the last build
     int* ref_vis;       // visibility (hashed) at the last build
+    // ctrl: [0] rebuild this step, [1] rebuilds so far, [2] the last build
+    // overflowed the particle-particle lists, [3] rebuild at the next step,
+    // [4] the translated ghost lists of this step are built without the
+    // cache (a particle wrapped, or an image outside the domain's other
+    // directions), [5] the ghost lists' gate this step ([0] or [4]), [6]
+    // [4] again, as the ghost kernels' skin switch, [7] rebuild requests of
+    // this step, moved to [3] at its end
     int* ctrl;
     float* drift;       // per particle: the drift bound since the last build (rounded up)
     double skin;
@@ -247,6 +258,7 @@ struct StepArgs {
     double skin;       // positional skin of the culling stages (the pair cache; 0 without it)
     const int* gate;   // pair cache: the selection runs only when *gate != 0 (null: always)
     const float* drift;  // pair cache: per-particle drift bounds (see PairCacheDev)
+    const int* noskin;   // non-null and nonzero: this step's selection takes no skin
     unsigned int* flags;
     unsigned long long* stats;  // optional: pairs, clusters, clusters kept, contacts (narrow kernels)
 };
@@ -288,8 +300,18 @@ void radix_sort_keys(const long long* keys, int n, long long num_keys, unsigned 
                      const int* gate = nullptr);
 // ints needed for bcount and bscan_tmp for n keys
 void radix_sort_scratch(int n, size_t& bcount_ints, size_t& bscan_ints);
-void launch_wrap(ObjDev& P, const FdGrid& g, int dim, cudaStream_t s);
-void launch_ghost_build(const ObjDev& P, GhostDev& Gh, int kind, cudaStream_t s);
+// ctrl (the pair cache's, or null): a wrap requests the uncached ghost
+// stage this step and a rebuild at the next
+void launch_wrap(ObjDev& P, const FdGrid& g, int dim, cudaStream_t s, int* ctrl = nullptr);
+// ext_skin > 0 (the pair cache, ctrl non-null): particles within ext_skin of
+// the image band get images too (Gh.live marks the true ones); an image
+// outside the domain in a direction it is not translated along (the
+// reference hashes it into a clamped cell) makes this step's ghost stage
+// uncached
+void launch_ghost_build(const ObjDev& P, GhostDev& Gh, int kind, cudaStream_t s, double ext_skin = 0.0,
+                        int* ctrl = nullptr);
+// the ghost lists' gate and skin switch of this step (ctrl[5], ctrl[6])
+void launch_ghost_gate(int* ctrl, cudaStream_t s);
 // sector periodicity: turn bodies that left the quarter sector back in, then
 // build the three turned image sets (R90, R180, R270)
 void launch_sector_wrap(ObjDev& P, const FdGrid& g, cudaStream_t s);
@@ -308,16 +330,22 @@ void launch_broad_pp_nl(const ObjDev& P, const GeoSetDev& G, const CellTableDev&
 // the state of a rebuild step as the new reference and clear the flag
 void launch_pair_cache_check(const ObjDev& P, const PairCacheDev& c, cudaStream_t s);
 void launch_pair_cache_commit(const ObjDev& P, const PairCacheDev& c, const PairListDev& L, cudaStream_t s);
+// end of a cached step: a rebuild whose ghost lists overflowed is not kept,
+// this step's requests become the next step's rebuild, the flags clear
+void launch_pair_cache_end(const PairCacheDev& c, const PairListDev* ghost_lists, int n_ghost_lists, cudaStream_t s);
 // wall_range (null: every wall): per particle, the first wall and the wall
 // count it may meet (a batch of simulations tiled into one)
 void launch_broad_pw(const ObjDev& P, const GeoSetDev& G, const ObjDev& W, const GeoSetDev& GW,
                      const FdGrid& wg, PairListDev& L, unsigned int* flags, double probe, cudaStream_t s,
                      const int2* wall_range = nullptr);
+// skin, gate and noskin: the pair cache (ctrl[5], ctrl[6]), as for the
+// particle-particle list
 void launch_broad_ghost(const ObjDev& P, const GeoSetDev& G, const GhostDev& Gh, PairListDev& L,
-                        unsigned int* flags, double probe, cudaStream_t s);
-// a.gate non-null (particle-particle list under the pair cache): on steps
-// without a rebuild the selection is skipped and the previous step's pairs
-// and slots are carried into this step's list
+                        unsigned int* flags, double probe, cudaStream_t s, double skin = 0.0,
+                        const int* gate = nullptr, const int* noskin = nullptr);
+// a.gate non-null (particle-particle and translated ghost lists under the
+// pair cache): on steps without a rebuild the selection is skipped and the
+// previous step's pairs and slots are carried into this step's list
 void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& M, const ObjDev& W,
                    const GeoSetDev& GW, const MatDev& MW, const FdGrid& pgrid, const FdGrid& wgrid,
                    const GhostDev* gh, PairListDev& L, const StepArgs& a, int with_force, bool mixed, cudaStream_t s);

@@ -4,7 +4,9 @@ rebuild and run the exact double-precision node predicate on every slot, so
 the contact lists must be the ones a full detection gives:
 
 * against the CPU oracle, step by step on the fixture cases (walls, periodic
-  ghosts, millimetre pour), with the tolerances of the uncached parity tests:
+  ghosts, millimetre pour, and a tall periodic column whose upper images the
+  reference hashes into clamped cells), with the tolerances of the uncached
+  parity tests:
   contact lists equal, overlaps to 1e-9 relative, forces and torques to 1e-10
   relative to the largest entry, positions to 1e-13;
 * against the same run without the cache on a settled, bonded slab of the
@@ -21,7 +23,17 @@ import parity_cases as PC
 
 pytestmark = pytest.mark.gpu
 
-CASES = ["cluster", "periodic", "pour_mm"]
+CASES = ["cluster", "periodic", "pour_mm", "periodic_tall"]
+
+
+def _case(name):
+    if name == "periodic_tall":
+        # a periodic column taller than it is wide: images of the upper
+        # bodies lie above max y, which the reference's ghost hash tests z
+        # against (they go to a clamped cell), so those steps build the
+        # ghost lists without the cache
+        return PC.periodic(nx=2, ny=2, nz=6)
+    return PC.CASES[name]()
 
 
 def _same_lists(got, ref):
@@ -33,7 +45,7 @@ def _same_lists(got, ref):
 
 @pytest.mark.parametrize("name", CASES)
 def test_cached_steps_vs_oracle(fundem, oracle_mod, name):
-    sc = PC.CASES[name]()
+    sc = _case(name)
     g = fundem.Simulation.from_scenario(sc)
     r = max(g.geometry(k)["radius"] for k in range(len(sc.particle_geometries)))
     g.set_pair_cache(1, 0.05 * r)
@@ -67,6 +79,8 @@ def test_cached_equals_full_detection_on_settled_slab(fundem):
         s.set_pair_cache(mode)
         s.detect()
         sims[mode] = s
+    sims[1].set_profiling(False, counters=True)
+    sims[1].work_counters()
     n_checked = 0
     for block in range(15):
         for s in sims.values():
@@ -81,6 +95,11 @@ def test_cached_equals_full_detection_on_settled_slab(fundem):
         assert rel_err(sb["pos"], sa["pos"]) < 1e-12, block
         assert np.array_equal(sims[0].bonds()["activated"], sims[1].bonds()["activated"])
         n_checked += 1
+    wc = sims[1].work_counters()
+    sims[1].set_profiling(False)
+    # carried steps skip most slots by the slot bound and test the rest
+    assert wc[5] > 0 and wc[6] > 0, wc
+    print(f"cached predicate pass: {wc[5]} slots tested, {wc[6]} skipped by the slot bound")
     rebuilds, steps, _ = sims[1].pair_cache_stats()
     assert steps == 300
     # the platen moves the top of the slab by 0.5 um per step: the cache is
