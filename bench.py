@@ -248,6 +248,17 @@ def run_fundem(args, rank, world, dist):
     sim.set_pair_cache(args.pair_cache, args.pair_skin)
     sim.step(args.warmup)
     sim.sync()
+    shape = None
+    if not args.no_autotune:
+        # the narrow phase's launch shape, tuned on this state (untimed;
+        # results do not depend on it)
+        from fundem_b200 import autotune
+        best, times = autotune.launch_shape(sim, steps=10)
+        shape = {"chosen_blocks_per_sm": list(sim.launch_shape()),
+                 "order": ["select", "probe", "contact", "sums"],
+                 "ms_per_step": {",".join(str(v) for v in k): 1e3 * t / 10 for k, t in times.items()},
+                 "note": "autotune.launch_shape after the warm-up steps (10 steps per candidate, 0 = default)"}
+        log0(f"launch shape {sim.launch_shape()}")
     pc0 = sim.pair_cache_stats()
     pairs = sim.num_pairs(0)
     contacts = sim.num_contacts(0) + sim.num_contacts(1) + sum(sim.num_contacts(k) for k in (2, 3, 4))
@@ -421,6 +432,7 @@ def run_fundem(args, rank, world, dist):
                                "rebuilds (a particle drifting half the skin rebuilds them); the exact FP64 "
                                "node predicate runs on every slot every step"},
         "kernel_ms_per_step": {k: v[0] / max(args.steps, 1) for k, v in kt.items()},
+        "launch_shape": shape,
         "kernel_timing": "a second pass of K steps right after the headline, with CUDA-event timers on the "
                          "simulation's stream around each kernel group",
         "reference_gpu": ref_gpu,
@@ -766,6 +778,7 @@ def main():
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision comparison")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint cost measurement")
     ap.add_argument("--adjoint-steps", type=int, default=20000)
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default narrow-phase launch shape")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched calibration measurement")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference's own CUDA build on the same state")

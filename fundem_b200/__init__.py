@@ -31,7 +31,8 @@ EXPORTS = [
     "fundem_device_view_get", "fundem_num_contacts", "fundem_get_contacts", "fundem_set_contacts",
     "fundem_num_pairs", "fundem_num_bonds", "fundem_get_bonds", "fundem_set_bond_activation",
     "fundem_get_geometry", "fundem_get_grid", "fundem_launch_count", "fundem_set_profiling",
-    "fundem_kernel_time", "fundem_work_counters", "fundem_slot_counters", "fundem_prefix_sum", "fundem_prefix_sum_noalloc", "fundem_last_error",
+    "fundem_kernel_time", "fundem_work_counters", "fundem_slot_counters", "fundem_set_launch_shape",
+    "fundem_get_launch_shape", "fundem_prefix_sum", "fundem_prefix_sum_noalloc", "fundem_last_error",
     "fundem_adjoint_begin", "fundem_adjoint_forward", "fundem_adjoint_backward", "fundem_adjoint_end",
     "fundem_step_graph", "fundem_set_neighbour_list", "fundem_checkpoint_write", "fundem_checkpoint_read",
     "fundem_levelset_grid", "fundem_set_periodic_sector", "fundem_set_inertia_mode",
@@ -114,6 +115,8 @@ def lib():
         L.fundem_kernel_time.argtypes = [P, I, C.POINTER(C.c_double), C.POINTER(LL)]
         L.fundem_work_counters.argtypes = [P, C.POINTER(C.c_ulonglong)]
         L.fundem_slot_counters.argtypes = [P, C.POINTER(C.c_ulonglong)]
+        L.fundem_set_launch_shape.argtypes = [P, C.POINTER(C.c_int)]
+        L.fundem_get_launch_shape.argtypes = [P, C.POINTER(C.c_int)]
         L.fundem_prefix_sum.argtypes = [P, P, LL, P]
         L.fundem_prefix_sum_noalloc.argtypes = [P, P, LL, P]
         L.fundem_last_error.restype = C.c_char_p
@@ -579,6 +582,17 @@ class Simulation:
         a = (C.c_ulonglong * 5)()
         self._check(self.L.fundem_work_counters(self.h, a), "work_counters")
         return tuple(int(x) for x in a) + tuple(int(x) for x in b)
+
+    def set_launch_shape(self, select=0, probe=0, contact=0, sums=0):
+        """Blocks per SM of the narrow phase's selection, predicate pass,
+        contact-law pass and pair sums (0: default)."""
+        a = (C.c_int * 4)(int(select), int(probe), int(contact), int(sums))
+        self._check(self.L.fundem_set_launch_shape(self.h, a), "set_launch_shape")
+
+    def launch_shape(self):
+        a = (C.c_int * 4)()
+        self._check(self.L.fundem_get_launch_shape(self.h, a), "launch_shape")
+        return tuple(int(x) for x in a)
 
     def status_word(self):
         w = C.c_uint()

@@ -7,6 +7,10 @@ small K costs more checkpoints; a large K records longer segments (device
 memory grows with K).  The gradients are the same for every K, because each
 re-run repeats the forward run bit for bit.
 
+`launch_shape` picks the narrow phase's grids (blocks per SM of the
+selection, the predicate pass, the contact-law pass and the pair sums): the
+kernels loop over their work grid-stride, so the shape changes only speed.
+
 `autotune_chunk` in fundem_b200.batch does the same for the number of steps
 per CUDA graph in batched runs.
 """
@@ -41,3 +45,33 @@ def checkpoint_interval(make_sim, steps, dl_dpos, dl_dvel, candidates=(25, 50, 1
     if not times:
         raise ValueError("no candidate checkpoint interval fits the run")
     return min(times, key=times.get), times
+
+
+LAUNCH_SHAPES = ((0, 0, 0, 0), (8, 4, 4, 4), (4, 8, 4, 4), (4, 4, 8, 8), (4, 2, 2, 2), (8, 8, 8, 8), (2, 4, 4, 4))
+
+
+def launch_shape(sim, steps=20, candidates=LAUNCH_SHAPES, timer=None):
+    """Time `steps` steps of `sim` under each candidate launch shape
+    (select, probe, contact, sums blocks per SM; 0 = default), leave the
+    fastest set and return (best, {shape: seconds}).  Advances the
+    simulation by len(candidates) * steps steps (plus one untimed step per
+    candidate after the shape changes).  timer() returns a stop callable
+    giving seconds (default: wall clock around synchronised runs)."""
+    times = {}
+    for shape in candidates:
+        sim.set_launch_shape(*shape)
+        sim.step(1)
+        sim.sync()
+        if timer is None:
+            t0 = time.perf_counter()
+            sim.step(steps)
+            sim.sync()
+            times[tuple(shape)] = time.perf_counter() - t0
+        else:
+            stop = timer()
+            sim.step(steps)
+            times[tuple(shape)] = stop()
+            sim.sync()
+    best = min(times, key=times.get)
+    sim.set_launch_shape(*best)
+    return best, times

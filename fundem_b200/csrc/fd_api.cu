@@ -946,8 +946,12 @@ struct fundem_sim {
         a.records = records;
         a.flags = flags.p;
         a.stats = counters ? stats.p : nullptr;
+        for (int k = 0; k < 4; ++k) a.shape[k] = launch_shape[k];
         return a;
     }
+    // narrow-phase launch shape in blocks per SM (0: defaults), set by
+    // fundem_set_launch_shape
+    int launch_shape[4] = {0, 0, 0, 0};
 
     fd::BondDev bond_view()
     {
@@ -2336,6 +2340,28 @@ int fundem_work_counters(fundem_sim* s, unsigned long long out[5])
         FD_CUDA(cudaMemcpy(out, s->stats.p, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
         FD_CUDA(cudaMemsetAsync(s->stats.p, 0, 8 * sizeof(unsigned long long), s->stream));
     });
+}
+
+int fundem_set_launch_shape(fundem_sim* s, const int blocks_per_sm[4])
+{
+    if (!s || !blocks_per_sm) return FUNDEM_ERR_ARG;
+    for (int k = 0; k < 4; ++k)
+        if (blocks_per_sm[k] < 0 || blocks_per_sm[k] > 64) {
+            s->last_error = "blocks per SM must lie in 0 (the default) .. 64";
+            return FUNDEM_ERR_ARG;
+        }
+    return guard(s, [&] {
+        for (int k = 0; k < 4; ++k) s->launch_shape[k] = blocks_per_sm[k];
+        s->drop_graph();  // recorded graphs hold the old grids
+    });
+}
+
+int fundem_get_launch_shape(fundem_sim* s, int blocks_per_sm[4])
+{
+    if (!s || !blocks_per_sm) return FUNDEM_ERR_ARG;
+    const int def[4] = {FD_SELECT_MIN_BLOCKS, FD_PROBE_MIN_BLOCKS, 4, 4};
+    for (int k = 0; k < 4; ++k) blocks_per_sm[k] = s->launch_shape[k] > 0 ? s->launch_shape[k] : def[k];
+    return FUNDEM_OK;
 }
 
 int fundem_slot_counters(fundem_sim* s, unsigned long long out[2])

@@ -1411,18 +1411,6 @@ __device__ __forceinline__ bool node_filtered(const float4 p, const CullXf& x, c
     return true;
 }
 
-#ifndef FD_SELECT_MIN_BLOCKS
-#define FD_SELECT_MIN_BLOCKS 4
-#endif
-#ifndef FD_CONTACT_MIN_BLOCKS
-#define FD_CONTACT_MIN_BLOCKS 2
-#endif
-// the predicate pass of the contact kernels: latency-bound gathers, so as
-// many resident warps as fit without spilling
-#ifndef FD_PROBE_MIN_BLOCKS
-#define FD_PROBE_MIN_BLOCKS 4
-#endif
-
 // ---------------------------------------------------------------------------
 // narrow phase, stage 1: one warp per candidate pair.  The clusters of A's
 // surface nodes are culled against B, the nodes of the surviving clusters are
@@ -1922,12 +1910,41 @@ __global__ void __launch_bounds__(TPB, PASS == 0 ? FD_PROBE_MIN_BLOCKS : FD_CONT
     const int lane = threadIdx.x & 31;
     const bool periodic = (KIND == FD_PP || KIND == FD_PW) && (n.a.periodic_x || n.a.periodic_y);
     const int stride = gridDim.x * blockDim.x;
+    // pair cache, as in k_contact; the single-precision predicate's own
+    // rounding (a few 1e-7 of the SDF values) is covered by a margin of
+    // 1e-4 of B's grid spacing
+    constexpr bool TRANSLATED = KIND == FD_GX || KIND == FD_GY || KIND == FD_GXY;
+    const bool cache = (KIND == FD_PP || TRANSLATED) && PASS == 0 && n.a.gate != nullptr && L.c_phi0 != nullptr &&
+                       n.a.drift != nullptr;
+    const bool carried = cache && *n.a.gate == 0;
+    const bool slot_test = carried;
+    const bool phi0_store = cache && !carried;
+    const bool live_test = TRANSLATED && PASS == 0 && n.gh.live != nullptr;
     int hits = 0;
     for (int s0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); s0 < nitems; s0 += stride) {
         const int t = s0 + lane;
         const int s = (PASS == 1 && t < nitems) ? L.c_hit[t] : t;
         bool hit = false;
-        if (t < nitems) {
+        bool continue_slot = false;
+        if ((slot_test || live_test) && t < nitems) {
+            const int p = L.c_pair[s];
+            const int A = L.pairA[p];
+            const int B = L.pairB[p];
+            if (live_test && !n.gh.live[B]) {
+                L.c_node[s] = -1;
+                if (phi0_store) L.c_phi0[s] = __int_as_float(0xff800000);  // -inf: never skipped
+                continue_slot = true;
+            } else if (slot_test) {
+                const FdGeo& GB = Slave<KIND>::geo(n, B);
+                const float lip = __fmul_ru(__double2float_ru(GB.lip), 1.000001f);
+                const float bound = __fmul_ru(lip, __fadd_ru(n.a.drift[A], n.a.drift[B]));
+                if (L.c_phi0[s] > __fadd_ru(bound, __double2float_ru(1e-4 * GB.spacing))) {
+                    L.c_node[s] = -1;
+                    continue_slot = true;
+                }
+            }
+        }
+        if (t < nitems && !continue_slot) {
             const int p = L.c_pair[s];
             const int k = L.c_k[s];
             const int A = L.pairA[p];
@@ -1949,7 +1966,9 @@ __global__ void __launch_bounds__(TPB, PASS == 0 ? FD_PROBE_MIN_BLOCKS : FD_CONT
             const v3f r = tof(rd);  // node offset from A's centre
             int3 lo, hi;
             fd_node_range(gp, sg, lo, hi);
-            float ov = 0.f, fx = 0.f, fy = 0.f, fz = 0.f, pv[8];
+            // an overlap the predicate did not reach stays +inf (a slot that
+            // is never skipped)
+            float ov = PASS == 0 ? __int_as_float(0x7f800000) : 0.f, fx = 0.f, fy = 0.f, fz = 0.f, pv[8];
             if (aux.x >= lo.x && aux.x <= hi.x && aux.y >= lo.y && aux.y <= hi.y && aux.z >= lo.z && aux.z <= hi.z) {
                 const double3 rel = mk3(gp.x - cB.x, gp.y - cB.y, gp.z - cB.z);
                 if (!Slave<KIND>::radius_test || xm_len2(rel) <= GB.radius * GB.radius) {
@@ -1992,6 +2011,7 @@ __global__ void __launch_bounds__(TPB, PASS == 0 ? FD_PROBE_MIN_BLOCKS : FD_CONT
                     }
                 }
             }
+            if (phi0_store) L.c_phi0[s] = -ov;
             int nid = -1;
             if (PASS == 1 && hit) {
                 // gradient with the x weight truncated as the reference does
@@ -2726,10 +2746,13 @@ void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& 
     if (gh) n.gh = *gh; else memset(&n.gh, 0, sizeof(n.gh));
     n.L = L; n.a = a; n.with_force = with_force;
     const long long need = ((long long)L.cap_pairs + NARROW_WARPS - 1) / NARROW_WARPS;
-    // grid-stride kernels: one resident wave at most (the pair and slot
-    // counts are known only on the device)
-    const int grid = (int)(need < 148 * FD_SELECT_MIN_BLOCKS ? (need > 0 ? need : 1) : 148 * FD_SELECT_MIN_BLOCKS);
-    const int cgrid = 148 * 4;
+    // grid-stride kernels sized in blocks per SM (the pair and slot counts
+    // are known only on the device): the defaults fill one resident wave
+    const int sel_bps = a.shape[0] > 0 ? a.shape[0] : FD_SELECT_MIN_BLOCKS;
+    const int grid = (int)std::max(1ll, std::min(need, 148ll * sel_bps));
+    const int pgrid0 = 148 * (a.shape[1] > 0 ? a.shape[1] : FD_PROBE_MIN_BLOCKS);
+    const int cgrid = 148 * (a.shape[2] > 0 ? a.shape[2] : 4);
+    const int sgrid = 148 * (a.shape[3] > 0 ? a.shape[3] : 4);
 #define FD_NARROW_CASE(K)                                                              \
     case K:                                                                            \
         k_select<K><<<grid, NARROW_WARPS * 32, 0, s>>>(n); note_launch();                             \
@@ -2738,10 +2761,10 @@ void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& 
             note_launch();                                                             \
         }                                                                              \
         if (mixed) {                                                                   \
-            k_contact32<K, 0><<<cgrid, TPB, 0, s>>>(n); note_launch();                                \
+            k_contact32<K, 0><<<pgrid0, TPB, 0, s>>>(n); note_launch();                               \
             k_contact32<K, 1><<<cgrid, TPB, 0, s>>>(n); note_launch();                                \
         } else {                                                                       \
-            k_contact<K, 0><<<cgrid, TPB, 0, s>>>(n); note_launch();                                  \
+            k_contact<K, 0><<<pgrid0, TPB, 0, s>>>(n); note_launch();                                 \
             k_contact<K, 1><<<cgrid, TPB, 0, s>>>(n); note_launch();                                  \
         }                                                                              \
         break;
@@ -2758,19 +2781,19 @@ void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& 
         // the ghost traits read, so they share the ghost kernels
         k_select<FD_GX><<<grid, NARROW_WARPS * 32, 0, s>>>(n); note_launch();
         if (mixed) {
-            k_contact32<FD_GX, 0><<<cgrid, TPB, 0, s>>>(n); note_launch();
+            k_contact32<FD_GX, 0><<<pgrid0, TPB, 0, s>>>(n); note_launch();
             k_contact32<FD_GX, 1><<<cgrid, TPB, 0, s>>>(n); note_launch();
         } else {
-            k_contact<FD_GX, 0><<<cgrid, TPB, 0, s>>>(n); note_launch();
+            k_contact<FD_GX, 0><<<pgrid0, TPB, 0, s>>>(n); note_launch();
             k_contact<FD_GX, 1><<<cgrid, TPB, 0, s>>>(n); note_launch();
         }
         break;
     }
 #undef FD_NARROW_CASE
     if (mixed) {
-        k_pair_sum32<<<148 * 4, TPB, 0, s>>>(L, with_force);
+        k_pair_sum32<<<sgrid, TPB, 0, s>>>(L, with_force);
     } else {
-        k_pair_sum<<<148 * 4, TPB, 0, s>>>(L, with_force);
+        k_pair_sum<<<sgrid, TPB, 0, s>>>(L, with_force);
     }
     note_launch();
 }

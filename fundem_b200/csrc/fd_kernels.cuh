@@ -2,6 +2,20 @@
 #pragma once
 #include "fd_internal.cuh"
 
+// resident blocks per SM the narrow-phase kernels are compiled for (their
+// default grids fill one wave of them)
+#ifndef FD_SELECT_MIN_BLOCKS
+#define FD_SELECT_MIN_BLOCKS 4
+#endif
+#ifndef FD_CONTACT_MIN_BLOCKS
+#define FD_CONTACT_MIN_BLOCKS 2
+#endif
+// the predicate pass of the contact kernels: latency-bound gathers, so as
+// many resident warps as fit without spilling
+#ifndef FD_PROBE_MIN_BLOCKS
+#define FD_PROBE_MIN_BLOCKS 4
+#endif
+
 namespace fd {
 
 // Everything one simulation keeps on the device.  Plain pointers; ownership
@@ -259,6 +273,9 @@ struct StepArgs {
     const int* gate;   // pair cache: the selection runs only when *gate != 0 (null: always)
     const float* drift;  // pair cache: per-particle drift bounds (see PairCacheDev)
     const int* noskin;   // non-null and nonzero: this step's selection takes no skin
+    // launch shape of the narrow phase, in blocks per SM (0: the default):
+    // selection, predicate pass, contact-law pass, pair sums
+    int shape[4];
     unsigned int* flags;
     unsigned long long* stats;  // optional: pairs, clusters, clusters kept, contacts (narrow kernels)
 };

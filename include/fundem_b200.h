@@ -390,6 +390,14 @@ int fundem_work_counters(fundem_sim* sim, unsigned long long out[5]);
    the partner at the last rebuild by more than the SDF's Lipschitz bound
    times both bodies' drift since (such a slot cannot hold a contact) */
 int fundem_slot_counters(fundem_sim* sim, unsigned long long out[2]);
+/* launch shape of the narrow phase, in blocks per SM, for the selection, the
+   predicate pass, the contact-law pass and the per-pair sums (grid-stride
+   kernels: results do not depend on it); 0 keeps a kernel's default, each
+   value 0..64.  The reference takes a caller-chosen grid per launcher
+   (gridD, blockD of every launcher, e.g. LSParticleContactDetectionKernel.cu:609).
+   fundem_get_launch_shape returns the shape in use, defaults resolved. */
+int fundem_set_launch_shape(fundem_sim* sim, const int blocks_per_sm[4]);
+int fundem_get_launch_shape(fundem_sim* sim, int blocks_per_sm[4]);
 
 #ifdef __cplusplus
 }
