@@ -259,6 +259,12 @@ def run_fundem(args, rank, world, dist):
                  "ms_per_step": {",".join(str(v) for v in k): 1e3 * t / 10 for k, t in times.items()},
                  "note": "autotune.launch_shape after the warm-up steps (10 steps per candidate, 0 = default)"}
         log0(f"launch shape {sim.launch_shape()}")
+    if not args.no_graph:
+        # the headline replays one CUDA graph of K steps (fundem_step_graph);
+        # record it here, untimed, for both list generations it can start on
+        sim.step_graph(args.steps)
+        sim.step_graph(args.steps)
+        sim.sync()
     pc0 = sim.pair_cache_stats()
     pairs = sim.num_pairs(0)
     contacts = sim.num_contacts(0) + sim.num_contacts(1) + sum(sim.num_contacts(k) for k in (2, 3, 4))
@@ -273,9 +279,13 @@ def run_fundem(args, rank, world, dist):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if args.profile:
         torch.cuda.profiler.start()
-    # the headline: K plain steps, no kernel timers
+    # the headline: K steps, no kernel timers (one graph replay, or plain
+    # launches with --no-graph)
     e0.record()
-    sim.step(args.steps)
+    if args.no_graph:
+        sim.step(args.steps)
+    else:
+        sim.step_graph(args.steps)
     e1.record()
     torch.cuda.synchronize()
     if args.profile:
@@ -290,6 +300,15 @@ def run_fundem(args, rank, world, dist):
     contacts_end = sim.num_contacts(0) + sim.num_contacts(1) + sum(sim.num_contacts(k) for k in (2, 3, 4))
     t_max, value = aggregate(ms, n, args.steps, world, dist, "cuda")
     log0(f"timed: {ms / args.steps:.4f} ms/step, clocks {clk}")
+    # the same K steps with plain launches (every kernel launched from the
+    # host), for comparison
+    torch.cuda.synchronize()
+    e0.record()
+    sim.step(args.steps)
+    e1.record()
+    torch.cuda.synchronize()
+    plain_ms = e0.elapsed_time(e1) / args.steps
+    log0(f"plain launches: {plain_ms:.4f} ms/step")
     # the same K steps again with the kernel-group timers on (CUDA events on
     # the simulation's stream around each group): per-kernel times and the
     # roofline's launch duration
@@ -417,6 +436,9 @@ def run_fundem(args, rank, world, dist):
                 "note": "state uploaded from host arrays, each step a one-step CUDA-graph replay "
                         "(fundem_step_graph) followed by a read of the status word, state downloaded"},
         "graph": graph,
+        "headline_path": "plain launches (fundem_step)" if args.no_graph else
+                         "one CUDA graph of K steps replayed (fundem_step_graph), recorded before the timed region",
+        "plain_launches_ms_per_step": plain_ms,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk, "unit": "GB/s",
                      "frac": (achieved / pk) if achieved else None,
                      "traffic": (traffic_per_pair * pairs) if traffic_per_pair else None,
@@ -544,11 +566,19 @@ def mixed_vs_fp64(sc, dev, args, dist, world):
     ms = {}
     for prec, s in sims.items():
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if not args.no_graph:
+            # timed as the headline: a K-step graph, recorded untimed
+            s.step_graph(args.steps)
+            s.step_graph(args.steps)
+            s.sync()
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
         e0.record()
-        s.step(args.steps)
+        if args.no_graph:
+            s.step(args.steps)
+        else:
+            s.step_graph(args.steps)
         e1.record()
         torch.cuda.synchronize()
         s.sync()
@@ -779,6 +809,7 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint cost measurement")
     ap.add_argument("--adjoint-steps", type=int, default=20000)
     ap.add_argument("--no-autotune", action="store_true", help="keep the default narrow-phase launch shape")
+    ap.add_argument("--no-graph", action="store_true", help="time plain launches instead of a K-step graph replay")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched calibration measurement")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference's own CUDA build on the same state")

@@ -1,4 +1,4 @@
-// fd_adjoint.cu -- reverse sweep of the timestep for translating bodies.
+// fd_adjoint.cu -- reverse sweep of the timestep.
 //
 // The forward step (LSSolver.h:1033-1107 with the contact law of
 // contactKernel.cuh:4-77 and the bond law of contactKernel.cuh:138-199) is
@@ -12,10 +12,17 @@
 //   [Phi^T]  xbar_{n+1}, vbar_h, Sbar_n, parameter adjoints
 //   vbar_h  += vbar_{n+1} + xbar_{n+1} dt
 //   xbar_n   = xbar_{n+1};  vbar_n = vbar_h;  Fbar_n = vbar_h dt / (2 m)
+// Turning bodies add (particleIntegrationKernel.cu:3-48, myQua.h:77-93)
+//   w_h     = w_n + W(q_n, w_n, T_n) dt / 2,  W = I_w^-1 (T - w x I_w w),
+//             I_w = R(q) I R(q)^T
+//   q_{n+1} = normalise(q_n + (0, w_h dt / 2) (x) q_n)
+//   (F, T_{n+1}, S_{n+1}) = Phi(x, q_{n+1}, v_h, w_h, S_n; ...)
+//   w_{n+1} = w_h + W(q_{n+1}, w_h, T_{n+1}) dt / 2
+// reversed with forward-mode duals over (q, w) per particle, and the torques'
+// lever arms and the partner's orientation in Phi's Jacobian.
 // Contact topology is frozen at each step (replayed from the forward
 // record), including the stick/slip branch of each contact and bond
-// breakage.  Orientations do not change (zero inverse inertia), so only
-// translations are differentiated.
+// breakage.
 //
 // Phi^T is applied contact by contact: the local Jacobian of (force, new
 // spring) with respect to (node position relative to the partner, relative
@@ -622,14 +629,15 @@ __global__ void k_adj_particle(AdjParticles a, double dt)
             else whb[k - 4] += g;
         }
     }
-    // first half kick wh = w_n + W(q_n, w_n, T_n) dt / 2 (skipped for fixed bodies)
+    // first half kick wh = w_n + W(q_n, w_n, T_n) dt / 2 (skipped for fixed
+    // bodies), w_n the angular velocity the previous step ended with
     double wbn[3] = {whb[0], whb[1], whb[2]};
     double Teb[3] = {0.0, 0.0, 0.0};
     if (im != 0.0) {
         const double h = 0.5 * dt;
         D7 q[4];
         for (int k = 0; k < 4; ++k) q[k] = D7::var(pp[k], k);
-        const V3<D7> w{D7::var(pp[4], 4), D7::var(pp[5], 5), D7::var(pp[6], 6)};
+        const V3<D7> w{D7::var(pp[10], 4), D7::var(pp[11], 5), D7::var(pp[12], 6)};
         const V3<D7> acc = w_accel(q, w, make_double3(pp[7], pp[8], pp[9]), geo);
         for (int k = 0; k < 7; ++k) {
             const double g = h * (whb[0] * acc.x.d[k] + whb[1] * acc.y.d[k] + whb[2] * acc.z.d[k]);
@@ -665,7 +673,9 @@ __global__ void k_adj_record(ObjDev P, double* dst, int what)
     }
     if (what & ADJ_REC_T) {
         const double3 t = P.torque[i];
+        const double3 w = P.angvel[i];
         d[7] = t.x; d[8] = t.y; d[9] = t.z;
+        d[10] = w.x; d[11] = w.y; d[12] = w.z;
     }
 }
 

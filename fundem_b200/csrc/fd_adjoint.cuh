@@ -32,7 +32,10 @@ struct AdjParticles {
     double* Tb;     // adjoint of the step's torques
     double* Teb;    // adjoint of the torques reaching the next step's first half-kick
 };
-constexpr int ADJ_PREC = 10;  // doubles per particle and step in the record
+// doubles per particle and step in the record: orientation after the drift
+// (4), angular velocity at force time (3), torque (3), angular velocity at the
+// step's end, after the second half kick (3)
+constexpr int ADJ_PREC = 13;
 
 struct AdjContactArgs {
     AdjRec rec;            // the list at this step
@@ -64,7 +67,8 @@ void adj_contacts(const AdjParticles& a, const AdjContactArgs& c, cudaStream_t s
 void adj_bonds(const AdjParticles& a, const AdjBondArgs& b, cudaStream_t s);
 void adj_particles(const AdjParticles& a, double dt, cudaStream_t s);
 // the record of turning bodies: orientation and angular velocity (after a
-// drift), torque (after the forces), or all three (a segment's start)
+// drift), torque and angular velocity at the end of the step (after the
+// second half kick), or all (a segment's start)
 void adj_record_rot(const ObjDev& P, double* dst, int what, cudaStream_t s);
 enum { ADJ_REC_QW = 1, ADJ_REC_T = 2 };
 

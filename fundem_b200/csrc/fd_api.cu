@@ -852,6 +852,7 @@ struct fundem_sim {
         int steps = 0;
         double key[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // gravity, dt, precision, records, counters, periodicity
         unsigned long long epoch = 0, gepoch = 0;  // allocation counters at the capture
+        long long kernels = 0;                     // kernel launches one replay runs
     };
     StepGraph graphs[2];
     cudaStream_t cap_stream = nullptr;
@@ -1894,6 +1895,7 @@ int fundem_step_graph(fundem_sim* s, int nsteps, const double g[3], double dt)
             const unsigned long long epoch = s->alloc_epoch, gepoch = g_alloc_epoch.load();
             s->stream = s->cap_stream;
             s->capturing = true;
+            const long long launches0 = s->launches;
             cudaGraph_t graph = nullptr;
             cudaError_t e = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
             try {
@@ -1921,6 +1923,10 @@ int fundem_step_graph(fundem_sim* s, int nsteps, const double g[3], double dt)
             e = cudaGraphInstantiate(&G.exec, graph, 0);
             cudaGraphDestroy(graph);
             FD_CUDA(e);
+            // the capture noted the kernels without running them: they count
+            // when a replay runs them
+            G.kernels = s->launches - launches0;
+            s->launches = launches0;
             G.steps = nsteps;
             std::copy(key, key + 8, G.key);
             G.epoch = epoch;
@@ -1933,6 +1939,7 @@ int fundem_step_graph(fundem_sim* s, int nsteps, const double g[3], double dt)
         }
         s->pc_prepare();
         FD_CUDA(cudaGraphLaunch(G.exec, s->stream));
+        s->launches += G.kernels;
         // the launch leaves the newest lists in the generation nsteps flips on
         if (nsteps & 1)
             for (int k = 0; k < FD_NKIND; ++k) s->lists[k].cur ^= 1;
