@@ -853,6 +853,7 @@ struct fundem_sim {
         double key[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // gravity, dt, precision, records, counters, periodicity
         unsigned long long epoch = 0, gepoch = 0;  // allocation counters at the capture
         long long kernels = 0;                     // kernel launches one replay runs
+        long long pc_steps = 0;                    // steps of it that run the pair cache
     };
     StepGraph graphs[2];
     cudaStream_t cap_stream = nullptr;
@@ -1895,7 +1896,7 @@ int fundem_step_graph(fundem_sim* s, int nsteps, const double g[3], double dt)
             const unsigned long long epoch = s->alloc_epoch, gepoch = g_alloc_epoch.load();
             s->stream = s->cap_stream;
             s->capturing = true;
-            const long long launches0 = s->launches;
+            const long long launches0 = s->launches, pc_steps0 = s->pc_steps;
             cudaGraph_t graph = nullptr;
             cudaError_t e = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
             try {
@@ -1927,6 +1928,8 @@ int fundem_step_graph(fundem_sim* s, int nsteps, const double g[3], double dt)
             // when a replay runs them
             G.kernels = s->launches - launches0;
             s->launches = launches0;
+            G.pc_steps = s->pc_steps - pc_steps0;
+            s->pc_steps = pc_steps0;
             G.steps = nsteps;
             std::copy(key, key + 8, G.key);
             G.epoch = epoch;
@@ -1940,6 +1943,7 @@ int fundem_step_graph(fundem_sim* s, int nsteps, const double g[3], double dt)
         s->pc_prepare();
         FD_CUDA(cudaGraphLaunch(G.exec, s->stream));
         s->launches += G.kernels;
+        s->pc_steps += G.pc_steps;
         // the launch leaves the newest lists in the generation nsteps flips on
         if (nsteps & 1)
             for (int k = 0; k < FD_NKIND; ++k) s->lists[k].cur ^= 1;

@@ -242,25 +242,33 @@ __global__ void __launch_bounds__(RS_TPB) k_rs_scatter(const unsigned long long*
 // dense table: objects per cell (atomic count), slots by an atomic scatter,
 // then each cell's slots put in ascending object index, so the table equals
 // the one a stable sort of the hashes gives
-__global__ void k_cell_count(const long long* hash, int n, long long num, int* count)
+__global__ void k_clear_cells(int* a, int* b, long long n, const int* gate)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || (gate && *gate == 0)) return;
+    a[i] = 0;
+    b[i] = 0;
+}
+__global__ void k_cell_count(const long long* hash, int n, long long num, int* count, const int* gate)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= n || (gate && *gate == 0)) return;
     const long long h = hash[i];
     if (h >= 0 && h < num) atomicAdd(&count[h], 1);
 }
-__global__ void k_cell_scatter(const long long* hash, int n, long long num, const int* start, int* fill, int* sorted)
+__global__ void k_cell_scatter(const long long* hash, int n, long long num, const int* start, int* fill, int* sorted,
+                               const int* gate)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= n || (gate && *gate == 0)) return;
     const long long h = hash[i];
     if (h < 0 || h >= num) return;
     sorted[start[h] + atomicAdd(&fill[h], 1)] = i;
 }
-__global__ void k_cell_order(long long num, const int* count, const int* start, int* sorted)
+__global__ void k_cell_order(long long num, const int* count, const int* start, int* sorted, const int* gate)
 {
     const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= num) return;
+    if (c >= num || (gate && *gate == 0)) return;
     const int m = count[c];
     if (m < 2) return;
     int* seg = sorted + start[c];
@@ -739,6 +747,23 @@ __device__ __forceinline__ void partner_search_range(double3 c, double reach, co
     hi.z = cell_index_clamped(c.z + reach, g.minb.z, g.inv.z, g.size.z);
 }
 
+// The cells a body's ghost search covers: those within `reach` of its
+// centre, and every cell next to a cell its nodes (within rA of the centre)
+// can occupy.  The predicate takes an image as a candidate of a node when the
+// image's cell is next to the node's (LSParticleContactDetectionKernel.cu:
+// 431-607); an image outside the domain in y or z sits in a clamped cell
+// (mySpatialGrid.cu:214-240) that its position does not reach, and only the
+// node neighbourhoods find it.
+__device__ __forceinline__ void ghost_search_range(double3 c, double rA, double reach, const FdGrid& g, int3& lo,
+                                                   int3& hi)
+{
+    partner_search_range(c, reach, g, lo, hi);
+    int3 blo, bhi;
+    body_search_range(c, rA, g, blo, bhi);
+    lo = make_int3(min(lo.x, blo.x), min(lo.y, blo.y), min(lo.z, blo.z));
+    hi = make_int3(max(hi.x, bhi.x), max(hi.y, bhi.y), max(hi.z, bhi.z));
+}
+
 #ifndef FD_BROAD_LANES
 #define FD_BROAD_LANES 8
 #endif
@@ -814,21 +839,11 @@ __global__ void __launch_bounds__(TPB) k_broad_cells(ObjDev P, GeoSetDev G, Cell
             nl.ref[A] = cA;
             nl.vis[A] = P.hash[A] >= 0;
         }
-        if (NLB) {
-            // periodic directions: the cell range wraps around
-            const int3 s3 = T.g.size;
-            if (nl.periodic_x) {
-                lo.x = (int)floor((cA.x - reach - T.g.minb.x) * T.g.inv.x);
-                hi.x = (int)floor((cA.x + reach - T.g.minb.x) * T.g.inv.x);
-                if (hi.x - lo.x + 1 >= s3.x) { lo.x = 0; hi.x = s3.x - 1; }
-            }
-            if (nl.periodic_y) {
-                lo.y = (int)floor((cA.y - reach - T.g.minb.y) * T.g.inv.y);
-                hi.y = (int)floor((cA.y + reach - T.g.minb.y) * T.g.inv.y);
-                if (hi.y - lo.y + 1 >= s3.y) { lo.y = 0; hi.y = s3.y - 1; }
-            }
+        if (GHOST) {
+            ghost_search_range(cA, rA * (1.0 + 8.0 * BOUND_REL) + skin, reach, T.g, lo, hi);
+        } else {
+            partner_search_range(cA, reach, T.g, lo, hi);
         }
-        partner_search_range(cA, reach, T.g, lo, hi);
         if (occ) {
             // only the cells that hold ghost images
             lo.x = max(lo.x, occ[0]); lo.y = max(lo.y, occ[1]); lo.z = max(lo.z, occ[2]);
@@ -843,12 +858,8 @@ __global__ void __launch_bounds__(TPB) k_broad_cells(ObjDev P, GeoSetDev G, Cell
         int cc = 0, cs = 0;
         const int ci = c0 + gl;
         if (ci < ncell) {
-            int x = lo.x + ci % nx, y = lo.y + (ci / nx) % ny;
+            const int x = lo.x + ci % nx, y = lo.y + (ci / nx) % ny;
             const int z = lo.z + ci / (nx * ny);
-            if (NLB) {
-                x = ((x % T.g.size.x) + T.g.size.x) % T.g.size.x;
-                y = ((y % T.g.size.y) + T.g.size.y) % T.g.size.y;
-            }
             const long long h = fd_lin3(x, y, z, T.g.size);
             cc = cell_lookup(T, h, cs);
         }
@@ -1107,7 +1118,7 @@ __global__ void k_ghost_searchers(ObjDev P, GeoSetDev G, FdGrid g, const int* oc
     const double rA = G.geo[P.geo[A]].radius;
     const double reach = (rA + G.grid_rmax) * (1.0 + 8.0 * BOUND_REL) + skin;
     int3 lo, hi;
-    partner_search_range(P.pos[A], reach, g, lo, hi);
+    ghost_search_range(P.pos[A], rA * (1.0 + 8.0 * BOUND_REL) + skin, reach, g, lo, hi);
     const bool any = max(lo.x, occ[0]) <= min(hi.x, occ[3]) && max(lo.y, occ[1]) <= min(hi.y, occ[4]) &&
                      max(lo.z, occ[2]) <= min(hi.z, occ[5]);
     if (any) {
@@ -2633,12 +2644,18 @@ void launch_cell_table(ObjDev& O, CellTableDev& T, int* scan_tmp, size_t, cudaSt
         return;
     }
     // dense grids: count, scan, scatter, then each cell in object order
-    cudaMemsetAsync(T.count, 0, sizeof(int) * T.g.num, s);
-    k_cell_count<<<nblocks(O.n), TPB, 0, s>>>(O.hash, O.n, T.g.num, T.count); note_launch();
-    scan_exclusive(T.count, T.start, T.g.num, scan_tmp, s);
-    cudaMemsetAsync(T.fill, 0, sizeof(int) * T.g.num, s);
-    k_cell_scatter<<<nblocks(O.n), TPB, 0, s>>>(O.hash, O.n, T.g.num, T.start, T.fill, T.sorted); note_launch();
-    k_cell_order<<<nblocks(T.g.num), TPB, 0, s>>>(T.g.num, T.count, T.start, T.sorted); note_launch();
+    if (gate) {
+        k_clear_cells<<<nblocks(T.g.num), TPB, 0, s>>>(T.count, T.fill, T.g.num, gate);
+        note_launch();
+    } else {
+        cudaMemsetAsync(T.count, 0, sizeof(int) * T.g.num, s);
+        cudaMemsetAsync(T.fill, 0, sizeof(int) * T.g.num, s);
+    }
+    k_cell_count<<<nblocks(O.n), TPB, 0, s>>>(O.hash, O.n, T.g.num, T.count, gate); note_launch();
+    scan_exclusive(T.count, T.start, T.g.num, scan_tmp, s, gate);
+    k_cell_scatter<<<nblocks(O.n), TPB, 0, s>>>(O.hash, O.n, T.g.num, T.start, T.fill, T.sorted, gate);
+    note_launch();
+    k_cell_order<<<nblocks(T.g.num), TPB, 0, s>>>(T.g.num, T.count, T.start, T.sorted, gate); note_launch();
 }
 void launch_wrap(ObjDev& P, const FdGrid& g, int dim, cudaStream_t s, int* ctrl)
 {
