@@ -486,6 +486,7 @@ struct PairList {
     // slot and pair scratch of the current step only
     DevArray<int> c_pair, c_hit, p_hist_cnt;
     DevArray<float> c_phi0;  // pair cache: slot bounds of the last rebuild
+    DevArray<float> p_bound; // pair cache: per-pair drift bound of a carried step
     DevArray<double> c_force;
     DevArray<int4> p_aux;
     bool allocated = false;
@@ -507,7 +508,7 @@ struct PairList {
         }
         c_pair.alloc(cap_contacts); c_hit.alloc(cap_contacts, false); c_force.alloc((size_t)cap_contacts * 9);
         c_phi0.alloc(cap_contacts, false);
-        p_aux.alloc(cap_pairs); p_hist_cnt.alloc(cap_pairs);
+        p_aux.alloc(cap_pairs); p_hist_cnt.alloc(cap_pairs); p_bound.alloc(cap_pairs, false);
         allocated = true;
     }
     void grow(int capp, int capc)
@@ -519,6 +520,7 @@ struct PairList {
             }
             p_aux.grow(capp, 0);
             p_hist_cnt.grow(capp, 0);
+            p_bound.grow(capp, 0);
             cap_pairs = capp;
         }
         if (capc > cap_contacts) {
@@ -552,6 +554,7 @@ struct PairList {
         v.c_pair = c_pair.p; v.c_hit = c_hit.p; v.c_k = c.c_k.p; v.o_c_k = o.c_k.p; v.c_force = c_force.p; v.p_aux = p_aux.p; v.p_hist_cnt = p_hist_cnt.p;
         v.o_c_node = o.c_node.p; v.o_c_spring = o.c_spring.p;
         v.c_phi0 = c_phi0.p;
+        v.p_bound = p_bound.p;
         return v;
     }
 };

@@ -1057,7 +1057,8 @@ __global__ void k_pc_check(ObjDev P, PairCacheDev c)
 // a step without a rebuild: this step's pairs and slots are the previous
 // step's, carried over; each pair's history is its own slots of the previous
 // step, and its partner's cell is taken from this step's hash
-__global__ void k_pc_carry(PairListDev L, int n_obj, const long long* hash, FdGrid g, const int* gate)
+__global__ void k_pc_carry(PairListDev L, int n_obj, const long long* hash, FdGrid g, const int* gate,
+                           const float* drift, const int* geo_of, const FdGeo* geos, float spacing_margin)
 {
     if (*gate != 0) return;
     const int npairs = min(L.o_counters[0], L.cap_pairs);
@@ -1073,10 +1074,22 @@ __global__ void k_pc_carry(PairListDev L, int n_obj, const long long* hash, FdGr
         L.seg_cnt[i] = L.o_seg_cnt[i];
     }
     for (long long p = t0; p < npairs; p += stride) {
+        const int A = L.o_pairA[p];
         const int B = L.o_pairB[p];
         const int off = L.o_c_off[p], cnt = L.o_c_cnt[p];
-        L.pairA[p] = L.o_pairA[p];
+        L.pairA[p] = A;
         L.pairB[p] = B;
+        if (drift && L.p_bound) {
+            // the slot bound's right-hand side for the pair (see k_contact):
+            // lip_B (drift_A + drift_B), rounded up, plus a margin in units of
+            // B's grid spacing (the single-precision predicate's rounding)
+            const FdGeo& GB = geos[geo_of[B]];
+            const float lip = __double2float_ru(GB.lip);
+            float bound = __fmul_ru(lip, __fadd_ru(drift[A], drift[B]));
+            if (spacing_margin > 0.f)
+                bound = __fadd_ru(__fmul_ru(bound, 1.000001f), __fmul_ru(spacing_margin, __double2float_ru(GB.spacing)));
+            L.p_bound[p] = bound;
+        }
         L.c_off[p] = off;
         L.c_cnt[p] = cnt;
         if (cnt > 0) {
@@ -1589,9 +1602,7 @@ __global__ void __launch_bounds__(TPB, PASS == 0 ? FD_PROBE_MIN_BLOCKS : FD_CONT
         bool hit = false;
         if ((slot_test || live_test) && t < nitems) {
             const int p = L.c_pair[s];
-            const int A = L.pairA[p];
-            const int B = L.pairB[p];
-            if (live_test && !n.gh.live[B]) {
+            if (live_test && !n.gh.live[L.pairB[p]]) {
                 L.c_node[s] = -1;
                 if (phi0_store) L.c_phi0[s] = __int_as_float(0xff800000);  // -inf: never skipped
                 continue_slot = true;
@@ -1600,10 +1611,9 @@ __global__ void __launch_bounds__(TPB, PASS == 0 ? FD_PROBE_MIN_BLOCKS : FD_CONT
                 // was outside B at the rebuild by more than the SDF can change
                 // under both bodies' drift since: |grad phi| <= lip (trilinear
                 // bound), and the node's offset in B's frame moved by at most
-                // the sum of the drift bounds (an image moves with its body)
-                const float lip = __double2float_ru(Slave<KIND>::geo(n, B).lip);
-                const float bound = __fmul_ru(lip, __fadd_ru(n.a.drift[A], n.a.drift[B]));
-                if (L.c_phi0[s] > __fadd_ru(bound, 1e-12f)) {
+                // the sum of the drift bounds (an image moves with its body);
+                // k_pc_carry stored lip_B (drift_A + drift_B) per pair
+                if (L.c_phi0[s] > __fadd_ru(L.p_bound[p], 1e-12f)) {
                     L.c_node[s] = -1;
                     continue_slot = true;
                 }
@@ -1645,9 +1655,11 @@ __global__ void __launch_bounds__(TPB, PASS == 0 ? FD_PROBE_MIN_BLOCKS : FD_CONT
                 int hist = -1;
                 {
                     // the previous slots of the pair are ascending in node
-                    // key; a node appears at most once per pair
+                    // key; a node appears at most once per pair.  A carried
+                    // layout keeps each slot's previous self at its index.
                     const int oc_off = aux.w, oc_end = aux.w + L.p_hist_cnt[p];
                     int lo = oc_off, hi = oc_end;
+                    if (s >= oc_off && s < oc_end && L.o_c_k[s] == k) lo = hi = s;
                     while (lo < hi) {
                         const int mid = (lo + hi) >> 1;
                         if (L.o_c_k[mid] < k) lo = mid + 1; else hi = mid;
@@ -1815,11 +1827,18 @@ __global__ void k_pair_sum(PairListDev L, int with_force)
             o = L.c_off[p];
             c = L.c_cnt[p];
         }
-        for (int j = l; j < c; j += 8) {
-            if (L.c_node[o + j] < 0) continue;
-            const double* f = L.c_force + 9ll * (o + j);
+        // slots l, l + 8, l + 16, ... in order; four node ids loaded ahead
+        for (int j0 = l; j0 < c; j0 += 32) {
+            int nd[4];
 #pragma unroll
-            for (int t = 0; t < 9; ++t) acc[t] += f[t];
+            for (int u = 0; u < 4; ++u) nd[u] = j0 + 8 * u < c ? L.c_node[o + j0 + 8 * u] : -1;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (nd[u] < 0) continue;
+                const double* f = L.c_force + 9ll * (o + j0 + 8 * u);
+#pragma unroll
+                for (int t = 0; t < 9; ++t) acc[t] += f[t];
+            }
         }
         // pairs without contact slots keep no sum: k_reduce skips them by
         // their slot count
@@ -1923,7 +1942,7 @@ __global__ void __launch_bounds__(TPB, PASS == 0 ? FD_PROBE_MIN_BLOCKS : FD_CONT
     const int stride = gridDim.x * blockDim.x;
     // pair cache, as in k_contact; the single-precision predicate's own
     // rounding (a few 1e-7 of the SDF values) is covered by a margin of
-    // 1e-4 of B's grid spacing
+    // 1e-4 of B's grid spacing in the pair bound
     constexpr bool TRANSLATED = KIND == FD_GX || KIND == FD_GY || KIND == FD_GXY;
     const bool cache = (KIND == FD_PP || TRANSLATED) && PASS == 0 && n.a.gate != nullptr && L.c_phi0 != nullptr &&
                        n.a.drift != nullptr;
@@ -1939,17 +1958,15 @@ __global__ void __launch_bounds__(TPB, PASS == 0 ? FD_PROBE_MIN_BLOCKS : FD_CONT
         bool continue_slot = false;
         if ((slot_test || live_test) && t < nitems) {
             const int p = L.c_pair[s];
-            const int A = L.pairA[p];
-            const int B = L.pairB[p];
+            const int B = live_test ? L.pairB[p] : 0;
             if (live_test && !n.gh.live[B]) {
                 L.c_node[s] = -1;
                 if (phi0_store) L.c_phi0[s] = __int_as_float(0xff800000);  // -inf: never skipped
                 continue_slot = true;
             } else if (slot_test) {
-                const FdGeo& GB = Slave<KIND>::geo(n, B);
-                const float lip = __fmul_ru(__double2float_ru(GB.lip), 1.000001f);
-                const float bound = __fmul_ru(lip, __fadd_ru(n.a.drift[A], n.a.drift[B]));
-                if (L.c_phi0[s] > __fadd_ru(bound, __double2float_ru(1e-4 * GB.spacing))) {
+                // k_pc_carry's pair bound carries the margin of 1e-4 of B's
+                // grid spacing in this precision
+                if (L.c_phi0[s] > __fadd_ru(L.p_bound[p], 1e-12f)) {
                     L.c_node[s] = -1;
                     continue_slot = true;
                 }
@@ -2042,6 +2059,7 @@ __global__ void __launch_bounds__(TPB, PASS == 0 ? FD_PROBE_MIN_BLOCKS : FD_CONT
                 {
                     const int oc_off = aux.w, oc_end = aux.w + L.p_hist_cnt[p];
                     int lo2 = oc_off, hi2 = oc_end;
+                    if (s >= oc_off && s < oc_end && L.o_c_k[s] == k) lo2 = hi2 = s;
                     while (lo2 < hi2) {
                         const int mid = (lo2 + hi2) >> 1;
                         if (L.o_c_k[mid] < k) lo2 = mid + 1; else hi2 = mid;
@@ -2184,11 +2202,17 @@ __global__ void k_pair_sum32(PairListDev L, int with_force)
             o = L.c_off[p];
             c = L.c_cnt[p];
         }
-        for (int j = l; j < c; j += 8) {
-            if (L.c_node[o + j] < 0) continue;
-            const float* f = cf + 9ll * (o + j);
+        for (int j0 = l; j0 < c; j0 += 32) {
+            int nd[4];
 #pragma unroll
-            for (int t = 0; t < 9; ++t) acc[t] += f[t];
+            for (int u = 0; u < 4; ++u) nd[u] = j0 + 8 * u < c ? L.c_node[o + j0 + 8 * u] : -1;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (nd[u] < 0) continue;
+                const float* f = cf + 9ll * (o + j0 + 8 * u);
+#pragma unroll
+                for (int t = 0; t < 9; ++t) acc[t] += f[t];
+            }
         }
         if (__any_sync(0xffffffffu, c > 0)) {
 #pragma unroll
@@ -2774,7 +2798,8 @@ void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& 
     case K:                                                                            \
         k_select<K><<<grid, NARROW_WARPS * 32, 0, s>>>(n); note_launch();                             \
         if (a.gate) {                                                                  \
-            k_pc_carry<<<148 * 8, TPB, 0, s>>>(L, P.n, gh ? gh->hash : P.hash, pgrid, a.gate);        \
+            k_pc_carry<<<148 * 8, TPB, 0, s>>>(L, P.n, gh ? gh->hash : P.hash, pgrid, a.gate,      \
+                                                a.drift, P.geo, G.geo, mixed ? 1e-4f : 0.f);     \
             note_launch();                                                             \
         }                                                                              \
         if (mixed) {                                                                   \
