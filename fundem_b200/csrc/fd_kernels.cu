@@ -417,10 +417,22 @@ __device__ __forceinline__ int image_hash(GhostDev& Gh, int i, double3 r)
 }
 
 // The image of a particle in the first cell column (row, or both) sits one
-// period beyond the domain.  Under the pair cache (ctrl non-null) the
-// particles within ext_skin of that band get images as well, so that a
+// period beyond the domain; every other particle keeps its own position.  A
+// particle enters the image table when that position lies outside the
+// domain, tested as the reference tests it (z against max y): the shifted
+// ones, and unshifted ones above max y.  Gh.live marks these entries.
+// Under the pair cache (ctrl non-null) particles without an entry that lie
+// within ext_skin of the image band get a shifted entry too, so that a
 // rebuild lists the pairs of every particle that can gain an image before
-// the next rebuild; Gh.live marks the particles that have one now.
+// the next rebuild.
+__device__ __forceinline__ int image_out_mask(double3 r, const FdGrid& g)
+{
+    int m = 0;
+    if (r.x < g.minb.x || r.x >= g.maxb.x) m |= 1;
+    if (r.y < g.minb.y || r.y >= g.maxb.y) m |= 2;
+    if (r.z < g.minb.z || r.z >= g.maxb.y) m |= 4;
+    return m;
+}
 __global__ void k_ghost_build(ObjDev P, GhostDev Gh, int kind, double ext_skin, int* ctrl)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -428,23 +440,27 @@ __global__ void k_ghost_build(ObjDev P, GhostDev Gh, int kind, double ext_skin, 
     const FdGrid& g = Gh.cells.g;
     const double3 p = P.pos[i];
     const double3 ox = mk3(g.maxb.x - g.minb.x, 0., 0.), oy = mk3(0., g.maxb.y - g.minb.y, 0.);
+    const double3 shift = kind == FD_GX ? ox : kind == FD_GY ? oy : ox + oy;
     const int3 c = fd_cell_of(p, g);
-    const bool bx = ctrl && (p.x - g.minb.x) * g.inv.x < 1.0 + ext_skin * g.inv.x * 1.01;
-    const bool by = ctrl && (p.y - g.minb.y) * g.inv.y < 1.0 + ext_skin * g.inv.y * 1.01;
-    bool live = false, ext = false;
-    if (kind == FD_GX) { live = c.x == 0; ext = live || bx; }
-    if (kind == FD_GY) { live = c.y == 0; ext = live || by; }
-    if (kind == FD_GXY) { live = c.x == 0 && c.y == 0; ext = live || ((c.x == 0 || bx) && (c.y == 0 || by)); }
-    double3 r = p;
-    if (ext) {
-        if (kind == FD_GX) r = r + ox;
-        if (kind == FD_GY) r = r + oy;
-        if (kind == FD_GXY) r = r + (ox + oy);
+    bool shifted = false;
+    if (kind == FD_GX) shifted = c.x == 0;
+    if (kind == FD_GY) shifted = c.y == 0;
+    if (kind == FD_GXY) shifted = c.x == 0 && c.y == 0;
+    const double3 ru = shifted ? p + shift : p;
+    const bool live = image_out_mask(ru, g) != 0;
+    bool band = false;
+    if (ctrl && !live) {
+        const bool bx = (p.x - g.minb.x) * g.inv.x < 1.0 + ext_skin * g.inv.x * 1.01;
+        const bool by = (p.y - g.minb.y) * g.inv.y < 1.0 + ext_skin * g.inv.y * 1.01;
+        if (kind == FD_GX) band = bx;
+        if (kind == FD_GY) band = by;
+        if (kind == FD_GXY) band = bx && by;
     }
+    const double3 r = live ? ru : band ? p + shift : p;
     Gh.pos[i] = r;
     if (Gh.live) Gh.live[i] = live ? 1 : 0;
     const int outm = image_hash(Gh, i, r);
-    if (ctrl && ext) {
+    if (ctrl && (live || band)) {
         // outside the domain across the translation only: its cell is the
         // natural one in the other directions, and candidacy follows the
         // geometry; otherwise (a clamped cell) this step is built uncached
