@@ -782,6 +782,7 @@ struct fundem_sim {
     DevArray<fd_quat> pc_ref_q;
     DevArray<int> pc_ref_vis, pc_ctrl;
     DevArray<float> pc_drift;
+    DevArray<float4> pc_disp;
     int pc_mode = -1;          // -1: from the particle count, 0: off, 1: on
     double pc_skin_set = 0.0;  // <= 0: PC_SKIN * the largest bounding radius
     bool pc_on = false;
@@ -796,6 +797,7 @@ struct fundem_sim {
         const size_t m = std::max(P.n(), 1);
         pc_ref_pos.alloc(m); pc_ref_q.alloc(m); pc_ref_vis.alloc(m);
         pc_drift.alloc(m, false);
+        pc_disp.alloc(m, false);
         pc_ctrl.alloc(8);
     }
     double pc_skin() const { return pc_skin_set > 0.0 ? pc_skin_set : PC_SKIN * pgeo.rmax; }
@@ -817,7 +819,8 @@ struct fundem_sim {
         // centre) and a node inside a partner's SDF grid (at most the grid
         // radius from the partner's centre)
         const double reach = std::max(2.0 * pgeo.rmax, pgeo.grid_rmax);
-        return fd::PairCacheDev{pc_ref_pos.p, pc_ref_q.p, pc_ref_vis.p, pc_ctrl.p, pc_drift.p, pc_skin(), reach};
+        return fd::PairCacheDev{pc_ref_pos.p, pc_ref_q.p, pc_ref_vis.p, pc_ctrl.p, pc_drift.p, pc_disp.p, pc_skin(),
+                                reach};
     }
     // before steps (outside any stream capture): a pending forced rebuild is
     // written to the device flag
@@ -1118,6 +1121,7 @@ struct fundem_sim {
                 ap.skin = pcv.skin;
                 ap.gate = pcv.ctrl;
                 ap.drift = pcv.drift;
+                ap.disp = pcv.disp;
             }
             fd::launch_narrow(FD_PP, Pv, G, M, Wv, GW, MW, pgrid, wgrid, nullptr, Lpp, ap, with_force, mixed(), stream);
         }
@@ -1187,6 +1191,7 @@ struct fundem_sim {
                     ag.gate = gctrl + 5;
                     ag.noskin = gctrl + 6;
                     ag.drift = pcv.drift;
+                    ag.disp = pcv.disp;
                     fd::launch_broad_ghost(Pv, G, gh, Lg[d], flags.p, probe, stream, pcv.skin, gctrl + 5, gctrl + 6);
                 } else {
                     fd::launch_broad_ghost(Pv, G, gh, Lg[d], flags.p, probe, stream);

@@ -1057,6 +1057,7 @@ __global__ void k_pc_check(ObjDev P, PairCacheDev c)
     const double drift = sqrt(lengthSq3(d)) + c.reach * chord;
     // every particle's bound, for the slot test of the predicate pass
     c.drift[i] = __double2float_ru(drift);
+    c.disp[i] = make_float4((float)d.x, (float)d.y, (float)d.z, __double2float_ru(c.reach * chord));
     if (c.ctrl[0] != 0) return;
     if (c.ctrl[2] != 0 || c.ctrl[3] != 0) {
         // the last build overflowed its lists, or the last step asked for a
@@ -1074,7 +1075,8 @@ __global__ void k_pc_check(ObjDev P, PairCacheDev c)
 // step's, carried over; each pair's history is its own slots of the previous
 // step, and its partner's cell is taken from this step's hash
 __global__ void k_pc_carry(PairListDev L, int n_obj, const long long* hash, FdGrid g, const int* gate,
-                           const float* drift, const int* geo_of, const FdGeo* geos, float spacing_margin)
+                           const float* drift, const float4* disp, const int* geo_of, const FdGeo* geos,
+                           float spacing_margin)
 {
     if (*gate != 0) return;
     const int npairs = min(L.o_counters[0], L.cap_pairs);
@@ -1095,13 +1097,26 @@ __global__ void k_pc_carry(PairListDev L, int n_obj, const long long* hash, FdGr
         const int off = L.o_c_off[p], cnt = L.o_c_cnt[p];
         L.pairA[p] = A;
         L.pairB[p] = B;
-        if (drift && L.p_bound) {
+        if (drift && disp && L.p_bound) {
             // the slot bound's right-hand side for the pair (see k_contact):
-            // lip_B (drift_A + drift_B), rounded up, plus a margin in units of
-            // B's grid spacing (the single-precision predicate's rounding)
+            // lip_B times how far a node can have moved in B's frame, plus a
+            // margin in units of B's grid spacing (the single-precision
+            // predicate's rounding).  The node's offset from B's centre moved
+            // by at most |dc_A - dc_B| + the two rotation parts (lever arms up
+            // to the reach); the displacements are stored in single
+            // precision, whose rounding (1e-7 of each) the term
+            // 1e-6 (drift_A + drift_B) covers; never more than the sum of
+            // the two drift bounds.
             const FdGeo& GB = geos[geo_of[B]];
             const float lip = __double2float_ru(GB.lip);
-            float bound = __fmul_ru(lip, __fadd_ru(drift[A], drift[B]));
+            const float4 a = disp[A], b = disp[B];
+            const float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+            const float dab = __fadd_ru(drift[A], drift[B]);
+            const float rel = __fadd_ru(__fadd_ru(__fsqrt_ru(__fadd_ru(__fadd_ru(__fmul_ru(dx, dx), __fmul_ru(dy, dy)),
+                                                                       __fmul_ru(dz, dz))),
+                                                  __fadd_ru(a.w, b.w)),
+                                        __fmul_ru(1e-6f, dab));
+            float bound = __fmul_ru(lip, fminf(rel, dab));
             if (spacing_margin > 0.f)
                 bound = __fadd_ru(__fmul_ru(bound, 1.000001f), __fmul_ru(spacing_margin, __double2float_ru(GB.spacing)));
             L.p_bound[p] = bound;
@@ -2815,7 +2830,7 @@ void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& 
         k_select<K><<<grid, NARROW_WARPS * 32, 0, s>>>(n); note_launch();                             \
         if (a.gate) {                                                                  \
             k_pc_carry<<<148 * 8, TPB, 0, s>>>(L, P.n, gh ? gh->hash : P.hash, pgrid, a.gate,      \
-                                                a.drift, P.geo, G.geo, mixed ? 1e-4f : 0.f);     \
+                                                a.drift, a.disp, P.geo, G.geo, mixed ? 1e-4f : 0.f); \
             note_launch();                                                             \
         }                                                                              \
         if (mixed) {                                                                   \

@@ -258,6 +258,8 @@ struct PairCacheDev {
     // this step, moved to [3] at its end
     int* ctrl;
     float* drift;       // per particle: the drift bound since the last build (rounded up)
+    float4* disp;       // per particle: displacement since the last build (x, y, z) and
+                        // the rotation part of the drift bound (rounded up)
     double skin;
     double reach;       // largest lever arm of a rotation in the drift bound:
                         // 2 r_max, or a larger SDF-grid radius
@@ -274,6 +276,7 @@ struct StepArgs {
     double skin;       // positional skin of the culling stages (the pair cache; 0 without it)
     const int* gate;   // pair cache: the selection runs only when *gate != 0 (null: always)
     const float* drift;  // pair cache: per-particle drift bounds (see PairCacheDev)
+    const float4* disp;  // pair cache: per-particle displacements (see PairCacheDev)
     const int* noskin;   // non-null and nonzero: this step's selection takes no skin
     // launch shape of the narrow phase, in blocks per SM (0: the default):
     // selection, predicate pass, contact-law pass, pair sums
