@@ -487,6 +487,7 @@ struct PairList {
     DevArray<int> c_pair, c_hit, p_hist_cnt;
     DevArray<float> c_phi0;  // pair cache: slot bounds of the last rebuild
     DevArray<float> p_bound; // pair cache: per-pair drift bound of a carried step
+    DevArray<int> carry_n;   // pair cache: carried steps since the layout was built
     DevArray<double> c_force;
     DevArray<int4> p_aux;
     bool allocated = false;
@@ -509,6 +510,7 @@ struct PairList {
         c_pair.alloc(cap_contacts); c_hit.alloc(cap_contacts, false); c_force.alloc((size_t)cap_contacts * 9);
         c_phi0.alloc(cap_contacts, false);
         p_aux.alloc(cap_pairs); p_hist_cnt.alloc(cap_pairs); p_bound.alloc(cap_pairs, false);
+        carry_n.alloc(1);
         allocated = true;
     }
     void grow(int capp, int capc)
@@ -555,6 +557,7 @@ struct PairList {
         v.o_c_node = o.c_node.p; v.o_c_spring = o.c_spring.p;
         v.c_phi0 = c_phi0.p;
         v.p_bound = p_bound.p;
+        v.carry_n = carry_n.p;
         return v;
     }
 };

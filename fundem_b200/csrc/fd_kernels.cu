@@ -1083,20 +1083,29 @@ __global__ void k_pc_carry(PairListDev L, int n_obj, const long long* hash, FdGr
     const int nslots = min(L.o_counters[1], L.cap_contacts);
     const long long stride = (long long)gridDim.x * blockDim.x;
     const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    // the layout (segments, pairs, slot keys) is copied into the other
+    // generation on the first carried step after a build; from the second on
+    // both generations hold it already
+    const bool copy = L.carry_n == nullptr || *L.carry_n == 0;
     if (t0 == 0) {
         *L.n_pairs = L.o_counters[0];
         *L.n_slots = L.o_counters[1];
     }
-    for (long long i = t0; i < n_obj; i += stride) {
-        L.seg_off[i] = L.o_seg_off[i];
-        L.seg_cnt[i] = L.o_seg_cnt[i];
-    }
+    if (copy)
+        for (long long i = t0; i < n_obj; i += stride) {
+            L.seg_off[i] = L.o_seg_off[i];
+            L.seg_cnt[i] = L.o_seg_cnt[i];
+        }
     for (long long p = t0; p < npairs; p += stride) {
         const int A = L.o_pairA[p];
         const int B = L.o_pairB[p];
         const int off = L.o_c_off[p], cnt = L.o_c_cnt[p];
-        L.pairA[p] = A;
-        L.pairB[p] = B;
+        if (copy) {
+            L.pairA[p] = A;
+            L.pairB[p] = B;
+            L.c_off[p] = off;
+            L.c_cnt[p] = cnt;
+        }
         if (drift && disp && L.p_bound) {
             // the slot bound's right-hand side for the pair (see k_contact):
             // lip_B times how far a node can have moved in B's frame, plus a
@@ -1121,8 +1130,6 @@ __global__ void k_pc_carry(PairListDev L, int n_obj, const long long* hash, FdGr
                 bound = __fadd_ru(__fmul_ru(bound, 1.000001f), __fmul_ru(spacing_margin, __double2float_ru(GB.spacing)));
             L.p_bound[p] = bound;
         }
-        L.c_off[p] = off;
-        L.c_cnt[p] = cnt;
         if (cnt > 0) {
             int3 bc;
             decode_cell(hash[B], g.size, bc);
@@ -1130,7 +1137,8 @@ __global__ void k_pc_carry(PairListDev L, int n_obj, const long long* hash, FdGr
             L.p_hist_cnt[p] = cnt;
         }
     }
-    for (long long k = t0; k < nslots; k += stride) L.c_k[k] = L.o_c_k[k];
+    if (copy)
+        for (long long k = t0; k < nslots; k += stride) L.c_k[k] = L.o_c_k[k];
 }
 
 // after the particle-particle narrow phase of a rebuild step: its state is the
@@ -1483,6 +1491,8 @@ template <int KIND>
 __global__ void __launch_bounds__(NARROW_WARPS * 32, FD_SELECT_MIN_BLOCKS) k_select(NarrowArgs n)
 {
     if (n.a.gate && *n.a.gate == 0) return;
+    // a new layout: the next carried step copies it (k_pc_carry)
+    if (blockIdx.x == 0 && threadIdx.x == 0 && n.L.carry_n) *n.L.carry_n = 0;
     __shared__ unsigned short s_node[NARROW_WARPS][MAX_NODE_QUEUE];
     // work counters, summed per block and added to the global ones once
     __shared__ unsigned long long s_stats[4];
@@ -1625,6 +1635,7 @@ __global__ void __launch_bounds__(TPB, PASS == 0 ? FD_PROBE_MIN_BLOCKS : FD_CONT
     const bool slot_test = carried;
     const bool phi0_store = cache && !carried;
     const bool live_test = TRANSLATED && PASS == 0 && n.gh.live != nullptr;
+    if (carried && blockIdx.x == 0 && threadIdx.x == 0 && L.carry_n) atomicAdd(L.carry_n, 1);
     int hits = 0;
     for (int s0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); s0 < nitems; s0 += stride) {
         const int t = s0 + lane;
@@ -1981,6 +1992,7 @@ __global__ void __launch_bounds__(TPB, PASS == 0 ? FD_PROBE_MIN_BLOCKS : FD_CONT
     const bool slot_test = carried;
     const bool phi0_store = cache && !carried;
     const bool live_test = TRANSLATED && PASS == 0 && n.gh.live != nullptr;
+    if (carried && blockIdx.x == 0 && threadIdx.x == 0 && L.carry_n) atomicAdd(L.carry_n, 1);
     int hits = 0;
     for (int s0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); s0 < nitems; s0 += stride) {
         const int t = s0 + lane;

@@ -61,6 +61,7 @@ struct PairListDev {
     int* n_slots;      // device counter: slots used
     int* n_hits;       // device counter: contacts (n_slots + 1)
     int cap_contacts;  // slot capacity
+    int* carry_n;      // pair cache: carried steps since the layout was built
     float* p_bound;    // pair cache, carried steps: per pair, how far the SDF can
                        // have moved at a node since the rebuild (k_pc_carry)
     float* c_phi0;     // pair cache: per slot, the node's signed distance to the
