@@ -332,16 +332,19 @@ def run_fundem(args, rank, world, dist):
         # record it once, outside the timing
         sim.step_graph(1)
         sim.sync()
+    # every step's status word goes to a page-locked ring, read after the sync
+    ring = torch.zeros(max(e2e_steps, 1), dtype=torch.int32, pin_memory=True)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     sim.set_state(**host)
-    for _ in range(e2e_steps):
+    for k in range(e2e_steps):
         sim.step_graph(1)
-        sim.status_word()
+        sim.status_word_to(ring.data_ptr() + 4 * k)
     sim.state(out=back)
     sim.sync()
     t_e2e = time.perf_counter() - t0
-    log0(f"end to end: {t_e2e:.4f} s")
+    status_ok = bool(torch.all(ring[:e2e_steps] == 0).item()) if e2e_steps else None
+    log0(f"end to end: {t_e2e:.4f} s, status words clean: {status_ok}")
     # narrow-phase work counters, on a few extra steps outside the timed regions
     wc_steps = 10
     sim.set_profiling(False, counters=True)
@@ -433,8 +436,10 @@ def run_fundem(args, rank, world, dist):
                    "timed_from": "the settled, bonded bed with the platen released (workloads.bonded_column)"},
         "e2e": {"value": e2e_val, "unit": METRIC, "h2d_bytes_per_step": state_bytes / args.steps,
                 "d2h_bytes_per_step": 4 + state_bytes / args.steps,
-                "note": "state uploaded from host arrays, each step a one-step CUDA-graph replay "
-                        "(fundem_step_graph) followed by a read of the status word, state downloaded"},
+                "status_words_clean": status_ok,
+                "note": "state uploaded from page-locked host arrays, each step a one-step CUDA-graph replay "
+                        "(fundem_step_graph) followed by a copy of its status word into a page-locked ring "
+                        "(checked after the final sync), state downloaded"},
         "graph": graph,
         "headline_path": "plain launches (fundem_step)" if args.no_graph else
                          "one CUDA graph of K steps replayed (fundem_step_graph), recorded before the timed region",

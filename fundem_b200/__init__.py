@@ -599,6 +599,13 @@ class Simulation:
         self._check(self.L.fundem_status_word(self.h, C.byref(w)), "status_word")
         return w.value
 
+    def status_word_to(self, address):
+        """Enqueue a copy of the status word to a host address (page-locked
+        memory: the copy does not stall the host; the word is there after
+        sync())."""
+        self._check(self.L.fundem_status_word(self.h, C.cast(C.c_void_p(int(address)), C.POINTER(C.c_uint))),
+                    "status_word")
+
     def launch_count(self):
         n = C.c_longlong()
         self._check(self.L.fundem_launch_count(self.h, C.byref(n)), "launch_count")
