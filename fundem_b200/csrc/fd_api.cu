@@ -786,6 +786,11 @@ struct fundem_sim {
     DevArray<int> pc_ref_vis, pc_ctrl;
     DevArray<float> pc_drift;
     DevArray<float4> pc_disp;
+    DevArray<double3> pc_wref_pos;
+    DevArray<fd_quat> pc_wref_q;
+    DevArray<long long> pc_wref_hash;
+    DevArray<float> pc_wdrift;
+    DevArray<float4> pc_wdisp;
     int pc_mode = -1;          // -1: from the particle count, 0: off, 1: on
     double pc_skin_set = 0.0;  // <= 0: PC_SKIN * the largest bounding radius
     bool pc_on = false;
@@ -801,6 +806,9 @@ struct fundem_sim {
         pc_ref_pos.alloc(m); pc_ref_q.alloc(m); pc_ref_vis.alloc(m);
         pc_drift.alloc(m, false);
         pc_disp.alloc(m, false);
+        const size_t mw = std::max(W.n(), 1);
+        pc_wref_pos.alloc(mw); pc_wref_q.alloc(mw); pc_wref_hash.alloc(mw);
+        pc_wdrift.alloc(mw, false); pc_wdisp.alloc(mw, false);
         pc_ctrl.alloc(8);
     }
     double pc_skin() const { return pc_skin_set > 0.0 ? pc_skin_set : PC_SKIN * pgeo.rmax; }
@@ -823,7 +831,7 @@ struct fundem_sim {
         // radius from the partner's centre)
         const double reach = std::max(2.0 * pgeo.rmax, pgeo.grid_rmax);
         return fd::PairCacheDev{pc_ref_pos.p, pc_ref_q.p, pc_ref_vis.p, pc_ctrl.p, pc_drift.p, pc_disp.p, pc_skin(),
-                                reach};
+                                reach, pc_wref_pos.p, pc_wref_q.p, pc_wref_hash.p, pc_wdrift.p, pc_wdisp.p};
     }
     // before steps (outside any stream capture): a pending forced rebuild is
     // written to the device flag
@@ -1102,6 +1110,7 @@ struct fundem_sim {
         fd::launch_cell_table(Pv, T, scan_tmp.p, scan_tmp.n, stream, pc ? pcv.ctrl : nullptr);
         // wall hash (visibility and cell for the node test)
         if (W.n_dev > 0) fd::launch_hash(Wv, wgrid, stream);
+        if (pc && W.n_dev > 0) fd::launch_pair_cache_check_walls(Wv, GW, pcv, stream);
         tend(FUNDEM_T_HASH);
         int active[FD_NKIND] = {1, 1, 0, 0, 0};
         if (new_generation)
@@ -1138,11 +1147,27 @@ struct fundem_sim {
         PairListDev Lpw = lists[FD_PW].view();
         tbegin(FUNDEM_T_BROAD);
         fd::launch_broad_pw(Pv, G, Wv, GW, wgrid, Lpw, flags.p, probe, stream,
-                            wall_groups.empty() ? nullptr : d_wall_groups.p);
+                            wall_groups.empty() ? nullptr : d_wall_groups.p, pc ? pcv.skin : 0.0,
+                            pc ? pcv.ctrl : nullptr);
         tend(FUNDEM_T_BROAD);
         tbegin(FUNDEM_T_NARROW_PW);
         a.rec = recording ? recording->rec(FD_PW, record_step) : fd::AdjRec{};
-        fd::launch_narrow(FD_PW, Pv, G, M, Wv, GW, MW, pgrid, wgrid, nullptr, Lpw, a, with_force, mixed(), stream);
+        {
+            // the particle-wall list shares the cache (wall drifts and cells
+            // in its rebuild flag)
+            fd::StepArgs aw = a;
+            if (pc) {
+                aw.skin = pcv.skin;
+                aw.gate = pcv.ctrl;
+                aw.drift = pcv.drift;
+                aw.disp = pcv.disp;
+                aw.driftB = pcv.wdrift;
+                aw.dispB = pcv.wdisp;
+            }
+            fd::launch_narrow(FD_PW, Pv, G, M, Wv, GW, MW, pgrid, wgrid, nullptr, Lpw, aw, with_force, mixed(),
+                              stream);
+        }
+        if (pc && W.n_dev > 0) fd::launch_pair_cache_commit_walls(Wv, pcv, stream);
         if (recording)
             FD_CUDA(cudaMemcpyAsync(recording->ns(FD_PW, record_step), Lpw.n_slots, sizeof(int),
                                     cudaMemcpyDeviceToDevice, stream));
@@ -1267,7 +1292,7 @@ struct fundem_sim {
             if (needp || needc) {
                 L.grow(std::max(needp, L.cap_pairs), std::max(needc, L.cap_contacts));
                 // the slot-to-pair map of a cached list is not kept by a growth
-                if (k == FD_PP || k == FD_GX || k == FD_GY || k == FD_GXY) pc_force = true;
+                if (k != FD_GR90 && k != FD_GR180 && k != FD_GR270) pc_force = true;
             }
         }
     }

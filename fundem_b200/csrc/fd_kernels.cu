@@ -1075,8 +1075,8 @@ __global__ void k_pc_check(ObjDev P, PairCacheDev c)
 // step's, carried over; each pair's history is its own slots of the previous
 // step, and its partner's cell is taken from this step's hash
 __global__ void k_pc_carry(PairListDev L, int n_obj, const long long* hash, FdGrid g, const int* gate,
-                           const float* drift, const float4* disp, const int* geo_of, const FdGeo* geos,
-                           float spacing_margin)
+                           const float* drift, const float4* disp, const float* driftB, const float4* dispB,
+                           const int* geo_of, const FdGeo* geos, float spacing_margin)
 {
     if (*gate != 0) return;
     const int npairs = min(L.o_counters[0], L.cap_pairs);
@@ -1118,9 +1118,9 @@ __global__ void k_pc_carry(PairListDev L, int n_obj, const long long* hash, FdGr
             // the two drift bounds.
             const FdGeo& GB = geos[geo_of[B]];
             const float lip = __double2float_ru(GB.lip);
-            const float4 a = disp[A], b = disp[B];
+            const float4 a = disp[A], b = dispB[B];
             const float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
-            const float dab = __fadd_ru(drift[A], drift[B]);
+            const float dab = __fadd_ru(drift[A], driftB[B]);
             const float rel = __fadd_ru(__fadd_ru(__fsqrt_ru(__fadd_ru(__fadd_ru(__fmul_ru(dx, dx), __fmul_ru(dy, dy)),
                                                                        __fmul_ru(dz, dz))),
                                                   __fadd_ru(a.w, b.w)),
@@ -1158,6 +1158,35 @@ __global__ void k_pc_commit(ObjDev P, PairCacheDev c, PairListDev L)
     }
 }
 
+// walls: the drift bound of each wall since the last build (rotation lever
+// arm: its SDF-grid radius, the farthest a node inside its grid can be), and
+// a rebuild when it exceeds skin / 2 or the wall's cell changed (the
+// particle-wall candidates follow the wall's cell)
+__global__ void k_pc_check_walls(ObjDev W, GeoSetDev GW, PairCacheDev c)
+{
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= W.n) return;
+    const double3 d = W.pos[w] - c.wref_pos[w];
+    const fd_quat q = W.q[w], r = c.wref_q[w];
+    const double vx = r.q0 * q.q1 - q.q0 * r.q1 - (q.q2 * r.q3 - q.q3 * r.q2);
+    const double vy = r.q0 * q.q2 - q.q0 * r.q2 - (q.q3 * r.q1 - q.q1 * r.q3);
+    const double vz = r.q0 * q.q3 - q.q0 * r.q3 - (q.q1 * r.q2 - q.q2 * r.q1);
+    const double rot = GW.geo[W.geo[w]].grid_radius * 2.0 * sqrt(vx * vx + vy * vy + vz * vz);
+    const double drift = sqrt(lengthSq3(d)) + rot;
+    c.wdrift[w] = __double2float_ru(drift);
+    c.wdisp[w] = make_float4((float)d.x, (float)d.y, (float)d.z, __double2float_ru(rot));
+    if (c.ctrl[0] != 0) return;
+    if (!(drift <= 0.5 * c.skin * (1.0 - 1e-6)) || W.hash[w] != c.wref_hash[w]) c.ctrl[0] = 1;
+}
+__global__ void k_pc_commit_walls(ObjDev W, PairCacheDev c)
+{
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= W.n || c.ctrl[0] == 0) return;
+    c.wref_pos[w] = W.pos[w];
+    c.wref_q[w] = W.q[w];
+    c.wref_hash[w] = W.hash[w];
+}
+
 // ghost phases: particles whose search box reaches the cells holding ghost
 // images are listed for k_broad_cells<true, true>; the others get empty
 // segments here
@@ -1185,14 +1214,14 @@ __global__ void k_ghost_searchers(ObjDev P, GeoSetDev G, FdGrid g, const int* oc
 // of walls it can meet (the walls of its own simulation in a batch of
 // simulations tiled into one)
 __global__ void k_broad_pw(ObjDev P, GeoSetDev G, ObjDev W, GeoSetDev GW, FdGrid wg, PairListDev L,
-                           unsigned int* flags, double probe, const int2* wall_range)
+                           unsigned int* flags, double probe, const int2* wall_range, double skin, const int* gate)
 {
     const int A = blockIdx.x * blockDim.x + threadIdx.x;
-    if (A >= P.n) return;
+    if (A >= P.n || (gate && *gate == 0)) return;
     const double3 cA = P.pos[A];
     const double rA = G.geo[P.geo[A]].radius;
     int3 lo, hi;
-    body_search_range(cA, rA * (1.0 + BOUND_REL), wg, lo, hi);
+    body_search_range(cA, rA * (1.0 + BOUND_REL) + skin, wg, lo, hi);
     int buf[MAX_CAND];
     int cnt = 0, total = 0;
     const int2 wr = wall_range ? wall_range[A] : make_int2(0, W.n);
@@ -1204,10 +1233,10 @@ __global__ void k_broad_pw(ObjDev P, GeoSetDev G, ObjDev W, GeoSetDev GW, FdGrid
         decode_cell(h, wg.size, c);
         if (c.x < lo.x || c.x > hi.x || c.y < lo.y || c.y > hi.y || c.z < lo.z || c.z > hi.z) continue;
         const FdGeo& GB = GW.geo[W.geo[w]];
-        const double rs = rA + GB.grid_radius;
+        const double rs = rA + GB.grid_radius + skin;
         const double3 cW = W.pos[w];
         if (lengthSq3(cA - cW) > rs * rs * (1.0 + 4.0 * BOUND_REL)) continue;
-        if (body_culled32(cA, rA, cW, W.rot + 3ll * w, false, GB, GW, probe)) continue;
+        if (body_culled32(cA, rA + skin, cW, W.rot + 3ll * w, false, GB, GW, probe)) continue;
         if (cnt < MAX_CAND) buf[cnt++] = w;
         ++total;
     }
@@ -1629,8 +1658,8 @@ __global__ void __launch_bounds__(TPB, PASS == 0 ? FD_PROBE_MIN_BLOCKS : FD_CONT
     // A translated ghost list under the cache also holds the pairs of
     // particles that have no image this step: their slots hold no contact.
     constexpr bool TRANSLATED = KIND == FD_GX || KIND == FD_GY || KIND == FD_GXY;
-    const bool cache = (KIND == FD_PP || TRANSLATED) && PASS == 0 && n.a.gate != nullptr && L.c_phi0 != nullptr &&
-                       n.a.drift != nullptr;
+    const bool cache = (KIND == FD_PP || KIND == FD_PW || TRANSLATED) && PASS == 0 && n.a.gate != nullptr &&
+                       L.c_phi0 != nullptr && n.a.drift != nullptr;
     const bool carried = cache && *n.a.gate == 0;
     const bool slot_test = carried;
     const bool phi0_store = cache && !carried;
@@ -1986,8 +2015,8 @@ __global__ void __launch_bounds__(TPB, PASS == 0 ? FD_PROBE_MIN_BLOCKS : FD_CONT
     // rounding (a few 1e-7 of the SDF values) is covered by a margin of
     // 1e-4 of B's grid spacing in the pair bound
     constexpr bool TRANSLATED = KIND == FD_GX || KIND == FD_GY || KIND == FD_GXY;
-    const bool cache = (KIND == FD_PP || TRANSLATED) && PASS == 0 && n.a.gate != nullptr && L.c_phi0 != nullptr &&
-                       n.a.drift != nullptr;
+    const bool cache = (KIND == FD_PP || KIND == FD_PW || TRANSLATED) && PASS == 0 && n.a.gate != nullptr &&
+                       L.c_phi0 != nullptr && n.a.drift != nullptr;
     const bool carried = cache && *n.a.gate == 0;
     const bool slot_test = carried;
     const bool phi0_store = cache && !carried;
@@ -2040,6 +2069,7 @@ __global__ void __launch_bounds__(TPB, PASS == 0 ? FD_PROBE_MIN_BLOCKS : FD_CONT
             // an overlap the predicate did not reach stays +inf (a slot that
             // is never skipped)
             float ov = PASS == 0 ? __int_as_float(0x7f800000) : 0.f, fx = 0.f, fy = 0.f, fz = 0.f, pv[8];
+            float phi0v = __int_as_float(0xff800000);  // the slot bound to store (-inf: never skipped)
             if (aux.x >= lo.x && aux.x <= hi.x && aux.y >= lo.y && aux.y <= hi.y && aux.z >= lo.z && aux.z <= hi.z) {
                 const double3 rel = mk3(gp.x - cB.x, gp.y - cB.y, gp.z - cB.z);
                 if (!Slave<KIND>::radius_test || xm_len2(rel) <= GB.radius * GB.radius) {
@@ -2068,6 +2098,7 @@ __global__ void __launch_bounds__(TPB, PASS == 0 ? FD_PROBE_MIN_BLOCKS : FD_CONT
 #pragma unroll
                             for (int c = 0; c < 8; ++c) pv[c] = (float)pd[c];
                             ov = (float)ovd;
+                            phi0v = __double2float_rd(-ovd);
                             hit = ovd >= -n.a.probe;
                         } else {
                             const float* S = SB.sdf32 + c0;
@@ -2077,12 +2108,13 @@ __global__ void __launch_bounds__(TPB, PASS == 0 ? FD_PROBE_MIN_BLOCKS : FD_CONT
                             const float c00 = pv[0] * (1.f - fx) + pv[1] * fx, c10 = pv[2] * (1.f - fx) + pv[3] * fx;
                             const float c01 = pv[4] * (1.f - fx) + pv[5] * fx, c11 = pv[6] * (1.f - fx) + pv[7] * fx;
                             ov = -((c00 * (1.f - fy) + c10 * fy) * (1.f - fz) + (c01 * (1.f - fy) + c11 * fy) * fz);
+                            phi0v = -ov;
                             hit = ov >= -(float)n.a.probe;
                         }
                     }
                 }
             }
-            if (phi0_store) L.c_phi0[s] = -ov;
+            if (phi0_store) L.c_phi0[s] = phi0v;
             int nid = -1;
             if (PASS == 1 && hit) {
                 // gradient with the x weight truncated as the reference does
@@ -2798,10 +2830,21 @@ void launch_pair_cache_end(const PairCacheDev& c, const PairListDev* ghost_lists
 
 void launch_broad_pw(const ObjDev& P, const GeoSetDev& G, const ObjDev& W, const GeoSetDev& GW,
                      const FdGrid& wg, PairListDev& L, unsigned int* flags, double probe, cudaStream_t s,
-                     const int2* wall_range)
+                     const int2* wall_range, double skin, const int* gate)
 {
     cudaMemsetAsync(L.n_pairs, 0, sizeof(int), s);
-    if (P.n > 0) { k_broad_pw<<<nblocks(P.n), TPB, 0, s>>>(P, G, W, GW, wg, L, flags, probe, wall_range); note_launch(); }
+    if (P.n > 0) {
+        k_broad_pw<<<nblocks(P.n), TPB, 0, s>>>(P, G, W, GW, wg, L, flags, probe, wall_range, skin, gate);
+        note_launch();
+    }
+}
+void launch_pair_cache_check_walls(const ObjDev& W, const GeoSetDev& GW, const PairCacheDev& c, cudaStream_t s)
+{
+    if (W.n > 0) { k_pc_check_walls<<<nblocks(W.n), TPB, 0, s>>>(W, GW, c); note_launch(); }
+}
+void launch_pair_cache_commit_walls(const ObjDev& W, const PairCacheDev& c, cudaStream_t s)
+{
+    if (W.n > 0) { k_pc_commit_walls<<<nblocks(W.n), TPB, 0, s>>>(W, c); note_launch(); }
 }
 void launch_broad_ghost(const ObjDev& P, const GeoSetDev& G, const GhostDev& Gh, PairListDev& L,
                         unsigned int* flags, double probe, cudaStream_t s, double skin, const int* gate,
@@ -2841,8 +2884,11 @@ void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& 
     case K:                                                                            \
         k_select<K><<<grid, NARROW_WARPS * 32, 0, s>>>(n); note_launch();                             \
         if (a.gate) {                                                                  \
-            k_pc_carry<<<148 * 8, TPB, 0, s>>>(L, P.n, gh ? gh->hash : P.hash, pgrid, a.gate,      \
-                                                a.drift, a.disp, P.geo, G.geo, mixed ? 1e-4f : 0.f); \
+            const bool wall = K == FD_PW;                                              \
+            k_pc_carry<<<148 * 8, TPB, 0, s>>>(                                        \
+                L, P.n, wall ? W.hash : gh ? gh->hash : P.hash, wall ? wgrid : pgrid, a.gate, a.drift, \
+                a.disp, a.driftB ? a.driftB : a.drift, a.dispB ? a.dispB : a.disp,      \
+                wall ? W.geo : P.geo, wall ? GW.geo : G.geo, (mixed && !wall) ? 1e-4f : 0.f);          \
             note_launch();                                                             \
         }                                                                              \
         if (mixed) {                                                                   \

@@ -264,6 +264,14 @@ struct PairCacheDev {
     double skin;
     double reach;       // largest lever arm of a rotation in the drift bound:
                         // 2 r_max, or a larger SDF-grid radius
+    // walls (the particle-wall list): state and cell at the last build, and
+    // their drift bounds and displacements as for the particles (rotation
+    // lever arm: the wall's SDF-grid radius)
+    double3* wref_pos;
+    fd_quat* wref_q;
+    long long* wref_hash;
+    float* wdrift;
+    float4* wdisp;
 };
 
 struct StepArgs {
@@ -278,6 +286,8 @@ struct StepArgs {
     const int* gate;   // pair cache: the selection runs only when *gate != 0 (null: always)
     const float* drift;  // pair cache: per-particle drift bounds (see PairCacheDev)
     const float4* disp;  // pair cache: per-particle displacements (see PairCacheDev)
+    const float* driftB; // the partners' drift bounds and displacements when they
+    const float4* dispB; // are walls (null: the particles')
     const int* noskin;   // non-null and nonzero: this step's selection takes no skin
     // launch shape of the narrow phase, in blocks per SM (0: the default):
     // selection, predicate pass, contact-law pass, pair sums
@@ -353,6 +363,10 @@ void launch_broad_pp_nl(const ObjDev& P, const GeoSetDev& G, const CellTableDev&
 // the state of a rebuild step as the new reference and clear the flag
 void launch_pair_cache_check(const ObjDev& P, const PairCacheDev& c, cudaStream_t s);
 void launch_pair_cache_commit(const ObjDev& P, const PairCacheDev& c, const PairListDev& L, cudaStream_t s);
+// walls: flag a rebuild when a wall drifted by more than skin / 2 or changed
+// cell; after the particle-wall narrow phase of a rebuild, keep their state
+void launch_pair_cache_check_walls(const ObjDev& W, const GeoSetDev& GW, const PairCacheDev& c, cudaStream_t s);
+void launch_pair_cache_commit_walls(const ObjDev& W, const PairCacheDev& c, cudaStream_t s);
 // end of a cached step: a rebuild whose ghost lists overflowed is not kept,
 // this step's requests become the next step's rebuild, the flags clear
 void launch_pair_cache_end(const PairCacheDev& c, const PairListDev* ghost_lists, int n_ghost_lists, cudaStream_t s);
@@ -360,7 +374,7 @@ void launch_pair_cache_end(const PairCacheDev& c, const PairListDev* ghost_lists
 // count it may meet (a batch of simulations tiled into one)
 void launch_broad_pw(const ObjDev& P, const GeoSetDev& G, const ObjDev& W, const GeoSetDev& GW,
                      const FdGrid& wg, PairListDev& L, unsigned int* flags, double probe, cudaStream_t s,
-                     const int2* wall_range = nullptr);
+                     const int2* wall_range = nullptr, double skin = 0.0, const int* gate = nullptr);
 // skin, gate and noskin: the pair cache (ctrl[5], ctrl[6]), as for the
 // particle-particle list
 void launch_broad_ghost(const ObjDev& P, const GeoSetDev& G, const GhostDev& Gh, PairListDev& L,
