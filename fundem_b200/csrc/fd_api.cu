@@ -835,6 +835,23 @@ struct fundem_sim {
     }
     // before steps (outside any stream capture): a pending forced rebuild is
     // written to the device flag
+    // before a forced rebuild (outside any capture): the lists it builds hold
+    // the skin's extra pairs and slots, so each cached list gets room for
+    // four times its current counts
+    void pc_reserve()
+    {
+        if (!pc_active() || !pc_force) return;
+        FD_CUDA(cudaStreamSynchronize(stream));
+        for (int k : {FD_PP, FD_PW, FD_GX, FD_GY, FD_GXY}) {
+            PairList& L = lists[k];
+            if (!L.allocated) continue;
+            int c[2] = {0, 0};
+            FD_CUDA(cudaMemcpy(c, L.gen[L.cur].counters.p, sizeof(c), cudaMemcpyDeviceToHost));
+            const int needp = 4 * c[0], needc = 4 * c[1];
+            if (needp > L.cap_pairs || needc > L.cap_contacts)
+                L.grow(std::max(needp, L.cap_pairs), std::max(needc, L.cap_contacts));
+        }
+    }
     void pc_prepare()
     {
         if (!pc_active() || !pc_force) return;
@@ -1235,8 +1252,9 @@ struct fundem_sim {
             tend(FUNDEM_T_GHOST);
         }
         if (pc) {
-            PairListDev gl[3];
+            PairListDev gl[4];
             int ng = 0;
+            gl[ng++] = Lpw;
             for (int d = 0; d < 3 && pcg; ++d)
                 if (ghosts[d].active) gl[ng++] = Lg[d];
             fd::launch_pair_cache_end(pcv, gl, ng, stream);
@@ -1868,6 +1886,7 @@ int fundem_step_begin(fundem_sim* s, const double g[3], double dt)
     if (!s->setup_done) return FUNDEM_ERR_STATE;
     return guard(s, [&] {
         if (++s->hook_steps % CAPACITY_CHECK == 0) s->ensure_capacity();
+        s->pc_reserve();
         s->pc_prepare();
         s->front(d3(g), dt);
         s->detect_all(true, dt);
@@ -1890,6 +1909,7 @@ int fundem_step(fundem_sim* s, int nsteps, const double g[3], double dt)
         for (int k = 0; k < nsteps; ++k) {
             // list capacities follow the counts every CAPACITY_CHECK steps
             if (k > 0 && k % CAPACITY_CHECK == 0) s->ensure_capacity();
+            s->pc_reserve();
             s->pc_prepare();
             s->front(d3(g), dt);
             s->detect_all(true, dt);
@@ -1905,6 +1925,7 @@ int fundem_step_graph(fundem_sim* s, int nsteps, const double g[3], double dt)
     if (!s->setup_done) return FUNDEM_ERR_STATE;
     return guard(s, [&] {
         FD_CUDA(cudaSetDevice(s->device));
+        s->pc_reserve();  // before the graph is looked up: it may grow the lists
         const double key[8] = {g[0], g[1], g[2], dt, (double)s->precision, (double)s->records,
                                (double)s->counters,
                                (double)(s->pc_active() * 8 + s->sector * 4 + s->perX * 2 + s->perY)};

@@ -479,18 +479,18 @@ __global__ void k_ghost_gate(int* ctrl)
 }
 
 // end of a cached step
-struct GhostCounts {
-    int* n_pairs[3];
-    int* n_slots[3];
-    int cap_pairs[3];
-    int cap_contacts[3];
+struct CachedCounts {
+    int* n_pairs[4];
+    int* n_slots[4];
+    int cap_pairs[4];
+    int cap_contacts[4];
     int n;
 };
-__global__ void k_pc_end(int* ctrl, GhostCounts gc)
+// a build of the particle-wall or ghost lists that overflowed is not kept
+__global__ void k_pc_end(int* ctrl, CachedCounts gc)
 {
-    if (ctrl[5] != 0)
-        for (int k = 0; k < gc.n; ++k)
-            if (*gc.n_pairs[k] > gc.cap_pairs[k] || *gc.n_slots[k] > gc.cap_contacts[k]) ctrl[7] = 1;
+    for (int k = 0; k < gc.n; ++k)
+        if (*gc.n_pairs[k] > gc.cap_pairs[k] || *gc.n_slots[k] > gc.cap_contacts[k]) ctrl[7] = 1;
     ctrl[3] = ctrl[7];
     ctrl[7] = 0;
     ctrl[0] = 0;
@@ -2814,15 +2814,15 @@ void launch_pair_cache_commit(const ObjDev& P, const PairCacheDev& c, const Pair
 {
     if (P.n > 0) { k_pc_commit<<<nblocks(P.n), TPB, 0, s>>>(P, c, L); note_launch(); }
 }
-void launch_pair_cache_end(const PairCacheDev& c, const PairListDev* ghost_lists, int n_ghost_lists, cudaStream_t s)
+void launch_pair_cache_end(const PairCacheDev& c, const PairListDev* lists, int n_lists, cudaStream_t s)
 {
-    GhostCounts gc{};
-    gc.n = std::min(n_ghost_lists, 3);
+    CachedCounts gc{};
+    gc.n = std::min(n_lists, 4);
     for (int k = 0; k < gc.n; ++k) {
-        gc.n_pairs[k] = ghost_lists[k].n_pairs;
-        gc.n_slots[k] = ghost_lists[k].n_slots;
-        gc.cap_pairs[k] = ghost_lists[k].cap_pairs;
-        gc.cap_contacts[k] = ghost_lists[k].cap_contacts;
+        gc.n_pairs[k] = lists[k].n_pairs;
+        gc.n_slots[k] = lists[k].n_slots;
+        gc.cap_pairs[k] = lists[k].cap_pairs;
+        gc.cap_contacts[k] = lists[k].cap_contacts;
     }
     k_pc_end<<<1, 1, 0, s>>>(c.ctrl, gc);
     note_launch();

@@ -367,9 +367,10 @@ void launch_pair_cache_commit(const ObjDev& P, const PairCacheDev& c, const Pair
 // cell; after the particle-wall narrow phase of a rebuild, keep their state
 void launch_pair_cache_check_walls(const ObjDev& W, const GeoSetDev& GW, const PairCacheDev& c, cudaStream_t s);
 void launch_pair_cache_commit_walls(const ObjDev& W, const PairCacheDev& c, cudaStream_t s);
-// end of a cached step: a rebuild whose ghost lists overflowed is not kept,
-// this step's requests become the next step's rebuild, the flags clear
-void launch_pair_cache_end(const PairCacheDev& c, const PairListDev* ghost_lists, int n_ghost_lists, cudaStream_t s);
+// end of a cached step: a list (particle-wall, ghosts) that overflowed asks
+// for a rebuild, this step's requests become the next step's rebuild, the
+// flags clear
+void launch_pair_cache_end(const PairCacheDev& c, const PairListDev* lists, int n_lists, cudaStream_t s);
 // wall_range (null: every wall): per particle, the first wall and the wall
 // count it may meet (a batch of simulations tiled into one)
 void launch_broad_pw(const ObjDev& P, const GeoSetDev& G, const ObjDev& W, const GeoSetDev& GW,
