@@ -837,7 +837,8 @@ struct fundem_sim {
     // written to the device flag
     // before a forced rebuild (outside any capture): the lists it builds hold
     // the skin's extra pairs and slots, so each cached list gets room for
-    // four times its current counts
+    // four (particle pairs) or eight (walls and images, whose slots grow more
+    // with the skin) times its current counts
     void pc_reserve()
     {
         if (!pc_active() || !pc_force) return;
@@ -847,7 +848,8 @@ struct fundem_sim {
             if (!L.allocated) continue;
             int c[2] = {0, 0};
             FD_CUDA(cudaMemcpy(c, L.gen[L.cur].counters.p, sizeof(c), cudaMemcpyDeviceToHost));
-            const int needp = 4 * c[0], needc = 4 * c[1];
+            const int f = k == FD_PP ? 4 : 8;
+            const int needp = f * c[0], needc = f * c[1];
             if (needp > L.cap_pairs || needc > L.cap_contacts)
                 L.grow(std::max(needp, L.cap_pairs), std::max(needc, L.cap_contacts));
         }
