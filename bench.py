@@ -452,6 +452,7 @@ def run_fundem(args, rank, world, dist):
                      "kernel": "k_narrow<PP> (narrow phase + contact law)", "peak_source": pk_kind,
                      "kernel_ms": nar_avg, "algorithmic_bytes": nar_bytes,
                      "step_achieved_gbs": step_bytes / (t_max / args.steps / 1e3) / 1e9},
+        "roofline_fp64": fp64_roofline(wc, wc_steps, nar_avg),
         "contact_updates_per_s": world * 0.5 * (contacts + contacts_end) * args.steps / (t_max / 1e3),
         "pair_cache": {"skin_m": pc1[2], "rebuilds_in_timed_steps": pc1[0] - pc0[0],
                        "timed_steps": pc1[1] - pc0[1],
@@ -481,6 +482,31 @@ def run_fundem(args, rank, world, dist):
 GRAPH_CHUNK = 50  # steps per CUDA graph in the graph-replay measurement
 # ncu summary holding the narrow phase's DRAM bytes per candidate pair
 TRAFFIC_PROFILE = "profiles/narrow_pp_traffic_bonded_column_65k.md"
+
+
+# the secondary flop model of the narrow phase: about 100 FP64 flops per node
+# given the exact predicate (two rotations, the grid mapping, the trilinear
+# value) and about 120 per contact (normal, contact point, the contact law)
+FLOPS_PER_TESTED_NODE = 100.0
+FLOPS_PER_CONTACT = 120.0
+FP64_PEAK_TFLOPS = 37.0  # nominal B200 FP64 (datasheet); no measured figure exists
+
+
+def fp64_roofline(wc, wc_steps, narrow_ms):
+    """The particle-particle narrow phase against FP64 throughput: flops per
+    step from the flop model and the work counters (nodes given the exact
+    predicate by the cached predicate pass, node contacts), over the group's
+    time per step."""
+    if not narrow_ms or wc_steps <= 0:
+        return None
+    tested = wc[5] / wc_steps if len(wc) > 5 else 0.0
+    contacts = wc[3] / wc_steps
+    flops = FLOPS_PER_TESTED_NODE * tested + FLOPS_PER_CONTACT * contacts
+    achieved = flops / (narrow_ms / 1e3) / 1e12
+    return {"bound": "fp64", "achieved": achieved, "peak": FP64_PEAK_TFLOPS, "unit": "TFLOP/s",
+            "frac": achieved / FP64_PEAK_TFLOPS, "peak_source": "nominal (no measured FP64 figure)",
+            "flops_per_step": flops, "model": f"{FLOPS_PER_TESTED_NODE:g} per node tested, "
+                                              f"{FLOPS_PER_CONTACT:g} per contact"}
 
 
 def profiled_traffic_per_pair():
