@@ -837,8 +837,8 @@ struct fundem_sim {
     // written to the device flag
     // before a forced rebuild (outside any capture): the lists it builds hold
     // the skin's extra pairs and slots, so each cached list gets room for
-    // four (particle pairs) or eight (walls and images, whose slots grow more
-    // with the skin) times its current counts
+    // four (particle pairs) or 32 (walls and images: few slots per pair
+    // without the skin, many more with it) times its current counts
     void pc_reserve()
     {
         if (!pc_active() || !pc_force) return;
@@ -848,7 +848,7 @@ struct fundem_sim {
             if (!L.allocated) continue;
             int c[2] = {0, 0};
             FD_CUDA(cudaMemcpy(c, L.gen[L.cur].counters.p, sizeof(c), cudaMemcpyDeviceToHost));
-            const int f = k == FD_PP ? 4 : 8;
+            const int f = k == FD_PP ? 4 : 32;
             const int needp = f * c[0], needc = f * c[1];
             if (needp > L.cap_pairs || needc > L.cap_contacts)
                 L.grow(std::max(needp, L.cap_pairs), std::max(needc, L.cap_contacts));
@@ -878,7 +878,7 @@ struct fundem_sim {
         return fd::RevDev{rev_cnt.p, rev_off.p, rev_fill.p, rev_code.p, (int)rev_code.n};
     }
     long long launches = 0;
-    long long hook_steps = 0;  // fundem_step_begin calls, for capacity checks
+    long long hook_steps = 0;  // steps of fundem_step and fundem_step_begin, for capacity checks
     // Captured runs of steps (fundem_step_graph).  A capture fixes which of
     // the two list generations each step writes and reads its history from,
     // so there is one graph per generation the run starts on: for an odd
@@ -1909,8 +1909,9 @@ int fundem_step(fundem_sim* s, int nsteps, const double g[3], double dt)
     return guard(s, [&] {
         FD_CUDA(cudaSetDevice(s->device));
         for (int k = 0; k < nsteps; ++k) {
-            // list capacities follow the counts every CAPACITY_CHECK steps
-            if (k > 0 && k % CAPACITY_CHECK == 0) s->ensure_capacity();
+            // list capacities follow the counts every CAPACITY_CHECK steps,
+            // counted across calls
+            if (++s->hook_steps % CAPACITY_CHECK == 0) s->ensure_capacity();
             s->pc_reserve();
             s->pc_prepare();
             s->front(d3(g), dt);
