@@ -2076,10 +2076,12 @@ int fundem_set_objects(fundem_sim* s, int wall, const double* pos, const double*
         s->pc_force = true;  // the pair cache rebuilds at the next step
         const size_t n = O.n();
         const bool dev = (O.n_dev == (int)n) && !O.dirty && n > 0;
+        // with the state on the device, the device copy is the one kept (the
+        // host copy is refreshed from it wherever it is read, pull())
         auto put = [&](void* ddst, void* hdst, const double* src, size_t bytes) {
             if (!src || bytes == 0) return;
-            std::memcpy(hdst, src, bytes);
             if (dev) FD_CUDA(cudaMemcpyAsync(ddst, src, bytes, cudaMemcpyHostToDevice, s->stream));
+            else std::memcpy(hdst, src, bytes);
         };
         put(O.d_pos.p, O.pos.data(), pos, sizeof(double3) * n);
         put(O.d_vel.p, O.vel.data(), vel, sizeof(double3) * n);
