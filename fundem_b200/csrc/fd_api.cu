@@ -795,6 +795,7 @@ struct fundem_sim {
     double pc_skin_set = 0.0;  // <= 0: PC_SKIN * the largest bounding radius
     bool pc_on = false;
     bool pc_force = true;      // the next cached step rebuilds
+    bool lists_exact = true;   // the lists hold an exact detection (no skin)
     long long pc_steps = 0;    // steps run with the cache
     void configure_pc()
     {
@@ -835,20 +836,21 @@ struct fundem_sim {
     }
     // before steps (outside any stream capture): a pending forced rebuild is
     // written to the device flag
-    // before a forced rebuild (outside any capture): the lists it builds hold
-    // the skin's extra pairs and slots, so each cached list gets room for
-    // four (particle pairs) or 32 (walls and images: few slots per pair
-    // without the skin, many more with it) times its current counts
+    // before the first cached build after an exact detection (outside any
+    // capture): it lists the skin's extra pairs and slots, so each cached
+    // list gets room for eight (particle pairs) or 32 (walls and images: few
+    // slots per pair without the skin, many more with it) times the exact
+    // counts; later builds grow with the capacity checks
     void pc_reserve()
     {
-        if (!pc_active() || !pc_force) return;
+        if (!pc_active() || !pc_force || !lists_exact) return;
         FD_CUDA(cudaStreamSynchronize(stream));
         for (int k : {FD_PP, FD_PW, FD_GX, FD_GY, FD_GXY}) {
             PairList& L = lists[k];
             if (!L.allocated) continue;
             int c[2] = {0, 0};
             FD_CUDA(cudaMemcpy(c, L.gen[L.cur].counters.p, sizeof(c), cudaMemcpyDeviceToHost));
-            const int f = k == FD_PP ? 4 : 32;
+            const int f = k == FD_PP ? 8 : 32;
             const int needp = f * c[0], needc = f * c[1];
             if (needp > L.cap_pairs || needc > L.cap_contacts)
                 L.grow(std::max(needp, L.cap_pairs), std::max(needc, L.cap_contacts));
@@ -1125,6 +1127,7 @@ struct fundem_sim {
         } else if (pc_on) {
             pc_force = true;
         }
+        lists_exact = !pc;
         // with the cache, the particle table serves only rebuild steps
         fd::launch_cell_table(Pv, T, scan_tmp.p, scan_tmp.n, stream, pc ? pcv.ctrl : nullptr);
         // wall hash (visibility and cell for the node test)
