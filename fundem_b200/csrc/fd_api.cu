@@ -851,7 +851,13 @@ struct fundem_sim {
             int c[2] = {0, 0};
             FD_CUDA(cudaMemcpy(c, L.gen[L.cur].counters.p, sizeof(c), cudaMemcpyDeviceToHost));
             const int f = k == FD_PP ? 8 : 32;
-            const int needp = f * c[0], needc = f * c[1];
+            int needp = f * c[0], needc = f * c[1];
+            if (k == FD_PW) {
+                // particles reach the walls over the run: room for every
+                // particle to meet up to four walls, with eight slots each
+                needp = std::max<long long>(needp, (long long)P.n() * std::min(W.n(), 4));
+                needc = std::max<long long>(needc, 8ll * P.n());
+            }
             if (needp > L.cap_pairs || needc > L.cap_contacts)
                 L.grow(std::max(needp, L.cap_pairs), std::max(needc, L.cap_contacts));
         }
