@@ -854,9 +854,13 @@ struct fundem_sim {
             int needp = f * c[0], needc = f * c[1];
             if (k == FD_PW) {
                 // particles reach the walls over the run: room for every
-                // particle to meet up to four walls, with eight slots each
+                // particle to meet up to four walls, and for an eighth of
+                // the nodes of every pair within the skin of its wall (a flat
+                // face parallel to the wall)
+                int max_nodes = 1;
+                for (const FdGeo& g : pgeo.table) max_nodes = std::max(max_nodes, g.node_count);
                 needp = std::max<long long>(needp, (long long)P.n() * std::min(W.n(), 4));
-                needc = std::max<long long>(needc, 8ll * P.n());
+                needc = std::max<long long>(needc, 8ll * P.n() + (long long)c[0] * max_nodes / 8);
             }
             if (needp > L.cap_pairs || needc > L.cap_contacts)
                 L.grow(std::max(needp, L.cap_pairs), std::max(needc, L.cap_contacts));
@@ -868,6 +872,29 @@ struct fundem_sim {
         const int one = 1;
         FD_CUDA(cudaMemcpyAsync(pc_ctrl.p, &one, sizeof(int), cudaMemcpyHostToDevice, stream));
         pc_force = false;
+        pc_verify = true;
+    }
+    // after the first steps of a forced rebuild (outside any capture): a
+    // cached list that overflowed is grown at once and rebuilt at the next
+    // step (its overflow stays reported)
+    bool pc_verify = false;
+    void pc_check_overflow()
+    {
+        if (!pc_verify || !pc_active()) return;
+        pc_verify = false;
+        FD_CUDA(cudaStreamSynchronize(stream));
+        bool over = false;
+        for (int k : {FD_PP, FD_PW, FD_GX, FD_GY, FD_GXY}) {
+            PairList& L = lists[k];
+            if (!L.allocated) continue;
+            int c[2] = {0, 0};
+            FD_CUDA(cudaMemcpy(c, L.gen[L.cur].counters.p, sizeof(c), cudaMemcpyDeviceToHost));
+            over = over || c[0] > L.cap_pairs || c[1] > L.cap_contacts;
+        }
+        if (over) {
+            ensure_capacity();
+            pc_force = true;
+        }
     }
     // reverse index over the particle and ghost lists (capacity: their pair
     // capacities together)
@@ -1897,6 +1924,7 @@ int fundem_step_begin(fundem_sim* s, const double g[3], double dt)
     if (!s->setup_done) return FUNDEM_ERR_STATE;
     return guard(s, [&] {
         if (++s->hook_steps % CAPACITY_CHECK == 0) s->ensure_capacity();
+        s->pc_check_overflow();
         s->pc_reserve();
         s->pc_prepare();
         s->front(d3(g), dt);
@@ -1921,6 +1949,7 @@ int fundem_step(fundem_sim* s, int nsteps, const double g[3], double dt)
             // list capacities follow the counts every CAPACITY_CHECK steps,
             // counted across calls
             if (++s->hook_steps % CAPACITY_CHECK == 0) s->ensure_capacity();
+            s->pc_check_overflow();
             s->pc_reserve();
             s->pc_prepare();
             s->front(d3(g), dt);
@@ -1937,7 +1966,8 @@ int fundem_step_graph(fundem_sim* s, int nsteps, const double g[3], double dt)
     if (!s->setup_done) return FUNDEM_ERR_STATE;
     return guard(s, [&] {
         FD_CUDA(cudaSetDevice(s->device));
-        s->pc_reserve();  // before the graph is looked up: it may grow the lists
+        s->pc_check_overflow();  // before the graph is looked up: these may grow the lists
+        s->pc_reserve();
         const double key[8] = {g[0], g[1], g[2], dt, (double)s->precision, (double)s->records,
                                (double)s->counters,
                                (double)(s->pc_active() * 8 + s->sector * 4 + s->perX * 2 + s->perY)};
