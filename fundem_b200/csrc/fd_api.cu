@@ -488,6 +488,7 @@ struct PairList {
     DevArray<float> c_phi0;  // pair cache: slot bounds of the last rebuild
     DevArray<float> p_bound; // pair cache: per-pair drift bound of a carried step
     DevArray<int> carry_n;   // pair cache: carried steps since the layout was built
+    DevArray<int> c_test, n_test;  // pair cache: slots listed for the predicate pass
     DevArray<double> c_force;
     DevArray<int4> p_aux;
     bool allocated = false;
@@ -511,6 +512,8 @@ struct PairList {
         c_phi0.alloc(cap_contacts, false);
         p_aux.alloc(cap_pairs); p_hist_cnt.alloc(cap_pairs); p_bound.alloc(cap_pairs, false);
         carry_n.alloc(1);
+        c_test.alloc(cap_contacts, false);
+        n_test.alloc(1);
         allocated = true;
     }
     void grow(int capp, int capc)
@@ -536,6 +539,7 @@ struct PairList {
             c_pair.grow(capc, 0);
             c_hit.grow(capc, 0);
             c_phi0.grow(capc, 0);  // rewritten by the rebuild a grow forces
+            c_test.grow(capc, 0);
             c_force.grow((size_t)capc * 9, 0);
             cap_contacts = capc;
         }
@@ -558,6 +562,8 @@ struct PairList {
         v.c_phi0 = c_phi0.p;
         v.p_bound = p_bound.p;
         v.carry_n = carry_n.p;
+        v.c_test = c_test.p;
+        v.n_test = n_test.p;
         return v;
     }
 };

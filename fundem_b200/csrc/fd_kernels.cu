@@ -1644,51 +1644,83 @@ __global__ void __launch_bounds__(NARROW_WARPS * 32, FD_SELECT_MIN_BLOCKS) k_sel
 // keeps node id -1.  Force and torques go to the slot; stage 3 sums them per
 // pair.
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// pair cache, carried steps: the slots the predicate pass must test.  A slot
+// is skipped when its node was outside B at the rebuild by more than the SDF
+// can change under the pair's relative motion since (|grad phi| <= lip, the
+// trilinear bound; k_pc_carry stored the pair's bound), or when B is an image
+// entry that is not live this step; the others are listed, so that the
+// predicate pass runs full warps.
+// ---------------------------------------------------------------------------
+template <int KIND>
+__global__ void __launch_bounds__(TPB) k_slot_filter(NarrowArgs n)
+{
+    PairListDev& L = n.L;
+    if (n.a.gate == nullptr || *n.a.gate != 0 || L.c_test == nullptr) return;
+    constexpr bool TRANSLATED = KIND == FD_GX || KIND == FD_GY || KIND == FD_GXY;
+    const bool live_test = TRANSLATED && n.gh.live != nullptr;
+    const int nitems = min(*L.n_slots, L.cap_contacts);
+    const int lane = threadIdx.x & 31;
+    const int stride = gridDim.x * blockDim.x;
+    int tested = 0, skipped = 0;
+    for (int s0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); s0 < nitems; s0 += stride) {
+        const int s = s0 + lane;
+        bool keep = false;
+        if (s < nitems) {
+            const int p = L.c_pair[s];
+            if (live_test && !n.gh.live[L.pairB[p]]) keep = false;
+            else keep = !(L.c_phi0[s] > __fadd_ru(L.p_bound[p], 1e-12f));
+            if (!keep) L.c_node[s] = -1;
+        }
+        const unsigned int m = __ballot_sync(0xffffffffu, keep);
+        if (m) {
+            int base = 0;
+            if (lane == 0) base = atomicAdd(L.n_test, __popc(m));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (keep) L.c_test[base + __popc(m & ((1u << lane) - 1u))] = s;
+        }
+        tested += __popc(m);
+        skipped += __popc(__ballot_sync(0xffffffffu, s < nitems)) - __popc(m);
+    }
+    if (n.a.stats && lane == 0) {
+        if (tested) atomicAdd(&n.a.stats[5], (unsigned long long)tested);
+        if (skipped) atomicAdd(&n.a.stats[6], (unsigned long long)skipped);
+    }
+}
+
 template <int KIND, int PASS>
 __global__ void __launch_bounds__(TPB, PASS == 0 ? FD_PROBE_MIN_BLOCKS : FD_CONTACT_MIN_BLOCKS) k_contact(NarrowArgs n)
 {
     PairListDev& L = n.L;
-    // pass 0: every slot; pass 1: the slots pass 0 listed as contacts
-    const int nitems = PASS == 0 ? min(*L.n_slots, L.cap_contacts) : min(*L.n_hits, L.cap_contacts);
-    const int lane = threadIdx.x & 31;
-    const bool periodic = (KIND == FD_PP || KIND == FD_PW) && (n.a.periodic_x || n.a.periodic_y);
-    const int stride = gridDim.x * blockDim.x;
-    // pair cache (particle-particle and translated ghost lists, predicate
-    // pass): a carried step tests the slot bound, a rebuild step stores it.
-    // A translated ghost list under the cache also holds the pairs of
-    // particles that have no image this step: their slots hold no contact.
+    // pair cache (particle-particle, particle-wall and translated image
+    // lists, predicate pass): a carried step tests the slots k_slot_filter
+    // listed, a rebuild step tests every slot and stores its bound.  An image
+    // list under the cache also holds the pairs of particles that have no
+    // image entry this step: their slots hold no contact.
     constexpr bool TRANSLATED = KIND == FD_GX || KIND == FD_GY || KIND == FD_GXY;
     const bool cache = (KIND == FD_PP || KIND == FD_PW || TRANSLATED) && PASS == 0 && n.a.gate != nullptr &&
                        L.c_phi0 != nullptr && n.a.drift != nullptr;
-    const bool carried = cache && *n.a.gate == 0;
-    const bool slot_test = carried;
+    const bool carried = cache && *n.a.gate == 0 && L.c_test != nullptr;
     const bool phi0_store = cache && !carried;
-    const bool live_test = TRANSLATED && PASS == 0 && n.gh.live != nullptr;
+    const bool live_test = TRANSLATED && PASS == 0 && n.gh.live != nullptr && !carried;
+    // pass 0: every slot (or the listed ones); pass 1: the slots pass 0
+    // listed as contacts
+    const int nitems = PASS == 0 ? min(carried ? *L.n_test : *L.n_slots, L.cap_contacts)
+                                 : min(*L.n_hits, L.cap_contacts);
+    const int lane = threadIdx.x & 31;
+    const bool periodic = (KIND == FD_PP || KIND == FD_PW) && (n.a.periodic_x || n.a.periodic_y);
+    const int stride = gridDim.x * blockDim.x;
     if (carried && blockIdx.x == 0 && threadIdx.x == 0 && L.carry_n) atomicAdd(L.carry_n, 1);
     int hits = 0;
     for (int s0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); s0 < nitems; s0 += stride) {
         const int t = s0 + lane;
         bool continue_slot = false;
-        const int s = (PASS == 1 && t < nitems) ? L.c_hit[t] : t;
+        const int s = t < nitems ? (PASS == 1 ? L.c_hit[t] : carried ? L.c_test[t] : t) : t;
         bool hit = false;
-        if ((slot_test || live_test) && t < nitems) {
-            const int p = L.c_pair[s];
-            if (live_test && !n.gh.live[L.pairB[p]]) {
-                L.c_node[s] = -1;
-                if (phi0_store) L.c_phi0[s] = __int_as_float(0xff800000);  // -inf: never skipped
-                continue_slot = true;
-            } else if (slot_test) {
-                // a step that carries the pair cache skips a slot whose node
-                // was outside B at the rebuild by more than the SDF can change
-                // under both bodies' drift since: |grad phi| <= lip (trilinear
-                // bound), and the node's offset in B's frame moved by at most
-                // the sum of the drift bounds (an image moves with its body);
-                // k_pc_carry stored lip_B (drift_A + drift_B) per pair
-                if (L.c_phi0[s] > __fadd_ru(L.p_bound[p], 1e-12f)) {
-                    L.c_node[s] = -1;
-                    continue_slot = true;
-                }
-            }
+        if (live_test && t < nitems && !n.gh.live[L.pairB[L.c_pair[s]]]) {
+            L.c_node[s] = -1;
+            if (phi0_store) L.c_phi0[s] = __int_as_float(0xff800000);  // -inf: never skipped
+            continue_slot = true;
         }
         if (t < nitems && !continue_slot) {
             const int p = L.c_pair[s];
@@ -1856,12 +1888,11 @@ __global__ void __launch_bounds__(TPB, PASS == 0 ? FD_PROBE_MIN_BLOCKS : FD_CONT
                 if (n.a.rec.hit && s < n.a.rec.cap) n.a.rec.hit[s] = hit ? 1 : 0;
             }
         }
-        if (cache && n.a.stats) {
-            // slots given the exact predicate, slots the bound skipped
+        if (phi0_store && n.a.stats) {
+            // a rebuild step gives every slot the exact predicate (carried
+            // steps are counted by k_slot_filter)
             const unsigned int tested = __ballot_sync(0xffffffffu, t < nitems && !continue_slot);
-            const unsigned int skipped = __ballot_sync(0xffffffffu, continue_slot);
             if (lane == 0 && tested) atomicAdd(&n.a.stats[5], (unsigned long long)__popc(tested));
-            if (lane == 0 && skipped) atomicAdd(&n.a.stats[6], (unsigned long long)__popc(skipped));
         }
         if (PASS == 0) {
             // contacts are listed for pass 1, one atomic per warp
@@ -2017,34 +2048,23 @@ __global__ void __launch_bounds__(TPB, PASS == 0 ? FD_PROBE_MIN_BLOCKS : FD_CONT
     constexpr bool TRANSLATED = KIND == FD_GX || KIND == FD_GY || KIND == FD_GXY;
     const bool cache = (KIND == FD_PP || KIND == FD_PW || TRANSLATED) && PASS == 0 && n.a.gate != nullptr &&
                        L.c_phi0 != nullptr && n.a.drift != nullptr;
-    const bool carried = cache && *n.a.gate == 0;
-    const bool slot_test = carried;
+    const bool carried = cache && *n.a.gate == 0 && L.c_test != nullptr;
     const bool phi0_store = cache && !carried;
-    const bool live_test = TRANSLATED && PASS == 0 && n.gh.live != nullptr;
+    const bool live_test = TRANSLATED && PASS == 0 && n.gh.live != nullptr && !carried;
+    const int nitems_c = PASS == 0 && carried ? min(*L.n_test, L.cap_contacts) : nitems;
     if (carried && blockIdx.x == 0 && threadIdx.x == 0 && L.carry_n) atomicAdd(L.carry_n, 1);
     int hits = 0;
-    for (int s0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); s0 < nitems; s0 += stride) {
+    for (int s0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); s0 < nitems_c; s0 += stride) {
         const int t = s0 + lane;
-        const int s = (PASS == 1 && t < nitems) ? L.c_hit[t] : t;
+        const int s = t < nitems_c ? (PASS == 1 ? L.c_hit[t] : carried ? L.c_test[t] : t) : t;
         bool hit = false;
         bool continue_slot = false;
-        if ((slot_test || live_test) && t < nitems) {
-            const int p = L.c_pair[s];
-            const int B = live_test ? L.pairB[p] : 0;
-            if (live_test && !n.gh.live[B]) {
-                L.c_node[s] = -1;
-                if (phi0_store) L.c_phi0[s] = __int_as_float(0xff800000);  // -inf: never skipped
-                continue_slot = true;
-            } else if (slot_test) {
-                // k_pc_carry's pair bound carries the margin of 1e-4 of B's
-                // grid spacing in this precision
-                if (L.c_phi0[s] > __fadd_ru(L.p_bound[p], 1e-12f)) {
-                    L.c_node[s] = -1;
-                    continue_slot = true;
-                }
-            }
+        if (live_test && t < nitems_c && !n.gh.live[L.pairB[L.c_pair[s]]]) {
+            L.c_node[s] = -1;
+            if (phi0_store) L.c_phi0[s] = __int_as_float(0xff800000);  // -inf: never skipped
+            continue_slot = true;
         }
-        if (t < nitems && !continue_slot) {
+        if (t < nitems_c && !continue_slot) {
             const int p = L.c_pair[s];
             const int k = L.c_k[s];
             const int A = L.pairA[p];
@@ -2889,6 +2909,9 @@ void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& 
                 L, P.n, wall ? W.hash : gh ? gh->hash : P.hash, wall ? wgrid : pgrid, a.gate, a.drift, \
                 a.disp, a.driftB ? a.driftB : a.drift, a.dispB ? a.dispB : a.disp,      \
                 wall ? W.geo : P.geo, wall ? GW.geo : G.geo, (mixed && !wall) ? 1e-4f : 0.f);          \
+            note_launch();                                                             \
+            cudaMemsetAsync(L.n_test, 0, sizeof(int), s);                              \
+            k_slot_filter<K><<<pgrid0, TPB, 0, s>>>(n);                                \
             note_launch();                                                             \
         }                                                                              \
         if (mixed) {                                                                   \

@@ -62,6 +62,9 @@ struct PairListDev {
     int* n_hits;       // device counter: contacts (n_slots + 1)
     int cap_contacts;  // slot capacity
     int* carry_n;      // pair cache: carried steps since the layout was built
+    int* c_test;       // pair cache, carried steps: the slots the bound does not
+                       // skip, listed for the predicate pass (n_test of them)
+    int* n_test;
     float* p_bound;    // pair cache, carried steps: per pair, how far the SDF can
                        // have moved at a node since the rebuild (k_pc_carry)
     float* c_phi0;     // pair cache: per slot, the node's signed distance to the
