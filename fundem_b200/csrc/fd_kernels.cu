@@ -1645,40 +1645,49 @@ __global__ void __launch_bounds__(NARROW_WARPS * 32, FD_SELECT_MIN_BLOCKS) k_sel
 // pair.
 // ---------------------------------------------------------------------------
 // ---------------------------------------------------------------------------
-// pair cache, carried steps: the slots the predicate pass must test.  A slot
-// is skipped when its node was outside B at the rebuild by more than the SDF
-// can change under the pair's relative motion since (|grad phi| <= lip, the
-// trilinear bound; k_pc_carry stored the pair's bound), or when B is an image
-// entry that is not live this step; the others are listed, so that the
-// predicate pass runs full warps.
+// pair cache, particle-particle list, carried steps: the slots the predicate
+// pass must test.  A slot is skipped when its node was outside B at the
+// rebuild by more than the SDF can change under the pair's relative motion
+// since (|grad phi| <= lip, the trilinear bound; k_pc_carry stored the pair's
+// bound); the others are listed, so that the predicate pass runs full warps.
+// The wall and image lists are short: there the extra pass cost more than
+// the idle lanes, and the predicate pass tests the bound itself.
 // ---------------------------------------------------------------------------
-template <int KIND>
 __global__ void __launch_bounds__(TPB) k_slot_filter(NarrowArgs n)
 {
     PairListDev& L = n.L;
     if (n.a.gate == nullptr || *n.a.gate != 0 || L.c_test == nullptr) return;
-    constexpr bool TRANSLATED = KIND == FD_GX || KIND == FD_GY || KIND == FD_GXY;
-    const bool live_test = TRANSLATED && n.gh.live != nullptr;
     const int nitems = min(*L.n_slots, L.cap_contacts);
     const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
     const int stride = gridDim.x * blockDim.x;
+    // one atomic per block and pass over its TPB slots: a per-warp atomic on
+    // the one counter queued some 40,000 same-address atomics a step
+    __shared__ int w_count[TPB / 32];
+    __shared__ int b_base;
     int tested = 0, skipped = 0;
-    for (int s0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); s0 < nitems; s0 += stride) {
-        const int s = s0 + lane;
+    for (int s0 = blockIdx.x * blockDim.x; s0 < nitems; s0 += stride) {
+        const int s = s0 + threadIdx.x;
         bool keep = false;
         if (s < nitems) {
-            const int p = L.c_pair[s];
-            if (live_test && !n.gh.live[L.pairB[p]]) keep = false;
-            else keep = !(L.c_phi0[s] > __fadd_ru(L.p_bound[p], 1e-12f));
+            keep = !(L.c_phi0[s] > __fadd_ru(L.p_bound[L.c_pair[s]], 1e-12f));
             if (!keep) L.c_node[s] = -1;
         }
         const unsigned int m = __ballot_sync(0xffffffffu, keep);
-        if (m) {
-            int base = 0;
-            if (lane == 0) base = atomicAdd(L.n_test, __popc(m));
-            base = __shfl_sync(0xffffffffu, base, 0);
-            if (keep) L.c_test[base + __popc(m & ((1u << lane) - 1u))] = s;
+        if (lane == 0) w_count[warp] = __popc(m);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int total = 0;
+            for (int w = 0; w < TPB / 32; ++w) {
+                const int c = w_count[w];
+                w_count[w] = total;
+                total += c;
+            }
+            b_base = total ? atomicAdd(L.n_test, total) : 0;
         }
+        __syncthreads();
+        if (keep) L.c_test[b_base + w_count[warp] + __popc(m & ((1u << lane) - 1u))] = s;
+        __syncthreads();
         tested += __popc(m);
         skipped += __popc(__ballot_sync(0xffffffffu, s < nitems)) - __popc(m);
     }
@@ -1693,19 +1702,22 @@ __global__ void __launch_bounds__(TPB, PASS == 0 ? FD_PROBE_MIN_BLOCKS : FD_CONT
 {
     PairListDev& L = n.L;
     // pair cache (particle-particle, particle-wall and translated image
-    // lists, predicate pass): a carried step tests the slots k_slot_filter
-    // listed, a rebuild step tests every slot and stores its bound.  An image
-    // list under the cache also holds the pairs of particles that have no
-    // image entry this step: their slots hold no contact.
+    // lists, predicate pass): a rebuild step tests every slot and stores its
+    // bound; a carried step tests the slots k_slot_filter listed (the
+    // particle-particle list) or tests the slot bound here (the others).  An
+    // image list under the cache also holds the pairs of particles that have
+    // no image entry this step: their slots hold no contact.
     constexpr bool TRANSLATED = KIND == FD_GX || KIND == FD_GY || KIND == FD_GXY;
     const bool cache = (KIND == FD_PP || KIND == FD_PW || TRANSLATED) && PASS == 0 && n.a.gate != nullptr &&
                        L.c_phi0 != nullptr && n.a.drift != nullptr;
-    const bool carried = cache && *n.a.gate == 0 && L.c_test != nullptr;
+    const bool carried = cache && *n.a.gate == 0;
+    const bool listed = KIND == FD_PP && carried && L.c_test != nullptr;
+    const bool slot_test = carried && !listed;
     const bool phi0_store = cache && !carried;
-    const bool live_test = TRANSLATED && PASS == 0 && n.gh.live != nullptr && !carried;
+    const bool live_test = TRANSLATED && PASS == 0 && n.gh.live != nullptr;
     // pass 0: every slot (or the listed ones); pass 1: the slots pass 0
     // listed as contacts
-    const int nitems = PASS == 0 ? min(carried ? *L.n_test : *L.n_slots, L.cap_contacts)
+    const int nitems = PASS == 0 ? min(listed ? *L.n_test : *L.n_slots, L.cap_contacts)
                                  : min(*L.n_hits, L.cap_contacts);
     const int lane = threadIdx.x & 31;
     const bool periodic = (KIND == FD_PP || KIND == FD_PW) && (n.a.periodic_x || n.a.periodic_y);
@@ -1715,12 +1727,19 @@ __global__ void __launch_bounds__(TPB, PASS == 0 ? FD_PROBE_MIN_BLOCKS : FD_CONT
     for (int s0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); s0 < nitems; s0 += stride) {
         const int t = s0 + lane;
         bool continue_slot = false;
-        const int s = t < nitems ? (PASS == 1 ? L.c_hit[t] : carried ? L.c_test[t] : t) : t;
+        const int s = t < nitems ? (PASS == 1 ? L.c_hit[t] : listed ? L.c_test[t] : t) : t;
         bool hit = false;
-        if (live_test && t < nitems && !n.gh.live[L.pairB[L.c_pair[s]]]) {
-            L.c_node[s] = -1;
-            if (phi0_store) L.c_phi0[s] = __int_as_float(0xff800000);  // -inf: never skipped
-            continue_slot = true;
+        if ((slot_test || live_test) && t < nitems) {
+            const int p = L.c_pair[s];
+            if (live_test && !n.gh.live[L.pairB[p]]) {
+                L.c_node[s] = -1;
+                if (phi0_store) L.c_phi0[s] = __int_as_float(0xff800000);  // -inf: never skipped
+                continue_slot = true;
+            } else if (slot_test && L.c_phi0[s] > __fadd_ru(L.p_bound[p], 1e-12f)) {
+                // the bound k_slot_filter tests for the particle-particle list
+                L.c_node[s] = -1;
+                continue_slot = true;
+            }
         }
         if (t < nitems && !continue_slot) {
             const int p = L.c_pair[s];
@@ -1888,11 +1907,13 @@ __global__ void __launch_bounds__(TPB, PASS == 0 ? FD_PROBE_MIN_BLOCKS : FD_CONT
                 if (n.a.rec.hit && s < n.a.rec.cap) n.a.rec.hit[s] = hit ? 1 : 0;
             }
         }
-        if (phi0_store && n.a.stats) {
-            // a rebuild step gives every slot the exact predicate (carried
-            // steps are counted by k_slot_filter)
+        if (cache && !listed && n.a.stats) {
+            // slots given the exact predicate, slots skipped (k_slot_filter
+            // counts the listed steps)
             const unsigned int tested = __ballot_sync(0xffffffffu, t < nitems && !continue_slot);
+            const unsigned int skipped = __ballot_sync(0xffffffffu, continue_slot);
             if (lane == 0 && tested) atomicAdd(&n.a.stats[5], (unsigned long long)__popc(tested));
+            if (lane == 0 && skipped) atomicAdd(&n.a.stats[6], (unsigned long long)__popc(skipped));
         }
         if (PASS == 0) {
             // contacts are listed for pass 1, one atomic per warp
@@ -2048,21 +2069,31 @@ __global__ void __launch_bounds__(TPB, PASS == 0 ? FD_PROBE_MIN_BLOCKS : FD_CONT
     constexpr bool TRANSLATED = KIND == FD_GX || KIND == FD_GY || KIND == FD_GXY;
     const bool cache = (KIND == FD_PP || KIND == FD_PW || TRANSLATED) && PASS == 0 && n.a.gate != nullptr &&
                        L.c_phi0 != nullptr && n.a.drift != nullptr;
-    const bool carried = cache && *n.a.gate == 0 && L.c_test != nullptr;
+    const bool carried = cache && *n.a.gate == 0;
+    const bool listed = KIND == FD_PP && carried && L.c_test != nullptr;
+    const bool slot_test = carried && !listed;
     const bool phi0_store = cache && !carried;
-    const bool live_test = TRANSLATED && PASS == 0 && n.gh.live != nullptr && !carried;
-    const int nitems_c = PASS == 0 && carried ? min(*L.n_test, L.cap_contacts) : nitems;
+    const bool live_test = TRANSLATED && PASS == 0 && n.gh.live != nullptr;
+    const int nitems_c = PASS == 0 && listed ? min(*L.n_test, L.cap_contacts) : nitems;
     if (carried && blockIdx.x == 0 && threadIdx.x == 0 && L.carry_n) atomicAdd(L.carry_n, 1);
     int hits = 0;
     for (int s0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); s0 < nitems_c; s0 += stride) {
         const int t = s0 + lane;
-        const int s = t < nitems_c ? (PASS == 1 ? L.c_hit[t] : carried ? L.c_test[t] : t) : t;
+        const int s = t < nitems_c ? (PASS == 1 ? L.c_hit[t] : listed ? L.c_test[t] : t) : t;
         bool hit = false;
         bool continue_slot = false;
-        if (live_test && t < nitems_c && !n.gh.live[L.pairB[L.c_pair[s]]]) {
-            L.c_node[s] = -1;
-            if (phi0_store) L.c_phi0[s] = __int_as_float(0xff800000);  // -inf: never skipped
-            continue_slot = true;
+        if ((slot_test || live_test) && t < nitems_c) {
+            const int p = L.c_pair[s];
+            if (live_test && !n.gh.live[L.pairB[p]]) {
+                L.c_node[s] = -1;
+                if (phi0_store) L.c_phi0[s] = __int_as_float(0xff800000);  // -inf: never skipped
+                continue_slot = true;
+            } else if (slot_test && L.c_phi0[s] > __fadd_ru(L.p_bound[p], 1e-12f)) {
+                // k_pc_carry's pair bound carries the margin of 1e-4 of B's
+                // grid spacing in this precision
+                L.c_node[s] = -1;
+                continue_slot = true;
+            }
         }
         if (t < nitems_c && !continue_slot) {
             const int p = L.c_pair[s];
@@ -2910,9 +2941,11 @@ void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& 
                 a.disp, a.driftB ? a.driftB : a.drift, a.dispB ? a.dispB : a.disp,      \
                 wall ? W.geo : P.geo, wall ? GW.geo : G.geo, (mixed && !wall) ? 1e-4f : 0.f);          \
             note_launch();                                                             \
-            cudaMemsetAsync(L.n_test, 0, sizeof(int), s);                              \
-            k_slot_filter<K><<<pgrid0, TPB, 0, s>>>(n);                                \
-            note_launch();                                                             \
+            if (K == FD_PP) {                                                          \
+                cudaMemsetAsync(L.n_test, 0, sizeof(int), s);                          \
+                k_slot_filter<<<pgrid0, TPB, 0, s>>>(n);                               \
+                note_launch();                                                         \
+            }                                                                          \
         }                                                                              \
         if (mixed) {                                                                   \
             k_contact32<K, 0><<<pgrid0, TPB, 0, s>>>(n); note_launch();                               \
