@@ -944,10 +944,21 @@ struct fundem_sim {
             g.exec = nullptr;
         }
     }
+    // translated periodicity: the image detection runs on its own stream
+    // beside the particle-particle and particle-wall detection, on a copy of
+    // the positions that the periodic wraps change (the lists already
+    // detected saw them unwrapped); the wrapped positions come back when the
+    // branches join
+    cudaStream_t img_stream = nullptr;
+    cudaEvent_t img_fork = nullptr, img_join = nullptr;
+    DevArray<double3> img_pos;
     ~fundem_sim()
     {
         drop_graph();
         if (cap_stream) cudaStreamDestroy(cap_stream);
+        if (img_stream) cudaStreamDestroy(img_stream);
+        if (img_fork) cudaEventDestroy(img_fork);
+        if (img_join) cudaEventDestroy(img_join);
     }
     AdjState adj;
     AdjTape tape;
@@ -1137,6 +1148,12 @@ struct fundem_sim {
                 ghosts[d].cells.alloc(pgrid, np);
             }
         }
+        if ((perX || perY) && !sector) {
+            img_pos.alloc(std::max(np, 1), false);
+            if (!img_stream) FD_CUDA(cudaStreamCreateWithFlags(&img_stream, cudaStreamNonBlocking));
+            if (!img_fork) FD_CUDA(cudaEventCreateWithFlags(&img_fork, cudaEventDisableTiming));
+            if (!img_join) FD_CUDA(cudaEventCreateWithFlags(&img_join, cudaEventDisableTiming));
+        }
         size_t st = std::max<size_t>(fd::scan_tmp_size(pgrid.num), fd::scan_tmp_size(np));
         scan_tmp.alloc(st + 16);
         if (!flags.p) flags.alloc(1);
@@ -1176,6 +1193,88 @@ struct fundem_sim {
         int active[FD_NKIND] = {1, 1, 0, 0, 0};
         if (new_generation)
             for (int k = 0; k < FD_NKIND; ++k) lists[k].cur ^= 1;
+        PairListDev Lg[6];
+        // the translated image sets share the pair cache (not with sector
+        // periodicity): their pairs and slots are kept with the particle
+        // pairs', and a wrap or an image in a clamped cell rebuilds them
+        const bool pcg = pc && !sector;
+        int* gctrl = pcg ? pcv.ctrl : nullptr;
+        bool img_wrapped = false;
+        // PeriodicBoundaryXY2D then PeriodicBoundarySector::updateGhostSpatialGrid
+        // (LSSolver.h:780-784), then the detection of every image set, on
+        // stream gs with the particle set Pg.  wrap_src non-null: Pg.pos is a
+        // separate array, and the first wrap fills it from wrap_src.
+        auto image_stage = [&](cudaStream_t gs, ObjDev Pg, const double3* wrap_src) {
+            tbegin(FUNDEM_T_GHOST);
+            const int kinds[6] = {FD_GX, FD_GY, FD_GXY, FD_GR90, FD_GR180, FD_GR270};
+            for (int d = 0; d < 3; ++d) {
+                if (!ghosts[d].active) continue;
+                if (d < 2) {
+                    fd::launch_wrap(Pg, pgrid, d, gs, gctrl, img_wrapped ? nullptr : wrap_src);
+                    img_wrapped = true;
+                }
+                fd::GhostDev gh = ghosts[d].view(pcg);
+                fd::launch_ghost_build(Pg, gh, kinds[d], gs, pcg ? pcv.skin : 0.0, gctrl);
+            }
+            if (pcg) fd::launch_ghost_gate(gctrl, gs);
+            for (int d = 0; d < 3; ++d) {
+                if (!ghosts[d].active) continue;
+                fd::GhostDev gh = ghosts[d].view(pcg);
+                ObjDev ghostobj = Pg;
+                ghostobj.hash = ghosts[d].hash.p;
+                fd::launch_cell_table(ghostobj, gh.cells, scan_tmp.p, scan_tmp.n, gs, pcg ? gctrl + 5 : nullptr);
+            }
+            if (sector) {
+                fd::launch_sector_wrap(Pg, pgrid, gs);
+                fd::GhostDev sv[3] = {ghosts[3].view(), ghosts[4].view(), ghosts[5].view()};
+                fd::launch_sector_images(Pg, sv, gs);
+                for (int d = 3; d < 6; ++d) {
+                    ObjDev ghostobj = Pg;
+                    ghostobj.hash = ghosts[d].hash.p;
+                    fd::launch_cell_table(ghostobj, sv[d - 3].cells, scan_tmp.p, scan_tmp.n, gs);
+                }
+            }
+            for (int d = 0; d < 6; ++d) {
+                if (!ghosts[d].active) continue;
+                const bool cached = pcg && d < 3;
+                fd::GhostDev gh = ghosts[d].view(cached);
+                Lg[d] = lists[kinds[d]].view();
+                fd::StepArgs ag = a;
+                if (cached) {
+                    ag.skin = pcv.skin;
+                    ag.gate = gctrl + 5;
+                    ag.noskin = gctrl + 6;
+                    ag.drift = pcv.drift;
+                    ag.disp = pcv.disp;
+                    fd::launch_broad_ghost(Pg, G, gh, Lg[d], flags.p, probe, gs, pcv.skin, gctrl + 5, gctrl + 6);
+                } else {
+                    fd::launch_broad_ghost(Pg, G, gh, Lg[d], flags.p, probe, gs);
+                }
+                ag.rec = recording ? recording->rec(kinds[d], record_step) : fd::AdjRec{};
+                fd::launch_narrow(kinds[d], Pg, G, M, Wv, GW, MW, pgrid, wgrid, &gh, Lg[d], ag, with_force, mixed(),
+                                  gs);
+                if (recording)
+                    FD_CUDA(cudaMemcpyAsync(recording->ns(kinds[d], record_step), Lg[d].n_slots, sizeof(int),
+                                            cudaMemcpyDeviceToDevice, gs));
+                active[kinds[d]] = 1;
+            }
+            tend(FUNDEM_T_GHOST);
+        };
+        // translated periodicity outside per-stage timing: the image stage
+        // runs beside the particle and wall lists.  It reads and writes
+        // nothing they touch: its own lists, tables and image arrays, the
+        // wrapped copy of the positions, the pair cache's words 4-7 (which
+        // those lists do not read) and, with atomics, the flags and counters.
+        const bool img_branch = (perX || perY) && !sector && img_stream && img_pos.p && img_pos.n >= (size_t)Pv.n &&
+                                (!profiling || capturing);
+        if (img_branch) {
+            FD_CUDA(cudaEventRecord(img_fork, stream));
+            FD_CUDA(cudaStreamWaitEvent(img_stream, img_fork, 0));
+            ObjDev Pg = Pv;
+            Pg.pos = img_pos.p;
+            image_stage(img_stream, Pg, Pv.pos);
+            FD_CUDA(cudaEventRecord(img_join, img_stream));
+        }
         PairListDev Lpp = lists[FD_PP].view();
         tbegin(FUNDEM_T_BROAD);
         if (use_nl) {
@@ -1233,67 +1332,14 @@ struct fundem_sim {
             FD_CUDA(cudaMemcpyAsync(recording->ns(FD_PW, record_step), Lpw.n_slots, sizeof(int),
                                     cudaMemcpyDeviceToDevice, stream));
         tend(FUNDEM_T_NARROW_PW);
-        PairListDev Lg[6];
-        // the translated image sets share the pair cache (not with sector
-        // periodicity): their pairs and slots are kept with the particle
-        // pairs', and a wrap or an image in a clamped cell rebuilds them
-        const bool pcg = pc && !sector;
-        int* gctrl = pcg ? pcv.ctrl : nullptr;
-        if (perX || perY || sector) {
-            tbegin(FUNDEM_T_GHOST);
-            // PeriodicBoundaryXY2D then PeriodicBoundarySector::updateGhostSpatialGrid
-            // (LSSolver.h:780-784), then the detection of every image set
-            const int kinds[6] = {FD_GX, FD_GY, FD_GXY, FD_GR90, FD_GR180, FD_GR270};
-            for (int d = 0; d < 3; ++d) {
-                if (!ghosts[d].active) continue;
-                if (d == 0) fd::launch_wrap(Pv, pgrid, 0, stream, gctrl);
-                if (d == 1) fd::launch_wrap(Pv, pgrid, 1, stream, gctrl);
-                fd::GhostDev gh = ghosts[d].view(pcg);
-                fd::launch_ghost_build(Pv, gh, kinds[d], stream, pcg ? pcv.skin : 0.0, gctrl);
-            }
-            if (pcg) fd::launch_ghost_gate(gctrl, stream);
-            for (int d = 0; d < 3; ++d) {
-                if (!ghosts[d].active) continue;
-                fd::GhostDev gh = ghosts[d].view(pcg);
-                ObjDev ghostobj = Pv;
-                ghostobj.hash = ghosts[d].hash.p;
-                fd::launch_cell_table(ghostobj, gh.cells, scan_tmp.p, scan_tmp.n, stream, pcg ? gctrl + 5 : nullptr);
-            }
-            if (sector) {
-                fd::launch_sector_wrap(Pv, pgrid, stream);
-                fd::GhostDev sv[3] = {ghosts[3].view(), ghosts[4].view(), ghosts[5].view()};
-                fd::launch_sector_images(Pv, sv, stream);
-                for (int d = 3; d < 6; ++d) {
-                    ObjDev ghostobj = Pv;
-                    ghostobj.hash = ghosts[d].hash.p;
-                    fd::launch_cell_table(ghostobj, sv[d - 3].cells, scan_tmp.p, scan_tmp.n, stream);
-                }
-            }
-            for (int d = 0; d < 6; ++d) {
-                if (!ghosts[d].active) continue;
-                const bool cached = pcg && d < 3;
-                fd::GhostDev gh = ghosts[d].view(cached);
-                Lg[d] = lists[kinds[d]].view();
-                fd::StepArgs ag = a;
-                if (cached) {
-                    ag.skin = pcv.skin;
-                    ag.gate = gctrl + 5;
-                    ag.noskin = gctrl + 6;
-                    ag.drift = pcv.drift;
-                    ag.disp = pcv.disp;
-                    fd::launch_broad_ghost(Pv, G, gh, Lg[d], flags.p, probe, stream, pcv.skin, gctrl + 5, gctrl + 6);
-                } else {
-                    fd::launch_broad_ghost(Pv, G, gh, Lg[d], flags.p, probe, stream);
-                }
-                ag.rec = recording ? recording->rec(kinds[d], record_step) : fd::AdjRec{};
-                fd::launch_narrow(kinds[d], Pv, G, M, Wv, GW, MW, pgrid, wgrid, &gh, Lg[d], ag, with_force, mixed(),
-                                  stream);
-                if (recording)
-                    FD_CUDA(cudaMemcpyAsync(recording->ns(kinds[d], record_step), Lg[d].n_slots, sizeof(int),
-                                            cudaMemcpyDeviceToDevice, stream));
-                active[kinds[d]] = 1;
-            }
-            tend(FUNDEM_T_GHOST);
+        if (img_branch) {
+            // the image detection ran beside; its wrapped positions replace
+            // the ones the particle and wall lists were detected with
+            FD_CUDA(cudaStreamWaitEvent(stream, img_join, 0));
+            if (img_wrapped && Pv.n > 0)
+                FD_CUDA(cudaMemcpyAsync(Pv.pos, img_pos.p, sizeof(double3) * Pv.n, cudaMemcpyDeviceToDevice, stream));
+        } else if (perX || perY || sector) {
+            image_stage(stream, Pv, nullptr);
         }
         if (pc) {
             PairListDev gl[4];

@@ -375,11 +375,11 @@ __device__ __forceinline__ int wrap_code(double3 cA, double3 ri, double3 cB, dou
            27 * (sh(rj.y - cB.y, Ly) + 1);
 }
 
-__global__ void k_wrap(ObjDev P, FdGrid g, int dim, int* ctrl)
+__global__ void k_wrap(ObjDev P, FdGrid g, int dim, int* ctrl, const double3* src)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.n) return;
-    const double3 p0 = P.pos[i];
+    const double3 p0 = src ? src[i] : P.pos[i];
     const double3 p1 = dim == 0 ? wrap_x(p0, g) : wrap_y(p0, g);
     P.pos[i] = p1;
     // under the pair cache a wrap changes which particles have images: the
@@ -2807,9 +2807,9 @@ void launch_cell_table(ObjDev& O, CellTableDev& T, int* scan_tmp, size_t, cudaSt
     note_launch();
     k_cell_order<<<nblocks(T.g.num), TPB, 0, s>>>(T.g.num, T.count, T.start, T.sorted, gate); note_launch();
 }
-void launch_wrap(ObjDev& P, const FdGrid& g, int dim, cudaStream_t s, int* ctrl)
+void launch_wrap(ObjDev& P, const FdGrid& g, int dim, cudaStream_t s, int* ctrl, const double3* src)
 {
-    if (P.n > 0) { k_wrap<<<nblocks(P.n), TPB, 0, s>>>(P, g, dim, ctrl); note_launch(); }
+    if (P.n > 0) { k_wrap<<<nblocks(P.n), TPB, 0, s>>>(P, g, dim, ctrl, src); note_launch(); }
 }
 void launch_ghost_build(const ObjDev& P, GhostDev& Gh, int kind, cudaStream_t s, double ext_skin, int* ctrl)
 {

@@ -338,7 +338,9 @@ void radix_sort_keys(const long long* keys, int n, long long num_keys, unsigned 
 void radix_sort_scratch(int n, size_t& bcount_ints, size_t& bscan_ints);
 // ctrl (the pair cache's, or null): a wrap requests the uncached ghost
 // stage this step and a rebuild at the next
-void launch_wrap(ObjDev& P, const FdGrid& g, int dim, cudaStream_t s, int* ctrl = nullptr);
+// src: positions to wrap into P.pos (null: P.pos in place)
+void launch_wrap(ObjDev& P, const FdGrid& g, int dim, cudaStream_t s, int* ctrl = nullptr,
+                 const double3* src = nullptr);
 // ext_skin > 0 (the pair cache, ctrl non-null): particles within ext_skin of
 // the image band get images too (Gh.live marks the true ones); an image
 // outside the domain in a direction it is not translated along (the
