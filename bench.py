@@ -253,11 +253,14 @@ def run_fundem(args, rank, world, dist):
         # the narrow phase's launch shape, tuned on this state (untimed;
         # results do not depend on it)
         from fundem_b200 import autotune
-        best, times = autotune.launch_shape(sim, steps=10)
+        tune_steps = 40
+        best, times = autotune.launch_shape(sim, steps=tune_steps, restart=True)
         shape = {"chosen_blocks_per_sm": list(sim.launch_shape()),
                  "order": ["select", "probe", "contact", "sums"],
-                 "ms_per_step": {",".join(str(v) for v in k): 1e3 * t / 10 for k, t in times.items()},
-                 "note": "autotune.launch_shape after the warm-up steps (10 steps per candidate, 0 = default)"}
+                 "ms_per_step": {",".join(str(v) for v in k): 1e3 * t / tune_steps for k, t in times.items()},
+                 "note": f"autotune.launch_shape after the warm-up steps: every candidate runs {tune_steps} steps "
+                         "from one checkpoint of that state (a pair-cache rebuild first, then the same steps "
+                         "for all), 0 = default"}
         log0(f"launch shape {sim.launch_shape()}")
     if not args.no_graph:
         # the headline replays one CUDA graph of K steps (fundem_step_graph);

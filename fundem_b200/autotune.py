@@ -50,28 +50,49 @@ def checkpoint_interval(make_sim, steps, dl_dpos, dl_dvel, candidates=(25, 50, 1
 LAUNCH_SHAPES = ((0, 0, 0, 0), (8, 4, 4, 4), (4, 8, 4, 4), (4, 4, 8, 8), (4, 2, 2, 2), (8, 8, 8, 8), (2, 4, 4, 4))
 
 
-def launch_shape(sim, steps=20, candidates=LAUNCH_SHAPES, timer=None):
+def launch_shape(sim, steps=20, candidates=LAUNCH_SHAPES, timer=None, restart=False):
     """Time `steps` steps of `sim` under each candidate launch shape
     (select, probe, contact, sums blocks per SM; 0 = default), leave the
-    fastest set and return (best, {shape: seconds}).  Advances the
-    simulation by len(candidates) * steps steps (plus one untimed step per
-    candidate after the shape changes).  timer() returns a stop callable
-    giving seconds (default: wall clock around synchronised runs)."""
+    fastest set and return (best, {shape: seconds}).  timer() returns a stop
+    callable giving seconds (default: wall clock around synchronised runs).
+
+    restart=False: the candidates run one after another from the current
+    state, each after one untimed step; the simulation advances by
+    len(candidates) * (steps + 1) steps.  restart=True: every candidate runs
+    from the same checkpoint of the current state (written to a temporary
+    file), which starts it with a pair-cache rebuild, so that all of them do
+    the same work, rebuild steps included (the selection's shape matters only
+    there); the simulation ends `steps` steps after the checkpoint."""
     times = {}
-    for shape in candidates:
-        sim.set_launch_shape(*shape)
-        sim.step(1)
-        sim.sync()
-        if timer is None:
-            t0 = time.perf_counter()
-            sim.step(steps)
+    tmp = None
+    if restart:
+        import os
+        import tempfile
+        fd, tmp = tempfile.mkstemp(suffix=".fdck")
+        os.close(fd)
+        sim.checkpoint_write(tmp)
+    try:
+        for shape in candidates:
+            if restart:
+                sim.checkpoint_read(tmp)
+            sim.set_launch_shape(*shape)
+            if not restart:
+                sim.step(1)
             sim.sync()
-            times[tuple(shape)] = time.perf_counter() - t0
-        else:
-            stop = timer()
-            sim.step(steps)
-            times[tuple(shape)] = stop()
-            sim.sync()
+            if timer is None:
+                t0 = time.perf_counter()
+                sim.step(steps)
+                sim.sync()
+                times[tuple(shape)] = time.perf_counter() - t0
+            else:
+                stop = timer()
+                sim.step(steps)
+                times[tuple(shape)] = stop()
+                sim.sync()
+    finally:
+        if tmp is not None:
+            import os
+            os.remove(tmp)
     best = min(times, key=times.get)
     sim.set_launch_shape(*best)
     return best, times

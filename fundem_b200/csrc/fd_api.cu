@@ -905,17 +905,24 @@ struct fundem_sim {
     // reverse index over the particle and ghost lists (capacity: their pair
     // capacities together)
     DevArray<int> rev_cnt, rev_off, rev_fill, rev_code;
+    // the reverse index holds the pairs of the lists the last step used
+    // (a reallocation empties it: the next step builds it whatever the flags)
+    bool rev_valid = false;
     fd::RevDev rev_view()
     {
         const int np = std::max(P.n(), 1);
         if (rev_cnt.n < (size_t)np) {
             rev_cnt.alloc(np); rev_off.alloc(np); rev_fill.alloc(np);
+            rev_valid = false;
         }
         long long cap = 0;
         for (int k : {FD_PP, FD_GX, FD_GY, FD_GXY, FD_GR90, FD_GR180, FD_GR270})
             if (lists[k].allocated) cap += lists[k].cap_pairs;
         cap = std::max<long long>(cap, 16);
-        if (rev_code.n < (size_t)cap) rev_code.alloc((size_t)cap, false);
+        if (rev_code.n < (size_t)cap) {
+            rev_code.alloc((size_t)cap, false);
+            rev_valid = false;
+        }
         return fd::RevDev{rev_cnt.p, rev_off.p, rev_fill.p, rev_code.p, (int)rev_code.n};
     }
     long long launches = 0;
@@ -944,21 +951,23 @@ struct fundem_sim {
             g.exec = nullptr;
         }
     }
-    // translated periodicity: the image detection runs on its own stream
-    // beside the particle-particle and particle-wall detection, on a copy of
-    // the positions that the periodic wraps change (the lists already
-    // detected saw them unwrapped); the wrapped positions come back when the
-    // branches join
-    cudaStream_t img_stream = nullptr;
-    cudaEvent_t img_fork = nullptr, img_join = nullptr;
+    // the particle-wall list (branch 1) and, with translated periodicity,
+    // the image lists (branch 0) are detected on streams of their own beside
+    // the particle-particle list.  The image branch works on a copy of the
+    // positions that the periodic wraps change (the other lists are detected
+    // with them unwrapped); the wrapped positions come back at the join.
+    cudaStream_t br_stream[2] = {nullptr, nullptr};
+    cudaEvent_t br_fork = nullptr, br_join[2] = {nullptr, nullptr};
     DevArray<double3> img_pos;
     ~fundem_sim()
     {
         drop_graph();
         if (cap_stream) cudaStreamDestroy(cap_stream);
-        if (img_stream) cudaStreamDestroy(img_stream);
-        if (img_fork) cudaEventDestroy(img_fork);
-        if (img_join) cudaEventDestroy(img_join);
+        for (int b = 0; b < 2; ++b) {
+            if (br_stream[b]) cudaStreamDestroy(br_stream[b]);
+            if (br_join[b]) cudaEventDestroy(br_join[b]);
+        }
+        if (br_fork) cudaEventDestroy(br_fork);
     }
     AdjState adj;
     AdjTape tape;
@@ -1148,12 +1157,12 @@ struct fundem_sim {
                 ghosts[d].cells.alloc(pgrid, np);
             }
         }
-        if ((perX || perY) && !sector) {
-            img_pos.alloc(std::max(np, 1), false);
-            if (!img_stream) FD_CUDA(cudaStreamCreateWithFlags(&img_stream, cudaStreamNonBlocking));
-            if (!img_fork) FD_CUDA(cudaEventCreateWithFlags(&img_fork, cudaEventDisableTiming));
-            if (!img_join) FD_CUDA(cudaEventCreateWithFlags(&img_join, cudaEventDisableTiming));
+        if ((perX || perY) && !sector) img_pos.alloc(std::max(np, 1), false);
+        for (int b = 0; b < 2; ++b) {
+            if (!br_stream[b]) FD_CUDA(cudaStreamCreateWithFlags(&br_stream[b], cudaStreamNonBlocking));
+            if (!br_join[b]) FD_CUDA(cudaEventCreateWithFlags(&br_join[b], cudaEventDisableTiming));
         }
+        if (!br_fork) FD_CUDA(cudaEventCreateWithFlags(&br_fork, cudaEventDisableTiming));
         size_t st = std::max<size_t>(fd::scan_tmp_size(pgrid.num), fd::scan_tmp_size(np));
         scan_tmp.alloc(st + 16);
         if (!flags.p) flags.alloc(1);
@@ -1260,20 +1269,55 @@ struct fundem_sim {
             }
             tend(FUNDEM_T_GHOST);
         };
-        // translated periodicity outside per-stage timing: the image stage
-        // runs beside the particle and wall lists.  It reads and writes
-        // nothing they touch: its own lists, tables and image arrays, the
-        // wrapped copy of the positions, the pair cache's words 4-7 (which
-        // those lists do not read) and, with atomics, the flags and counters.
-        const bool img_branch = (perX || perY) && !sector && img_stream && img_pos.p && img_pos.n >= (size_t)Pv.n &&
-                                (!profiling || capturing);
+        PairListDev Lpw = lists[FD_PW].view();
+        auto wall_stage = [&](cudaStream_t ws) {
+            tbegin(FUNDEM_T_BROAD);
+            fd::launch_broad_pw(Pv, G, Wv, GW, wgrid, Lpw, flags.p, probe, ws,
+                                wall_groups.empty() ? nullptr : d_wall_groups.p, pc ? pcv.skin : 0.0,
+                                pc ? pcv.ctrl : nullptr);
+            tend(FUNDEM_T_BROAD);
+            tbegin(FUNDEM_T_NARROW_PW);
+            // the particle-wall list shares the cache (wall drifts and cells
+            // in its rebuild flag)
+            fd::StepArgs aw = a;
+            aw.rec = recording ? recording->rec(FD_PW, record_step) : fd::AdjRec{};
+            if (pc) {
+                aw.skin = pcv.skin;
+                aw.gate = pcv.ctrl;
+                aw.drift = pcv.drift;
+                aw.disp = pcv.disp;
+                aw.driftB = pcv.wdrift;
+                aw.dispB = pcv.wdisp;
+            }
+            fd::launch_narrow(FD_PW, Pv, G, M, Wv, GW, MW, pgrid, wgrid, nullptr, Lpw, aw, with_force, mixed(), ws);
+            if (pc && W.n_dev > 0) fd::launch_pair_cache_commit_walls(Wv, pcv, ws);
+            if (recording)
+                FD_CUDA(cudaMemcpyAsync(recording->ns(FD_PW, record_step), Lpw.n_slots, sizeof(int),
+                                        cudaMemcpyDeviceToDevice, ws));
+            tend(FUNDEM_T_NARROW_PW);
+        };
+        // outside per-stage timing the wall list and the images (translated
+        // periodicity) run beside the particle-particle list.  Each branch
+        // reads and writes nothing another one writes: its own lists, tables
+        // and image arrays; the wall references of the pair cache (branch 1);
+        // the wrapped copy of the positions and the pair cache's words 4-7,
+        // which the others do not read (branch 0); the flags and counters
+        // with atomics.  The pair cache's rebuild flag (word 0) and drifts
+        // are written before the fork.
+        const bool branches = br_stream[0] && br_stream[1] && (!profiling || capturing);
+        const bool img_branch = branches && (perX || perY) && !sector && img_pos.p && img_pos.n >= (size_t)Pv.n;
+        if (branches) FD_CUDA(cudaEventRecord(br_fork, stream));
         if (img_branch) {
-            FD_CUDA(cudaEventRecord(img_fork, stream));
-            FD_CUDA(cudaStreamWaitEvent(img_stream, img_fork, 0));
+            FD_CUDA(cudaStreamWaitEvent(br_stream[0], br_fork, 0));
             ObjDev Pg = Pv;
             Pg.pos = img_pos.p;
-            image_stage(img_stream, Pg, Pv.pos);
-            FD_CUDA(cudaEventRecord(img_join, img_stream));
+            image_stage(br_stream[0], Pg, Pv.pos);
+            FD_CUDA(cudaEventRecord(br_join[0], br_stream[0]));
+        }
+        if (branches) {
+            FD_CUDA(cudaStreamWaitEvent(br_stream[1], br_fork, 0));
+            wall_stage(br_stream[1]);
+            FD_CUDA(cudaEventRecord(br_join[1], br_stream[1]));
         }
         PairListDev Lpp = lists[FD_PP].view();
         tbegin(FUNDEM_T_BROAD);
@@ -1304,52 +1348,28 @@ struct fundem_sim {
             FD_CUDA(cudaMemcpyAsync(recording->ns(FD_PP, record_step), Lpp.n_slots, sizeof(int),
                                     cudaMemcpyDeviceToDevice, stream));
         tend(FUNDEM_T_NARROW_PP);
-        PairListDev Lpw = lists[FD_PW].view();
-        tbegin(FUNDEM_T_BROAD);
-        fd::launch_broad_pw(Pv, G, Wv, GW, wgrid, Lpw, flags.p, probe, stream,
-                            wall_groups.empty() ? nullptr : d_wall_groups.p, pc ? pcv.skin : 0.0,
-                            pc ? pcv.ctrl : nullptr);
-        tend(FUNDEM_T_BROAD);
-        tbegin(FUNDEM_T_NARROW_PW);
-        a.rec = recording ? recording->rec(FD_PW, record_step) : fd::AdjRec{};
-        {
-            // the particle-wall list shares the cache (wall drifts and cells
-            // in its rebuild flag)
-            fd::StepArgs aw = a;
-            if (pc) {
-                aw.skin = pcv.skin;
-                aw.gate = pcv.ctrl;
-                aw.drift = pcv.drift;
-                aw.disp = pcv.disp;
-                aw.driftB = pcv.wdrift;
-                aw.dispB = pcv.wdisp;
-            }
-            fd::launch_narrow(FD_PW, Pv, G, M, Wv, GW, MW, pgrid, wgrid, nullptr, Lpw, aw, with_force, mixed(),
-                              stream);
-        }
-        if (pc && W.n_dev > 0) fd::launch_pair_cache_commit_walls(Wv, pcv, stream);
-        if (recording)
-            FD_CUDA(cudaMemcpyAsync(recording->ns(FD_PW, record_step), Lpw.n_slots, sizeof(int),
-                                    cudaMemcpyDeviceToDevice, stream));
-        tend(FUNDEM_T_NARROW_PW);
+        if (branches) FD_CUDA(cudaStreamWaitEvent(stream, br_join[1], 0));
+        else wall_stage(stream);
         if (img_branch) {
             // the image detection ran beside; its wrapped positions replace
             // the ones the particle and wall lists were detected with
-            FD_CUDA(cudaStreamWaitEvent(stream, img_join, 0));
+            FD_CUDA(cudaStreamWaitEvent(stream, br_join[0], 0));
             if (img_wrapped && Pv.n > 0)
                 FD_CUDA(cudaMemcpyAsync(Pv.pos, img_pos.p, sizeof(double3) * Pv.n, cudaMemcpyDeviceToDevice, stream));
         } else if (perX || perY || sector) {
             image_stage(stream, Pv, nullptr);
         }
-        if (pc) {
+        auto pc_end = [&] {
+            if (!pc) return;
             PairListDev gl[4];
             int ng = 0;
             gl[ng++] = Lpw;
             for (int d = 0; d < 3 && pcg; ++d)
                 if (ghosts[d].active) gl[ng++] = Lg[d];
             fd::launch_pair_cache_end(pcv, gl, ng, stream);
-        }
+        };
         if (!with_force) {
+            pc_end();
             FD_CUDA(cudaGetLastError());
             return;
         }
@@ -1357,7 +1377,15 @@ struct fundem_sim {
         PairListDev views[FD_NKIND];
         for (int k = 0; k < FD_NKIND; ++k) views[k] = lists[k].view();
         fd::RevDev rv = rev_view();
-        fd::launch_reverse(Pv, views, active, rv, scan_tmp.p, scan_tmp.n, stream);
+        // the reverse index depends only on the lists' pairs: under the pair
+        // cache (without sector images, whose lists are detected afresh every
+        // step) a step that keeps them keeps the index.  The gate is the
+        // rebuild flag of the particle pairs, or of the image lists, which
+        // also rebuild with them.
+        const bool ghosts_cached = pcg && (ghosts[0].active || ghosts[1].active || ghosts[2].active);
+        const int* rev_gate = (pc && !sector && rev_valid) ? (ghosts_cached ? gctrl + 5 : pcv.ctrl) : nullptr;
+        fd::launch_reverse(Pv, views, active, rv, scan_tmp.p, scan_tmp.n, stream, rev_gate);
+        rev_valid = true;
         fd::BondDev bd = bond_view();
         if (recording && bd.n > 0) {
             bd.rec_active = recording->bond_active.p + (long long)record_step * bd.n;
@@ -1366,6 +1394,7 @@ struct fundem_sim {
         }
         if (bd.n > 0) fd::launch_bonds(Pv, bd, mixed(), stream);
         fd::launch_reduce(Pv, views, active, rv, bd, mixed(), stream);
+        pc_end();
 
         tend(FUNDEM_T_REDUCE);
         FD_CUDA(cudaGetLastError());

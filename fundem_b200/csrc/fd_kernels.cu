@@ -2373,6 +2373,7 @@ struct RevArgs {
     int active[REV_LISTS];
     RevDev R;
     int n_obj;
+    const int* gate;  // non-null: build only when *gate != 0
 };
 
 // the pair behind a flat index over the active lists
@@ -2390,6 +2391,7 @@ __device__ __forceinline__ bool rev_locate(const RevArgs& r, int idx, int& k, in
 
 __global__ void k_rev_count(RevArgs r)
 {
+    if (r.gate && *r.gate == 0) return;
     for (int idx = blockIdx.x * blockDim.x + threadIdx.x;; idx += gridDim.x * blockDim.x) {
         int k, p;
         if (!rev_locate(r, idx, k, p)) return;
@@ -2400,6 +2402,7 @@ __global__ void k_rev_count(RevArgs r)
 }
 __global__ void k_rev_fill(RevArgs r)
 {
+    if (r.gate && *r.gate == 0) return;
     for (int idx = blockIdx.x * blockDim.x + threadIdx.x;; idx += gridDim.x * blockDim.x) {
         int k, p;
         if (!rev_locate(r, idx, k, p)) return;
@@ -2415,7 +2418,7 @@ __global__ void k_rev_fill(RevArgs r)
 __global__ void k_rev_sort(RevArgs r)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= r.n_obj) return;
+    if (i >= r.n_obj || (r.gate && *r.gate == 0)) return;
     const int o = r.R.off[i];
     const int cnt = min(r.R.cnt[i], r.R.cap - o);
     int* seg = r.R.code + o;
@@ -2986,7 +2989,7 @@ void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& 
 }
 
 void launch_reverse(const ObjDev& P, PairListDev* lists, const int* active, RevDev& R, int* scan_tmp, size_t,
-                    cudaStream_t s)
+                    cudaStream_t s, const int* gate)
 {
     if (P.n <= 0) return;
     RevArgs r;
@@ -2996,11 +2999,16 @@ void launch_reverse(const ObjDev& P, PairListDev* lists, const int* active, RevD
     }
     r.R = R;
     r.n_obj = P.n;
-    cudaMemsetAsync(R.cnt, 0, sizeof(int) * P.n, s);
-    cudaMemsetAsync(R.fill, 0, sizeof(int) * P.n, s);
+    r.gate = gate;
+    if (gate) {
+        k_clear_cells<<<nblocks(P.n), TPB, 0, s>>>(R.cnt, R.fill, P.n, gate); note_launch();
+    } else {
+        cudaMemsetAsync(R.cnt, 0, sizeof(int) * P.n, s);
+        cudaMemsetAsync(R.fill, 0, sizeof(int) * P.n, s);
+    }
     const int g = 148 * 8;
     k_rev_count<<<g, TPB, 0, s>>>(r); note_launch();
-    scan_exclusive(R.cnt, R.off, P.n, scan_tmp, s);
+    scan_exclusive(R.cnt, R.off, P.n, scan_tmp, s, gate);
     k_rev_fill<<<g, TPB, 0, s>>>(r); note_launch();
     k_rev_sort<<<nblocks(P.n), TPB, 0, s>>>(r); note_launch();
 }

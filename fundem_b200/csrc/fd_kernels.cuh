@@ -392,8 +392,10 @@ void launch_broad_ghost(const ObjDev& P, const GeoSetDev& G, const GhostDev& Gh,
 void launch_narrow(int kind, const ObjDev& P, const GeoSetDev& G, const MatDev& M, const ObjDev& W,
                    const GeoSetDev& GW, const MatDev& MW, const FdGrid& pgrid, const FdGrid& wgrid,
                    const GhostDev* gh, PairListDev& L, const StepArgs& a, int with_force, bool mixed, cudaStream_t s);
+// gate (non-null): the index is rebuilt only when *gate != 0 (a step whose
+// lists keep their pairs keeps the index of the step that built them)
 void launch_reverse(const ObjDev& P, PairListDev* lists, const int* active, RevDev& R, int* scan_tmp,
-                    size_t scan_tmp_ints, cudaStream_t s);
+                    size_t scan_tmp_ints, cudaStream_t s, const int* gate = nullptr);
 // mixed: single-precision contact law, bond law and force sums
 void launch_bonds(const ObjDev& P, BondDev& B, bool mixed, cudaStream_t s);
 void launch_reduce(ObjDev& P, PairListDev* lists, const int* active, const RevDev& R, const BondDev& B, bool mixed,

@@ -57,3 +57,28 @@ def test_autotuner_leaves_the_fastest_shape(fundem):
     assert s.launch_shape() == tuple(d if v == 0 else v for v, d in zip(best, (4, 4, 4, 4)))
     s.sync()
     s.close()
+
+
+def test_autotuner_restart_runs_every_candidate_from_one_state(fundem):
+    """restart=True: each candidate starts from one checkpoint, so the
+    simulation ends `steps` steps after the state the tuner found, as an
+    uninterrupted run does."""
+    from fundem_b200 import autotune
+    sc = _slab(seed=5)
+    s = fundem.Simulation.from_scenario(sc, records=False)
+    s.detect()
+    s.step(20)
+    cands = ((0, 0, 0, 0), (8, 2, 2, 8))
+    best, times = autotune.launch_shape(s, steps=15, candidates=cands, restart=True)
+    assert set(times) == set(cands) and best == min(times, key=times.get)
+    s.sync()
+    r = fundem.Simulation.from_scenario(sc, records=False)
+    r.detect()
+    r.step(35)
+    r.sync()
+    ss, sr = s.state(), r.state()
+    for k in ("pos", "vel", "force", "torque"):
+        assert np.array_equal(ss[k], sr[k]), k
+    assert np.array_equal(keys(canonical(s.contacts(fundem.PP))), keys(canonical(r.contacts(fundem.PP))))
+    s.close()
+    r.close()
