@@ -1297,26 +1297,44 @@ struct fundem_sim {
             tend(FUNDEM_T_NARROW_PW);
         };
         // outside per-stage timing the wall list and the images (translated
-        // periodicity) run beside the particle-particle list.  Each branch
-        // reads and writes nothing another one writes: its own lists, tables
-        // and image arrays; the wall references of the pair cache (branch 1);
-        // the wrapped copy of the positions and the pair cache's words 4-7,
-        // which the others do not read (branch 0); the flags and counters
-        // with atomics.  The pair cache's rebuild flag (word 0) and drifts
-        // are written before the fork.
+        // periodicity) run beside the particle-particle list, and the bonds
+        // at the end of one of them.  Each branch reads and writes nothing
+        // another one writes: its own lists, tables and image arrays; the
+        // wall references of the pair cache (branch 1); the wrapped copy of
+        // the positions and the pair cache's words 4-7, which the others do
+        // not read (branch 0); the bond arrays (the branch that runs the
+        // bonds); the flags and counters with atomics.  The pair cache's
+        // rebuild flag (word 0) and drifts are written before the fork.
         const bool branches = br_stream[0] && br_stream[1] && (!profiling || capturing);
         const bool img_branch = branches && (perX || perY) && !sector && img_pos.p && img_pos.n >= (size_t)Pv.n;
+        // the bonds read only positions (after the wraps) and orientations:
+        // they run at the end of a branch, off the particle pairs' path
+        fd::BondDev bd = bond_view();
+        if (recording && bd.n > 0) {
+            bd.rec_active = recording->bond_active.p + (long long)record_step * bd.n;
+            bd.rec_rij = recording->bond_rij.p + 3ll * record_step * bd.n;
+            bd.rec_dn = recording->bond_dn.p + 3ll * record_step * bd.n;
+        }
+        bool bonds_done = false;
         if (branches) FD_CUDA(cudaEventRecord(br_fork, stream));
         if (img_branch) {
             FD_CUDA(cudaStreamWaitEvent(br_stream[0], br_fork, 0));
             ObjDev Pg = Pv;
             Pg.pos = img_pos.p;
             image_stage(br_stream[0], Pg, Pv.pos);
+            if (with_force && bd.n > 0) {
+                fd::launch_bonds(Pg, bd, mixed(), br_stream[0]);
+                bonds_done = true;
+            }
             FD_CUDA(cudaEventRecord(br_join[0], br_stream[0]));
         }
         if (branches) {
             FD_CUDA(cudaStreamWaitEvent(br_stream[1], br_fork, 0));
             wall_stage(br_stream[1]);
+            if (with_force && bd.n > 0 && !bonds_done && !(perX || perY || sector)) {
+                fd::launch_bonds(Pv, bd, mixed(), br_stream[1]);
+                bonds_done = true;
+            }
             FD_CUDA(cudaEventRecord(br_join[1], br_stream[1]));
         }
         PairListDev Lpp = lists[FD_PP].view();
@@ -1386,13 +1404,7 @@ struct fundem_sim {
         const int* rev_gate = (pc && !sector && rev_valid) ? (ghosts_cached ? gctrl + 5 : pcv.ctrl) : nullptr;
         fd::launch_reverse(Pv, views, active, rv, scan_tmp.p, scan_tmp.n, stream, rev_gate);
         rev_valid = true;
-        fd::BondDev bd = bond_view();
-        if (recording && bd.n > 0) {
-            bd.rec_active = recording->bond_active.p + (long long)record_step * bd.n;
-            bd.rec_rij = recording->bond_rij.p + 3ll * record_step * bd.n;
-            bd.rec_dn = recording->bond_dn.p + 3ll * record_step * bd.n;
-        }
-        if (bd.n > 0) fd::launch_bonds(Pv, bd, mixed(), stream);
+        if (bd.n > 0 && !bonds_done) fd::launch_bonds(Pv, bd, mixed(), stream);
         fd::launch_reduce(Pv, views, active, rv, bd, mixed(), stream);
         pc_end();
 
