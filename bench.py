@@ -459,13 +459,17 @@ def run_fundem(args, rank, world, dist):
         "contact_updates_per_s": world * 0.5 * (contacts + contacts_end) * args.steps / (t_max / 1e3),
         "pair_cache": {"skin_m": pc1[2], "rebuilds_in_timed_steps": pc1[0] - pc0[0],
                        "timed_steps": pc1[1] - pc0[1],
-                       "note": "candidate pairs and contact slots of the particle-particle list kept between "
-                               "rebuilds (a particle drifting half the skin rebuilds them); the exact FP64 "
-                               "node predicate runs on every slot every step"},
+                       "note": "candidate pairs and contact slots of the particle-particle, particle-wall and "
+                               "image lists kept between rebuilds (a particle drifting half the skin rebuilds "
+                               "them); on the steps between, the exact FP64 node predicate runs on every slot "
+                               "that a per-pair bound on the SDF's change since the rebuild does not rule out"},
         "kernel_ms_per_step": {k: v[0] / max(args.steps, 1) for k, v in kt.items()},
         "launch_shape": shape,
         "kernel_timing": "a second pass of K steps right after the headline, with CUDA-event timers on the "
-                         "simulation's stream around each kernel group",
+                         "simulation's stream around each kernel group (all stages on that one stream)",
+        "streams": "headline and plain launches: the particle-particle list on the simulation's stream; the "
+                   "particle-wall list and the image lists (with the bonds at the end of one of them) on two "
+                   "more streams, forked after the hash stage and joined before the force sums",
         "reference_gpu": ref_gpu,
         "narrow_work_per_step": {"pairs": wc[0] / wc_steps, "clusters": wc[1] / wc_steps,
                                  "clusters_kept": wc[2] / wc_steps, "node_contacts": wc[3] / wc_steps,
