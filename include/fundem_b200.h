@@ -43,7 +43,11 @@ const char* fundem_status_string(int status);
 
 /* LSSolver(dir, stream, maxGPUThread, device), kernel/LSSolver.h:14-21, and
    activateGPUDevice, LSSolver.h:601-613 (which calls exit(1) on failure;
-   this returns FUNDEM_ERR_CUDA).  stream may be NULL (the legacy stream). */
+   this returns FUNDEM_ERR_CUDA).  stream may be NULL (the legacy stream).
+   Every call's work is ordered on that stream; inside a step the simulation
+   forks the particle-wall and image detection onto two streams of its own
+   and joins them back before the force sums, so a call's work still ends on
+   the given stream. */
 int fundem_create(fundem_sim** out, int device, void* stream);
 int fundem_destroy(fundem_sim* sim);
 /* precision of the contact path.  FUNDEM_FP64 reproduces the reference.

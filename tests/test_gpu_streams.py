@@ -1,0 +1,58 @@
+"""The streams of a step.  After the hash stage the particle-wall list and,
+with translated periodicity, the image lists run on streams of their own
+beside the particle-particle list, with the bonds at the end of one of them;
+with the per-stage timers on (fundem_set_profiling) every stage runs on the
+simulation's stream in the reference's order (LSSolver.h:1201-1215 and
+:780-784: particle pairs, walls, wraps, images).  The branches share nothing
+they write, so both orders give the same run bit for bit, with plain
+launches and in graph replays, periodic (bonds on the image branch) or not
+(bonds on the wall branch)."""
+import dataclasses
+
+import numpy as np
+import pytest
+
+from conftest import canonical, keys
+
+pytestmark = pytest.mark.gpu
+
+
+def _slab(periodic):
+    from fundem_b200 import workloads
+    sim, sc, info = workloads.bonded_column(n=2048, footprint=(16, 16), seed=4, platen_speed=20.0)
+    sim.close()
+    if not periodic:
+        sc = dataclasses.replace(sc, periodic_x=False, periodic_y=False)
+    return sc
+
+
+def _run(fundem, sc, serial, graph, steps=60):
+    s = fundem.Simulation.from_scenario(sc, records=False)
+    s.set_profiling(serial)
+    s.detect()
+    if graph:
+        for _ in range(steps // 20):
+            s.step_graph(20)
+    else:
+        s.step(steps)
+    s.sync()
+    st = s.state()
+    lists = {k: canonical(s.contacts(k)) for k in (fundem.PP, fundem.PW, fundem.GX, fundem.GY, fundem.GXY)}
+    bonds = s.bonds()["activated"].copy()
+    s.close()
+    return st, lists, bonds
+
+
+@pytest.mark.parametrize("periodic", [True, False])
+def test_branches_match_the_serial_order(fundem, periodic):
+    sc = _slab(periodic)
+    ref = _run(fundem, sc, serial=True, graph=False)
+    assert sum(len(keys(c)) for c in ref[1].values()) > 1000
+    for graph in (False, True):
+        st, lists, bonds = _run(fundem, sc, serial=False, graph=graph)
+        for k in ("pos", "vel", "angvel", "quat", "force", "torque"):
+            assert np.array_equal(st[k], ref[0][k]), (graph, k)
+        for kind, c in lists.items():
+            assert np.array_equal(keys(c), keys(ref[1][kind])), (graph, kind)
+            assert np.array_equal(c["spring"], ref[1][kind]["spring"]), (graph, kind)
+        assert np.array_equal(bonds, ref[2]), graph
