@@ -119,10 +119,8 @@ __global__ void k_scan_add(int* out, long long n, const int* tile_off, const int
 // ---------------------------------------------------------------------------
 // integration, particleIntegrationKernel.cu:3-48 and myQua.h:77-93
 // ---------------------------------------------------------------------------
-__global__ void k_kick(ObjDev P, GeoSetDev G, double3 g, double h)
+__device__ __forceinline__ void kick_one(ObjDev& P, const GeoSetDev& G, double3 g, double h, int i)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.n) return;
     const int gi = P.geo[i];
     const FdGeo& geo = G.geo[gi];
     const double invM = geo.inv_mass;
@@ -132,6 +130,13 @@ __global__ void k_kick(ObjDev P, GeoSetDev G, double3 g, double h)
     const fd_quat q = P.q[i];
     const double3 Iw = fd_smv(fd_rot_tensor(q, geo.inertia), w);
     P.angvel[i] = w + fd_smv(fd_rot_tensor(q, geo.inv_inertia), P.torque[i] - cross3(w, Iw)) * h;
+}
+
+__global__ void k_kick(ObjDev P, GeoSetDev G, double3 g, double h)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.n) return;
+    kick_one(P, G, g, h, i);
 }
 
 __device__ __forceinline__ fd_quat quat_integrate(fd_quat q, double3 w, double dt)
@@ -146,12 +151,29 @@ __device__ __forceinline__ fd_quat quat_integrate(fd_quat q, double3 w, double d
     return fd_normalize_q(s);
 }
 
+__device__ __forceinline__ void drift_one(ObjDev& O, double dt, int i)
+{
+    O.pos[i] = O.pos[i] + dt * O.vel[i];
+    O.q[i] = quat_integrate(O.q[i], O.angvel[i], dt);
+}
+
 __global__ void k_drift(ObjDev O, double dt)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= O.n) return;
-    O.pos[i] = O.pos[i] + dt * O.vel[i];
-    O.q[i] = quat_integrate(O.q[i], O.angvel[i], dt);
+    drift_one(O, dt, i);
+}
+
+// the second half kick of one step, then the first half kick and the drift
+// of the next (no force is computed between them): one pass over the state
+// instead of three, each half kick the same arithmetic as k_kick's
+__global__ void k_kick_drift(ObjDev P, GeoSetDev G, double3 g, double h, double dt)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.n) return;
+    kick_one(P, G, g, h, i);
+    kick_one(P, G, g, h, i);
+    drift_one(P, dt, i);
 }
 
 // ---------------------------------------------------------------------------
@@ -2746,6 +2768,10 @@ void launch_kick(const ObjDev& P, const GeoSetDev& G, double3 gravity, double h,
 void launch_drift(const ObjDev& O, double dt, cudaStream_t s)
 {
     if (O.n > 0) { k_drift<<<nblocks(O.n), TPB, 0, s>>>(O, dt); note_launch(); }
+}
+void launch_kick_drift(const ObjDev& P, const GeoSetDev& G, double3 gravity, double h, double dt, cudaStream_t s)
+{
+    if (P.n > 0) { k_kick_drift<<<nblocks(P.n), TPB, 0, s>>>(P, G, gravity, h, dt); note_launch(); }
 }
 void launch_hash(const ObjDev& O, const FdGrid& g, cudaStream_t s)
 {

@@ -320,6 +320,9 @@ struct BondViewDev {
 // integration and hashing
 void launch_kick(const ObjDev& P, const GeoSetDev& G, double3 gravity, double h, cudaStream_t s);
 void launch_drift(const ObjDev& O, double dt, cudaStream_t s);
+// launch_kick(h), launch_kick(h) and launch_drift(dt) of the particles in one
+// pass: the end of one step and the start of the next
+void launch_kick_drift(const ObjDev& P, const GeoSetDev& G, double3 gravity, double h, double dt, cudaStream_t s);
 // cell hash of each object (-1 outside the grid) and its single-precision
 // rotation rows
 void launch_hash(const ObjDev& O, const FdGrid& g, cudaStream_t s);

@@ -56,3 +56,30 @@ def test_branches_match_the_serial_order(fundem, periodic):
             assert np.array_equal(keys(c), keys(ref[1][kind])), (graph, kind)
             assert np.array_equal(c["spring"], ref[1][kind]["spring"]), (graph, kind)
         assert np.array_equal(bonds, ref[2]), graph
+
+
+def test_fused_step_boundary_matches_the_hooked_steps(fundem):
+    """fundem_step and its graph run one step's second half kick with the
+    next step's first half kick and drift in one kernel (k_kick_drift); the
+    hooked form (fundem_step_begin / fundem_step_end) launches them one by
+    one.  Both give the same run bit for bit."""
+    sc = _slab(True)
+    runs = []
+    for form in ("hooked", "step", "graph"):
+        s = fundem.Simulation.from_scenario(sc, records=False)
+        s.detect()
+        if form == "hooked":
+            for _ in range(40):
+                s.step_begin()
+                s.step_end()
+        elif form == "step":
+            s.step(40)
+        else:
+            s.step_graph(20)
+            s.step_graph(20)
+        s.sync()
+        runs.append(s.state())
+        s.close()
+    for st in runs[1:]:
+        for k in ("pos", "vel", "angvel", "quat", "force", "torque"):
+            assert np.array_equal(st[k], runs[0][k]), k
