@@ -1682,25 +1682,45 @@ __global__ void __launch_bounds__(TPB) k_slot_filter(NarrowArgs n)
     const int nitems = min(*L.n_slots, L.cap_contacts);
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    const int stride = gridDim.x * blockDim.x;
-    // one atomic per block and pass over its TPB slots: a per-warp atomic on
-    // the one counter queued some 40,000 same-address atomics a step
-    __shared__ int w_count[TPB / 32];
+    // a block's pass covers SF_UNROLL * TPB slots (slot s0 + u * TPB + tid
+    // for u = 0 .. SF_UNROLL - 1), listed in slot order with one atomic: one
+    // slot per thread and pass spent a third of its issue slots waiting at
+    // the pass's barriers
+    constexpr int SF_UNROLL = 4;
+    constexpr int NW = TPB / 32;
+    const long long stride = (long long)gridDim.x * blockDim.x * SF_UNROLL;
+    __shared__ int w_count[SF_UNROLL * NW];
     __shared__ int b_base;
     int tested = 0, skipped = 0;
-    for (int s0 = blockIdx.x * blockDim.x; s0 < nitems; s0 += stride) {
-        const int s = s0 + threadIdx.x;
-        bool keep = false;
-        if (s < nitems) {
-            keep = !(L.c_phi0[s] > __fadd_ru(L.p_bound[L.c_pair[s]], 1e-12f));
-            if (!keep) L.c_node[s] = -1;
+    for (long long s0 = (long long)blockIdx.x * blockDim.x * SF_UNROLL; s0 < nitems; s0 += stride) {
+        int sl[SF_UNROLL], pr[SF_UNROLL];
+        bool in[SF_UNROLL];
+        float phi0[SF_UNROLL];
+#pragma unroll
+        for (int u = 0; u < SF_UNROLL; ++u) {
+            const long long t = s0 + u * TPB + threadIdx.x;
+            in[u] = t < nitems;
+            sl[u] = in[u] ? (int)t : 0;
+            pr[u] = in[u] ? L.c_pair[sl[u]] : 0;
+            phi0[u] = in[u] ? L.c_phi0[sl[u]] : 0.f;
         }
-        const unsigned int m = __ballot_sync(0xffffffffu, keep);
-        if (lane == 0) w_count[warp] = __popc(m);
+        unsigned int m[SF_UNROLL];
+#pragma unroll
+        for (int u = 0; u < SF_UNROLL; ++u) {
+            bool keep = false;
+            if (in[u]) {
+                keep = !(phi0[u] > __fadd_ru(L.p_bound[pr[u]], 1e-12f));
+                if (!keep) L.c_node[sl[u]] = -1;
+            }
+            m[u] = __ballot_sync(0xffffffffu, keep);
+            if (lane == 0) w_count[u * NW + warp] = __popc(m[u]);
+            tested += __popc(m[u]);
+            skipped += __popc(__ballot_sync(0xffffffffu, in[u])) - __popc(m[u]);
+        }
         __syncthreads();
         if (threadIdx.x == 0) {
             int total = 0;
-            for (int w = 0; w < TPB / 32; ++w) {
+            for (int w = 0; w < SF_UNROLL * NW; ++w) {
                 const int c = w_count[w];
                 w_count[w] = total;
                 total += c;
@@ -1708,10 +1728,11 @@ __global__ void __launch_bounds__(TPB) k_slot_filter(NarrowArgs n)
             b_base = total ? atomicAdd(L.n_test, total) : 0;
         }
         __syncthreads();
-        if (keep) L.c_test[b_base + w_count[warp] + __popc(m & ((1u << lane) - 1u))] = s;
+#pragma unroll
+        for (int u = 0; u < SF_UNROLL; ++u)
+            if ((m[u] >> lane) & 1u)
+                L.c_test[b_base + w_count[u * NW + warp] + __popc(m[u] & ((1u << lane) - 1u))] = sl[u];
         __syncthreads();
-        tested += __popc(m);
-        skipped += __popc(__ballot_sync(0xffffffffu, s < nitems)) - __popc(m);
     }
     if (n.a.stats && lane == 0) {
         if (tested) atomicAdd(&n.a.stats[5], (unsigned long long)tested);
