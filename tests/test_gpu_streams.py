@@ -26,8 +26,9 @@ def _slab(periodic):
     return sc
 
 
-def _run(fundem, sc, serial, graph, steps=60):
+def _run(fundem, sc, serial, graph, steps=60, cache=-1):
     s = fundem.Simulation.from_scenario(sc, records=False)
+    s.set_pair_cache(cache)
     s.set_profiling(serial)
     s.detect()
     if graph:
@@ -43,13 +44,15 @@ def _run(fundem, sc, serial, graph, steps=60):
     return st, lists, bonds
 
 
-@pytest.mark.parametrize("periodic", [True, False])
-def test_branches_match_the_serial_order(fundem, periodic):
+@pytest.mark.parametrize("periodic,cache", [(True, -1), (False, -1), (True, 1)])
+def test_branches_match_the_serial_order(fundem, periodic, cache):
+    """cache 1: the pair cache on at this size (slot filter, carried lists,
+    the reverse index kept between rebuilds)."""
     sc = _slab(periodic)
-    ref = _run(fundem, sc, serial=True, graph=False)
+    ref = _run(fundem, sc, serial=True, graph=False, cache=cache)
     assert sum(len(keys(c)) for c in ref[1].values()) > 1000
     for graph in (False, True):
-        st, lists, bonds = _run(fundem, sc, serial=False, graph=graph)
+        st, lists, bonds = _run(fundem, sc, serial=False, graph=graph, cache=cache)
         for k in ("pos", "vel", "angvel", "quat", "force", "torque"):
             assert np.array_equal(st[k], ref[0][k]), (graph, k)
         for kind, c in lists.items():
