@@ -560,7 +560,10 @@ class Simulation:
         return dict(min=mn, max=mx, inv_cell=inv, size=sz)
 
     def set_profiling(self, on, counters=False):
-        """Kernel-group timers (on) and narrow-phase work counters (counters)."""
+        """Kernel-group timers (on) and narrow-phase work counters (counters).
+        With the timers on, plain steps run every stage on the simulation's
+        stream (the same results bit for bit), so each group's time is its
+        own."""
         self._check(self.L.fundem_set_profiling(self.h, int(bool(on)) | (2 if counters else 0)), "set_profiling")
 
     def kernel_times(self):

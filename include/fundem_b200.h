@@ -378,9 +378,11 @@ enum {
     FUNDEM_T_INTEGRATE = 0, FUNDEM_T_HASH = 1, FUNDEM_T_BROAD = 2, FUNDEM_T_NARROW_PP = 3,
     FUNDEM_T_NARROW_PW = 4, FUNDEM_T_GHOST = 5, FUNDEM_T_REDUCE = 6, FUNDEM_NTIMERS = 7
 };
-/* on: FUNDEM_PROF_TIMERS times the kernel groups; FUNDEM_PROF_COUNTERS
-   also counts narrow-phase work (one shared-memory atomic per pair and a few
-   global atomics per block, so keep it out of timed runs); 0 turns both off */
+/* on: FUNDEM_PROF_TIMERS times the kernel groups (plain steps then run every
+   stage on the simulation's stream, so that each timer sees its own stage;
+   the results are the same bit for bit); FUNDEM_PROF_COUNTERS also counts
+   narrow-phase work (one shared-memory atomic per pair and a few global
+   atomics per block, so keep it out of timed runs); 0 turns both off */
 enum { FUNDEM_PROF_TIMERS = 1, FUNDEM_PROF_COUNTERS = 2 };
 int fundem_set_profiling(fundem_sim* sim, int on);
 int fundem_kernel_time(fundem_sim* sim, int group, double* ms_total, long long* count);
